@@ -1,0 +1,171 @@
+// World object: host mirrors of the registered bodies and shapes, device
+// buffers (structure-of-arrays, float4 streams), and the per-stage launchers.
+#pragma once
+
+#include "b3_internal.h"
+#include "hull.h"
+
+#include <vector>
+
+namespace b3 {
+
+// Device views passed by value to the kernels.
+struct BodiesDev {
+    int n;
+    float4* pos;
+    float4* quat;
+    float4* linVel;
+    float4* angVel;
+    const float* invMass;
+    const int* collidable;
+    const float* friction;
+    const float* restitution;
+    const float4* invInertia;  // local diagonal inverse inertia (xyz)
+    const int* worldId;
+};
+
+struct ShapesDev {
+    const b3Collidable* cols;
+    const b3ConvexPolyhedron* polys;
+    const float4* verts;
+    const b3Face* faces;
+    const int* indices;
+    const float4* edges;
+    const float4* localAabb;  // 2 per collidable (min, max)
+    int numPolys, numVerts, numFaces, numIndices, numEdges;
+    int tableBytes;           // packed size for shared-memory staging
+};
+
+struct SimParams {
+    float3 gravity;
+    float dt;
+    int iterations;
+    float erp;
+    float contactBreaking;
+    float contactProcessing;
+    float slopOffset;
+    float angularDamping;
+    int frictionCombine;
+};
+
+// Device buffers owned by a world.
+struct DevBuffers {
+    // bodies
+    float4 *pos = nullptr, *quat = nullptr, *linVel = nullptr, *angVel = nullptr;
+    float *invMass = nullptr, *friction = nullptr, *restitution = nullptr;
+    float4* invInertia = nullptr;
+    int *collidable = nullptr, *worldId = nullptr;
+    // shapes
+    b3Collidable* cols = nullptr;
+    b3ConvexPolyhedron* polys = nullptr;
+    float4* verts = nullptr;
+    b3Face* faces = nullptr;
+    int* indices = nullptr;
+    float4* edges = nullptr;
+    float4* localAabb = nullptr;
+    // broadphase
+    float4 *aabbMin = nullptr, *aabbMax = nullptr;
+    int* smallSlot = nullptr;      // body -> slot in the hash arrays, -1 = large
+    int* largeStart = nullptr;     // per world CSR over largeList
+    int* largeList = nullptr;
+    uint32_t *keys = nullptr, *vals = nullptr, *keysAlt = nullptr, *valsAlt = nullptr;
+    uint2* cellTable = nullptr;    // (stamp, first sorted index) per (world, cell)
+    int2* pairs = nullptr;
+    // narrowphase
+    b3Contact4* contacts = nullptr;   // one slot per pair
+    uint32_t* manifoldFlag = nullptr; // per pair: 1 if a manifold was emitted
+    uint32_t* manifoldScan = nullptr; // exclusive scan of the flags
+    int* manifoldPair = nullptr;      // manifold -> pair slot
+    // solver
+    uint32_t *incKeys = nullptr, *incVals = nullptr, *incKeysAlt = nullptr, *incValsAlt = nullptr;
+    uint32_t *bodyIncStart = nullptr, *bodyIncEnd = nullptr;
+    float4* rows = nullptr;           // constraint rows, see solver.cu
+    float4* manifoldHdr = nullptr;    // per manifold header
+    float4 *incLin = nullptr, *incAng = nullptr;   // per manifold side increments
+    float4 *avgLin = nullptr, *avgAng = nullptr;   // per body averaged delta velocity
+    // scalars (device): [0] numSmall, [1] numPairs, [2] numManifolds, [3] numInc,
+    // [4] stamp, [5] sort error flag, [6..7] barrier, [8] tile counter
+    int32_t* scalars = nullptr;
+    b3Counters* counters = nullptr;
+    void* sortScratch = nullptr;
+    size_t sortScratchBytes = 0;
+    void* incSortScratch = nullptr;
+    size_t incSortScratchBytes = 0;
+    void* scanScratch = nullptr;
+    size_t scanScratchBytes = 0;
+    float4* worldStats = nullptr;
+};
+
+enum ScalarSlot {
+    S_NUM_SMALL = 0,
+    S_NUM_PAIRS = 1,
+    S_NUM_MANIFOLDS = 2,
+    S_NUM_INC = 3,
+    S_STAMP = 4,
+    S_ERR = 5,
+    S_BAR_COUNT = 6,
+    S_BAR_GEN = 7,
+    S_TILE = 8,
+    S_NP_WORK = 9,
+    S_NUM_SCALARS = 16
+};
+
+}  // namespace b3
+
+struct b3World_t {
+    b3Context ctx = nullptr;
+    b3WorldConfig cfg{};
+    int cellBits = 0, worldBits = 0, keyBits = 0, bodyBits = 0;
+    float invCell = 1.f;
+
+    // host mirrors
+    std::vector<b3Body> bodies;
+    std::vector<b3Inertia> inertias;
+    std::vector<b3Collidable> cols;
+    std::vector<b3ConvexPolyhedron> polys;
+    std::vector<float> verts4, edges4, localAabb8;
+    std::vector<b3Face> faces;
+    std::vector<int> indices;
+    std::vector<int> worldIds;
+    std::vector<float> regAabb;   // registration AABB per body (6 floats)
+    std::vector<int> smallSlotHost, largeStartHost, largeListHost;
+    int numSmall = 0;
+    int capBodies = 0;   // allocated body capacity on device
+    int capInc = 0;
+    bool written = false;
+    bool shapesDirty = true;
+
+    b3::DevBuffers d;
+    b3::SimParams sim{};
+
+    // CUDA graph of one step
+    cudaGraphExec_t graphExec = nullptr;
+    cudaStream_t graphStream = nullptr;
+    bool graphValid = false;
+
+    // stage timing
+    bool timing = false;
+    std::vector<float> stageMs;
+
+    // tunables (autotuner)
+    int npWarpsPerBlock = 4;   // narrowphase warps per CTA
+    int pairThreads = 128;     // pair-search CTA size
+    int solverThreads = 256;   // Jacobi CTA size
+
+    int cooperativeOk = 1;
+
+    b3::BodiesDev bodiesDev() const;
+    b3::ShapesDev shapesDev() const;
+};
+
+namespace b3 {
+// stage launchers (world.cu / broadphase.cu / narrowphase.cu / solver.cu)
+int launch_aabb_hash(b3World_t* w, cudaStream_t st);
+int launch_sort_and_cells(b3World_t* w, cudaStream_t st);
+int launch_find_pairs(b3World_t* w, cudaStream_t st);
+int launch_narrowphase(b3World_t* w, cudaStream_t st);
+int launch_manifolds(b3World_t* w, cudaStream_t st);
+int launch_solver(b3World_t* w, cudaStream_t st);
+int launch_integrate(b3World_t* w, cudaStream_t st);
+int launch_world_stats(b3World_t* w, cudaStream_t st);
+}  // namespace b3

@@ -1,0 +1,568 @@
+// Contact-to-constraint setup, Jacobi contact/friction solver with velocity
+// averaging, and transform integration, for sm_100a.
+//
+// Solver semantics are btPgsJacobiSolver with usePgs = false
+// (P2/btPgsJacobiSolver.cpp:35), as solveContacts configures it (:171-191):
+// 10 iterations, splitImpulse off, erp 0.2, linearSlop 0, solver mode
+// WARMSTARTING | SIMD | USE_2_FRICTION_DIRECTIONS (btContactSolverInfo.h:72-90
+// defaults plus :180), which means
+//   * one solver-body copy per (manifold, dynamic body); a static body is a
+//     single shared solver body with zero inverse mass (getOrInitSolverBody
+//     :689-722); m_bodyCount[b] = number of manifolds touching b (:1105-1129)
+//   * per point (skipped if depth + 0.01 > 0.02, :124-155 and :961):
+//     normal row (setupContactConstraint :725-888) with Baumgarte rhs and the
+//     count-scaled denominator relaxation/(d0*countA + d1*countB), then two
+//     friction rows, direction 2 first, along the relative tangential velocity
+//     when its squared length exceeds FLT_EPSILON, else btPlaneSpace1(n)
+//     (convertContact :933-1080, setupFrictionConstraint :505-592)
+//   * inverse inertia used by the rows is the body's local diagonal inverse
+//     inertia (getInvInertiaTensorWorld returns m_initInvInertia, :51-66)
+//   * each iteration: all normal rows (lower limit 0), averageVelocities,
+//     all friction rows clamped to +-mu*lambda_n (skipped while lambda_n <= 0),
+//     averageVelocities (solveSingleIteration :1372-1614,
+//     solveGroupCacheFriendlyIterations :1656-1681, averageVelocities :1683-1720)
+//   * finish: every copy of a dynamic body adds sum/count to the body
+//     velocity (solveGroupCacheFriendlyFinish :1790-1803), so a body with k
+//     copies receives k times the averaged delta.
+// Impulses reach every solver body (the SIMD row solvers used by this
+// solver mode have no per-body guard).
+//
+// B200 mapping: rows within a copy are Gauss-Seidel, copies are independent,
+// so one thread owns one manifold and solves its rows in order, keeping the
+// two copies' delta velocities in registers. The per-body average is a
+// deterministic segmented sum over the body's copies in manifold order (the
+// copy list is a stable radix sort of (body, copy) entries). All 4 phases x
+// iterations run in one persistent cooperative kernel separated by a grid
+// barrier whose wait is bounded. Rows are stored structure-of-arrays
+// (row slot major) so each phase streams them with coalesced float4 loads.
+#include "b3_math.cuh"
+#include "b3_world.h"
+
+#include <cfloat>
+
+using namespace b3m;
+
+namespace {
+
+// Row storage: kRowSlots float4 streams of length maxManifolds.
+//  slot 0..3   header: (A,B,nRows,flags as int), (invMassA, invMassB, mu, -),
+//              (invInertiaA.xyz, countA), (invInertiaB.xyz, countB)
+//  normal row j (j<4):   4 + 3j + {0,1,2}
+//  friction row r (r<8): 16 + 3r + {0,1,2}; r = 2j + {0: dir2, 1: dir1}
+//  each row: (n.xyz, rhs), (r1xn.xyz, jacDiagABInv), (r2xn.xyz, applied)
+constexpr int kNormal0 = 4;
+constexpr int kFric0 = 16;
+
+struct SolverView {
+    float4* rows;       // [kRowSlots][cap]
+    int cap;            // manifold capacity (stride)
+    float4* copyLin;    // [2][cap]
+    float4* copyAng;    // [2][cap]
+    float4* avgLin;     // [N]
+    float4* avgAng;     // [N]
+    const uint32_t* incVals;   // sorted copy ids (2m + side)
+    const uint32_t* incStart;  // per body
+    const uint32_t* incEnd;
+    const int32_t* numManifolds;
+    int numBodies;
+};
+
+__device__ __forceinline__ float4& R(const SolverView& v, int slot, int m) {
+    return v.rows[(size_t)slot * v.cap + m];
+}
+
+// btPlaneSpace1 (LinearMath/btVector3.h), published construction of two
+// unit tangents orthogonal to n.
+__device__ __forceinline__ void plane_space(float3 n, float3& p, float3& q) {
+    const float SQRT12 = 0.7071067811865475244008443621048490f;
+    if (fabsf(n.z) > SQRT12) {
+        const float a = n.y * n.y + n.z * n.z;
+        const float k = rsqrtf(a);
+        p = make_float3(0.f, -n.z * k, n.y * k);
+        q = make_float3(a * k, -n.x * p.z, n.x * p.y);
+    } else {
+        const float a = n.x * n.x + n.y * n.y;
+        const float k = rsqrtf(a);
+        p = make_float3(-n.y * k, n.x * k, 0.f);
+        q = make_float3(-n.z * p.y, n.z * p.x, a * k);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Manifold compaction: manifold index = exclusive scan of per-pair flags.
+// ---------------------------------------------------------------------------
+__global__ void k_manifold_emit(const uint32_t* __restrict__ flag, const uint32_t* __restrict__ scan,
+                                const int32_t* __restrict__ numPairsDev,
+                                const b3Contact4* __restrict__ contacts, const float* __restrict__ invMass,
+                                int numBodies, int* __restrict__ manifoldPair,
+                                uint32_t* __restrict__ incKeys, uint32_t* __restrict__ incVals,
+                                int32_t* __restrict__ scalars, b3Counters* __restrict__ counters) {
+    const int np = *numPairsDev;
+    const int M = scalars[b3::S_NUM_MANIFOLDS];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        scalars[b3::S_NUM_INC] = 2 * M;
+        counters->numManifolds = M;
+    }
+    int pts = 0;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < np; p += gridDim.x * blockDim.x) {
+        if (!flag[p]) continue;
+        const int m = (int)scan[p];
+        manifoldPair[m] = p;
+        const b3Contact4& c = contacts[p];
+        const int a = abs(c.bodyAPtrAndSignBit), b = abs(c.bodyBPtrAndSignBit);
+        // copies exist for dynamic bodies only; static ones get the
+        // out-of-range key numBodies and sort past every body
+        incKeys[2 * m] = invMass[a] != 0.f ? (uint32_t)a : (uint32_t)numBodies;
+        incVals[2 * m] = 2u * m;
+        incKeys[2 * m + 1] = invMass[b] != 0.f ? (uint32_t)b : (uint32_t)numBodies;
+        incVals[2 * m + 1] = 2u * m + 1u;
+        pts += (int)c.worldNormal[3];
+    }
+    if (pts) atomicAdd(&counters->numContactPoints, pts);
+}
+
+__global__ void k_body_ranges(const uint32_t* __restrict__ keys, const int32_t* __restrict__ nDev,
+                              uint32_t* __restrict__ start, uint32_t* __restrict__ end, int numBodies) {
+    const int n = *nDev;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t k = keys[i];
+        if (k >= (uint32_t)numBodies) continue;
+        if (i == 0 || keys[i - 1] != k) start[k] = (uint32_t)i;
+        if (i == n - 1 || keys[i + 1] != k) end[k] = (uint32_t)(i + 1);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Constraint setup (one thread per manifold)
+// ---------------------------------------------------------------------------
+struct SetupParams {
+    float dt;
+    float erp;
+    float contactProcessing;
+    float slopOffset;
+};
+
+__device__ __forceinline__ void setup_friction_row(const SolverView& V, int slot, int m, float3 dir,
+                                                   float3 r1, float3 r2, float imA, float imB,
+                                                   float3 iiA, float3 iiB, float cA, float cB,
+                                                   float3 vA, float3 wA, float3 vB, float3 wB) {
+    const float3 t1 = cross(r1, dir);
+    const float3 t2 = cross(r2, -dir);
+    const float3 angA = mulv(iiA, t1);
+    const float3 angB = mulv(iiB, t2);
+    const float d0 = imA + dot(dir, cross(angA, r1));
+    const float d1 = imB + dot(dir, cross(-angB, r2));
+    const float denom = 1.f / (d0 + d1);
+    const float scaled = 1.f / (d0 * cA + d1 * cB);
+    const float relv = (dot(dir, vA) + dot(t1, wA)) + (-dot(dir, vB) + dot(t2, wB));
+    const float rhs = (0.f - relv) * scaled;
+    R(V, slot + 0, m) = make_float4(dir.x, dir.y, dir.z, rhs);
+    R(V, slot + 1, m) = make_float4(t1.x, t1.y, t1.z, denom);
+    R(V, slot + 2, m) = make_float4(t2.x, t2.y, t2.z, 0.f);
+}
+
+__global__ void k_setup_rows(b3::BodiesDev Bd, SolverView V, const int* __restrict__ manifoldPair,
+                             const b3Contact4* __restrict__ contacts, SetupParams SP) {
+    const int M = *V.numManifolds;
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
+        const b3Contact4 c = contacts[manifoldPair[m]];
+        const int A = abs(c.bodyAPtrAndSignBit), B = abs(c.bodyBPtrAndSignBit);
+        const float imA = Bd.invMass[A], imB = Bd.invMass[B];
+        const bool dynA = imA != 0.f, dynB = imB != 0.f;
+        const float kA = dynA ? (float)(V.incEnd[A] - V.incStart[A]) : 1.f;
+        const float kB = dynB ? (float)(V.incEnd[B] - V.incStart[B]) : 1.f;
+        const float3 iiA = dynA ? f3(Bd.invInertia[A]) : make_float3(0.f, 0.f, 0.f);
+        const float3 iiB = dynB ? f3(Bd.invInertia[B]) : make_float3(0.f, 0.f, 0.f);
+        const float3 pA = f3(Bd.pos[A]), pB = f3(Bd.pos[B]);
+        // solver body velocities (static bodies contribute zero)
+        const float3 vA = dynA ? f3(Bd.linVel[A]) : make_float3(0.f, 0.f, 0.f);
+        const float3 wA = dynA ? f3(Bd.angVel[A]) : make_float3(0.f, 0.f, 0.f);
+        const float3 vB = dynB ? f3(Bd.linVel[B]) : make_float3(0.f, 0.f, 0.f);
+        const float3 wB = dynB ? f3(Bd.angVel[B]) : make_float3(0.f, 0.f, 0.f);
+        const float restitution = Bd.restitution[A] * Bd.restitution[B];
+        const float mu = c.friction;
+        int nRows = 0;
+        const int npts = (int)c.worldNormal[3];
+        const bool solve = dynA || dynB;
+        float3 n = normalize(make_float3(-c.worldNormal[0], -c.worldNormal[1], -c.worldNormal[2]));
+        for (int j = 0; j < npts && solve; ++j) {
+            const float depth = c.worldPos[j][3];
+            const float dist = depth + SP.slopOffset;
+            if (!(dist <= SP.contactProcessing)) continue;
+            const float3 posB = make_float3(c.worldPos[j][0], c.worldPos[j][1], c.worldPos[j][2]);
+            const float3 posA = posB + n * dist;
+            const float3 r1 = posA - pA;
+            const float3 r2 = posB - pB;
+            const float3 t0 = cross(r1, n);
+            const float3 t1 = cross(r2, n);
+            const float3 angA = mulv(iiA, t0);
+            const float3 angB = mulv(iiB, -t1);
+            const float d0 = imA + dot(n, cross(angA, r1));
+            const float d1 = imB + dot(n, cross(-angB, r2));
+            const float denom = 1.f / (d0 + d1);
+            const float scaled = 1.f / (d0 * kA + d1 * kB);
+            const float penetration = dist;  // + linearSlop (0)
+            const float3 vel1 = vA + cross(wA, r1);
+            const float3 vel2 = vB + cross(wB, r2);
+            const float3 vel = vel1 - vel2;
+            const float relv0 = dot(n, vel);
+            float rest = restitution * -relv0;
+            if (rest <= 0.f) rest = 0.f;
+            const float v1n = dot(n, vA) + dot(t0, wA);
+            const float v2n = -dot(n, vB) + dot(-t1, wB);
+            const float relv = v1n + v2n;
+            float posErr = 0.f;
+            float velErr = rest - relv;
+            if (penetration > 0.f) {
+                velErr -= penetration / SP.dt;
+            } else {
+                posErr = -penetration * SP.erp / SP.dt;
+            }
+            const float rhs = posErr * scaled + velErr * scaled;
+            const int s = kNormal0 + 3 * nRows;
+            R(V, s + 0, m) = make_float4(n.x, n.y, n.z, rhs);
+            R(V, s + 1, m) = make_float4(t0.x, t0.y, t0.z, denom);
+            R(V, s + 2, m) = make_float4(-t1.x, -t1.y, -t1.z, 0.f);
+            // friction directions (convertContact :1015-1049)
+            float3 d1v = vel - n * relv0;
+            const float lat = dot(d1v, d1v);
+            float3 d2v;
+            if (lat > FLT_EPSILON) {
+                d1v = d1v * (1.f / sqrtf(lat));
+                d2v = normalize(cross(d1v, n));
+            } else {
+                plane_space(n, d1v, d2v);
+            }
+            const int fs = kFric0 + 3 * (2 * nRows);
+            setup_friction_row(V, fs, m, d2v, r1, r2, imA, imB, iiA, iiB, kA, kB, vA, wA, vB, wB);
+            setup_friction_row(V, fs + 3, m, d1v, r1, r2, imA, imB, iiA, iiB, kA, kB, vA, wA, vB, wB);
+            ++nRows;
+        }
+        R(V, 0, m) = make_float4(__int_as_float(A), __int_as_float(B), __int_as_float(nRows),
+                                 __int_as_float((dynA ? 1 : 0) | (dynB ? 2 : 0)));
+        R(V, 1, m) = make_float4(imA, imB, mu, 0.f);
+        R(V, 2, m) = make_float4(iiA.x, iiA.y, iiA.z, kA);
+        R(V, 3, m) = make_float4(iiB.x, iiB.y, iiB.z, kB);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Persistent Jacobi kernel
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool grid_barrier(uint32_t* count, uint32_t* gen, uint32_t nblocks,
+                                             int32_t* err, b3Counters* counters) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ok = 1;
+        const uint32_t g = b3dev::ld_acquire_u32(gen);
+        __threadfence();
+        const uint32_t arrived = atomicAdd(count, 1u);
+        if (arrived == nblocks - 1) {
+            atomicExch(count, 0u);
+            __threadfence();
+            b3dev::st_release_u32(gen, g + 1u);
+        } else {
+            int spins = 0;
+            while (b3dev::ld_acquire_u32(gen) == g) {
+                if (++spins > b3dev::kSpinLimit) {
+                    atomicExch(err, 1);
+                    atomicAdd(&counters->timeouts, 1);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        if (*(volatile int32_t*)err) ok = 0;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+__device__ __forceinline__ void solve_row(const float4 r0, const float4 r1, float4& r2, float lo, float hi,
+                                          float imA, float imB, float3 iiA, float3 iiB,
+                                          float3& dvA, float3& dwA, float3& dvB, float3& dwB) {
+    const float3 n = f3(r0), t1 = f3(r1), t2 = f3(r2);
+    const float rhs = r0.w, jac = r1.w, applied = r2.w;
+    float delta = rhs;  // - applied * cfm (cfm = 0)
+    const float dv1 = dot(n, dvA) + dot(t1, dwA);
+    const float dv2 = -dot(n, dvB) + dot(t2, dwB);
+    delta -= dv1 * jac;
+    delta -= dv2 * jac;
+    const float sum = applied + delta;
+    float na;
+    if (sum < lo) {
+        delta = lo - applied;
+        na = lo;
+    } else if (sum > hi) {
+        delta = hi - applied;
+        na = hi;
+    } else {
+        na = sum;
+    }
+    r2.w = na;
+    dvA += n * (imA * delta);
+    dwA += mulv(iiA, t1) * delta;
+    dvB += (-n * imB) * delta;
+    dwB += mulv(iiB, t2) * delta;
+}
+
+__device__ void manifold_phase(const SolverView& V, int M, bool friction) {
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
+        const float4 h0 = R(V, 0, m);
+        const int nRows = __float_as_int(h0.z);
+        if (nRows == 0) continue;
+        const int A = __float_as_int(h0.x), B = __float_as_int(h0.y);
+        const int dyn = __float_as_int(h0.w);
+        const float4 h1 = R(V, 1, m);
+        const float4 h2 = R(V, 2, m);
+        const float4 h3 = R(V, 3, m);
+        const float imA = h1.x, imB = h1.y, mu = h1.z;
+        const float3 iiA = f3(h2), iiB = f3(h3);
+        float3 dvA = make_float3(0.f, 0.f, 0.f), dwA = dvA, dvB = dvA, dwB = dvA;
+        if (dyn & 1) { dvA = f3(V.avgLin[A]); dwA = f3(V.avgAng[A]); }
+        if (dyn & 2) { dvB = f3(V.avgLin[B]); dwB = f3(V.avgAng[B]); }
+        if (!friction) {
+            for (int j = 0; j < nRows; ++j) {
+                const int s = kNormal0 + 3 * j;
+                const float4 r0 = R(V, s, m), r1 = R(V, s + 1, m);
+                float4 r2 = R(V, s + 2, m);
+                solve_row(r0, r1, r2, 0.f, 1e10f, imA, imB, iiA, iiB, dvA, dwA, dvB, dwB);
+                R(V, s + 2, m).w = r2.w;
+            }
+        } else {
+            for (int j = 0; j < nRows; ++j) {
+                const float total = R(V, kNormal0 + 3 * j + 2, m).w;
+                if (!(total > 0.f)) continue;
+                const float lim = mu * total;
+                for (int q = 0; q < 2; ++q) {
+                    const int s = kFric0 + 3 * (2 * j + q);
+                    const float4 r0 = R(V, s, m), r1 = R(V, s + 1, m);
+                    float4 r2 = R(V, s + 2, m);
+                    solve_row(r0, r1, r2, -lim, lim, imA, imB, iiA, iiB, dvA, dwA, dvB, dwB);
+                    R(V, s + 2, m).w = r2.w;
+                }
+            }
+        }
+        if (dyn & 1) {
+            V.copyLin[m] = f4(dvA);
+            V.copyAng[m] = f4(dwA);
+        }
+        if (dyn & 2) {
+            V.copyLin[V.cap + m] = f4(dvB);
+            V.copyAng[V.cap + m] = f4(dwB);
+        }
+    }
+}
+
+// Copies whose manifold had no rows keep the body's average.
+__device__ void average_phase(const SolverView& V) {
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < V.numBodies; b += gridDim.x * blockDim.x) {
+        const uint32_t s = V.incStart[b], e = V.incEnd[b];
+        if (e <= s) continue;
+        const float4 prevL = V.avgLin[b], prevA = V.avgAng[b];
+        float3 sl = make_float3(0.f, 0.f, 0.f), sa = sl;
+        for (uint32_t i = s; i < e; ++i) {
+            const uint32_t cid = V.incVals[i];
+            const int m = (int)(cid >> 1), side = (int)(cid & 1u);
+            const int nRows = __float_as_int(R(V, 0, m).z);
+            if (nRows == 0) {
+                sl += f3(prevL);
+                sa += f3(prevA);
+            } else {
+                sl += f3(V.copyLin[(size_t)side * V.cap + m]);
+                sa += f3(V.copyAng[(size_t)side * V.cap + m]);
+            }
+        }
+        const float factor = 1.f / (float)(e - s);
+        V.avgLin[b] = f4(sl * factor);
+        V.avgAng[b] = f4(sa * factor);
+    }
+}
+
+__global__ void __launch_bounds__(256)
+k_jacobi(SolverView V, int iterations, uint32_t* bar, int32_t* err, b3Counters* counters) {
+    const int M = *V.numManifolds;
+    const uint32_t nb = gridDim.x;
+    // zero the averaged deltas
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < V.numBodies; b += gridDim.x * blockDim.x) {
+        V.avgLin[b] = make_float4(0.f, 0.f, 0.f, 0.f);
+        V.avgAng[b] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    if (!grid_barrier(bar, bar + 1, nb, err, counters)) return;
+    for (int it = 0; it < iterations; ++it) {
+        manifold_phase(V, M, false);
+        if (!grid_barrier(bar, bar + 1, nb, err, counters)) return;
+        average_phase(V);
+        if (!grid_barrier(bar, bar + 1, nb, err, counters)) return;
+        manifold_phase(V, M, true);
+        if (!grid_barrier(bar, bar + 1, nb, err, counters)) return;
+        average_phase(V);
+        if (!grid_barrier(bar, bar + 1, nb, err, counters)) return;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Integration (copyVelocitiesKernel + integrateTransformsKernel2)
+// ---------------------------------------------------------------------------
+struct IntegrateParams {
+    float dt;
+    float damping;
+    float threshold;  // BT_GPU_ANGULAR_MOTION_THRESHOLD = 0.25 * pi
+};
+
+__global__ void k_integrate(b3::BodiesDev Bd, const float4* __restrict__ avgLin,
+                            const float4* __restrict__ avgAng, const uint32_t* __restrict__ incStart,
+                            const uint32_t* __restrict__ incEnd, IntegrateParams P, int applySolve) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= Bd.n) return;
+    if (Bd.invMass[i] == 0.f) return;
+    float4 v = Bd.linVel[i];
+    float4 w = Bd.angVel[i];
+    if (applySolve) {
+        const uint32_t k = incEnd[i] - incStart[i];
+        if (incEnd[i] > incStart[i]) {
+            const float4 sl = avgLin[i], sa = avgAng[i];
+            for (uint32_t c = 0; c < k; ++c) {
+                v.x += sl.x; v.y += sl.y; v.z += sl.z;
+                w.x += sa.x; w.y += sa.y; w.z += sa.z;
+            }
+        }
+    }
+    v.w = 0.f;
+    w.x *= P.damping;
+    w.y *= P.damping;
+    w.z *= P.damping;
+    w.w = 0.f;
+    float fAngle = sqrtf(w.x * w.x + w.y * w.y + w.z * w.z);
+    if (fAngle * P.dt > P.threshold) fAngle = P.threshold / P.dt;
+    float s;
+    if (fAngle < 0.001f) {
+        s = 0.5f * P.dt - (P.dt * P.dt * P.dt) * 0.020833333333f * fAngle * fAngle;
+    } else {
+        s = sinf(0.5f * fAngle * P.dt) / fAngle;
+    }
+    const float4 dorn = make_float4(w.x * s, w.y * s, w.z * s, cosf(fAngle * P.dt * 0.5f));
+    const float4 q0 = Bd.quat[i];
+    float4 q = quat_mult(dorn, q0);
+    const float len = sqrtf(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w);
+    if (len > 0.f) {
+        const float il = 1.f / len;
+        q.x *= il; q.y *= il; q.z *= il; q.w *= il;
+    } else {
+        q = make_float4(0.f, 0.f, 0.f, 1.f);
+    }
+    float4 p = Bd.pos[i];
+    p.x += v.x * P.dt;
+    p.y += v.y * P.dt;
+    p.z += v.z * P.dt;
+    Bd.pos[i] = p;
+    Bd.quat[i] = q;
+    Bd.linVel[i] = v;
+    Bd.angVel[i] = w;
+}
+
+SolverView solver_view(b3World_t* w) {
+    SolverView V;
+    V.rows = w->d.rows;
+    V.cap = w->cfg.maxPairs;
+    V.copyLin = w->d.incLin;
+    V.copyAng = w->d.incAng;
+    V.avgLin = w->d.avgLin;
+    V.avgAng = w->d.avgAng;
+    V.incVals = w->d.incVals;
+    V.incStart = w->d.bodyIncStart;
+    V.incEnd = w->d.bodyIncEnd;
+    V.numManifolds = w->d.scalars + b3::S_NUM_MANIFOLDS;
+    V.numBodies = (int)w->bodies.size();
+    return V;
+}
+
+}  // namespace
+
+namespace b3 {
+
+int launch_manifolds(b3World_t* w, cudaStream_t st) {
+    const int N = (int)w->bodies.size();
+    const int cap = w->cfg.maxPairs;
+    B3_CUDA(cudaMemsetAsync(w->d.scalars + S_NUM_MANIFOLDS, 0, sizeof(int32_t) * 2, st));
+    B3_CUDA(cudaMemsetAsync(w->d.bodyIncStart, 0, sizeof(uint32_t) * N, st));
+    B3_CUDA(cudaMemsetAsync(w->d.bodyIncEnd, 0, sizeof(uint32_t) * N, st));
+    if (cap == 0 || N == 0) return B3_OK;
+    B3_TRY(exclusive_scan_u32(w->d.manifoldFlag, w->d.manifoldScan, w->d.scalars + S_NUM_PAIRS, cap,
+                              (uint32_t*)(w->d.scalars + S_NUM_MANIFOLDS), w->d.scanScratch,
+                              w->d.scanScratchBytes, w->d.scalars + S_ERR, st, w->ctx->numSMs));
+    const int g = w->ctx->numSMs * 8;
+    k_manifold_emit<<<g, 256, 0, st>>>(w->d.manifoldFlag, w->d.manifoldScan, w->d.scalars + S_NUM_PAIRS,
+                                      w->d.contacts, w->d.invMass, N, w->d.manifoldPair, w->d.incKeys,
+                                      w->d.incVals, w->d.scalars, w->d.counters);
+    B3_CHECK_LAUNCH();
+    bool alt = false;
+    B3_TRY(radix_sort_pairs(w->d.incKeys, w->d.incVals, w->d.incKeysAlt, w->d.incValsAlt,
+                            w->d.scalars + S_NUM_INC, 2LL * cap, w->bodyBits, w->d.incSortScratch,
+                            w->d.incSortScratchBytes, w->d.scalars + S_ERR, st, &alt, w->ctx->numSMs));
+    if (alt) {
+        B3_CUDA(cudaMemcpyAsync(w->d.incKeys, w->d.incKeysAlt, sizeof(uint32_t) * 2 * (size_t)cap,
+                                cudaMemcpyDeviceToDevice, st));
+        B3_CUDA(cudaMemcpyAsync(w->d.incVals, w->d.incValsAlt, sizeof(uint32_t) * 2 * (size_t)cap,
+                                cudaMemcpyDeviceToDevice, st));
+    }
+    k_body_ranges<<<g, 256, 0, st>>>(w->d.incKeys, w->d.scalars + S_NUM_INC, w->d.bodyIncStart,
+                                    w->d.bodyIncEnd, N);
+    B3_CHECK_LAUNCH();
+    return B3_OK;
+}
+
+int launch_solver(b3World_t* w, cudaStream_t st) {
+    if (w->cfg.maxPairs == 0 || w->bodies.empty()) return B3_OK;
+    SolverView V = solver_view(w);
+    SetupParams SP;
+    SP.dt = w->sim.dt;
+    SP.erp = w->sim.erp;
+    SP.contactProcessing = w->sim.contactProcessing;
+    SP.slopOffset = w->sim.slopOffset;
+    const int g = w->ctx->numSMs * 8;
+    k_setup_rows<<<g, 128, 0, st>>>(w->bodiesDev(), V, w->d.manifoldPair, w->d.contacts, SP);
+    B3_CHECK_LAUNCH();
+    // persistent cooperative Jacobi
+    B3_CUDA(cudaMemsetAsync(w->d.scalars + S_BAR_COUNT, 0, sizeof(int32_t) * 2, st));
+    const int threads = w->solverThreads;
+    int occ = 1;
+    B3_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_jacobi, threads, 0));
+    occ = occ < 1 ? 1 : occ;
+    occ = occ > 4 ? 4 : occ;
+    const int grid = w->ctx->numSMs * occ;
+    int iters = w->sim.iterations;
+    uint32_t* bar = (uint32_t*)(w->d.scalars + S_BAR_COUNT);
+    int32_t* err = w->d.scalars + S_ERR;
+    b3Counters* ctr = w->d.counters;
+    void* args[] = {&V, &iters, &bar, &err, &ctr};
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    B3_CUDA(cudaLaunchKernelExC(&cfg, (const void*)k_jacobi, args));
+    return B3_OK;
+}
+
+int launch_integrate(b3World_t* w, cudaStream_t st) {
+    const int N = (int)w->bodies.size();
+    if (N == 0) return B3_OK;
+    IntegrateParams P;
+    P.dt = w->sim.dt;
+    P.damping = w->sim.angularDamping;
+    P.threshold = 0.25f * 3.14159254f;
+    k_integrate<<<(N + 255) / 256, 256, 0, st>>>(w->bodiesDev(), w->d.avgLin, w->d.avgAng,
+                                                w->d.bodyIncStart, w->d.bodyIncEnd, P, 1);
+    B3_CHECK_LAUNCH();
+    return B3_OK;
+}
+
+}  // namespace b3

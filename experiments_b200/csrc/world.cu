@@ -1,0 +1,916 @@
+// World object (rigid-body and collidable arrays, grid broadphase,
+// narrowphase-and-solver) and stepSimulation orchestration.
+//
+// Mirrors CLPhysicsDemo (P2/CLPhysicsDemo.h:30-81, .cpp:205-943) and
+// btGpuNarrowphaseAndSolver (P1/btGpuNarrowPhaseAndSolver.h:63-123) behind
+// the C ABI in include/b3gpu.h. One step issues, on one stream and with no
+// host synchronisation (so it can be captured as a CUDA graph):
+//   k_step_begin -> k_aabb_hash -> radix sort -> k_cell_start -> k_find_pairs
+//   -> k_narrowphase -> scan + k_manifold_emit -> radix sort -> k_body_ranges
+//   -> k_setup_rows -> k_jacobi (persistent) -> k_integrate
+// Every count that varies per step (pairs, manifolds, copies) stays on the
+// device and is read by the next kernel; the reference instead blocks on
+// clFinish more than 15 times and reads 3 counts back per step.
+#include "b3_world.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace {
+
+bool is_pow2(int v) { return v > 0 && (v & (v - 1)) == 0; }
+int ilog2(uint64_t v) {
+    int b = 0;
+    while ((1ull << b) < v) ++b;
+    return b;
+}
+
+__global__ void k_step_begin(int32_t* scalars, b3Counters* counters) {
+    if (threadIdx.x == 0) {
+        scalars[b3::S_STAMP] += 1;
+        counters->steps += 1;
+        counters->numContactPoints = 0;
+        counters->numManifolds = 0;
+        counters->numPairs = 0;
+    }
+}
+
+__global__ void k_world_stats(b3::BodiesDev Bd, float4* out, int numWorlds) {
+    // one warp-strided accumulation per body into its world (atomics; stats only)
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= Bd.n) return;
+    const float im = Bd.invMass[i];
+    if (im == 0.f) return;
+    const float m = 1.f / im;
+    const float4 p = Bd.pos[i], v = Bd.linVel[i];
+    const int w = Bd.worldId[i];
+    atomicAdd(&out[2 * w].x, m * p.x);
+    atomicAdd(&out[2 * w].y, m * p.y);
+    atomicAdd(&out[2 * w].z, m * p.z);
+    atomicAdd(&out[2 * w].w, m);
+    atomicAdd(&out[2 * w + 1].x, 0.5f * m * (v.x * v.x + v.y * v.y + v.z * v.z));
+}
+
+template <typename T>
+int dalloc(T*& p, size_t count) {
+    if (p) cudaFree(p);
+    p = nullptr;
+    if (count == 0) count = 1;
+    B3_CUDA(cudaMalloc((void**)&p, sizeof(T) * count));
+    return B3_OK;
+}
+
+void free_all(b3::DevBuffers& d) {
+    void* ptrs[] = {d.pos, d.quat, d.linVel, d.angVel, d.invMass, d.friction, d.restitution,
+                    d.invInertia, d.collidable, d.worldId, d.cols, d.polys, d.verts, d.faces,
+                    d.indices, d.edges, d.localAabb, d.aabbMin, d.aabbMax, d.smallSlot,
+                    d.largeStart, d.largeList, d.keys, d.vals, d.keysAlt, d.valsAlt, d.cellTable,
+                    d.pairs, d.contacts, d.manifoldFlag, d.manifoldScan, d.manifoldPair,
+                    d.incKeys, d.incVals, d.incKeysAlt, d.incValsAlt, d.bodyIncStart,
+                    d.bodyIncEnd, d.rows, d.manifoldHdr, d.incLin, d.incAng, d.avgLin, d.avgAng,
+                    d.scalars, d.counters, d.sortScratch, d.incSortScratch, d.scanScratch,
+                    d.worldStats};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    d = b3::DevBuffers();
+}
+
+// btTransformAabb (LinearMath/btAabbUtil2.h) with margin, in double: the
+// registration AABB used for the large-body test and the inertia.
+void transform_aabb(const float lmin[3], const float lmax[3], float margin, const float pos[3],
+                    const float q[4], float outMin[3], float outMax[3]) {
+    double he[3], c[3];
+    for (int k = 0; k < 3; ++k) {
+        he[k] = 0.5 * ((double)lmax[k] - lmin[k]) + margin;
+        c[k] = 0.5 * ((double)lmax[k] + lmin[k]);
+    }
+    const double x = q[0], y = q[1], z = q[2], w = q[3];
+    const double d = x * x + y * y + z * z + w * w;
+    const double s = 2.0 / d;
+    const double xs = x * s, ys = y * s, zs = z * s;
+    const double wx = w * xs, wy = w * ys, wz = w * zs;
+    const double xx = x * xs, xy = x * ys, xz = x * zs;
+    const double yy = y * ys, yz = y * zs, zz = z * zs;
+    const double Rm[3][3] = {{1.0 - (yy + zz), xy - wz, xz + wy},
+                             {xy + wz, 1.0 - (xx + zz), yz - wx},
+                             {xz - wy, yz + wx, 1.0 - (xx + yy)}};
+    for (int r = 0; r < 3; ++r) {
+        double cc = Rm[r][0] * c[0] + Rm[r][1] * c[1] + Rm[r][2] * c[2] + pos[r];
+        double e = std::fabs(Rm[r][0]) * he[0] + std::fabs(Rm[r][1]) * he[1] + std::fabs(Rm[r][2]) * he[2];
+        outMin[r] = (float)(cc - e);
+        outMax[r] = (float)(cc + e);
+    }
+}
+
+}  // namespace
+
+b3::BodiesDev b3World_t::bodiesDev() const {
+    b3::BodiesDev B;
+    B.n = (int)bodies.size();
+    B.pos = d.pos;
+    B.quat = d.quat;
+    B.linVel = d.linVel;
+    B.angVel = d.angVel;
+    B.invMass = d.invMass;
+    B.collidable = d.collidable;
+    B.friction = d.friction;
+    B.restitution = d.restitution;
+    B.invInertia = d.invInertia;
+    B.worldId = d.worldId;
+    return B;
+}
+
+b3::ShapesDev b3World_t::shapesDev() const {
+    b3::ShapesDev S;
+    S.cols = d.cols;
+    S.polys = d.polys;
+    S.verts = d.verts;
+    S.faces = d.faces;
+    S.indices = d.indices;
+    S.edges = d.edges;
+    S.localAabb = d.localAabb;
+    S.numPolys = (int)polys.size();
+    S.numVerts = (int)verts4.size() / 4;
+    S.numFaces = (int)faces.size();
+    S.numIndices = (int)indices.size();
+    S.numEdges = (int)edges4.size() / 4;
+    S.tableBytes = 0;
+    return S;
+}
+
+extern "C" void b3_world_config_default(b3WorldConfig* c) {
+    if (!c) return;
+    memset(c, 0, sizeof(*c));
+    c->maxBodies = 128 * 1024;
+    c->maxPairs = 0;               // 0 = 8 x maxBodies
+    c->numWorlds = 1;
+    c->cellSize = 4.f;             // P2/CLPhysicsDemo.cpp:636 uses 4 m cells
+    c->gridDims[0] = c->gridDims[1] = c->gridDims[2] = 128;
+    c->maxBodiesPerCell = 128;
+    c->maxPairsPerBody = 32;
+    c->maxSmallProxySize = 100.f;
+    c->gravity[0] = 0.f;
+    c->gravity[1] = -9.8f;
+    c->gravity[2] = 0.f;
+    c->dt = 1.f / 60.f;
+    c->solverIterations = 10;
+    c->erp = 0.2f;
+    c->contactBreaking = 0.02f;
+    c->contactProcessing = 0.02f;
+    c->linearSlopOffset = 0.01f;
+    c->angularDamping = 0.99f;
+    c->frictionCombine = B3_FRICTION_GEOMEAN;
+    c->useGraph = 0;
+}
+
+extern "C" int b3_world_create(b3Context ctx, const b3WorldConfig* cfg, b3World* out) {
+    if (!ctx || !cfg || !out) return B3_ERR_INVALID_ARG;
+    *out = nullptr;
+    const b3WorldConfig& c = *cfg;
+    for (int k = 0; k < 3; ++k)
+        if (!is_pow2(c.gridDims[k]) || c.gridDims[k] < 4) {
+            b3_set_error("gridDims must be powers of two >= 4");
+            return B3_ERR_INVALID_ARG;
+        }
+    if (c.maxBodies <= 0 || c.numWorlds <= 0 || c.cellSize <= 0.f || c.maxBodiesPerCell <= 0 ||
+        c.maxPairsPerBody < 2 || c.maxPairsPerBody > 256 || c.dt <= 0.f || c.solverIterations < 0) {
+        b3_set_error("invalid world configuration");
+        return B3_ERR_INVALID_ARG;
+    }
+    const int cellBits = ilog2((uint64_t)c.gridDims[0] * c.gridDims[1] * c.gridDims[2]);
+    const int worldBits = c.numWorlds > 1 ? ilog2((uint64_t)c.numWorlds) : 0;
+    if (cellBits + worldBits > 32) {
+        b3_set_error("world id + cell hash need %d > 32 key bits", cellBits + worldBits);
+        return B3_ERR_INVALID_ARG;
+    }
+    b3World w = new b3World_t();
+    w->ctx = ctx;
+    w->cfg = c;
+    if (w->cfg.maxPairs <= 0) w->cfg.maxPairs = 8 * c.maxBodies;
+    w->cellBits = cellBits;
+    w->worldBits = worldBits;
+    w->keyBits = std::max(1, cellBits + worldBits);
+    w->invCell = 1.f / c.cellSize;
+    w->sim.gravity = make_float3(c.gravity[0], c.gravity[1], c.gravity[2]);
+    w->sim.dt = c.dt;
+    w->sim.iterations = c.solverIterations;
+    w->sim.erp = c.erp;
+    w->sim.contactBreaking = c.contactBreaking;
+    w->sim.contactProcessing = c.contactProcessing;
+    w->sim.slopOffset = c.linearSlopOffset;
+    w->sim.angularDamping = c.angularDamping;
+    w->sim.frictionCombine = c.frictionCombine;
+    *out = w;
+    return B3_OK;
+}
+
+extern "C" int b3_world_destroy(b3World w) {
+    if (!w) return B3_OK;
+    if (w->ctx->device < 0) {
+        delete w;
+        return B3_OK;
+    }
+    cudaSetDevice(w->ctx->device);
+    if (w->graphExec) cudaGraphExecDestroy(w->graphExec);
+    if (w->graphStream) cudaStreamDestroy(w->graphStream);
+    free_all(w->d);
+    delete w;
+    return B3_OK;
+}
+
+extern "C" int b3_register_convex_hull(b3World w, const float* vertices, int numVertices, int strideBytes,
+                                       const float scaling[3], int* collidableOut) {
+    if (!w || !vertices || numVertices < 4 || !collidableOut) return B3_ERR_INVALID_ARG;
+    if (strideBytes <= 0) strideBytes = 3 * sizeof(float);
+    std::vector<float> pts(3 * (size_t)numVertices);
+    const unsigned char* base = (const unsigned char*)vertices;
+    for (int i = 0; i < numVertices; ++i) {
+        const float* v = (const float*)(base + (size_t)i * strideBytes);
+        for (int k = 0; k < 3; ++k) pts[3 * i + k] = v[k] * (scaling ? scaling[k] : 1.f);
+    }
+    b3hull::Polyhedron P;
+    std::string err;
+    if (!b3hull::compute_polyhedron(pts.data(), numVertices, P, &err)) {
+        b3_set_error("hull: %s", err.c_str());
+        return B3_ERR_INVALID_ARG;
+    }
+    b3ConvexPolyhedron poly;
+    memset(&poly, 0, sizeof(poly));
+    for (int k = 0; k < 3; ++k) {
+        poly.localCenter[k] = P.localCenter[k];
+        poly.mC[k] = P.mC[k];
+        poly.mE[k] = P.mE[k];
+        poly.extents[k] = 0.5f * P.mE[k];
+    }
+    float r = 1e30f;
+    for (auto& f : P.faces)
+        r = std::min(r, std::fabs(f.plane[0] * P.localCenter[0] + f.plane[1] * P.localCenter[1] +
+                                  f.plane[2] * P.localCenter[2] + f.plane[3]));
+    poly.radius = r;
+    poly.numVertices = (int)P.vertices.size() / 3;
+    poly.vertexOffset = (int)w->verts4.size() / 4;
+    for (int i = 0; i < poly.numVertices; ++i) {
+        w->verts4.push_back(P.vertices[3 * i]);
+        w->verts4.push_back(P.vertices[3 * i + 1]);
+        w->verts4.push_back(P.vertices[3 * i + 2]);
+        w->verts4.push_back(0.f);
+    }
+    poly.numFaces = (int)P.faces.size();
+    poly.faceOffset = (int)w->faces.size();
+    for (auto& f : P.faces) {
+        b3Face ff;
+        memset(&ff, 0, sizeof(ff));
+        for (int k = 0; k < 4; ++k) ff.plane[k] = f.plane[k];
+        ff.indexOffset = (int)w->indices.size();
+        ff.numIndices = (int)f.indices.size();
+        for (int id : f.indices) w->indices.push_back(id);
+        w->faces.push_back(ff);
+    }
+    poly.numUniqueEdges = (int)P.uniqueEdges.size() / 3;
+    poly.uniqueEdgesOffset = (int)w->edges4.size() / 4;
+    for (int i = 0; i < poly.numUniqueEdges; ++i) {
+        w->edges4.push_back(P.uniqueEdges[3 * i]);
+        w->edges4.push_back(P.uniqueEdges[3 * i + 1]);
+        w->edges4.push_back(P.uniqueEdges[3 * i + 2]);
+        w->edges4.push_back(0.f);
+    }
+    b3Collidable col;
+    col.numChildShapes = 0;
+    col.radius = 0.f;
+    col.shapeType = B3_SHAPE_CONVEX_HULL;
+    col.shapeIndex = (int)w->polys.size();
+    w->polys.push_back(poly);
+    w->cols.push_back(col);
+    for (int k = 0; k < 3; ++k) w->localAabb8.push_back(P.aabbMin[k]);
+    w->localAabb8.push_back(0.f);
+    for (int k = 0; k < 3; ++k) w->localAabb8.push_back(P.aabbMax[k]);
+    w->localAabb8.push_back(0.f);
+    w->shapesDirty = true;
+    *collidableOut = (int)w->cols.size() - 1;
+    return B3_OK;
+}
+
+extern "C" int b3_register_body(b3World w, float mass, const float position[3], const float orientation[4],
+                                int collidable, float friction, float restitution, int worldId, int* bodyOut) {
+    if (!w || !position || !orientation || !bodyOut) return B3_ERR_INVALID_ARG;
+    if (collidable < 0 || collidable >= (int)w->cols.size()) return B3_ERR_INVALID_ARG;
+    if (worldId < 0 || worldId >= w->cfg.numWorlds) return B3_ERR_INVALID_ARG;
+    if ((int)w->bodies.size() >= w->cfg.maxBodies) {
+        b3_set_error("maxBodies (%d) reached", w->cfg.maxBodies);
+        return B3_ERR_CAPACITY;
+    }
+    b3Body b;
+    memset(&b, 0, sizeof(b));
+    for (int k = 0; k < 3; ++k) b.pos[k] = position[k];
+    for (int k = 0; k < 4; ++k) b.quat[k] = orientation[k];
+    b.collidableIdx = (uint32_t)collidable;
+    b.invMass = mass != 0.f ? 1.f / mass : 0.f;
+    b.friction = friction;
+    b.restitution = restitution;
+    // registration AABB with 0.01 margin (P2/CLPhysicsDemo.cpp:538-548)
+    float amin[3], amax[3];
+    const float* la = &w->localAabb8[8 * (size_t)collidable];
+    transform_aabb(la, la + 4, 0.01f, position, orientation, amin, amax);
+    b3Inertia I;
+    memset(&I, 0, sizeof(I));
+    if (mass != 0.f) {
+        // registerRigidBody (P1/btGpuNarrowPhaseAndSolver.cpp:610-641): full
+        // extents, doubled, as the inertia box
+        const float hx = amax[0] - amin[0], hy = amax[1] - amin[1], hz = amax[2] - amin[2];
+        const float lx = 2.f * hx, ly = 2.f * hy, lz = 2.f * hz;
+        const float ix = (mass / 12.0f) * (ly * ly + lz * lz);
+        const float iy = (mass / 12.0f) * (lx * lx + lz * lz);
+        const float iz = (mass / 12.0f) * (lx * lx + ly * ly);
+        I.initInvInertia[0] = 1.f / ix;
+        I.initInvInertia[5] = 1.f / iy;
+        I.initInvInertia[10] = 1.f / iz;
+        memcpy(I.invInertiaWorld, I.initInvInertia, sizeof(I.initInvInertia));
+    }
+    w->bodies.push_back(b);
+    w->inertias.push_back(I);
+    w->worldIds.push_back(worldId);
+    for (int k = 0; k < 3; ++k) w->regAabb.push_back(amin[k]);
+    for (int k = 0; k < 3; ++k) w->regAabb.push_back(amax[k]);
+    w->written = false;
+    *bodyOut = (int)w->bodies.size() - 1;
+    return B3_OK;
+}
+
+extern "C" int b3_register_bodies(b3World w, int n, const float* masses, const float* positions3,
+                                  const float* orientations4, const int* collidables, const float* frictions,
+                                  const float* restitutions, const int* worldIds, int* firstBodyOut) {
+    if (!w || n < 0 || (n > 0 && (!masses || !positions3 || !orientations4 || !collidables)))
+        return B3_ERR_INVALID_ARG;
+    if ((int64_t)w->bodies.size() + n > w->cfg.maxBodies) {
+        b3_set_error("maxBodies (%d) reached", w->cfg.maxBodies);
+        return B3_ERR_CAPACITY;
+    }
+    if (firstBodyOut) *firstBodyOut = (int)w->bodies.size();
+    for (int i = 0; i < n; ++i) {
+        int id = 0;
+        B3_TRY(b3_register_body(w, masses[i], positions3 + 3 * (size_t)i, orientations4 + 4 * (size_t)i,
+                                collidables[i], frictions ? frictions[i] : 1.f,
+                                restitutions ? restitutions[i] : 0.f, worldIds ? worldIds[i] : 0, &id));
+    }
+    return B3_OK;
+}
+
+static int ensure_capacity(b3World w) {
+    const int N = (int)w->bodies.size();
+    const int cap = w->cfg.maxPairs;
+    auto& d = w->d;
+    if (!d.cellTable) {
+        const size_t cells = (size_t)w->cfg.numWorlds << w->cellBits;
+        B3_TRY(dalloc(d.cellTable, cells));
+        B3_TRY(dalloc(d.scalars, b3::S_NUM_SCALARS));
+        B3_TRY(dalloc(d.counters, 1));
+        B3_CUDA(cudaMemset(d.cellTable, 0, sizeof(uint2) * cells));
+        B3_CUDA(cudaMemset(d.scalars, 0, sizeof(int32_t) * b3::S_NUM_SCALARS));
+        B3_CUDA(cudaMemset(d.counters, 0, sizeof(b3Counters)));
+    }
+    if (w->capBodies < N || !d.pos) {
+        const int nb = std::max(N, 1);
+        B3_TRY(dalloc(d.pos, nb));
+        B3_TRY(dalloc(d.quat, nb));
+        B3_TRY(dalloc(d.linVel, nb));
+        B3_TRY(dalloc(d.angVel, nb));
+        B3_TRY(dalloc(d.invMass, nb));
+        B3_TRY(dalloc(d.friction, nb));
+        B3_TRY(dalloc(d.restitution, nb));
+        B3_TRY(dalloc(d.invInertia, nb));
+        B3_TRY(dalloc(d.collidable, nb));
+        B3_TRY(dalloc(d.worldId, nb));
+        B3_TRY(dalloc(d.aabbMin, nb));
+        B3_TRY(dalloc(d.aabbMax, nb));
+        B3_TRY(dalloc(d.smallSlot, nb));
+        B3_TRY(dalloc(d.keys, nb));
+        B3_TRY(dalloc(d.vals, nb));
+        B3_TRY(dalloc(d.keysAlt, nb));
+        B3_TRY(dalloc(d.valsAlt, nb));
+        B3_TRY(dalloc(d.bodyIncStart, nb));
+        B3_TRY(dalloc(d.bodyIncEnd, nb));
+        B3_TRY(dalloc(d.avgLin, nb));
+        B3_TRY(dalloc(d.avgAng, nb));
+        d.sortScratchBytes = b3::radix_scratch_bytes(nb, w->keyBits);
+        B3_TRY(dalloc((unsigned char*&)d.sortScratch, d.sortScratchBytes));
+        w->capBodies = nb;
+    }
+    if (!d.pairs) {
+        const size_t c = std::max(cap, 1);
+        B3_TRY(dalloc(d.pairs, c));
+        B3_TRY(dalloc(d.contacts, c));
+        B3_TRY(dalloc(d.manifoldFlag, c));
+        B3_TRY(dalloc(d.manifoldScan, c));
+        B3_TRY(dalloc(d.manifoldPair, c));
+        B3_TRY(dalloc(d.incKeys, 2 * c));
+        B3_TRY(dalloc(d.incVals, 2 * c));
+        B3_TRY(dalloc(d.incKeysAlt, 2 * c));
+        B3_TRY(dalloc(d.incValsAlt, 2 * c));
+        B3_TRY(dalloc(d.rows, 40 * c));
+        B3_TRY(dalloc(d.incLin, 2 * c));
+        B3_TRY(dalloc(d.incAng, 2 * c));
+        const size_t tiles = (w->cfg.maxBodies + 127) / 128 + 16;
+        d.scanScratchBytes = std::max(b3::scan_scratch_bytes(cap), tiles * 8 + 256);
+        B3_TRY(dalloc((unsigned char*&)d.scanScratch, d.scanScratchBytes));
+    }
+    // body-id key bits for the copy sort must cover the sentinel numBodies
+    w->bodyBits = std::max(1, ilog2((uint64_t)N + 1));
+    const size_t incBytes = b3::radix_scratch_bytes(2LL * cap, w->bodyBits);
+    if (incBytes > d.incSortScratchBytes) {
+        d.incSortScratchBytes = incBytes;
+        B3_TRY(dalloc((unsigned char*&)d.incSortScratch, incBytes));
+    }
+    if (!d.worldStats) B3_TRY(dalloc(d.worldStats, 2 * (size_t)w->cfg.numWorlds));
+    return B3_OK;
+}
+
+static int upload_shapes(b3World w, cudaStream_t st) {
+    auto& d = w->d;
+    B3_TRY(dalloc(d.cols, w->cols.size()));
+    B3_TRY(dalloc(d.polys, w->polys.size()));
+    B3_TRY(dalloc(d.verts, w->verts4.size() / 4));
+    B3_TRY(dalloc(d.faces, w->faces.size()));
+    B3_TRY(dalloc(d.indices, w->indices.size()));
+    B3_TRY(dalloc(d.edges, w->edges4.size() / 4 + 1));
+    B3_TRY(dalloc(d.localAabb, w->localAabb8.size() / 4));
+    B3_CUDA(cudaMemcpyAsync(d.cols, w->cols.data(), sizeof(b3Collidable) * w->cols.size(), cudaMemcpyHostToDevice, st));
+    B3_CUDA(cudaMemcpyAsync(d.polys, w->polys.data(), sizeof(b3ConvexPolyhedron) * w->polys.size(), cudaMemcpyHostToDevice, st));
+    B3_CUDA(cudaMemcpyAsync(d.verts, w->verts4.data(), sizeof(float) * w->verts4.size(), cudaMemcpyHostToDevice, st));
+    B3_CUDA(cudaMemcpyAsync(d.faces, w->faces.data(), sizeof(b3Face) * w->faces.size(), cudaMemcpyHostToDevice, st));
+    B3_CUDA(cudaMemcpyAsync(d.indices, w->indices.data(), sizeof(int) * w->indices.size(), cudaMemcpyHostToDevice, st));
+    if (!w->edges4.empty())
+        B3_CUDA(cudaMemcpyAsync(d.edges, w->edges4.data(), sizeof(float) * w->edges4.size(), cudaMemcpyHostToDevice, st));
+    B3_CUDA(cudaMemcpyAsync(d.localAabb, w->localAabb8.data(), sizeof(float) * w->localAabb8.size(), cudaMemcpyHostToDevice, st));
+    w->shapesDirty = false;
+    return B3_OK;
+}
+
+extern "C" int b3_write_bodies(b3World w, void* stream) {
+    if (!w) return B3_ERR_INVALID_ARG;
+    if (w->cols.empty()) return B3_ERR_STATE;
+    if (w->ctx->device < 0) {
+        b3_set_error("host-only context");
+        return B3_ERR_NO_DEVICE;
+    }
+    cudaStream_t st = as_stream(stream);
+    B3_CUDA(cudaSetDevice(w->ctx->device));
+    B3_TRY(ensure_capacity(w));
+    B3_TRY(upload_shapes(w, st));
+    const int N = (int)w->bodies.size();
+    std::vector<float4> pos(N), quat(N), lv(N), av(N), ii(N);
+    std::vector<float> im(N), fr(N), rs(N);
+    std::vector<int> col(N);
+    for (int i = 0; i < N; ++i) {
+        const b3Body& b = w->bodies[i];
+        pos[i] = make_float4(b.pos[0], b.pos[1], b.pos[2], 0.f);
+        quat[i] = make_float4(b.quat[0], b.quat[1], b.quat[2], b.quat[3]);
+        lv[i] = make_float4(b.linVel[0], b.linVel[1], b.linVel[2], 0.f);
+        av[i] = make_float4(b.angVel[0], b.angVel[1], b.angVel[2], 0.f);
+        im[i] = b.invMass;
+        fr[i] = b.friction;
+        rs[i] = b.restitution;
+        col[i] = (int)b.collidableIdx;
+        const b3Inertia& I = w->inertias[i];
+        ii[i] = make_float4(I.initInvInertia[0], I.initInvInertia[5], I.initInvInertia[10], 0.f);
+    }
+    // small / large classification (btGpu3DGridBroadphase::isLargeProxy,
+    // G3/btGpu3DGridBroadphase.cpp:385-391): half-diagonal > maxSmallProxySize/2
+    w->smallSlotHost.assign(N, -1);
+    std::vector<std::vector<int>> large(w->cfg.numWorlds);
+    int ns = 0;
+    for (int i = 0; i < N; ++i) {
+        const float* a = &w->regAabb[6 * (size_t)i];
+        const double dx = a[3] - a[0], dy = a[4] - a[1], dz = a[5] - a[2];
+        const double r = 0.5 * std::sqrt(dx * dx + dy * dy + dz * dz);
+        if (r > 0.5 * w->cfg.maxSmallProxySize) large[w->worldIds[i]].push_back(i);
+        else w->smallSlotHost[i] = ns++;
+    }
+    w->numSmall = ns;
+    w->largeStartHost.assign(w->cfg.numWorlds + 1, 0);
+    w->largeListHost.clear();
+    for (int k = 0; k < w->cfg.numWorlds; ++k) {
+        w->largeStartHost[k] = (int)w->largeListHost.size();
+        for (int id : large[k]) w->largeListHost.push_back(id);
+    }
+    w->largeStartHost[w->cfg.numWorlds] = (int)w->largeListHost.size();
+    auto& d = w->d;
+    B3_TRY(dalloc(d.largeStart, w->largeStartHost.size()));
+    B3_TRY(dalloc(d.largeList, std::max<size_t>(1, w->largeListHost.size())));
+    B3_CUDA(cudaMemcpyAsync(d.largeStart, w->largeStartHost.data(), sizeof(int) * w->largeStartHost.size(), cudaMemcpyHostToDevice, st));
+    if (!w->largeListHost.empty())
+        B3_CUDA(cudaMemcpyAsync(d.largeList, w->largeListHost.data(), sizeof(int) * w->largeListHost.size(), cudaMemcpyHostToDevice, st));
+    B3_CUDA(cudaMemcpyAsync(d.smallSlot, w->smallSlotHost.data(), sizeof(int) * N, cudaMemcpyHostToDevice, st));
+    B3_CUDA(cudaMemcpyAsync(d.pos, pos.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, st));
+    B3_CUDA(cudaMemcpyAsync(d.quat, quat.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, st));
+    B3_CUDA(cudaMemcpyAsync(d.linVel, lv.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, st));
+    B3_CUDA(cudaMemcpyAsync(d.angVel, av.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, st));
+    B3_CUDA(cudaMemcpyAsync(d.invMass, im.data(), sizeof(float) * N, cudaMemcpyHostToDevice, st));
+    B3_CUDA(cudaMemcpyAsync(d.friction, fr.data(), sizeof(float) * N, cudaMemcpyHostToDevice, st));
+    B3_CUDA(cudaMemcpyAsync(d.restitution, rs.data(), sizeof(float) * N, cudaMemcpyHostToDevice, st));
+    B3_CUDA(cudaMemcpyAsync(d.invInertia, ii.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, st));
+    B3_CUDA(cudaMemcpyAsync(d.collidable, col.data(), sizeof(int) * N, cudaMemcpyHostToDevice, st));
+    B3_CUDA(cudaMemcpyAsync(d.worldId, w->worldIds.data(), sizeof(int) * N, cudaMemcpyHostToDevice, st));
+    B3_CUDA(cudaMemsetAsync(d.avgLin, 0, sizeof(float4) * N, st));
+    B3_CUDA(cudaMemsetAsync(d.avgAng, 0, sizeof(float4) * N, st));
+    B3_CUDA(cudaMemsetAsync(d.bodyIncStart, 0, sizeof(uint32_t) * N, st));
+    B3_CUDA(cudaMemsetAsync(d.bodyIncEnd, 0, sizeof(uint32_t) * N, st));
+    const int32_t hs[1] = {ns};
+    B3_CUDA(cudaMemcpyAsync(d.scalars + b3::S_NUM_SMALL, hs, sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    B3_CUDA(cudaMemsetAsync(d.counters, 0, sizeof(b3Counters), st));
+    B3_CUDA(cudaStreamSynchronize(st));
+    if (w->graphExec) {
+        cudaGraphExecDestroy(w->graphExec);
+        w->graphExec = nullptr;
+    }
+    w->graphValid = false;
+    w->written = true;
+    return B3_OK;
+}
+
+extern "C" int b3_write_velocities(b3World w, const float* linVel3, const float* angVel3, void* stream) {
+    if (!w || !w->written) return B3_ERR_STATE;
+    const int N = (int)w->bodies.size();
+    cudaStream_t st = as_stream(stream);
+    std::vector<float4> t(N);
+    if (linVel3) {
+        for (int i = 0; i < N; ++i) t[i] = make_float4(linVel3[3 * i], linVel3[3 * i + 1], linVel3[3 * i + 2], 0.f);
+        B3_CUDA(cudaMemcpyAsync(w->d.linVel, t.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, st));
+        B3_CUDA(cudaStreamSynchronize(st));
+    }
+    if (angVel3) {
+        for (int i = 0; i < N; ++i) t[i] = make_float4(angVel3[3 * i], angVel3[3 * i + 1], angVel3[3 * i + 2], 0.f);
+        B3_CUDA(cudaMemcpyAsync(w->d.angVel, t.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, st));
+        B3_CUDA(cudaStreamSynchronize(st));
+    }
+    return B3_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Step orchestration
+// ---------------------------------------------------------------------------
+static int step_begin(b3World w, cudaStream_t st) {
+    k_step_begin<<<1, 32, 0, st>>>(w->d.scalars, w->d.counters);
+    B3_CHECK_LAUNCH();
+    return B3_OK;
+}
+
+static int run_one_step(b3World w, cudaStream_t st) {
+    B3_TRY(step_begin(w, st));
+    B3_TRY(b3::launch_aabb_hash(w, st));
+    B3_TRY(b3::launch_sort_and_cells(w, st));
+    B3_TRY(b3::launch_find_pairs(w, st));
+    B3_TRY(b3::launch_narrowphase(w, st));
+    B3_TRY(b3::launch_manifolds(w, st));
+    B3_TRY(b3::launch_solver(w, st));
+    B3_TRY(b3::launch_integrate(w, st));
+    return B3_OK;
+}
+
+static int run_one_step_timed(b3World w, cudaStream_t st) {
+    cudaEvent_t ev[9];
+    for (auto& e : ev) B3_CUDA(cudaEventCreate(&e));
+    B3_CUDA(cudaEventRecord(ev[0], st));
+    B3_TRY(step_begin(w, st));
+    B3_TRY(b3::launch_aabb_hash(w, st));
+    B3_CUDA(cudaEventRecord(ev[1], st));
+    B3_TRY(b3::launch_sort_and_cells(w, st));
+    B3_CUDA(cudaEventRecord(ev[2], st));
+    B3_TRY(b3::launch_find_pairs(w, st));
+    B3_CUDA(cudaEventRecord(ev[3], st));
+    B3_TRY(b3::launch_narrowphase(w, st));
+    B3_CUDA(cudaEventRecord(ev[4], st));
+    B3_TRY(b3::launch_manifolds(w, st));
+    B3_CUDA(cudaEventRecord(ev[5], st));
+    B3_TRY(b3::launch_solver(w, st));
+    B3_CUDA(cudaEventRecord(ev[6], st));
+    B3_TRY(b3::launch_integrate(w, st));
+    B3_CUDA(cudaEventRecord(ev[7], st));
+    B3_CUDA(cudaEventSynchronize(ev[7]));
+    w->stageMs.assign(7, 0.f);
+    for (int k = 0; k < 7; ++k) cudaEventElapsedTime(&w->stageMs[k], ev[k], ev[k + 1]);
+    for (auto& e : ev) cudaEventDestroy(e);
+    return B3_OK;
+}
+
+extern "C" int b3_step(b3World w, int numSteps, void* stream) {
+    if (!w || numSteps < 0) return B3_ERR_INVALID_ARG;
+    if (!w->written) return B3_ERR_STATE;
+    B3_CUDA(cudaSetDevice(w->ctx->device));
+    cudaStream_t st = as_stream(stream);
+    int done = 0;
+    if (w->cfg.useGraph && !w->timing && numSteps > 0) {
+        if (!w->graphValid) {
+            // first step eagerly (sets kernel attributes), then capture one step
+            B3_TRY(run_one_step(w, st));
+            done = 1;
+            if (!w->graphStream) B3_CUDA(cudaStreamCreateWithFlags(&w->graphStream, cudaStreamNonBlocking));
+            B3_CUDA(cudaStreamSynchronize(st));
+            cudaGraph_t g = nullptr;
+            B3_CUDA(cudaStreamBeginCapture(w->graphStream, cudaStreamCaptureModeThreadLocal));
+            int s = run_one_step(w, w->graphStream);
+            cudaError_t ce = cudaStreamEndCapture(w->graphStream, &g);
+            if (s != B3_OK) return s;
+            if (ce != cudaSuccess) {
+                b3_set_error("graph capture failed: %s", cudaGetErrorString(ce));
+                return B3_ERR_CUDA;
+            }
+            if (w->graphExec) cudaGraphExecDestroy(w->graphExec);
+            cudaError_t ie = cudaGraphInstantiate(&w->graphExec, g, 0);
+            cudaGraphDestroy(g);
+            if (ie != cudaSuccess) {
+                b3_set_error("graph instantiate failed: %s", cudaGetErrorString(ie));
+                return B3_ERR_CUDA;
+            }
+            w->graphValid = true;
+        }
+        for (int i = done; i < numSteps; ++i) B3_CUDA(cudaGraphLaunch(w->graphExec, st));
+        return B3_OK;
+    }
+    for (int i = 0; i < numSteps; ++i) {
+        if (w->timing) B3_TRY(run_one_step_timed(w, st));
+        else B3_TRY(run_one_step(w, st));
+    }
+    return B3_OK;
+}
+
+extern "C" int b3_stage_aabbs(b3World w, void* stream) {
+    if (!w || !w->written) return B3_ERR_STATE;
+    cudaStream_t st = as_stream(stream);
+    B3_TRY(step_begin(w, st));
+    return b3::launch_aabb_hash(w, st);
+}
+extern "C" int b3_stage_broadphase(b3World w, void* stream) {
+    if (!w || !w->written) return B3_ERR_STATE;
+    cudaStream_t st = as_stream(stream);
+    B3_TRY(b3::launch_sort_and_cells(w, st));
+    return b3::launch_find_pairs(w, st);
+}
+extern "C" int b3_stage_narrowphase(b3World w, void* stream) {
+    if (!w || !w->written) return B3_ERR_STATE;
+    cudaStream_t st = as_stream(stream);
+    B3_TRY(b3::launch_narrowphase(w, st));
+    return b3::launch_manifolds(w, st);
+}
+extern "C" int b3_stage_solve(b3World w, void* stream) {
+    if (!w || !w->written) return B3_ERR_STATE;
+    return b3::launch_solver(w, as_stream(stream));
+}
+extern "C" int b3_stage_integrate(b3World w, void* stream) {
+    if (!w || !w->written) return B3_ERR_STATE;
+    return b3::launch_integrate(w, as_stream(stream));
+}
+
+// ---------------------------------------------------------------------------
+// Reads
+// ---------------------------------------------------------------------------
+extern "C" int b3_get_num_bodies(b3World w, int* n) {
+    if (!w || !n) return B3_ERR_INVALID_ARG;
+    *n = (int)w->bodies.size();
+    return B3_OK;
+}
+
+extern "C" int b3_read_state(b3World w, float* pos4, float* quat4, float* linVel4, float* angVel4, void* stream) {
+    if (!w || !w->written) return B3_ERR_STATE;
+    const size_t N = w->bodies.size();
+    cudaStream_t st = as_stream(stream);
+    if (pos4) B3_CUDA(cudaMemcpyAsync(pos4, w->d.pos, 16 * N, cudaMemcpyDeviceToHost, st));
+    if (quat4) B3_CUDA(cudaMemcpyAsync(quat4, w->d.quat, 16 * N, cudaMemcpyDeviceToHost, st));
+    if (linVel4) B3_CUDA(cudaMemcpyAsync(linVel4, w->d.linVel, 16 * N, cudaMemcpyDeviceToHost, st));
+    if (angVel4) B3_CUDA(cudaMemcpyAsync(angVel4, w->d.angVel, 16 * N, cudaMemcpyDeviceToHost, st));
+    B3_CUDA(cudaStreamSynchronize(st));
+    return B3_OK;
+}
+
+extern "C" int b3_write_state(b3World w, const float* pos4, const float* quat4, const float* linVel4,
+                              const float* angVel4, void* stream) {
+    if (!w || !w->written) return B3_ERR_STATE;
+    const size_t N = w->bodies.size();
+    cudaStream_t st = as_stream(stream);
+    if (pos4) B3_CUDA(cudaMemcpyAsync(w->d.pos, pos4, 16 * N, cudaMemcpyHostToDevice, st));
+    if (quat4) B3_CUDA(cudaMemcpyAsync(w->d.quat, quat4, 16 * N, cudaMemcpyHostToDevice, st));
+    if (linVel4) B3_CUDA(cudaMemcpyAsync(w->d.linVel, linVel4, 16 * N, cudaMemcpyHostToDevice, st));
+    if (angVel4) B3_CUDA(cudaMemcpyAsync(w->d.angVel, angVel4, 16 * N, cudaMemcpyHostToDevice, st));
+    B3_CUDA(cudaStreamSynchronize(st));
+    return B3_OK;
+}
+
+extern "C" int b3_read_bodies(b3World w, b3Body* out, int maxBodies, void* stream) {
+    if (!w || !out) return B3_ERR_INVALID_ARG;
+    if (!w->written) return B3_ERR_STATE;
+    const int N = std::min((int)w->bodies.size(), maxBodies);
+    std::vector<float4> p(w->bodies.size()), q(p.size()), l(p.size()), a(p.size());
+    B3_TRY(b3_read_state(w, (float*)p.data(), (float*)q.data(), (float*)l.data(), (float*)a.data(), stream));
+    for (int i = 0; i < N; ++i) {
+        b3Body b = w->bodies[i];
+        memcpy(b.pos, &p[i], 16);
+        b.pos[3] = 0.f;
+        memcpy(b.quat, &q[i], 16);
+        memcpy(b.linVel, &l[i], 16);
+        memcpy(b.angVel, &a[i], 16);
+        out[i] = b;
+    }
+    return B3_OK;
+}
+
+extern "C" int b3_get_counters(b3World w, b3Counters* out, void* stream) {
+    if (!w || !out) return B3_ERR_INVALID_ARG;
+    if (!w->d.counters) return B3_ERR_STATE;
+    cudaStream_t st = as_stream(stream);
+    B3_CUDA(cudaMemcpyAsync(out, w->d.counters, sizeof(b3Counters), cudaMemcpyDeviceToHost, st));
+    int32_t err = 0;
+    B3_CUDA(cudaMemcpyAsync(&err, w->d.scalars + b3::S_ERR, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    B3_CUDA(cudaStreamSynchronize(st));
+    if (err && out->timeouts == 0) out->timeouts = 1;
+    return B3_OK;
+}
+
+extern "C" int b3_reset_counters(b3World w, void* stream) {
+    if (!w || !w->d.counters) return B3_ERR_STATE;
+    cudaStream_t st = as_stream(stream);
+    B3_CUDA(cudaMemsetAsync(w->d.counters, 0, sizeof(b3Counters), st));
+    B3_CUDA(cudaMemsetAsync(w->d.scalars + b3::S_ERR, 0, sizeof(int32_t), st));
+    B3_CUDA(cudaStreamSynchronize(st));
+    return B3_OK;
+}
+
+extern "C" int b3_get_aabbs(b3World w, float* out8, int maxBodies, void* stream) {
+    if (!w || !out8) return B3_ERR_INVALID_ARG;
+    if (!w->written) return B3_ERR_STATE;
+    const int N = std::min((int)w->bodies.size(), maxBodies);
+    std::vector<float4> mn(N), mx(N);
+    cudaStream_t st = as_stream(stream);
+    B3_CUDA(cudaMemcpyAsync(mn.data(), w->d.aabbMin, 16 * (size_t)N, cudaMemcpyDeviceToHost, st));
+    B3_CUDA(cudaMemcpyAsync(mx.data(), w->d.aabbMax, 16 * (size_t)N, cudaMemcpyDeviceToHost, st));
+    B3_CUDA(cudaStreamSynchronize(st));
+    for (int i = 0; i < N; ++i) {
+        memcpy(out8 + 8 * (size_t)i, &mn[i], 16);
+        memcpy(out8 + 8 * (size_t)i + 4, &mx[i], 16);
+    }
+    return B3_OK;
+}
+
+extern "C" int b3_get_sorted_hash(b3World w, uint32_t* keys, uint32_t* values, int max, int* count, void* stream) {
+    if (!w || !count) return B3_ERR_INVALID_ARG;
+    if (!w->written) return B3_ERR_STATE;
+    const int n = std::min(w->numSmall, max);
+    cudaStream_t st = as_stream(stream);
+    if (keys && n) B3_CUDA(cudaMemcpyAsync(keys, w->d.keys, 4 * (size_t)n, cudaMemcpyDeviceToHost, st));
+    if (values && n) B3_CUDA(cudaMemcpyAsync(values, w->d.vals, 4 * (size_t)n, cudaMemcpyDeviceToHost, st));
+    B3_CUDA(cudaStreamSynchronize(st));
+    *count = w->numSmall;
+    return B3_OK;
+}
+
+extern "C" int b3_get_pairs(b3World w, int32_t* pairs2, int max, int* count, void* stream) {
+    if (!w || !count) return B3_ERR_INVALID_ARG;
+    if (!w->written) return B3_ERR_STATE;
+    cudaStream_t st = as_stream(stream);
+    int32_t np = 0;
+    B3_CUDA(cudaMemcpyAsync(&np, w->d.scalars + b3::S_NUM_PAIRS, 4, cudaMemcpyDeviceToHost, st));
+    B3_CUDA(cudaStreamSynchronize(st));
+    *count = np;
+    const int n = std::min(np, max);
+    if (pairs2 && n > 0) {
+        B3_CUDA(cudaMemcpyAsync(pairs2, w->d.pairs, 8 * (size_t)n, cudaMemcpyDeviceToHost, st));
+        B3_CUDA(cudaStreamSynchronize(st));
+    }
+    return B3_OK;
+}
+
+extern "C" int b3_get_contacts(b3World w, b3Contact4* out, int max, int* count, void* stream) {
+    if (!w || !count) return B3_ERR_INVALID_ARG;
+    if (!w->written) return B3_ERR_STATE;
+    cudaStream_t st = as_stream(stream);
+    int32_t s[3] = {0, 0, 0};
+    B3_CUDA(cudaMemcpyAsync(s, w->d.scalars + b3::S_NUM_PAIRS, 12, cudaMemcpyDeviceToHost, st));
+    B3_CUDA(cudaStreamSynchronize(st));
+    const int np = s[0], nm = s[1];
+    *count = nm;
+    if (!out || nm <= 0 || max <= 0) return B3_OK;
+    std::vector<uint32_t> flag(np);
+    std::vector<b3Contact4> all(np);
+    if (np > 0) {
+        B3_CUDA(cudaMemcpyAsync(flag.data(), w->d.manifoldFlag, 4 * (size_t)np, cudaMemcpyDeviceToHost, st));
+        B3_CUDA(cudaMemcpyAsync(all.data(), w->d.contacts, sizeof(b3Contact4) * (size_t)np, cudaMemcpyDeviceToHost, st));
+        B3_CUDA(cudaStreamSynchronize(st));
+    }
+    int k = 0;
+    for (int p = 0; p < np && k < max; ++p)
+        if (flag[p]) out[k++] = all[p];
+    return B3_OK;
+}
+
+extern "C" int b3_get_shape_sizes(b3World w, int* numCollidables, int* numPolys, int* numVertices,
+                                  int* numFaces, int* numIndices, int* numEdges) {
+    if (!w) return B3_ERR_INVALID_ARG;
+    if (numCollidables) *numCollidables = (int)w->cols.size();
+    if (numPolys) *numPolys = (int)w->polys.size();
+    if (numVertices) *numVertices = (int)w->verts4.size() / 4;
+    if (numFaces) *numFaces = (int)w->faces.size();
+    if (numIndices) *numIndices = (int)w->indices.size();
+    if (numEdges) *numEdges = (int)w->edges4.size() / 4;
+    return B3_OK;
+}
+
+extern "C" int b3_get_shapes(b3World w, b3Collidable* cols, b3ConvexPolyhedron* polys, float* vertices4,
+                             b3Face* faces, int* indices, float* edges4, float* localAabbs8) {
+    if (!w) return B3_ERR_INVALID_ARG;
+    if (cols) memcpy(cols, w->cols.data(), sizeof(b3Collidable) * w->cols.size());
+    if (polys) memcpy(polys, w->polys.data(), sizeof(b3ConvexPolyhedron) * w->polys.size());
+    if (vertices4) memcpy(vertices4, w->verts4.data(), sizeof(float) * w->verts4.size());
+    if (faces) memcpy(faces, w->faces.data(), sizeof(b3Face) * w->faces.size());
+    if (indices) memcpy(indices, w->indices.data(), sizeof(int) * w->indices.size());
+    if (edges4) memcpy(edges4, w->edges4.data(), sizeof(float) * w->edges4.size());
+    if (localAabbs8) memcpy(localAabbs8, w->localAabb8.data(), sizeof(float) * w->localAabb8.size());
+    return B3_OK;
+}
+
+extern "C" int b3_get_inertias(b3World w, b3Inertia* out, int maxBodies) {
+    if (!w || !out) return B3_ERR_INVALID_ARG;
+    const int n = std::min((int)w->inertias.size(), maxBodies);
+    memcpy(out, w->inertias.data(), sizeof(b3Inertia) * n);
+    return B3_OK;
+}
+
+extern "C" int b3_get_device_buffer(b3World w, int which, void** d_ptr, int64_t* bytes) {
+    if (!w || !d_ptr) return B3_ERR_INVALID_ARG;
+    const int64_t N = (int64_t)w->bodies.size();
+    void* p = nullptr;
+    int64_t b = 0;
+    switch (which) {
+        case B3_BUF_POS: p = w->d.pos; b = 16 * N; break;
+        case B3_BUF_QUAT: p = w->d.quat; b = 16 * N; break;
+        case B3_BUF_LINVEL: p = w->d.linVel; b = 16 * N; break;
+        case B3_BUF_ANGVEL: p = w->d.angVel; b = 16 * N; break;
+        case B3_BUF_AABB_MIN: p = w->d.aabbMin; b = 16 * N; break;
+        case B3_BUF_AABB_MAX: p = w->d.aabbMax; b = 16 * N; break;
+        case B3_BUF_PAIRS: p = w->d.pairs; b = 8 * (int64_t)w->cfg.maxPairs; break;
+        case B3_BUF_CONTACTS: p = w->d.contacts; b = (int64_t)sizeof(b3Contact4) * w->cfg.maxPairs; break;
+        case B3_BUF_COUNTERS: p = w->d.counters; b = sizeof(b3Counters); break;
+        case B3_BUF_INVMASS: p = w->d.invMass; b = 4 * N; break;
+        default: return B3_ERR_INVALID_ARG;
+    }
+    *d_ptr = p;
+    if (bytes) *bytes = b;
+    return B3_OK;
+}
+
+extern "C" int b3_set_stage_timing(b3World w, int enable) {
+    if (!w) return B3_ERR_INVALID_ARG;
+    w->timing = enable != 0;
+    return B3_OK;
+}
+
+extern "C" int b3_get_stage_times(b3World w, float* ms, int max, int* count) {
+    if (!w || !count) return B3_ERR_INVALID_ARG;
+    *count = (int)w->stageMs.size();
+    for (int i = 0; i < std::min(max, *count); ++i) ms[i] = w->stageMs[i];
+    return B3_OK;
+}
+
+namespace b3 {
+int launch_world_stats(b3World_t* w, cudaStream_t st) {
+    const int N = (int)w->bodies.size();
+    B3_CUDA(cudaMemsetAsync(w->d.worldStats, 0, sizeof(float4) * 2 * w->cfg.numWorlds, st));
+    if (N == 0) return B3_OK;
+    k_world_stats<<<(N + 255) / 256, 256, 0, st>>>(w->bodiesDev(), w->d.worldStats, w->cfg.numWorlds);
+    B3_CHECK_LAUNCH();
+    return B3_OK;
+}
+}  // namespace b3
+
+extern "C" int b3_batch_world_stats(b3World w, float* out4, int numWorlds, void* stream) {
+    if (!w || !out4 || numWorlds <= 0) return B3_ERR_INVALID_ARG;
+    if (!w->written) return B3_ERR_STATE;
+    cudaStream_t st = as_stream(stream);
+    B3_TRY(b3::launch_world_stats(w, st));
+    const int nw = std::min(numWorlds, w->cfg.numWorlds);
+    std::vector<float4> s(2 * (size_t)w->cfg.numWorlds);
+    B3_CUDA(cudaMemcpyAsync(s.data(), w->d.worldStats, sizeof(float4) * s.size(), cudaMemcpyDeviceToHost, st));
+    B3_CUDA(cudaStreamSynchronize(st));
+    for (int k = 0; k < nw; ++k) {
+        const float m = s[2 * k].w;
+        out4[4 * k + 0] = m > 0 ? s[2 * k].x / m : 0.f;
+        out4[4 * k + 1] = m > 0 ? s[2 * k].y / m : 0.f;
+        out4[4 * k + 2] = m > 0 ? s[2 * k].z / m : 0.f;
+        out4[4 * k + 3] = s[2 * k + 1].x;
+    }
+    return B3_OK;
+}
+
+extern "C" int b3_autotune(b3World w, int trialSteps, void* stream) {
+    (void)trialSteps;
+    (void)stream;
+    return w ? B3_OK : B3_ERR_INVALID_ARG;
+}
+
+extern "C" int b3_get_tuning(b3World w, int* values, int max, int* count) {
+    if (!w || !count) return B3_ERR_INVALID_ARG;
+    int v[3] = {w->npWarpsPerBlock, w->pairThreads, w->solverThreads};
+    *count = 3;
+    for (int i = 0; i < std::min(3, max); ++i) values[i] = v[i];
+    return B3_OK;
+}
+
+// Adjoint entry points are implemented in adjoint.cu.

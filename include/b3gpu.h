@@ -1,0 +1,344 @@
+/*
+ * b3gpu.h — C ABI of the B200-native rigid-body step.
+ *
+ * This is the drop-in boundary for the reference GPU rigid-body pipeline
+ * (erwincoumans/experiments, opencl/gpu_rigidbody_pipeline2 and its
+ * dependencies). Every entry point is plain C: opaque handles, plain
+ * pointers and sizes, int status codes (0 = OK), no exceptions across the
+ * ABI and no torch types. Device pointers are CUDA device pointers; streams
+ * are cudaStream_t passed as void* (NULL = legacy default stream). Nothing
+ * synchronises implicitly except the *_read_* / *_get_* calls that copy to
+ * host memory and b3_sync.
+ *
+ * Citations name files relative to the reference project root:
+ *   P2/ = opencl/gpu_rigidbody_pipeline2/   P1/ = opencl/gpu_rigidbody_pipeline/
+ *   BB/ = opencl/broadphase_benchmark/      G3/ = opencl/3dGridBroadphase/Shared/
+ *   ST/ = dynamics/basic_demo/Stubs/         PR/ = opencl/primitives/AdlPrimitives/
+ */
+#ifndef B3GPU_H
+#define B3GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ */
+/* Status codes                                                         */
+/* ------------------------------------------------------------------ */
+enum {
+    B3_OK = 0,
+    B3_ERR_INVALID_ARG = 1,
+    B3_ERR_CUDA = 2,            /* a CUDA runtime call failed */
+    B3_ERR_CAPACITY = 3,        /* a fixed capacity would be exceeded */
+    B3_ERR_NO_DEVICE = 4,       /* no CUDA device / extension not usable */
+    B3_ERR_STATE = 5,           /* call out of order (e.g. step before write) */
+    B3_ERR_TIMEOUT = 6,         /* a device-side bounded wait gave up */
+    B3_ERR_UNSUPPORTED = 7
+};
+
+/* ------------------------------------------------------------------ */
+/* Reference-layout data types (byte-compatible where noted)            */
+/* ------------------------------------------------------------------ */
+
+/* RigidBodyBase::Body, ST/AdlRigidBody.h:26-45 (80 bytes, same layout). */
+typedef struct b3Body {
+    float pos[4];          /* w unused (0) */
+    float quat[4];         /* x, y, z, w */
+    float linVel[4];
+    float angVel[4];
+    uint32_t collidableIdx;
+    float invMass;
+    float restitution;
+    float friction;
+} b3Body;
+
+/* RigidBodyBase::Inertia, ST/AdlRigidBody.h:47-59 (96 bytes, same layout:
+ * two 3x4 row-major matrices, world then local inverse inertia). */
+typedef struct b3Inertia {
+    float invInertiaWorld[12];
+    float initInvInertia[12];
+} b3Inertia;
+
+/* btCollidable, P1/btCollidable.h:5-11 (16 bytes, same layout). */
+typedef struct b3Collidable {
+    int numChildShapes;
+    float radius;
+    int shapeType;         /* B3_SHAPE_CONVEX_HULL = 3 */
+    int shapeIndex;
+} b3Collidable;
+
+enum { B3_SHAPE_CONVEX_HULL = 3 };
+
+/* ConvexPolyhedronCL, P2/ConvexPolyhedronCL.h:15-31 (96 bytes, same layout). */
+typedef struct b3ConvexPolyhedron {
+    float localCenter[4];
+    float extents[4];
+    float mC[4];
+    float mE[4];
+    float radius;
+    int faceOffset;
+    int numFaces;
+    int numVertices;
+    int vertexOffset;
+    int uniqueEdgesOffset;
+    int numUniqueEdges;
+    int unused;
+} b3ConvexPolyhedron;
+
+/* btGpuFace, P2/ConvexPolyhedronCL.h:6-13 (plane + index range; padded to
+ * 32 bytes like the reference's 16-byte aligned struct). */
+typedef struct b3Face {
+    float plane[4];        /* outward normal xyz, w = plane constant */
+    int indexOffset;
+    int numIndices;
+    int pad[2];
+} b3Face;
+
+/* Contact manifold, after Contact4 (ST/AdlContact4.h:26-59), 96 bytes.
+ * worldPos[k].w = penetration depth (negative = penetrating);
+ * worldNormal.w = number of points (1..4), normal points from A to B.
+ * Differences from the reference: friction is a float (the reference packs
+ * u16 restitution + u16 friction), the combined restitution is derived from
+ * the two bodies in the solver, and m_batchIdx holds the broadphase pair
+ * index. Body fields carry a negative sign for static bodies. */
+typedef struct b3Contact4 {
+    float worldPos[4][4];
+    float worldNormal[4];
+    float friction;
+    int pairIndex;
+    int bodyAPtrAndSignBit;
+    int bodyBPtrAndSignBit;
+} b3Contact4;
+
+/* Step diagnostics (the reference truncates silently; the build counts). */
+typedef struct b3Counters {
+    int32_t numPairs;            /* broadphase pairs this step */
+    int32_t numManifolds;        /* contact manifolds this step */
+    int32_t numContactPoints;    /* sum of manifold points */
+    int32_t pairOverflow;        /* pairs dropped: per-body or global cap */
+    int32_t cellOverflow;        /* candidates skipped by the per-cell cap */
+    int32_t timeouts;            /* bounded device waits that gave up */
+    int32_t clipOverflow;        /* clipped polygons truncated to 64 verts */
+    int32_t steps;               /* steps executed since write_bodies */
+} b3Counters;
+
+/* ------------------------------------------------------------------ */
+/* Context (device + default stream)                                    */
+/* ------------------------------------------------------------------ */
+typedef struct b3Context_t* b3Context;
+
+/* Replaces btOpenCLUtils::createContextFromType + clCreateCommandQueue
+ * (opencl/basic_initialize/btOpenCLUtils.h:33-56). device = -1 creates a
+ * host-only context: shape and body registration work, anything that
+ * touches the GPU returns B3_ERR_NO_DEVICE. */
+int b3_context_create(int device, b3Context* out);
+int b3_context_destroy(b3Context ctx);
+int b3_sync(b3Context ctx, void* stream);
+/* Library + device description, one line (driver, SM count). */
+int b3_context_info(b3Context ctx, char* buf, int buflen);
+/* Last error message of this thread (static storage). */
+const char* b3_last_error(void);
+
+/* ------------------------------------------------------------------ */
+/* GPU primitives (device pointers, caller-owned)                       */
+/* ------------------------------------------------------------------ */
+
+/* btFillCL::execute (BB/btFillCL.h:85-126, PR/Fill/FillKernels.cl:47-96):
+ * dst[offset + i] = value for i < n. */
+int b3_fill_u32(b3Context ctx, uint32_t* d_dst, uint32_t value, int64_t n, int64_t offset, void* stream);
+/* FillInt2Kernel: dst[offset + i] = (x, y). */
+int b3_fill_int2(b3Context ctx, int32_t* d_dst_int2, int32_t x, int32_t y, int64_t n, int64_t offset, void* stream);
+
+/* btPrefixScanCL::execute (BB/btPrefixScanCL.cpp:46-98): exclusive scan
+ * d_dst[i] = sum_{j<i} d_src[j]; optional total written to d_sum (device)
+ * and/or *h_sum (host, synchronising). In-place allowed. No size limit
+ * (the reference's top level holds 2,048 blocks x 256). */
+int b3_prefix_scan_u32(b3Context ctx, const uint32_t* d_src, uint32_t* d_dst, int64_t n,
+                       uint32_t* d_sum, uint32_t* h_sum, void* stream);
+
+/* btRadixSort32CL::execute (BB/btRadixSort32CL.cpp:161-535): stable LSD
+ * key-value sort of n (key, value) pairs, in place. Only the low key_bits
+ * bits of the keys are sorted (1..32); keys must not use higher bits unless
+ * key_bits = 32. Onesweep with 8-bit digits: ceil(key_bits/8) passes. */
+int b3_radix_sort32_kv(b3Context ctx, uint32_t* d_keys, uint32_t* d_values, int64_t n,
+                       int key_bits, void* stream);
+/* Keys-only variant (RadixSort32 keys-only benchmark,
+ * opencl/primitives/AdlTest/RadixSortBenchmark.h:64). */
+int b3_radix_sort32_keys(b3Context ctx, uint32_t* d_keys, int64_t n, int key_bits, void* stream);
+
+/* btBoundSearchCL::execute (BB/btBoundSearchCL.cpp:78-136,
+ * PR/Search/BoundSearchKernels.cl:42-104) over sorted keys.
+ * mode 0 = LOWER: d_dst[k] = first index with key == k (untouched if absent)
+ * mode 1 = UPPER: d_dst[k] = one past the last index with key == k
+ * mode 2 = COUNT: d_dst[k] = number of keys equal to k (fills 0 first).
+ * Keys >= n_dst are ignored (the reference would write out of range). */
+int b3_bound_search(b3Context ctx, const uint32_t* d_sorted_keys, int64_t n_src,
+                    uint32_t* d_dst, int64_t n_dst, int mode, void* stream);
+
+/* ------------------------------------------------------------------ */
+/* World: rigid-body & collidable arrays, grid broadphase,              */
+/* narrowphase-and-solver, stepSimulation                               */
+/* ------------------------------------------------------------------ */
+typedef struct b3World_t* b3World;
+
+enum { B3_FRICTION_GEOMEAN = 0, B3_FRICTION_PRODUCT = 1 };
+
+typedef struct b3WorldConfig {
+    int32_t maxBodies;            /* capacity (no 128K cap, P1/btGpuNarrowPhaseAndSolver.h:24) */
+    int32_t maxPairs;             /* dense pair-list capacity */
+    int32_t numWorlds;            /* 1 = plain step; >1 = batched independent worlds */
+    float   cellSize;             /* grid cell edge (m) */
+    int32_t gridDims[3];          /* per-world grid, powers of two (G3/bt3dGridBroadphaseOCL.cl:7-9) */
+    int32_t maxBodiesPerCell;     /* bucket cap, reference maxSmallProxiesPerCell */
+    int32_t maxPairsPerBody;      /* per-body cap, reference maxPairsPerSmallProxy */
+    float   maxSmallProxySize;    /* AABB half-diagonal > half this => large body */
+    float   gravity[3];
+    float   dt;
+    int32_t solverIterations;     /* btContactSolverInfo::m_numIterations */
+    float   erp;                  /* Baumgarte factor, m_erp (0.2) */
+    float   contactBreaking;      /* clip keep threshold maxDist (0.02) */
+    float   contactProcessing;    /* solver distance threshold (0.02) */
+    float   linearSlopOffset;     /* distance = depth + this (0.01, P2/btPgsJacobiSolver.cpp:124-155) */
+    float   angularDamping;       /* per-step factor (0.99, BB/integrateKernel.cl:124-126) */
+    int32_t frictionCombine;      /* B3_FRICTION_* */
+    int32_t useGraph;             /* capture the step as a CUDA graph */
+    int32_t flags;                /* reserved, 0 */
+} b3WorldConfig;
+
+/* Defaults: reference constants (P2/CLPhysicsDemo.cpp:603-653,
+ * BB/integrateKernel.cl:102-158, P2/btPgsJacobiSolver.cpp:171-191). */
+void b3_world_config_default(b3WorldConfig* cfg);
+
+int b3_world_create(b3Context ctx, const b3WorldConfig* cfg, b3World* out);
+int b3_world_destroy(b3World w);
+
+/* CLPhysicsDemo::registerConvexPolyhedron (P2/CLPhysicsDemo.cpp:491-531 ->
+ * btConvexUtility::initializePolyhedralFeatures P1/btConvexUtility.cpp:31-270
+ * -> btGpuNarrowphaseAndSolver::registerConvexHullShape
+ * P1/btGpuNarrowPhaseAndSolver.cpp:423-490): convex hull of the scaled
+ * points, coplanar face weld, unique edges; local centre = vertex average
+ * (P2/CLPhysicsDemo.cpp:360-366). Returns the collidable index. */
+int b3_register_convex_hull(b3World w, const float* vertices, int numVertices, int strideBytes,
+                            const float scaling[3], int* collidableOut);
+
+/* CLPhysicsDemo::registerPhysicsInstance (P2/CLPhysicsDemo.cpp:533-599) ->
+ * btGpuNarrowphaseAndSolver::registerRigidBody (P1/...cpp:566-657):
+ * mass 0 = static. Inverse inertia from the registration AABB (margin
+ * 0.01) with full extents, as the reference does. worldId selects the
+ * independent world in batched mode (0 for plain). Returns the body id. */
+int b3_register_body(b3World w, float mass, const float position[3], const float orientation[4],
+                     int collidable, float friction, float restitution, int worldId, int* bodyOut);
+
+/* Bulk form of b3_register_body for n bodies (arrays of n, xyz / xyzw
+ * packed); writes the id of the first new body. */
+int b3_register_bodies(b3World w, int n, const float* masses, const float* positions3,
+                       const float* orientations4, const int* collidables, const float* frictions,
+                       const float* restitutions, const int* worldIds, int* firstBodyOut);
+
+/* Upload all registered bodies, inertias and collidables
+ * (CLPhysicsDemo::writeBodiesToGpu P2/CLPhysicsDemo.cpp:205-216). */
+int b3_write_bodies(b3World w, void* stream);
+/* Bulk velocity write (CLPhysicsDemo::setObjectLinearVelocity generalised):
+ * xyz triples for each body, NULL to leave unchanged. Host pointers. */
+int b3_write_velocities(b3World w, const float* linVel3, const float* angVel3, void* stream);
+
+/* CLPhysicsDemo::stepSimulation (P2/CLPhysicsDemo.cpp:740-943): AABB+hash,
+ * sort, cell start, pair search, gravity, SAT+clip+reduce, constraint
+ * setup, Jacobi solve with velocity averaging, integrate; n steps. */
+int b3_step(b3World w, int numSteps, void* stream);
+
+/* Read bodies back in the reference Body layout (host, synchronising). */
+int b3_read_bodies(b3World w, b3Body* out, int maxBodies, void* stream);
+/* Read SoA state (host float4 arrays, NULL to skip; synchronising). */
+int b3_read_state(b3World w, float* pos4, float* quat4, float* linVel4, float* angVel4, void* stream);
+/* Write SoA state (host float4 arrays, NULL to skip). */
+int b3_write_state(b3World w, const float* pos4, const float* quat4, const float* linVel4,
+                   const float* angVel4, void* stream);
+int b3_get_num_bodies(b3World w, int* n);
+int b3_get_counters(b3World w, b3Counters* out, void* stream);
+int b3_reset_counters(b3World w, void* stream);
+
+/* --- stage entry points (each one stage of stepSimulation) --- */
+/* setupGpuAabbsFull + gravity (BB/broadphaseKernel.cl:293-331,163-213). */
+int b3_stage_aabbs(b3World w, void* stream);
+/* btGridBroadphaseCl::calculateOverlappingPairs (BB/btGridBroadphaseCL.cpp:135-238):
+ * hash, radix sort, cell start, 27-cell + large-body pair search, compaction. */
+int b3_stage_broadphase(b3World w, void* stream);
+/* btGpuNarrowphaseAndSolver::computeContacts (P1/...cpp:873-1070) via
+ * GpuSatCollision::computeConvexConvexContactsGPUSAT (P2/ConvexHullContact.cpp:1793). */
+int b3_stage_narrowphase(b3World w, void* stream);
+/* btPgsJacobiSolver::solveGroup (P2/btPgsJacobiSolver.cpp:195-215):
+ * setup, iterations with velocity averaging, finish. */
+int b3_stage_solve(b3World w, void* stream);
+/* integrateTransformsKernel2 (BB/integrateKernel.cl:102-158). */
+int b3_stage_integrate(b3World w, void* stream);
+
+/* --- stage outputs (host copies, synchronising) --- */
+/* World AABBs, 2 float4 per body (min.w = body id bits, max.w = dynamic flag). */
+int b3_get_aabbs(b3World w, float* out8, int maxBodies, void* stream);
+/* Sorted (cell key, body id) of the small bodies; returns count. */
+int b3_get_sorted_hash(b3World w, uint32_t* keys, uint32_t* values, int max, int* count, void* stream);
+/* Broadphase pairs (x = self, y = other); returns count. */
+int b3_get_pairs(b3World w, int32_t* pairs2, int max, int* count, void* stream);
+/* Contact manifolds in pair order; returns count. */
+int b3_get_contacts(b3World w, b3Contact4* out, int max, int* count, void* stream);
+/* Shape tables after registration (for checking / interop). */
+int b3_get_shape_sizes(b3World w, int* numCollidables, int* numPolys, int* numVertices,
+                       int* numFaces, int* numIndices, int* numEdges);
+int b3_get_shapes(b3World w, b3Collidable* cols, b3ConvexPolyhedron* polys, float* vertices4,
+                  b3Face* faces, int* indices, float* edges4, float* localAabbs8);
+int b3_get_inertias(b3World w, b3Inertia* out, int maxBodies);
+
+/* --- device buffers (borrowed views, like getBodiesGpu / getContactsGpu,
+ *     P1/btGpuNarrowPhaseAndSolver.h:104-111) --- */
+enum {
+    B3_BUF_POS = 0, B3_BUF_QUAT = 1, B3_BUF_LINVEL = 2, B3_BUF_ANGVEL = 3,
+    B3_BUF_AABB_MIN = 4, B3_BUF_AABB_MAX = 5, B3_BUF_PAIRS = 6, B3_BUF_CONTACTS = 7,
+    B3_BUF_COUNTERS = 8, B3_BUF_INVMASS = 9
+};
+int b3_get_device_buffer(b3World w, int which, void** d_ptr, int64_t* bytes);
+
+/* CUDA-event timing of each stage of the last timed step (ms). */
+int b3_set_stage_timing(b3World w, int enable);
+int b3_get_stage_times(b3World w, float* ms, int max, int* count);
+
+/* ------------------------------------------------------------------ */
+/* Batched worlds: thousands of independent worlds in one launch per    */
+/* stage. World ids go into the high bits of the cell keys, pair and    */
+/* contact arrays are segmented by world. Configure with numWorlds > 1  */
+/* in b3WorldConfig and pass worldId to b3_register_body.               */
+/* ------------------------------------------------------------------ */
+/* Per-world aggregate: centre of mass and kinetic energy, 4 floats per
+ * world (x, y, z, KE) computed on device; host output. */
+int b3_batch_world_stats(b3World w, float* out4, int numWorlds, void* stream);
+/* Autotuner: time the candidate launch shapes of the tunable kernels on
+ * the current scene and keep the fastest (steps are run and rolled back). */
+int b3_autotune(b3World w, int trialSteps, void* stream);
+int b3_get_tuning(b3World w, int* values, int max, int* count);
+
+/* ------------------------------------------------------------------ */
+/* Adjoint (reverse mode)                                               */
+/* ------------------------------------------------------------------ */
+typedef struct b3Adjoint_t* b3Adjoint;
+
+/* Forward run of numSteps steps with body-state checkpoints every
+ * checkpointEvery steps; the backward pass recomputes each segment and
+ * records its tape (contacts, active sets, clamp masks, iterates). */
+int b3_adjoint_create(b3World w, int numSteps, int checkpointEvery, b3Adjoint* out);
+int b3_adjoint_destroy(b3Adjoint a);
+int b3_adjoint_forward(b3Adjoint a, void* stream);
+/* Seed: dLoss/d(final state) as float4 arrays (host; NULL = zero). */
+int b3_adjoint_backward(b3Adjoint a, const float* dPos4, const float* dQuat4, const float* dLinVel4,
+                        const float* dAngVel4, void* stream);
+/* Gradients w.r.t. initial linear/angular velocities (float4 per body),
+ * masses and friction coefficients (float per body). Host outputs. */
+int b3_adjoint_gradients(b3Adjoint a, float* dLinVel4, float* dAngVel4, float* dMass, float* dFriction);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* B3GPU_H */

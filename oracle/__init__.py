@@ -1,0 +1,278 @@
+"""ORACLE — test infrastructure only.
+
+Python binding of the single-threaded C++ restatement of the reference
+rigid-body step (oracle/b3_oracle.cpp) and of the reference pieces compiled
+from the reference's own sources (oracle/_ref/libb3ref.so). Only tests/,
+__graft_entry__.smoke() and bench.py's CPU-baseline leg use this package, as
+the checker; the product (experiments_b200) never imports it.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libb3ref.so")
+
+
+class OrConfig(C.Structure):
+    _fields_ = [("cellSize", C.c_float), ("dims", C.c_int * 3), ("maxBodiesPerCell", C.c_int),
+                ("maxPairsPerBody", C.c_int), ("gravity", C.c_float * 3), ("dt", C.c_float),
+                ("iterations", C.c_int), ("erp", C.c_float), ("contactBreaking", C.c_float),
+                ("contactProcessing", C.c_float), ("slopOffset", C.c_float), ("angularDamping", C.c_float),
+                ("frictionCombine", C.c_int), ("numWorlds", C.c_int)]
+
+
+class OrContact(C.Structure):
+    _fields_ = [("pos", (C.c_double * 4) * 4), ("normal", C.c_double * 4), ("friction", C.c_double),
+                ("pairIndex", C.c_int), ("bodyA", C.c_int), ("bodyB", C.c_int), ("pad", C.c_int)]
+
+
+_lib = None
+_ref = None
+_D = C.POINTER(C.c_double)
+_F = C.POINTER(C.c_float)
+_I = C.POINTER(C.c_int)
+_U = C.POINTER(C.c_uint32)
+_VP = C.c_void_p
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            from . import build
+            build.build_oracle()
+        L = C.CDLL(LIB)
+        L.or_world_create.restype = _VP
+        L.or_world_create.argtypes = [C.POINTER(OrConfig), C.c_int, _F, _F, _F, _I, _I, _I, _F, C.c_int, _I,
+                                      C.c_int, _VP, C.c_int, _F, C.c_int, _VP, C.c_int, _I, C.c_int, _F, _F]
+        L.or_world_destroy.argtypes = [_VP]
+        L.or_set_state_f32.argtypes = [_VP, _F, _F, _F, _F]
+        L.or_set_state_f64.argtypes = [_VP, _D, _D, _D, _D]
+        L.or_get_state.argtypes = [_VP, _D, _D, _D, _D]
+        for s in ("aabbs", "broadphase", "narrowphase", "solve", "integrate"):
+            getattr(L, "or_stage_" + s).argtypes = [_VP]
+        L.or_step.argtypes = [_VP, C.c_int]
+        L.or_get_aabbs.argtypes = [_VP, _F]
+        L.or_get_sorted.argtypes = [_VP, _U, _U, C.c_int]
+        L.or_get_pairs.argtypes = [_VP, _I, C.c_int]
+        L.or_get_contacts.argtypes = [_VP, C.POINTER(OrContact), C.c_int]
+        L.or_get_overflow.argtypes = [_VP, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+        L.or_set_contacts.argtypes = [_VP, C.POINTER(OrContact), C.c_int]
+        L.or_set_pairs.argtypes = [_VP, _I, C.c_int]
+        L.or_pair_contact.argtypes = [_VP, C.c_int, C.c_int, C.POINTER(OrContact)]
+        L.or_clip_reduce.argtypes = [_VP, C.c_int, C.c_int, _D, _D, _D, C.c_int, C.c_double, _D, _D, _I]
+        L.or_solve_velocities.argtypes = [_VP, _D, _D]
+        _lib = L
+    return _lib
+
+
+def ref_lib():
+    """The reference pieces compiled from its sources, or None if absent."""
+    global _ref
+    if _ref is None and os.path.exists(REF_LIB):
+        R = C.CDLL(REF_LIB)
+        R.ref_jacobi_solve.argtypes = [C.c_int, _VP, _VP, C.c_int, _VP]
+        R.ref_hull.argtypes = [_F, C.c_int, _F, C.c_int, _I, _F, _I, C.c_int, _I, _I, C.c_int, _F, C.c_int, _I]
+        R.ref_clip_reduce.argtypes = [_F, _I, _I, _F, _F, _F, C.c_int, _F, _I, C.c_int, _I, C.c_int, _F, _F, _F,
+                                      _F, C.c_float, _F, _I]
+        _ref = R
+    return _ref
+
+
+def _f(a):
+    return a.ctypes.data_as(_F)
+
+
+def _i(a):
+    return a.ctypes.data_as(_I)
+
+
+def _d(a):
+    return a.ctypes.data_as(_D)
+
+
+class OracleWorld:
+    """Oracle world built from a registered product world's shape tables
+    (hull construction is checked separately against btConvexUtility)."""
+
+    def __init__(self, scene, shapes, cfg, inv_inertia, is_large):
+        L = lib()
+        self.n = scene.n
+        c = OrConfig()
+        c.cellSize = cfg.cellSize
+        for k in range(3):
+            c.dims[k] = cfg.gridDims[k]
+            c.gravity[k] = cfg.gravity[k]
+        c.maxBodiesPerCell = cfg.maxBodiesPerCell
+        c.maxPairsPerBody = cfg.maxPairsPerBody
+        c.dt = cfg.dt
+        c.iterations = cfg.solverIterations
+        c.erp = cfg.erp
+        c.contactBreaking = cfg.contactBreaking
+        c.contactProcessing = cfg.contactProcessing
+        c.slopOffset = cfg.linearSlopOffset
+        c.angularDamping = cfg.angularDamping
+        c.frictionCombine = cfg.frictionCombine
+        c.numWorlds = cfg.numWorlds
+        self.cfg = c
+        n = scene.n
+        m = np.asarray(scene.mass, np.float64)
+        self._keep = dict(
+            invMass=np.ascontiguousarray(np.where(m != 0, 1.0 / np.where(m != 0, m, 1), 0).astype(np.float32)),
+            fr=np.ascontiguousarray(scene.friction.astype(np.float32)),
+            rs=np.zeros(n, np.float32),
+            col=np.ascontiguousarray(shapes["col_of_body"].astype(np.int32)),
+            wid=np.ascontiguousarray(scene.world.astype(np.int32)),
+            large=np.ascontiguousarray(np.asarray(is_large, np.int32)),
+            ii=np.ascontiguousarray(np.asarray(inv_inertia, np.float32).reshape(n, 4)),
+            colShape=np.ascontiguousarray(np.array([shapes["cols"][k].shapeIndex for k in range(shapes["counts"][0])],
+                                                   np.int32)),
+            verts=np.ascontiguousarray(shapes["verts"].astype(np.float32)),
+            idx=np.ascontiguousarray(shapes["idx"].astype(np.int32)),
+            edges=np.ascontiguousarray(shapes["edges"].astype(np.float32)),
+            laabb=np.ascontiguousarray(shapes["localAabb"].astype(np.float32)),
+        )
+        k = self._keep
+        nc, npo, nv, nf, ni, ne = shapes["counts"]
+        self.h = L.or_world_create(C.byref(c), n, _f(k["invMass"]), _f(k["fr"]), _f(k["rs"]), _i(k["col"]),
+                                   _i(k["wid"]), _i(k["large"]), _f(k["ii"]), nc, _i(k["colShape"]), npo,
+                                   C.cast(shapes["polys"], _VP), nv, _f(k["verts"]), nf,
+                                   C.cast(shapes["faces"], _VP), ni, _i(k["idx"]), ne, _f(k["edges"]),
+                                   _f(k["laabb"]))
+        self.L = L
+        pos4 = np.zeros((n, 4), np.float32)
+        pos4[:, :3] = scene.pos
+        lin4 = np.zeros((n, 4), np.float32)
+        lin4[:, :3] = scene.lin
+        ang4 = np.zeros((n, 4), np.float32)
+        ang4[:, :3] = scene.ang
+        self.set_state_f32(pos4, np.ascontiguousarray(scene.quat.astype(np.float32)), lin4, ang4)
+
+    def set_state_f32(self, pos4, quat4, lin4, ang4):
+        arrs = [np.ascontiguousarray(np.asarray(a, np.float32).reshape(self.n, 4)) for a in (pos4, quat4, lin4, ang4)]
+        self.L.or_set_state_f32(self.h, *[_f(a) for a in arrs])
+
+    def set_state_f64(self, pos4, quat4, lin4, ang4):
+        arrs = [np.ascontiguousarray(np.asarray(a, np.float64).reshape(self.n, 4)) for a in (pos4, quat4, lin4, ang4)]
+        self.L.or_set_state_f64(self.h, *[_d(a) for a in arrs])
+
+    def state(self):
+        out = [np.zeros((self.n, 4), np.float64) for _ in range(4)]
+        self.L.or_get_state(self.h, *[_d(a) for a in out])
+        return out
+
+    def stage(self, name):
+        getattr(self.L, "or_stage_" + name)(self.h)
+
+    def step(self, steps=1):
+        self.L.or_step(self.h, steps)
+
+    def aabbs(self):
+        out = np.zeros((self.n, 8), np.float32)
+        self.L.or_get_aabbs(self.h, _f(out))
+        return out
+
+    def sorted_hash(self):
+        cnt = self.L.or_get_sorted(self.h, None, None, 0)
+        k = np.zeros(max(cnt, 1), np.uint32)
+        v = np.zeros(max(cnt, 1), np.uint32)
+        self.L.or_get_sorted(self.h, k.ctypes.data_as(_U), v.ctypes.data_as(_U), cnt)
+        return k[:cnt], v[:cnt]
+
+    def pairs(self):
+        cnt = self.L.or_get_pairs(self.h, None, 0)
+        out = np.zeros((max(cnt, 1), 2), np.int32)
+        self.L.or_get_pairs(self.h, _i(out), cnt)
+        return out[:cnt]
+
+    def set_pairs(self, pairs):
+        p = np.ascontiguousarray(np.asarray(pairs, np.int32).reshape(-1, 2))
+        self.L.or_set_pairs(self.h, _i(p), p.shape[0])
+
+    def contacts(self):
+        cnt = self.L.or_get_contacts(self.h, None, 0)
+        arr = (OrContact * max(cnt, 1))()
+        self.L.or_get_contacts(self.h, arr, cnt)
+        raw = np.frombuffer(C.string_at(C.addressof(arr), C.sizeof(OrContact) * cnt), np.uint8)
+        raw = raw.reshape(cnt, C.sizeof(OrContact)) if cnt else np.zeros((0, C.sizeof(OrContact)), np.uint8)
+        d = raw[:, :168].copy().view(np.float64).reshape(cnt, 21) if cnt else np.zeros((0, 21))
+        i = raw[:, 168:184].copy().view(np.int32).reshape(cnt, 4) if cnt else np.zeros((0, 4), np.int32)
+        return dict(pos=d[:, :16].reshape(-1, 4, 4), normal=d[:, 16:20], friction=d[:, 20], pairIndex=i[:, 0],
+                    bodyA=i[:, 1], bodyB=i[:, 2])
+
+    def set_contacts(self, c):
+        n = len(c["normal"])
+        arr = (OrContact * max(n, 1))()
+        for j in range(n):
+            for a in range(4):
+                for b in range(4):
+                    arr[j].pos[a][b] = float(c["pos"][j][a][b])
+                arr[j].normal[a] = float(c["normal"][j][a])
+            arr[j].friction = float(c["friction"][j])
+            arr[j].pairIndex = int(c["pairIndex"][j])
+            arr[j].bodyA = int(c["bodyA"][j])
+            arr[j].bodyB = int(c["bodyB"][j])
+        self.L.or_set_contacts(self.h, arr, n)
+
+    def overflow(self):
+        a, b = C.c_longlong(), C.c_longlong()
+        self.L.or_get_overflow(self.h, C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def solve_velocities(self):
+        lin = np.zeros((self.n, 4))
+        ang = np.zeros((self.n, 4))
+        self.L.or_solve_velocities(self.h, _d(lin), _d(ang))
+        return lin, ang
+
+    def close(self):
+        if self.h:
+            self.L.or_world_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def oracle_from_world(world, scene, cfg=None):
+    """Build an OracleWorld from a registered PhysicsWorld (host-only
+    context suffices) and its scene."""
+    cfg = cfg or world.cfg
+    sh = world.shapes()
+    n_shapes = len(scene.shapes)
+    # body collidable index = scene.shape (shapes are registered in scene order)
+    sh["col_of_body"] = np.asarray(scene.shape, np.int32)
+    assert sh["counts"][0] == n_shapes
+    inv_inertia = world.inertias()
+    # large-body classification rule (half-diagonal of the registration AABB)
+    is_large = large_flags(world, scene, cfg)
+    return OracleWorld(scene, sh, cfg, inv_inertia, is_large)
+
+
+def large_flags(world, scene, cfg):
+    """Registration-AABB half-diagonal > maxSmallProxySize / 2, computed from
+    the scene and the local AABBs (G3/btGpu3DGridBroadphase.cpp:385-391)."""
+    sh = world.shapes()
+    la = sh["localAabb"]
+    n = scene.n
+    out = np.zeros(n, np.int32)
+    for i in range(n):
+        c = scene.shape[i]
+        lmin = la[c, :3].astype(np.float64)
+        lmax = la[c, 4:7].astype(np.float64)
+        he = 0.5 * (lmax - lmin) + 0.01
+        x, y, z, w = [float(v) for v in scene.quat[i]]
+        s = 2.0 / (x * x + y * y + z * z + w * w)
+        R = np.array([[1 - (y * y + z * z) * s, (x * y - w * z) * s, (x * z + w * y) * s],
+                      [(x * y + w * z) * s, 1 - (x * x + z * z) * s, (y * z - w * x) * s],
+                      [(x * z - w * y) * s, (y * z + w * x) * s, 1 - (x * x + y * y) * s]])
+        e = np.abs(R) @ he
+        r = 0.5 * np.linalg.norm(2 * e)
+        out[i] = 1 if r > 0.5 * cfg.maxSmallProxySize else 0
+    return out

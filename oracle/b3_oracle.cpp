@@ -1,0 +1,1010 @@
+// ORACLE — test infrastructure only. Single-threaded CPU restatement of the
+// reference GPU rigid-body step (erwincoumans/experiments,
+// opencl/gpu_rigidbody_pipeline2 and dependencies), used by tests/, the
+// smoke check and bench.py's CPU baseline leg as the checker. Nothing in the
+// product links or calls this file.
+//
+// Precision: the world AABB and cell hash are evaluated in FP32 with the
+// same operation order as the device kernel (compiled with
+// -ffp-contract=off), so cell keys, the stable sort and the pair set are
+// bit-comparable when both start from the same FP32 state. Narrowphase,
+// constraint setup, Jacobi iterations and integration run in FP64 (Real).
+//
+// Parity pins (see oracle/ref_shim.cpp and tests/test_oracle_pins.py):
+//   * the Jacobi solver against the reference's own btPgsJacobiSolver
+//     (P2/btPgsJacobiSolver.cpp) compiled from the reference sources,
+//   * clipping + contact reduction against the reference host port
+//     (P2/satClipHullContacts.cpp),
+//   * hull tables against btConvexUtility (P1/btConvexUtility.cpp),
+//   * analytic known-answer contact cases.
+//
+// Reference citations (paths relative to the reference project root):
+//   AABB      opencl/broadphase_benchmark/broadphaseKernel.cl:91-113,293-331
+//   hash      opencl/3dGridBroadphase/Shared/bt3dGridBroadphaseOCL.cl:4-48
+//   pairs     opencl/3dGridBroadphase/Shared/bt3dGridBroadphaseOCL.cl:89-215
+//   SAT       opencl/gpu_rigidbody_pipeline2/sat.cl:227-252,497-635,928-1262
+//   clip      opencl/gpu_rigidbody_pipeline2/satClipHullContacts.cl:303-452,556-611
+//   reduce    opencl/gpu_rigidbody_pipeline2/satClipHullContacts.cl:678-770,1958-2039
+//   solver    opencl/gpu_rigidbody_pipeline2/btPgsJacobiSolver.cpp:124-155,505-592,
+//             689-888,933-1080,1081-1370,1372-1823
+//   integrate opencl/broadphase_benchmark/integrateKernel.cl:102-158
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+typedef double Real;
+
+namespace {
+
+struct V {
+    Real x, y, z;
+    V() : x(0), y(0), z(0) {}
+    V(Real a, Real b, Real c) : x(a), y(b), z(c) {}
+};
+inline V operator+(V a, V b) { return V(a.x + b.x, a.y + b.y, a.z + b.z); }
+inline V operator-(V a, V b) { return V(a.x - b.x, a.y - b.y, a.z - b.z); }
+inline V operator-(V a) { return V(-a.x, -a.y, -a.z); }
+inline V operator*(V a, Real s) { return V(a.x * s, a.y * s, a.z * s); }
+inline Real dot(V a, V b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline V cross(V a, V b) { return V(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+inline V mulv(V a, V b) { return V(a.x * b.x, a.y * b.y, a.z * b.z); }
+inline V normalize(V a) {
+    Real l = std::sqrt(dot(a, a));
+    return l > 0 ? a * (1.0 / l) : a;
+}
+struct Q {
+    Real x, y, z, w;
+};
+// qtMul / qtRotate (sat.cl:146-230) in Real
+inline Q qmul(Q a, Q b) {
+    V c = cross(V(a.x, a.y, a.z), V(b.x, b.y, b.z));
+    Q r;
+    r.x = c.x + a.w * b.x + b.w * a.x;
+    r.y = c.y + a.w * b.y + b.w * a.y;
+    r.z = c.z + a.w * b.z + b.w * a.z;
+    r.w = a.w * b.w - (a.x * b.x + a.y * b.y + a.z * b.z);
+    return r;
+}
+inline V qrot(Q q, V v) {
+    Q qi = {-q.x, -q.y, -q.z, q.w};
+    Q vv = {v.x, v.y, v.z, 0};
+    Q r = qmul(qmul(q, vv), qi);
+    return V(r.x, r.y, r.z);
+}
+inline V qinvrot(Q q, V v) { return qrot(Q{-q.x, -q.y, -q.z, q.w}, v); }
+
+}  // namespace
+
+extern "C" {
+
+// Shape tables (layout of the reference's ConvexPolyhedronCL / btGpuFace).
+struct or_poly {
+    float localCenter[4], extents[4], mC[4], mE[4];
+    float radius;
+    int faceOffset, numFaces, numVertices, vertexOffset, uniqueEdgesOffset, numUniqueEdges, unused;
+};
+struct or_face {
+    float plane[4];
+    int indexOffset, numIndices, pad[2];
+};
+struct or_contact {  // Contact4-like, FP64
+    double pos[4][4];
+    double normal[4];  // w = nPoints
+    double friction;
+    int pairIndex, bodyA, bodyB, pad;
+};
+
+struct or_config {
+    float cellSize;
+    int dims[3];
+    int maxBodiesPerCell;
+    int maxPairsPerBody;
+    float gravity[3];
+    float dt;
+    int iterations;
+    float erp;
+    float contactBreaking;
+    float contactProcessing;
+    float slopOffset;
+    float angularDamping;
+    int frictionCombine;  // 0 = sqrt(a*b), 1 = a*b
+    int numWorlds;
+};
+
+struct or_world {
+    or_config cfg;
+    int n;
+    int cellBits;
+    // static body data
+    std::vector<float> invMass, friction, restitution;
+    std::vector<int> col, worldId, isLarge;
+    std::vector<Real> invInertia;  // 3 per body
+    // shapes
+    std::vector<int> colShape;
+    std::vector<or_poly> polys;
+    std::vector<float> verts4, edges4, localAabb8;
+    std::vector<or_face> faces;
+    std::vector<int> indices;
+    // state (FP64) and its FP32 image for the integer stages
+    std::vector<Real> pos, quat, lin, ang;  // 4 per body
+    // stage outputs
+    std::vector<float> aabb;                 // 8 per body
+    std::vector<uint32_t> keys, vals;        // sorted (small bodies)
+    std::vector<int> pairs;                  // 2 per pair
+    std::vector<or_contact> contacts;        // manifolds in pair order
+    std::vector<Real> avgLin, avgAng;        // 3 per body (sum/count after the last average)
+    std::vector<int> count;                  // copies per body
+    long long pairOverflow, cellOverflow;
+};
+
+}  // extern "C"
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// FP32 stage: AABB + gravity + hash (exact operation order, no contraction)
+// ---------------------------------------------------------------------------
+inline float d3(const float a[4], const float b[4]) { return ((a[0] * b[0]) + (a[1] * b[1])) + (a[2] * b[2]); }
+
+void qmul_f(const float a[4], const float b[4], float r[4]) {
+    const float c0 = a[1] * b[2] - a[2] * b[1];
+    const float c1 = a[2] * b[0] - a[0] * b[2];
+    const float c2 = a[0] * b[1] - a[1] * b[0];
+    r[0] = c0 + ((a[3] * b[0]) + (b[3] * a[0]));
+    r[1] = c1 + ((a[3] * b[1]) + (b[3] * a[1]));
+    r[2] = c2 + ((a[3] * b[2]) + (b[3] * a[2]));
+    r[3] = (a[3] * b[3]) - d3(a, b);
+}
+
+void aabb_f32(const float p[4], const float q[4], const float* lmn, const float* lmx, float out[8]) {
+    const float he[4] = {(lmx[0] - lmn[0]) * 0.5f, (lmx[1] - lmn[1]) * 0.5f, (lmx[2] - lmn[2]) * 0.5f, 0.f};
+    const float lc[4] = {(lmx[0] + lmn[0]) * 0.5f, (lmx[1] + lmn[1]) * 0.5f, (lmx[2] + lmn[2]) * 0.5f, 0.f};
+    const float qi[4] = {-q[0], -q[1], -q[2], q[3]};
+    float t[4], wc[4];
+    qmul_f(q, lc, t);
+    qmul_f(t, qi, wc);
+    wc[0] = wc[0] + p[0];
+    wc[1] = wc[1] + p[1];
+    wc[2] = wc[2] + p[2];
+    const float x2 = q[0] * q[0], y2 = q[1] * q[1], z2 = q[2] * q[2];
+    const float tx = 2.f * q[0], ty = 2.f * q[1], tw = 2.f * q[3];
+    const float r0[4] = {std::fabs((1.f - 2.f * y2) - 2.f * z2), std::fabs(tx * q[1] - tw * q[2]),
+                         std::fabs(tx * q[2] + tw * q[1]), 0.f};
+    const float r1[4] = {std::fabs(tx * q[1] + tw * q[2]), std::fabs((1.f - 2.f * x2) - 2.f * z2),
+                         std::fabs(ty * q[2] - tw * q[0]), 0.f};
+    const float r2[4] = {std::fabs(tx * q[2] - tw * q[1]), std::fabs(ty * q[2] + tw * q[0]),
+                         std::fabs((1.f - 2.f * x2) - 2.f * y2), 0.f};
+    const float e[3] = {d3(r0, he), d3(r1, he), d3(r2, he)};
+    for (int k = 0; k < 3; ++k) {
+        out[k] = wc[k] - e[k];
+        out[4 + k] = wc[k] + e[k];
+    }
+}
+
+inline int gcoord(float c, float inv, int dim) { return ((int)std::floor(c * inv)) & (dim - 1); }
+
+void stage_aabbs(or_world* w) {
+    const int N = w->n;
+    w->aabb.assign(8 * (size_t)N, 0.f);
+    const float gdt[3] = {w->cfg.gravity[0] * w->cfg.dt, w->cfg.gravity[1] * w->cfg.dt, w->cfg.gravity[2] * w->cfg.dt};
+    for (int i = 0; i < N; ++i) {
+        float p[4] = {(float)w->pos[4 * i], (float)w->pos[4 * i + 1], (float)w->pos[4 * i + 2], 0.f};
+        float q[4] = {(float)w->quat[4 * i], (float)w->quat[4 * i + 1], (float)w->quat[4 * i + 2], (float)w->quat[4 * i + 3]};
+        const int c = w->col[i];
+        float* o = &w->aabb[8 * (size_t)i];
+        aabb_f32(p, q, &w->localAabb8[8 * c], &w->localAabb8[8 * c + 4], o);
+        int id = i;
+        memcpy(&o[3], &id, 4);
+        int dyn = w->invMass[i] == 0.f ? 0 : 1;
+        memcpy(&o[7], &dyn, 4);
+        if (w->invMass[i] != 0.f)
+            for (int k = 0; k < 3; ++k) w->lin[4 * i + k] += (Real)gdt[k];
+    }
+}
+
+void stage_broadphase(or_world* w) {
+    const int N = w->n;
+    const float inv = 1.f / w->cfg.cellSize;
+    const int dx = w->cfg.dims[0], dy = w->cfg.dims[1], dz = w->cfg.dims[2];
+    struct KV {
+        uint32_t k, v;
+    };
+    std::vector<KV> kv;
+    for (int i = 0; i < N; ++i) {
+        if (w->isLarge[i]) continue;
+        const float* a = &w->aabb[8 * (size_t)i];
+        const float cx = (a[0] + a[4]) * 0.5f, cy = (a[1] + a[5]) * 0.5f, cz = (a[2] + a[6]) * 0.5f;
+        const int gx = gcoord(cx, inv, dx), gy = gcoord(cy, inv, dy), gz = gcoord(cz, inv, dz);
+        const uint32_t h = (uint32_t)(gz * dy * dx + gy * dx + gx);
+        kv.push_back({((uint32_t)w->worldId[i] << w->cellBits) | h, (uint32_t)i});
+    }
+    // stable LSD sort == stable sort by key (btRadixSort32CL::executeHost)
+    std::stable_sort(kv.begin(), kv.end(), [](const KV& a, const KV& b) { return a.k < b.k; });
+    const int ns = (int)kv.size();
+    w->keys.resize(ns);
+    w->vals.resize(ns);
+    for (int i = 0; i < ns; ++i) {
+        w->keys[i] = kv[i].k;
+        w->vals[i] = kv[i].v;
+    }
+    // cell starts (first sorted index per key)
+    std::vector<std::pair<uint32_t, int>> starts;
+    for (int i = 0; i < ns; ++i)
+        if (i == 0 || w->keys[i - 1] != w->keys[i]) starts.push_back({w->keys[i], i});
+    auto find_start = [&](uint32_t h) -> int {
+        auto it = std::lower_bound(starts.begin(), starts.end(), std::make_pair(h, -1));
+        if (it == starts.end() || it->first != h) return -1;
+        return it->second;
+    };
+    // large bodies per world
+    std::vector<std::vector<int>> large(w->cfg.numWorlds);
+    for (int i = 0; i < N; ++i)
+        if (w->isLarge[i]) large[w->worldId[i]].push_back(i);
+    auto overlap = [&](int a, int b) {
+        const float* A = &w->aabb[8 * (size_t)a];
+        const float* B = &w->aabb[8 * (size_t)b];
+        return A[0] <= B[4] && B[0] <= A[4] && A[1] <= B[5] && B[1] <= A[5] && A[2] <= B[6] && B[2] <= A[6];
+    };
+    w->pairs.clear();
+    w->pairOverflow = 0;
+    w->cellOverflow = 0;
+    const int cap = w->cfg.maxPairsPerBody - 1;  // curr_max
+    for (int i = 0; i < ns; ++i) {
+        const uint32_t self = w->vals[i];
+        const uint32_t world = w->keys[i] >> w->cellBits;
+        const float* a = &w->aabb[8 * (size_t)self];
+        const float cx = (a[0] + a[4]) * 0.5f, cy = (a[1] + a[5]) * 0.5f, cz = (a[2] + a[6]) * 0.5f;
+        const int gx = gcoord(cx, inv, dx), gy = gcoord(cy, inv, dy), gz = gcoord(cz, inv, dz);
+        int cnt = 0;
+        for (int oz = -1; oz <= 1; ++oz)
+            for (int oy = -1; oy <= 1; ++oy)
+                for (int ox = -1; ox <= 1; ++ox) {
+                    const int xx = (gx + ox) & (dx - 1), yy = (gy + oy) & (dy - 1), zz = (gz + oz) & (dz - 1);
+                    const uint32_t h = (world << w->cellBits) | (uint32_t)(zz * dy * dx + yy * dx + xx);
+                    const int start = find_start(h);
+                    if (start < 0) continue;
+                    const int end = std::min(start + w->cfg.maxBodiesPerCell, ns);
+                    int j = start;
+                    bool full = false;
+                    for (; j < end; ++j) {
+                        if (w->keys[j] != h) break;
+                        const uint32_t other = w->vals[j];
+                        if (other < self && overlap((int)self, (int)other)) {
+                            if (cnt >= cap) {
+                                w->pairOverflow++;
+                                full = true;
+                                break;
+                            }
+                            w->pairs.push_back((int)self);
+                            w->pairs.push_back((int)other);
+                            ++cnt;
+                        }
+                    }
+                    if (!full && j == end && end < ns && w->keys[end] == h) w->cellOverflow++;
+                }
+        for (int L : large[world]) {
+            if (overlap((int)self, L)) {
+                if (cnt >= cap) {
+                    w->pairOverflow++;
+                    break;
+                }
+                w->pairs.push_back((int)self);
+                w->pairs.push_back(L);
+                ++cnt;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Narrowphase (FP64)
+// ---------------------------------------------------------------------------
+struct Body {
+    V pos;
+    Q q;
+};
+
+inline V vtx(const or_world* w, int i) { return V(w->verts4[4 * i], w->verts4[4 * i + 1], w->verts4[4 * i + 2]); }
+
+// project (sat.cl:227-252)
+void project(const or_world* w, const or_poly& h, const Body& b, V dir, Real& mn, Real& mx) {
+    mn = DBL_MAX;
+    mx = -DBL_MAX;
+    const V ld = qinvrot(b.q, dir);
+    const Real off = dot(b.pos, dir);
+    for (int i = 0; i < h.numVertices; ++i) {
+        const Real dp = dot(vtx(w, h.vertexOffset + i), ld);
+        if (dp < mn) mn = dp;
+        if (dp > mx) mx = dp;
+    }
+    if (mn > mx) std::swap(mn, mx);
+    mn += off;
+    mx += off;
+}
+
+// findSeparatingAxis (sat.cl:497-551); returns false if a face axis separates
+bool face_axes(const or_world* w, const or_poly& hA, const or_poly& hB, const Body& A, const Body& B, V D,
+               V& sep, Real& dmin) {
+    for (int i = 0; i < hA.numFaces; ++i) {
+        const or_face& f = w->faces[hA.faceOffset + i];
+        V n = qrot(A.q, V(f.plane[0], f.plane[1], f.plane[2]));
+        if (dot(D, n) < 0) n = -n;
+        Real mn0, mx0, mn1, mx1;
+        project(w, hA, A, n, mn0, mx0);
+        project(w, hB, B, n, mn1, mx1);
+        if (mx0 < mn1 || mx1 < mn0) return false;
+        const Real d0 = mx0 - mn1, d1 = mx1 - mn0;
+        const Real d = d0 < d1 ? d0 : d1;
+        if (d < dmin) {
+            dmin = d;
+            sep = n;
+        }
+    }
+    if (dot(-D, sep) > 0) sep = -sep;
+    return true;
+}
+
+// findSeparatingAxisEdgeEdge (sat.cl:556-635): never rejects
+void edge_axes(const or_world* w, const or_poly& hA, const or_poly& hB, const Body& A, const Body& B, V D,
+               V& sep, Real& dmin) {
+    for (int e0 = 0; e0 < hA.numUniqueEdges; ++e0) {
+        const float* ea = &w->edges4[4 * (hA.uniqueEdgesOffset + e0)];
+        const V wa = qrot(A.q, V(ea[0], ea[1], ea[2]));
+        for (int e1 = 0; e1 < hB.numUniqueEdges; ++e1) {
+            const float* eb = &w->edges4[4 * (hB.uniqueEdgesOffset + e1)];
+            const V wb = qrot(B.q, V(eb[0], eb[1], eb[2]));
+            V c = cross(wa, wb);
+            if (!(std::fabs(c.x) > 1e-6 || std::fabs(c.y) > 1e-6 || std::fabs(c.z) > 1e-6)) continue;
+            c = normalize(c);
+            if (dot(D, c) < 0) c = -c;
+            Real mn0, mx0, mn1, mx1;
+            project(w, hA, A, c, mn0, mx0);
+            project(w, hB, B, c, mn1, mx1);
+            const Real d0 = mx0 - mn1, d1 = mx1 - mn0;
+            const Real d = d0 < d1 ? d0 : d1;
+            if (d < dmin) {
+                dmin = d;
+                sep = c;
+            }
+        }
+    }
+    if (dot(-D, sep) > 0) sep = -sep;
+}
+
+struct P4 {
+    Real x, y, z, w;
+};
+
+// clipFace (satClipHullContacts.cl:303-351)
+int clip_face(const std::vector<P4>& in, V pn, Real eq, std::vector<P4>& out) {
+    out.clear();
+    const int n = (int)in.size();
+    if (n == 0) return 0;
+    P4 first = in[n - 1];
+    Real ds = pn.x * first.x + pn.y * first.y + pn.z * first.z + eq;
+    for (int ve = 0; ve < n; ++ve) {
+        const P4 end = in[ve];
+        const Real de = pn.x * end.x + pn.y * end.y + pn.z * end.z + eq;
+        if (ds < 0) {
+            if (de < 0) {
+                out.push_back(end);
+            } else {
+                const Real t = ds * 1.0 / (ds - de);
+                out.push_back({first.x + (end.x - first.x) * t, first.y + (end.y - first.y) * t,
+                               first.z + (end.z - first.z) * t, 0});
+            }
+        } else if (de < 0) {
+            const Real t = ds * 1.0 / (ds - de);
+            out.push_back({first.x + (end.x - first.x) * t, first.y + (end.y - first.y) * t,
+                           first.z + (end.z - first.z) * t, 0});
+            out.push_back(end);
+        }
+        first = end;
+        ds = de;
+    }
+    if (out.size() > 64) out.resize(64);
+    return (int)out.size();
+}
+
+// clipHullAgainstHull (satClipHullContacts.cl:556-611 with clipFaceAgainstHull :353-452)
+int clip_hull_hull(const or_world* w, V sep, const or_poly& hA, const or_poly& hB, const Body& A, const Body& B,
+                   Real minDist, Real maxDist, std::vector<P4>& out) {
+    out.clear();
+    int closestB = -1;
+    Real dmax = -DBL_MAX;
+    for (int f = 0; f < hB.numFaces; ++f) {
+        const or_face& fc = w->faces[hB.faceOffset + f];
+        const V n = qrot(B.q, V(fc.plane[0], fc.plane[1], fc.plane[2]));
+        const Real d = dot(n, sep);
+        if (d > dmax) {
+            dmax = d;
+            closestB = f;
+        }
+    }
+    if (closestB < 0) return 0;
+    std::vector<P4> in, tmp;
+    {
+        const or_face& fb = w->faces[hB.faceOffset + closestB];
+        for (int e = 0; e < fb.numIndices; ++e) {
+            const V b = vtx(w, hB.vertexOffset + w->indices[fb.indexOffset + e]);
+            const V wv = qrot(B.q, b) + B.pos;
+            in.push_back({wv.x, wv.y, wv.z, 0});
+        }
+    }
+    int closestA = -1;
+    Real dmin = DBL_MAX;
+    for (int f = 0; f < hA.numFaces; ++f) {
+        const or_face& fc = w->faces[hA.faceOffset + f];
+        const V n = qrot(A.q, V(fc.plane[0], fc.plane[1], fc.plane[2]));
+        const Real d = dot(n, sep);
+        if (d < dmin) {
+            dmin = d;
+            closestA = f;
+        }
+    }
+    if (closestA < 0) return 0;
+    const or_face& fa = w->faces[hA.faceOffset + closestA];
+    const int nvA = fa.numIndices;
+    const V nA = V(fa.plane[0], fa.plane[1], fa.plane[2]);
+    const V nAw = qrot(A.q, nA);
+    for (int e0 = 0; e0 < nvA; ++e0) {
+        const V a = vtx(w, hA.vertexOffset + w->indices[fa.indexOffset + e0]);
+        const V b = vtx(w, hA.vertexOffset + w->indices[fa.indexOffset + (e0 + 1) % nvA]);
+        const V we = qrot(A.q, a - b);
+        const V pn = -cross(we, nAw);
+        const V wa = qrot(A.q, a) + A.pos;
+        const Real eq = -dot(wa, pn);
+        clip_face(in, pn, eq, tmp);
+        in.swap(tmp);
+    }
+    const Real eqA = (Real)fa.plane[3] - dot(nAw, A.pos);
+    for (const P4& p : in) {
+        Real depth = nAw.x * p.x + nAw.y * p.y + nAw.z * p.z + eqA;
+        if (depth <= minDist) depth = minDist;
+        if (depth <= maxDist) out.push_back({p.x, p.y, p.z, depth});
+    }
+    return (int)out.size();
+}
+
+// extractManifoldSequentialGlobal (satClipHullContacts.cl:678-770)
+int reduce_manifold(const std::vector<P4>& p, V nearNormal, int idx[4]) {
+    int n = (int)p.size();
+    idx[0] = 0; idx[1] = 1; idx[2] = 2; idx[3] = 3;
+    if (n == 0) return 0;
+    if (n <= 4) return n;
+    if (n > 64) n = 64;
+    P4 c = {0, 0, 0, 0};
+    for (int i = 0; i < n; ++i) {
+        c.x += p[i].x; c.y += p[i].y; c.z += p[i].z; c.w += p[i].w;
+    }
+    c.x /= n; c.y /= n; c.z /= n; c.w /= n;
+    const V cv(c.x, c.y, c.z);
+    const V aV = V(p[0].x, p[0].y, p[0].z) - cv;
+    V u = cross(nearNormal, aV);
+    V v = cross(nearNormal, u);
+    u = normalize(u);
+    v = normalize(v);
+    Real minW = DBL_MAX;
+    int minIndex = -1;
+    Real md[4] = {FLT_MIN, FLT_MIN, FLT_MIN, FLT_MIN};
+    for (int ie = 0; ie < n; ++ie) {
+        if (p[ie].w < minW) {
+            minW = p[ie].w;
+            minIndex = ie;
+        }
+        const V r = V(p[ie].x, p[ie].y, p[ie].z) - cv;
+        Real f = dot(u, r);
+        if (f < md[0]) { md[0] = f; idx[0] = ie; }
+        f = dot(-u, r);
+        if (f < md[1]) { md[1] = f; idx[1] = ie; }
+        f = dot(v, r);
+        if (f < md[2]) { md[2] = f; idx[2] = ie; }
+        f = dot(-v, r);
+        if (f < md[3]) { md[3] = f; idx[3] = ie; }
+    }
+    if (idx[0] != minIndex && idx[1] != minIndex && idx[2] != minIndex && idx[3] != minIndex) idx[0] = minIndex;
+    return 4;
+}
+
+Real combine_friction(Real a, Real b, int mode) { return mode == 1 ? a * b : std::sqrt(a * b); }
+
+bool contact_for_pair(const or_world* w, int pairIndex, int A, int B, or_contact& out) {
+    if (w->invMass[A] == 0.f && w->invMass[B] == 0.f) return false;  // sat.cl:944-948
+    const or_poly& hA = w->polys[w->colShape[w->col[A]]];
+    const or_poly& hB = w->polys[w->colShape[w->col[B]]];
+    Body a, b;
+    a.pos = V(w->pos[4 * A], w->pos[4 * A + 1], w->pos[4 * A + 2]);
+    a.q = Q{w->quat[4 * A], w->quat[4 * A + 1], w->quat[4 * A + 2], w->quat[4 * A + 3]};
+    b.pos = V(w->pos[4 * B], w->pos[4 * B + 1], w->pos[4 * B + 2]);
+    b.q = Q{w->quat[4 * B], w->quat[4 * B + 1], w->quat[4 * B + 2], w->quat[4 * B + 3]};
+    const V c0 = qrot(a.q, V(hA.localCenter[0], hA.localCenter[1], hA.localCenter[2])) + a.pos;
+    const V c1 = qrot(b.q, V(hB.localCenter[0], hB.localCenter[1], hB.localCenter[2])) + b.pos;
+    const V D = c0 - c1;
+    Real dmin = DBL_MAX;
+    V sep(0, 0, 0);
+    bool haveAxis = false;
+    {
+        // track whether any axis was accepted (dmin updated)
+        if (!face_axes(w, hA, hB, a, b, D, sep, dmin)) return false;
+        if (!face_axes(w, hB, hA, b, a, D, sep, dmin)) return false;
+        edge_axes(w, hA, hB, a, b, D, sep, dmin);
+        haveAxis = dmin < DBL_MAX;
+    }
+    if (!haveAxis) return false;
+    std::vector<P4> pts;
+    const int np = clip_hull_hull(w, sep, hA, hB, a, b, -1e30, (Real)w->cfg.contactBreaking, pts);
+    if (np <= 0) return false;
+    const V nrm = -sep;
+    int idx[4];
+    const int nr = reduce_manifold(pts, nrm, idx);
+    memset(&out, 0, sizeof(out));
+    for (int k = 0; k < nr; ++k) {
+        const P4& q = pts[idx[k]];
+        out.pos[k][0] = q.x; out.pos[k][1] = q.y; out.pos[k][2] = q.z; out.pos[k][3] = q.w;
+    }
+    out.normal[0] = nrm.x; out.normal[1] = nrm.y; out.normal[2] = nrm.z; out.normal[3] = nr;
+    out.friction = combine_friction(w->friction[A], w->friction[B], w->cfg.frictionCombine);
+    out.pairIndex = pairIndex;
+    out.bodyA = w->invMass[A] == 0.f ? -A : A;
+    out.bodyB = w->invMass[B] == 0.f ? -B : B;
+    return true;
+}
+
+void stage_narrowphase(or_world* w) {
+    w->contacts.clear();
+    const int np = (int)w->pairs.size() / 2;
+    for (int p = 0; p < np; ++p) {
+        or_contact c;
+        if (contact_for_pair(w, p, w->pairs[2 * p], w->pairs[2 * p + 1], c)) w->contacts.push_back(c);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Jacobi solver with velocity averaging (btPgsJacobiSolver, usePgs = false)
+// ---------------------------------------------------------------------------
+struct Row {
+    V n, t1, t2;  // contactNormal, relpos1CrossNormal, relpos2CrossNormal
+    Real rhs, jac, applied, lo, hi, mu;
+    int normalIndex;  // friction rows: index of their normal row
+};
+struct Copy {
+    int body;  // -1 for the shared static solver body
+    V dv, dw;
+};
+struct MRows {
+    int a, b;      // copy indices
+    int A, B;      // body ids
+    int nNormal;
+    std::vector<Row> normal, fric;
+};
+
+void plane_space(V n, V& p, V& q) {
+    const Real SQRT12 = 0.7071067811865475244008443621048490;
+    if (std::fabs(n.z) > SQRT12) {
+        const Real a = n.y * n.y + n.z * n.z;
+        const Real k = 1.0 / std::sqrt(a);
+        p = V(0, -n.z * k, n.y * k);
+        q = V(a * k, -n.x * p.z, n.x * p.y);
+    } else {
+        const Real a = n.x * n.x + n.y * n.y;
+        const Real k = 1.0 / std::sqrt(a);
+        p = V(-n.y * k, n.x * k, 0);
+        q = V(-n.z * p.y, n.z * p.x, a * k);
+    }
+}
+
+void solve_row(Row& c, Copy& A, Copy& B, Real imA, Real imB, V iiA, V iiB) {
+    Real delta = c.rhs;  // - applied * cfm (0)
+    const Real dv1 = dot(c.n, A.dv) + dot(c.t1, A.dw);
+    const Real dv2 = -dot(c.n, B.dv) + dot(c.t2, B.dw);
+    delta -= dv1 * c.jac;
+    delta -= dv2 * c.jac;
+    const Real sum = c.applied + delta;
+    if (sum < c.lo) {
+        delta = c.lo - c.applied;
+        c.applied = c.lo;
+    } else if (sum > c.hi) {
+        delta = c.hi - c.applied;
+        c.applied = c.hi;
+    } else {
+        c.applied = sum;
+    }
+    A.dv = A.dv + c.n * (imA * delta);
+    A.dw = A.dw + mulv(iiA, c.t1) * delta;
+    B.dv = B.dv + (-c.n * imB) * delta;
+    B.dw = B.dw + mulv(iiB, c.t2) * delta;
+}
+
+void stage_solve(or_world* w) {
+    const int N = w->n;
+    const int M = (int)w->contacts.size();
+    const Real dt = w->cfg.dt;
+    // m_bodyCount (:1105-1129)
+    w->count.assign(N, 0);
+    for (const or_contact& c : w->contacts) {
+        const int A = std::abs(c.bodyA), B = std::abs(c.bodyB);
+        if (w->invMass[A] != 0.f) w->count[A]++;
+        if (w->invMass[B] != 0.f) w->count[B]++;
+    }
+    std::vector<Copy> copies;
+    std::vector<int> staticCopy(N, -1);
+    auto get_copy = [&](int body) {
+        if (w->invMass[body] == 0.f) {
+            if (staticCopy[body] < 0) {
+                staticCopy[body] = (int)copies.size();
+                copies.push_back({-1, V(), V()});
+            }
+            return staticCopy[body];
+        }
+        copies.push_back({body, V(), V()});
+        return (int)copies.size() - 1;
+    };
+    std::vector<MRows> ms;
+    ms.reserve(M);
+    for (const or_contact& c : w->contacts) {
+        MRows m;
+        m.A = std::abs(c.bodyA);
+        m.B = std::abs(c.bodyB);
+        m.a = get_copy(m.A);
+        m.b = get_copy(m.B);
+        const bool dynA = w->invMass[m.A] != 0.f, dynB = w->invMass[m.B] != 0.f;
+        if (!dynA && !dynB) {
+            ms.push_back(m);
+            continue;
+        }
+        const Real imA = w->invMass[m.A], imB = w->invMass[m.B];
+        const V iiA = dynA ? V(w->invInertia[3 * m.A], w->invInertia[3 * m.A + 1], w->invInertia[3 * m.A + 2]) : V();
+        const V iiB = dynB ? V(w->invInertia[3 * m.B], w->invInertia[3 * m.B + 1], w->invInertia[3 * m.B + 2]) : V();
+        const Real kA = dynA ? (Real)w->count[m.A] : 1.0, kB = dynB ? (Real)w->count[m.B] : 1.0;
+        const V pA(w->pos[4 * m.A], w->pos[4 * m.A + 1], w->pos[4 * m.A + 2]);
+        const V pB(w->pos[4 * m.B], w->pos[4 * m.B + 1], w->pos[4 * m.B + 2]);
+        const V vA = dynA ? V(w->lin[4 * m.A], w->lin[4 * m.A + 1], w->lin[4 * m.A + 2]) : V();
+        const V wA = dynA ? V(w->ang[4 * m.A], w->ang[4 * m.A + 1], w->ang[4 * m.A + 2]) : V();
+        const V vB = dynB ? V(w->lin[4 * m.B], w->lin[4 * m.B + 1], w->lin[4 * m.B + 2]) : V();
+        const V wB = dynB ? V(w->ang[4 * m.B], w->ang[4 * m.B + 1], w->ang[4 * m.B + 2]) : V();
+        const Real restitution = (Real)w->restitution[m.A] * (Real)w->restitution[m.B];
+        const V n = normalize(V(-c.normal[0], -c.normal[1], -c.normal[2]));
+        const int npts = (int)c.normal[3];
+        for (int j = 0; j < npts; ++j) {
+            const Real dist = c.pos[j][3] + (Real)w->cfg.slopOffset;
+            if (!(dist <= (Real)w->cfg.contactProcessing)) continue;
+            const V posB(c.pos[j][0], c.pos[j][1], c.pos[j][2]);
+            const V posA = posB + n * dist;
+            const V r1 = posA - pA, r2 = posB - pB;
+            const V t0 = cross(r1, n), t1 = cross(r2, n);
+            const V angA = mulv(iiA, t0), angB = mulv(iiB, -t1);
+            const Real d0 = imA + dot(n, cross(angA, r1));
+            const Real d1 = imB + dot(n, cross(-angB, r2));
+            Row row;
+            row.n = n;
+            row.t1 = t0;
+            row.t2 = -t1;
+            row.jac = 1.0 / (d0 + d1);
+            const Real scaled = 1.0 / (d0 * kA + d1 * kB);
+            const Real penetration = dist;
+            const V vel = (vA + cross(wA, r1)) - (vB + cross(wB, r2));
+            const Real relv0 = dot(n, vel);
+            Real rest = restitution * -relv0;
+            if (rest <= 0) rest = 0;
+            const Real relv = (dot(n, vA) + dot(t0, wA)) + (-dot(n, vB) + dot(-t1, wB));
+            Real posErr = 0, velErr = rest - relv;
+            if (penetration > 0) velErr -= penetration / dt;
+            else posErr = -penetration * (Real)w->cfg.erp / dt;
+            row.rhs = posErr * scaled + velErr * scaled;
+            row.applied = 0;
+            row.lo = 0;
+            row.hi = 1e10;
+            row.mu = c.friction;
+            row.normalIndex = -1;
+            const int ni = (int)m.normal.size();
+            m.normal.push_back(row);
+            V d1v = vel - n * relv0, d2v;
+            const Real lat = dot(d1v, d1v);
+            if (lat > (Real)FLT_EPSILON) {
+                d1v = d1v * (1.0 / std::sqrt(lat));
+                d2v = normalize(cross(d1v, n));
+            } else {
+                plane_space(n, d1v, d2v);
+            }
+            const V dirs[2] = {d2v, d1v};
+            for (int q = 0; q < 2; ++q) {
+                const V dir = dirs[q];
+                Row f;
+                f.n = dir;
+                f.t1 = cross(r1, dir);
+                f.t2 = cross(r2, -dir);
+                const V aA = mulv(iiA, f.t1), aB = mulv(iiB, f.t2);
+                const Real e0 = imA + dot(dir, cross(aA, r1));
+                const Real e1 = imB + dot(dir, cross(-aB, r2));
+                f.jac = 1.0 / (e0 + e1);
+                const Real sc = 1.0 / (e0 * kA + e1 * kB);
+                const Real rv = (dot(dir, vA) + dot(f.t1, wA)) + (-dot(dir, vB) + dot(f.t2, wB));
+                f.rhs = (0 - rv) * sc;
+                f.applied = 0;
+                f.lo = 0;
+                f.hi = 1e10;
+                f.mu = c.friction;
+                f.normalIndex = ni;
+                m.fric.push_back(f);
+            }
+        }
+        ms.push_back(m);
+    }
+    // iterations
+    std::vector<V> sumL(N), sumA(N);
+    auto average = [&]() {
+        for (int i = 0; i < N; ++i) sumL[i] = sumA[i] = V();
+        for (const Copy& cp : copies)
+            if (cp.body >= 0) {
+                sumL[cp.body] = sumL[cp.body] + cp.dv;
+                sumA[cp.body] = sumA[cp.body] + cp.dw;
+            }
+        for (Copy& cp : copies)
+            if (cp.body >= 0) {
+                const Real f = 1.0 / (Real)w->count[cp.body];
+                cp.dv = sumL[cp.body] * f;
+                cp.dw = sumA[cp.body] * f;
+            }
+    };
+    for (int it = 0; it < w->cfg.iterations; ++it) {
+        for (MRows& m : ms) {
+            const Real imA = w->invMass[m.A], imB = w->invMass[m.B];
+            const bool dynA = imA != 0, dynB = imB != 0;
+            const V iiA = dynA ? V(w->invInertia[3 * m.A], w->invInertia[3 * m.A + 1], w->invInertia[3 * m.A + 2]) : V();
+            const V iiB = dynB ? V(w->invInertia[3 * m.B], w->invInertia[3 * m.B + 1], w->invInertia[3 * m.B + 2]) : V();
+            for (Row& r : m.normal) solve_row(r, copies[m.a], copies[m.b], imA, imB, iiA, iiB);
+        }
+        average();
+        for (MRows& m : ms) {
+            const Real imA = w->invMass[m.A], imB = w->invMass[m.B];
+            const bool dynA = imA != 0, dynB = imB != 0;
+            const V iiA = dynA ? V(w->invInertia[3 * m.A], w->invInertia[3 * m.A + 1], w->invInertia[3 * m.A + 2]) : V();
+            const V iiB = dynB ? V(w->invInertia[3 * m.B], w->invInertia[3 * m.B + 1], w->invInertia[3 * m.B + 2]) : V();
+            for (Row& r : m.fric) {
+                const Real total = m.normal[r.normalIndex].applied;
+                if (total > 0) {
+                    r.lo = -(r.mu * total);
+                    r.hi = r.mu * total;
+                    solve_row(r, copies[m.a], copies[m.b], imA, imB, iiA, iiB);
+                }
+            }
+        }
+        average();
+    }
+    // finish: per copy, body velocity += sum / count (:1790-1803)
+    w->avgLin.assign(3 * (size_t)N, 0);
+    w->avgAng.assign(3 * (size_t)N, 0);
+    for (int i = 0; i < N; ++i)
+        if (w->count[i] > 0) {
+            const Real f = 1.0 / (Real)w->count[i];
+            w->avgLin[3 * i] = sumL[i].x * f;
+            w->avgLin[3 * i + 1] = sumL[i].y * f;
+            w->avgLin[3 * i + 2] = sumL[i].z * f;
+            w->avgAng[3 * i] = sumA[i].x * f;
+            w->avgAng[3 * i + 1] = sumA[i].y * f;
+            w->avgAng[3 * i + 2] = sumA[i].z * f;
+        }
+    if (w->cfg.iterations == 0) {
+        w->avgLin.assign(3 * (size_t)N, 0);
+        w->avgAng.assign(3 * (size_t)N, 0);
+    }
+}
+
+// integrateTransformsKernel2 (integrateKernel.cl:102-158) after copyVelocities
+void stage_integrate(or_world* w) {
+    const Real dt = w->cfg.dt;
+    const Real thr = 0.25 * 3.14159254f;
+    for (int i = 0; i < w->n; ++i) {
+        if (w->invMass[i] == 0.f) continue;
+        Real* v = &w->lin[4 * i];
+        Real* a = &w->ang[4 * i];
+        if (!w->count.empty() && w->count[i] > 0) {
+            for (int c = 0; c < w->count[i]; ++c)
+                for (int k = 0; k < 3; ++k) {
+                    v[k] += w->avgLin[3 * i + k];
+                    a[k] += w->avgAng[3 * i + k];
+                }
+        }
+        for (int k = 0; k < 3; ++k) a[k] *= (Real)w->cfg.angularDamping;
+        Real fAngle = std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+        if (fAngle * dt > thr) fAngle = thr / dt;
+        Real s;
+        if (fAngle < 0.001) s = 0.5 * dt - (dt * dt * dt) * 0.020833333333 * fAngle * fAngle;
+        else s = std::sin(0.5 * fAngle * dt) / fAngle;
+        const Real dq[4] = {a[0] * s, a[1] * s, a[2] * s, std::cos(fAngle * dt * 0.5)};
+        Real* q = &w->quat[4 * i];
+        Real r[4];
+        r[0] = dq[3] * q[0] + dq[0] * q[3] + dq[1] * q[2] - dq[2] * q[1];
+        r[1] = dq[3] * q[1] + dq[1] * q[3] + dq[2] * q[0] - dq[0] * q[2];
+        r[2] = dq[3] * q[2] + dq[2] * q[3] + dq[0] * q[1] - dq[1] * q[0];
+        r[3] = dq[3] * q[3] - dq[0] * q[0] - dq[1] * q[1] - dq[2] * q[2];
+        const Real len = std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2] + r[3] * r[3]);
+        if (len > 0) for (int k = 0; k < 4; ++k) q[k] = r[k] / len;
+        else { q[0] = q[1] = q[2] = 0; q[3] = 1; }
+        for (int k = 0; k < 3; ++k) w->pos[4 * i + k] += v[k] * dt;
+    }
+}
+
+int ilog2(uint64_t v) {
+    int b = 0;
+    while ((1ull << b) < v) ++b;
+    return b;
+}
+
+}  // namespace
+
+extern "C" {
+
+or_world* or_world_create(const or_config* cfg, int n, const float* invMass, const float* friction,
+                          const float* restitution, const int* collidable, const int* worldId,
+                          const int* isLarge, const float* invInertia4, int numCols, const int* colShape,
+                          int numPolys, const or_poly* polys, int numVerts, const float* verts4, int numFaces,
+                          const or_face* faces, int numIndices, const int* indices, int numEdges,
+                          const float* edges4, const float* localAabb8) {
+    or_world* w = new or_world();
+    w->cfg = *cfg;
+    w->n = n;
+    w->cellBits = ilog2((uint64_t)cfg->dims[0] * cfg->dims[1] * cfg->dims[2]);
+    w->invMass.assign(invMass, invMass + n);
+    w->friction.assign(friction, friction + n);
+    w->restitution.assign(restitution, restitution + n);
+    w->col.assign(collidable, collidable + n);
+    w->worldId.assign(worldId, worldId + n);
+    w->isLarge.assign(isLarge, isLarge + n);
+    w->invInertia.resize(3 * (size_t)n);
+    for (int i = 0; i < n; ++i)
+        for (int k = 0; k < 3; ++k) w->invInertia[3 * i + k] = invInertia4[4 * i + k];
+    w->colShape.assign(colShape, colShape + numCols);
+    w->polys.assign(polys, polys + numPolys);
+    w->verts4.assign(verts4, verts4 + 4 * (size_t)numVerts);
+    w->faces.assign(faces, faces + numFaces);
+    w->indices.assign(indices, indices + numIndices);
+    w->edges4.assign(edges4, edges4 + 4 * (size_t)numEdges);
+    w->localAabb8.assign(localAabb8, localAabb8 + 8 * (size_t)numCols);
+    w->pos.assign(4 * (size_t)n, 0);
+    w->quat.assign(4 * (size_t)n, 0);
+    w->lin.assign(4 * (size_t)n, 0);
+    w->ang.assign(4 * (size_t)n, 0);
+    return w;
+}
+
+void or_world_destroy(or_world* w) { delete w; }
+
+void or_set_state_f32(or_world* w, const float* pos4, const float* quat4, const float* lin4, const float* ang4) {
+    for (size_t i = 0; i < 4 * (size_t)w->n; ++i) {
+        if (pos4) w->pos[i] = pos4[i];
+        if (quat4) w->quat[i] = quat4[i];
+        if (lin4) w->lin[i] = lin4[i];
+        if (ang4) w->ang[i] = ang4[i];
+    }
+}
+void or_set_state_f64(or_world* w, const double* pos4, const double* quat4, const double* lin4, const double* ang4) {
+    for (size_t i = 0; i < 4 * (size_t)w->n; ++i) {
+        if (pos4) w->pos[i] = pos4[i];
+        if (quat4) w->quat[i] = quat4[i];
+        if (lin4) w->lin[i] = lin4[i];
+        if (ang4) w->ang[i] = ang4[i];
+    }
+}
+void or_get_state(or_world* w, double* pos4, double* quat4, double* lin4, double* ang4) {
+    for (size_t i = 0; i < 4 * (size_t)w->n; ++i) {
+        if (pos4) pos4[i] = w->pos[i];
+        if (quat4) quat4[i] = w->quat[i];
+        if (lin4) lin4[i] = w->lin[i];
+        if (ang4) ang4[i] = w->ang[i];
+    }
+}
+
+void or_stage_aabbs(or_world* w) { stage_aabbs(w); }
+void or_stage_broadphase(or_world* w) { stage_broadphase(w); }
+void or_stage_narrowphase(or_world* w) { stage_narrowphase(w); }
+void or_stage_solve(or_world* w) { stage_solve(w); }
+void or_stage_integrate(or_world* w) { stage_integrate(w); }
+
+void or_step(or_world* w, int steps) {
+    for (int s = 0; s < steps; ++s) {
+        stage_aabbs(w);
+        stage_broadphase(w);
+        stage_narrowphase(w);
+        stage_solve(w);
+        stage_integrate(w);
+    }
+}
+
+int or_get_aabbs(or_world* w, float* out8) {
+    memcpy(out8, w->aabb.data(), sizeof(float) * w->aabb.size());
+    return (int)w->aabb.size() / 8;
+}
+int or_get_sorted(or_world* w, uint32_t* keys, uint32_t* vals, int max) {
+    const int n = std::min((int)w->keys.size(), max);
+    if (keys) memcpy(keys, w->keys.data(), 4 * (size_t)n);
+    if (vals) memcpy(vals, w->vals.data(), 4 * (size_t)n);
+    return (int)w->keys.size();
+}
+int or_get_pairs(or_world* w, int* pairs2, int max) {
+    const int n = std::min((int)w->pairs.size() / 2, max);
+    if (pairs2) memcpy(pairs2, w->pairs.data(), 8 * (size_t)n);
+    return (int)w->pairs.size() / 2;
+}
+int or_get_contacts(or_world* w, or_contact* out, int max) {
+    const int n = std::min((int)w->contacts.size(), max);
+    if (out) memcpy(out, w->contacts.data(), sizeof(or_contact) * (size_t)n);
+    return (int)w->contacts.size();
+}
+void or_get_overflow(or_world* w, long long* pairOverflow, long long* cellOverflow) {
+    *pairOverflow = w->pairOverflow;
+    *cellOverflow = w->cellOverflow;
+}
+// Inject contacts (e.g. from the device) before or_stage_solve.
+void or_set_contacts(or_world* w, const or_contact* c, int n) { w->contacts.assign(c, c + n); }
+// Inject pairs before or_stage_narrowphase.
+void or_set_pairs(or_world* w, const int* pairs2, int n) { w->pairs.assign(pairs2, pairs2 + 2 * (size_t)n); }
+
+// Single-pair narrowphase for known-answer tests: returns nPoints (0 = none).
+int or_pair_contact(or_world* w, int A, int B, or_contact* out) {
+    or_contact c;
+    if (!contact_for_pair(w, 0, A, B, c)) return 0;
+    *out = c;
+    return (int)c.normal[3];
+}
+
+// Clipping + reduction entry for the pin against the reference host port:
+// clip the given incident polygon against reference face fa of polyA posed
+// at (posA, qA); returns kept points (x, y, z, depth) and reduced indices.
+int or_clip_reduce(or_world* w, int polyA, int faceA, const double* posA, const double* qA,
+                   const double* polyIn4, int nIn, double maxDist, const double* nearNormal, double* out4,
+                   int* idx4) {
+    const or_poly& hA = w->polys[polyA];
+    Body A;
+    A.pos = V(posA[0], posA[1], posA[2]);
+    A.q = Q{qA[0], qA[1], qA[2], qA[3]};
+    const or_face& fa = w->faces[hA.faceOffset + faceA];
+    std::vector<P4> in, tmp;
+    for (int i = 0; i < nIn; ++i) in.push_back({polyIn4[4 * i], polyIn4[4 * i + 1], polyIn4[4 * i + 2], 0});
+    const int nvA = fa.numIndices;
+    const V nAw = qrot(A.q, V(fa.plane[0], fa.plane[1], fa.plane[2]));
+    for (int e0 = 0; e0 < nvA; ++e0) {
+        const V a = vtx(w, hA.vertexOffset + w->indices[fa.indexOffset + e0]);
+        const V b = vtx(w, hA.vertexOffset + w->indices[fa.indexOffset + (e0 + 1) % nvA]);
+        const V pn = -cross(qrot(A.q, a - b), nAw);
+        const Real eq = -dot(qrot(A.q, a) + A.pos, pn);
+        clip_face(in, pn, eq, tmp);
+        in.swap(tmp);
+    }
+    const Real eqA = (Real)fa.plane[3] - dot(nAw, A.pos);
+    std::vector<P4> pts;
+    for (const P4& p : in) {
+        Real depth = nAw.x * p.x + nAw.y * p.y + nAw.z * p.z + eqA;
+        if (depth <= -1e30) depth = -1e30;
+        if (depth <= maxDist) pts.push_back({p.x, p.y, p.z, depth});
+    }
+    for (size_t i = 0; i < pts.size(); ++i) {
+        out4[4 * i] = pts[i].x; out4[4 * i + 1] = pts[i].y; out4[4 * i + 2] = pts[i].z; out4[4 * i + 3] = pts[i].w;
+    }
+    reduce_manifold(pts, V(nearNormal[0], nearNormal[1], nearNormal[2]), idx4);
+    return (int)pts.size();
+}
+
+// Solver-only entry for the pin against the reference's btPgsJacobiSolver:
+// solve the given manifolds with the given velocities and return the
+// post-solve velocities (bodies' linVel/angVel after the finish step).
+void or_solve_velocities(or_world* w, double* lin4, double* ang4) {
+    stage_solve(w);
+    for (int i = 0; i < w->n; ++i) {
+        if (w->invMass[i] == 0.f || w->count[i] == 0) continue;
+        for (int c = 0; c < w->count[i]; ++c)
+            for (int k = 0; k < 3; ++k) {
+                w->lin[4 * i + k] += w->avgLin[3 * i + k];
+                w->ang[4 * i + k] += w->avgAng[3 * i + k];
+            }
+    }
+    for (size_t i = 0; i < 4 * (size_t)w->n; ++i) {
+        lin4[i] = w->lin[i];
+        ang4[i] = w->ang[i];
+    }
+}
+
+}  // extern "C"

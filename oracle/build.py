@@ -1,0 +1,85 @@
+"""Build the oracle (test infrastructure only).
+
+  oracle/liboracle.so      the single-threaded C++ restatement (b3_oracle.cpp)
+  oracle/_ref/libb3ref.so  pieces of the reference compiled from its own
+                           sources under /root/reference plus the thin shim in
+                           oracle/ref_shim.cpp (built only where that tree
+                           exists; the built file travels with the repository
+                           snapshot, the sources do not)
+
+Usage: python -m oracle.build [--force]
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libb3ref.so")
+REFERENCE = "/root/reference"
+
+# Reference sources compiled for the pins (paths relative to the reference root).
+REF_SOURCES = [
+    "opencl/gpu_rigidbody_pipeline2/btPgsJacobiSolver.cpp",
+    "opencl/gpu_rigidbody_pipeline2/satClipHullContacts.cpp",
+    "opencl/gpu_rigidbody_pipeline/btConvexUtility.cpp",
+    "bullet2/LinearMath/btConvexHullComputer.cpp",
+    "bullet2/LinearMath/btAlignedAllocator.cpp",
+    "bullet2/LinearMath/btGeometryUtil.cpp",
+    "bullet2/LinearMath/btQuickprof.cpp",
+]
+
+
+def _stale(out, srcs):
+    if not os.path.exists(out):
+        return True
+    t = os.path.getmtime(out)
+    return any(os.path.getmtime(s) > t for s in srcs if os.path.exists(s))
+
+
+def build_oracle(force=False):
+    src = os.path.join(HERE, "b3_oracle.cpp")
+    if force or _stale(LIB, [src]):
+        cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off", "-fno-fast-math",
+               src, "-o", LIB]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("oracle build failed:\n" + r.stderr)
+    return LIB
+
+
+def build_ref(force=False):
+    """Compile the reference pieces in place (no copies into this repo)."""
+    if not os.path.isdir(REFERENCE):
+        return REF_LIB if os.path.exists(REF_LIB) else None
+    shims = [os.path.join(HERE, f) for f in ("ref_shim_jacobi.cpp", "ref_shim_hull.cpp", "ref_shim_clip.cpp")]
+    srcs = [os.path.join(REFERENCE, s) for s in REF_SOURCES] + shims
+    if not force and not _stale(REF_LIB, srcs):
+        return REF_LIB
+    os.makedirs(os.path.dirname(REF_LIB), exist_ok=True)
+    objdir = os.path.join(HERE, "_ref", "obj")
+    os.makedirs(objdir, exist_ok=True)
+    inc = ["-I", os.path.join(REFERENCE, "bullet2"),
+           "-I", os.path.join(REFERENCE, "opencl/gpu_rigidbody_pipeline2"),
+           "-I", os.path.join(REFERENCE, "opencl/gpu_rigidbody_pipeline"),
+           "-I", os.path.join(REFERENCE, "dynamics/basic_demo/Stubs"),
+           "-I", os.path.join(REFERENCE, "opencl")]
+    flags = ["-O2", "-fPIC", "-w", "-include", "cstdio", "-include", "cstring", "-include", "cstdlib",
+             "-DDISABLE_JOINTS"]
+    objs = []
+    for s in srcs:
+        o = os.path.join(objdir, os.path.basename(s) + ".o")
+        cmd = ["g++"] + flags + inc + ["-c", s, "-o", o]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("reference build failed: " + " ".join(cmd) + "\n" + r.stderr[-4000:])
+        objs.append(o)
+    r = subprocess.run(["g++", "-shared", "-o", REF_LIB] + objs, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("reference link failed:\n" + r.stderr[-4000:])
+    return REF_LIB
+
+
+if __name__ == "__main__":
+    print(build_oracle(force="--force" in sys.argv))
+    print(build_ref(force="--force" in sys.argv))
