@@ -272,7 +272,7 @@ def random_pile(seed, n=64, worlds=1, box=4.0, hull_frac=0.5, pool=8, velocity=0
     dyn = _bodies(sid, mass, pos, q, fr, wid, lin=lin, ang=ang)
     b = _concat([grounds, dyn])
     return Scene(name=f"pile_{n}x{worlds}", shapes=shapes, num_worlds=worlds,
-                 config=dict(cellSize=1.0, gridDims=(16, 16, 16)), steps=1, **b)
+                 config=dict(cellSize=1.0, gridDims=(16, 16, 16), maxPairs=max(4096, 40 * total)), steps=1, **b)
 
 
 SCENES = {"c1": c1, "c2": c2, "c3": c3, "c4": c4, "c5": c5}
@@ -285,7 +285,7 @@ def world_config(scene, **over):
     kw = dict(maxBodies=n, numWorlds=scene.num_worlds, maxPairsPerBody=32, maxBodiesPerCell=64,
               maxSmallProxySize=4.0 * scene.config.get("cellSize", 1.0), solverIterations=10,
               dt=1.0 / 60.0)
-    kw["maxPairs"] = max(1024, 10 * n)
+    kw["maxPairs"] = max(4096, 16 * n)
     kw.update(scene.config)
     kw.update(over)
     return b3.default_config(**kw)

@@ -13,6 +13,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
+LIB_F32 = os.path.join(HERE, "liboracle_f32.so")
 REF_LIB = os.path.join(HERE, "_ref", "libb3ref.so")
 
 
@@ -21,7 +22,7 @@ class OrConfig(C.Structure):
                 ("maxPairsPerBody", C.c_int), ("gravity", C.c_float * 3), ("dt", C.c_float),
                 ("iterations", C.c_int), ("erp", C.c_float), ("contactBreaking", C.c_float),
                 ("contactProcessing", C.c_float), ("slopOffset", C.c_float), ("angularDamping", C.c_float),
-                ("frictionCombine", C.c_int), ("numWorlds", C.c_int)]
+                ("frictionCombine", C.c_int), ("numWorlds", C.c_int), ("maxPairs", C.c_int)]
 
 
 class OrContact(C.Structure):
@@ -30,6 +31,7 @@ class OrContact(C.Structure):
 
 
 _lib = None
+_lib32 = None
 _ref = None
 _D = C.POINTER(C.c_double)
 _F = C.POINTER(C.c_float)
@@ -38,13 +40,16 @@ _U = C.POINTER(C.c_uint32)
 _VP = C.c_void_p
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(LIB):
+def lib(f32=False):
+    """The FP64 oracle, or with f32=True the same restatement in FP32 (used
+    to tell precision effects from logic differences)."""
+    global _lib, _lib32
+    if (_lib32 if f32 else _lib) is None:
+        path = LIB_F32 if f32 else LIB
+        if not os.path.exists(path):
             from . import build
             build.build_oracle()
-        L = C.CDLL(LIB)
+        L = C.CDLL(path)
         L.or_world_create.restype = _VP
         L.or_world_create.argtypes = [C.POINTER(OrConfig), C.c_int, _F, _F, _F, _I, _I, _I, _F, C.c_int, _I,
                                       C.c_int, _VP, C.c_int, _F, C.c_int, _VP, C.c_int, _I, C.c_int, _F, _F]
@@ -65,8 +70,11 @@ def lib():
         L.or_pair_contact.argtypes = [_VP, C.c_int, C.c_int, C.POINTER(OrContact)]
         L.or_clip_reduce.argtypes = [_VP, C.c_int, C.c_int, _D, _D, _D, C.c_int, C.c_double, _D, _D, _I]
         L.or_solve_velocities.argtypes = [_VP, _D, _D]
-        _lib = L
-    return _lib
+        if f32:
+            _lib32 = L
+        else:
+            _lib = L
+    return _lib32 if f32 else _lib
 
 
 def ref_lib():
@@ -98,8 +106,8 @@ class OracleWorld:
     """Oracle world built from a registered product world's shape tables
     (hull construction is checked separately against btConvexUtility)."""
 
-    def __init__(self, scene, shapes, cfg, inv_inertia, is_large):
-        L = lib()
+    def __init__(self, scene, shapes, cfg, inv_inertia, is_large, f32=False):
+        L = lib(f32)
         self.n = scene.n
         c = OrConfig()
         c.cellSize = cfg.cellSize
@@ -117,6 +125,7 @@ class OracleWorld:
         c.angularDamping = cfg.angularDamping
         c.frictionCombine = cfg.frictionCombine
         c.numWorlds = cfg.numWorlds
+        c.maxPairs = cfg.maxPairs
         self.cfg = c
         n = scene.n
         m = np.asarray(scene.mass, np.float64)
@@ -240,7 +249,7 @@ class OracleWorld:
             pass
 
 
-def oracle_from_world(world, scene, cfg=None):
+def oracle_from_world(world, scene, cfg=None, f32=False):
     """Build an OracleWorld from a registered PhysicsWorld (host-only
     context suffices) and its scene."""
     cfg = cfg or world.cfg
@@ -252,7 +261,7 @@ def oracle_from_world(world, scene, cfg=None):
     inv_inertia = world.inertias()
     # large-body classification rule (half-diagonal of the registration AABB)
     is_large = large_flags(world, scene, cfg)
-    return OracleWorld(scene, sh, cfg, inv_inertia, is_large)
+    return OracleWorld(scene, sh, cfg, inv_inertia, is_large, f32=f32)
 
 
 def large_flags(world, scene, cfg):

@@ -33,9 +33,13 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <limits>
 #include <vector>
 
-typedef double Real;
+#ifndef ORACLE_REAL
+#define ORACLE_REAL double
+#endif
+typedef ORACLE_REAL Real;
 
 namespace {
 
@@ -112,6 +116,7 @@ struct or_config {
     float angularDamping;
     int frictionCombine;  // 0 = sqrt(a*b), 1 = a*b
     int numWorlds;
+    int maxPairs;         // global pair capacity (0 = unlimited)
 };
 
 struct or_world {
@@ -297,6 +302,11 @@ void stage_broadphase(or_world* w) {
             }
         }
     }
+    // global capacity: the device keeps the first maxPairs pairs in order
+    if (w->cfg.maxPairs > 0 && (long long)w->pairs.size() / 2 > w->cfg.maxPairs) {
+        w->pairOverflow += (long long)w->pairs.size() / 2 - w->cfg.maxPairs;
+        w->pairs.resize(2 * (size_t)w->cfg.maxPairs);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -311,8 +321,8 @@ inline V vtx(const or_world* w, int i) { return V(w->verts4[4 * i], w->verts4[4 
 
 // project (sat.cl:227-252)
 void project(const or_world* w, const or_poly& h, const Body& b, V dir, Real& mn, Real& mx) {
-    mn = DBL_MAX;
-    mx = -DBL_MAX;
+    mn = std::numeric_limits<Real>::max();
+    mx = -std::numeric_limits<Real>::max();
     const V ld = qinvrot(b.q, dir);
     const Real off = dot(b.pos, dir);
     for (int i = 0; i < h.numVertices; ++i) {
@@ -409,12 +419,45 @@ int clip_face(const std::vector<P4>& in, V pn, Real eq, std::vector<P4>& out) {
     return (int)out.size();
 }
 
+#ifdef ORACLE_LOCAL_FRAME
+// clipFace with the plane given by a normal and a point on it
+int clip_face_pt(const std::vector<P4>& in, V pn, V a, std::vector<P4>& out) {
+    out.clear();
+    const int n = (int)in.size();
+    if (n == 0) return 0;
+    P4 first = in[n - 1];
+    Real ds = pn.x * (first.x - a.x) + pn.y * (first.y - a.y) + pn.z * (first.z - a.z);
+    for (int ve = 0; ve < n; ++ve) {
+        const P4 end = in[ve];
+        const Real de = pn.x * (end.x - a.x) + pn.y * (end.y - a.y) + pn.z * (end.z - a.z);
+        if (ds < 0) {
+            if (de < 0) {
+                out.push_back(end);
+            } else {
+                const Real t = ds * 1.0 / (ds - de);
+                out.push_back({first.x + (end.x - first.x) * t, first.y + (end.y - first.y) * t,
+                               first.z + (end.z - first.z) * t, 0});
+            }
+        } else if (de < 0) {
+            const Real t = ds * 1.0 / (ds - de);
+            out.push_back({first.x + (end.x - first.x) * t, first.y + (end.y - first.y) * t,
+                           first.z + (end.z - first.z) * t, 0});
+            out.push_back(end);
+        }
+        first = end;
+        ds = de;
+    }
+    if (out.size() > 64) out.resize(64);
+    return (int)out.size();
+}
+#endif
+
 // clipHullAgainstHull (satClipHullContacts.cl:556-611 with clipFaceAgainstHull :353-452)
 int clip_hull_hull(const or_world* w, V sep, const or_poly& hA, const or_poly& hB, const Body& A, const Body& B,
                    Real minDist, Real maxDist, std::vector<P4>& out) {
     out.clear();
     int closestB = -1;
-    Real dmax = -DBL_MAX;
+    Real dmax = -std::numeric_limits<Real>::max();
     for (int f = 0; f < hB.numFaces; ++f) {
         const or_face& fc = w->faces[hB.faceOffset + f];
         const V n = qrot(B.q, V(fc.plane[0], fc.plane[1], fc.plane[2]));
@@ -426,16 +469,23 @@ int clip_hull_hull(const or_world* w, V sep, const or_poly& hA, const or_poly& h
     }
     if (closestB < 0) return 0;
     std::vector<P4> in, tmp;
+#ifdef ORACLE_LOCAL_FRAME
+    // Same arithmetic in a frame centred on body A (numerics experiment for
+    // the FP32 build only): clip planes as (normal, point), no plane constant.
+    const V orgA = A.pos;
+#else
+    const V orgA(0, 0, 0);
+#endif
     {
         const or_face& fb = w->faces[hB.faceOffset + closestB];
         for (int e = 0; e < fb.numIndices; ++e) {
             const V b = vtx(w, hB.vertexOffset + w->indices[fb.indexOffset + e]);
-            const V wv = qrot(B.q, b) + B.pos;
+            const V wv = qrot(B.q, b) + (B.pos - orgA);
             in.push_back({wv.x, wv.y, wv.z, 0});
         }
     }
     int closestA = -1;
-    Real dmin = DBL_MAX;
+    Real dmin = std::numeric_limits<Real>::max();
     for (int f = 0; f < hA.numFaces; ++f) {
         const or_face& fc = w->faces[hA.faceOffset + f];
         const V n = qrot(A.q, V(fc.plane[0], fc.plane[1], fc.plane[2]));
@@ -455,16 +505,25 @@ int clip_hull_hull(const or_world* w, V sep, const or_poly& hA, const or_poly& h
         const V b = vtx(w, hA.vertexOffset + w->indices[fa.indexOffset + (e0 + 1) % nvA]);
         const V we = qrot(A.q, a - b);
         const V pn = -cross(we, nAw);
+#ifdef ORACLE_LOCAL_FRAME
+        const V wa = qrot(A.q, a);
+        clip_face_pt(in, pn, wa, tmp);
+#else
         const V wa = qrot(A.q, a) + A.pos;
         const Real eq = -dot(wa, pn);
         clip_face(in, pn, eq, tmp);
+#endif
         in.swap(tmp);
     }
+#ifdef ORACLE_LOCAL_FRAME
+    const Real eqA = (Real)fa.plane[3];
+#else
     const Real eqA = (Real)fa.plane[3] - dot(nAw, A.pos);
+#endif
     for (const P4& p : in) {
         Real depth = nAw.x * p.x + nAw.y * p.y + nAw.z * p.z + eqA;
         if (depth <= minDist) depth = minDist;
-        if (depth <= maxDist) out.push_back({p.x, p.y, p.z, depth});
+        if (depth <= maxDist) out.push_back({p.x + orgA.x, p.y + orgA.y, p.z + orgA.z, depth});
     }
     return (int)out.size();
 }
@@ -487,7 +546,7 @@ int reduce_manifold(const std::vector<P4>& p, V nearNormal, int idx[4]) {
     V v = cross(nearNormal, u);
     u = normalize(u);
     v = normalize(v);
-    Real minW = DBL_MAX;
+    Real minW = std::numeric_limits<Real>::max();
     int minIndex = -1;
     Real md[4] = {FLT_MIN, FLT_MIN, FLT_MIN, FLT_MIN};
     for (int ie = 0; ie < n; ++ie) {
@@ -523,7 +582,7 @@ bool contact_for_pair(const or_world* w, int pairIndex, int A, int B, or_contact
     const V c0 = qrot(a.q, V(hA.localCenter[0], hA.localCenter[1], hA.localCenter[2])) + a.pos;
     const V c1 = qrot(b.q, V(hB.localCenter[0], hB.localCenter[1], hB.localCenter[2])) + b.pos;
     const V D = c0 - c1;
-    Real dmin = DBL_MAX;
+    Real dmin = std::numeric_limits<Real>::max();
     V sep(0, 0, 0);
     bool haveAxis = false;
     {
@@ -531,7 +590,7 @@ bool contact_for_pair(const or_world* w, int pairIndex, int A, int B, or_contact
         if (!face_axes(w, hA, hB, a, b, D, sep, dmin)) return false;
         if (!face_axes(w, hB, hA, b, a, D, sep, dmin)) return false;
         edge_axes(w, hA, hB, a, b, D, sep, dmin);
-        haveAxis = dmin < DBL_MAX;
+        haveAxis = dmin < std::numeric_limits<Real>::max();
     }
     if (!haveAxis) return false;
     std::vector<P4> pts;

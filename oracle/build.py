@@ -15,6 +15,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
+LIB_F32 = os.path.join(HERE, "liboracle_f32.so")
 REF_LIB = os.path.join(HERE, "_ref", "libb3ref.so")
 REFERENCE = "/root/reference"
 
@@ -39,12 +40,13 @@ def _stale(out, srcs):
 
 def build_oracle(force=False):
     src = os.path.join(HERE, "b3_oracle.cpp")
-    if force or _stale(LIB, [src]):
-        cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off", "-fno-fast-math",
-               src, "-o", LIB]
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if r.returncode != 0:
-            raise RuntimeError("oracle build failed:\n" + r.stderr)
+    for out, extra in ((LIB, []), (LIB_F32, ["-DORACLE_REAL=float"])):
+        if force or _stale(out, [src]):
+            cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off", "-fno-fast-math"] + \
+                extra + [src, "-o", out]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError("oracle build failed:\n" + r.stderr)
     return LIB
 
 
