@@ -159,6 +159,20 @@ int b3_fill_int2(b3Context ctx, int32_t* d_dst_int2, int32_t x, int32_t y, int64
 int b3_prefix_scan_u32(b3Context ctx, const uint32_t* d_src, uint32_t* d_dst, int64_t n,
                        uint32_t* d_sum, uint32_t* h_sum, void* stream);
 
+/* Exclusive scan that allocates nothing. It has no counterpart in the
+ * reference. For callers that cannot call cudaMalloc (an engine that owns
+ * all GPU memory through its own pool, a real-time loop that must never
+ * allocate, a plug-in whose allocator belongs to another runtime): same
+ * result as b3_prefix_scan_u32, but the scratch is a fixed 33 KB device
+ * array inside the library, so no context is needed either.
+ * Limit: n <= 16,777,216 (larger n returns B3_ERR_CAPACITY). All calls on
+ * a device share that array: calls that overlap on the GPU race, so keep
+ * them on one stream. The first call on a device looks up the array's
+ * address; make it before any stream capture. The total goes to d_sum
+ * (device, may be NULL). */
+int b3_prefix_scan_u32_static(const uint32_t* d_src, uint32_t* d_dst, int64_t n, uint32_t* d_sum,
+                              void* stream);
+
 /* btRadixSort32CL::execute (BB/btRadixSort32CL.cpp:161-535): stable LSD
  * key-value sort of n (key, value) pairs, in place. Only the low key_bits
  * bits of the keys are sorted (1..32); keys must not use higher bits unless
