@@ -32,6 +32,7 @@
 // order and every run is deterministic.
 #include "b3_math.cuh"
 #include "b3_world.h"
+#include "b3_ff.cuh"
 
 #include <cfloat>
 
@@ -39,8 +40,13 @@ using namespace b3m;
 
 namespace {
 
+using namespace b3ff;
+
 constexpr int kMaxPoly = 64;  // capacityWorldVerts (satClipHullContacts.cl:1027)
 constexpr int kChunk = 4;     // pairs per work grab
+constexpr int kKeep = 4;      // near-minimum axis candidates kept per lane
+constexpr int kMaxCand = 32;  // candidates refined in float-float per pair
+constexpr int kNone = 0x7fffffff;
 
 struct NpParams {
     float minDist;
@@ -49,28 +55,23 @@ struct NpParams {
     int maxPairs;
 };
 
-struct __align__(16) WarpScratch {
-    float4 poly[2][kMaxPoly];
+// Per-warp shared scratch: two float-float polygons (x, y, z, depth).
+struct __align__(16) FfVert {
+    float xh, xl, yh, yl, zh, zl, wh, wl;
 };
+struct __align__(16) WarpScratch {
+    FfVert poly[2][kMaxPoly];
+    int cand[kMaxCand];
+};
+
+__device__ __forceinline__ ff3 vget(const FfVert& v) { return {{v.xh, v.xl}, {v.yh, v.yl}, {v.zh, v.zl}}; }
+__device__ __forceinline__ ff wget(const FfVert& v) { return {v.wh, v.wl}; }
+__device__ __forceinline__ FfVert vput(ff3 p, ff w) {
+    return {p.x.hi, p.x.lo, p.y.hi, p.y.lo, p.z.hi, p.z.lo, w.hi, w.lo};
+}
 
 __device__ __forceinline__ float combine_friction(float a, float b, int mode) {
     return mode == B3_FRICTION_PRODUCT ? a * b : sqrtf(a * b);
-}
-
-// project hull (local verts) onto world axis dir
-__device__ __forceinline__ void project(const float4* __restrict__ verts, int off, int nv,
-                                        const Mat3& R, float3 pos, float3 dir, float& mn, float& mx) {
-    const float3 ld = mul_t(R, dir);
-    const float offs = dot(pos, dir);
-    float lo = FLT_MAX, hi = -FLT_MAX;
-    for (int i = 0; i < nv; ++i) {
-        const float4 v = __ldg(&verts[off + i]);
-        const float dp = v.x * ld.x + v.y * ld.y + v.z * ld.z;
-        lo = fminf(lo, dp);
-        hi = fmaxf(hi, dp);
-    }
-    mn = lo + offs;
-    mx = hi + offs;
 }
 
 // lexicographic (value, index) minimum across the warp
@@ -85,132 +86,305 @@ __device__ __forceinline__ void warp_argmin(float& v, int& idx) {
         }
     }
 }
+__device__ __forceinline__ void warp_argmin_ff(ff& v, int& idx) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        ff ov;
+        ov.hi = __shfl_xor_sync(0xffffffffu, v.hi, o);
+        ov.lo = __shfl_xor_sync(0xffffffffu, v.lo, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
+        if (lt(ov, v) || (eq(ov, v) && (unsigned)oi < (unsigned)idx)) {
+            v = ov;
+            idx = oi;
+        }
+    }
+}
 
 struct PairCtx {
     int A, B;
     float invMassA, invMassB;
     const b3ConvexPolyhedron* pa;
     const b3ConvexPolyhedron* pb;
+    float4 qA, qB;
     Mat3 RA, RB;
+    ffmat FA, FB;  // float-float rotation matrices
     float3 posA, posB;
 };
 
-// Find the minimum-penetration axis. Returns false if separated / no axis.
-__device__ bool find_axis(const PairCtx& c, const b3::ShapesDev& S, float3& sep) {
-    const int lane = threadIdx.x & 31;
+// FP32 projection of a hull onto world axis dir, relative to the hull's own
+// position (the caller adds the position offset)
+__device__ __forceinline__ void project_rel(const float4* __restrict__ verts, int off, int nv, const Mat3& R,
+                                            float3 dir, float& mn, float& mx) {
+    const float3 ld = mul_t(R, dir);
+    float lo = FLT_MAX, hi = -FLT_MAX;
+    for (int i = 0; i < nv; ++i) {
+        const float4 v = __ldg(&verts[off + i]);
+        const float dp = v.x * ld.x + v.y * ld.y + v.z * ld.z;
+        lo = fminf(lo, dp);
+        hi = fmaxf(hi, dp);
+    }
+    mn = lo;
+    mx = hi;
+}
+
+// Axis index space (sequential order of the reference): faces of A
+// [0, FA), faces of B [FA, FA+FB), edge pairs e0*EB+e1 after that.
+__device__ __forceinline__ bool axis_f32(const PairCtx& c, const b3::ShapesDev& S, int idx, float3 D,
+                                         float3 rel, float delta, float3& n, float& d, float& err, bool& isFace) {
     const b3ConvexPolyhedron& pa = *c.pa;
     const b3ConvexPolyhedron& pb = *c.pb;
-    const float4 lcA = make_float4(pa.localCenter[0], pa.localCenter[1], pa.localCenter[2], 0.f);
-    const float4 lcB = make_float4(pb.localCenter[0], pb.localCenter[1], pb.localCenter[2], 0.f);
-    const float3 c0 = mul(c.RA, f3(lcA)) + c.posA;
-    const float3 c1 = mul(c.RB, f3(lcB)) + c.posB;
-    const float3 D = c0 - c1;
-    float best = FLT_MAX;
-    int bestIdx = 0x7fffffff;
-    float3 bestAxis = make_float3(0.f, 0.f, 0.f);
-    bool separated = false;
-    // faces of A
-    for (int f = lane; f < pa.numFaces; f += 32) {
-        const float4 pl = __ldg((const float4*)&S.faces[pa.faceOffset + f].plane[0]);
-        float3 n = mul(c.RA, make_float3(pl.x, pl.y, pl.z));
-        if (dot(D, n) < 0.f) n = -n;
-        float mn0, mx0, mn1, mx1;
-        project(S.verts, pa.vertexOffset, pa.numVertices, c.RA, c.posA, n, mn0, mx0);
-        project(S.verts, pb.vertexOffset, pb.numVertices, c.RB, c.posB, n, mn1, mx1);
-        if (mx0 < mn1 || mx1 < mn0) separated = true;
-        const float d = fminf(mx0 - mn1, mx1 - mn0);
-        if (d < best) {
-            best = d;
-            bestIdx = f;
-            bestAxis = n;
-        }
-    }
-    if (__any_sync(0xffffffffu, separated)) return false;
-    // faces of B (findSeparatingAxis(hullB, hullA, ...), same DeltaC2)
-    for (int f = lane; f < pb.numFaces; f += 32) {
-        const float4 pl = __ldg((const float4*)&S.faces[pb.faceOffset + f].plane[0]);
-        float3 n = mul(c.RB, make_float3(pl.x, pl.y, pl.z));
-        if (dot(D, n) < 0.f) n = -n;
-        float mn0, mx0, mn1, mx1;
-        project(S.verts, pb.vertexOffset, pb.numVertices, c.RB, c.posB, n, mn0, mx0);
-        project(S.verts, pa.vertexOffset, pa.numVertices, c.RA, c.posA, n, mn1, mx1);
-        if (mx0 < mn1 || mx1 < mn0) separated = true;
-        const float d = fminf(mx0 - mn1, mx1 - mn0);
-        if (d < best) {
-            best = d;
-            bestIdx = pa.numFaces + f;
-            bestAxis = n;
-        }
-    }
-    if (__any_sync(0xffffffffu, separated)) return false;
-    // edge x edge
-    const int EA = pa.numUniqueEdges, EB = pb.numUniqueEdges;
-    const int base = pa.numFaces + pb.numFaces;
-    for (int e = lane; e < EA * EB; e += 32) {
+    const int FA = pa.numFaces, FB = pb.numFaces;
+    if (idx < FA + FB) {
+        isFace = true;
+        const bool onA = idx < FA;
+        const float4 pl = __ldg((const float4*)&S.faces[onA ? pa.faceOffset + idx : pb.faceOffset + idx - FA].plane[0]);
+        n = mul(onA ? c.RA : c.RB, make_float3(pl.x, pl.y, pl.z));
+        err = delta;
+    } else {
+        isFace = false;
+        const int e = idx - FA - FB;
+        const int EB = pb.numUniqueEdges;
         const int e0 = e / EB, e1 = e - e0 * EB;
-        const float4 ea = __ldg(&S.edges[pa.uniqueEdgesOffset + e0]);
-        const float4 eb = __ldg(&S.edges[pb.uniqueEdgesOffset + e1]);
-        const float3 wa = mul(c.RA, f3(ea));
-        const float3 wb = mul(c.RB, f3(eb));
+        const float3 wa = mul(c.RA, f3(__ldg(&S.edges[pa.uniqueEdgesOffset + e0])));
+        const float3 wb = mul(c.RB, f3(__ldg(&S.edges[pb.uniqueEdgesOffset + e1])));
         float3 cr = cross(wa, wb);
-        if (fabsf(cr.x) > 1e-6f || fabsf(cr.y) > 1e-6f || fabsf(cr.z) > 1e-6f) {
-            cr = normalize(cr);
-            if (dot(D, cr) < 0.f) cr = -cr;
-            float mn0, mx0, mn1, mx1;
-            project(S.verts, pa.vertexOffset, pa.numVertices, c.RA, c.posA, cr, mn0, mx0);
-            project(S.verts, pb.vertexOffset, pb.numVertices, c.RB, c.posB, cr, mn1, mx1);
-            const float d = fminf(mx0 - mn1, mx1 - mn0);
-            if (d < best) {
-                best = d;
-                bestIdx = base + e;
-                bestAxis = cr;
-            }
-        }
+        if (!(fabsf(cr.x) > 1e-6f || fabsf(cr.y) > 1e-6f || fabsf(cr.z) > 1e-6f)) return false;
+        const float cl = length(cr);
+        n = cr * (1.f / cl);
+        err = delta * (1.f + 1.f / cl);
     }
-    float bv = best;
-    int bi = bestIdx;
-    warp_argmin(bv, bi);
-    if (bi == 0x7fffffff) return false;
-    const unsigned who = __ballot_sync(0xffffffffu, bestIdx == bi && best == bv);
-    const int src = __ffs(who) - 1;
-    sep.x = __shfl_sync(0xffffffffu, bestAxis.x, src);
-    sep.y = __shfl_sync(0xffffffffu, bestAxis.y, src);
-    sep.z = __shfl_sync(0xffffffffu, bestAxis.z, src);
-    if (dot(-D, sep) > 0.f) sep = -sep;
+    if (dot(D, n) < 0.f) n = -n;
+    float mn0, mx0, mn1, mx1;
+    project_rel(S.verts, pa.vertexOffset, pa.numVertices, c.RA, n, mn0, mx0);
+    project_rel(S.verts, pb.vertexOffset, pb.numVertices, c.RB, n, mn1, mx1);
+    const float off = dot(rel, n);  // posB - posA along n
+    mn1 += off;
+    mx1 += off;
+    d = fminf(mx0 - mn1, mx1 - mn0);
     return true;
 }
 
-// One Sutherland-Hodgman step: keep the part behind plane (n, eq).
-// Warp-parallel, output order identical to the sequential loop.
-__device__ int clip_poly(const float4* in, int nin, float3 pn, float eq, float4* out, int* ovf) {
+// float-float evaluation of one axis: oriented axis and depth; false if
+// the edge pair is degenerate
+__device__ bool axis_ff(const PairCtx& c, const b3::ShapesDev& S, int idx, ff3 Dff, ff3& n, ff& d, bool& isFace) {
+    const b3ConvexPolyhedron& pa = *c.pa;
+    const b3ConvexPolyhedron& pb = *c.pb;
+    const int FA = pa.numFaces, FB = pb.numFaces;
+    if (idx < FA + FB) {
+        isFace = true;
+        const bool onA = idx < FA;
+        const float4 pl = __ldg((const float4*)&S.faces[onA ? pa.faceOffset + idx : pb.faceOffset + idx - FA].plane[0]);
+        n = mrot(onA ? c.FA : c.FB, make_float3(pl.x, pl.y, pl.z));
+    } else {
+        isFace = false;
+        const int e = idx - FA - FB;
+        const int EB = pb.numUniqueEdges;
+        const int e0 = e / EB, e1 = e - e0 * EB;
+        const float4 ea = __ldg(&S.edges[pa.uniqueEdgesOffset + e0]);
+        const float4 eb = __ldg(&S.edges[pb.uniqueEdgesOffset + e1]);
+        const ff3 wa = mrot(c.FA, make_float3(ea.x, ea.y, ea.z));
+        const ff3 wb = mrot(c.FB, make_float3(eb.x, eb.y, eb.z));
+        const ff3 cr = cross3(wa, wb);
+        if (dot3(cr, cr).hi <= 0.f) return false;
+        n = normalize3(cr);
+    }
+    if (dot3(Dff, n).hi < 0.f) n = neg3(n);
+    // projections (P2/sat.cl:227-252) in float-float
+    ff lo[2], hi[2];
+    for (int h = 0; h < 2; ++h) {
+        const b3ConvexPolyhedron& p = h == 0 ? pa : pb;
+        const float3 pos = h == 0 ? c.posA : c.posB;
+        const ff3 ld = mrot_t(h == 0 ? c.FA : c.FB, n);
+        ff mn = mk(FLT_MAX), mx = mk(-FLT_MAX);
+        for (int i = 0; i < p.numVertices; ++i) {
+            const float4 v = __ldg(&S.verts[p.vertexOffset + i]);
+            const ff dp = add(add(mulf(ld.x, v.x), mulf(ld.y, v.y)), mulf(ld.z, v.z));
+            if (lt(dp, mn)) mn = dp;
+            if (lt(mx, dp)) mx = dp;
+        }
+        const ff offs = add(add(mulf(n.x, pos.x), mulf(n.y, pos.y)), mulf(n.z, pos.z));
+        lo[h] = add(mn, offs);
+        hi[h] = add(mx, offs);
+    }
+    const ff d0 = sub(hi[0], lo[1]), d1 = sub(hi[1], lo[0]);
+    d = lt(d0, d1) ? d0 : d1;
+    return true;
+}
+
+// Separating-axis search (findSeparatingAxisKernel, P2/sat.cl:928-1262):
+// FP32 sweep over all axes by the warp, then float-float refinement of every
+// axis whose FP32 depth is within delta of the minimum. Returns false if a
+// face axis separates or no axis exists.
+__device__ bool find_axis(const PairCtx& c, const b3::ShapesDev& S, WarpScratch& W, ff3& sep, int* ovfCounter) {
+    const int lane = threadIdx.x & 31;
+    const b3ConvexPolyhedron& pa = *c.pa;
+    const b3ConvexPolyhedron& pb = *c.pb;
+    const float3 lcA = make_float3(pa.localCenter[0], pa.localCenter[1], pa.localCenter[2]);
+    const float3 lcB = make_float3(pb.localCenter[0], pb.localCenter[1], pb.localCenter[2]);
+    const float3 rel = c.posB - c.posA;
+    const float3 D = mul(c.RA, lcA) - (mul(c.RB, lcB) + rel);
+    const int nFace = pa.numFaces + pb.numFaces;
+    const int nAxes = nFace + pa.numUniqueEdges * pb.numUniqueEdges;
+    const float scale = 1.f + sqrtf(pa.mE[0] * pa.mE[0] + pa.mE[1] * pa.mE[1] + pa.mE[2] * pa.mE[2]) +
+                        sqrtf(pb.mE[0] * pb.mE[0] + pb.mE[1] * pb.mE[1] + pb.mE[2] * pb.mE[2]) + length(rel);
+    // FP32 depth error bound for well-conditioned axes (a few ulps of the
+    // largest projected coordinate); edge axes add a term inversely
+    // proportional to |e0 x e1| (their normalisation amplifies rounding)
+    const float delta = 1e-6f * scale;
+    float kd[kKeep];
+    int ki[kKeep];
+#pragma unroll
+    for (int k = 0; k < kKeep; ++k) {
+        kd[k] = FLT_MAX;
+        ki[k] = kNone;
+    }
+    // face axes whose separation test is ambiguous in FP32 (|d| <= delta)
+    int amb[2] = {kNone, kNone};
+    bool ambOverflow = false;
+    float sepMin = FLT_MAX;
+    float upper = FLT_MAX;  // min over axes of (d + err): bounds the true minimum depth
+    for (int idx = lane; idx < nAxes; idx += 32) {
+        float3 n;
+        float d, err;
+        bool isFace;
+        if (!axis_f32(c, S, idx, D, rel, delta, n, d, err, isFace)) continue;
+        if (isFace) {
+            sepMin = fminf(sepMin, d);
+            if (fabsf(d) <= delta) {
+                if (amb[0] == kNone) amb[0] = idx;
+                else if (amb[1] == kNone) amb[1] = idx;
+                else ambOverflow = true;
+            }
+        }
+        upper = fminf(upper, d + err);
+        const float lo = d - err;  // lower bound of this axis' depth
+        if (!(lo < kd[kKeep - 1])) continue;  // also drops NaN
+        // insertion into the lane's sorted keep list (indices increase)
+        float cd = lo;
+        int ci = idx;
+#pragma unroll
+        for (int k = 0; k < kKeep; ++k) {
+            if (cd < kd[k]) {
+                const float td = kd[k];
+                const int ti = ki[k];
+                kd[k] = cd;
+                ki[k] = ci;
+                cd = td;
+                ci = ti;
+            }
+        }
+    }
+    // clearly separated by a face axis
+    float sm = sepMin;
+    int dummy = 0;
+    warp_argmin(sm, dummy);
+    if (sm < -delta) return false;
+    float best = upper;
+    int bi = 0;
+    warp_argmin(best, bi);
+    if (!(best < FLT_MAX)) return false;
+    const float lim = best;
+    // collect candidates
+    int count = 0;
+    bool overflow = kd[kKeep - 1] <= lim || ambOverflow;
+    for (int k = 0; k < kKeep + 2; ++k) {
+        const int id = k < kKeep ? ki[k] : amb[k - kKeep];
+        const bool take = id != kNone && (k >= kKeep || kd[k] <= lim);
+        const unsigned m = __ballot_sync(0xffffffffu, take);
+        const int pos = count + __popc(m & b3dev::lanemask_lt());
+        if (take && pos < kMaxCand) W.cand[pos] = id;
+        count += __popc(m);
+    }
+    if (__any_sync(0xffffffffu, overflow) || count > kMaxCand) {
+        // more near-minimum axes than the keep lists hold: rescan
+        count = 0;
+        for (int base = 0; base < nAxes; base += 32) {
+            const int idx = base + lane;
+            float3 n;
+            float d = FLT_MAX, err = 0.f;
+            bool isFace;
+            bool take = false;
+            if (idx < nAxes && axis_f32(c, S, idx, D, rel, delta, n, d, err, isFace))
+                take = d - err <= lim || (isFace && fabsf(d) <= delta);
+            const unsigned m = __ballot_sync(0xffffffffu, take);
+            const int pos = count + __popc(m & b3dev::lanemask_lt());
+            if (take && pos < kMaxCand) W.cand[pos] = idx;
+            count += __popc(m);
+        }
+        if (count > kMaxCand) {
+            if (lane == 0) atomicAdd(ovfCounter, 1);
+            count = kMaxCand;
+        }
+    }
+    __syncwarp();
+    // float-float refinement of the candidates
+    const ff3 lcAw = mrot(c.FA, make_float3(lcA.x, lcA.y, lcA.z));
+    const ff3 lcBw = mrot(c.FB, make_float3(lcB.x, lcB.y, lcB.z));
+    const ff3 Dff = sub3(add3(lcAw, mk3(c.posA.x, c.posA.y, c.posA.z)), add3(lcBw, mk3(c.posB.x, c.posB.y, c.posB.z)));
+    ff bd = mk(FLT_MAX);
+    int bidx = kNone;
+    ff3 bn = mk3(0.f, 0.f, 0.f);
+    bool fsep = false;
+    if (lane < count) {
+        const int idx = W.cand[lane];
+        ff3 n;
+        ff d;
+        bool isFace;
+        if (axis_ff(c, S, idx, Dff, n, d, isFace)) {
+            if (isFace && d.hi < 0.f) fsep = true;
+            bd = d;
+            bidx = idx;
+            bn = n;
+        }
+    }
+    if (__any_sync(0xffffffffu, fsep)) return false;
+    ff wd = bd;
+    int widx = bidx;
+    warp_argmin_ff(wd, widx);
+    if (widx == kNone) return false;
+    const unsigned who = __ballot_sync(0xffffffffu, bidx == widx);
+    const int src = __ffs(who) - 1;
+    sep.x.hi = __shfl_sync(0xffffffffu, bn.x.hi, src);
+    sep.x.lo = __shfl_sync(0xffffffffu, bn.x.lo, src);
+    sep.y.hi = __shfl_sync(0xffffffffu, bn.y.hi, src);
+    sep.y.lo = __shfl_sync(0xffffffffu, bn.y.lo, src);
+    sep.z.hi = __shfl_sync(0xffffffffu, bn.z.hi, src);
+    sep.z.lo = __shfl_sync(0xffffffffu, bn.z.lo, src);
+    if (dot3(neg3(Dff), sep).hi > 0.f) sep = neg3(sep);
+    return true;
+}
+
+// One Sutherland-Hodgman step in float-float (clipFace,
+// satClipHullContacts.cl:303-351), one polygon vertex per lane; output
+// order identical to the sequential loop.
+__device__ int clip_poly_ff(const FfVert* in, int nin, ff3 pn, ff eq, FfVert* out, int* ovf) {
     const int lane = threadIdx.x & 31;
     int total = 0;
     for (int base = 0; base < nin; base += 32) {
         const int ve = base + lane;
         int cnt = 0;
-        float4 o0 = make_float4(0, 0, 0, 0), o1 = make_float4(0, 0, 0, 0);
+        ff3 o0 = mk3(0.f, 0.f, 0.f), o1 = o0;
         if (ve < nin) {
-            const float4 s = in[ve == 0 ? nin - 1 : ve - 1];
-            const float4 e = in[ve];
-            const float ds = pn.x * s.x + pn.y * s.y + pn.z * s.z + eq;
-            const float de = pn.x * e.x + pn.y * e.y + pn.z * e.z + eq;
-            if (ds < 0.f) {
-                if (de < 0.f) {
+            const ff3 s = vget(in[ve == 0 ? nin - 1 : ve - 1]);
+            const ff3 e = vget(in[ve]);
+            const ff ds = add(dot3(pn, s), eq);
+            const ff de = add(dot3(pn, e), eq);
+            const bool sNeg = ds.hi < 0.f, eNeg = de.hi < 0.f;
+            if (sNeg || eNeg) {
+                if (sNeg && eNeg) {
                     o0 = e;
                     cnt = 1;
                 } else {
-                    const float t = ds * 1.f / (ds - de);
-                    o0 = make_float4(s.x + (e.x - s.x) * t, s.y + (e.y - s.y) * t, s.z + (e.z - s.z) * t, 0.f);
+                    const ff t = div(ds, sub(ds, de));
+                    o0 = add3(s, scale3(sub3(e, s), t));
                     cnt = 1;
+                    if (!sNeg) {
+                        o1 = e;
+                        cnt = 2;
+                    }
                 }
-            } else if (de < 0.f) {
-                const float t = ds * 1.f / (ds - de);
-                o0 = make_float4(s.x + (e.x - s.x) * t, s.y + (e.y - s.y) * t, s.z + (e.z - s.z) * t, 0.f);
-                o1 = e;
-                cnt = 2;
             }
         }
-        // exclusive prefix of cnt across lanes
         int x = cnt;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -219,10 +393,10 @@ __device__ int clip_poly(const float4* in, int nin, float3 pn, float eq, float4*
         }
         const int pos = total + x - cnt;
         if (cnt >= 1) {
-            if (pos < kMaxPoly) out[pos] = o0; else atomicAdd(ovf, 1);
+            if (pos < kMaxPoly) out[pos] = vput(o0, mk(0.f)); else atomicAdd(ovf, 1);
         }
         if (cnt == 2) {
-            if (pos + 1 < kMaxPoly) out[pos + 1] = o1; else atomicAdd(ovf, 1);
+            if (pos + 1 < kMaxPoly) out[pos + 1] = vput(o1, mk(0.f)); else atomicAdd(ovf, 1);
         }
         total += __shfl_sync(0xffffffffu, x, 31);
     }
@@ -230,72 +404,96 @@ __device__ int clip_poly(const float4* in, int nin, float3 pn, float eq, float4*
     return min(total, kMaxPoly);
 }
 
-// clipHullAgainstHull: returns the number of kept points, stored with
-// w = depth in W.poly[*outBuf].
-__device__ int clip_hull_hull(const PairCtx& c, const b3::ShapesDev& S, const NpParams& P,
-                              float3 sep, WarpScratch& W, int* outBuf, int* ovf) {
+// First face minimising sign * dot(R n_f, sep) (the reference's strict
+// comparisons: the first extreme face wins). FP32 sweep, then faces within
+// a small window of the FP32 extreme are re-ranked in float-float.
+__device__ int select_face(const b3::ShapesDev& S, const b3ConvexPolyhedron& h, const Mat3& R, const ffmat& F,
+                           float3 sepf, ff3 sep, float sign) {
+    const int lane = threadIdx.x & 31;
+    float bv = FLT_MAX;
+    int bi = kNone;
+    for (int f = lane; f < h.numFaces; f += 32) {
+        const float4 pl = __ldg((const float4*)&S.faces[h.faceOffset + f].plane[0]);
+        const float d = sign * dot(mul(R, make_float3(pl.x, pl.y, pl.z)), sepf);
+        if (d < bv) { bv = d; bi = f; }
+    }
+    float wv = bv;
+    int wi = bi;
+    warp_argmin(wv, wi);
+    if (wi == kNone) return kNone;
+    const float lim = wv + 4e-6f;
+    ff rv = mk(FLT_MAX);
+    int ri = kNone;
+    for (int f = lane; f < h.numFaces; f += 32) {
+        const float4 pl = __ldg((const float4*)&S.faces[h.faceOffset + f].plane[0]);
+        const float3 nl = make_float3(pl.x, pl.y, pl.z);
+        if (!(sign * dot(mul(R, nl), sepf) <= lim)) continue;
+        ff d = dot3(mrot(F, nl), sep);
+        if (sign < 0.f) d = neg(d);
+        if (lt(d, rv)) { rv = d; ri = f; }
+    }
+    warp_argmin_ff(rv, ri);
+    return ri == kNone ? wi : ri;
+}
+
+// clipHullAgainstHull (satClipHullContacts.cl:556-611 + clipFaceAgainstHull
+// :353-452) in float-float; kept points (x, y, z, depth) end in
+// W.poly[*outBuf].
+__device__ int clip_hull_hull(const PairCtx& c, const b3::ShapesDev& S, const NpParams& P, ff3 sep,
+                              WarpScratch& W, int* outBuf, int* ovf) {
     const int lane = threadIdx.x & 31;
     const b3ConvexPolyhedron& pa = *c.pa;
     const b3ConvexPolyhedron& pb = *c.pb;
-    // incident face of B: max dot(nB, sep), first wins
-    float bv = FLT_MAX;
-    int bi = 0x7fffffff;
-    for (int f = lane; f < pb.numFaces; f += 32) {
-        const float4 pl = __ldg((const float4*)&S.faces[pb.faceOffset + f].plane[0]);
-        const float d = -dot(mul(c.RB, make_float3(pl.x, pl.y, pl.z)), sep);
-        if (d < bv) { bv = d; bi = f; }
-    }
-    warp_argmin(bv, bi);
-    // reference face of A: min dot(nA, sep), first wins
-    float av = FLT_MAX;
-    int ai = 0x7fffffff;
-    for (int f = lane; f < pa.numFaces; f += 32) {
-        const float4 pl = __ldg((const float4*)&S.faces[pa.faceOffset + f].plane[0]);
-        const float d = dot(mul(c.RA, make_float3(pl.x, pl.y, pl.z)), sep);
-        if (d < av) { av = d; ai = f; }
-    }
-    warp_argmin(av, ai);
-    if (ai == 0x7fffffff || bi == 0x7fffffff) return 0;
+    const float3 sepf = to_f3(sep);
+    // incident face of B: max dot(nB, sep); reference face of A: min dot(nA, sep)
+    const int bi = select_face(S, pb, c.RB, c.FB, sepf, sep, -1.f);
+    const int ai = select_face(S, pa, c.RA, c.FA, sepf, sep, 1.f);
+    if (ai == kNone || bi == kNone) return 0;
     const b3Face fB = S.faces[pb.faceOffset + bi];
     const b3Face fA = S.faces[pa.faceOffset + ai];
+    const ff3 posA = mk3(c.posA.x, c.posA.y, c.posA.z);
+    const ff3 posB = mk3(c.posB.x, c.posB.y, c.posB.z);
     int nIn = min(fB.numIndices, kMaxPoly);
     for (int k = lane; k < nIn; k += 32) {
         const float4 v = __ldg(&S.verts[pb.vertexOffset + S.indices[fB.indexOffset + k]]);
-        W.poly[0][k] = f4(mul(c.RB, f3(v)) + c.posB);
+        W.poly[0][k] = vput(add3(mrot(c.FB, make_float3(v.x, v.y, v.z)), posB), mk(0.f));
     }
     __syncwarp();
     int cur = 0;
-    const float3 nAw = mul(c.RA, make_float3(fA.plane[0], fA.plane[1], fA.plane[2]));
+    const ff3 nAw = mrot(c.FA, make_float3(fA.plane[0], fA.plane[1], fA.plane[2]));
     const int nvA = fA.numIndices;
     for (int e0 = 0; e0 < nvA; ++e0) {
         const float4 a = __ldg(&S.verts[pa.vertexOffset + S.indices[fA.indexOffset + e0]]);
         const float4 b = __ldg(&S.verts[pa.vertexOffset + S.indices[fA.indexOffset + (e0 + 1) % nvA]]);
-        const float3 we = mul(c.RA, make_float3(a.x - b.x, a.y - b.y, a.z - b.z));
-        const float3 pn = -cross(we, nAw);
-        const float3 wa = mul(c.RA, f3(a)) + c.posA;
-        const float eq = -dot(wa, pn);
-        nIn = clip_poly(W.poly[cur], nIn, pn, eq, W.poly[cur ^ 1], ovf);
+        // a - b of two FP32 vertices is exact in float-float
+        const ff3 edge = sub3(mk3(a.x, a.y, a.z), mk3(b.x, b.y, b.z));
+        const ff3 we{add(add(mul(c.FA.m[0][0], edge.x), mul(c.FA.m[0][1], edge.y)), mul(c.FA.m[0][2], edge.z)),
+                     add(add(mul(c.FA.m[1][0], edge.x), mul(c.FA.m[1][1], edge.y)), mul(c.FA.m[1][2], edge.z)),
+                     add(add(mul(c.FA.m[2][0], edge.x), mul(c.FA.m[2][1], edge.y)), mul(c.FA.m[2][2], edge.z))};
+        const ff3 pn = neg3(cross3(we, nAw));
+        const ff3 wa = add3(mrot(c.FA, make_float3(a.x, a.y, a.z)), posA);
+        const ff eq = neg(dot3(wa, pn));
+        nIn = clip_poly_ff(W.poly[cur], nIn, pn, eq, W.poly[cur ^ 1], ovf);
         cur ^= 1;
     }
     // keep points behind the witness face (clipFaceAgainstHull :433-452)
-    const float eqA = fA.plane[3] - dot(nAw, c.posA);
+    const ff eqA = sub(mk(fA.plane[3]), dot3(nAw, posA));
+    const ff minD = mk(P.minDist), maxD = mk(P.maxDist);
     int total = 0;
     for (int base = 0; base < nIn; base += 32) {
         const int k = base + lane;
         bool keep = false;
-        float4 pt = make_float4(0.f, 0.f, 0.f, 0.f);
+        ff3 p = mk3(0.f, 0.f, 0.f);
+        ff depth = mk(0.f);
         if (k < nIn) {
-            pt = W.poly[cur][k];
-            float depth = dot(nAw, f3(pt)) + eqA;
-            if (depth <= P.minDist) depth = P.minDist;
-            if (depth <= P.maxDist) {
-                keep = true;
-                pt.w = depth;
-            }
+            p = vget(W.poly[cur][k]);
+            depth = add(dot3(nAw, p), eqA);
+            if (le(depth, minD)) depth = minD;
+            keep = le(depth, maxD);
         }
         const unsigned m = __ballot_sync(0xffffffffu, keep);
         const int pos = total + __popc(m & b3dev::lanemask_lt());
-        if (keep) W.poly[cur ^ 1][pos] = pt;
+        if (keep) W.poly[cur ^ 1][pos] = vput(p, depth);
         total += __popc(m);
     }
     __syncwarp();
@@ -304,60 +502,46 @@ __device__ int clip_hull_hull(const PairCtx& c, const b3::ShapesDev& S, const Np
 }
 
 // extractManifoldSequentialGlobal (P2/satClipHullContacts.cl:678-770) over
-// n > 4 points in p; returns the 4 chosen indices.
-__device__ int4 reduce_manifold(const float4* p, int n, float3 nearNormal) {
+// n > 4 float-float points; returns the 4 chosen indices.
+__device__ int4 reduce_manifold(const FfVert* p, int n, ff3 nearNormal) {
     const int lane = threadIdx.x & 31;
-    // centre (float4 incl. w)
-    float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
+    // centre in point order (sequential float-float sum on every lane)
+    ff3 s = mk3(0.f, 0.f, 0.f);
+    for (int k = 0; k < n; ++k) s = add3(s, vget(p[k]));
+    const ff invn = div(mk(1.f), mk((float)n));
+    const ff3 center = scale3(s, invn);
+    const ff3 aV = sub3(vget(p[0]), center);
+    ff3 u = cross3(nearNormal, aV);
+    ff3 v = cross3(nearNormal, u);
+    u = normalize3(u);
+    v = normalize3(v);
+    ff mw = mk(FLT_MAX), f0 = mk(FLT_MIN), f1 = mk(FLT_MIN), f2 = mk(FLT_MIN), f3v = mk(FLT_MIN);
+    int iw = kNone, i0 = kNone, i1 = kNone, i2 = kNone, i3 = kNone;
     for (int k = lane; k < n; k += 32) {
-        const float4 q = p[k];
-        s.x += q.x; s.y += q.y; s.z += q.z; s.w += q.w;
+        const ff w = wget(p[k]);
+        if (lt(w, mw)) { mw = w; iw = k; }
+        const ff3 r = sub3(vget(p[k]), center);
+        const ff du = dot3(u, r), dv = dot3(v, r);
+        if (lt(du, f0)) { f0 = du; i0 = k; }
+        if (lt(neg(du), f1)) { f1 = neg(du); i1 = k; }
+        if (lt(dv, f2)) { f2 = dv; i2 = k; }
+        if (lt(neg(dv), f3v)) { f3v = neg(dv); i3 = k; }
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
-        s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
-        s.z += __shfl_xor_sync(0xffffffffu, s.z, o);
-        s.w += __shfl_xor_sync(0xffffffffu, s.w, o);
-    }
-    const float inv = 1.f / (float)n;
-    const float3 center = make_float3(s.x * inv, s.y * inv, s.z * inv);
-    const float3 aV = f3(p[0]) - center;
-    float3 u = cross(nearNormal, aV);
-    float3 v = cross(nearNormal, u);
-    u = normalize(u);
-    v = normalize(v);
-    float mw = FLT_MAX, f0 = FLT_MIN, f1 = FLT_MIN, f2 = FLT_MIN, f3v = FLT_MIN;
-    int iw = -1, i0 = 0x7fffffff, i1 = 0x7fffffff, i2 = 0x7fffffff, i3 = 0x7fffffff;
-    for (int k = lane; k < n; k += 32) {
-        const float4 q = p[k];
-        if (q.w < mw) { mw = q.w; iw = k; }
-        const float3 r = f3(q) - center;
-        const float du = dot(u, r), dv = dot(v, r);
-        if (du < f0) { f0 = du; i0 = k; }
-        if (-du < f1) { f1 = -du; i1 = k; }
-        if (dv < f2) { f2 = dv; i2 = k; }
-        if (-dv < f3v) { f3v = -dv; i3 = k; }
-    }
-    if (iw < 0) iw = 0x7fffffff;
-    warp_argmin(mw, iw);
-    warp_argmin(f0, i0);
-    warp_argmin(f1, i1);
-    warp_argmin(f2, i2);
-    warp_argmin(f3v, i3);
-    int4 idx = make_int4(i0 == 0x7fffffff ? 0 : i0, i1 == 0x7fffffff ? 1 : i1,
-                         i2 == 0x7fffffff ? 2 : i2, i3 == 0x7fffffff ? 3 : i3);
-    const int minIndex = (iw == 0x7fffffff) ? -1 : iw;
-    if (idx.x != minIndex && idx.y != minIndex && idx.z != minIndex && idx.w != minIndex)
-        idx.x = minIndex;
+    warp_argmin_ff(mw, iw);
+    warp_argmin_ff(f0, i0);
+    warp_argmin_ff(f1, i1);
+    warp_argmin_ff(f2, i2);
+    warp_argmin_ff(f3v, i3);
+    int4 idx = make_int4(i0 == kNone ? 0 : i0, i1 == kNone ? 1 : i1, i2 == kNone ? 2 : i2, i3 == kNone ? 3 : i3);
+    const int minIndex = iw == kNone ? -1 : iw;
+    if (idx.x != minIndex && idx.y != minIndex && idx.z != minIndex && idx.w != minIndex) idx.x = minIndex;
     return idx;
 }
 
 __global__ void __launch_bounds__(128)
-k_narrowphase(const int2* __restrict__ pairs, const int32_t* __restrict__ numPairsDev,
-              b3::BodiesDev Bd, b3::ShapesDev S, NpParams P, b3Contact4* __restrict__ contacts,
-              uint32_t* __restrict__ manifoldFlag, int32_t* __restrict__ workCounter,
-              b3Counters* __restrict__ counters) {
+k_narrowphase(const int2* __restrict__ pairs, const int32_t* __restrict__ numPairsDev, b3::BodiesDev Bd,
+              b3::ShapesDev S, NpParams P, b3Contact4* __restrict__ contacts, uint32_t* __restrict__ manifoldFlag,
+              int32_t* __restrict__ workCounter, b3Counters* __restrict__ counters) {
     extern __shared__ __align__(16) unsigned char np_smem[];
     const int lane = threadIdx.x & 31;
     WarpScratch& W = reinterpret_cast<WarpScratch*>(np_smem)[threadIdx.x >> 5];
@@ -378,21 +562,25 @@ k_narrowphase(const int2* __restrict__ pairs, const int32_t* __restrict__ numPai
             const b3Collidable colA = S.cols[Bd.collidable[c.A]];
             const b3Collidable colB = S.cols[Bd.collidable[c.B]];
             int nOut = 0, buf = 0;
-            float3 sep = make_float3(0.f, 0.f, 0.f);
-            if (!(c.invMassA == 0.f && c.invMassB == 0.f) &&
-                colA.shapeType == B3_SHAPE_CONVEX_HULL && colB.shapeType == B3_SHAPE_CONVEX_HULL) {
+            ff3 sep = mk3(0.f, 0.f, 0.f);
+            if (!(c.invMassA == 0.f && c.invMassB == 0.f) && colA.shapeType == B3_SHAPE_CONVEX_HULL &&
+                colB.shapeType == B3_SHAPE_CONVEX_HULL) {
                 c.pa = &S.polys[colA.shapeIndex];
                 c.pb = &S.polys[colB.shapeIndex];
-                c.RA = quat_to_mat(Bd.quat[c.A]);
-                c.RB = quat_to_mat(Bd.quat[c.B]);
+                c.qA = Bd.quat[c.A];
+                c.qB = Bd.quat[c.B];
+                c.RA = quat_to_mat(c.qA);
+                c.RB = quat_to_mat(c.qB);
+                c.FA = quat_mat(c.qA);
+                c.FB = quat_mat(c.qB);
                 c.posA = f3(Bd.pos[c.A]);
                 c.posB = f3(Bd.pos[c.B]);
-                if (find_axis(c, S, sep))
+                if (find_axis(c, S, W, sep, &counters->clipOverflow))
                     nOut = clip_hull_hull(c, S, P, sep, W, &buf, &counters->clipOverflow);
             }
             if (nOut > 0) {
-                const float4* pts = W.poly[buf];
-                const float3 nrm = -sep;
+                const FfVert* pts = W.poly[buf];
+                const ff3 nrm = neg3(sep);
                 int4 idx = make_int4(0, 1, 2, 3);
                 int nRed = nOut;
                 if (nOut > 4) {
@@ -402,13 +590,15 @@ k_narrowphase(const int2* __restrict__ pairs, const int32_t* __restrict__ numPai
                 b3Contact4* out = &contacts[p];
                 if (lane < nRed) {
                     const int k = lane == 0 ? idx.x : lane == 1 ? idx.y : lane == 2 ? idx.z : idx.w;
-                    const float4 q = pts[k];
-                    *reinterpret_cast<float4*>(&out->worldPos[lane][0]) = q;
+                    const FfVert q = pts[k];
+                    *reinterpret_cast<float4*>(&out->worldPos[lane][0]) =
+                        make_float4(q.xh + q.xl, q.yh + q.yl, q.zh + q.zl, q.wh + q.wl);
                 } else if (lane < 4) {
                     *reinterpret_cast<float4*>(&out->worldPos[lane][0]) = make_float4(0.f, 0.f, 0.f, 0.f);
                 }
                 if (lane == 4) {
-                    *reinterpret_cast<float4*>(&out->worldNormal[0]) = make_float4(nrm.x, nrm.y, nrm.z, (float)nRed);
+                    const float3 n = to_f3(nrm);
+                    *reinterpret_cast<float4*>(&out->worldNormal[0]) = make_float4(n.x, n.y, n.z, (float)nRed);
                     out->friction = combine_friction(Bd.friction[c.A], Bd.friction[c.B], P.frictionCombine);
                     out->pairIndex = p;
                     out->bodyAPtrAndSignBit = c.invMassA == 0.f ? -c.A : c.A;
