@@ -263,6 +263,8 @@ def main():
         "config": {"workload": WORKLOADS[args.workload], "bodies": sc.n, "worlds": sc.num_worlds,
                    "pairs": res["counters"]["numPairs"], "manifolds": res["counters"]["numManifolds"],
                    "contact_points": res["counters"]["numContactPoints"], "iterations": 10,
+                   "refined_axes": res["counters"].get("refinedAxes"),
+                   "refined_clips": res["counters"].get("refinedClips"),
                    "parallelism": "replicas" if world_size > 1 else "single",
                    "l2": "working set exceeds L2" if sc.n > 100000 else "working set L2-resident; no flush"},
         "contacts_per_s": res["counters"]["numContactPoints"] * args.steps * world_size / (res["ms"] / 1e3),

@@ -70,7 +70,8 @@ class Contact4(C.Structure):
 class Counters(C.Structure):
     _fields_ = [("numPairs", C.c_int32), ("numManifolds", C.c_int32), ("numContactPoints", C.c_int32),
                 ("pairOverflow", C.c_int32), ("cellOverflow", C.c_int32), ("timeouts", C.c_int32),
-                ("clipOverflow", C.c_int32), ("steps", C.c_int32)]
+                ("clipOverflow", C.c_int32), ("steps", C.c_int32), ("refinedAxes", C.c_int32),
+                ("refinedClips", C.c_int32)]
 
     def as_dict(self):
         return {f: int(getattr(self, f)) for f, _ in self._fields_}

@@ -62,7 +62,7 @@ __device__ __forceinline__ ff mulf(ff a, float b) {
     p.lo = __fmaf_rn(a.lo, b, p.lo);
     return fast_two_sum(p.hi, p.lo);
 }
-__device__ __forceinline__ ff div(ff a, ff b) {
+__device__ __noinline__ ff div(ff a, ff b) {
     const float q1 = __fdiv_rn(a.hi, b.hi);
     const ff r = sub(a, mulf(b, q1));
     const float q2 = __fdiv_rn(r.hi, b.hi);
@@ -71,7 +71,7 @@ __device__ __forceinline__ ff div(ff a, ff b) {
     ff q = fast_two_sum(q1, q2);
     return add(q, mk(q3));
 }
-__device__ __forceinline__ ff sqrt_ff(ff a) {
+__device__ __noinline__ ff sqrt_ff(ff a) {
     if (a.hi <= 0.f) return mk(0.f);
     const float s = __fsqrt_rn(a.hi);
     // one Newton step: s + (a - s^2) / (2 s)
@@ -87,12 +87,12 @@ __device__ __forceinline__ ff3 add3(ff3 a, ff3 b) { return {add(a.x, b.x), add(a
 __device__ __forceinline__ ff3 sub3(ff3 a, ff3 b) { return {sub(a.x, b.x), sub(a.y, b.y), sub(a.z, b.z)}; }
 __device__ __forceinline__ ff3 neg3(ff3 a) { return {neg(a.x), neg(a.y), neg(a.z)}; }
 __device__ __forceinline__ ff3 scale3(ff3 a, ff s) { return {mul(a.x, s), mul(a.y, s), mul(a.z, s)}; }
-__device__ __forceinline__ ff dot3(ff3 a, ff3 b) { return add(add(mul(a.x, b.x), mul(a.y, b.y)), mul(a.z, b.z)); }
-__device__ __forceinline__ ff3 cross3(ff3 a, ff3 b) {
+__device__ __noinline__ ff dot3(ff3 a, ff3 b) { return add(add(mul(a.x, b.x), mul(a.y, b.y)), mul(a.z, b.z)); }
+__device__ __noinline__ ff3 cross3(ff3 a, ff3 b) {
     return {sub(mul(a.y, b.z), mul(a.z, b.y)), sub(mul(a.z, b.x), mul(a.x, b.z)),
             sub(mul(a.x, b.y), mul(a.y, b.x))};
 }
-__device__ __forceinline__ ff3 normalize3(ff3 a) {
+__device__ __noinline__ ff3 normalize3(ff3 a) {
     const ff l2 = dot3(a, a);
     if (l2.hi <= 0.f) return a;
     const ff l = sqrt_ff(l2);
@@ -129,7 +129,7 @@ __device__ __forceinline__ ff3 qinvrot(float4 q, ff3 v) {
 struct ffmat {
     ff m[3][3];
 };
-__device__ __forceinline__ ffmat quat_mat(float4 q) {
+__device__ __noinline__ ffmat quat_mat(float4 q) {
     const ff xx = two_prod(q.x, q.x), yy = two_prod(q.y, q.y), zz = two_prod(q.z, q.z), ww = two_prod(q.w, q.w);
     const ff xy = two_prod(q.x, q.y), xz = two_prod(q.x, q.z), yz = two_prod(q.y, q.z);
     const ff wx = two_prod(q.w, q.x), wy = two_prod(q.w, q.y), wz = two_prod(q.w, q.z);
@@ -147,7 +147,7 @@ __device__ __forceinline__ ffmat quat_mat(float4 q) {
     return R;
 }
 // R v for an FP32 vector
-__device__ __forceinline__ ff3 mrot(const ffmat& R, float3 v) {
+__device__ __noinline__ ff3 mrot(const ffmat& R, float3 v) {
     ff3 r;
     r.x = add(add(mulf(R.m[0][0], v.x), mulf(R.m[0][1], v.y)), mulf(R.m[0][2], v.z));
     r.y = add(add(mulf(R.m[1][0], v.x), mulf(R.m[1][1], v.y)), mulf(R.m[1][2], v.z));
@@ -155,7 +155,7 @@ __device__ __forceinline__ ff3 mrot(const ffmat& R, float3 v) {
     return r;
 }
 // R^T v for a float-float vector
-__device__ __forceinline__ ff3 mrot_t(const ffmat& R, ff3 v) {
+__device__ __noinline__ ff3 mrot_t(const ffmat& R, ff3 v) {
     ff3 r;
     r.x = add(add(mul(R.m[0][0], v.x), mul(R.m[1][0], v.y)), mul(R.m[2][0], v.z));
     r.y = add(add(mul(R.m[0][1], v.x), mul(R.m[1][1], v.y)), mul(R.m[2][1], v.z));

@@ -61,7 +61,9 @@ struct __align__(16) FfVert {
 };
 struct __align__(16) WarpScratch {
     FfVert poly[2][kMaxPoly];
+    FfVert planes[kMaxPoly];  // float-float clip planes (normal, constant)
     int cand[kMaxCand];
+    int refinedAxes, refinedClips;  // float-float fallbacks taken by this warp
 };
 
 __device__ __forceinline__ ff3 vget(const FfVert& v) { return {{v.xh, v.xl}, {v.yh, v.yl}, {v.zh, v.zl}}; }
@@ -108,6 +110,7 @@ struct PairCtx {
     float4 qA, qB;
     Mat3 RA, RB;
     ffmat FA, FB;  // float-float rotation matrices
+    bool haveFF;   // FA/FB valid
     float3 posA, posB;
 };
 
@@ -151,7 +154,9 @@ __device__ __forceinline__ bool axis_f32(const PairCtx& c, const b3::ShapesDev& 
         if (!(fabsf(cr.x) > 1e-6f || fabsf(cr.y) > 1e-6f || fabsf(cr.z) > 1e-6f)) return false;
         const float cl = length(cr);
         n = cr * (1.f / cl);
-        err = delta * (1.f + 1.f / cl);
+        // direction error of the normalised FP32 cross product is ~ulp/cl;
+        // its depth error scales with the projected extents (delta / 1e-6)
+        err = delta + 0.3f * delta / cl;
     }
     if (dot(D, n) < 0.f) n = -n;
     float mn0, mx0, mn1, mx1;
@@ -166,7 +171,7 @@ __device__ __forceinline__ bool axis_f32(const PairCtx& c, const b3::ShapesDev& 
 
 // float-float evaluation of one axis: oriented axis and depth; false if
 // the edge pair is degenerate
-__device__ bool axis_ff(const PairCtx& c, const b3::ShapesDev& S, int idx, ff3 Dff, ff3& n, ff& d, bool& isFace) {
+__device__ __noinline__ bool axis_ff(const PairCtx& c, const b3::ShapesDev& S, int idx, ff3 Dff, ff3& n, ff& d, bool& isFace) {
     const b3ConvexPolyhedron& pa = *c.pa;
     const b3ConvexPolyhedron& pb = *c.pb;
     const int FA = pa.numFaces, FB = pb.numFaces;
@@ -215,7 +220,7 @@ __device__ bool axis_ff(const PairCtx& c, const b3::ShapesDev& S, int idx, ff3 D
 // FP32 sweep over all axes by the warp, then float-float refinement of every
 // axis whose FP32 depth is within delta of the minimum. Returns false if a
 // face axis separates or no axis exists.
-__device__ bool find_axis(const PairCtx& c, const b3::ShapesDev& S, WarpScratch& W, ff3& sep, int* ovfCounter) {
+__device__ __noinline__ bool find_axis(PairCtx& c, const b3::ShapesDev& S, WarpScratch& W, ff3& sep, int* ovfCounter) {
     const int lane = threadIdx.x & 31;
     const b3ConvexPolyhedron& pa = *c.pa;
     const b3ConvexPolyhedron& pb = *c.pb;
@@ -243,35 +248,47 @@ __device__ bool find_axis(const PairCtx& c, const b3::ShapesDev& S, WarpScratch&
     bool ambOverflow = false;
     float sepMin = FLT_MAX;
     float upper = FLT_MAX;  // min over axes of (d + err): bounds the true minimum depth
-    for (int idx = lane; idx < nAxes; idx += 32) {
-        float3 n;
-        float d, err;
-        bool isFace;
-        if (!axis_f32(c, S, idx, D, rel, delta, n, d, err, isFace)) continue;
-        if (isFace) {
-            sepMin = fminf(sepMin, d);
-            if (fabsf(d) <= delta) {
-                if (amb[0] == kNone) amb[0] = idx;
-                else if (amb[1] == kNone) amb[1] = idx;
-                else ambOverflow = true;
+    // faces of A and B first; a separating face axis ends the search before
+    // the edge pairs, as the reference returns early (P2/sat.cl:527-530)
+    for (int pass = 0; pass < 2; ++pass) {
+        const int i0 = pass == 0 ? 0 : nFace;
+        const int i1 = pass == 0 ? nFace : nAxes;
+        for (int idx = i0 + lane; idx < i1; idx += 32) {
+            float3 n;
+            float d, err;
+            bool isFace;
+            if (!axis_f32(c, S, idx, D, rel, delta, n, d, err, isFace)) continue;
+            if (isFace) {
+                sepMin = fminf(sepMin, d);
+                if (fabsf(d) <= delta) {
+                    if (amb[0] == kNone) amb[0] = idx;
+                    else if (amb[1] == kNone) amb[1] = idx;
+                    else ambOverflow = true;
+                }
+            }
+            upper = fminf(upper, d + err);
+            const float lo = d - err;  // lower bound of this axis' depth
+            if (!(lo < kd[kKeep - 1])) continue;  // also drops NaN
+            // insertion into the lane's sorted keep list (indices increase)
+            float cd = lo;
+            int ci = idx;
+    #pragma unroll
+            for (int k = 0; k < kKeep; ++k) {
+                if (cd < kd[k]) {
+                    const float td = kd[k];
+                    const int ti = ki[k];
+                    kd[k] = cd;
+                    ki[k] = ci;
+                    cd = td;
+                    ci = ti;
+                }
             }
         }
-        upper = fminf(upper, d + err);
-        const float lo = d - err;  // lower bound of this axis' depth
-        if (!(lo < kd[kKeep - 1])) continue;  // also drops NaN
-        // insertion into the lane's sorted keep list (indices increase)
-        float cd = lo;
-        int ci = idx;
-#pragma unroll
-        for (int k = 0; k < kKeep; ++k) {
-            if (cd < kd[k]) {
-                const float td = kd[k];
-                const int ti = ki[k];
-                kd[k] = cd;
-                ki[k] = ci;
-                cd = td;
-                ci = ti;
-            }
+        if (pass == 0) {
+            float sm0 = sepMin;
+            int dz = 0;
+            warp_argmin(sm0, dz);
+            if (sm0 < -delta) return false;
         }
     }
     // clearly separated by a face axis
@@ -317,7 +334,64 @@ __device__ bool find_axis(const PairCtx& c, const b3::ShapesDev& S, WarpScratch&
         }
     }
     __syncwarp();
-    // float-float refinement of the candidates
+    // A single well-conditioned winner needs no refinement: a face axis, or
+    // an edge axis with |e0 x e1| >= 0.01 (FP32 normal error < 1e-5), whose
+    // orientation test is not near zero.
+    if (count == 1) {
+        const int idx = W.cand[0];
+        float3 n;
+        float d, err;
+        bool isFace;
+        if (axis_f32(c, S, idx, D, rel, delta, n, d, err, isFace) && err <= 31.f * delta &&
+            fabsf(dot(D, n)) > 1e-5f * (length(D) + 1e-3f)) {
+            if (dot(-D, n) > 0.f) n = -n;
+            sep = mk3(n.x, n.y, n.z);
+            c.haveFF = false;
+            return true;
+        }
+    }
+    // Several candidates that are the same direction within 1e-5 (parallel
+    // faces, or edge pairs spanning a face's normal): whichever the exact
+    // arithmetic picks, the normal agrees within tolerance and the clip
+    // faces follow from it, so the FP32 first minimum is kept. Candidates
+    // that decide separation (|depth| near zero) still go to float-float.
+    if (count <= 32) {
+        float3 n = make_float3(0.f, 0.f, 0.f);
+        float d = FLT_MAX, err = 0.f;
+        bool isFace = false, ok = true;
+        int myIdx = kNone;
+        if (lane < count) {
+            myIdx = W.cand[lane];
+            ok = axis_f32(c, S, myIdx, D, rel, delta, n, d, err, isFace) && err <= 31.f * delta &&
+                 !(isFace && fabsf(d) <= delta) && fabsf(dot(D, n)) > 1e-5f * (length(D) + 1e-3f);
+            if (!ok) myIdx = kNone;
+        }
+        const float3 n0 = make_float3(__shfl_sync(0xffffffffu, n.x, 0), __shfl_sync(0xffffffffu, n.y, 0),
+                                      __shfl_sync(0xffffffffu, n.z, 0));
+        if (lane < count && ok) {
+            const float3 dd = n - n0;
+            if (fmaxf(fabsf(dd.x), fmaxf(fabsf(dd.y), fabsf(dd.z))) > 1e-5f) ok = false;
+        }
+        if (__all_sync(0xffffffffu, ok)) {
+            float bd = (lane < count) ? d : FLT_MAX;
+            int bidx = (lane < count) ? myIdx : kNone;
+            warp_argmin(bd, bidx);
+            const unsigned who = __ballot_sync(0xffffffffu, lane < count && myIdx == bidx);
+            const int src = __ffs(who) - 1;
+            float3 w = make_float3(__shfl_sync(0xffffffffu, n.x, src), __shfl_sync(0xffffffffu, n.y, src),
+                                   __shfl_sync(0xffffffffu, n.z, src));
+            if (dot(-D, w) > 0.f) w = -w;
+            sep = mk3(w.x, w.y, w.z);
+            c.haveFF = false;
+            return true;
+        }
+    }
+    if (lane == 0) ++W.refinedAxes;
+    // float-float refinement of the candidates (matrices built only for
+    // pairs that got this far)
+    c.FA = quat_mat(c.qA);
+    c.FB = quat_mat(c.qB);
+    c.haveFF = true;
     const ff3 lcAw = mrot(c.FA, make_float3(lcA.x, lcA.y, lcA.z));
     const ff3 lcBw = mrot(c.FB, make_float3(lcB.x, lcB.y, lcB.z));
     const ff3 Dff = sub3(add3(lcAw, mk3(c.posA.x, c.posA.y, c.posA.z)), add3(lcBw, mk3(c.posB.x, c.posB.y, c.posB.z)));
@@ -356,19 +430,34 @@ __device__ bool find_axis(const PairCtx& c, const b3::ShapesDev& S, WarpScratch&
 
 // One Sutherland-Hodgman step in float-float (clipFace,
 // satClipHullContacts.cl:303-351), one polygon vertex per lane; output
-// order identical to the sequential loop.
-__device__ int clip_poly_ff(const FfVert* in, int nin, ff3 pn, ff eq, FfVert* out, int* ovf) {
+// order identical to the sequential loop. Each lane evaluates its own
+// vertex's plane distance once; the edge start takes it from the previous
+// lane.
+__device__ __noinline__ int clip_poly_ff(const FfVert* in, int nin, const FfVert& plane, FfVert* out, int* ovf) {
     const int lane = threadIdx.x & 31;
+    const ff3 pn = vget(plane);
+    const ff eq = wget(plane);
     int total = 0;
     for (int base = 0; base < nin; base += 32) {
         const int ve = base + lane;
+        const int sv = ve == 0 ? nin - 1 : ve - 1;
+        ff3 e = mk3(0.f, 0.f, 0.f), s = e;
+        ff de = mk(0.f);
+        if (ve < nin) {
+            e = vget(in[ve]);
+            s = vget(in[sv]);
+            de = add(dot3(pn, e), eq);
+        }
+        // distance of the edge start: previous lane's, or recomputed at the
+        // chunk boundary and for the wrap-around edge of a long polygon
+        ff ds;
+        ds.hi = __shfl_up_sync(0xffffffffu, de.hi, 1);
+        ds.lo = __shfl_up_sync(0xffffffffu, de.lo, 1);
+        const bool own = lane == 0;
+        if (ve < nin && own) ds = add(dot3(pn, s), eq);
         int cnt = 0;
         ff3 o0 = mk3(0.f, 0.f, 0.f), o1 = o0;
         if (ve < nin) {
-            const ff3 s = vget(in[ve == 0 ? nin - 1 : ve - 1]);
-            const ff3 e = vget(in[ve]);
-            const ff ds = add(dot3(pn, s), eq);
-            const ff de = add(dot3(pn, e), eq);
             const bool sNeg = ds.hi < 0.f, eNeg = de.hi < 0.f;
             if (sNeg || eNeg) {
                 if (sNeg && eNeg) {
@@ -404,11 +493,203 @@ __device__ int clip_poly_ff(const FfVert* in, int nin, ff3 pn, ff eq, FfVert* ou
     return min(total, kMaxPoly);
 }
 
+// ---------------------------------------------------------------------------
+// FP32 fast path with error bounds. Clipping runs in a frame centred on body
+// A (magnitudes of about the hull size, not the world), planes are kept as
+// (normal, point) so no large plane constant cancels, and every decision or
+// intersection whose FP32 error bound exceeds ~1e-6 m marks the pair for the
+// float-float path.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void put_f32(FfVert& v, float3 p, float w) {
+    v = {p.x, 0.f, p.y, 0.f, p.z, 0.f, w, 0.f};
+}
+__device__ __forceinline__ float3 get_f32(const FfVert& v) { return make_float3(v.xh, v.yh, v.zh); }
+
+__device__ __noinline__ int clip_poly_f32(const FfVert* in, int nin, float3 pn, float3 ap, FfVert* out, bool* bad,
+                                          int* ovf) {
+    const int lane = threadIdx.x & 31;
+    const float pnl = length(pn);
+    const float apl = length(ap);
+    int total = 0;
+    for (int base = 0; base < nin; base += 32) {
+        const int ve = base + lane;
+        int cnt = 0;
+        float3 o0 = make_float3(0.f, 0.f, 0.f), o1 = o0;
+        if (ve < nin) {
+            const float3 sv = get_f32(in[ve == 0 ? nin - 1 : ve - 1]);
+            const float3 ev = get_f32(in[ve]);
+            const float ds = dot(pn, sv - ap);
+            const float de = dot(pn, ev - ap);
+            // FP32 error of ds/de: a few ulps of the magnitudes involved
+            const float es = 2.5e-7f * pnl * (1.f + length(sv) + apl);
+            const float ee = 2.5e-7f * pnl * (1.f + length(ev) + apl);
+            if (fabsf(ds) <= es || fabsf(de) <= ee) *bad = true;
+            const bool sNeg = ds < 0.f, eNeg = de < 0.f;
+            if (sNeg || eNeg) {
+                if (sNeg && eNeg) {
+                    o0 = ev;
+                    cnt = 1;
+                } else {
+                    const float den = ds - de;
+                    const float t = ds * 1.f / den;
+                    if (length(ev - sv) * (es + ee) > 2e-6f * fabsf(den)) *bad = true;
+                    o0 = sv + (ev - sv) * t;
+                    cnt = 1;
+                    if (!sNeg) {
+                        o1 = ev;
+                        cnt = 2;
+                    }
+                }
+            }
+        }
+        int x = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        const int pos = total + x - cnt;
+        if (cnt >= 1) {
+            if (pos < kMaxPoly) put_f32(out[pos], o0, 0.f); else atomicAdd(ovf, 1);
+        }
+        if (cnt == 2) {
+            if (pos + 1 < kMaxPoly) put_f32(out[pos + 1], o1, 0.f); else atomicAdd(ovf, 1);
+        }
+        total += __shfl_sync(0xffffffffu, x, 31);
+    }
+    __syncwarp();
+    return min(total, kMaxPoly);
+}
+
+__device__ __noinline__ int clip_f32(const PairCtx& c, const b3::ShapesDev& S, const NpParams& P, int ai, int bi,
+                                     WarpScratch& W, int* outBuf, bool* doubt, int* ovf) {
+    const int lane = threadIdx.x & 31;
+    const b3ConvexPolyhedron& pa = *c.pa;
+    const b3ConvexPolyhedron& pb = *c.pb;
+    if (ai == kNone || bi == kNone) return 0;
+    const b3Face fB = S.faces[pb.faceOffset + bi];
+    const b3Face fA = S.faces[pa.faceOffset + ai];
+    const float3 rel = c.posB - c.posA;
+    int nIn = min(fB.numIndices, kMaxPoly);
+    for (int k = lane; k < nIn; k += 32) {
+        const float4 v = __ldg(&S.verts[pb.vertexOffset + S.indices[fB.indexOffset + k]]);
+        put_f32(W.poly[0][k], mul(c.RB, f3(v)) + rel, 0.f);
+    }
+    __syncwarp();
+    bool bad = false;
+    int cur = 0;
+    const float3 nAw = mul(c.RA, make_float3(fA.plane[0], fA.plane[1], fA.plane[2]));
+    const int nvA = fA.numIndices;
+    for (int e0 = 0; e0 < nvA; ++e0) {
+        const float4 a = __ldg(&S.verts[pa.vertexOffset + S.indices[fA.indexOffset + e0]]);
+        const float4 b = __ldg(&S.verts[pa.vertexOffset + S.indices[fA.indexOffset + (e0 + 1) % nvA]]);
+        const float3 we = mul(c.RA, make_float3(a.x - b.x, a.y - b.y, a.z - b.z));
+        const float3 pn = -cross(we, nAw);
+        const float3 ap = mul(c.RA, f3(a));
+        nIn = clip_poly_f32(W.poly[cur], nIn, pn, ap, W.poly[cur ^ 1], &bad, ovf);
+        cur ^= 1;
+    }
+    // keep points behind the witness face; in A's frame the plane constant is
+    // the face's own (clipFaceAgainstHull :433-452)
+    int total = 0;
+    for (int base = 0; base < nIn; base += 32) {
+        const int k = base + lane;
+        bool keep = false;
+        float3 p = make_float3(0.f, 0.f, 0.f);
+        float depth = 0.f;
+        if (k < nIn) {
+            p = get_f32(W.poly[cur][k]);
+            depth = dot(nAw, p) + fA.plane[3];
+            if (fabsf(depth - P.maxDist) <= 5e-7f * (1.f + length(p))) bad = true;
+            if (depth <= P.minDist) depth = P.minDist;
+            keep = depth <= P.maxDist;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        const int pos = total + __popc(m & b3dev::lanemask_lt());
+        if (keep) put_f32(W.poly[cur ^ 1][pos], p + c.posA, depth);
+        total += __popc(m);
+    }
+    __syncwarp();
+    *doubt = __any_sync(0xffffffffu, bad);
+    *outBuf = cur ^ 1;
+    return total;
+}
+
+// count of lanes' values within gap of the warp minimum (near-tie test)
+__device__ __forceinline__ int near_count(float best, float v, bool valid, float gap) {
+    int c = (valid && v <= best + gap) ? 1 : 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    return c;
+}
+
+// FP32 extractManifoldSequentialGlobal; *tie set when an arg-min is within
+// FP32 error of another candidate or of the FLT_MIN threshold.
+__device__ __noinline__ int4 reduce_f32(const FfVert* p, int n, float3 nearNormal, bool* tie) {
+    const int lane = threadIdx.x & 31;
+    const float3 o = get_f32(p[0]);  // subtract a point first: world magnitudes cancel
+    float3 s = make_float3(0.f, 0.f, 0.f);
+    for (int k = lane; k < n; k += 32) s += get_f32(p[k]) - o;
+#pragma unroll
+    for (int q = 16; q > 0; q >>= 1) {
+        s.x += __shfl_xor_sync(0xffffffffu, s.x, q);
+        s.y += __shfl_xor_sync(0xffffffffu, s.y, q);
+        s.z += __shfl_xor_sync(0xffffffffu, s.z, q);
+    }
+    const float3 cr = s * (1.f / (float)n);  // centre relative to o
+    const float3 aV = -cr;
+    float3 u = cross(nearNormal, aV);
+    float3 v = cross(nearNormal, u);
+    u = normalize(u);
+    v = normalize(v);
+    float fw[2], fu[2], fv[2];
+    float mw = FLT_MAX, f0 = FLT_MIN, f1 = FLT_MIN, f2 = FLT_MIN, f3v = FLT_MIN;
+    int iw = kNone, i0 = kNone, i1 = kNone, i2 = kNone, i3 = kNone;
+    for (int j = 0; j < 2; ++j) {
+        const int k = lane + 32 * j;
+        fw[j] = FLT_MAX; fu[j] = 0.f; fv[j] = 0.f;
+        if (k < n) {
+            const float3 r = (get_f32(p[k]) - o) - cr;
+            fw[j] = p[k].wh;
+            fu[j] = dot(u, r);
+            fv[j] = dot(v, r);
+            if (fw[j] < mw) { mw = fw[j]; iw = k; }
+            if (fu[j] < f0) { f0 = fu[j]; i0 = k; }
+            if (-fu[j] < f1) { f1 = -fu[j]; i1 = k; }
+            if (fv[j] < f2) { f2 = fv[j]; i2 = k; }
+            if (-fv[j] < f3v) { f3v = -fv[j]; i3 = k; }
+        }
+    }
+    warp_argmin(mw, iw);
+    warp_argmin(f0, i0);
+    warp_argmin(f1, i1);
+    warp_argmin(f2, i2);
+    warp_argmin(f3v, i3);
+    const float gap = 2e-6f, gapw = 1e-6f;
+    int worst = 0;
+    for (int j = 0; j < 2; ++j) {
+        const bool ok = lane + 32 * j < n;
+        worst = max(worst, near_count(mw, fw[j], ok, gapw));
+        worst = max(worst, near_count(f0, fu[j], ok, gap));
+        worst = max(worst, near_count(f1, -fu[j], ok, gap));
+        worst = max(worst, near_count(f2, fv[j], ok, gap));
+        worst = max(worst, near_count(f3v, -fv[j], ok, gap));
+    }
+    // values near the FLT_MIN start (i.e. near zero) are ambiguous too
+    *tie = worst > 1 || fabsf(f0) <= gap || fabsf(f1) <= gap || fabsf(f2) <= gap || fabsf(f3v) <= gap;
+    int4 idx = make_int4(i0 == kNone ? 0 : i0, i1 == kNone ? 1 : i1, i2 == kNone ? 2 : i2, i3 == kNone ? 3 : i3);
+    const int minIndex = iw == kNone ? -1 : iw;
+    if (idx.x != minIndex && idx.y != minIndex && idx.z != minIndex && idx.w != minIndex) idx.x = minIndex;
+    return idx;
+}
+
 // First face minimising sign * dot(R n_f, sep) (the reference's strict
 // comparisons: the first extreme face wins). FP32 sweep, then faces within
 // a small window of the FP32 extreme are re-ranked in float-float.
-__device__ int select_face(const b3::ShapesDev& S, const b3ConvexPolyhedron& h, const Mat3& R, const ffmat& F,
-                           float3 sepf, ff3 sep, float sign) {
+__device__ __noinline__ int select_face(const b3::ShapesDev& S, PairCtx& c, bool sideA, float3 sepf, ff3 sep,
+                                        float sign) {
+    const b3ConvexPolyhedron& h = sideA ? *c.pa : *c.pb;
+    const Mat3& R = sideA ? c.RA : c.RB;
     const int lane = threadIdx.x & 31;
     float bv = FLT_MAX;
     int bi = kNone;
@@ -422,6 +703,21 @@ __device__ int select_face(const b3::ShapesDev& S, const b3ConvexPolyhedron& h, 
     warp_argmin(wv, wi);
     if (wi == kNone) return kNone;
     const float lim = wv + 4e-6f;
+    // near-ties only: count faces inside the window
+    int inWin = 0;
+    for (int f = lane; f < h.numFaces; f += 32) {
+        const float4 pl = __ldg((const float4*)&S.faces[h.faceOffset + f].plane[0]);
+        if (sign * dot(mul(R, make_float3(pl.x, pl.y, pl.z)), sepf) <= lim) ++inWin;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) inWin += __shfl_xor_sync(0xffffffffu, inWin, o);
+    if (inWin <= 1) return wi;
+    if (!c.haveFF) {
+        c.FA = quat_mat(c.qA);
+        c.FB = quat_mat(c.qB);
+        c.haveFF = true;
+    }
+    const ffmat& F = sideA ? c.FA : c.FB;
     ff rv = mk(FLT_MAX);
     int ri = kNone;
     for (int f = lane; f < h.numFaces; f += 32) {
@@ -439,15 +735,16 @@ __device__ int select_face(const b3::ShapesDev& S, const b3ConvexPolyhedron& h, 
 // clipHullAgainstHull (satClipHullContacts.cl:556-611 + clipFaceAgainstHull
 // :353-452) in float-float; kept points (x, y, z, depth) end in
 // W.poly[*outBuf].
-__device__ int clip_hull_hull(const PairCtx& c, const b3::ShapesDev& S, const NpParams& P, ff3 sep,
-                              WarpScratch& W, int* outBuf, int* ovf) {
+__device__ __noinline__ int clip_hull_hull(PairCtx& c, const b3::ShapesDev& S, const NpParams& P, ff3 sep,
+                              int ai, int bi, WarpScratch& W, int* outBuf, int* ovf) {
+    if (!c.haveFF) {
+        c.FA = quat_mat(c.qA);
+        c.FB = quat_mat(c.qB);
+        c.haveFF = true;
+    }
     const int lane = threadIdx.x & 31;
     const b3ConvexPolyhedron& pa = *c.pa;
     const b3ConvexPolyhedron& pb = *c.pb;
-    const float3 sepf = to_f3(sep);
-    // incident face of B: max dot(nB, sep); reference face of A: min dot(nA, sep)
-    const int bi = select_face(S, pb, c.RB, c.FB, sepf, sep, -1.f);
-    const int ai = select_face(S, pa, c.RA, c.FA, sepf, sep, 1.f);
     if (ai == kNone || bi == kNone) return 0;
     const b3Face fB = S.faces[pb.faceOffset + bi];
     const b3Face fA = S.faces[pa.faceOffset + ai];
@@ -461,10 +758,11 @@ __device__ int clip_hull_hull(const PairCtx& c, const b3::ShapesDev& S, const Np
     __syncwarp();
     int cur = 0;
     const ff3 nAw = mrot(c.FA, make_float3(fA.plane[0], fA.plane[1], fA.plane[2]));
-    const int nvA = fA.numIndices;
-    for (int e0 = 0; e0 < nvA; ++e0) {
+    const int nvA = min(fA.numIndices, kMaxPoly);
+    // side planes of the reference face, one per lane
+    for (int e0 = lane; e0 < nvA; e0 += 32) {
         const float4 a = __ldg(&S.verts[pa.vertexOffset + S.indices[fA.indexOffset + e0]]);
-        const float4 b = __ldg(&S.verts[pa.vertexOffset + S.indices[fA.indexOffset + (e0 + 1) % nvA]]);
+        const float4 b = __ldg(&S.verts[pa.vertexOffset + S.indices[fA.indexOffset + (e0 + 1) % fA.numIndices]]);
         // a - b of two FP32 vertices is exact in float-float
         const ff3 edge = sub3(mk3(a.x, a.y, a.z), mk3(b.x, b.y, b.z));
         const ff3 we{add(add(mul(c.FA.m[0][0], edge.x), mul(c.FA.m[0][1], edge.y)), mul(c.FA.m[0][2], edge.z)),
@@ -472,8 +770,11 @@ __device__ int clip_hull_hull(const PairCtx& c, const b3::ShapesDev& S, const Np
                      add(add(mul(c.FA.m[2][0], edge.x), mul(c.FA.m[2][1], edge.y)), mul(c.FA.m[2][2], edge.z))};
         const ff3 pn = neg3(cross3(we, nAw));
         const ff3 wa = add3(mrot(c.FA, make_float3(a.x, a.y, a.z)), posA);
-        const ff eq = neg(dot3(wa, pn));
-        nIn = clip_poly_ff(W.poly[cur], nIn, pn, eq, W.poly[cur ^ 1], ovf);
+        W.planes[e0] = vput(pn, neg(dot3(wa, pn)));
+    }
+    __syncwarp();
+    for (int e0 = 0; e0 < nvA; ++e0) {
+        nIn = clip_poly_ff(W.poly[cur], nIn, W.planes[e0], W.poly[cur ^ 1], ovf);
         cur ^= 1;
     }
     // keep points behind the witness face (clipFaceAgainstHull :433-452)
@@ -503,7 +804,7 @@ __device__ int clip_hull_hull(const PairCtx& c, const b3::ShapesDev& S, const Np
 
 // extractManifoldSequentialGlobal (P2/satClipHullContacts.cl:678-770) over
 // n > 4 float-float points; returns the 4 chosen indices.
-__device__ int4 reduce_manifold(const FfVert* p, int n, ff3 nearNormal) {
+__device__ __noinline__ int4 reduce_manifold(const FfVert* p, int n, ff3 nearNormal) {
     const int lane = threadIdx.x & 31;
     // centre in point order (sequential float-float sum on every lane)
     ff3 s = mk3(0.f, 0.f, 0.f);
@@ -546,6 +847,11 @@ k_narrowphase(const int2* __restrict__ pairs, const int32_t* __restrict__ numPai
     const int lane = threadIdx.x & 31;
     WarpScratch& W = reinterpret_cast<WarpScratch*>(np_smem)[threadIdx.x >> 5];
     const int numPairs = *numPairsDev;
+    if (lane == 0) {
+        W.refinedAxes = 0;
+        W.refinedClips = 0;
+    }
+    __syncwarp();
     for (;;) {
         int chunk = 0;
         if (lane == 0) chunk = atomicAdd(workCounter, kChunk);
@@ -571,12 +877,21 @@ k_narrowphase(const int2* __restrict__ pairs, const int32_t* __restrict__ numPai
                 c.qB = Bd.quat[c.B];
                 c.RA = quat_to_mat(c.qA);
                 c.RB = quat_to_mat(c.qB);
-                c.FA = quat_mat(c.qA);
-                c.FB = quat_mat(c.qB);
                 c.posA = f3(Bd.pos[c.A]);
                 c.posB = f3(Bd.pos[c.B]);
-                if (find_axis(c, S, W, sep, &counters->clipOverflow))
-                    nOut = clip_hull_hull(c, S, P, sep, W, &buf, &counters->clipOverflow);
+                c.haveFF = false;
+                if (find_axis(c, S, W, sep, &counters->clipOverflow)) {
+                    const float3 sepf = to_f3(sep);
+                    // incident face of B: max dot(nB, sep); reference face of A: min dot(nA, sep)
+                    const int bi = select_face(S, c, false, sepf, sep, -1.f);
+                    const int ai = select_face(S, c, true, sepf, sep, 1.f);
+                    bool doubt = false;
+                    nOut = clip_f32(c, S, P, ai, bi, W, &buf, &doubt, &counters->clipOverflow);
+                    if (doubt) {
+                        if (lane == 0) ++W.refinedClips;
+                        nOut = clip_hull_hull(c, S, P, sep, ai, bi, W, &buf, &counters->clipOverflow);
+                    }
+                }
             }
             if (nOut > 0) {
                 const FfVert* pts = W.poly[buf];
@@ -584,7 +899,9 @@ k_narrowphase(const int2* __restrict__ pairs, const int32_t* __restrict__ numPai
                 int4 idx = make_int4(0, 1, 2, 3);
                 int nRed = nOut;
                 if (nOut > 4) {
-                    idx = reduce_manifold(pts, nOut, nrm);
+                    bool tie = false;
+                    idx = reduce_f32(pts, min(nOut, kMaxPoly), to_f3(nrm), &tie);
+                    if (tie) idx = reduce_manifold(pts, nOut, nrm);
                     nRed = 4;
                 }
                 b3Contact4* out = &contacts[p];
@@ -610,6 +927,10 @@ k_narrowphase(const int2* __restrict__ pairs, const int32_t* __restrict__ numPai
             }
             __syncwarp();
         }
+    }
+    if (lane == 0) {
+        if (W.refinedAxes) atomicAdd(&counters->refinedAxes, W.refinedAxes);
+        if (W.refinedClips) atomicAdd(&counters->refinedClips, W.refinedClips);
     }
 }
 

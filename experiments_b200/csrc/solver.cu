@@ -38,6 +38,7 @@
 #include "b3_math.cuh"
 #include "b3_world.h"
 
+#include <algorithm>
 #include <cfloat>
 
 using namespace b3m;
@@ -308,98 +309,92 @@ __device__ __forceinline__ void solve_row(const float4 r0, const float4 r1, floa
     dwB += mulv(iiB, t2) * delta;
 }
 
-__device__ void manifold_phase(const SolverView& V, int M, bool friction) {
+// Averaged delta velocity of body b over its copies in buffer buf
+// (averageVelocities, P2/btPgsJacobiSolver.cpp:1683-1720): copies in
+// manifold order, sum then multiply by 1/count.
+__device__ __forceinline__ void body_average(const SolverView& V, int b, int buf, float3& lin, float3& ang) {
+    const uint32_t s = V.incStart[b], e = V.incEnd[b];
+    float3 sl = make_float3(0.f, 0.f, 0.f), sa = sl;
+    for (uint32_t i = s; i < e; ++i) {
+        const uint32_t cid = V.incVals[i];
+        const size_t at = (size_t)(buf * 2 + (int)(cid & 1u)) * V.cap + (cid >> 1);
+        sl += f3(V.copyLin[at]);
+        sa += f3(V.copyAng[at]);
+    }
+    const float factor = 1.f / (float)(e - s);
+    lin = sl * factor;
+    ang = sa * factor;
+}
+
+// One phase for every manifold: start each copy from its body's average of
+// the previous phase (zero in the first phase), solve the manifold's normal
+// or friction rows in order, store both copies in buffer outBuf. A copy of a
+// manifold without rows keeps the average, as in the reference.
+__device__ void manifold_phase(const SolverView& V, int M, bool friction, bool first, int inBuf, int outBuf) {
     for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
         const float4 h0 = R(V, 0, m);
         const int nRows = __float_as_int(h0.z);
-        if (nRows == 0) continue;
         const int A = __float_as_int(h0.x), B = __float_as_int(h0.y);
         const int dyn = __float_as_int(h0.w);
-        const float4 h1 = R(V, 1, m);
-        const float4 h2 = R(V, 2, m);
-        const float4 h3 = R(V, 3, m);
-        const float imA = h1.x, imB = h1.y, mu = h1.z;
-        const float3 iiA = f3(h2), iiB = f3(h3);
         float3 dvA = make_float3(0.f, 0.f, 0.f), dwA = dvA, dvB = dvA, dwB = dvA;
-        if (dyn & 1) { dvA = f3(V.avgLin[A]); dwA = f3(V.avgAng[A]); }
-        if (dyn & 2) { dvB = f3(V.avgLin[B]); dwB = f3(V.avgAng[B]); }
-        if (!friction) {
-            for (int j = 0; j < nRows; ++j) {
-                const int s = kNormal0 + 3 * j;
-                const float4 r0 = R(V, s, m), r1 = R(V, s + 1, m);
-                float4 r2 = R(V, s + 2, m);
-                solve_row(r0, r1, r2, 0.f, 1e10f, imA, imB, iiA, iiB, dvA, dwA, dvB, dwB);
-                R(V, s + 2, m).w = r2.w;
-            }
-        } else {
-            for (int j = 0; j < nRows; ++j) {
-                const float total = R(V, kNormal0 + 3 * j + 2, m).w;
-                if (!(total > 0.f)) continue;
-                const float lim = mu * total;
-                for (int q = 0; q < 2; ++q) {
-                    const int s = kFric0 + 3 * (2 * j + q);
+        if (!first) {
+            if (dyn & 1) body_average(V, A, inBuf, dvA, dwA);
+            if (dyn & 2) body_average(V, B, inBuf, dvB, dwB);
+        }
+        if (nRows > 0) {
+            const float4 h1 = R(V, 1, m);
+            const float4 h2 = R(V, 2, m);
+            const float4 h3 = R(V, 3, m);
+            const float imA = h1.x, imB = h1.y, mu = h1.z;
+            const float3 iiA = f3(h2), iiB = f3(h3);
+            if (!friction) {
+                for (int j = 0; j < nRows; ++j) {
+                    const int s = kNormal0 + 3 * j;
                     const float4 r0 = R(V, s, m), r1 = R(V, s + 1, m);
                     float4 r2 = R(V, s + 2, m);
-                    solve_row(r0, r1, r2, -lim, lim, imA, imB, iiA, iiB, dvA, dwA, dvB, dwB);
+                    solve_row(r0, r1, r2, 0.f, 1e10f, imA, imB, iiA, iiB, dvA, dwA, dvB, dwB);
                     R(V, s + 2, m).w = r2.w;
+                }
+            } else {
+                for (int j = 0; j < nRows; ++j) {
+                    const float total = R(V, kNormal0 + 3 * j + 2, m).w;
+                    if (!(total > 0.f)) continue;
+                    const float lim = mu * total;
+                    for (int q = 0; q < 2; ++q) {
+                        const int s = kFric0 + 3 * (2 * j + q);
+                        const float4 r0 = R(V, s, m), r1 = R(V, s + 1, m);
+                        float4 r2 = R(V, s + 2, m);
+                        solve_row(r0, r1, r2, -lim, lim, imA, imB, iiA, iiB, dvA, dwA, dvB, dwB);
+                        R(V, s + 2, m).w = r2.w;
+                    }
                 }
             }
         }
         if (dyn & 1) {
-            V.copyLin[m] = f4(dvA);
-            V.copyAng[m] = f4(dwA);
+            const size_t at = (size_t)(outBuf * 2 + 0) * V.cap + m;
+            V.copyLin[at] = f4(dvA);
+            V.copyAng[at] = f4(dwA);
         }
         if (dyn & 2) {
-            V.copyLin[V.cap + m] = f4(dvB);
-            V.copyAng[V.cap + m] = f4(dwB);
+            const size_t at = (size_t)(outBuf * 2 + 1) * V.cap + m;
+            V.copyLin[at] = f4(dvB);
+            V.copyAng[at] = f4(dwB);
         }
     }
 }
 
-// Copies whose manifold had no rows keep the body's average.
-__device__ void average_phase(const SolverView& V) {
-    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < V.numBodies; b += gridDim.x * blockDim.x) {
-        const uint32_t s = V.incStart[b], e = V.incEnd[b];
-        if (e <= s) continue;
-        const float4 prevL = V.avgLin[b], prevA = V.avgAng[b];
-        float3 sl = make_float3(0.f, 0.f, 0.f), sa = sl;
-        for (uint32_t i = s; i < e; ++i) {
-            const uint32_t cid = V.incVals[i];
-            const int m = (int)(cid >> 1), side = (int)(cid & 1u);
-            const int nRows = __float_as_int(R(V, 0, m).z);
-            if (nRows == 0) {
-                sl += f3(prevL);
-                sa += f3(prevA);
-            } else {
-                sl += f3(V.copyLin[(size_t)side * V.cap + m]);
-                sa += f3(V.copyAng[(size_t)side * V.cap + m]);
-            }
-        }
-        const float factor = 1.f / (float)(e - s);
-        V.avgLin[b] = f4(sl * factor);
-        V.avgAng[b] = f4(sa * factor);
-    }
-}
-
+// Phases p = 0 .. 2*iterations-1 alternate normal (even) and friction (odd)
+// rows; the averaging of the reference happens at the start of the next
+// phase from the double-buffered copies, so phases are separated by one
+// bounded grid barrier each.
 __global__ void __launch_bounds__(256)
 k_jacobi(SolverView V, int iterations, uint32_t* bar, int32_t* err, b3Counters* counters) {
     const int M = *V.numManifolds;
     const uint32_t nb = gridDim.x;
-    // zero the averaged deltas
-    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < V.numBodies; b += gridDim.x * blockDim.x) {
-        V.avgLin[b] = make_float4(0.f, 0.f, 0.f, 0.f);
-        V.avgAng[b] = make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-    if (!grid_barrier(bar, bar + 1, nb, err, counters)) return;
-    for (int it = 0; it < iterations; ++it) {
-        manifold_phase(V, M, false);
-        if (!grid_barrier(bar, bar + 1, nb, err, counters)) return;
-        average_phase(V);
-        if (!grid_barrier(bar, bar + 1, nb, err, counters)) return;
-        manifold_phase(V, M, true);
-        if (!grid_barrier(bar, bar + 1, nb, err, counters)) return;
-        average_phase(V);
-        if (!grid_barrier(bar, bar + 1, nb, err, counters)) return;
+    const int phases = 2 * iterations;
+    for (int p = 0; p < phases; ++p) {
+        if (p > 0 && !grid_barrier(bar, bar + 1, nb, err, counters)) return;
+        manifold_phase(V, M, (p & 1) != 0, p == 0, (p - 1) & 1, p & 1);
     }
 }
 
@@ -412,22 +407,21 @@ struct IntegrateParams {
     float threshold;  // BT_GPU_ANGULAR_MOTION_THRESHOLD = 0.25 * pi
 };
 
-__global__ void k_integrate(b3::BodiesDev Bd, const float4* __restrict__ avgLin,
-                            const float4* __restrict__ avgAng, const uint32_t* __restrict__ incStart,
-                            const uint32_t* __restrict__ incEnd, IntegrateParams P, int applySolve) {
+__global__ void k_integrate(b3::BodiesDev Bd, SolverView V, int finalBuf, IntegrateParams P, int applySolve) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= Bd.n) return;
     if (Bd.invMass[i] == 0.f) return;
     float4 v = Bd.linVel[i];
     float4 w = Bd.angVel[i];
-    if (applySolve) {
-        const uint32_t k = incEnd[i] - incStart[i];
-        if (incEnd[i] > incStart[i]) {
-            const float4 sl = avgLin[i], sa = avgAng[i];
-            for (uint32_t c = 0; c < k; ++c) {
-                v.x += sl.x; v.y += sl.y; v.z += sl.z;
-                w.x += sa.x; w.y += sa.y; w.z += sa.z;
-            }
+    // solveGroupCacheFriendlyFinish (:1790-1803): each of the k copies adds
+    // sum/k of the last averaging to the body velocity
+    if (applySolve && V.incEnd[i] > V.incStart[i]) {
+        const uint32_t k = V.incEnd[i] - V.incStart[i];
+        float3 sl, sa;
+        body_average(V, i, finalBuf, sl, sa);
+        for (uint32_t c = 0; c < k; ++c) {
+            v.x += sl.x; v.y += sl.y; v.z += sl.z;
+            w.x += sa.x; w.y += sa.y; w.z += sa.z;
         }
     }
     v.w = 0.f;
@@ -532,7 +526,11 @@ int launch_solver(b3World_t* w, cudaStream_t st) {
     B3_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_jacobi, threads, 0));
     occ = occ < 1 ? 1 : occ;
     occ = occ > 4 ? 4 : occ;
-    const int grid = w->ctx->numSMs * occ;
+    // size the persistent grid to the expected manifold count (about 3 per
+    // body): fewer blocks make each grid barrier cheaper on small scenes
+    const long long est = std::min<long long>((long long)w->cfg.maxPairs, 3LL * (long long)w->bodies.size());
+    const int want = (int)std::max<long long>(1, (est + threads - 1) / threads);
+    const int grid = std::min(w->ctx->numSMs * occ, want);
     int iters = w->sim.iterations;
     uint32_t* bar = (uint32_t*)(w->d.scalars + S_BAR_COUNT);
     int32_t* err = w->d.scalars + S_ERR;
@@ -559,8 +557,9 @@ int launch_integrate(b3World_t* w, cudaStream_t st) {
     P.dt = w->sim.dt;
     P.damping = w->sim.angularDamping;
     P.threshold = 0.25f * 3.14159254f;
-    k_integrate<<<(N + 255) / 256, 256, 0, st>>>(w->bodiesDev(), w->d.avgLin, w->d.avgAng,
-                                                w->d.bodyIncStart, w->d.bodyIncEnd, P, 1);
+    const int iters = w->sim.iterations;
+    k_integrate<<<(N + 255) / 256, 256, 0, st>>>(w->bodiesDev(), solver_view(w), (2 * iters - 1) & 1, P,
+                                                iters > 0 ? 1 : 0);
     B3_CHECK_LAUNCH();
     return B3_OK;
 }

@@ -33,6 +33,8 @@ __global__ void k_step_begin(int32_t* scalars, b3Counters* counters) {
         counters->numContactPoints = 0;
         counters->numManifolds = 0;
         counters->numPairs = 0;
+        counters->refinedAxes = 0;
+        counters->refinedClips = 0;
     }
 }
 
@@ -408,8 +410,8 @@ static int ensure_capacity(b3World w) {
         B3_TRY(dalloc(d.incKeysAlt, 2 * c));
         B3_TRY(dalloc(d.incValsAlt, 2 * c));
         B3_TRY(dalloc(d.rows, 40 * c));
-        B3_TRY(dalloc(d.incLin, 2 * c));
-        B3_TRY(dalloc(d.incAng, 2 * c));
+        B3_TRY(dalloc(d.incLin, 4 * c));  // [2 phase buffers][2 sides][capacity]
+        B3_TRY(dalloc(d.incAng, 4 * c));
         const size_t tiles = (w->cfg.maxBodies + 127) / 128 + 16;
         d.scanScratchBytes = std::max(b3::scan_scratch_bytes(cap), tiles * 8 + 256);
         B3_TRY(dalloc((unsigned char*&)d.scanScratch, d.scanScratchBytes));

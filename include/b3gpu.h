@@ -123,6 +123,8 @@ typedef struct b3Counters {
     int32_t timeouts;            /* bounded device waits that gave up */
     int32_t clipOverflow;        /* clipped polygons truncated to 64 verts */
     int32_t steps;               /* steps executed since write_bodies */
+    int32_t refinedAxes;         /* pairs whose axis choice was re-ranked in float-float */
+    int32_t refinedClips;        /* pairs whose clipping was redone in float-float */
 } b3Counters;
 
 /* ------------------------------------------------------------------ */
