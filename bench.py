@@ -2,15 +2,33 @@
 
 python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2] [--impl b3|reference]
 
-Prints one JSON line (rank 0). `value` is whole-job body-steps/s with the
-scene resident in HBM, timed with CUDA events over K graph-replayed steps
-(max over ranks). `e2e` is the same metric through the C ABI with the body
-state uploaded from pinned host memory and positions/orientations read
-back every step. The per-kernel roofline uses live CUDA-event stage times.
+Prints one JSON line on rank 0.
+
+* value: whole-job body-steps/s of the plain step on the workload (default
+  the 131,072-body mixed-hull scene), the scene resident in HBM. Each of
+  the K timed steps is one replay of the captured step graph bracketed by
+  CUDA events on the launching stream; a 256 MiB write flushes L2 between
+  steps, outside the events. Max over ranks; for N > 1 every rank steps its
+  own replica (weak scaling, no collective on the data path).
+* e2e: the same metric through the C ABI with host buffers: every step
+  uploads the body state from pinned host memory, steps, and reads the
+  state back (H2D + D2H inside the timed region).
+* roofline: the dominant kernel of the step from live per-stage CUDA-event
+  times. The narrowphase is FP32-ALU bound (SAT projections), so its
+  roofline is FP32 FLOP/s against the CUDA-core peak; the other stages are
+  HBM bound and use the measured copy bandwidth. All stages are listed in
+  stage_roofline.
+* cpu_baseline: the oracle (single-threaded C++ port of the reference step)
+  on the host, a bounded sample of the same scene.
+* forms: the batched 4,096-world step against the plain per-world step on
+  the same GPU (body-steps/s of each; per-world time sampled on a subset).
+--impl reference: the oracle port on all host cores (independent replicas,
+  one process per core), same metric and workload.
 """
 import argparse
 import json
 import math
+import multiprocessing as mp
 import os
 import subprocess
 import sys
@@ -23,11 +41,14 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOADS = {
-    "c1": "Plain step, 4,096 unit cubes over a 200x200x1 m ground box (configs[0])",
-    "c2": "Plain step, 131,072 mixed hulls: 1/2 cubes, 1/4 12-point hulls, 1/4 42-vertex icospheres (configs[1])",
-    "c3": "Batched step, 4,096 worlds of log-uniform[8,512] cubes/12-point hulls (configs[2])",
-    "c5": "Plain step, 1,048,576 unit cubes (configs[4] forward)",
+    "c1": "plain step, 4,096 unit cubes over a 200x200x1 m ground box, 10 Jacobi iterations",
+    "c2": "plain step, 131,072 bodies (1/2 unit cubes, 1/4 12-point hulls, 1/4 42-vertex icospheres), "
+          "64x32x64 lattice at 1.2 m, 10 Jacobi iterations",
+    "c3": "batched step, 4,096 worlds of log-uniform[8,512] cubes / 12-point hulls, 10 Jacobi iterations",
+    "c5": "plain step, 1,048,576 unit cubes, 128x64x128 lattice, 10 Jacobi iterations",
 }
+STAGES = ["aabb_hash", "sort_cells", "find_pairs", "narrowphase", "manifolds", "solve", "integrate"]
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 148 SMs x 128 FP32 lanes x FMA x 1.965 GHz
 
 
 def peaks():
@@ -40,7 +61,7 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle sampling during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -53,10 +74,11 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            time.sleep(0.3)  # let the sampler start before the timed region
         except Exception:
             self.proc = None
         return self
@@ -67,6 +89,7 @@ class ClockSampler:
 
     def __exit__(self, *a):
         if self.proc:
+            time.sleep(0.15)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=2)
@@ -74,19 +97,25 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        if not self.rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        good = [r for r in self.rows if len(r) >= 9]
+        if not good:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in good if num(r[1]) is not None]
+        mx = [num(r[2]) for r in good if num(r[2]) is not None]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = set()
-        for r in self.rows:
-            if len(r) > 8:
-                for k, nm in enumerate(names):
-                    if r[5 + k].lower().startswith("active"):
-                        reasons.add(nm)
+        for r in good:
+            for k, nm in enumerate(names):
+                if r[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.rows)}
+                "reasons": sorted(reasons), "samples": len(good)}
 
 
 def make_scene(name):
@@ -94,29 +123,65 @@ def make_scene(name):
     return {"c1": scenes.c1, "c2": scenes.c2, "c3": scenes.c3, "c5": scenes.c5}[name]()
 
 
-def stage_bytes(scene_n, counters, key_bits, body_bits, iters):
-    """Algorithmic HBM bytes per launch of each stage (compulsory traffic,
-    each intermediate written once and read once)."""
-    N = scene_n
+def sat_flops(world, scene):
+    """Algorithmic FP32 work of the narrowphase over the current pair list
+    (SURVEY 8(d) model: 8 (VA+VB)(FA+FB+EA*EB) per pair for the separating
+    axis test, 64 V_inc V_ref for the clip of pairs with a manifold)."""
+    sh = world.shapes()
+    polys = sh["polys"]
+    V = np.array([polys[k].numVertices for k in range(sh["counts"][1])], np.float64)
+    F = np.array([polys[k].numFaces for k in range(sh["counts"][1])], np.float64)
+    E = np.array([polys[k].numUniqueEdges for k in range(sh["counts"][1])], np.float64)
+    colshape = np.array([sh["cols"][k].shapeIndex for k in range(sh["counts"][0])], np.int64)
+    pairs = world.pairs()
+    if len(pairs) == 0:
+        return 0.0
+    sa = colshape[scene.shape[pairs[:, 0]]]
+    sb = colshape[scene.shape[pairs[:, 1]]]
+    dyn = (scene.mass[pairs[:, 0]] > 0) | (scene.mass[pairs[:, 1]] > 0)
+    sat = 8.0 * (V[sa] + V[sb]) * (F[sa] + F[sb] + E[sa] * E[sb])
+    c = world.contacts()
+    clip = 64.0 * 4.0 * 4.0 * len(c["normal"])
+    return float(np.sum(sat[dyn]) + clip)
+
+
+def stage_bytes(n, counters, key_bits, body_bits, iters):
+    """Compulsory HBM bytes per launch of each stage (SURVEY 8(d) model: each
+    intermediate written once and read once)."""
     P = counters["numPairs"]
     C = counters["numManifolds"]
     S = 8 * (2 * math.ceil(key_bits / 8) + 1)
     S2 = 8 * (2 * math.ceil(body_bits / 8) + 1)
     return {
-        "aabb_hash": N * (64 + 8 + 32 + 8),            # pos+quat read, vel rw (dyn), aabb write, key/val write
-        "sort_cells": N * (S + 12),
-        "find_pairs": N * (8 + 32) + P * (8 + 32),      # sorted key/val + own AABB, pair write + other AABB
-        "narrowphase": P * (8 + 64) + C * 96,           # pair + two poses, manifold write
-        "manifolds": P * 8 + C * (96 + 16) + 2 * C * S2,
-        "solve": C * (96 + 640) + iters * (C * 2 * 576 + N * 4 * 64),
-        "integrate": N * (64 + 64 + 32),
+        "aabb_hash": n * (64 + 16 + 32 + 8),
+        "sort_cells": n * (S + 12),
+        "find_pairs": n * (8 + 32) + P * 8,
+        "narrowphase": P * (8 + 64) + C * 96,
+        "manifolds": P * 8 + C * 96 + 2 * C * S2,
+        "solve": C * (96 + 368) + iters * (200 * C + 64 * n),
+        "integrate": n * (64 + 64),
     }
 
 
-STAGES = ["aabb_hash", "sort_cells", "find_pairs", "narrowphase", "manifolds", "solve", "integrate"]
+def flush_l2(buf):
+    buf.add_(1)
 
 
-def run_b3(args, rank, world_size, local_rank):
+def time_steps(w, steps, stream, flush):
+    """Sum of per-step device times of graph replays, L2 flushed in between."""
+    import torch
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for e0, e1 in evs:
+        if flush is not None:
+            flush_l2(flush)
+        e0.record(stream)
+        w.stepSimulation(1, stream=stream.cuda_stream)
+        e1.record(stream)
+    torch.cuda.synchronize()
+    return sum(e0.elapsed_time(e1) for e0, e1 in evs)
+
+
+def run_b3(args, world_size, local_rank):
     import torch
     from experiments_b200 import b3, scenes
     torch.cuda.set_device(local_rank)
@@ -124,22 +189,17 @@ def run_b3(args, rank, world_size, local_rank):
     sc = make_scene(args.workload)
     w = scenes.build_world(ctx, sc, useGraph=1)
     st = torch.cuda.current_stream()
-    stream = st.cuda_stream
+    flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > 126 MB L2
     for _ in range(args.warmup):
-        w.stepSimulation(1, stream=stream)
+        w.stepSimulation(1, stream=st.cuda_stream)
     torch.cuda.synchronize()
     if world_size > 1:
         import torch.distributed as dist
         dist.barrier()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
     with ClockSampler(local_rank) as clk:
-        torch.cuda.synchronize()
-        e0.record(st)
-        w.stepSimulation(args.steps, stream=stream)
-        e1.record(st)
-        torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
+        ms = time_steps(w, args.steps, st, flush)
+    torch.cuda.synchronize()
     if world_size > 1:
         import torch.distributed as dist
         t = torch.tensor([ms], device="cuda")
@@ -147,63 +207,111 @@ def run_b3(args, rank, world_size, local_rank):
         ms = float(t.item())
         dist.barrier()
     counters = w.counters()
-    # stage breakdown: extra untimed steps with per-stage CUDA events
+    kernels = w.tuning()[3]
+    # per-stage CUDA-event breakdown on an identical world advanced to the
+    # same step (eager launches; timing only, not part of `value`)
     w2 = scenes.build_world(ctx, sc, useGraph=0)
-    for _ in range(args.warmup):
-        w2.stepSimulation(1)
+    w2.stepSimulation(args.warmup + args.steps - 3)
     w2.set_stage_timing(True)
     acc = np.zeros(len(STAGES))
-    reps = 3
-    for _ in range(reps):
+    for _ in range(3):
+        flush_l2(flush)
         w2.stepSimulation(1)
         acc += np.array(w2.stage_times()[:len(STAGES)])
-    stage_ms = acc / reps
+    stage_ms = acc / 3
     c2 = w2.counters()
+    flops = sat_flops(w2, sc)
     w2.close()
-    # e2e: through the C ABI with host buffers every step
-    n = sc.n
+    # e2e through the C ABI with pinned host buffers
     pos, quat, lin, ang = w.read_state()
     hp = torch.from_numpy(pos).pin_memory().numpy()
     hq = torch.from_numpy(quat).pin_memory().numpy()
     hl = torch.from_numpy(lin).pin_memory().numpy()
     ha = torch.from_numpy(ang).pin_memory().numpy()
-    e2e_steps = max(1, min(args.steps, 20))
+    e2e_steps = max(3, min(args.steps, 20))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    e2 = torch.cuda.Event(enable_timing=True)
-    e3 = torch.cuda.Event(enable_timing=True)
-    e2.record(st)
     for _ in range(e2e_steps):
-        w.write_state(hp, hq, hl, ha, stream=stream)
-        w.stepSimulation(1, stream=stream)
-        p_, q_, l_, a_ = w.read_state(stream=stream)
+        w.write_state(hp, hq, hl, ha, stream=st.cuda_stream)
+        w.stepSimulation(1, stream=st.cuda_stream)
+        p_, q_, l_, a_ = w.read_state(stream=st.cuda_stream)
         hp[:], hq[:], hl[:], ha[:] = p_, q_, l_, a_
-    e3.record(st)
     torch.cuda.synchronize()
-    e2e_ms = e2.elapsed_time(e3) / e2e_steps
-    wall_e2e = (time.perf_counter() - t0) / e2e_steps * 1e3
-    e2e_ms = max(e2e_ms, wall_e2e)
-    return dict(sc=sc, ms=ms, counters=counters, stage_ms=stage_ms, c2=c2, clocks=clk.summary(),
-                e2e_ms=e2e_ms, w=w, n=n)
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
+    return dict(sc=sc, ms=ms, counters=counters, stage_ms=stage_ms, c2=c2, clocks=clk.summary(), e2e_ms=e2e_ms,
+                w=w, kernels=kernels, flops=flops, ctx=ctx)
 
 
-def cpu_baseline_port(sc_name, budget_s=15.0):
-    """The oracle (single-threaded port) on a bounded sample of the workload."""
+def forms_comparison(ctx, steps=10, sample_worlds=32):
+    """Batched 4,096-world step vs the plain step run world by world."""
+    import torch
+    from experiments_b200 import scenes
+    sc = scenes.c3()
+    wb = scenes.build_world(ctx, sc, useGraph=1)
+    st = torch.cuda.current_stream()
+    for _ in range(3):
+        wb.stepSimulation(1, stream=st.cuda_stream)
+    ms_b = time_steps(wb, steps, st, None)
+    batched = sc.n * steps / (ms_b / 1e3)
+    # plain per-world step: each world in its own plain world, stepped one
+    # world at a time (the reference's one-scene-per-pipeline usage)
+    counts = sc.extra["counts"]
+    rng = np.random.default_rng(0)
+    pick = rng.choice(len(counts), size=min(sample_worlds, len(counts)), replace=False)
+    total_ms = 0.0
+    bodies = 0
+    for wid in pick:
+        sub = scenes.select_worlds(sc, [int(wid)])
+        wp = scenes.build_world(ctx, sub, useGraph=1)
+        for _ in range(3):
+            wp.stepSimulation(1, stream=st.cuda_stream)
+        total_ms += time_steps(wp, steps, st, None)
+        bodies += sub.n
+        wp.close()
+    # extrapolate the sampled per-world times to all worlds
+    per_body_ms = total_ms / max(bodies, 1)
+    plain = sc.n * steps / (per_body_ms * sc.n / 1e3)
+    wb.close()
+    return {"batched_body_steps_per_s": batched, "plain_per_world_body_steps_per_s": plain,
+            "speedup": batched / plain, "worlds": int(sc.num_worlds), "bodies": int(sc.n),
+            "plain_sample": f"{len(pick)} of {sc.num_worlds} worlds, {steps} steps each, graph replay",
+            "steps": steps}
+
+
+def _oracle_worker(args):
+    name, budget_s, seed_steps = args
+    sys.path.insert(0, ROOT)
     import oracle
     from experiments_b200 import b3, scenes
-    sc = make_scene(sc_name)
+    sc = make_scene(name)
     hc = b3.Context(-1)
     w = b3.PhysicsWorld(hc, scenes.world_config(sc))
     scenes.register_scene(w, sc)
     o = oracle.oracle_from_world(w, sc)
+    if seed_steps:
+        o.step(seed_steps)
     t0 = time.perf_counter()
     steps = 0
     while time.perf_counter() - t0 < budget_s and steps < 1000:
         o.step(1)
         steps += 1
-    dt = time.perf_counter() - t0
-    return {"value": sc.n * steps / dt, "unit": "body-steps/s", "cores": 1, "kind": "port",
-            "sample": f"{steps} steps of the full {sc.n}-body scene in {dt:.1f} s, 1 thread"}
+    return sc.n, steps, time.perf_counter() - t0
+
+
+def cpu_baseline_port(name, budget_s=12.0, procs=1):
+    """The oracle port on `procs` host cores (independent replicas)."""
+    if procs <= 1:
+        n, steps, dt = _oracle_worker((name, budget_s, 0))
+        return {"value": n * steps / dt, "unit": "body-steps/s", "cores": 1, "kind": "port",
+                "sample": f"first {steps} steps of the full {n}-body scene ({dt:.1f} s), 1 thread"}
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_oracle_worker, [(name, budget_s, 0)] * procs)
+    total = sum(n * s / dt for n, s, dt in res)
+    n, s, dt = res[0]
+    return {"value": total, "unit": "body-steps/s", "cores": procs, "kind": "port",
+            "sample": f"{procs} independent replicas, each the first ~{s} steps of the full {n}-body scene "
+                      f"(~{dt:.0f} s)"}
 
 
 def main():
@@ -214,22 +322,25 @@ def main():
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="b3", choices=["b3", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world_size = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     args.warmup = max(3, args.warmup)
+    cfg = {"workload": WORKLOADS[args.workload]}
 
     if args.impl == "reference":
         if rank != 0:
             return
-        r = cpu_baseline_port(args.workload, budget_s=max(10.0, min(60.0, args.steps * 2.0)))
+        procs = max(1, os.cpu_count() or 1)
+        r = cpu_baseline_port(args.workload, budget_s=20.0, procs=procs)
         line = {"metric": "body-steps/s", "value": r["value"], "unit": "body-steps/s", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "impl": "reference", "config": {"workload": WORKLOADS[args.workload]},
-                "cpu_baseline": r, "e2e": {"value": r["value"], "unit": "body-steps/s",
-                                           "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+                "config": cfg, "cpu_baseline": r,
+                "e2e": {"value": r["value"], "unit": "body-steps/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
 
@@ -239,44 +350,55 @@ def main():
         from datetime import timedelta
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    res = run_b3(args, rank, world_size, local_rank)
+    res = run_b3(args, world_size, local_rank)
     sc = res["sc"]
     ms_per_step = res["ms"] / args.steps
     value = sc.n * args.steps * world_size / (res["ms"] / 1e3)
-    peak, peak_kind = peaks()
-    from experiments_b200 import b3 as _b3  # noqa: F401
+    hbm_peak, peak_kind = peaks()
     w = res["w"]
-    key_bits = w.cfg.gridDims[0].bit_length() - 1 + w.cfg.gridDims[1].bit_length() - 1 + \
-        w.cfg.gridDims[2].bit_length() - 1 + (max(1, sc.num_worlds - 1).bit_length() if sc.num_worlds > 1 else 0)
+    dims = list(w.cfg.gridDims)
+    key_bits = sum(int(d).bit_length() - 1 for d in dims) + \
+        ((int(sc.num_worlds) - 1).bit_length() if sc.num_worlds > 1 else 0)
     body_bits = max(1, int(sc.n).bit_length())
     sb = stage_bytes(sc.n, res["c2"], key_bits, body_bits, 10)
     sm = dict(zip(STAGES, res["stage_ms"].tolist()))
+    stage_roof = {}
+    for k in STAGES:
+        if k == "narrowphase":
+            ach = res["flops"] / (sm[k] / 1e3) / 1e12
+            stage_roof[k] = {"bound": "fp32", "achieved": ach, "peak": FP32_PEAK_TFLOPS, "unit": "TFLOP/s",
+                             "frac": ach / FP32_PEAK_TFLOPS, "ms": sm[k]}
+        else:
+            ach = sb[k] / (sm[k] / 1e3) / 1e9
+            stage_roof[k] = {"bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
+                             "frac": ach / hbm_peak, "ms": sm[k]}
     dom = max(sm, key=lambda k: sm[k])
-    achieved = sb[dom] / (sm[dom] / 1e3) / 1e9
-    passes = math.ceil(key_bits / 8)
-    passes2 = math.ceil(body_bits / 8)
-    launches = 1 + 1 + (1 + passes) + 1 + 1 + 1 + 2 + 1 + (1 + passes2) + 1 + 1 + 1 + 1
+    roof = dict(stage_roof[dom])
+    roof["kernel"] = dom
+    roof["traffic"] = None
+    roof["peak_kind"] = "nominal FP32 CUDA-core peak" if roof["bound"] == "fp32" else peak_kind
+    cfg.update({"bodies": int(sc.n), "worlds": int(sc.num_worlds), "pairs": res["counters"]["numPairs"],
+                "manifolds": res["counters"]["numManifolds"],
+                "contact_points": res["counters"]["numContactPoints"], "iterations": 10, "dt": 1 / 60,
+                "refined_axes": res["counters"]["refinedAxes"], "refined_clips": res["counters"]["refinedClips"],
+                "l2": "flushed between timed steps (256 MiB write outside the events)",
+                "parallelism": f"replicas x{world_size}" if world_size > 1 else "single GPU",
+                "error": "pairs/keys bit-exact; contacts 1e-5 m / normals 1e-4; one step 1e-5 m, 1e-4 m/s "
+                         "(tests/test_gpu_parity.py)"})
     line = {
         "metric": "body-steps/s", "value": value, "unit": "body-steps/s", "n_gpus": world_size,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOADS[args.workload], "bodies": sc.n, "worlds": sc.num_worlds,
-                   "pairs": res["counters"]["numPairs"], "manifolds": res["counters"]["numManifolds"],
-                   "contact_points": res["counters"]["numContactPoints"], "iterations": 10,
-                   "refined_axes": res["counters"].get("refinedAxes"),
-                   "refined_clips": res["counters"].get("refinedClips"),
-                   "parallelism": "replicas" if world_size > 1 else "single",
-                   "l2": "working set exceeds L2" if sc.n > 100000 else "working set L2-resident; no flush"},
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
+        "config": cfg,
         "contacts_per_s": res["counters"]["numContactPoints"] * args.steps * world_size / (res["ms"] / 1e3),
-        "stage_ms": sm,
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind},
-        "clocks": res["clocks"],
-        "e2e": {"value": sc.n / (res["e2e_ms"] / 1e3) * world_size, "unit": "body-steps/s",
+        "roofline": roof, "stage_roofline": stage_roof, "clocks": res["clocks"],
+        "e2e": {"value": sc.n * world_size / (res["e2e_ms"] / 1e3), "unit": "body-steps/s",
                 "h2d_bytes_per_step": 64 * sc.n, "d2h_bytes_per_step": 64 * sc.n},
-        "gpu_launches": launches * args.steps,
+        "gpu_launches": int(res["kernels"]) * args.steps,
     }
-    if rank == 0 and not args.no_cpu_baseline and world_size == 1:
+    if rank == 0 and world_size == 1 and not args.no_forms:
+        line["forms"] = forms_comparison(res["ctx"])
+    if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_port(args.workload)
     if rank == 0:
         print(json.dumps(line))

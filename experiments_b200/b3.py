@@ -456,6 +456,13 @@ class PhysicsWorld:
         return np.array([[a.initInvInertia[0], a.initInvInertia[5], a.initInvInertia[10], 0.0] for a in arr],
                         np.float32).reshape(-1, 4)
 
+    def tuning(self):
+        """(narrowphase warps/CTA, pair CTA size, solver CTA size, kernels per captured step)."""
+        v = (C.c_int * 8)()
+        cnt = C.c_int()
+        _check(self.lib.b3_get_tuning(self.h, v, 8, C.byref(cnt)), "b3_get_tuning")
+        return list(v)[:cnt.value]
+
     def set_stage_timing(self, on=True):
         _check(self.lib.b3_set_stage_timing(self.h, 1 if on else 0), "b3_set_stage_timing")
 

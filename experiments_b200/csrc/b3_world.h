@@ -149,6 +149,7 @@ struct b3World_t {
 
     // tunables (autotuner)
     int npWarpsPerBlock = 4;   // narrowphase warps per CTA
+    int kernelsPerStep = 0;    // kernel nodes in the captured step graph
     int pairThreads = 128;     // pair-search CTA size
     int solverThreads = 256;   // Jacobi CTA size
 

@@ -618,6 +618,18 @@ extern "C" int b3_step(b3World w, int numSteps, void* stream) {
                 return B3_ERR_CUDA;
             }
             if (w->graphExec) cudaGraphExecDestroy(w->graphExec);
+            {
+                size_t nn = 0;
+                cudaGraphGetNodes(g, nullptr, &nn);
+                std::vector<cudaGraphNode_t> nodes(nn);
+                if (nn) cudaGraphGetNodes(g, nodes.data(), &nn);
+                int kn = 0;
+                for (auto nd : nodes) {
+                    cudaGraphNodeType t;
+                    if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++kn;
+                }
+                w->kernelsPerStep = kn;
+            }
             cudaError_t ie = cudaGraphInstantiate(&w->graphExec, g, 0);
             cudaGraphDestroy(g);
             if (ie != cudaSuccess) {
@@ -909,9 +921,9 @@ extern "C" int b3_autotune(b3World w, int trialSteps, void* stream) {
 
 extern "C" int b3_get_tuning(b3World w, int* values, int max, int* count) {
     if (!w || !count) return B3_ERR_INVALID_ARG;
-    int v[3] = {w->npWarpsPerBlock, w->pairThreads, w->solverThreads};
-    *count = 3;
-    for (int i = 0; i < std::min(3, max); ++i) values[i] = v[i];
+    int v[4] = {w->npWarpsPerBlock, w->pairThreads, w->solverThreads, w->kernelsPerStep};
+    *count = 4;
+    for (int i = 0; i < std::min(4, max); ++i) values[i] = v[i];
     return B3_OK;
 }
 

@@ -308,3 +308,18 @@ def build_world(ctx, scene, **over):
     if np.any(scene.lin) or np.any(scene.ang):
         w.write_velocities(scene.lin, scene.ang)
     return w
+
+
+def select_worlds(scene, world_ids):
+    """Sub-scene holding only the given worlds, renumbered 0..k-1 (a single
+    world becomes a plain one-world scene)."""
+    world_ids = list(world_ids)
+    remap = {w: i for i, w in enumerate(world_ids)}
+    keep = np.isin(scene.world, world_ids)
+    b = dict(shape=scene.shape[keep], mass=scene.mass[keep], pos=scene.pos[keep], quat=scene.quat[keep],
+             friction=scene.friction[keep], world=np.array([remap[int(w)] for w in scene.world[keep]], np.int32),
+             lin=scene.lin[keep], ang=scene.ang[keep])
+    cfg = dict(scene.config)
+    cfg.pop("maxPairs", None)
+    return Scene(name=f"{scene.name}_sel{len(world_ids)}", shapes=scene.shapes, num_worlds=len(world_ids),
+                 config=cfg, steps=scene.steps, **b)

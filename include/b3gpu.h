@@ -333,6 +333,8 @@ int b3_batch_world_stats(b3World w, float* out4, int numWorlds, void* stream);
 /* Autotuner: time the candidate launch shapes of the tunable kernels on
  * the current scene and keep the fastest (steps are run and rolled back). */
 int b3_autotune(b3World w, int trialSteps, void* stream);
+/* values: narrowphase warps per CTA, pair-search CTA size, solver CTA size,
+ * kernel launches per step of the captured step graph (0 before capture). */
 int b3_get_tuning(b3World w, int* values, int max, int* count);
 
 /* ------------------------------------------------------------------ */

@@ -268,20 +268,16 @@ def large_flags(world, scene, cfg):
     """Registration-AABB half-diagonal > maxSmallProxySize / 2, computed from
     the scene and the local AABBs (G3/btGpu3DGridBroadphase.cpp:385-391)."""
     sh = world.shapes()
-    la = sh["localAabb"]
-    n = scene.n
-    out = np.zeros(n, np.int32)
-    for i in range(n):
-        c = scene.shape[i]
-        lmin = la[c, :3].astype(np.float64)
-        lmax = la[c, 4:7].astype(np.float64)
-        he = 0.5 * (lmax - lmin) + 0.01
-        x, y, z, w = [float(v) for v in scene.quat[i]]
-        s = 2.0 / (x * x + y * y + z * z + w * w)
-        R = np.array([[1 - (y * y + z * z) * s, (x * y - w * z) * s, (x * z + w * y) * s],
-                      [(x * y + w * z) * s, 1 - (x * x + z * z) * s, (y * z - w * x) * s],
-                      [(x * z - w * y) * s, (y * z + w * x) * s, 1 - (x * x + y * y) * s]])
-        e = np.abs(R) @ he
-        r = 0.5 * np.linalg.norm(2 * e)
-        out[i] = 1 if r > 0.5 * cfg.maxSmallProxySize else 0
-    return out
+    la = sh["localAabb"].astype(np.float64)
+    c = np.asarray(scene.shape)
+    lmin, lmax = la[c, :3], la[c, 4:7]
+    he = 0.5 * (lmax - lmin) + 0.01
+    q = scene.quat.astype(np.float64)
+    x, y, z, w = q[:, 0], q[:, 1], q[:, 2], q[:, 3]
+    s = 2.0 / (x * x + y * y + z * z + w * w)
+    R = np.stack([np.stack([1 - (y * y + z * z) * s, (x * y - w * z) * s, (x * z + w * y) * s], 1),
+                  np.stack([(x * y + w * z) * s, 1 - (x * x + z * z) * s, (y * z - w * x) * s], 1),
+                  np.stack([(x * z - w * y) * s, (y * z + w * x) * s, 1 - (x * x + y * y) * s], 1)], 1)
+    e = np.einsum("nij,nj->ni", np.abs(R), he)
+    r = np.linalg.norm(e, axis=1)
+    return (r > 0.5 * cfg.maxSmallProxySize).astype(np.int32)
