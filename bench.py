@@ -44,10 +44,15 @@ WORKLOADS = {
     "c1": "plain step, 4,096 unit cubes over a 200x200x1 m ground box, 10 Jacobi iterations",
     "c2": "plain step, 131,072 bodies (1/2 unit cubes, 1/4 12-point hulls, 1/4 42-vertex icospheres), "
           "64x32x64 lattice at 1.2 m, 10 Jacobi iterations",
+    "c2s": "plain step, 16,384 bodies (the 131,072-body mix on a 32x16x32 lattice at 1.2 m), "
+           "10 Jacobi iterations (small case for profiler captures)",
     "c3": "batched step, 4,096 worlds of log-uniform[8,512] cubes / 12-point hulls, 10 Jacobi iterations",
     "c5": "plain step, 1,048,576 unit cubes, 128x64x128 lattice, 10 Jacobi iterations",
 }
 STAGES = ["aabb_hash", "sort_cells", "find_pairs", "narrowphase", "manifolds", "solve", "integrate"]
+# DRAM bytes per pair of k_narrowphase (read + write) from the ncu capture in
+# profiles/kernels_c2s_plain_step.md, scaled by the timed workload's pair count
+NARROWPHASE_DRAM_BYTES_PER_PAIR = 2.61e6 / 36735
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 148 SMs x 128 FP32 lanes x FMA x 1.965 GHz
 
 
@@ -120,13 +125,14 @@ class ClockSampler:
 
 def make_scene(name):
     from experiments_b200 import scenes
-    return {"c1": scenes.c1, "c2": scenes.c2, "c3": scenes.c3, "c5": scenes.c5}[name]()
+    return {"c1": scenes.c1, "c2": scenes.c2, "c2s": lambda: scenes.c2(dims=(32, 16, 32)), "c3": scenes.c3,
+            "c5": scenes.c5}[name]()
 
 
 def sat_flops(world, scene):
     """Algorithmic FP32 work of the narrowphase over the current pair list
-    (SURVEY 8(d) model: 8 (VA+VB)(FA+FB+EA*EB) per pair for the separating
-    axis test, 64 V_inc V_ref for the clip of pairs with a manifold)."""
+    (8 (VA+VB)(FA+FB+EA*EB) per pair for the separating axis test,
+    64 V_inc V_ref for the clip of pairs with a manifold)."""
     sh = world.shapes()
     polys = sh["polys"]
     V = np.array([polys[k].numVertices for k in range(sh["counts"][1])], np.float64)
@@ -146,8 +152,8 @@ def sat_flops(world, scene):
 
 
 def stage_bytes(n, counters, key_bits, body_bits, iters):
-    """Compulsory HBM bytes per launch of each stage (SURVEY 8(d) model: each
-    intermediate written once and read once)."""
+    """Compulsory HBM bytes per launch of each stage (each intermediate
+    written once and read once; hull and cell tables assumed on chip)."""
     P = counters["numPairs"]
     C = counters["numManifolds"]
     S = 8 * (2 * math.ceil(key_bits / 8) + 1)
@@ -161,6 +167,16 @@ def stage_bytes(n, counters, key_bits, body_bits, iters):
         "solve": C * (96 + 368) + iters * (200 * C + 64 * n),
         "integrate": n * (64 + 64),
     }
+
+
+def step_bytes(n, counters, key_bits, iters):
+    """Compulsory HBM bytes of one whole step:
+    N (128 + 20 + 8 + S + 12 + 32) + 80 P + 368 C + I (200 C + 64 N),
+    S = 8 (2 ceil(kbits / 8) + 1) the radix sort term."""
+    P = counters["numPairs"]
+    C = counters["numManifolds"]
+    S = 8 * (2 * math.ceil(key_bits / 8) + 1)
+    return n * (128 + 20 + 8 + S + 12 + 32) + 80 * P + 368 * C + iters * (200 * C + 64 * n)
 
 
 def flush_l2(buf):
@@ -372,10 +388,16 @@ def main():
             ach = sb[k] / (sm[k] / 1e3) / 1e9
             stage_roof[k] = {"bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
                              "frac": ach / hbm_peak, "ms": sm[k]}
+    b_step = step_bytes(sc.n, res["counters"], key_bits, 10)
+    step_roof = {"bound": "hbm", "achieved": b_step / (ms_per_step / 1e3) / 1e9, "peak": hbm_peak,
+                 "unit": "GB/s", "bytes_per_step": b_step, "peak_kind": peak_kind}
+    step_roof["frac"] = step_roof["achieved"] / hbm_peak
     dom = max(sm, key=lambda k: sm[k])
     roof = dict(stage_roof[dom])
     roof["kernel"] = dom
-    roof["traffic"] = None
+    roof["traffic"] = NARROWPHASE_DRAM_BYTES_PER_PAIR * res["c2"]["numPairs"] if dom == "narrowphase" else None
+    roof["traffic_source"] = "ncu dram bytes per pair on the 16,384-body case, scaled by pairs" \
+        if dom == "narrowphase" else None
     roof["peak_kind"] = "nominal FP32 CUDA-core peak" if roof["bound"] == "fp32" else peak_kind
     cfg.update({"bodies": int(sc.n), "worlds": int(sc.num_worlds), "pairs": res["counters"]["numPairs"],
                 "manifolds": res["counters"]["numManifolds"],
@@ -391,7 +413,7 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
         "config": cfg,
         "contacts_per_s": res["counters"]["numContactPoints"] * args.steps * world_size / (res["ms"] / 1e3),
-        "roofline": roof, "stage_roofline": stage_roof, "clocks": res["clocks"],
+        "roofline": roof, "step_roofline": step_roof, "stage_roofline": stage_roof, "clocks": res["clocks"],
         "e2e": {"value": sc.n * world_size / (res["e2e_ms"] / 1e3), "unit": "body-steps/s",
                 "h2d_bytes_per_step": 64 * sc.n, "d2h_bytes_per_step": 64 * sc.n},
         "gpu_launches": int(res["kernels"]) * args.steps,

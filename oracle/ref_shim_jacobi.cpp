@@ -15,3 +15,9 @@ extern "C" int ref_jacobi_solve(int numBodies, void* bodies80, void* inertias96,
                          numContacts, (Contact4*)contacts96);
     return 0;
 }
+
+// The solver's translation unit emits btTypedConstraint's vtable, which names
+// serialize(); joints are compiled out (DISABLE_JOINTS) and no constraint
+// object is ever created, so this definition only satisfies the linker.
+#include "BulletDynamics/ConstraintSolver/btTypedConstraint.h"
+const char* btTypedConstraint::serialize(void*, btSerializer*) const { return 0; }
