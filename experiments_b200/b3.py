@@ -135,6 +135,11 @@ SIGNATURES = [
     ("b3_stage_narrowphase", _I, [_P, _P]),
     ("b3_stage_solve", _I, [_P, _P]),
     ("b3_stage_integrate", _I, [_P, _P]),
+    ("b3_grid_broadphase_calculate_overlapping_pairs", _I, [_P, _P]),
+    ("b3_grid_broadphase_get_pair_count", _I, [_P, _IP, _P]),
+    ("b3_narrowphase_compute_contacts", _I, [_P, _P, _I, _P]),
+    ("b3_solver_solve_jacobi", _I, [_P, _P]),
+    ("b3_integrate", _I, [_P, _P]),
     ("b3_get_aabbs", _I, [_P, _FP, _I, _P]),
     ("b3_get_sorted_hash", _I, [_P, _U32P, _U32P, _I, _IP, _P]),
     ("b3_get_pairs", _I, [_P, _IP, _I, _IP, _P]),
@@ -147,6 +152,7 @@ SIGNATURES = [
     ("b3_set_stage_timing", _I, [_P, _I]),
     ("b3_get_stage_times", _I, [_P, _FP, _I, _IP]),
     ("b3_batch_world_stats", _I, [_P, _FP, _I, _P]),
+    ("b3_batch_world_offsets", _I, [_P, _IP, _I, _IP]),
     ("b3_autotune", _I, [_P, _I, _P]),
     ("b3_get_tuning", _I, [_P, _IP, _I, _IP]),
     ("b3_adjoint_create", _I, [_P, _I, _I, C.POINTER(_P)]),
@@ -476,6 +482,20 @@ class PhysicsWorld:
         out = np.zeros((num_worlds, 4), np.float32)
         _check(self.lib.b3_batch_world_stats(self.h, fptr(out), num_worlds, None), "b3_batch_world_stats")
         return out
+
+    def world_offsets(self):
+        """Body-count prefix sums per world (numWorlds + 1 entries)."""
+        nw = C.c_int()
+        _check(self.lib.b3_batch_world_offsets(self.h, None, 0, C.byref(nw)), "b3_batch_world_offsets")
+        out = np.zeros(nw.value + 1, np.int32)
+        _check(self.lib.b3_batch_world_offsets(self.h, iptr(out), len(out), C.byref(nw)), "b3_batch_world_offsets")
+        return out
+
+    def compute_contacts(self, d_pairs=None, num_pairs=0, stream=None):
+        """Narrowphase on caller device pairs (int2) or, with None, on the
+        world's own broadphase pairs."""
+        _check(self.lib.b3_narrowphase_compute_contacts(self.h, d_pairs, num_pairs, stream),
+               "b3_narrowphase_compute_contacts")
 
     def device_buffer(self, which):
         p = C.c_void_p()

@@ -675,6 +675,62 @@ extern "C" int b3_stage_integrate(b3World w, void* stream) {
     return b3::launch_integrate(w, as_stream(stream));
 }
 
+// Entry points under the reference object API's names.
+extern "C" int b3_grid_broadphase_calculate_overlapping_pairs(b3World w, void* stream) {
+    return b3_stage_broadphase(w, stream);
+}
+
+extern "C" int b3_grid_broadphase_get_pair_count(b3World w, int* count, void* stream) {
+    if (!w || !count) return B3_ERR_INVALID_ARG;
+    if (!w->written) return B3_ERR_STATE;
+    cudaStream_t st = as_stream(stream);
+    int np = 0;
+    B3_CUDA(cudaMemcpyAsync(&np, w->d.scalars + b3::S_NUM_PAIRS, 4, cudaMemcpyDeviceToHost, st));
+    B3_CUDA(cudaStreamSynchronize(st));
+    *count = np;
+    return B3_OK;
+}
+
+extern "C" int b3_narrowphase_compute_contacts(b3World w, const int32_t* d_pairs, int numPairs, void* stream) {
+    if (!w) return B3_ERR_INVALID_ARG;
+    if (!w->written) return B3_ERR_STATE;
+    cudaStream_t st = as_stream(stream);
+    if (d_pairs) {
+        if (numPairs < 0) return B3_ERR_INVALID_ARG;
+        if (numPairs > w->cfg.maxPairs) {
+            b3_set_error("b3_narrowphase_compute_contacts: %d pairs exceed maxPairs %d", numPairs, w->cfg.maxPairs);
+            return B3_ERR_CAPACITY;
+        }
+        if (numPairs > 0)
+            B3_CUDA(cudaMemcpyAsync(w->d.pairs, d_pairs, (size_t)numPairs * sizeof(int2), cudaMemcpyDeviceToDevice,
+                                    st));
+        // pageable source: the copy is staged before the call returns
+        B3_CUDA(cudaMemcpyAsync(w->d.scalars + b3::S_NUM_PAIRS, &numPairs, 4, cudaMemcpyHostToDevice, st));
+    }
+    B3_TRY(b3::launch_narrowphase(w, st));
+    return b3::launch_manifolds(w, st);
+}
+
+extern "C" int b3_solver_solve_jacobi(b3World w, void* stream) { return b3_stage_solve(w, stream); }
+
+extern "C" int b3_integrate(b3World w, void* stream) { return b3_stage_integrate(w, stream); }
+
+extern "C" int b3_batch_world_offsets(b3World w, int* offsets, int maxWorlds, int* numWorlds) {
+    if (!w || !numWorlds) return B3_ERR_INVALID_ARG;
+    const int nw = w->cfg.numWorlds > 0 ? w->cfg.numWorlds : 1;
+    *numWorlds = nw;
+    if (!offsets) return B3_OK;
+    if (maxWorlds < nw + 1) return B3_ERR_CAPACITY;
+    std::vector<int> cnt(nw + 1, 0);
+    for (int id : w->worldIds) {
+        if (id < 0 || id >= nw) return B3_ERR_STATE;
+        ++cnt[id + 1];
+    }
+    for (int k = 0; k < nw; ++k) cnt[k + 1] += cnt[k];
+    for (int k = 0; k <= nw; ++k) offsets[k] = cnt[k];
+    return B3_OK;
+}
+
 // ---------------------------------------------------------------------------
 // Reads
 // ---------------------------------------------------------------------------

@@ -292,6 +292,26 @@ int b3_stage_solve(b3World w, void* stream);
 /* integrateTransformsKernel2 (BB/integrateKernel.cl:102-158). */
 int b3_stage_integrate(b3World w, void* stream);
 
+/* --- the same stages under the reference object API's names --- */
+/* btGridBroadphaseCl::calculateOverlappingPairs (BB/btGridBroadphaseCL.cpp:135-238);
+ * same as b3_stage_broadphase (uses the AABBs of b3_stage_aabbs). */
+int b3_grid_broadphase_calculate_overlapping_pairs(b3World w, void* stream);
+/* btGridBroadphaseCl::getNumOverlap (BB/btGridBroadphaseCL.h:48-51):
+ * pairs found by the last broadphase (synchronising). */
+int b3_grid_broadphase_get_pair_count(b3World w, int* count, void* stream);
+/* btGpuNarrowphaseAndSolver::computeContacts(pairs, nPairs, aabbs, nObjects)
+ * (P1/btGpuNarrowPhaseAndSolver.h:101): contacts for caller-provided device
+ * pairs (int2 (self, other), numPairs <= maxPairs; copied into the world's
+ * pair buffer), or for the world's own broadphase pairs when d_pairs is
+ * NULL. Also builds the manifold list the solver consumes. */
+int b3_narrowphase_compute_contacts(b3World w, const int32_t* d_pairs, int numPairs, void* stream);
+/* btPgsJacobiSolver::solveContacts (P2/btPgsJacobiSolver.cpp:171-189) on the
+ * device: same as b3_stage_solve. */
+int b3_solver_solve_jacobi(b3World w, void* stream);
+/* integrateTransformsKernel2 (BB/integrateKernel.cl:102-158): same as
+ * b3_stage_integrate. */
+int b3_integrate(b3World w, void* stream);
+
 /* --- stage outputs (host copies, synchronising) --- */
 /* World AABBs, 2 float4 per body (min.w = body id bits, max.w = dynamic flag). */
 int b3_get_aabbs(b3World w, float* out8, int maxBodies, void* stream);
@@ -330,6 +350,11 @@ int b3_get_stage_times(b3World w, float* ms, int max, int* count);
 /* Per-world aggregate: centre of mass and kinetic energy, 4 floats per
  * world (x, y, z, KE) computed on device; host output. */
 int b3_batch_world_stats(b3World w, float* out4, int numWorlds, void* stream);
+/* Body-count prefix sums per world: offsets[k+1] - offsets[k] bodies carry
+ * worldId k (numWorlds + 1 entries; bodies registered in world order occupy
+ * [offsets[k], offsets[k+1])). offsets NULL = query numWorlds only. Used to
+ * partition worlds across GPUs by body count. */
+int b3_batch_world_offsets(b3World w, int* offsets, int maxWorlds, int* numWorlds);
 /* Autotuner: time the candidate launch shapes of the tunable kernels on
  * the current scene and keep the fastest (steps are run and rolled back). */
 int b3_autotune(b3World w, int trialSteps, void* stream);
