@@ -160,6 +160,7 @@ SIGNATURES = [
     ("b3_adjoint_forward", _I, [_P, _P]),
     ("b3_adjoint_backward", _I, [_P, _FP, _FP, _FP, _FP, _P]),
     ("b3_adjoint_gradients", _I, [_P, _FP, _FP, _FP, _FP]),
+    ("b3_adjoint_info", _I, [_P, _IP]),
 ]
 
 
@@ -507,6 +508,64 @@ class PhysicsWorld:
     def close(self):
         if self.h:
             self.lib.b3_world_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Adjoint:
+    """Reverse-mode gradients of a loss of the final state with respect to
+    the initial velocities, masses and friction coefficients
+    (b3_adjoint_*): forward() runs num_steps steps with checkpoints every
+    checkpoint_every steps, backward(seeds) runs the reverse sweep."""
+
+    def __init__(self, world, num_steps, checkpoint_every):
+        self.world = world
+        self.lib = world.lib
+        h = _P()
+        _check(self.lib.b3_adjoint_create(world.h, int(num_steps), int(checkpoint_every), C.byref(h)),
+               "b3_adjoint_create")
+        self.h = h
+
+    def forward(self, stream=None):
+        _check(self.lib.b3_adjoint_forward(self.h, _stream(stream)), "b3_adjoint_forward")
+
+    def backward(self, d_pos=None, d_quat=None, d_lin=None, d_ang=None, stream=None):
+        n = self.world.n
+
+        def arr(x):
+            if x is None:
+                return None
+            a = np.zeros((n, 4), np.float32)
+            x = np.asarray(x, np.float32).reshape(n, -1)
+            a[:, :x.shape[1]] = x
+            return a
+
+        keep = [arr(x) for x in (d_pos, d_quat, d_lin, d_ang)]
+        ptrs = [fptr(a) if a is not None else None for a in keep]
+        _check(self.lib.b3_adjoint_backward(self.h, *ptrs, _stream(stream)), "b3_adjoint_backward")
+
+    def gradients(self):
+        n = self.world.n
+        gl = np.zeros((n, 4), np.float32)
+        ga = np.zeros((n, 4), np.float32)
+        gm = np.zeros(n, np.float32)
+        gf = np.zeros(n, np.float32)
+        _check(self.lib.b3_adjoint_gradients(self.h, fptr(gl), fptr(ga), fptr(gm), fptr(gf)), "b3_adjoint_gradients")
+        return dict(lin=gl[:, :3], ang=ga[:, :3], mass=gm, friction=gf)
+
+    def unclassified(self):
+        v = C.c_int()
+        _check(self.lib.b3_adjoint_info(self.h, C.byref(v)), "b3_adjoint_info")
+        return v.value
+
+    def close(self):
+        if self.h:
+            self.lib.b3_adjoint_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -160,6 +160,15 @@ struct b3World_t {
 };
 
 namespace b3 {
+// Record of one Jacobi solve for the reverse sweep: every phase's solver-body
+// copies (both sides of every manifold) and the row impulses after it.
+struct JacobiTape {
+    float4* copyLin;   // [2 * iterations][2 sides][maxPairs]
+    float4* copyAng;
+    float4* lamN;      // [iterations][maxPairs]: normal rows 0..3 after each normal phase
+    float4* lamF;      // [iterations][2][maxPairs]: friction rows 0..7 after each friction phase
+};
+
 // stage launchers (world.cu / broadphase.cu / narrowphase.cu / solver.cu)
 int launch_aabb_hash(b3World_t* w, cudaStream_t st);
 int launch_sort_and_cells(b3World_t* w, cudaStream_t st);
@@ -167,6 +176,9 @@ int launch_find_pairs(b3World_t* w, cudaStream_t st);
 int launch_narrowphase(b3World_t* w, cudaStream_t st);
 int launch_manifolds(b3World_t* w, cudaStream_t st);
 int launch_solver(b3World_t* w, cudaStream_t st);
+int launch_solver_taped(b3World_t* w, cudaStream_t st, const JacobiTape* tape);
 int launch_integrate(b3World_t* w, cudaStream_t st);
 int launch_world_stats(b3World_t* w, cudaStream_t st);
+// one eager step (world.cu); tape may be null
+int run_step(b3World_t* w, cudaStream_t st, const JacobiTape* tape);
 }  // namespace b3

@@ -35,59 +35,15 @@
 // iterations run in one persistent cooperative kernel separated by a grid
 // barrier whose wait is bounded. Rows are stored structure-of-arrays
 // (row slot major) so each phase streams them with coalesced float4 loads.
-#include "b3_math.cuh"
-#include "b3_world.h"
+#include "solver_common.cuh"
 
 #include <algorithm>
 #include <cfloat>
 
 using namespace b3m;
+using namespace b3solver;
 
 namespace {
-
-// Row storage: kRowSlots float4 streams of length maxManifolds.
-//  slot 0..3   header: (A,B,nRows,flags as int), (invMassA, invMassB, mu, -),
-//              (invInertiaA.xyz, countA), (invInertiaB.xyz, countB)
-//  normal row j (j<4):   4 + 3j + {0,1,2}
-//  friction row r (r<8): 16 + 3r + {0,1,2}; r = 2j + {0: dir2, 1: dir1}
-//  each row: (n.xyz, rhs), (r1xn.xyz, jacDiagABInv), (r2xn.xyz, applied)
-constexpr int kNormal0 = 4;
-constexpr int kFric0 = 16;
-
-struct SolverView {
-    float4* rows;       // [kRowSlots][cap]
-    int cap;            // manifold capacity (stride)
-    float4* copyLin;    // [2][cap]
-    float4* copyAng;    // [2][cap]
-    float4* avgLin;     // [N]
-    float4* avgAng;     // [N]
-    const uint32_t* incVals;   // sorted copy ids (2m + side)
-    const uint32_t* incStart;  // per body
-    const uint32_t* incEnd;
-    const int32_t* numManifolds;
-    int numBodies;
-};
-
-__device__ __forceinline__ float4& R(const SolverView& v, int slot, int m) {
-    return v.rows[(size_t)slot * v.cap + m];
-}
-
-// btPlaneSpace1 (LinearMath/btVector3.h), published construction of two
-// unit tangents orthogonal to n.
-__device__ __forceinline__ void plane_space(float3 n, float3& p, float3& q) {
-    const float SQRT12 = 0.7071067811865475244008443621048490f;
-    if (fabsf(n.z) > SQRT12) {
-        const float a = n.y * n.y + n.z * n.z;
-        const float k = rsqrtf(a);
-        p = make_float3(0.f, -n.z * k, n.y * k);
-        q = make_float3(a * k, -n.x * p.z, n.x * p.y);
-    } else {
-        const float a = n.x * n.x + n.y * n.y;
-        const float k = rsqrtf(a);
-        p = make_float3(-n.y * k, n.x * k, 0.f);
-        q = make_float3(-n.z * p.y, n.z * p.x, a * k);
-    }
-}
 
 // ---------------------------------------------------------------------------
 // Manifold compaction: manifold index = exclusive scan of per-pair flags.
@@ -250,87 +206,13 @@ __global__ void k_setup_rows(b3::BodiesDev Bd, SolverView V, const int* __restri
 // ---------------------------------------------------------------------------
 // Persistent Jacobi kernel
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ bool grid_barrier(uint32_t* count, uint32_t* gen, uint32_t nblocks,
-                                             int32_t* err, b3Counters* counters) {
-    __shared__ int ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        ok = 1;
-        const uint32_t g = b3dev::ld_acquire_u32(gen);
-        __threadfence();
-        const uint32_t arrived = atomicAdd(count, 1u);
-        if (arrived == nblocks - 1) {
-            atomicExch(count, 0u);
-            __threadfence();
-            b3dev::st_release_u32(gen, g + 1u);
-        } else {
-            int spins = 0;
-            while (b3dev::ld_acquire_u32(gen) == g) {
-                if (++spins > b3dev::kSpinLimit) {
-                    atomicExch(err, 1);
-                    atomicAdd(&counters->timeouts, 1);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(64);
-            }
-        }
-        if (*(volatile int32_t*)err) ok = 0;
-    }
-    __syncthreads();
-    return ok != 0;
-}
-
-__device__ __forceinline__ void solve_row(const float4 r0, const float4 r1, float4& r2, float lo, float hi,
-                                          float imA, float imB, float3 iiA, float3 iiB,
-                                          float3& dvA, float3& dwA, float3& dvB, float3& dwB) {
-    const float3 n = f3(r0), t1 = f3(r1), t2 = f3(r2);
-    const float rhs = r0.w, jac = r1.w, applied = r2.w;
-    float delta = rhs;  // - applied * cfm (cfm = 0)
-    const float dv1 = dot(n, dvA) + dot(t1, dwA);
-    const float dv2 = -dot(n, dvB) + dot(t2, dwB);
-    delta -= dv1 * jac;
-    delta -= dv2 * jac;
-    const float sum = applied + delta;
-    float na;
-    if (sum < lo) {
-        delta = lo - applied;
-        na = lo;
-    } else if (sum > hi) {
-        delta = hi - applied;
-        na = hi;
-    } else {
-        na = sum;
-    }
-    r2.w = na;
-    dvA += n * (imA * delta);
-    dwA += mulv(iiA, t1) * delta;
-    dvB += (-n * imB) * delta;
-    dwB += mulv(iiB, t2) * delta;
-}
-
-// Averaged delta velocity of body b over its copies in buffer buf
-// (averageVelocities, P2/btPgsJacobiSolver.cpp:1683-1720): copies in
-// manifold order, sum then multiply by 1/count.
-__device__ __forceinline__ void body_average(const SolverView& V, int b, int buf, float3& lin, float3& ang) {
-    const uint32_t s = V.incStart[b], e = V.incEnd[b];
-    float3 sl = make_float3(0.f, 0.f, 0.f), sa = sl;
-    for (uint32_t i = s; i < e; ++i) {
-        const uint32_t cid = V.incVals[i];
-        const size_t at = (size_t)(buf * 2 + (int)(cid & 1u)) * V.cap + (cid >> 1);
-        sl += f3(V.copyLin[at]);
-        sa += f3(V.copyAng[at]);
-    }
-    const float factor = 1.f / (float)(e - s);
-    lin = sl * factor;
-    ang = sa * factor;
-}
-
 // One phase for every manifold: start each copy from its body's average of
 // the previous phase (zero in the first phase), solve the manifold's normal
 // or friction rows in order, store both copies in buffer outBuf. A copy of a
 // manifold without rows keeps the average, as in the reference.
-__device__ void manifold_phase(const SolverView& V, int M, bool friction, bool first, int inBuf, int outBuf) {
+template <bool TAPE>
+__device__ void manifold_phase(const SolverView& V, int M, bool friction, bool first, int inBuf, int outBuf,
+                               const b3::JacobiTape& T, int phase) {
     for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
         const float4 h0 = R(V, 0, m);
         const int nRows = __float_as_int(h0.z);
@@ -341,6 +223,7 @@ __device__ void manifold_phase(const SolverView& V, int M, bool friction, bool f
             if (dyn & 1) body_average(V, A, inBuf, dvA, dwA);
             if (dyn & 2) body_average(V, B, inBuf, dvB, dwB);
         }
+        float lam[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         if (nRows > 0) {
             const float4 h1 = R(V, 1, m);
             const float4 h2 = R(V, 2, m);
@@ -354,10 +237,15 @@ __device__ void manifold_phase(const SolverView& V, int M, bool friction, bool f
                     float4 r2 = R(V, s + 2, m);
                     solve_row(r0, r1, r2, 0.f, 1e10f, imA, imB, iiA, iiB, dvA, dwA, dvB, dwB);
                     R(V, s + 2, m).w = r2.w;
+                    if (TAPE) lam[j] = r2.w;
                 }
             } else {
                 for (int j = 0; j < nRows; ++j) {
                     const float total = R(V, kNormal0 + 3 * j + 2, m).w;
+                    if (TAPE) {
+                        lam[2 * j] = R(V, kFric0 + 3 * (2 * j) + 2, m).w;
+                        lam[2 * j + 1] = R(V, kFric0 + 3 * (2 * j + 1) + 2, m).w;
+                    }
                     if (!(total > 0.f)) continue;
                     const float lim = mu * total;
                     for (int q = 0; q < 2; ++q) {
@@ -366,6 +254,7 @@ __device__ void manifold_phase(const SolverView& V, int M, bool friction, bool f
                         float4 r2 = R(V, s + 2, m);
                         solve_row(r0, r1, r2, -lim, lim, imA, imB, iiA, iiB, dvA, dwA, dvB, dwB);
                         R(V, s + 2, m).w = r2.w;
+                        if (TAPE) lam[2 * j + q] = r2.w;
                     }
                 }
             }
@@ -380,6 +269,22 @@ __device__ void manifold_phase(const SolverView& V, int M, bool friction, bool f
             V.copyLin[at] = f4(dvB);
             V.copyAng[at] = f4(dwB);
         }
+        if (TAPE) {
+            // every phase's copies and the impulses after it, for the
+            // reverse sweep (both sides, zero for a static side)
+            const size_t a0 = (size_t)(phase * 2 + 0) * V.cap + m, a1 = (size_t)(phase * 2 + 1) * V.cap + m;
+            T.copyLin[a0] = f4(dvA);
+            T.copyAng[a0] = f4(dwA);
+            T.copyLin[a1] = f4(dvB);
+            T.copyAng[a1] = f4(dwB);
+            const int it = phase >> 1;
+            if (!friction) {
+                T.lamN[(size_t)it * V.cap + m] = make_float4(lam[0], lam[1], lam[2], lam[3]);
+            } else {
+                T.lamF[(size_t)(2 * it) * V.cap + m] = make_float4(lam[0], lam[1], lam[2], lam[3]);
+                T.lamF[(size_t)(2 * it + 1) * V.cap + m] = make_float4(lam[4], lam[5], lam[6], lam[7]);
+            }
+        }
     }
 }
 
@@ -387,14 +292,15 @@ __device__ void manifold_phase(const SolverView& V, int M, bool friction, bool f
 // rows; the averaging of the reference happens at the start of the next
 // phase from the double-buffered copies, so phases are separated by one
 // bounded grid barrier each.
+template <bool TAPE>
 __global__ void __launch_bounds__(256)
-k_jacobi(SolverView V, int iterations, uint32_t* bar, int32_t* err, b3Counters* counters) {
+k_jacobi(SolverView V, int iterations, uint32_t* bar, int32_t* err, b3Counters* counters, b3::JacobiTape T) {
     const int M = *V.numManifolds;
     const uint32_t nb = gridDim.x;
     const int phases = 2 * iterations;
     for (int p = 0; p < phases; ++p) {
         if (p > 0 && !grid_barrier(bar, bar + 1, nb, err, counters)) return;
-        manifold_phase(V, M, (p & 1) != 0, p == 0, (p - 1) & 1, p & 1);
+        manifold_phase<TAPE>(V, M, (p & 1) != 0, p == 0, (p - 1) & 1, p & 1, T, p);
     }
 }
 
@@ -457,7 +363,9 @@ __global__ void k_integrate(b3::BodiesDev Bd, SolverView V, int finalBuf, Integr
     Bd.angVel[i] = w;
 }
 
-SolverView solver_view(b3World_t* w) {
+}  // namespace
+
+SolverView b3solver::solver_view(b3World_t* w) {
     SolverView V;
     V.rows = w->d.rows;
     V.cap = w->cfg.maxPairs;
@@ -472,8 +380,6 @@ SolverView solver_view(b3World_t* w) {
     V.numBodies = (int)w->bodies.size();
     return V;
 }
-
-}  // namespace
 
 namespace b3 {
 
@@ -508,7 +414,9 @@ int launch_manifolds(b3World_t* w, cudaStream_t st) {
     return B3_OK;
 }
 
-int launch_solver(b3World_t* w, cudaStream_t st) {
+int launch_solver(b3World_t* w, cudaStream_t st) { return launch_solver_taped(w, st, nullptr); }
+
+int launch_solver_taped(b3World_t* w, cudaStream_t st, const JacobiTape* tape) {
     if (w->cfg.maxPairs == 0 || w->bodies.empty()) return B3_OK;
     SolverView V = solver_view(w);
     SetupParams SP;
@@ -523,7 +431,8 @@ int launch_solver(b3World_t* w, cudaStream_t st) {
     B3_CUDA(cudaMemsetAsync(w->d.scalars + S_BAR_COUNT, 0, sizeof(int32_t) * 2, st));
     const int threads = w->solverThreads;
     int occ = 1;
-    B3_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_jacobi, threads, 0));
+    const void* kern = tape ? (const void*)k_jacobi<true> : (const void*)k_jacobi<false>;
+    B3_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, 0));
     occ = occ < 1 ? 1 : occ;
     occ = occ > 4 ? 4 : occ;
     // size the persistent grid to the expected manifold count (about 3 per
@@ -535,7 +444,8 @@ int launch_solver(b3World_t* w, cudaStream_t st) {
     uint32_t* bar = (uint32_t*)(w->d.scalars + S_BAR_COUNT);
     int32_t* err = w->d.scalars + S_ERR;
     b3Counters* ctr = w->d.counters;
-    void* args[] = {&V, &iters, &bar, &err, &ctr};
+    JacobiTape T = tape ? *tape : JacobiTape{};
+    void* args[] = {&V, &iters, &bar, &err, &ctr, &T};
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(threads);
@@ -546,7 +456,7 @@ int launch_solver(b3World_t* w, cudaStream_t st) {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    B3_CUDA(cudaLaunchKernelExC(&cfg, (const void*)k_jacobi, args));
+    B3_CUDA(cudaLaunchKernelExC(&cfg, kern, args));
     return B3_OK;
 }
 

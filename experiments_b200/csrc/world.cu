@@ -557,17 +557,20 @@ static int step_begin(b3World w, cudaStream_t st) {
     return B3_OK;
 }
 
-static int run_one_step(b3World w, cudaStream_t st) {
+// One eager step; with a tape, the Jacobi solve records its phases.
+int b3::run_step(b3World_t* w, cudaStream_t st, const JacobiTape* tape) {
     B3_TRY(step_begin(w, st));
     B3_TRY(b3::launch_aabb_hash(w, st));
     B3_TRY(b3::launch_sort_and_cells(w, st));
     B3_TRY(b3::launch_find_pairs(w, st));
     B3_TRY(b3::launch_narrowphase(w, st));
     B3_TRY(b3::launch_manifolds(w, st));
-    B3_TRY(b3::launch_solver(w, st));
+    B3_TRY(b3::launch_solver_taped(w, st, tape));
     B3_TRY(b3::launch_integrate(w, st));
     return B3_OK;
 }
+
+static int run_one_step(b3World w, cudaStream_t st) { return b3::run_step(w, st, nullptr); }
 
 static int run_one_step_timed(b3World w, cudaStream_t st) {
     cudaEvent_t ev[9];

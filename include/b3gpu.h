@@ -379,6 +379,9 @@ int b3_adjoint_backward(b3Adjoint a, const float* dPos4, const float* dQuat4, co
 /* Gradients w.r.t. initial linear/angular velocities (float4 per body),
  * masses and friction coefficients (float per body). Host outputs. */
 int b3_adjoint_gradients(b3Adjoint a, float* dLinVel4, float* dAngVel4, float* dMass, float* dFriction);
+/* Diagnostics of the last backward pass: contact points or axes that matched
+ * no feature of the clip (differentiated as rigidly attached instead). */
+int b3_adjoint_info(b3Adjoint a, int* unclassified);
 
 #ifdef __cplusplus
 }

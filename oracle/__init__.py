@@ -70,6 +70,9 @@ def lib(f32=False):
         L.or_pair_contact.argtypes = [_VP, C.c_int, C.c_int, C.POINTER(OrContact)]
         L.or_clip_reduce.argtypes = [_VP, C.c_int, C.c_int, _D, _D, _D, C.c_int, C.c_double, _D, _D, _I]
         L.or_solve_velocities.argtypes = [_VP, _D, _D]
+        L.or_active_hash.argtypes = [_VP, C.POINTER(C.c_uint64), C.c_int]
+        L.or_reset_active.argtypes = [_VP]
+        L.or_set_params_f64.argtypes = [_VP, _D, _D, _D]
         if f32:
             _lib32 = L
         else:
@@ -236,6 +239,24 @@ class OracleWorld:
         ang = np.zeros((self.n, 4))
         self.L.or_solve_velocities(self.h, _d(lin), _d(ang))
         return lin, ang
+
+    def set_params_f64(self, inv_mass=None, friction=None, inv_inertia3=None):
+        """Override body parameters in FP64 (None leaves a set unchanged)."""
+        keep = [None if a is None else np.ascontiguousarray(np.asarray(a, np.float64).reshape(-1))
+                for a in (inv_mass, friction, inv_inertia3)]
+        self.L.or_set_params_f64(self.h, *[None if a is None else _d(a) for a in keep])
+
+    def active_hash(self):
+        """Per-world signatures of the discrete choices since the last reset,
+        shape (worlds, 2): contact topology (pairs with manifolds, clip
+        sizes, reduced points) and row clamp states."""
+        nw = max(1, int(self.cfg.numWorlds))
+        out = np.zeros((nw, 2), np.uint64)
+        self.L.or_active_hash(self.h, out.ctypes.data_as(C.POINTER(C.c_uint64)), nw)
+        return out
+
+    def reset_active(self):
+        self.L.or_reset_active(self.h)
 
     def close(self):
         if self.h:

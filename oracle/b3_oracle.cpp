@@ -79,6 +79,7 @@ inline V qrot(Q q, V v) {
     return V(r.x, r.y, r.z);
 }
 inline V qinvrot(Q q, V v) { return qrot(Q{-q.x, -q.y, -q.z, q.w}, v); }
+inline uint64_t mix64(uint64_t h, uint64_t v) { return (h ^ (v + 0x9e3779b97f4a7c15ull)) * 0x100000001b3ull; }
 
 }  // namespace
 
@@ -124,7 +125,7 @@ struct or_world {
     int n;
     int cellBits;
     // static body data
-    std::vector<float> invMass, friction, restitution;
+    std::vector<Real> invMass, friction, restitution;  // set from FP32 inputs, or FP64 by or_set_params_f64
     std::vector<int> col, worldId, isLarge;
     std::vector<Real> invInertia;  // 3 per body
     // shapes
@@ -142,6 +143,11 @@ struct or_world {
     std::vector<or_contact> contacts;        // manifolds in pair order
     std::vector<Real> avgLin, avgAng;        // 3 per body (sum/count after the last average)
     std::vector<int> count;                  // copies per body
+    // per-world signature of the discrete choices (pairs with manifolds,
+    // clip size and reduced point indices, row clamp states), for telling
+    // which worlds keep their active set under a perturbation
+    std::vector<uint64_t> activeHash;   // row clamp states
+    std::vector<uint64_t> topoHash;     // pairs with manifolds, clip sizes, reduced points
     long long pairOverflow, cellOverflow;
 };
 
@@ -336,8 +342,12 @@ void project(const or_world* w, const or_poly& h, const Body& b, V dir, Real& mn
 }
 
 // findSeparatingAxis (sat.cl:497-551); returns false if a face axis separates
+// feature of the chosen separating axis (A face i, 1000 + B face i, or
+// 100000 + 1000 e0 + e1 for an edge pair), for the active-set signature
+int g_axisId = -1;
+
 bool face_axes(const or_world* w, const or_poly& hA, const or_poly& hB, const Body& A, const Body& B, V D,
-               V& sep, Real& dmin) {
+               V& sep, Real& dmin, int idBase) {
     for (int i = 0; i < hA.numFaces; ++i) {
         const or_face& f = w->faces[hA.faceOffset + i];
         V n = qrot(A.q, V(f.plane[0], f.plane[1], f.plane[2]));
@@ -351,6 +361,7 @@ bool face_axes(const or_world* w, const or_poly& hA, const or_poly& hB, const Bo
         if (d < dmin) {
             dmin = d;
             sep = n;
+            g_axisId = idBase + i;
         }
     }
     if (dot(-D, sep) > 0) sep = -sep;
@@ -378,6 +389,7 @@ void edge_axes(const or_world* w, const or_poly& hA, const or_poly& hB, const Bo
             if (d < dmin) {
                 dmin = d;
                 sep = c;
+                g_axisId = 100000 + 1000 * e0 + e1;
             }
         }
     }
@@ -587,8 +599,9 @@ bool contact_for_pair(const or_world* w, int pairIndex, int A, int B, or_contact
     bool haveAxis = false;
     {
         // track whether any axis was accepted (dmin updated)
-        if (!face_axes(w, hA, hB, a, b, D, sep, dmin)) return false;
-        if (!face_axes(w, hB, hA, b, a, D, sep, dmin)) return false;
+        g_axisId = -1;
+        if (!face_axes(w, hA, hB, a, b, D, sep, dmin, 0)) return false;
+        if (!face_axes(w, hB, hA, b, a, D, sep, dmin, 1000)) return false;
         edge_axes(w, hA, hB, a, b, D, sep, dmin);
         haveAxis = dmin < std::numeric_limits<Real>::max();
     }
@@ -600,6 +613,7 @@ bool contact_for_pair(const or_world* w, int pairIndex, int A, int B, or_contact
     int idx[4];
     const int nr = reduce_manifold(pts, nrm, idx);
     memset(&out, 0, sizeof(out));
+    out.pad = (int)std::min<size_t>(pts.size(), 127) | (idx[0] << 7) | (idx[1] << 13) | (idx[2] << 19) | (idx[3] << 25);
     for (int k = 0; k < nr; ++k) {
         const P4& q = pts[idx[k]];
         out.pos[k][0] = q.x; out.pos[k][1] = q.y; out.pos[k][2] = q.z; out.pos[k][3] = q.w;
@@ -617,7 +631,14 @@ void stage_narrowphase(or_world* w) {
     const int np = (int)w->pairs.size() / 2;
     for (int p = 0; p < np; ++p) {
         or_contact c;
-        if (contact_for_pair(w, p, w->pairs[2 * p], w->pairs[2 * p + 1], c)) w->contacts.push_back(c);
+        if (contact_for_pair(w, p, w->pairs[2 * p], w->pairs[2 * p + 1], c)) {
+            w->contacts.push_back(c);
+            const int A = std::abs(c.bodyA), B = std::abs(c.bodyB);
+            uint64_t& h = w->topoHash[w->worldId[A]];
+            h = mix64(h, ((uint64_t)A << 32) | (uint32_t)B);
+            h = mix64(h, (uint32_t)c.pad);
+            h = mix64(h, (uint64_t)(int64_t)g_axisId);
+        }
     }
 }
 
@@ -655,7 +676,8 @@ void plane_space(V n, V& p, V& q) {
     }
 }
 
-void solve_row(Row& c, Copy& A, Copy& B, Real imA, Real imB, V iiA, V iiB) {
+int solve_row(Row& c, Copy& A, Copy& B, Real imA, Real imB, V iiA, V iiB) {
+    int state = 0;
     Real delta = c.rhs;  // - applied * cfm (0)
     const Real dv1 = dot(c.n, A.dv) + dot(c.t1, A.dw);
     const Real dv2 = -dot(c.n, B.dv) + dot(c.t2, B.dw);
@@ -665,9 +687,11 @@ void solve_row(Row& c, Copy& A, Copy& B, Real imA, Real imB, V iiA, V iiB) {
     if (sum < c.lo) {
         delta = c.lo - c.applied;
         c.applied = c.lo;
+        state = 1;
     } else if (sum > c.hi) {
         delta = c.hi - c.applied;
         c.applied = c.hi;
+        state = 2;
     } else {
         c.applied = sum;
     }
@@ -675,6 +699,7 @@ void solve_row(Row& c, Copy& A, Copy& B, Real imA, Real imB, V iiA, V iiB) {
     A.dw = A.dw + mulv(iiA, c.t1) * delta;
     B.dv = B.dv + (-c.n * imB) * delta;
     B.dw = B.dw + mulv(iiB, c.t2) * delta;
+    return state;
 }
 
 void stage_solve(or_world* w) {
@@ -762,6 +787,10 @@ void stage_solve(or_world* w) {
             m.normal.push_back(row);
             V d1v = vel - n * relv0, d2v;
             const Real lat = dot(d1v, d1v);
+            // the setup's own branches belong to the active set too
+            w->activeHash[w->worldId[m.A]] = mix64(w->activeHash[w->worldId[m.A]],
+                                                   16 + (penetration > 0 ? 1 : 0) + (rest > 0 ? 2 : 0) +
+                                                       (lat > (Real)FLT_EPSILON ? 4 : 0) + 8 * j);
             if (lat > (Real)FLT_EPSILON) {
                 d1v = d1v * (1.0 / std::sqrt(lat));
                 d2v = normalize(cross(d1v, n));
@@ -814,7 +843,8 @@ void stage_solve(or_world* w) {
             const bool dynA = imA != 0, dynB = imB != 0;
             const V iiA = dynA ? V(w->invInertia[3 * m.A], w->invInertia[3 * m.A + 1], w->invInertia[3 * m.A + 2]) : V();
             const V iiB = dynB ? V(w->invInertia[3 * m.B], w->invInertia[3 * m.B + 1], w->invInertia[3 * m.B + 2]) : V();
-            for (Row& r : m.normal) solve_row(r, copies[m.a], copies[m.b], imA, imB, iiA, iiB);
+            uint64_t& h = w->activeHash[w->worldId[m.A]];
+            for (Row& r : m.normal) h = mix64(h, (uint64_t)solve_row(r, copies[m.a], copies[m.b], imA, imB, iiA, iiB));
         }
         average();
         for (MRows& m : ms) {
@@ -822,12 +852,15 @@ void stage_solve(or_world* w) {
             const bool dynA = imA != 0, dynB = imB != 0;
             const V iiA = dynA ? V(w->invInertia[3 * m.A], w->invInertia[3 * m.A + 1], w->invInertia[3 * m.A + 2]) : V();
             const V iiB = dynB ? V(w->invInertia[3 * m.B], w->invInertia[3 * m.B + 1], w->invInertia[3 * m.B + 2]) : V();
+            uint64_t& h = w->activeHash[w->worldId[m.A]];
             for (Row& r : m.fric) {
                 const Real total = m.normal[r.normalIndex].applied;
                 if (total > 0) {
                     r.lo = -(r.mu * total);
                     r.hi = r.mu * total;
-                    solve_row(r, copies[m.a], copies[m.b], imA, imB, iiA, iiB);
+                    h = mix64(h, 4 + (uint64_t)solve_row(r, copies[m.a], copies[m.b], imA, imB, iiA, iiB));
+                } else {
+                    h = mix64(h, 8);
                 }
             }
         }
@@ -912,6 +945,8 @@ or_world* or_world_create(const or_config* cfg, int n, const float* invMass, con
     w->restitution.assign(restitution, restitution + n);
     w->col.assign(collidable, collidable + n);
     w->worldId.assign(worldId, worldId + n);
+    w->activeHash.assign(std::max(1, cfg->numWorlds), 0ull);
+    w->topoHash.assign(std::max(1, cfg->numWorlds), 0ull);
     w->isLarge.assign(isLarge, isLarge + n);
     w->invInertia.resize(3 * (size_t)n);
     for (int i = 0; i < n; ++i)
@@ -931,6 +966,31 @@ or_world* or_world_create(const or_config* cfg, int n, const float* invMass, con
 }
 
 void or_world_destroy(or_world* w) { delete w; }
+
+// FP64 body parameters (finite differences need perturbations finer than
+// FP32 inputs resolve): inverse masses, friction coefficients and local
+// inverse inertia diagonals (3 per body); NULL leaves a set unchanged.
+void or_set_params_f64(or_world* w, const double* invMass, const double* friction, const double* invInertia3) {
+    for (int i = 0; i < w->n; ++i) {
+        if (invMass) w->invMass[i] = (Real)invMass[i];
+        if (friction) w->friction[i] = (Real)friction[i];
+        if (invInertia3)
+            for (int k = 0; k < 3; ++k) w->invInertia[3 * i + k] = (Real)invInertia3[3 * i + k];
+    }
+}
+
+// Per-world signatures of the discrete choices since the last reset:
+// out[2k] = contact topology, out[2k+1] = row clamp states.
+void or_active_hash(or_world* w, uint64_t* out, int numWorlds) {
+    for (int k = 0; k < numWorlds && k < (int)w->activeHash.size(); ++k) {
+        out[2 * k] = w->topoHash[k];
+        out[2 * k + 1] = w->activeHash[k];
+    }
+}
+void or_reset_active(or_world* w) {
+    std::fill(w->activeHash.begin(), w->activeHash.end(), 0ull);
+    std::fill(w->topoHash.begin(), w->topoHash.end(), 0ull);
+}
 
 void or_set_state_f32(or_world* w, const float* pos4, const float* quat4, const float* lin4, const float* ang4) {
     for (size_t i = 0; i < 4 * (size_t)w->n; ++i) {

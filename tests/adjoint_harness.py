@@ -1,0 +1,131 @@
+"""Test harness for the adjoint form: FP64 central differences on the oracle,
+the product's reverse sweep, and a torch.autograd.Function over it (the
+library itself does not depend on torch)."""
+import copy
+
+import numpy as np
+
+import oracle
+from experiments_b200 import b3, scenes
+
+
+def make_oracle(host_ctx, scene):
+    """Oracle world of a scene plus the per-body inverse inertia diagonal of
+    the registration (FP64 copy)."""
+    w = b3.PhysicsWorld(host_ctx, scenes.world_config(scene))
+    scenes.register_scene(w, scene)
+    o = oracle.oracle_from_world(w, scene)
+    ii = w.inertias()[:, :3].astype(np.float64)
+    w.close()
+    return o, ii
+
+
+def oracle_state_at(host_ctx, scene, steps):
+    """Oracle state after `steps` steps, rounded to FP32 (the state both sides
+    start from)."""
+    o, _ = make_oracle(host_ctx, scene)
+    o.step(steps)
+    st = [a.astype(np.float32).astype(np.float64) for a in o.state()]
+    o.close()
+    return st
+
+
+def world_functional(scene, state, seeds):
+    """Per-world linear functional sum <seed, state> over (pos, quat, lin, ang)."""
+    wid = np.asarray(scene.world)
+    out = np.zeros(scene.num_worlds)
+    for k in range(4):
+        cols = 4 if k == 1 else 3
+        contrib = np.sum(seeds[k][:, :cols] * state[k][:, :cols], axis=1)
+        np.add.at(out, wid, contrib)
+    return out
+
+
+def oracle_run(host_ctx, scene, state, steps, seeds, kind=None, delta=None, eps=0.0):
+    """Run the oracle `steps` steps from `state` with one parameter set
+    perturbed by eps * delta in FP64; returns the per-world functional and
+    the per-world active-set signatures."""
+    o, ii = make_oracle(host_ctx, scene)
+    pos, quat, lin, ang = [a.copy() for a in state]
+    m = np.asarray(scene.mass, np.float64)
+    im = np.where(m > 0, 1.0 / np.where(m > 0, m, 1), 0.0)
+    if kind == "lin":
+        lin[:, :3] += eps * delta
+    elif kind == "ang":
+        ang[:, :3] += eps * delta
+    elif kind == "mass":
+        m2 = m + eps * delta
+        im2 = np.where(m > 0, 1.0 / np.where(m > 0, m2, 1), 0.0)
+        scale = np.where(im > 0, im2 / np.where(im > 0, im, 1), 0.0)
+        o.set_params_f64(inv_mass=im2, inv_inertia3=ii * scale[:, None])
+    elif kind == "friction":
+        o.set_params_f64(friction=np.asarray(scene.friction, np.float64) + eps * delta)
+    o.set_state_f64(pos, quat, lin, ang)
+    o.reset_active()
+    o.step(steps)
+    st = o.state()
+    h = o.active_hash()
+    o.close()
+    return world_functional(scene, st, seeds), h
+
+
+def gpu_adjoint(ctx, scene, state, steps, seeds, checkpoint_every=16):
+    """The product's gradients of the per-world functional."""
+    w = scenes.build_world(ctx, scene, useGraph=1)
+    w.write_state(*[np.asarray(a, np.float32) for a in state])
+    adj = b3.Adjoint(w, steps, checkpoint_every)
+    adj.forward()
+    final = [a.astype(np.float64) for a in w.read_state()]
+    adj.backward(*[np.asarray(s, np.float32) for s in seeds])
+    g = adj.gradients()
+    g["unclassified"] = adj.unclassified()
+    g["final"] = final
+    adj.close()
+    w.close()
+    return g
+
+
+def random_seeds(scene, rng):
+    dyn = (np.asarray(scene.mass) > 0).astype(np.float64)
+    seeds = [rng.normal(size=(scene.n, 4)) * dyn[:, None] for _ in range(4)]
+    for k in (0, 2, 3):
+        seeds[k][:, 3] = 0.0
+    return seeds
+
+
+class Rollout:
+    """torch.autograd.Function over a batched world: (initial linear and
+    angular velocities, masses, friction) -> final positions."""
+
+    @staticmethod
+    def make(ctx, scene, steps, checkpoint_every=16):
+        import torch
+
+        class _F(torch.autograd.Function):
+            @staticmethod
+            def forward(fctx, lin0, ang0, mass, friction):
+                sc = copy.copy(scene)
+                sc.lin = lin0.detach().cpu().numpy().astype(np.float64)
+                sc.ang = ang0.detach().cpu().numpy().astype(np.float64)
+                sc.mass = mass.detach().cpu().numpy().astype(np.float64)
+                sc.friction = friction.detach().cpu().numpy().astype(np.float64)
+                w = scenes.build_world(ctx, sc, useGraph=1)
+                w.write_velocities(sc.lin, sc.ang)
+                adj = b3.Adjoint(w, steps, checkpoint_every)
+                adj.forward()
+                pos = torch.from_numpy(w.read_state()[0][:, :3].astype(np.float64))
+                fctx.adj, fctx.world = adj, w
+                return pos
+
+            @staticmethod
+            def backward(fctx, gpos):
+                adj = fctx.adj
+                adj.backward(d_pos=gpos.detach().cpu().numpy())
+                g = adj.gradients()
+                adj.close()
+                fctx.world.close()
+                return (torch.from_numpy(g["lin"].astype(np.float64)), torch.from_numpy(g["ang"].astype(np.float64)),
+                        torch.from_numpy(g["mass"].astype(np.float64)),
+                        torch.from_numpy(g["friction"].astype(np.float64)))
+
+        return _F

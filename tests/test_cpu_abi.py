@@ -137,3 +137,15 @@ def test_batch_world_offsets(host_ctx):
     counts = np.bincount(np.asarray(sc.world), minlength=16)
     assert np.array_equal(np.diff(off), counts)
     w.close()
+
+
+def test_adjoint_call_order(host_ctx):
+    lib = b3.load()
+    w = b3.PhysicsWorld(host_ctx, b3.default_config())
+    a = C.c_void_p()
+    # bodies not written (and no device): the adjoint cannot be created
+    assert lib.b3_adjoint_create(w.h, 10, 4, C.byref(a)) == 5
+    assert lib.b3_adjoint_create(w.h, 0, 4, C.byref(a)) == 1
+    assert lib.b3_adjoint_forward(None, None) == 1
+    assert lib.b3_adjoint_gradients(None, None, None, None, None) == 1
+    w.close()
