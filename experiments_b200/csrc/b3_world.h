@@ -74,6 +74,9 @@ struct DevBuffers {
     // narrowphase
     b3Contact4* contacts = nullptr;   // one slot per pair
     uint32_t* manifoldFlag = nullptr; // per pair: 1 if a manifold was emitted
+    float4* pairSep = nullptr;        // per pair: FP32 separating axis of the sweep
+    int* npFast = nullptr;            // queue: pairs whose axis the FP32 sweep decided
+    int* npSlow = nullptr;            // queue: pairs for the float-float path
     uint32_t* manifoldScan = nullptr; // exclusive scan of the flags
     int* manifoldPair = nullptr;      // manifold -> pair slot
     // solver
@@ -107,6 +110,10 @@ enum ScalarSlot {
     S_BAR_GEN = 7,
     S_TILE = 8,
     S_NP_WORK = 9,
+    S_NP_FAST = 10,       // pairs queued for the FP32 clip
+    S_NP_SLOW = 11,       // pairs queued for the float-float path
+    S_NP_WORK2 = 12,
+    S_NP_WORK3 = 13,
     S_NUM_SCALARS = 16
 };
 

@@ -220,7 +220,10 @@ __device__ __noinline__ bool axis_ff(const PairCtx& c, const b3::ShapesDev& S, i
 // FP32 sweep over all axes by the warp, then float-float refinement of every
 // axis whose FP32 depth is within delta of the minimum. Returns false if a
 // face axis separates or no axis exists.
-__device__ __noinline__ bool find_axis(PairCtx& c, const b3::ShapesDev& S, WarpScratch& W, ff3& sep, int* ovfCounter) {
+// FP32 part: 0 = separated (or no axis), 1 = decided in FP32 (sepf),
+// 2 = near-minimum candidates left in W.cand[0..count) for float-float.
+__device__ __forceinline__ int sweep_axes(PairCtx& c, const b3::ShapesDev& S, WarpScratch& W, float3& sepf,
+                                          int& count, int* ovfCounter) {
     const int lane = threadIdx.x & 31;
     const b3ConvexPolyhedron& pa = *c.pa;
     const b3ConvexPolyhedron& pb = *c.pb;
@@ -288,21 +291,21 @@ __device__ __noinline__ bool find_axis(PairCtx& c, const b3::ShapesDev& S, WarpS
             float sm0 = sepMin;
             int dz = 0;
             warp_argmin(sm0, dz);
-            if (sm0 < -delta) return false;
+            if (sm0 < -delta) return 0;
         }
     }
     // clearly separated by a face axis
     float sm = sepMin;
     int dummy = 0;
     warp_argmin(sm, dummy);
-    if (sm < -delta) return false;
+    if (sm < -delta) return 0;
     float best = upper;
     int bi = 0;
     warp_argmin(best, bi);
-    if (!(best < FLT_MAX)) return false;
+    if (!(best < FLT_MAX)) return 0;
     const float lim = best;
     // collect candidates
-    int count = 0;
+    count = 0;
     bool overflow = kd[kKeep - 1] <= lim || ambOverflow;
     for (int k = 0; k < kKeep + 2; ++k) {
         const int id = k < kKeep ? ki[k] : amb[k - kKeep];
@@ -345,9 +348,8 @@ __device__ __noinline__ bool find_axis(PairCtx& c, const b3::ShapesDev& S, WarpS
         if (axis_f32(c, S, idx, D, rel, delta, n, d, err, isFace) && err <= 31.f * delta &&
             fabsf(dot(D, n)) > 1e-5f * (length(D) + 1e-3f)) {
             if (dot(-D, n) > 0.f) n = -n;
-            sep = mk3(n.x, n.y, n.z);
-            c.haveFF = false;
-            return true;
+            sepf = n;
+            return 1;
         }
     }
     // Several candidates that are the same direction within 1e-5 (parallel
@@ -381,12 +383,20 @@ __device__ __noinline__ bool find_axis(PairCtx& c, const b3::ShapesDev& S, WarpS
             float3 w = make_float3(__shfl_sync(0xffffffffu, n.x, src), __shfl_sync(0xffffffffu, n.y, src),
                                    __shfl_sync(0xffffffffu, n.z, src));
             if (dot(-D, w) > 0.f) w = -w;
-            sep = mk3(w.x, w.y, w.z);
-            c.haveFF = false;
-            return true;
+            sepf = w;
+            return 1;
         }
     }
-    if (lane == 0) ++W.refinedAxes;
+    return 2;
+}
+
+// float-float re-ranking of the sweep's candidates
+__device__ __noinline__ bool refine_axes(PairCtx& c, const b3::ShapesDev& S, WarpScratch& W, int count, ff3& sep) {
+    const int lane = threadIdx.x & 31;
+    const b3ConvexPolyhedron& pa = *c.pa;
+    const b3ConvexPolyhedron& pb = *c.pb;
+    const float3 lcA = make_float3(pa.localCenter[0], pa.localCenter[1], pa.localCenter[2]);
+    const float3 lcB = make_float3(pb.localCenter[0], pb.localCenter[1], pb.localCenter[2]);
     // float-float refinement of the candidates (matrices built only for
     // pairs that got this far)
     c.FA = quat_mat(c.qA);
@@ -426,6 +436,22 @@ __device__ __noinline__ bool find_axis(PairCtx& c, const b3::ShapesDev& S, WarpS
     sep.z.lo = __shfl_sync(0xffffffffu, bn.z.lo, src);
     if (dot3(neg3(Dff), sep).hi > 0.f) sep = neg3(sep);
     return true;
+}
+
+// Separating-axis search: the FP32 sweep, then the float-float re-ranking
+// when the sweep leaves near-minimum candidates.
+__device__ __noinline__ bool find_axis(PairCtx& c, const b3::ShapesDev& S, WarpScratch& W, ff3& sep, int* ovfCounter) {
+    float3 sepf;
+    int count = 0;
+    const int r = sweep_axes(c, S, W, sepf, count, ovfCounter);
+    if (r == 0) return false;
+    if (r == 1) {
+        sep = mk3(sepf.x, sepf.y, sepf.z);
+        c.haveFF = false;
+        return true;
+    }
+    if ((threadIdx.x & 31) == 0) ++W.refinedAxes;
+    return refine_axes(c, S, W, count, sep);
 }
 
 // One Sutherland-Hodgman step in float-float (clipFace,
@@ -839,58 +865,188 @@ __device__ __noinline__ int4 reduce_manifold(const FfVert* p, int n, ff3 nearNor
     return idx;
 }
 
+// Per-pair context from the pair list; false for pairs the narrowphase skips
+// (two static bodies, sat.cl:944-948, or non-hull collidables).
+__device__ __forceinline__ bool pair_setup(PairCtx& c, int2 pr, const b3::BodiesDev& Bd, const b3::ShapesDev& S) {
+    c.A = pr.x;
+    c.B = pr.y;
+    c.invMassA = Bd.invMass[c.A];
+    c.invMassB = Bd.invMass[c.B];
+    const b3Collidable colA = S.cols[Bd.collidable[c.A]];
+    const b3Collidable colB = S.cols[Bd.collidable[c.B]];
+    if ((c.invMassA == 0.f && c.invMassB == 0.f) || colA.shapeType != B3_SHAPE_CONVEX_HULL ||
+        colB.shapeType != B3_SHAPE_CONVEX_HULL)
+        return false;
+    c.pa = &S.polys[colA.shapeIndex];
+    c.pb = &S.polys[colB.shapeIndex];
+    c.qA = Bd.quat[c.A];
+    c.qB = Bd.quat[c.B];
+    c.RA = quat_to_mat(c.qA);
+    c.RB = quat_to_mat(c.qB);
+    c.posA = f3(Bd.pos[c.A]);
+    c.posB = f3(Bd.pos[c.B]);
+    c.haveFF = false;
+    return true;
+}
+
+// Contact4 of pair p from the kept points pts[0..nOut) and the chosen
+// indices (newContactReductionKernel, P2/satClipHullContacts.cl:1958-2039).
+__device__ __forceinline__ void emit_contact(int p, const PairCtx& c, const FfVert* pts, int nRed, int4 idx,
+                                             float3 nrm, const b3::BodiesDev& Bd, const NpParams& P,
+                                             b3Contact4* __restrict__ contacts, uint32_t* __restrict__ manifoldFlag) {
+    const int lane = threadIdx.x & 31;
+    b3Contact4* out = &contacts[p];
+    if (lane < nRed) {
+        const int k = lane == 0 ? idx.x : lane == 1 ? idx.y : lane == 2 ? idx.z : idx.w;
+        const FfVert q = pts[k];
+        *reinterpret_cast<float4*>(&out->worldPos[lane][0]) =
+            make_float4(q.xh + q.xl, q.yh + q.yl, q.zh + q.zl, q.wh + q.wl);
+    } else if (lane < 4) {
+        *reinterpret_cast<float4*>(&out->worldPos[lane][0]) = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    if (lane == 4) {
+        *reinterpret_cast<float4*>(&out->worldNormal[0]) = make_float4(nrm.x, nrm.y, nrm.z, (float)nRed);
+        out->friction = combine_friction(Bd.friction[c.A], Bd.friction[c.B], P.frictionCombine);
+        out->pairIndex = p;
+        out->bodyAPtrAndSignBit = c.invMassA == 0.f ? -c.A : c.A;
+        out->bodyBPtrAndSignBit = c.invMassB == 0.f ? -c.B : c.B;
+        manifoldFlag[p] = 1u;
+    }
+}
+
+__device__ __forceinline__ int next_work(int32_t* counter, int limit) {
+    int w = 0;
+    if ((threadIdx.x & 31) == 0) w = atomicAdd(counter, kChunk);
+    w = __shfl_sync(0xffffffffu, w, 0);
+    return w < limit ? w : -1;
+}
+
+__device__ __forceinline__ void push(int* queue, int32_t* count, int p) {
+    if ((threadIdx.x & 31) == 0) queue[atomicAdd(count, 1)] = p;
+}
+
+// Stage 1, every pair: the FP32 separating-axis sweep. Separated pairs are
+// finished here; pairs whose axis the sweep decides go to the FP32 clip
+// queue with that axis; pairs with near-minimum candidates go to the
+// float-float queue.
 __global__ void __launch_bounds__(128)
-k_narrowphase(const int2* __restrict__ pairs, const int32_t* __restrict__ numPairsDev, b3::BodiesDev Bd,
-              b3::ShapesDev S, NpParams P, b3Contact4* __restrict__ contacts, uint32_t* __restrict__ manifoldFlag,
-              int32_t* __restrict__ workCounter, b3Counters* __restrict__ counters) {
+k_np_sweep(const int2* __restrict__ pairs, const int32_t* __restrict__ numPairsDev, b3::BodiesDev Bd,
+           b3::ShapesDev S, uint32_t* __restrict__ manifoldFlag, float4* __restrict__ pairSep,
+           int* __restrict__ fastQ, int* __restrict__ slowQ, int32_t* __restrict__ scalars,
+           b3Counters* __restrict__ counters) {
     extern __shared__ __align__(16) unsigned char np_smem[];
     const int lane = threadIdx.x & 31;
     WarpScratch& W = reinterpret_cast<WarpScratch*>(np_smem)[threadIdx.x >> 5];
     const int numPairs = *numPairsDev;
+    for (;;) {
+        const int chunk = next_work(scalars + b3::S_NP_WORK, numPairs);
+        if (chunk < 0) break;
+        const int chunkEnd = min(chunk + kChunk, numPairs);
+        for (int p = chunk; p < chunkEnd; ++p) {
+            PairCtx c;
+            int r = 0;
+            float3 sepf = make_float3(0.f, 0.f, 0.f);
+            if (pair_setup(c, pairs[p], Bd, S)) {
+                int count = 0;
+                r = sweep_axes(c, S, W, sepf, count, &counters->clipOverflow);
+            }
+            if (r == 0) {
+                if (lane == 0) manifoldFlag[p] = 0u;
+            } else if (r == 1) {
+                if (lane == 0) pairSep[p] = make_float4(sepf.x, sepf.y, sepf.z, 0.f);
+                push(fastQ, scalars + b3::S_NP_FAST, p);
+            } else {
+                push(slowQ, scalars + b3::S_NP_SLOW, p);
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// Stage 2, pairs with an FP32 axis: face selection, clipping and reduction
+// in FP32 with error bounds; any doubt sends the pair to the float-float
+// queue instead.
+__global__ void __launch_bounds__(128)
+k_np_clip(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, NpParams P,
+          const float4* __restrict__ pairSep, const int* __restrict__ fastQ, int* __restrict__ slowQ,
+          b3Contact4* __restrict__ contacts, uint32_t* __restrict__ manifoldFlag, int32_t* __restrict__ scalars,
+          b3Counters* __restrict__ counters) {
+    extern __shared__ __align__(16) unsigned char np_smem[];
+    const int lane = threadIdx.x & 31;
+    WarpScratch& W = reinterpret_cast<WarpScratch*>(np_smem)[threadIdx.x >> 5];
+    const int nFast = scalars[b3::S_NP_FAST];
+    for (;;) {
+        const int chunk = next_work(scalars + b3::S_NP_WORK2, nFast);
+        if (chunk < 0) break;
+        const int chunkEnd = min(chunk + kChunk, nFast);
+        for (int q = chunk; q < chunkEnd; ++q) {
+            const int p = fastQ[q];
+            PairCtx c;
+            pair_setup(c, pairs[p], Bd, S);
+            const float4 s4 = pairSep[p];
+            const float3 sepf = make_float3(s4.x, s4.y, s4.z);
+            const ff3 sep = mk3(sepf.x, sepf.y, sepf.z);
+            // incident face of B: max dot(nB, sep); reference face of A: min dot(nA, sep)
+            const int bi = select_face(S, c, false, sepf, sep, -1.f);
+            const int ai = select_face(S, c, true, sepf, sep, 1.f);
+            int buf = 0;
+            bool slow = false;
+            const int nOut = clip_f32(c, S, P, ai, bi, W, &buf, &slow, &counters->clipOverflow);
+            int4 idx = make_int4(0, 1, 2, 3);
+            int nRed = nOut;
+            if (!slow && nOut > 4) {
+                bool tie = false;
+                idx = reduce_f32(W.poly[buf], min(nOut, kMaxPoly), -sepf, &tie);
+                slow = tie;
+                nRed = 4;
+            }
+            if (slow) {
+                push(slowQ, scalars + b3::S_NP_SLOW, p);
+            } else if (nOut > 0) {
+                emit_contact(p, c, W.poly[buf], nRed, idx, -sepf, Bd, P, contacts, manifoldFlag);
+            } else if (lane == 0) {
+                manifoldFlag[p] = 0u;
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// Stage 3, the pairs either stage handed on: the whole chain with
+// float-float refinement of the axis, the faces, the clip and the reduction.
+__global__ void __launch_bounds__(128)
+k_np_exact(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, NpParams P,
+           const int* __restrict__ slowQ, b3Contact4* __restrict__ contacts, uint32_t* __restrict__ manifoldFlag,
+           int32_t* __restrict__ scalars, b3Counters* __restrict__ counters) {
+    extern __shared__ __align__(16) unsigned char np_smem[];
+    const int lane = threadIdx.x & 31;
+    WarpScratch& W = reinterpret_cast<WarpScratch*>(np_smem)[threadIdx.x >> 5];
+    const int nSlow = scalars[b3::S_NP_SLOW];
     if (lane == 0) {
         W.refinedAxes = 0;
         W.refinedClips = 0;
     }
     __syncwarp();
     for (;;) {
-        int chunk = 0;
-        if (lane == 0) chunk = atomicAdd(workCounter, kChunk);
-        chunk = __shfl_sync(0xffffffffu, chunk, 0);
-        if (chunk >= numPairs) break;
-        const int chunkEnd = min(chunk + kChunk, numPairs);
-        for (int p = chunk; p < chunkEnd; ++p) {
-            const int2 pr = pairs[p];
+        const int chunk = next_work(scalars + b3::S_NP_WORK3, nSlow);
+        if (chunk < 0) break;
+        const int chunkEnd = min(chunk + kChunk, nSlow);
+        for (int q = chunk; q < chunkEnd; ++q) {
+            const int p = slowQ[q];
             PairCtx c;
-            c.A = pr.x;
-            c.B = pr.y;
-            c.invMassA = Bd.invMass[c.A];
-            c.invMassB = Bd.invMass[c.B];
-            const b3Collidable colA = S.cols[Bd.collidable[c.A]];
-            const b3Collidable colB = S.cols[Bd.collidable[c.B]];
+            pair_setup(c, pairs[p], Bd, S);
             int nOut = 0, buf = 0;
             ff3 sep = mk3(0.f, 0.f, 0.f);
-            if (!(c.invMassA == 0.f && c.invMassB == 0.f) && colA.shapeType == B3_SHAPE_CONVEX_HULL &&
-                colB.shapeType == B3_SHAPE_CONVEX_HULL) {
-                c.pa = &S.polys[colA.shapeIndex];
-                c.pb = &S.polys[colB.shapeIndex];
-                c.qA = Bd.quat[c.A];
-                c.qB = Bd.quat[c.B];
-                c.RA = quat_to_mat(c.qA);
-                c.RB = quat_to_mat(c.qB);
-                c.posA = f3(Bd.pos[c.A]);
-                c.posB = f3(Bd.pos[c.B]);
-                c.haveFF = false;
-                if (find_axis(c, S, W, sep, &counters->clipOverflow)) {
-                    const float3 sepf = to_f3(sep);
-                    // incident face of B: max dot(nB, sep); reference face of A: min dot(nA, sep)
-                    const int bi = select_face(S, c, false, sepf, sep, -1.f);
-                    const int ai = select_face(S, c, true, sepf, sep, 1.f);
-                    bool doubt = false;
-                    nOut = clip_f32(c, S, P, ai, bi, W, &buf, &doubt, &counters->clipOverflow);
-                    if (doubt) {
-                        if (lane == 0) ++W.refinedClips;
-                        nOut = clip_hull_hull(c, S, P, sep, ai, bi, W, &buf, &counters->clipOverflow);
-                    }
+            if (find_axis(c, S, W, sep, &counters->clipOverflow)) {
+                const float3 sepf = to_f3(sep);
+                // incident face of B: max dot(nB, sep); reference face of A: min dot(nA, sep)
+                const int bi = select_face(S, c, false, sepf, sep, -1.f);
+                const int ai = select_face(S, c, true, sepf, sep, 1.f);
+                bool doubt = false;
+                nOut = clip_f32(c, S, P, ai, bi, W, &buf, &doubt, &counters->clipOverflow);
+                if (doubt) {
+                    if (lane == 0) ++W.refinedClips;
+                    nOut = clip_hull_hull(c, S, P, sep, ai, bi, W, &buf, &counters->clipOverflow);
                 }
             }
             if (nOut > 0) {
@@ -904,24 +1060,7 @@ k_narrowphase(const int2* __restrict__ pairs, const int32_t* __restrict__ numPai
                     if (tie) idx = reduce_manifold(pts, nOut, nrm);
                     nRed = 4;
                 }
-                b3Contact4* out = &contacts[p];
-                if (lane < nRed) {
-                    const int k = lane == 0 ? idx.x : lane == 1 ? idx.y : lane == 2 ? idx.z : idx.w;
-                    const FfVert q = pts[k];
-                    *reinterpret_cast<float4*>(&out->worldPos[lane][0]) =
-                        make_float4(q.xh + q.xl, q.yh + q.yl, q.zh + q.zl, q.wh + q.wl);
-                } else if (lane < 4) {
-                    *reinterpret_cast<float4*>(&out->worldPos[lane][0]) = make_float4(0.f, 0.f, 0.f, 0.f);
-                }
-                if (lane == 4) {
-                    const float3 n = to_f3(nrm);
-                    *reinterpret_cast<float4*>(&out->worldNormal[0]) = make_float4(n.x, n.y, n.z, (float)nRed);
-                    out->friction = combine_friction(Bd.friction[c.A], Bd.friction[c.B], P.frictionCombine);
-                    out->pairIndex = p;
-                    out->bodyAPtrAndSignBit = c.invMassA == 0.f ? -c.A : c.A;
-                    out->bodyBPtrAndSignBit = c.invMassB == 0.f ? -c.B : c.B;
-                    manifoldFlag[p] = 1u;
-                }
+                emit_contact(p, c, pts, nRed, idx, to_f3(nrm), Bd, P, contacts, manifoldFlag);
             } else if (lane == 0) {
                 manifoldFlag[p] = 0u;
             }
@@ -939,7 +1078,8 @@ k_narrowphase(const int2* __restrict__ pairs, const int32_t* __restrict__ numPai
 namespace b3 {
 
 int launch_narrowphase(b3World_t* w, cudaStream_t st) {
-    B3_CUDA(cudaMemsetAsync(w->d.scalars + S_NP_WORK, 0, sizeof(int32_t), st));
+    // work counters and queue lengths S_NP_WORK .. S_NP_WORK3
+    B3_CUDA(cudaMemsetAsync(w->d.scalars + S_NP_WORK, 0, sizeof(int32_t) * 5, st));
     if (w->cfg.maxPairs == 0 || w->bodies.empty()) return B3_OK;
     NpParams P;
     P.minDist = -1e30f;
@@ -948,14 +1088,24 @@ int launch_narrowphase(b3World_t* w, cudaStream_t st) {
     P.maxPairs = w->cfg.maxPairs;
     const int threads = 32 * w->npWarpsPerBlock;
     const size_t smem = sizeof(WarpScratch) * w->npWarpsPerBlock;
-    int occ = 1;
-    B3_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_narrowphase, threads, smem));
-    occ = occ < 1 ? 1 : occ;
-    const int grid = w->ctx->numSMs * occ;
-    k_narrowphase<<<grid, threads, smem, st>>>(w->d.pairs, w->d.scalars + S_NUM_PAIRS,
-                                              w->bodiesDev(), w->shapesDev(), P, w->d.contacts,
-                                              w->d.manifoldFlag, w->d.scalars + S_NP_WORK,
-                                              w->d.counters);
+    auto grid_of = [&](const void* k) -> int {
+        int occ = 1;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, threads, smem) != cudaSuccess || occ < 1) occ = 1;
+        return w->ctx->numSMs * occ;
+    };
+    const b3::BodiesDev Bd = w->bodiesDev();
+    const b3::ShapesDev S = w->shapesDev();
+    int32_t* sc = w->d.scalars;
+    k_np_sweep<<<grid_of((const void*)k_np_sweep), threads, smem, st>>>(
+        w->d.pairs, sc + S_NUM_PAIRS, Bd, S, w->d.manifoldFlag, w->d.pairSep, w->d.npFast, w->d.npSlow, sc,
+        w->d.counters);
+    B3_CHECK_LAUNCH();
+    k_np_clip<<<grid_of((const void*)k_np_clip), threads, smem, st>>>(
+        w->d.pairs, Bd, S, P, w->d.pairSep, w->d.npFast, w->d.npSlow, w->d.contacts, w->d.manifoldFlag, sc,
+        w->d.counters);
+    B3_CHECK_LAUNCH();
+    k_np_exact<<<grid_of((const void*)k_np_exact), threads, smem, st>>>(
+        w->d.pairs, Bd, S, P, w->d.npSlow, w->d.contacts, w->d.manifoldFlag, sc, w->d.counters);
     B3_CHECK_LAUNCH();
     return B3_OK;
 }
