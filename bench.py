@@ -21,7 +21,9 @@ Prints one JSON line on rank 0.
 * cpu_baseline: the oracle (single-threaded C++ port of the reference step)
   on the host, a bounded sample of the same scene.
 * forms: the batched 4,096-world step against the plain per-world step on
-  the same GPU (body-steps/s of each; per-world time sampled on a subset).
+  the same GPU (body-steps/s of each; per-world time sampled on a subset),
+  and the adjoint form (forward with checkpoints + reverse sweep) on the
+  256-world differentiable throw against its plain forward.
 --impl reference: the oracle port on all host cores (independent replicas,
   one process per core), same metric and workload.
 """
@@ -353,7 +355,9 @@ def adjoint_form(ctx, worlds=256, steps=120, checkpoint_every=16):
     fwd_ms = ev[0].elapsed_time(ev[1])
     bwd_ms = ev2[0].elapsed_time(ev2[1])
     g = adj.gradients()
-    finite = bool(np.isfinite(g["lin"]).all() and np.isfinite(g["mass"]).all())
+    fin = np.isfinite(g["lin"]).all(1) & np.isfinite(g["ang"]).all(1) & np.isfinite(g["mass"]) & \
+        np.isfinite(g["friction"])
+    finite_worlds = int(sum(bool(fin[wid == k].all()) for k in range(sc.num_worlds)))
     adj.close()
     w.close()
     total = fwd_ms + bwd_ms
@@ -362,9 +366,10 @@ def adjoint_form(ctx, worlds=256, steps=120, checkpoint_every=16):
             "adjoint_body_steps_per_s": sc.n * steps / (total / 1e3),
             "plain_body_steps_per_s": sc.n * steps / (plain_ms / 1e3),
             "forward_ms": fwd_ms, "backward_ms": bwd_ms, "plain_ms": plain_ms,
-            "cost_vs_plain": total / plain_ms, "gradients_finite": finite,
+            "cost_vs_plain": total / plain_ms, "worlds_with_finite_gradients": finite_worlds,
             "gradient_error": "one-step gradient vectors within 1e-3 (measured 1e-6..4e-4) of FP64 central "
-                              "differences (tests/test_gpu_adjoint.py)"}
+                              "differences (tests/test_gpu_adjoint.py); over 120 steps the throw is chaotic and "
+                              "gradients grow without bound in some worlds"}
 
 
 def _oracle_worker(args):

@@ -613,6 +613,20 @@ __device__ void geo_eval(const Geo& G, const b3::ShapesDev& S, const b3ConvexPol
     }
 }
 
+// The corner of side planes k, l on the incident face plane is well defined
+// (the three normals are not close to coplanar).
+__device__ bool corner_ok(const b3::ShapesDev& S, const b3ConvexPolyhedron& hA, const b3ConvexPolyhedron& hB,
+                          const b3Face& fa, const b3Face& fb, const Mat3& RA, const Mat3& RB, float3 nAw, int k,
+                          int l) {
+    const int nvA = fa.numIndices;
+    const float3 ka = vtx(S, hA, face_vertex(S, fa, k)), kb = vtx(S, hA, face_vertex(S, fa, (k + 1) % nvA));
+    const float3 la = vtx(S, hA, face_vertex(S, fa, l)), lb = vtx(S, hA, face_vertex(S, fa, (l + 1) % nvA));
+    const float3 pk = normalize(-cross(mul(RA, ka - kb), nAw));
+    const float3 pl = normalize(-cross(mul(RA, la - lb), nAw));
+    const float3 nb = mul(RB, make_float3(fb.plane[0], fb.plane[1], fb.plane[2]));
+    return fabsf(dot(pk, cross(pl, nb))) > 1e-3f;
+}
+
 // Classify the stored manifold against the forward poses (values only).
 __device__ void geo_classify(Geo& G, const b3::ShapesDev& S, const b3ConvexPolyhedron& hA,
                              const b3ConvexPolyhedron& hB, const Mat3& RA, const Mat3& RB, float3 xB, float3 sep,
@@ -700,7 +714,11 @@ __device__ void geo_classify(Geo& G, const b3::ShapesDev& S, const b3ConvexPolyh
             else if (e < onErr[1]) { onErr[1] = e; on[1] = k; }
         }
         if (on[0] < 0) { atomicAdd(unclassified, 1); continue; }
-        // an incident edge through the point?
+        // an incident edge through the point, crossing the side plane
+        // (not lying in it: the intersection must be well defined)
+        const float3 vk = vtx(S, hA, face_vertex(S, fa, on[0]));
+        const float3 vk1 = vtx(S, hA, face_vertex(S, fa, (on[0] + 1) % nvA));
+        const float3 pnk = normalize(-cross(mul(RA, vk - vk1), nAw));
         int edge = -1;
         float bestE = tol;
         for (int i = 0; i < nvB; ++i) {
@@ -709,6 +727,7 @@ __device__ void geo_classify(Geo& G, const b3::ShapesDev& S, const b3ConvexPolyh
             const float3 u = b - a;
             const float uu = dot(u, u);
             if (uu <= 0.f) continue;
+            if (fabsf(dot(pnk, u)) < 1e-3f * sqrtf(uu)) continue;
             const float t = dot(p[j] - a, u) / uu;
             if (t < -1e-4f || t > 1.f + 1e-4f) continue;
             const float e = length(a + u * t - p[j]);
@@ -719,7 +738,7 @@ __device__ void geo_classify(Geo& G, const b3::ShapesDev& S, const b3ConvexPolyh
             g.i0 = edge;
             g.i1 = (edge + 1) % nvB;
             g.k = on[0];
-        } else if (on[1] >= 0) {
+        } else if (on[1] >= 0 && corner_ok(S, hA, hB, fa, fb, RA, RB, nAw, on[0], on[1])) {
             g.kind = PK_CORNER;
             g.i0 = on[0];
             g.i1 = on[1];
@@ -843,6 +862,11 @@ k_adj_manifold(SolverView V, AdjView A, ManifoldArgs MA, StepParams P) {
             for (int j = 0; j < npts; ++j)
                 acc += gin[29 + 3 * j] * pD[j].x.d + gin[30 + 3 * j] * pD[j].y.d + gin[31 + 3 * j] * pD[j].z.d +
                        gin[41 + j] * dD[j].d;
+            if (!isfinite(acc)) {
+                // a degenerate feature slipped through the classification
+                atomicAdd(MA.unclassified, 1);
+                acc = 0.f;
+            }
             float* dst = body == 0 ? (kk < 3 ? &gxA.x : &gthA.x) : (kk < 3 ? &gxB.x : &gthB.x);
             dst[kk % 3] += acc;
         }

@@ -47,6 +47,11 @@ constexpr int kChunk = 4;     // pairs per work grab
 constexpr int kKeep = 4;      // near-minimum axis candidates kept per lane
 constexpr int kMaxCand = 32;  // candidates refined in float-float per pair
 constexpr int kNone = 0x7fffffff;
+// pairSep[p].w: how the pair reached the exact stage
+constexpr int kSepRefine = 0;      // near-minimum axes: float-float re-ranking
+constexpr int kSepDecided = 1;     // FP32 axis (FP32 clip stage)
+constexpr int kSepClipDoubt = 2;   // FP32 axis, clipping in doubt
+constexpr int kSepReduceTie = 3;   // FP32 axis and clip, reduction tie
 
 struct NpParams {
     float minDist;
@@ -953,9 +958,10 @@ k_np_sweep(const int2* __restrict__ pairs, const int32_t* __restrict__ numPairsD
             if (r == 0) {
                 if (lane == 0) manifoldFlag[p] = 0u;
             } else if (r == 1) {
-                if (lane == 0) pairSep[p] = make_float4(sepf.x, sepf.y, sepf.z, 0.f);
+                if (lane == 0) pairSep[p] = make_float4(sepf.x, sepf.y, sepf.z, (float)kSepDecided);
                 push(fastQ, scalars + b3::S_NP_FAST, p);
             } else {
+                if (lane == 0) pairSep[p] = make_float4(0.f, 0.f, 0.f, (float)kSepRefine);
                 push(slowQ, scalars + b3::S_NP_SLOW, p);
             }
             __syncwarp();
@@ -968,7 +974,7 @@ k_np_sweep(const int2* __restrict__ pairs, const int32_t* __restrict__ numPairsD
 // queue instead.
 __global__ void __launch_bounds__(128)
 k_np_clip(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, NpParams P,
-          const float4* __restrict__ pairSep, const int* __restrict__ fastQ, int* __restrict__ slowQ,
+          float4* __restrict__ pairSep, const int* __restrict__ fastQ, int* __restrict__ slowQ,
           b3Contact4* __restrict__ contacts, uint32_t* __restrict__ manifoldFlag, int32_t* __restrict__ scalars,
           b3Counters* __restrict__ counters) {
     extern __shared__ __align__(16) unsigned char np_smem[];
@@ -994,13 +1000,14 @@ k_np_clip(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, NpP
             const int nOut = clip_f32(c, S, P, ai, bi, W, &buf, &slow, &counters->clipOverflow);
             int4 idx = make_int4(0, 1, 2, 3);
             int nRed = nOut;
+            bool tie = false;
             if (!slow && nOut > 4) {
-                bool tie = false;
                 idx = reduce_f32(W.poly[buf], min(nOut, kMaxPoly), -sepf, &tie);
-                slow = tie;
                 nRed = 4;
             }
-            if (slow) {
+            if (slow || tie) {
+                // the exact stage redoes only the part in doubt
+                if (lane == 0) pairSep[p].w = (float)(slow ? kSepClipDoubt : kSepReduceTie);
                 push(slowQ, scalars + b3::S_NP_SLOW, p);
             } else if (nOut > 0) {
                 emit_contact(p, c, W.poly[buf], nRed, idx, -sepf, Bd, P, contacts, manifoldFlag);
@@ -1016,8 +1023,8 @@ k_np_clip(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, NpP
 // float-float refinement of the axis, the faces, the clip and the reduction.
 __global__ void __launch_bounds__(128)
 k_np_exact(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, NpParams P,
-           const int* __restrict__ slowQ, b3Contact4* __restrict__ contacts, uint32_t* __restrict__ manifoldFlag,
-           int32_t* __restrict__ scalars, b3Counters* __restrict__ counters) {
+           const float4* __restrict__ pairSep, const int* __restrict__ slowQ, b3Contact4* __restrict__ contacts,
+           uint32_t* __restrict__ manifoldFlag, int32_t* __restrict__ scalars, b3Counters* __restrict__ counters) {
     extern __shared__ __align__(16) unsigned char np_smem[];
     const int lane = threadIdx.x & 31;
     WarpScratch& W = reinterpret_cast<WarpScratch*>(np_smem)[threadIdx.x >> 5];
@@ -1037,13 +1044,23 @@ k_np_exact(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, Np
             pair_setup(c, pairs[p], Bd, S);
             int nOut = 0, buf = 0;
             ff3 sep = mk3(0.f, 0.f, 0.f);
-            if (find_axis(c, S, W, sep, &counters->clipOverflow)) {
+            const float4 s4 = pairSep[p];
+            const int why = (int)s4.w;
+            bool haveAxis;
+            if (why == kSepRefine) {
+                haveAxis = find_axis(c, S, W, sep, &counters->clipOverflow);
+            } else {
+                // axis decided by the FP32 sweep
+                sep = mk3(s4.x, s4.y, s4.z);
+                haveAxis = true;
+            }
+            if (haveAxis) {
                 const float3 sepf = to_f3(sep);
                 // incident face of B: max dot(nB, sep); reference face of A: min dot(nA, sep)
                 const int bi = select_face(S, c, false, sepf, sep, -1.f);
                 const int ai = select_face(S, c, true, sepf, sep, 1.f);
-                bool doubt = false;
-                nOut = clip_f32(c, S, P, ai, bi, W, &buf, &doubt, &counters->clipOverflow);
+                bool doubt = why == kSepClipDoubt;
+                if (!doubt) nOut = clip_f32(c, S, P, ai, bi, W, &buf, &doubt, &counters->clipOverflow);
                 if (doubt) {
                     if (lane == 0) ++W.refinedClips;
                     nOut = clip_hull_hull(c, S, P, sep, ai, bi, W, &buf, &counters->clipOverflow);
@@ -1105,7 +1122,7 @@ int launch_narrowphase(b3World_t* w, cudaStream_t st) {
         w->d.counters);
     B3_CHECK_LAUNCH();
     k_np_exact<<<grid_of((const void*)k_np_exact), threads, smem, st>>>(
-        w->d.pairs, Bd, S, P, w->d.npSlow, w->d.contacts, w->d.manifoldFlag, sc, w->d.counters);
+        w->d.pairs, Bd, S, P, w->d.pairSep, w->d.npSlow, w->d.contacts, w->d.manifoldFlag, sc, w->d.counters);
     B3_CHECK_LAUNCH();
     return B3_OK;
 }
