@@ -48,6 +48,8 @@ WORKLOADS = {
           "64x32x64 lattice at 1.2 m, 10 Jacobi iterations",
     "c2s": "plain step, 16,384 bodies (the 131,072-body mix on a 32x16x32 lattice at 1.2 m), "
            "10 Jacobi iterations (small case for profiler captures)",
+    "c3s": "batched step, 512 worlds of log-uniform[8,512] cubes / 12-point hulls, 10 Jacobi iterations "
+           "(small case for profiler captures)",
     "c3": "batched step, 4,096 worlds of log-uniform[8,512] cubes / 12-point hulls, 10 Jacobi iterations",
     "c5": "plain step, 1,048,576 unit cubes, 128x64x128 lattice, 10 Jacobi iterations",
 }
@@ -127,7 +129,7 @@ class ClockSampler:
 
 def make_scene(name):
     from experiments_b200 import scenes
-    return {"c1": scenes.c1, "c2": scenes.c2, "c2s": lambda: scenes.c2(dims=(32, 16, 32)), "c3": scenes.c3,
+    return {"c1": scenes.c1, "c2": scenes.c2, "c2s": lambda: scenes.c2(dims=(32, 16, 32)), "c3": scenes.c3, "c3s": lambda: scenes.c3(worlds=512),
             "c5": scenes.c5}[name]()
 
 

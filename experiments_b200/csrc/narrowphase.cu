@@ -536,22 +536,151 @@ __device__ __forceinline__ void put_f32(FfVert& v, float3 p, float w) {
 }
 __device__ __forceinline__ float3 get_f32(const FfVert& v) { return make_float3(v.xh, v.yh, v.zh); }
 
-__device__ __noinline__ int clip_poly_f32(const FfVert* in, int nin, float3 pn, float3 ap, FfVert* out, bool* bad,
-                                          int* ovf) {
+// Every vertex of the polygon being clipped carries the two constraints it
+// lies on (in FfVert.xl as two 16-bit tags): incident-face edge j (tag j)
+// or side plane k of the reference face (tag kPlaneTag + k). An edge of the
+// polygon lies on the tag its two ends share, so an intersection is
+// recomputed from its defining primitives, not interpolated between
+// already-rounded points: the original incident edge cut by plane k, or
+// the corner of two side planes on the incident face plane. The output
+// order is that of the sequential clip.
+constexpr int kPlaneTag = 64;
+// error budget of one FP32 intersection in metres: with the FP32 rounding
+// of world coordinates (< 4e-6 m up to 100 m) it stays inside the 1e-5 m
+// contact tolerance against the FP64 restatement
+constexpr float kCutBudget = 4e-6f;
+
+struct ClipGeom {
+    const b3::ShapesDev* S;
+    const b3ConvexPolyhedron* pa;
+    const b3ConvexPolyhedron* pb;
+    b3Face fA, fB;
+    Mat3 RA, RB;
+    float3 rel;      // posB - posA
+    float3 nAw;      // reference face normal (world)
+    float3 nIn;      // incident face normal (world)
+    float hIn;       // incident plane: nIn . x = hIn (A frame)
+    float eIn;       // error bound of hIn
+};
+
+// a . b with TwoProd / TwoSum compensation (Ogita-Rump-Oishi Dot2): the
+// error is that of the rounded inputs only
+__device__ __forceinline__ float dot2(float3 a, float3 b) {
+    // products and sums through the _rn intrinsics: no contraction may fuse
+    // them, or the error terms would be lost
+    const float p0 = __fmul_rn(a.x, b.x), e0 = __fmaf_rn(a.x, b.x, -p0);
+    const float p1 = __fmul_rn(a.y, b.y), e1 = __fmaf_rn(a.y, b.y, -p1);
+    const float p2 = __fmul_rn(a.z, b.z), e2 = __fmaf_rn(a.z, b.z, -p2);
+    float t = __fadd_rn(p0, p1);
+    float z = __fsub_rn(t, p0);
+    float s = __fadd_rn(__fsub_rn(p0, __fsub_rn(t, z)), __fsub_rn(p1, z));
+    const float t2 = __fadd_rn(t, p2);
+    z = __fsub_rn(t2, t);
+    s = __fadd_rn(s, __fadd_rn(__fsub_rn(t, __fsub_rn(t2, z)), __fsub_rn(p2, z)));
+    s = __fadd_rn(s, __fadd_rn(e0, __fadd_rn(e1, e2)));
+    return __fadd_rn(t2, s);
+}
+__device__ __forceinline__ bool exact_axes(const Mat3& R) {
+    const float m[9] = {R.r0.x, R.r0.y, R.r0.z, R.r1.x, R.r1.y, R.r1.z, R.r2.x, R.r2.y, R.r2.z};
+    bool ok = true;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) ok = ok && (m[i] == 0.f || m[i] == 1.f || m[i] == -1.f);
+    return ok;
+}
+
+__device__ __forceinline__ unsigned tag2(int a, int b) { return (unsigned)a | ((unsigned)b << 16); }
+__device__ __forceinline__ unsigned vtag(const FfVert& v) { return __float_as_uint(v.xl); }
+__device__ __forceinline__ void put_tagged(FfVert& v, float3 p, unsigned tags) {
+    v = {p.x, __uint_as_float(tags), p.y, 0.f, p.z, 0.f, 0.f, 0.f};
+}
+__device__ __forceinline__ int shared_tag(unsigned s, unsigned e) {
+    const int s0 = (int)(s & 0xffffu), s1 = (int)(s >> 16), e0 = (int)(e & 0xffffu), e1 = (int)(e >> 16);
+    if (s0 == e0 || s0 == e1) return s0;
+    if (s1 == e0 || s1 == e1) return s1;
+    return -1;
+}
+// incident face vertex j in A's frame
+__device__ __forceinline__ float3 inc_vertex(const ClipGeom& G, int j) {
+    const int n = G.fB.numIndices;
+    j = j % n;
+    const float4 v = __ldg(&G.S->verts[G.pb->vertexOffset + G.S->indices[G.fB.indexOffset + j]]);
+    return mul(G.RB, f3(v)) + G.rel;
+}
+// side plane k of the reference face: normal (not unit) and a point on it
+__device__ __forceinline__ void side_plane(const ClipGeom& G, int k, float3& pn, float3& ap) {
+    const int n = G.fA.numIndices;
+    const float4 a = __ldg(&G.S->verts[G.pa->vertexOffset + G.S->indices[G.fA.indexOffset + k]]);
+    const float4 b = __ldg(&G.S->verts[G.pa->vertexOffset + G.S->indices[G.fA.indexOffset + (k + 1) % n]]);
+    pn = -cross(mul(G.RA, make_float3(a.x - b.x, a.y - b.y, a.z - b.z)), G.nAw);
+    ap = mul(G.RA, f3(a));
+}
+
+// Intersection of the polygon edge on constraint `tag` with side plane k;
+// *bad when its FP32 error bound exceeds the budget.
+__device__ float3 exact_cut(const ClipGeom& G, int tag, int k, float3 pn, float3 ap, float3 sv, float3 ev,
+                            bool* bad) {
+    const float pnl = length(pn);
+    if (tag >= 0 && tag < kPlaneTag) {
+        // incident edge j cut by plane k, from its original end points
+        const float3 a = inc_vertex(G, tag), b = inc_vertex(G, tag + 1);
+        const float da = dot(pn, a - ap), db = dot(pn, b - ap);
+        const float den = da - db;
+        // FP32 error of da, db: the end points' transform (|R v| + |rel|)
+        // and the anchor, a few ulps each
+        const float base = length(G.rel) + length(ap) + 0.5f;
+        const float ea = 2.4e-7f * pnl * (length(a) + base);
+        const float eb = 2.4e-7f * pnl * (length(b) + base);
+        if (!(fabsf(den) > 0.f) || length(b - a) * (ea + eb) > kCutBudget * fabsf(den)) *bad = true;
+        const float t = da / den;
+        return a + (b - a) * t;
+    }
+    if (tag >= kPlaneTag && G.fB.pad[0]) {
+        // corner of side planes l and k on the (planar) incident face plane
+        // (Cramer); a welded, non-planar face keeps the interpolation below
+        float3 pl, al;
+        side_plane(G, tag - kPlaneTag, pl, al);
+        const float3 n1 = normalize(pl), n2 = normalize(pn), n3 = G.nIn;
+        const float h1 = dot(n1, al), h2 = dot(n2, ap), h3 = G.hIn;
+        const float3 c23 = cross(n2, n3), c31 = cross(n3, n1), c12 = cross(n1, n2);
+        const float det = dot(n1, c23);
+        const float3 p = (c23 * h1 + c31 * h2 + c12 * h3) * (1.f / det);
+        const float err = 3.6e-7f * (fabsf(h1) + fabsf(h2) + fabsf(h3) + length(p)) + G.eIn;
+        if (!(fabsf(det) > 0.f) || err > kCutBudget * fabsf(det)) *bad = true;
+        return p;
+    }
+    // interpolation between the current end points (an edge along a side
+    // plane of a non-planar incident face); no shared constraint means a
+    // degenerate polygon, which the float-float path decides
+    if (tag < 0) *bad = true;
+    const float ds = dot(pn, sv - ap), de = dot(pn, ev - ap);
+    const float den = ds - de;
+    const float apl = length(ap);
+    const float es = 2.5e-7f * pnl * (1.f + length(sv) + apl), ee = 2.5e-7f * pnl * (1.f + length(ev) + apl);
+    if (!(fabsf(den) > 0.f) || length(ev - sv) * (es + ee) > kCutBudget * fabsf(den)) *bad = true;
+    return sv + (ev - sv) * (ds / den);
+}
+
+__device__ __noinline__ int clip_poly_f32(const ClipGeom& G, const FfVert* in, int nin, int k, FfVert* out,
+                                          bool* bad, int* ovf) {
     const int lane = threadIdx.x & 31;
+    float3 pn, ap;
+    side_plane(G, k, pn, ap);
     const float pnl = length(pn);
     const float apl = length(ap);
+    const unsigned newTag = (unsigned)(kPlaneTag + k);
     int total = 0;
     for (int base = 0; base < nin; base += 32) {
         const int ve = base + lane;
         int cnt = 0;
         float3 o0 = make_float3(0.f, 0.f, 0.f), o1 = o0;
+        unsigned t0 = 0, t1 = 0;
         if (ve < nin) {
-            const float3 sv = get_f32(in[ve == 0 ? nin - 1 : ve - 1]);
-            const float3 ev = get_f32(in[ve]);
+            const FfVert& S0 = in[ve == 0 ? nin - 1 : ve - 1];
+            const FfVert& E0 = in[ve];
+            const float3 sv = get_f32(S0), ev = get_f32(E0);
             const float ds = dot(pn, sv - ap);
             const float de = dot(pn, ev - ap);
-            // FP32 error of ds/de: a few ulps of the magnitudes involved
+            // inside / outside decisions: FP32 error of ds, de
             const float es = 2.5e-7f * pnl * (1.f + length(sv) + apl);
             const float ee = 2.5e-7f * pnl * (1.f + length(ev) + apl);
             if (fabsf(ds) <= es || fabsf(de) <= ee) *bad = true;
@@ -559,15 +688,16 @@ __device__ __noinline__ int clip_poly_f32(const FfVert* in, int nin, float3 pn, 
             if (sNeg || eNeg) {
                 if (sNeg && eNeg) {
                     o0 = ev;
+                    t0 = vtag(E0);
                     cnt = 1;
                 } else {
-                    const float den = ds - de;
-                    const float t = ds * 1.f / den;
-                    if (length(ev - sv) * (es + ee) > 2e-6f * fabsf(den)) *bad = true;
-                    o0 = sv + (ev - sv) * t;
+                    const int tag = shared_tag(vtag(S0), vtag(E0));
+                    o0 = exact_cut(G, tag, k, pn, ap, sv, ev, bad);
+                    t0 = tag2(tag < 0 ? 0 : tag, newTag);
                     cnt = 1;
                     if (!sNeg) {
                         o1 = ev;
+                        t1 = vtag(E0);
                         cnt = 2;
                     }
                 }
@@ -581,10 +711,10 @@ __device__ __noinline__ int clip_poly_f32(const FfVert* in, int nin, float3 pn, 
         }
         const int pos = total + x - cnt;
         if (cnt >= 1) {
-            if (pos < kMaxPoly) put_f32(out[pos], o0, 0.f); else atomicAdd(ovf, 1);
+            if (pos < kMaxPoly) put_tagged(out[pos], o0, t0); else atomicAdd(ovf, 1);
         }
         if (cnt == 2) {
-            if (pos + 1 < kMaxPoly) put_f32(out[pos + 1], o1, 0.f); else atomicAdd(ovf, 1);
+            if (pos + 1 < kMaxPoly) put_tagged(out[pos + 1], o1, t1); else atomicAdd(ovf, 1);
         }
         total += __shfl_sync(0xffffffffu, x, 31);
     }
@@ -598,28 +728,37 @@ __device__ __noinline__ int clip_f32(const PairCtx& c, const b3::ShapesDev& S, c
     const b3ConvexPolyhedron& pa = *c.pa;
     const b3ConvexPolyhedron& pb = *c.pb;
     if (ai == kNone || bi == kNone) return 0;
-    const b3Face fB = S.faces[pb.faceOffset + bi];
-    const b3Face fA = S.faces[pa.faceOffset + ai];
-    const float3 rel = c.posB - c.posA;
-    int nIn = min(fB.numIndices, kMaxPoly);
+    ClipGeom G;
+    G.S = &S;
+    G.pa = c.pa;
+    G.pb = c.pb;
+    G.fB = S.faces[pb.faceOffset + bi];
+    G.fA = S.faces[pa.faceOffset + ai];
+    G.RA = c.RA;
+    G.RB = c.RB;
+    G.rel = c.posB - c.posA;
+    G.nAw = mul(c.RA, make_float3(G.fA.plane[0], G.fA.plane[1], G.fA.plane[2]));
+    G.nIn = mul(c.RB, make_float3(G.fB.plane[0], G.fB.plane[1], G.fB.plane[2]));
+    // incident plane in A's frame: nIn . x = -d_B + nIn . (posB - posA);
+    // rel is exact for nearby bodies, the dot is compensated, and the
+    // rounding of nIn only matters when B is rotated (times |rel|)
+    G.hIn = -G.fB.plane[3] + dot2(G.nIn, G.rel);
+    G.eIn = 2.5e-7f * (fabsf(G.fB.plane[3]) + fabsf(G.hIn)) + (exact_axes(c.RB) ? 0.f : 2.4e-7f * length(G.rel));
+    int nIn = min(G.fB.numIndices, kMaxPoly);
     for (int k = lane; k < nIn; k += 32) {
-        const float4 v = __ldg(&S.verts[pb.vertexOffset + S.indices[fB.indexOffset + k]]);
-        put_f32(W.poly[0][k], mul(c.RB, f3(v)) + rel, 0.f);
+        // vertex k lies on incident edges k-1 and k
+        put_tagged(W.poly[0][k], inc_vertex(G, k), tag2((k + nIn - 1) % nIn, k));
     }
     __syncwarp();
     bool bad = false;
     int cur = 0;
-    const float3 nAw = mul(c.RA, make_float3(fA.plane[0], fA.plane[1], fA.plane[2]));
-    const int nvA = fA.numIndices;
+    const int nvA = G.fA.numIndices;
     for (int e0 = 0; e0 < nvA; ++e0) {
-        const float4 a = __ldg(&S.verts[pa.vertexOffset + S.indices[fA.indexOffset + e0]]);
-        const float4 b = __ldg(&S.verts[pa.vertexOffset + S.indices[fA.indexOffset + (e0 + 1) % nvA]]);
-        const float3 we = mul(c.RA, make_float3(a.x - b.x, a.y - b.y, a.z - b.z));
-        const float3 pn = -cross(we, nAw);
-        const float3 ap = mul(c.RA, f3(a));
-        nIn = clip_poly_f32(W.poly[cur], nIn, pn, ap, W.poly[cur ^ 1], &bad, ovf);
+        nIn = clip_poly_f32(G, W.poly[cur], nIn, e0, W.poly[cur ^ 1], &bad, ovf);
         cur ^= 1;
     }
+    const float3 nAw = G.nAw;
+    const b3Face& fA = G.fA;
     // keep points behind the witness face; in A's frame the plane constant is
     // the face's own (clipFaceAgainstHull :433-452)
     int total = 0;

@@ -267,6 +267,15 @@ extern "C" int b3_register_convex_hull(b3World w, const float* vertices, int num
         for (int k = 0; k < 4; ++k) ff.plane[k] = f.plane[k];
         ff.indexOffset = (int)w->indices.size();
         ff.numIndices = (int)f.indices.size();
+        // pad[0] = 1 when every vertex lies on the stored plane (within
+        // FP32 rounding); a welded face of near-coplanar triangles does not
+        double off = 0.0, mag = 1.0;
+        for (int id : f.indices) {
+            const double x = P.vertices[3 * id], y = P.vertices[3 * id + 1], z = P.vertices[3 * id + 2];
+            off = std::max(off, std::fabs(x * ff.plane[0] + y * ff.plane[1] + z * ff.plane[2] + ff.plane[3]));
+            mag = std::max(mag, std::fabs(x) + std::fabs(y) + std::fabs(z));
+        }
+        ff.pad[0] = off <= 1e-6 * mag ? 1 : 0;
         for (int id : f.indices) w->indices.push_back(id);
         w->faces.push_back(ff);
     }
