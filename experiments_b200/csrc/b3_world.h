@@ -77,6 +77,7 @@ struct DevBuffers {
     float4* pairSep = nullptr;        // per pair: FP32 separating axis of the sweep
     int* npFast = nullptr;            // queue: pairs whose axis the FP32 sweep decided
     int* npSlow = nullptr;            // queue: pairs for the float-float path
+    int* npCand = nullptr;            // near-minimum axes of queued pairs (kNpCandSlots x 32)
     uint32_t* manifoldScan = nullptr; // exclusive scan of the flags
     int* manifoldPair = nullptr;      // manifold -> pair slot
     // solver
@@ -167,6 +168,10 @@ struct b3World_t {
 };
 
 namespace b3 {
+// slots of the narrowphase candidate store (pairs queued for float-float
+// axis ranking beyond this recompute their FP32 sweep)
+constexpr int kNpCandSlots = 1 << 20;
+
 // Record of one Jacobi solve for the reverse sweep: every phase's solver-body
 // copies (both sides of every manifold) and the row impulses after it.
 struct JacobiTape {

@@ -34,6 +34,7 @@
 #include "b3_world.h"
 #include "b3_ff.cuh"
 
+#include <algorithm>
 #include <cfloat>
 
 using namespace b3m;
@@ -1065,8 +1066,13 @@ __device__ __forceinline__ int next_work(int32_t* counter, int limit) {
     return w < limit ? w : -1;
 }
 
-__device__ __forceinline__ void push(int* queue, int32_t* count, int p) {
-    if ((threadIdx.x & 31) == 0) queue[atomicAdd(count, 1)] = p;
+__device__ __forceinline__ int push(int* queue, int32_t* count, int p) {
+    int slot = 0;
+    if ((threadIdx.x & 31) == 0) {
+        slot = atomicAdd(count, 1);
+        queue[slot] = p;
+    }
+    return __shfl_sync(0xffffffffu, slot, 0);
 }
 
 // Stage 1, every pair: the FP32 separating-axis sweep. Separated pairs are
@@ -1076,8 +1082,8 @@ __device__ __forceinline__ void push(int* queue, int32_t* count, int p) {
 __global__ void __launch_bounds__(128)
 k_np_sweep(const int2* __restrict__ pairs, const int32_t* __restrict__ numPairsDev, b3::BodiesDev Bd,
            b3::ShapesDev S, uint32_t* __restrict__ manifoldFlag, float4* __restrict__ pairSep,
-           int* __restrict__ fastQ, int* __restrict__ slowQ, int32_t* __restrict__ scalars,
-           b3Counters* __restrict__ counters) {
+           int* __restrict__ fastQ, int* __restrict__ slowQ, int* __restrict__ cand, int candSlots,
+           int32_t* __restrict__ scalars, b3Counters* __restrict__ counters) {
     extern __shared__ __align__(16) unsigned char np_smem[];
     const int lane = threadIdx.x & 31;
     WarpScratch& W = reinterpret_cast<WarpScratch*>(np_smem)[threadIdx.x >> 5];
@@ -1088,20 +1094,21 @@ k_np_sweep(const int2* __restrict__ pairs, const int32_t* __restrict__ numPairsD
         const int chunkEnd = min(chunk + kChunk, numPairs);
         for (int p = chunk; p < chunkEnd; ++p) {
             PairCtx c;
-            int r = 0;
+            int r = 0, count = 0;
             float3 sepf = make_float3(0.f, 0.f, 0.f);
-            if (pair_setup(c, pairs[p], Bd, S)) {
-                int count = 0;
-                r = sweep_axes(c, S, W, sepf, count, &counters->clipOverflow);
-            }
+            if (pair_setup(c, pairs[p], Bd, S)) r = sweep_axes(c, S, W, sepf, count, &counters->clipOverflow);
             if (r == 0) {
                 if (lane == 0) manifoldFlag[p] = 0u;
             } else if (r == 1) {
                 if (lane == 0) pairSep[p] = make_float4(sepf.x, sepf.y, sepf.z, (float)kSepDecided);
                 push(fastQ, scalars + b3::S_NP_FAST, p);
             } else {
-                if (lane == 0) pairSep[p] = make_float4(0.f, 0.f, 0.f, (float)kSepRefine);
-                push(slowQ, scalars + b3::S_NP_SLOW, p);
+                // keep the near-minimum candidates for the exact stage
+                const int slot = push(slowQ, scalars + b3::S_NP_SLOW, p);
+                const bool kept = slot < candSlots;
+                if (kept && lane < count) cand[(size_t)slot * kMaxCand + lane] = W.cand[lane];
+                if (lane == 0)
+                    pairSep[p] = make_float4(__int_as_float(kept ? count : -1), 0.f, 0.f, (float)kSepRefine);
             }
             __syncwarp();
         }
@@ -1162,7 +1169,8 @@ k_np_clip(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, NpP
 // float-float refinement of the axis, the faces, the clip and the reduction.
 __global__ void __launch_bounds__(128)
 k_np_exact(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, NpParams P,
-           const float4* __restrict__ pairSep, const int* __restrict__ slowQ, b3Contact4* __restrict__ contacts,
+           const float4* __restrict__ pairSep, const int* __restrict__ slowQ, const int* __restrict__ cand,
+           b3Contact4* __restrict__ contacts,
            uint32_t* __restrict__ manifoldFlag, int32_t* __restrict__ scalars, b3Counters* __restrict__ counters) {
     extern __shared__ __align__(16) unsigned char np_smem[];
     const int lane = threadIdx.x & 31;
@@ -1187,7 +1195,16 @@ k_np_exact(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, Np
             const int why = (int)s4.w;
             bool haveAxis;
             if (why == kSepRefine) {
-                haveAxis = find_axis(c, S, W, sep, &counters->clipOverflow);
+                const int count = __float_as_int(s4.x);
+                if (count > 0) {
+                    // the sweep's candidates: float-float ranking only
+                    if (lane < count) W.cand[lane] = cand[(size_t)q * kMaxCand + lane];
+                    __syncwarp();
+                    if (lane == 0) ++W.refinedAxes;
+                    haveAxis = refine_axes(c, S, W, count, sep);
+                } else {
+                    haveAxis = find_axis(c, S, W, sep, &counters->clipOverflow);
+                }
             } else {
                 // axis decided by the FP32 sweep
                 sep = mk3(s4.x, s4.y, s4.z);
@@ -1253,15 +1270,16 @@ int launch_narrowphase(b3World_t* w, cudaStream_t st) {
     const b3::ShapesDev S = w->shapesDev();
     int32_t* sc = w->d.scalars;
     k_np_sweep<<<grid_of((const void*)k_np_sweep), threads, smem, st>>>(
-        w->d.pairs, sc + S_NUM_PAIRS, Bd, S, w->d.manifoldFlag, w->d.pairSep, w->d.npFast, w->d.npSlow, sc,
-        w->d.counters);
+        w->d.pairs, sc + S_NUM_PAIRS, Bd, S, w->d.manifoldFlag, w->d.pairSep, w->d.npFast, w->d.npSlow,
+        w->d.npCand, std::min(w->cfg.maxPairs, kNpCandSlots), sc, w->d.counters);
     B3_CHECK_LAUNCH();
     k_np_clip<<<grid_of((const void*)k_np_clip), threads, smem, st>>>(
         w->d.pairs, Bd, S, P, w->d.pairSep, w->d.npFast, w->d.npSlow, w->d.contacts, w->d.manifoldFlag, sc,
         w->d.counters);
     B3_CHECK_LAUNCH();
     k_np_exact<<<grid_of((const void*)k_np_exact), threads, smem, st>>>(
-        w->d.pairs, Bd, S, P, w->d.pairSep, w->d.npSlow, w->d.contacts, w->d.manifoldFlag, sc, w->d.counters);
+        w->d.pairs, Bd, S, P, w->d.pairSep, w->d.npSlow, w->d.npCand, w->d.contacts, w->d.manifoldFlag, sc,
+        w->d.counters);
     B3_CHECK_LAUNCH();
     return B3_OK;
 }
