@@ -68,6 +68,9 @@ struct __align__(16) FfVert {
 struct __align__(16) WarpScratch {
     FfVert poly[2][kMaxPoly];
     FfVert planes[kMaxPoly];  // float-float clip planes (normal, constant)
+    float4 sideN[kMaxPoly];   // FP32 clip: side plane normals of the reference face
+    float4 sideP[kMaxPoly];   // FP32 clip: a point on each side plane
+    float4 incV[kMaxPoly];    // FP32 clip: incident face vertices (A frame)
     int cand[kMaxCand];
     int refinedAxes, refinedClips;  // float-float fallbacks taken by this warp
 };
@@ -228,7 +231,7 @@ __device__ __noinline__ bool axis_ff(const PairCtx& c, const b3::ShapesDev& S, i
 // face axis separates or no axis exists.
 // FP32 part: 0 = separated (or no axis), 1 = decided in FP32 (sepf),
 // 2 = near-minimum candidates left in W.cand[0..count) for float-float.
-__device__ __forceinline__ int sweep_axes(PairCtx& c, const b3::ShapesDev& S, WarpScratch& W, float3& sepf,
+__device__ __forceinline__ int sweep_axes(PairCtx& c, const b3::ShapesDev& S, int* cand, float3& sepf,
                                           int& count, int* ovfCounter) {
     const int lane = threadIdx.x & 31;
     const b3ConvexPolyhedron& pa = *c.pa;
@@ -318,7 +321,7 @@ __device__ __forceinline__ int sweep_axes(PairCtx& c, const b3::ShapesDev& S, Wa
         const bool take = id != kNone && (k >= kKeep || kd[k] <= lim);
         const unsigned m = __ballot_sync(0xffffffffu, take);
         const int pos = count + __popc(m & b3dev::lanemask_lt());
-        if (take && pos < kMaxCand) W.cand[pos] = id;
+        if (take && pos < kMaxCand) cand[pos] = id;
         count += __popc(m);
     }
     if (__any_sync(0xffffffffu, overflow) || count > kMaxCand) {
@@ -334,7 +337,7 @@ __device__ __forceinline__ int sweep_axes(PairCtx& c, const b3::ShapesDev& S, Wa
                 take = d - err <= lim || (isFace && fabsf(d) <= delta);
             const unsigned m = __ballot_sync(0xffffffffu, take);
             const int pos = count + __popc(m & b3dev::lanemask_lt());
-            if (take && pos < kMaxCand) W.cand[pos] = idx;
+            if (take && pos < kMaxCand) cand[pos] = idx;
             count += __popc(m);
         }
         if (count > kMaxCand) {
@@ -347,7 +350,7 @@ __device__ __forceinline__ int sweep_axes(PairCtx& c, const b3::ShapesDev& S, Wa
     // an edge axis with |e0 x e1| >= 0.01 (FP32 normal error < 1e-5), whose
     // orientation test is not near zero.
     if (count == 1) {
-        const int idx = W.cand[0];
+        const int idx = cand[0];
         float3 n;
         float d, err;
         bool isFace;
@@ -369,7 +372,7 @@ __device__ __forceinline__ int sweep_axes(PairCtx& c, const b3::ShapesDev& S, Wa
         bool isFace = false, ok = true;
         int myIdx = kNone;
         if (lane < count) {
-            myIdx = W.cand[lane];
+            myIdx = cand[lane];
             ok = axis_f32(c, S, myIdx, D, rel, delta, n, d, err, isFace) && err <= 31.f * delta &&
                  !(isFace && fabsf(d) <= delta) && fabsf(dot(D, n)) > 1e-5f * (length(D) + 1e-3f);
             if (!ok) myIdx = kNone;
@@ -449,7 +452,7 @@ __device__ __noinline__ bool refine_axes(PairCtx& c, const b3::ShapesDev& S, War
 __device__ __noinline__ bool find_axis(PairCtx& c, const b3::ShapesDev& S, WarpScratch& W, ff3& sep, int* ovfCounter) {
     float3 sepf;
     int count = 0;
-    const int r = sweep_axes(c, S, W, sepf, count, ovfCounter);
+    const int r = sweep_axes(c, S, W.cand, sepf, count, ovfCounter);
     if (r == 0) return false;
     if (r == 1) {
         sep = mk3(sepf.x, sepf.y, sepf.z);
@@ -552,9 +555,9 @@ constexpr int kPlaneTag = 64;
 constexpr float kCutBudget = 4e-6f;
 
 struct ClipGeom {
-    const b3::ShapesDev* S;
-    const b3ConvexPolyhedron* pa;
-    const b3ConvexPolyhedron* pb;
+    const float4* sideN;   // per side plane k: normal (not unit)
+    const float4* sideP;   // per side plane k: a point on it
+    const float4* incV;    // incident face vertices, A frame
     b3Face fA, fB;
     Mat3 RA, RB;
     float3 rel;      // posB - posA
@@ -602,18 +605,12 @@ __device__ __forceinline__ int shared_tag(unsigned s, unsigned e) {
 }
 // incident face vertex j in A's frame
 __device__ __forceinline__ float3 inc_vertex(const ClipGeom& G, int j) {
-    const int n = G.fB.numIndices;
-    j = j % n;
-    const float4 v = __ldg(&G.S->verts[G.pb->vertexOffset + G.S->indices[G.fB.indexOffset + j]]);
-    return mul(G.RB, f3(v)) + G.rel;
+    return f3(G.incV[j % G.fB.numIndices]);
 }
 // side plane k of the reference face: normal (not unit) and a point on it
 __device__ __forceinline__ void side_plane(const ClipGeom& G, int k, float3& pn, float3& ap) {
-    const int n = G.fA.numIndices;
-    const float4 a = __ldg(&G.S->verts[G.pa->vertexOffset + G.S->indices[G.fA.indexOffset + k]]);
-    const float4 b = __ldg(&G.S->verts[G.pa->vertexOffset + G.S->indices[G.fA.indexOffset + (k + 1) % n]]);
-    pn = -cross(mul(G.RA, make_float3(a.x - b.x, a.y - b.y, a.z - b.z)), G.nAw);
-    ap = mul(G.RA, f3(a));
+    pn = f3(G.sideN[k]);
+    ap = f3(G.sideP[k]);
 }
 
 // Intersection of the polygon edge on constraint `tag` with side plane k;
@@ -730,11 +727,13 @@ __device__ __noinline__ int clip_f32(const PairCtx& c, const b3::ShapesDev& S, c
     const b3ConvexPolyhedron& pb = *c.pb;
     if (ai == kNone || bi == kNone) return 0;
     ClipGeom G;
-    G.S = &S;
-    G.pa = c.pa;
-    G.pb = c.pb;
+    G.sideN = W.sideN;
+    G.sideP = W.sideP;
+    G.incV = W.incV;
     G.fB = S.faces[pb.faceOffset + bi];
     G.fA = S.faces[pa.faceOffset + ai];
+    G.fB.numIndices = min(G.fB.numIndices, kMaxPoly);
+    G.fA.numIndices = min(G.fA.numIndices, kMaxPoly);
     G.RA = c.RA;
     G.RB = c.RB;
     G.rel = c.posB - c.posA;
@@ -745,7 +744,20 @@ __device__ __noinline__ int clip_f32(const PairCtx& c, const b3::ShapesDev& S, c
     // rounding of nIn only matters when B is rotated (times |rel|)
     G.hIn = -G.fB.plane[3] + dot2(G.nIn, G.rel);
     G.eIn = 2.5e-7f * (fabsf(G.fB.plane[3]) + fabsf(G.hIn)) + (exact_axes(c.RB) ? 0.f : 2.4e-7f * length(G.rel));
-    int nIn = min(G.fB.numIndices, kMaxPoly);
+    int nIn = G.fB.numIndices;
+    const int nvA = G.fA.numIndices;
+    // per-pair tables in shared memory: incident vertices and side planes
+    for (int k = lane; k < nIn; k += 32) {
+        const float4 v = __ldg(&S.verts[pb.vertexOffset + S.indices[G.fB.indexOffset + k]]);
+        W.incV[k] = f4(mul(c.RB, f3(v)) + G.rel);
+    }
+    for (int k = lane; k < nvA; k += 32) {
+        const float4 a = __ldg(&S.verts[pa.vertexOffset + S.indices[G.fA.indexOffset + k]]);
+        const float4 b = __ldg(&S.verts[pa.vertexOffset + S.indices[G.fA.indexOffset + (k + 1) % nvA]]);
+        W.sideN[k] = f4(-cross(mul(c.RA, make_float3(a.x - b.x, a.y - b.y, a.z - b.z)), G.nAw));
+        W.sideP[k] = f4(mul(c.RA, f3(a)));
+    }
+    __syncwarp();
     for (int k = lane; k < nIn; k += 32) {
         // vertex k lies on incident edges k-1 and k
         put_tagged(W.poly[0][k], inc_vertex(G, k), tag2((k + nIn - 1) % nIn, k));
@@ -753,7 +765,6 @@ __device__ __noinline__ int clip_f32(const PairCtx& c, const b3::ShapesDev& S, c
     __syncwarp();
     bool bad = false;
     int cur = 0;
-    const int nvA = G.fA.numIndices;
     for (int e0 = 0; e0 < nvA; ++e0) {
         nIn = clip_poly_f32(G, W.poly[cur], nIn, e0, W.poly[cur ^ 1], &bad, ovf);
         cur ^= 1;
@@ -1086,7 +1097,7 @@ k_np_sweep(const int2* __restrict__ pairs, const int32_t* __restrict__ numPairsD
            int32_t* __restrict__ scalars, b3Counters* __restrict__ counters) {
     extern __shared__ __align__(16) unsigned char np_smem[];
     const int lane = threadIdx.x & 31;
-    WarpScratch& W = reinterpret_cast<WarpScratch*>(np_smem)[threadIdx.x >> 5];
+    int* wcand = reinterpret_cast<int*>(np_smem) + kMaxCand * (threadIdx.x >> 5);
     const int numPairs = *numPairsDev;
     for (;;) {
         const int chunk = next_work(scalars + b3::S_NP_WORK, numPairs);
@@ -1096,7 +1107,7 @@ k_np_sweep(const int2* __restrict__ pairs, const int32_t* __restrict__ numPairsD
             PairCtx c;
             int r = 0, count = 0;
             float3 sepf = make_float3(0.f, 0.f, 0.f);
-            if (pair_setup(c, pairs[p], Bd, S)) r = sweep_axes(c, S, W, sepf, count, &counters->clipOverflow);
+            if (pair_setup(c, pairs[p], Bd, S)) r = sweep_axes(c, S, wcand, sepf, count, &counters->clipOverflow);
             if (r == 0) {
                 if (lane == 0) manifoldFlag[p] = 0u;
             } else if (r == 1) {
@@ -1106,7 +1117,7 @@ k_np_sweep(const int2* __restrict__ pairs, const int32_t* __restrict__ numPairsD
                 // keep the near-minimum candidates for the exact stage
                 const int slot = push(slowQ, scalars + b3::S_NP_SLOW, p);
                 const bool kept = slot < candSlots;
-                if (kept && lane < count) cand[(size_t)slot * kMaxCand + lane] = W.cand[lane];
+                if (kept && lane < count) cand[(size_t)slot * kMaxCand + lane] = wcand[lane];
                 if (lane == 0)
                     pairSep[p] = make_float4(__int_as_float(kept ? count : -1), 0.f, 0.f, (float)kSepRefine);
             }
@@ -1269,7 +1280,11 @@ int launch_narrowphase(b3World_t* w, cudaStream_t st) {
     const b3::BodiesDev Bd = w->bodiesDev();
     const b3::ShapesDev S = w->shapesDev();
     int32_t* sc = w->d.scalars;
-    k_np_sweep<<<grid_of((const void*)k_np_sweep), threads, smem, st>>>(
+    const size_t smemSweep = sizeof(int) * kMaxCand * w->npWarpsPerBlock;
+    int occS = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occS, k_np_sweep, threads, smemSweep) != cudaSuccess || occS < 1)
+        occS = 1;
+    k_np_sweep<<<w->ctx->numSMs * occS, threads, smemSweep, st>>>(
         w->d.pairs, sc + S_NUM_PAIRS, Bd, S, w->d.manifoldFlag, w->d.pairSep, w->d.npFast, w->d.npSlow,
         w->d.npCand, std::min(w->cfg.maxPairs, kNpCandSlots), sc, w->d.counters);
     B3_CHECK_LAUNCH();
