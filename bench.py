@@ -217,6 +217,9 @@ def run_b3(args, world_size, local_rank):
     w = scenes.build_world(ctx, sc, useGraph=1)
     st = torch.cuda.current_stream()
     flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > 126 MB L2
+    # launch shapes chosen by the autotuner on this scene (state restored)
+    w.autotune(3, stream=st.cuda_stream)
+    tuning = w.tuning()
     for _ in range(args.warmup):
         w.stepSimulation(1, stream=st.cuda_stream)
     torch.cuda.synchronize()
@@ -238,6 +241,7 @@ def run_b3(args, world_size, local_rank):
     # per-stage CUDA-event breakdown on an identical world advanced to the
     # same step (eager launches; timing only, not part of `value`)
     w2 = scenes.build_world(ctx, sc, useGraph=0)
+    w2.set_tuning(tuning[:5])
     w2.stepSimulation(args.warmup + args.steps - 3)
     w2.set_stage_timing(True)
     acc = np.zeros(len(STAGES))
@@ -274,7 +278,7 @@ def run_b3(args, world_size, local_rank):
         t = torch.tensor([contact_points], device="cuda", dtype=torch.int64)
         dist.all_reduce(t, op=dist.ReduceOp.SUM)
         contact_points = int(t.item())
-    return dict(sc=sc, full=full, sharded=sharded, ms=ms, contact_points=contact_points, counters=counters, stage_ms=stage_ms, c2=c2, clocks=clk.summary(), e2e_ms=e2e_ms,
+    return dict(sc=sc, full=full, sharded=sharded, ms=ms, contact_points=contact_points, tuning=tuning, counters=counters, stage_ms=stage_ms, c2=c2, clocks=clk.summary(), e2e_ms=e2e_ms,
                 w=w, kernels=kernels, flops=flops, ctx=ctx)
 
 
@@ -285,6 +289,7 @@ def forms_comparison(ctx, steps=10, sample_worlds=32):
     sc = scenes.c3()
     wb = scenes.build_world(ctx, sc, useGraph=1)
     st = torch.cuda.current_stream()
+    wb.autotune(3, stream=st.cuda_stream)
     for _ in range(3):
         wb.stepSimulation(1, stream=st.cuda_stream)
     ms_b = time_steps(wb, steps, st, None)
@@ -486,6 +491,9 @@ def main():
                 "contact_points": res["counters"]["numContactPoints"], "iterations": 10, "dt": 1 / 60,
                 "refined_axes": res["counters"]["refinedAxes"], "refined_clips": res["counters"]["refinedClips"],
                 "l2": "flushed between timed steps (256 MiB write outside the events)",
+                "tuning": {"np_warps_per_cta": res["tuning"][0], "pair_cta": res["tuning"][1],
+                           "jacobi_cta": res["tuning"][2], "jacobi_blocks_per_sm": res["tuning"][4],
+                           "autotune_trials": res["tuning"][5], "kernels_per_step": int(res["kernels"])},
                 "parallelism": (f"worlds sharded x{world_size}" if res["sharded"] else f"replicas x{world_size}")
                 if world_size > 1 else "single GPU",
                 "error": "pairs/keys bit-exact; contacts 1e-5 m / normals 1e-4; one step 1e-5 m, 1e-4 m/s "

@@ -155,6 +155,7 @@ SIGNATURES = [
     ("b3_batch_world_offsets", _I, [_P, _IP, _I, _IP]),
     ("b3_autotune", _I, [_P, _I, _P]),
     ("b3_get_tuning", _I, [_P, _IP, _I, _IP]),
+    ("b3_set_tuning", _I, [_P, _IP, _I]),
     ("b3_adjoint_create", _I, [_P, _I, _I, C.POINTER(_P)]),
     ("b3_adjoint_destroy", _I, [_P]),
     ("b3_adjoint_forward", _I, [_P, _P]),
@@ -463,12 +464,22 @@ class PhysicsWorld:
         return np.array([[a.initInvInertia[0], a.initInvInertia[5], a.initInvInertia[10], 0.0] for a in arr],
                         np.float32).reshape(-1, 4)
 
+    def autotune(self, trial_steps=3, stream=None):
+        """b3_autotune: time the candidate launch shapes on the current scene
+        and keep the fastest; the body state is left as it was."""
+        _check(self.lib.b3_autotune(self.h, int(trial_steps), _stream(stream)), "b3_autotune")
+
     def tuning(self):
-        """(narrowphase warps/CTA, pair CTA size, solver CTA size, kernels per captured step)."""
+        """(narrowphase warps/CTA, pair CTA size, solver CTA size, kernels per
+        captured step, Jacobi blocks per SM cap, configurations timed)."""
         v = (C.c_int * 8)()
         cnt = C.c_int()
         _check(self.lib.b3_get_tuning(self.h, v, 8, C.byref(cnt)), "b3_get_tuning")
         return list(v)[:cnt.value]
+
+    def set_tuning(self, values):
+        v = (C.c_int * len(values))(*[int(x) for x in values])
+        _check(self.lib.b3_set_tuning(self.h, v, len(values)), "b3_set_tuning")
 
     def set_stage_timing(self, on=True):
         _check(self.lib.b3_set_stage_timing(self.h, 1 if on else 0), "b3_set_stage_timing")

@@ -160,6 +160,9 @@ struct b3World_t {
     int kernelsPerStep = 0;    // kernel nodes in the captured step graph
     int pairThreads = 128;     // pair-search CTA size
     int solverThreads = 256;   // Jacobi CTA size
+    int solverOccCap = 4;      // Jacobi persistent blocks per SM (at most)
+    int tunedTrials = 0;       // configurations the autotuner timed
+    int npSmemAttr = 0;        // dynamic shared memory attribute set on the narrowphase kernels
 
     int cooperativeOk = 1;
 

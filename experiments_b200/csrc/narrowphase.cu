@@ -1272,6 +1272,13 @@ int launch_narrowphase(b3World_t* w, cudaStream_t st) {
     P.maxPairs = w->cfg.maxPairs;
     const int threads = 32 * w->npWarpsPerBlock;
     const size_t smem = sizeof(WarpScratch) * w->npWarpsPerBlock;
+    if (smem > 48 * 1024 && (size_t)w->npSmemAttr < smem) {
+        // more than the default dynamic shared memory per block (8 warps);
+        // set once per size, before any capture (the first step is eager)
+        w->npSmemAttr = (int)smem;
+        B3_CUDA(cudaFuncSetAttribute(k_np_clip, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        B3_CUDA(cudaFuncSetAttribute(k_np_exact, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
     auto grid_of = [&](const void* k) -> int {
         int occ = 1;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, threads, smem) != cudaSuccess || occ < 1) occ = 1;

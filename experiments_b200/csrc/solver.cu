@@ -434,7 +434,7 @@ int launch_solver_taped(b3World_t* w, cudaStream_t st, const JacobiTape* tape) {
     const void* kern = tape ? (const void*)k_jacobi<true> : (const void*)k_jacobi<false>;
     B3_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, 0));
     occ = occ < 1 ? 1 : occ;
-    occ = occ > 4 ? 4 : occ;
+    occ = occ > w->solverOccCap ? w->solverOccCap : occ;
     // size the persistent grid to the expected manifold count (about 3 per
     // body): fewer blocks make each grid barrier cheaper on small scenes
     const long long est = std::min<long long>((long long)w->cfg.maxPairs, 3LL * (long long)w->bodies.size());

@@ -986,17 +986,102 @@ extern "C" int b3_batch_world_stats(b3World w, float* out4, int numWorlds, void*
     return B3_OK;
 }
 
+// Autotuner: coordinate descent over the launch shapes of the tunable
+// kernels on the world's current scene. Each trial restores the body state
+// and counters, runs one untimed step and then trialSteps timed eager steps
+// (CUDA events on the stream); the fastest value of each knob is kept, the
+// state is restored and the step graph is recaptured on the next b3_step.
 extern "C" int b3_autotune(b3World w, int trialSteps, void* stream) {
-    (void)trialSteps;
-    (void)stream;
-    return w ? B3_OK : B3_ERR_INVALID_ARG;
+    if (!w || trialSteps <= 0) return B3_ERR_INVALID_ARG;
+    if (!w->written) return B3_ERR_STATE;
+    B3_CUDA(cudaSetDevice(w->ctx->device));
+    cudaStream_t st = as_stream(stream);
+    const size_t N = w->bodies.size();
+    float4* save = nullptr;
+    B3_CUDA(cudaMalloc((void**)&save, 4 * N * sizeof(float4)));
+    float4* bufs[4] = {w->d.pos, w->d.quat, w->d.linVel, w->d.angVel};
+    b3Counters ctr;
+    int rc = B3_OK;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    auto restore = [&]() -> int {
+        for (int k = 0; k < 4; ++k)
+            B3_CUDA(cudaMemcpyAsync(bufs[k], save + k * N, N * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+        B3_CUDA(cudaMemcpyAsync(w->d.counters, &ctr, sizeof(ctr), cudaMemcpyHostToDevice, st));
+        return B3_OK;
+    };
+    auto trial = [&](float* ms) -> int {
+        B3_TRY(restore());
+        B3_TRY(b3::run_step(w, st, nullptr));
+        B3_TRY(restore());
+        B3_CUDA(cudaEventRecord(e0, st));
+        for (int i = 0; i < trialSteps; ++i) B3_TRY(b3::run_step(w, st, nullptr));
+        B3_CUDA(cudaEventRecord(e1, st));
+        B3_CUDA(cudaEventSynchronize(e1));
+        B3_CUDA(cudaEventElapsedTime(ms, e0, e1));
+        ++w->tunedTrials;
+        return B3_OK;
+    };
+    struct Knob {
+        int* v;
+        int cand[3];
+    };
+    Knob knobs[] = {{&w->npWarpsPerBlock, {1, 2, 4}}, {&w->solverThreads, {64, 128, 256}},
+                    {&w->solverOccCap, {1, 2, 4}}};
+    do {
+        for (int k = 0; k < 4 && rc == B3_OK; ++k)
+            if (cudaMemcpyAsync(save + k * N, bufs[k], N * sizeof(float4), cudaMemcpyDeviceToDevice, st) !=
+                cudaSuccess)
+                rc = B3_ERR_CUDA;
+        if (rc != B3_OK) break;
+        if (cudaMemcpyAsync(&ctr, w->d.counters, sizeof(ctr), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess || cudaEventCreate(&e0) != cudaSuccess ||
+            cudaEventCreate(&e1) != cudaSuccess) {
+            rc = B3_ERR_CUDA;
+            break;
+        }
+        for (Knob& kb : knobs) {
+            int best = *kb.v;
+            float bestMs = 1e30f;
+            for (int c : kb.cand) {
+                *kb.v = c;
+                float ms = 0.f;
+                if ((rc = trial(&ms)) != B3_OK) break;
+                if (ms < bestMs) {
+                    bestMs = ms;
+                    best = c;
+                }
+            }
+            *kb.v = best;
+            if (rc != B3_OK) break;
+        }
+        if (rc == B3_OK) rc = restore();
+        if (rc == B3_OK && cudaStreamSynchronize(st) != cudaSuccess) rc = B3_ERR_CUDA;
+    } while (false);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(save);
+    w->graphValid = false;  // recapture with the chosen shapes
+    return rc;
+}
+
+extern "C" int b3_set_tuning(b3World w, const int* values, int count) {
+    if (!w || !values || count < 3) return B3_ERR_INVALID_ARG;
+    const int np = values[0], st = values[2], cap = count >= 5 ? values[4] : w->solverOccCap;
+    if ((np != 1 && np != 2 && np != 4) || (st != 64 && st != 128 && st != 256) || cap < 1 || cap > 8)
+        return B3_ERR_INVALID_ARG;
+    w->npWarpsPerBlock = np;
+    w->solverThreads = st;
+    w->solverOccCap = cap;
+    w->graphValid = false;
+    return B3_OK;
 }
 
 extern "C" int b3_get_tuning(b3World w, int* values, int max, int* count) {
     if (!w || !count) return B3_ERR_INVALID_ARG;
-    int v[4] = {w->npWarpsPerBlock, w->pairThreads, w->solverThreads, w->kernelsPerStep};
-    *count = 4;
-    for (int i = 0; i < std::min(4, max); ++i) values[i] = v[i];
+    int v[6] = {w->npWarpsPerBlock, w->pairThreads, w->solverThreads, w->kernelsPerStep, w->solverOccCap,
+                w->tunedTrials};
+    *count = 6;
+    for (int i = 0; i < std::min(6, max); ++i) values[i] = v[i];
     return B3_OK;
 }
 

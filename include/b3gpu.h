@@ -355,12 +355,23 @@ int b3_batch_world_stats(b3World w, float* out4, int numWorlds, void* stream);
  * [offsets[k], offsets[k+1])). offsets NULL = query numWorlds only. Used to
  * partition worlds across GPUs by body count. */
 int b3_batch_world_offsets(b3World w, int* offsets, int maxWorlds, int* numWorlds);
-/* Autotuner: time the candidate launch shapes of the tunable kernels on
- * the current scene and keep the fastest (steps are run and rolled back). */
+/* Autotuner: coordinate descent over the launch shapes of the tunable
+ * kernels on the current scene (narrowphase warps per CTA 1/2/4, Jacobi
+ * CTA size 64/128/256, Jacobi persistent blocks per SM 1/2/4); each trial
+ * runs trialSteps eager steps from the same saved state, timed with CUDA
+ * events; the fastest value of each knob is kept, the body state and
+ * counters are restored, and the step graph is recaptured on the next
+ * b3_step. Synchronises the stream. */
 int b3_autotune(b3World w, int trialSteps, void* stream);
 /* values: narrowphase warps per CTA, pair-search CTA size, solver CTA size,
- * kernel launches per step of the captured step graph (0 before capture). */
+ * kernel launches per step of the captured step graph (0 before capture),
+ * Jacobi blocks per SM cap, configurations timed by the autotuner. */
 int b3_get_tuning(b3World w, int* values, int max, int* count);
+/* Set the tunables in b3_get_tuning's order (count >= 3; the pair-search
+ * CTA size and the launch count are read-only, index 4 is optional):
+ * narrowphase warps per CTA 1/2/4, Jacobi CTA size 64/128/256, Jacobi
+ * blocks per SM cap 1..8. */
+int b3_set_tuning(b3World w, const int* values, int count);
 
 /* ------------------------------------------------------------------ */
 /* Adjoint (reverse mode)                                               */

@@ -150,3 +150,27 @@ def test_long_run_aggregates(ctx):
     assert abs(pen_g - pen_o) < 0.05
     # bodies rest on the ground, none fell through
     assert gp[dyn, 1].min() > 0.3 and op[dyn, 1].min() > 0.3
+
+
+@pytest.mark.gpu
+def test_autotune_keeps_state_and_results(ctx):
+    """The autotuner restores the body state it started from, and the
+    chosen launch shapes do not change the results (bit for bit)."""
+    sc = scenes.random_pile(41, n=64, worlds=8, hull_frac=0.5)
+    a = scenes.build_world(ctx, sc, useGraph=1)
+    b = scenes.build_world(ctx, sc, useGraph=1)
+    a.stepSimulation(5)
+    b.stepSimulation(5)
+    before = a.read_state()
+    a.autotune(2)
+    after = a.read_state()
+    for x, y in zip(before, after):
+        assert np.array_equal(x, y)
+    t = a.tuning()
+    assert t[5] == 9 and t[0] in (1, 2, 4) and t[2] in (64, 128, 256) and t[4] in (1, 2, 4)
+    a.stepSimulation(10)
+    b.stepSimulation(10)
+    for x, y in zip(a.read_state(), b.read_state()):
+        assert np.array_equal(x, y)
+    a.close()
+    b.close()
