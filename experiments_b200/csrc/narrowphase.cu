@@ -1070,9 +1070,9 @@ __device__ __forceinline__ void emit_contact(int p, const PairCtx& c, const FfVe
     }
 }
 
-__device__ __forceinline__ int next_work(int32_t* counter, int limit) {
+__device__ __forceinline__ int next_work(int32_t* counter, int limit, int chunk = kChunk) {
     int w = 0;
-    if ((threadIdx.x & 31) == 0) w = atomicAdd(counter, kChunk);
+    if ((threadIdx.x & 31) == 0) w = atomicAdd(counter, chunk);
     w = __shfl_sync(0xffffffffu, w, 0);
     return w < limit ? w : -1;
 }
@@ -1193,9 +1193,10 @@ k_np_exact(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, Np
     }
     __syncwarp();
     for (;;) {
-        const int chunk = next_work(scalars + b3::S_NP_WORK3, nSlow);
+        // one pair per grab: the queued pairs differ widely in cost
+        const int chunk = next_work(scalars + b3::S_NP_WORK3, nSlow, 1);
         if (chunk < 0) break;
-        const int chunkEnd = min(chunk + kChunk, nSlow);
+        const int chunkEnd = min(chunk + 1, nSlow);
         for (int q = chunk; q < chunkEnd; ++q) {
             const int p = slowQ[q];
             PairCtx c;
