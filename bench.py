@@ -379,6 +379,54 @@ def adjoint_form(ctx, worlds=256, steps=120, checkpoint_every=16):
                               "gradients grow without bound in some worlds"}
 
 
+def scale_run(ctx, steps=32, checkpoint_every=8):
+    """1,048,576 cubes: the plain step and the adjoint (loss = sum of body
+    heights, checkpoints every 8 steps) on one GPU, with the device memory
+    the adjoint holds."""
+    import torch
+    from experiments_b200 import b3, scenes
+    sc = scenes.c5(steps=steps)
+    st = torch.cuda.current_stream()
+    w = scenes.build_world(ctx, sc, useGraph=1)
+    w.stepSimulation(3, stream=st.cuda_stream)
+    torch.cuda.synchronize()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    e[0].record(st)
+    w.stepSimulation(10, stream=st.cuda_stream)
+    e[1].record(st)
+    torch.cuda.synchronize()
+    plain_ms = e[0].elapsed_time(e[1]) / 10
+    counters = w.counters()
+    w.close()
+    torch.cuda.synchronize()
+    free0, total = torch.cuda.mem_get_info()
+    w = scenes.build_world(ctx, sc, useGraph=1)
+    adj = b3.Adjoint(w, steps, checkpoint_every)
+    free1, _ = torch.cuda.mem_get_info()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    ev[0].record(st)
+    adj.forward(stream=st.cuda_stream)
+    ev[1].record(st)
+    seed = np.zeros((sc.n, 4), np.float32)
+    seed[np.asarray(sc.mass) > 0, 1] = 1.0  # loss = sum of heights
+    adj.backward(d_pos=seed, stream=st.cuda_stream)
+    ev[2].record(st)
+    torch.cuda.synchronize()
+    g = adj.gradients()
+    out = {"workload": f"1,048,576 unit cubes, 128x64x128 lattice at 1.05 m, {steps} steps, checkpoints every "
+                       f"{checkpoint_every}", "bodies": int(sc.n),
+           "plain_ms_per_step": plain_ms, "plain_body_steps_per_s": sc.n / (plain_ms / 1e3),
+           "pairs": counters["numPairs"], "manifolds": counters["numManifolds"],
+           "adjoint_forward_ms": ev[0].elapsed_time(ev[1]), "adjoint_backward_ms": ev[1].elapsed_time(ev[2]),
+           "adjoint_body_steps_per_s": sc.n * steps / (ev[0].elapsed_time(ev[2]) / 1e3),
+           "world_plus_adjoint_device_gb": (free0 - free1) / 1e9 + 0.0,
+           "device_total_gb": total / 1e9,
+           "gradients_finite": bool(np.isfinite(g["lin"]).all())}
+    adj.close()
+    w.close()
+    return out
+
+
 def _oracle_worker(args):
     name, budget_s, seed_steps = args
     sys.path.insert(0, ROOT)
@@ -424,6 +472,7 @@ def main():
     ap.add_argument("--impl", default="b3", choices=["b3", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true")
+    ap.add_argument("--scale", action="store_true", help="also run the 1,048,576-body plain and adjoint steps")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world_size = int(os.environ.get("WORLD_SIZE", "1"))
@@ -514,6 +563,8 @@ def main():
     if rank == 0 and world_size == 1 and not args.no_forms:
         line["forms"] = forms_comparison(res["ctx"])
         line["forms"]["adjoint"] = adjoint_form(res["ctx"])
+    if rank == 0 and world_size == 1 and args.scale:
+        line["scale"] = scale_run(res["ctx"])
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_port(args.workload)
     if rank == 0:

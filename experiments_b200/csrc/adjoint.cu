@@ -1077,6 +1077,21 @@ extern "C" int b3_adjoint_create(b3World w, int numSteps, int checkpointEvery, b
     const size_t N = (size_t)a->N, cap = (size_t)a->cap;
     const size_t phases = 2 * (size_t)a->iterations;
     int rc = B3_OK;
+    // HBM sizing: checkpoints, one segment of pre-step states, the tape of
+    // one step and the adjoint buffers, checked against free device memory
+    {
+        const size_t f4 = sizeof(float4);
+        const size_t need = f4 * ((size_t)a->numCkpt * 4 * N + (size_t)a->K * 4 * N + phases * 4 * cap +
+                                  (size_t)a->iterations * 3 * cap + 7 * N + (size_t)kRowSlots * cap + 8 * cap +
+                                  3 * cap + (size_t)kContrib * 2 * cap) +
+                            2 * sizeof(float) * N;
+        size_t freeB = 0, totalB = 0;
+        if (cudaMemGetInfo(&freeB, &totalB) == cudaSuccess && need > freeB / 100 * 95) {
+            delete a;
+            b3_set_error("adjoint needs %.2f GB, %.2f GB free", need / 1e9, freeB / 1e9);
+            return B3_ERR_CAPACITY;
+        }
+    }
     auto fail = [&](int r) {
         for (void* p : a->owned) cudaFree(p);
         delete a;

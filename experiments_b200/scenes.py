@@ -243,7 +243,8 @@ def c5(seed=5, dims=(128, 64, 128), steps=32):
     """1,048,576 unit cubes (config 5)."""
     return lattice_scene("c5_cubes_1048576" if dims == (128, 64, 128) else f"cubes_{dims}", seed, dims, 1.05,
                          lambda n: np.ones(n, np.int32), lambda n: np.ones(n), lambda n: np.full(n, 0.6),
-                         config=dict(cellSize=1.0, gridDims=(256, 128, 256)), steps=steps,
+                         config=dict(cellSize=1.0, gridDims=(256, 128, 256),
+                                     maxPairs=8 * (dims[0] * dims[1] * dims[2] + 1)), steps=steps,
                          extra_shapes=[box_vertices(0.5, 0.5, 0.5)])
 
 
