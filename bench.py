@@ -18,14 +18,16 @@ Prints one JSON line on rank 0.
   roofline is FP32 FLOP/s against the CUDA-core peak; the other stages are
   HBM bound and use the measured copy bandwidth. All stages are listed in
   stage_roofline.
-* cpu_baseline: the oracle (single-threaded C++ port of the reference step)
-  on the host, a bounded sample of the same scene.
+* cpu_baseline: the reference's CPU rigid-body pipeline (bullet2
+  btDiscreteDynamicsWorld built from the reference's sources; the oracle port
+  where that library is absent) on one host thread, a bounded sample of the
+  same scene.
 * forms: the batched 4,096-world step against the plain per-world step on
   the same GPU (body-steps/s of each; per-world time sampled on a subset),
   and the adjoint form (forward with checkpoints + reverse sweep) on the
   256-world differentiable throw against its plain forward.
---impl reference: the oracle port on all host cores (independent replicas,
-  one process per core), same metric and workload.
+--impl reference: the same CPU pipeline on all host cores (independent
+  replicas, one process per core), same metric and workload.
 """
 import argparse
 import json
@@ -427,40 +429,52 @@ def scale_run(ctx, steps=32, checkpoint_every=8):
     return out
 
 
-def _oracle_worker(args):
-    name, budget_s, seed_steps = args
+def _cpu_worker(args):
+    """One CPU replica of the workload for `budget_s` seconds: the reference's
+    CPU pipeline (bullet2 btDiscreteDynamicsWorld) when built, else the
+    oracle port."""
+    name, budget_s = args
     sys.path.insert(0, ROOT)
     import oracle
     from experiments_b200 import b3, scenes
     sc = make_scene(name)
-    hc = b3.Context(-1)
-    w = b3.PhysicsWorld(hc, scenes.world_config(sc))
-    scenes.register_scene(w, sc)
-    o = oracle.oracle_from_world(w, sc)
-    if seed_steps:
-        o.step(seed_steps)
+    if oracle.bullet_lib() is not None:
+        wld = oracle.ReferenceCpuWorld(sc)
+        kind = "reference"
+    else:
+        hc = b3.Context(-1)
+        w = b3.PhysicsWorld(hc, scenes.world_config(sc))
+        scenes.register_scene(w, sc)
+        wld = oracle.oracle_from_world(w, sc)
+        kind = "port"
     t0 = time.perf_counter()
     steps = 0
     while time.perf_counter() - t0 < budget_s and steps < 1000:
-        o.step(1)
+        wld.step(1)
         steps += 1
-    return sc.n, steps, time.perf_counter() - t0
+    return sc.n, steps, time.perf_counter() - t0, kind
+
+
+CPU_KIND = {"reference": "bullet2 btDiscreteDynamicsWorld (btDbvtBroadphase + btSequentialImpulseConstraintSolver, "
+                         "10 iterations) built from the reference's bullet2 sources with g++ -O2",
+            "port": "the oracle (single-threaded C++ restatement of the reference step, FP64)"}
 
 
 def cpu_baseline_port(name, budget_s=12.0, procs=1):
-    """The oracle port on `procs` host cores (independent replicas)."""
+    """The reference's CPU pipeline (or the oracle port) on `procs` host
+    cores (independent replicas, one process each)."""
     if procs <= 1:
-        n, steps, dt = _oracle_worker((name, budget_s, 0))
-        return {"value": n * steps / dt, "unit": "body-steps/s", "cores": 1, "kind": "port",
-                "sample": f"first {steps} steps of the full {n}-body scene ({dt:.1f} s), 1 thread"}
+        n, steps, dt, kind = _cpu_worker((name, budget_s))
+        return {"value": n * steps / dt, "unit": "body-steps/s", "cores": 1, "kind": kind,
+                "sample": f"first {steps} steps of the full {n}-body scene ({dt:.1f} s), 1 thread; {CPU_KIND[kind]}"}
     ctx = mp.get_context("spawn")
     with ctx.Pool(procs) as pool:
-        res = pool.map(_oracle_worker, [(name, budget_s, 0)] * procs)
-    total = sum(n * s / dt for n, s, dt in res)
-    n, s, dt = res[0]
-    return {"value": total, "unit": "body-steps/s", "cores": procs, "kind": "port",
+        res = pool.map(_cpu_worker, [(name, budget_s)] * procs)
+    total = sum(n * s / dt for n, s, dt, _ in res)
+    n, s, dt, kind = res[0]
+    return {"value": total, "unit": "body-steps/s", "cores": procs, "kind": kind,
             "sample": f"{procs} independent replicas, each the first ~{s} steps of the full {n}-body scene "
-                      f"(~{dt:.0f} s)"}
+                      f"(~{dt:.0f} s); {CPU_KIND[kind]}"}
 
 
 def main():
@@ -487,7 +501,8 @@ def main():
         r = cpu_baseline_port(args.workload, budget_s=20.0, procs=procs)
         line = {"metric": "body-steps/s", "value": r["value"], "unit": "body-steps/s", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32" if r["kind"] == "reference" else "f64",
+                "data": "synthetic (seeded scene generator)", "impl": "reference",
                 "config": cfg, "cpu_baseline": r,
                 "e2e": {"value": r["value"], "unit": "body-steps/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}

@@ -15,6 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
 LIB_F32 = os.path.join(HERE, "liboracle_f32.so")
 REF_LIB = os.path.join(HERE, "_ref", "libb3ref.so")
+BULLET_LIB = os.path.join(HERE, "_ref", "libb3bullet.so")
 
 
 class OrConfig(C.Structure):
@@ -33,6 +34,7 @@ class OrContact(C.Structure):
 _lib = None
 _lib32 = None
 _ref = None
+_bullet = None
 _D = C.POINTER(C.c_double)
 _F = C.POINTER(C.c_float)
 _I = C.POINTER(C.c_int)
@@ -91,6 +93,67 @@ def ref_lib():
                                       _F, C.c_float, _F, _I]
         _ref = R
     return _ref
+
+
+def bullet_lib():
+    """The reference's CPU rigid-body pipeline (bullet2 btDiscreteDynamicsWorld)
+    compiled from its sources, or None if absent."""
+    global _bullet
+    if _bullet is None and os.path.exists(BULLET_LIB):
+        B = C.CDLL(BULLET_LIB)
+        B.rb_create.restype = _VP
+        B.rb_create.argtypes = [C.c_int, _I, _F, C.c_int, _I, _F, _F, _F, _F, _F, _F, _I, C.c_int, C.c_float,
+                                C.c_int, C.c_float, C.c_float, C.c_float]
+        B.rb_step.argtypes = [_VP, C.c_int]
+        B.rb_positions.argtypes = [_VP, _F]
+        B.rb_destroy.argtypes = [_VP]
+        _bullet = B
+    return _bullet
+
+
+class ReferenceCpuWorld:
+    """A scene in the reference's CPU pipeline (btDiscreteDynamicsWorld:
+    btDbvtBroadphase + btSequentialImpulseConstraintSolver, 10 iterations);
+    boxes as btBoxShape, other hulls as btConvexHullShape of the same points,
+    one dynamics world per independent world."""
+
+    def __init__(self, scene, dt=1.0 / 60.0, iterations=10, gravity=(0.0, -9.8, 0.0)):
+        B = bullet_lib()
+        if B is None:
+            raise RuntimeError("oracle/_ref/libb3bullet.so not built")
+        self.B = B
+        self.n = scene.n
+        pts = [np.asarray(v, np.float32).reshape(-1, 3) for v in scene.shapes]
+        offs = np.zeros(len(pts) + 1, np.int32)
+        offs[1:] = np.cumsum([len(p) for p in pts])
+        allp = np.ascontiguousarray(np.concatenate(pts).astype(np.float32))
+        f32 = lambda a, k: np.ascontiguousarray(np.asarray(a, np.float32).reshape(-1, k))
+        self._keep = [offs, allp, np.ascontiguousarray(np.asarray(scene.shape, np.int32)), f32(scene.mass, 1),
+                      f32(scene.pos, 3), f32(scene.quat, 4), f32(scene.friction, 1), f32(scene.lin, 3),
+                      f32(scene.ang, 3), np.ascontiguousarray(np.asarray(scene.world, np.int32))]
+        k = self._keep
+        self.h = B.rb_create(len(pts), _i(k[0]), _f(k[1]), self.n, _i(k[2]), _f(k[3]), _f(k[4]), _f(k[5]), _f(k[6]),
+                             _f(k[7]), _f(k[8]), _i(k[9]), int(scene.num_worlds), float(dt), int(iterations),
+                             *[float(g) for g in gravity])
+
+    def step(self, steps=1):
+        self.B.rb_step(self.h, int(steps))
+
+    def positions(self):
+        out = np.zeros((self.n, 3), np.float32)
+        self.B.rb_positions(self.h, _f(out))
+        return out
+
+    def close(self):
+        if self.h:
+            self.B.rb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _f(a):

@@ -17,6 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
 LIB_F32 = os.path.join(HERE, "liboracle_f32.so")
 REF_LIB = os.path.join(HERE, "_ref", "libb3ref.so")
+BULLET_LIB = os.path.join(HERE, "_ref", "libb3bullet.so")
 REFERENCE = "/root/reference"
 
 # Reference sources compiled for the pins (paths relative to the reference root).
@@ -82,6 +83,50 @@ def build_ref(force=False):
     return REF_LIB
 
 
+def bullet_sources():
+    """The reference's bullet2 core: LinearMath, BulletCollision, BulletDynamics."""
+    out = []
+    for sub in ("LinearMath", "BulletCollision", "BulletDynamics"):
+        for root, _, files in os.walk(os.path.join(REFERENCE, "bullet2", sub)):
+            out += [os.path.join(root, f) for f in sorted(files) if f.endswith(".cpp")]
+    return sorted(out)
+
+
+def build_bullet(force=False):
+    """The reference's CPU rigid-body pipeline (bullet2 btDiscreteDynamicsWorld)
+    as a shared library with the C shim oracle/ref_shim_bullet.cpp; the CPU
+    baseline of bench.py. Compiled in place from the reference sources with
+    g++ -O2; objects go to oracle/_ref/bullet_obj."""
+    if not os.path.isdir(REFERENCE):
+        return BULLET_LIB if os.path.exists(BULLET_LIB) else None
+    shim = os.path.join(HERE, "ref_shim_bullet.cpp")
+    srcs = bullet_sources() + [shim]
+    if not force and not _stale(BULLET_LIB, srcs):
+        return BULLET_LIB
+    from concurrent.futures import ThreadPoolExecutor
+    objdir = os.path.join(HERE, "_ref", "bullet_obj")
+    os.makedirs(objdir, exist_ok=True)
+    inc = ["-I", os.path.join(REFERENCE, "bullet2")]
+
+    def compile_one(src):
+        rel = os.path.relpath(src, REFERENCE) if src.startswith(REFERENCE) else os.path.basename(src)
+        o = os.path.join(objdir, rel.replace(os.sep, "_") + ".o")
+        if force or _stale(o, [src]):
+            r = subprocess.run(["g++", "-O2", "-fPIC", "-w"] + inc + ["-c", src, "-o", o], capture_output=True,
+                               text=True)
+            if r.returncode != 0:
+                raise RuntimeError("bullet2 build failed: " + src + "\n" + r.stderr[-3000:])
+        return o
+
+    with ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as ex:
+        objs = list(ex.map(compile_one, srcs))
+    r = subprocess.run(["g++", "-shared", "-o", BULLET_LIB] + objs, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("bullet2 link failed:\n" + r.stderr[-4000:])
+    return BULLET_LIB
+
+
 if __name__ == "__main__":
     print(build_oracle(force="--force" in sys.argv))
     print(build_ref(force="--force" in sys.argv))
+    print(build_bullet(force="--force" in sys.argv))
