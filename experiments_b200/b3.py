@@ -386,12 +386,19 @@ class PhysicsWorld:
         _check(f(self.h, _stream(stream)), "b3_stage_" + name)
 
     # readback -----------------------------------------------------------
-    def read_state(self, stream=None):
+    def read_state(self, stream=None, out=None):
+        """(pos, quat, linVel, angVel) as (n, 4) float32 arrays; `out` gives
+        the four arrays to fill (e.g. pinned host buffers)."""
         n = self.n
-        pos = np.zeros((n, 4), np.float32)
-        quat = np.zeros((n, 4), np.float32)
-        lin = np.zeros((n, 4), np.float32)
-        ang = np.zeros((n, 4), np.float32)
+        if out is not None:
+            pos, quat, lin, ang = out
+            for a in out:
+                assert a.dtype == np.float32 and a.shape == (n, 4) and a.flags["C_CONTIGUOUS"]
+        else:
+            pos = np.zeros((n, 4), np.float32)
+            quat = np.zeros((n, 4), np.float32)
+            lin = np.zeros((n, 4), np.float32)
+            ang = np.zeros((n, 4), np.float32)
         _check(self.lib.b3_read_state(self.h, fptr(pos), fptr(quat), fptr(lin), fptr(ang), _stream(stream)),
                "b3_read_state")
         return pos, quat, lin, ang
