@@ -75,6 +75,7 @@ def lib(f32=False):
         L.or_active_hash.argtypes = [_VP, C.POINTER(C.c_uint64), C.c_int]
         L.or_reset_active.argtypes = [_VP]
         L.or_set_params_f64.argtypes = [_VP, _D, _D, _D]
+        L.or_clip_face_world.argtypes = [_D, C.c_int, _D, _D, C.c_int, C.c_double, C.c_double, _D]
         if f32:
             _lib32 = L
         else:

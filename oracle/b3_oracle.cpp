@@ -1107,6 +1107,40 @@ int or_clip_reduce(or_world* w, int polyA, int faceA, const double* posA, const 
     return (int)pts.size();
 }
 
+// clipFacesAndContactReductionKernel (satClipHullContacts.cl:1845-1952) for
+// one pair given in world space, as the reference's own test data records
+// it: the reference face's vertices vertsA4[0..nA) and normal normalA, the
+// incident polygon polyB4[0..nB); side planes -cross(a - b, n) through a,
+// Sutherland-Hodgman clip, then depth = n . p - n . a0, clamped at minDist
+// and kept when <= maxDist. Writes (x, y, z, depth) and returns the count.
+int or_clip_face_world(const double* vertsA4, int nA, const double* normalA, const double* polyB4, int nB,
+                       double minDist, double maxDist, double* out4) {
+    std::vector<P4> in, tmp;
+    for (int i = 0; i < nB; ++i) in.push_back({polyB4[4 * i], polyB4[4 * i + 1], polyB4[4 * i + 2], 0});
+    const V n(normalA[0], normalA[1], normalA[2]);
+    for (int e0 = 0; e0 < nA; ++e0) {
+        const V a(vertsA4[4 * e0], vertsA4[4 * e0 + 1], vertsA4[4 * e0 + 2]);
+        const int e1 = (e0 + 1) % nA;
+        const V b(vertsA4[4 * e1], vertsA4[4 * e1 + 1], vertsA4[4 * e1 + 2]);
+        const V pn = -cross(a - b, n);
+        const Real eq = -dot(a, pn);
+        clip_face(in, pn, eq, tmp);
+        in.swap(tmp);
+    }
+    const V a0(vertsA4[0], vertsA4[1], vertsA4[2]);
+    const Real eqA = -dot(n, a0);
+    int k = 0;
+    for (const P4& p : in) {
+        Real depth = n.x * p.x + n.y * p.y + n.z * p.z + eqA;
+        if (depth <= minDist) depth = minDist;
+        if (depth <= maxDist) {
+            out4[4 * k] = p.x; out4[4 * k + 1] = p.y; out4[4 * k + 2] = p.z; out4[4 * k + 3] = depth;
+            ++k;
+        }
+    }
+    return k;
+}
+
 // Solver-only entry for the pin against the reference's btPgsJacobiSolver:
 // solve the given manifolds with the given velocities and return the
 // post-solve velocities (bodies' linVel/angVel after the finish step).

@@ -1,0 +1,219 @@
+"""Generate the golden fixtures under tests/golden/ from the reference tree
+(run here, where /root/reference exists; the fixtures are committed so the
+tests need no reference at run time).
+
+clip_faces_k11.npz
+    The reference's own recorded test vector for the clipping kernel:
+    testdata/clipFacesAndContactReductionKernel.7z holds the argument dump of
+    clipFacesAndContactReductionKernel (satClipHullContacts.cl:1845-1952)
+    before and after one launch, in the btLauncherCL serialisation
+    (BB/btLauncherCL.h:216-273: int nArgs, then per argument {isBuffer,
+    argIndex, sizeBytes, 16-byte value} followed by the buffer's bytes, then
+    int numWorkItems), the format the reference's own test
+    (opencl/tests/main.cpp:249-334) replays. Per pair with a separating
+    axis: the reference face's world vertices and normal, the incident
+    polygon, and the kernel's output points and count.
+
+The .7z container is read by the small reader below: one LZMA folder,
+LZMA-coded header (the layout both files in testdata/ use); Python's lzma
+module decodes the raw LZMA1 streams.
+
+Usage: python tests/golden/make_golden.py
+"""
+import lzma
+import os
+import struct
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REFERENCE = "/root/reference"
+
+
+def _num(b, i):
+    """7z variable-length number."""
+    first = b[i]
+    i += 1
+    mask = 0x80
+    val = 0
+    for k in range(8):
+        if first & mask == 0:
+            return val | ((first & (mask - 1)) << (8 * k)), i
+        val |= b[i] << (8 * k)
+        i += 1
+        mask >>= 1
+    return val, i
+
+
+def _lzma1(data, props, size):
+    lc = props[0] % 9
+    lp = (props[0] // 9) % 5
+    pb = props[0] // 45
+    dict_size = struct.unpack("<I", props[1:5])[0]
+    dec = lzma.LZMADecompressor(format=lzma.FORMAT_RAW,
+                                filters=[{"id": lzma.FILTER_LZMA1, "dict_size": dict_size, "lc": lc, "lp": lp,
+                                          "pb": pb}])
+    out = dec.decompress(data, max_length=size)
+    if len(out) != size:
+        raise ValueError("short LZMA stream")
+    return out
+
+
+def _streams_info(h, i):
+    """PackInfo + one-folder LZMA UnpackInfo (+ SubStreamsInfo sizes)."""
+    info = {}
+    while True:
+        t = h[i]
+        i += 1
+        if t == 0x00:
+            return info, i
+        if t == 0x06:  # PackInfo
+            info["packPos"], i = _num(h, i)
+            n, i = _num(h, i)
+            assert n == 1
+            assert h[i] == 0x09
+            info["packSize"], i = _num(h, i + 1)
+            while h[i] != 0x00:  # skip CRCs if present
+                i += 1
+            i += 1
+        elif t == 0x07:  # UnpackInfo
+            assert h[i] == 0x0B
+            nf, i = _num(h, i + 1)
+            assert nf == 1 and h[i] == 0x00
+            i += 1
+            nc, i = _num(h, i)
+            assert nc == 1
+            flags = h[i]
+            i += 1
+            idsize = flags & 0x0F
+            codec = h[i:i + idsize]
+            i += idsize
+            assert codec == b"\x03\x01\x01", "only LZMA folders"
+            if flags & 0x20:
+                psz, i = _num(h, i)
+                info["props"] = h[i:i + psz]
+                i += psz
+            assert h[i] == 0x0C
+            info["unpackSize"], i = _num(h, i + 1)
+            if h[i] == 0x0A:  # folder CRC
+                i += 1 + 1 + 4
+            assert h[i] == 0x00
+            i += 1
+        elif t == 0x08:  # SubStreamsInfo
+            sizes = []
+            if h[i] == 0x0D:
+                nstreams, i = _num(h, i + 1)
+            else:
+                nstreams = 1
+            if h[i] == 0x09:
+                i += 1
+                for _ in range(nstreams - 1):
+                    v, i = _num(h, i)
+                    sizes.append(v)
+            info["subsizes"] = sizes
+            while h[i] != 0x00:  # CRC digests
+                if h[i] == 0x0A:
+                    i += 1
+                    alldef = h[i]
+                    i += 1
+                    assert alldef == 1
+                    i += 4 * nstreams
+                else:
+                    break
+            assert h[i] == 0x00
+            i += 1
+        else:
+            raise ValueError(f"unsupported 7z property {t:#x}")
+
+
+def read_7z(path):
+    """{file name: bytes} of a single-folder LZMA 7z archive."""
+    d = open(path, "rb").read()
+    assert d[:6] == b"7z\xbc\xaf\x27\x1c"
+    off, size = struct.unpack("<QQ", d[12:28])
+    h = d[32 + off:32 + off + size]
+    if h[0] == 0x17:  # encoded header
+        info, _ = _streams_info(h, 1)
+        h = _lzma1(d[32 + info["packPos"]:32 + info["packPos"] + info["packSize"]], info["props"],
+                   info["unpackSize"])
+    assert h[0] == 0x01 and h[1] == 0x04  # Header, MainStreamsInfo
+    info, i = _streams_info(h, 2)
+    data = _lzma1(d[32 + info["packPos"]:32 + info["packPos"] + info["packSize"]], info["props"],
+                  info["unpackSize"])
+    sizes = info.get("subsizes", [])
+    sizes = sizes + [len(data) - sum(sizes)]
+    # FilesInfo: names (UTF-16LE, NUL-terminated)
+    names = []
+    j = h.index(b"\x11", i)
+    ln, j = _num(h, j + 1)
+    assert h[j] == 0x00
+    raw = h[j + 1:j + ln].decode("utf-16-le")
+    names = [x for x in raw.split("\x00") if x]
+    out, p = {}, 0
+    for name, sz in zip(names, sizes):
+        out[name] = data[p:p + sz]
+        p += sz
+    return out
+
+
+def launcher_args(blob):
+    """btLauncherCL argument dump -> (list of (isBuffer, bytes or 16-byte value), numWorkItems)."""
+    nargs = struct.unpack("<i", blob[:4])[0]
+    p = 4
+    args = []
+    for _ in range(nargs):
+        is_buf, idx, sz = struct.unpack("<iii", blob[p:p + 12])
+        val = blob[p + 12:p + 28]
+        p += 28
+        if is_buf:
+            args.append((True, blob[p:p + sz]))
+            p += sz
+        else:
+            args.append((False, val))
+    work = struct.unpack("<i", blob[p:p + 4])[0]
+    return args, work
+
+
+def make_clip_faces():
+    files = read_7z(os.path.join(REFERENCE, "testdata", "clipFacesAndContactReductionKernel.7z"))
+    before_name = [k for k in files if k.endswith("_before.bin")][0]
+    after_name = [k for k in files if k.endswith("_after.bin")][0]
+    before, work = launcher_args(files[before_name])
+    after, _ = launcher_args(files[after_name])
+    f4 = lambda b: np.frombuffer(b, np.float32).reshape(-1, 4)
+    i4 = lambda b: np.frombuffer(b, np.int32)
+    cap = struct.unpack("<i", before[11][1][:4])[0]
+    num_pairs = struct.unpack("<i", before[12][1][:4])[0]
+    has_sep = i4(before[3][1])
+    faces_b = i4(before[5][1]).reshape(-1, 4)
+    faces_a = i4(after[5][1]).reshape(-1, 4)
+    vA = f4(before[6][1]).reshape(-1, cap, 4)
+    nA = f4(before[7][1])
+    vB1 = f4(before[8][1]).reshape(-1, cap, 4)
+    out1 = f4(after[8][1]).reshape(-1, cap, 4)
+    out2 = f4(after[9][1]).reshape(-1, cap, 4)
+    keep = [p for p in range(num_pairs) if has_sep[p] and faces_b[p, 0] >= 0]
+    rec = dict(pairs=np.array(keep, np.int32), cap=np.int32(cap), numPairs=np.int32(num_pairs),
+               numWorkItems=np.int32(work))
+    nAv = faces_b[keep, 2]
+    nBv = faces_b[keep, 3]
+    rec["numVertsA"] = nAv.astype(np.int32)
+    rec["numVertsB"] = nBv.astype(np.int32)
+    rec["numOut"] = faces_a[keep, 3].astype(np.int32)
+    mA, mB = int(nAv.max()), int(nBv.max())
+    rec["vertsA"] = vA[keep, :mA].astype(np.float32)
+    rec["normalA"] = nA[keep].astype(np.float32)
+    rec["polyB"] = vB1[keep, :mB].astype(np.float32)
+    # the depth-filtered points are written through pVtxOut, which after the
+    # side planes' swaps names worldVertsB2 for an even number of planes and
+    # worldVertsB1 for an odd one
+    mO = max(int(faces_a[keep, 3].max()), 1)
+    outs = np.where((nAv % 2 == 0)[:, None, None], out2[keep, :mO], out1[keep, :mO])
+    rec["points"] = outs.astype(np.float32)
+    np.savez_compressed(os.path.join(HERE, "clip_faces_k11.npz"), **rec)
+    return rec
+
+
+if __name__ == "__main__":
+    r = make_clip_faces()
+    print("clip_faces_k11.npz:", len(r["pairs"]), "pairs with a clip, of", int(r["numPairs"]))
