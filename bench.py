@@ -558,7 +558,8 @@ def main():
                 "l2": "flushed between timed steps (256 MiB write outside the events)",
                 "tuning": {"np_warps_per_cta": res["tuning"][0], "pair_cta": res["tuning"][1],
                            "jacobi_cta": res["tuning"][2], "jacobi_blocks_per_sm": res["tuning"][4],
-                           "autotune_trials": res["tuning"][5], "kernels_per_step": int(res["kernels"])},
+                           "autotune_trials": res["tuning"][5], "jacobi_per_world_blocks": res["tuning"][6],
+                           "kernels_per_step": int(res["kernels"])},
                 "parallelism": (f"worlds sharded x{world_size}" if res["sharded"] else f"replicas x{world_size}")
                 if world_size > 1 else "single GPU",
                 "error": "pairs/keys bit-exact; contacts 1e-5 m / normals 1e-4; one step 1e-5 m, 1e-4 m/s "

@@ -98,6 +98,7 @@ struct DevBuffers {
     void* scanScratch = nullptr;
     size_t scanScratchBytes = 0;
     float4* worldStats = nullptr;
+    int *worldMStart = nullptr, *worldMEnd = nullptr;  // per world: manifold range (batched solver)
 };
 
 enum ScalarSlot {
@@ -161,6 +162,7 @@ struct b3World_t {
     int pairThreads = 128;     // pair-search CTA size
     int solverThreads = 256;   // Jacobi CTA size
     int solverOccCap = 4;      // Jacobi persistent blocks per SM (at most)
+    int solverMode = 0;        // Jacobi: 0 = grid barriers, 1 = one block per world (batched)
     int tunedTrials = 0;       // configurations the autotuner timed
     int npSmemAttr = 0;        // dynamic shared memory attribute set on the narrowphase kernels
 

@@ -211,9 +211,9 @@ __global__ void k_setup_rows(b3::BodiesDev Bd, SolverView V, const int* __restri
 // or friction rows in order, store both copies in buffer outBuf. A copy of a
 // manifold without rows keeps the average, as in the reference.
 template <bool TAPE>
-__device__ void manifold_phase(const SolverView& V, int M, bool friction, bool first, int inBuf, int outBuf,
-                               const b3::JacobiTape& T, int phase) {
-    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
+__device__ __forceinline__ void solve_manifold(const SolverView& V, int m, bool friction, bool first, int inBuf,
+                                               int outBuf, const b3::JacobiTape& T, int phase) {
+    {
         const float4 h0 = R(V, 0, m);
         const int nRows = __float_as_int(h0.z);
         const int A = __float_as_int(h0.x), B = __float_as_int(h0.y);
@@ -288,6 +288,13 @@ __device__ void manifold_phase(const SolverView& V, int M, bool friction, bool f
     }
 }
 
+template <bool TAPE>
+__device__ void manifold_phase(const SolverView& V, int M, bool friction, bool first, int inBuf, int outBuf,
+                               const b3::JacobiTape& T, int phase) {
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x)
+        solve_manifold<TAPE>(V, m, friction, first, inBuf, outBuf, T, phase);
+}
+
 // Phases p = 0 .. 2*iterations-1 alternate normal (even) and friction (odd)
 // rows; the averaging of the reference happens at the start of the next
 // phase from the double-buffered copies, so phases are separated by one
@@ -301,6 +308,43 @@ k_jacobi(SolverView V, int iterations, uint32_t* bar, int32_t* err, b3Counters* 
     for (int p = 0; p < phases; ++p) {
         if (p > 0 && !grid_barrier(bar, bar + 1, nb, err, counters)) return;
         manifold_phase<TAPE>(V, M, (p & 1) != 0, p == 0, (p - 1) & 1, p & 1, T, p);
+    }
+}
+
+// Batched worlds: the manifolds of one world are contiguous (the pair list
+// follows the world-major cell keys) and touch only that world's bodies, so
+// a block can run all phases of a world by itself with block barriers in
+// place of grid barriers. Same per-manifold arithmetic and averaging order
+// as k_jacobi, hence bit-identical results.
+// Span [start, end) of each world's manifolds. When a world's manifolds are
+// not contiguous (pairs between two large bodies come after the tiles) the
+// span covers foreign manifolds, which k_jacobi_worlds skips: every
+// manifold is still solved by its own world's block only.
+__global__ void k_world_ranges(SolverView V, const int* __restrict__ worldId, int* __restrict__ start,
+                               int* __restrict__ end) {
+    const int M = *V.numManifolds;
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
+        const int w = worldId[__float_as_int(R(V, 0, m).x)];
+        if (m == 0 || worldId[__float_as_int(R(V, 0, m - 1).x)] != w) atomicMin(&start[w], m);
+        if (m == M - 1 || worldId[__float_as_int(R(V, 0, m + 1).x)] != w) atomicMax(&end[w], m + 1);
+    }
+}
+
+template <bool TAPE>
+__global__ void __launch_bounds__(256)
+k_jacobi_worlds(SolverView V, int iterations, const int* __restrict__ start, const int* __restrict__ end,
+                int numWorlds, const int* __restrict__ worldId, b3::JacobiTape T) {
+    const int phases = 2 * iterations;
+    for (int w = blockIdx.x; w < numWorlds; w += gridDim.x) {
+        const int s = start[w], e = end[w];
+        if (s >= e) continue;
+        for (int p = 0; p < phases; ++p) {
+            if (p > 0) __syncthreads();
+            for (int m = s + (int)threadIdx.x; m < e; m += blockDim.x)
+                if (worldId[__float_as_int(R(V, 0, m).x)] == w)
+                    solve_manifold<TAPE>(V, m, (p & 1) != 0, p == 0, (p - 1) & 1, p & 1, T, p);
+        }
+        __syncthreads();
     }
 }
 
@@ -427,6 +471,29 @@ int launch_solver_taped(b3World_t* w, cudaStream_t st, const JacobiTape* tape) {
     const int g = w->ctx->numSMs * 8;
     k_setup_rows<<<g, 128, 0, st>>>(w->bodiesDev(), V, w->d.manifoldPair, w->d.contacts, SP);
     B3_CHECK_LAUNCH();
+    if (w->solverMode == 1 && w->cfg.numWorlds > 1) {
+        // one block per world at a time, block barriers between phases
+        const int nw = w->cfg.numWorlds;
+        B3_CUDA(cudaMemsetAsync(w->d.worldMStart, 0x7f, sizeof(int) * nw, st));  // 0x7f7f7f7f: above any index
+        B3_CUDA(cudaMemsetAsync(w->d.worldMEnd, 0, sizeof(int) * nw, st));
+        k_world_ranges<<<w->ctx->numSMs * 4, 256, 0, st>>>(V, w->d.worldId, w->d.worldMStart, w->d.worldMEnd);
+        B3_CHECK_LAUNCH();
+        const int threads = w->solverThreads;
+        const void* kw = tape ? (const void*)k_jacobi_worlds<true> : (const void*)k_jacobi_worlds<false>;
+        int occ = 1;
+        B3_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kw, threads, 0));
+        occ = occ < 1 ? 1 : occ;
+        const int grid = std::min(nw, w->ctx->numSMs * occ);
+        int iters = w->sim.iterations;
+        int nwv = nw;
+        JacobiTape T = tape ? *tape : JacobiTape{};
+        int* ws = w->d.worldMStart;
+        int* we = w->d.worldMEnd;
+        const int* wid = w->d.worldId;
+        void* args[] = {&V, &iters, &ws, &we, &nwv, &wid, &T};
+        B3_CUDA(cudaLaunchKernel(kw, dim3(grid), dim3(threads), args, 0, st));
+        return B3_OK;
+    }
     // persistent cooperative Jacobi
     B3_CUDA(cudaMemsetAsync(w->d.scalars + S_BAR_COUNT, 0, sizeof(int32_t) * 2, st));
     const int threads = w->solverThreads;

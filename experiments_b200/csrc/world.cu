@@ -73,7 +73,7 @@ void free_all(b3::DevBuffers& d) {
                     d.incKeys, d.incVals, d.incKeysAlt, d.incValsAlt, d.bodyIncStart,
                     d.bodyIncEnd, d.rows, d.manifoldHdr, d.incLin, d.incAng, d.avgLin, d.avgAng,
                     d.scalars, d.counters, d.sortScratch, d.incSortScratch, d.scanScratch,
-                    d.worldStats};
+                    d.worldStats, d.worldMStart, d.worldMEnd};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     d = b3::DevBuffers();
@@ -438,6 +438,10 @@ static int ensure_capacity(b3World w) {
         B3_TRY(dalloc((unsigned char*&)d.incSortScratch, incBytes));
     }
     if (!d.worldStats) B3_TRY(dalloc(d.worldStats, 2 * (size_t)w->cfg.numWorlds));
+    if (!d.worldMStart) {
+        B3_TRY(dalloc(d.worldMStart, (size_t)w->cfg.numWorlds));
+        B3_TRY(dalloc(d.worldMEnd, (size_t)w->cfg.numWorlds));
+    }
     return B3_OK;
 }
 
@@ -1026,7 +1030,8 @@ extern "C" int b3_autotune(b3World w, int trialSteps, void* stream) {
         int cand[3];
     };
     Knob knobs[] = {{&w->npWarpsPerBlock, {1, 2, 4}}, {&w->solverThreads, {64, 128, 256}},
-                    {&w->solverOccCap, {1, 2, 4}}};
+                    {&w->solverOccCap, {1, 2, 4}}, {&w->solverMode, {0, 1, 0}}};
+    const int numKnobs = w->cfg.numWorlds > 1 ? 4 : 3;  // per-world solver only for batched worlds
     do {
         for (int k = 0; k < 4 && rc == B3_OK; ++k)
             if (cudaMemcpyAsync(save + k * N, bufs[k], N * sizeof(float4), cudaMemcpyDeviceToDevice, st) !=
@@ -1039,7 +1044,8 @@ extern "C" int b3_autotune(b3World w, int trialSteps, void* stream) {
             rc = B3_ERR_CUDA;
             break;
         }
-        for (Knob& kb : knobs) {
+        for (int ki = 0; ki < numKnobs; ++ki) {
+            Knob& kb = knobs[ki];
             int best = *kb.v;
             float bestMs = 1e30f;
             for (int c : kb.cand) {
@@ -1067,21 +1073,24 @@ extern "C" int b3_autotune(b3World w, int trialSteps, void* stream) {
 extern "C" int b3_set_tuning(b3World w, const int* values, int count) {
     if (!w || !values || count < 3) return B3_ERR_INVALID_ARG;
     const int np = values[0], st = values[2], cap = count >= 5 ? values[4] : w->solverOccCap;
-    if ((np != 1 && np != 2 && np != 4) || (st != 64 && st != 128 && st != 256) || cap < 1 || cap > 8)
+    const int mode = count >= 7 ? values[6] : w->solverMode;
+    if ((np != 1 && np != 2 && np != 4) || (st != 64 && st != 128 && st != 256) || cap < 1 || cap > 8 ||
+        (mode != 0 && mode != 1))
         return B3_ERR_INVALID_ARG;
     w->npWarpsPerBlock = np;
     w->solverThreads = st;
     w->solverOccCap = cap;
+    w->solverMode = mode;
     w->graphValid = false;
     return B3_OK;
 }
 
 extern "C" int b3_get_tuning(b3World w, int* values, int max, int* count) {
     if (!w || !count) return B3_ERR_INVALID_ARG;
-    int v[6] = {w->npWarpsPerBlock, w->pairThreads, w->solverThreads, w->kernelsPerStep, w->solverOccCap,
-                w->tunedTrials};
-    *count = 6;
-    for (int i = 0; i < std::min(6, max); ++i) values[i] = v[i];
+    int v[7] = {w->npWarpsPerBlock, w->pairThreads, w->solverThreads, w->kernelsPerStep, w->solverOccCap,
+                w->tunedTrials, w->solverMode};
+    *count = 7;
+    for (int i = 0; i < std::min(7, max); ++i) values[i] = v[i];
     return B3_OK;
 }
 
