@@ -14,6 +14,19 @@ clip_faces_k11.npz
     axis: the reference face's world vertices and normal, the incident
     polygon, and the kernel's output points and count.
 
+jacobi_pins.npz
+    Outputs of the reference's btPgsJacobiSolver::solveContacts
+    (P2/btPgsJacobiSolver.cpp:171-189), compiled from the reference sources
+    into oracle/_ref/libb3ref.so, on the manifolds of three settled piles
+    (random_pile seeds 21-23, 40 bodies, 40 oracle steps): the Body /
+    Inertia / Contact4 arrays it was given and the velocities it returned.
+
+hull_pins.npz
+    btConvexUtility::initializePolyhedralFeatures
+    (P1/btConvexUtility.cpp:31-270) on every distinct shape of the plain and
+    batched workloads: vertices, face planes, face vertex cycles and unique
+    edges.
+
 The .7z container is read by the small reader below: one LZMA folder,
 LZMA-coded header (the layout both files in testdata/ use); Python's lzma
 module decodes the raw LZMA1 streams.
@@ -214,6 +227,91 @@ def make_clip_faces():
     return rec
 
 
+def _import_tests():
+    import sys
+    root = os.path.dirname(os.path.dirname(HERE))
+    for p in (root, os.path.join(root, "tests")):
+        if p not in sys.path:
+            sys.path.insert(0, p)
+
+
+def make_jacobi():
+    _import_tests()
+    import ctypes as C
+    import oracle
+    from experiments_b200 import b3, scenes
+    from helpers import host_oracle
+    ref = oracle.ref_lib()
+    hc = b3.Context(-1)
+    rec = {}
+    for seed in (21, 22, 23):
+        sc = scenes.random_pile(seed, n=40, velocity=0.5)
+        w, o = host_oracle(hc, sc)
+        o.step(40)
+        o.stage("aabbs")
+        o.stage("broadphase")
+        o.stage("narrowphase")
+        cts = o.contacts()
+        m = len(cts["normal"])
+        q = np.round(np.clip(cts["friction"], 0, 1) * 65535.0)
+        pos, quat, lin, ang = [a.astype(np.float32) for a in o.state()]
+        mass = np.asarray(sc.mass, np.float64)
+        body = np.zeros(sc.n, dtype=np.dtype([("pos", "<f4", 4), ("quat", "<f4", 4), ("lin", "<f4", 4),
+                                               ("ang", "<f4", 4), ("shape", "<u4"), ("invMass", "<f4"),
+                                               ("rest", "<f4"), ("fric", "<f4")]))
+        body["pos"], body["quat"], body["lin"], body["ang"] = pos, quat, lin, ang
+        body["invMass"] = np.where(mass != 0, 1.0 / np.where(mass != 0, mass, 1), 0)
+        body["fric"] = sc.friction
+        ii = w.inertias()
+        inert = np.zeros((sc.n, 24), np.float32)
+        for k in range(3):
+            inert[:, k * 4 + k] = ii[:, k]
+            inert[:, 12 + k * 4 + k] = ii[:, k]
+        c4 = np.zeros(m, dtype=np.dtype([("pos", "<f4", (4, 4)), ("nrm", "<f4", 4), ("rest", "<u2"),
+                                          ("fric", "<u2"), ("batch", "<i4"), ("a", "<i4"), ("b", "<i4")]))
+        c4["pos"] = cts["pos"]
+        c4["nrm"] = cts["normal"]
+        c4["fric"] = q.astype(np.uint16)
+        c4["a"] = np.abs(cts["bodyA"])
+        c4["b"] = np.abs(cts["bodyB"])
+        given = body.copy()
+        assert ref.ref_jacobi_solve(sc.n, body.ctypes.data, inert.ctypes.data, m, c4.ctypes.data) == 0
+        rec[f"s{seed}_body"] = given.view(np.uint8)
+        rec[f"s{seed}_inertia"] = inert
+        rec[f"s{seed}_contacts"] = c4.view(np.uint8)
+        rec[f"s{seed}_bodyA"] = cts["bodyA"].astype(np.int32)
+        rec[f"s{seed}_bodyB"] = cts["bodyB"].astype(np.int32)
+        rec[f"s{seed}_lin"] = body["lin"].copy()
+        rec[f"s{seed}_ang"] = body["ang"].copy()
+        w.close()
+        o.close()
+    np.savez_compressed(os.path.join(HERE, "jacobi_pins.npz"), **rec)
+    return rec
+
+
+def make_hulls():
+    _import_tests()
+    import test_cpu_pins as pins
+    from experiments_b200 import scenes
+    rec = {}
+    k = 0
+    for sc in (scenes.c2(dims=(4, 2, 4)), scenes.c3(worlds=4)):
+        for pts in sc.shapes:
+            v, p, faces, e = pins.ref_hull(pts)
+            rec[f"h{k}_points"] = np.asarray(pts, np.float32)
+            rec[f"h{k}_verts"] = v
+            rec[f"h{k}_planes"] = p
+            rec[f"h{k}_faces"] = np.concatenate([[len(f)] + list(f) for f in faces]).astype(np.int32)
+            rec[f"h{k}_edges"] = e
+            k += 1
+    rec["count"] = np.int32(k)
+    np.savez_compressed(os.path.join(HERE, "hull_pins.npz"), **rec)
+    return k
+
+
 if __name__ == "__main__":
     r = make_clip_faces()
     print("clip_faces_k11.npz:", len(r["pairs"]), "pairs with a clip, of", int(r["numPairs"]))
+    r = make_jacobi()
+    print("jacobi_pins.npz:", len(r) // 7, "piles")
+    print("hull_pins.npz:", make_hulls(), "shapes")

@@ -112,54 +112,63 @@ def workload_shapes(host_ctx):
     return out
 
 
+def check_hull_against_reference(pts, sh, k, rv, rp, rf, re):
+    """Product hull of shape k against the reference's btConvexUtility output
+    (vertices rv, planes rp, face cycles rf, unique edges re). Returns False
+    when the face partitions differ only by a weld decided at the 0.999
+    threshold (see below), True when everything matched."""
+    pv, pp, pf, pe = product_hull(sh, k)
+    assert len(rv) == len(pv), (k, len(rv), len(pv))
+    if len(rp) != len(pp):
+        # a weld decided at the 0.999 threshold itself: the reference
+        # computes its triangle normals from vertices moved by its
+        # integer grid, which can flip a dot product sitting at 0.999
+        assert _borderline_weld(pp) or _borderline_weld(rp), k
+        return False
+    # btConvexHullComputer returns vertices rebuilt from its integer
+    # grid (about 1e-4 m off the input points); the product keeps the
+    # input points exactly
+    vm = _match_rows(pv, rv, 2e-4)
+    assert vm is not None, k
+    # same face partition: match faces by their vertex sets
+    rsets = {frozenset(int(v) for v in f): j for j, f in enumerate(rf)}
+    for i, f in enumerate(pf):
+        a = [vm[v] for v in f]
+        j = rsets.get(frozenset(a))
+        assert j is not None, (k, i)
+        b = list(rf[j])
+        # same cycle and orientation (up to the starting vertex)
+        s0 = b.index(a[0])
+        assert b[s0:] + b[:s0] == a, (k, i, a, b)
+        na, nb = pp[i, :3], rp[j, :3]
+        # geometric agreement within the weld tolerance
+        assert float(np.dot(na, nb)) > 0.999, (k, i)
+        if len(a) == 3:
+            # same plane rule on both sides (normal from the first two
+            # edges, offset from the lowest vertex), each on its own
+            # vertices: the reference's are off its integer grid
+            for plane, vs in ((pp[i], pv[f]), (rp[j], rv[rf[j]])):
+                assert np.max(np.abs(plane - _plane_rule(vs))) < 2e-5, (k, i)
+        # welded faces take the plane of one member triangle; which one
+        # follows the face order of the hull computer
+    # unique edges: same directions up to sign (short edges inherit the
+    # reference's vertex offsets, hence the looser bound)
+    assert len(pe) == len(re), (k, len(pe), len(re))
+    pn = pe / np.linalg.norm(pe, axis=1, keepdims=True)
+    rn = re / np.linalg.norm(re, axis=1, keepdims=True)
+    for e in pn:
+        d = np.minimum(np.max(np.abs(rn - e), 1), np.max(np.abs(rn + e), 1))
+        assert d.min() < 1e-2, k
+    return True
+
+
 def test_hull_tables_match_btConvexUtility(workload_shapes):
     assert len(workload_shapes) > 100
     borderline = 0
     for pts, sh, k in workload_shapes:
         rv, rp, rf, re = ref_hull(pts)
-        pv, pp, pf, pe = product_hull(sh, k)
-        assert len(rv) == len(pv), (k, len(rv), len(pv))
-        if len(rp) != len(pp):
-            # a weld decided at the 0.999 threshold itself: the reference
-            # computes its triangle normals from vertices moved by its
-            # integer grid, which can flip a dot product sitting at 0.999
-            assert _borderline_weld(pp) or _borderline_weld(rp), k
+        if not check_hull_against_reference(pts, sh, k, rv, rp, rf, re):
             borderline += 1
-            continue
-        # btConvexHullComputer returns vertices rebuilt from its integer
-        # grid (about 1e-4 m off the input points); the product keeps the
-        # input points exactly
-        vm = _match_rows(pv, rv, 2e-4)
-        assert vm is not None, k
-        # same face partition: match faces by their vertex sets
-        rsets = {frozenset(int(v) for v in f): j for j, f in enumerate(rf)}
-        for i, f in enumerate(pf):
-            a = [vm[v] for v in f]
-            j = rsets.get(frozenset(a))
-            assert j is not None, (k, i)
-            b = list(rf[j])
-            # same cycle and orientation (up to the starting vertex)
-            s = b.index(a[0])
-            assert b[s:] + b[:s] == a, (k, i, a, b)
-            na, nb = pp[i, :3], rp[j, :3]
-            # geometric agreement within the weld tolerance
-            assert float(np.dot(na, nb)) > 0.999, (k, i)
-            if len(a) == 3:
-                # same plane rule on both sides (normal from the first two
-                # edges, offset from the lowest vertex), each on its own
-                # vertices: the reference's are off its integer grid
-                for plane, vs in ((pp[i], pv[f]), (rp[j], rv[rf[j]])):
-                    assert np.max(np.abs(plane - _plane_rule(vs))) < 2e-5, (k, i)
-            # welded faces take the plane of one member triangle; which one
-            # follows the face order of the hull computer
-        # unique edges: same directions up to sign (short edges inherit the
-        # reference's vertex offsets, hence the looser bound)
-        assert len(pe) == len(re), (k, len(pe), len(re))
-        pn = pe / np.linalg.norm(pe, axis=1, keepdims=True)
-        rn = re / np.linalg.norm(re, axis=1, keepdims=True)
-        for e in pn:
-            d = np.minimum(np.max(np.abs(rn - e), 1), np.max(np.abs(rn + e), 1))
-            assert d.min() < 1e-2, k
     assert borderline <= len(workload_shapes) // 50
 
 
