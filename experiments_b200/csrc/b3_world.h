@@ -32,6 +32,7 @@ struct ShapesDev {
     const int* indices;
     const float4* edges;
     const float4* localAabb;  // 2 per collidable (min, max)
+    const float* inradius;    // per polyhedron: lower bound of its support about localCenter
     int numPolys, numVerts, numFaces, numIndices, numEdges;
     int tableBytes;           // packed size for shared-memory staging
 };
@@ -63,6 +64,7 @@ struct DevBuffers {
     int* indices = nullptr;
     float4* edges = nullptr;
     float4* localAabb = nullptr;
+    float* polyInradius = nullptr;
     // broadphase
     float4 *aabbMin = nullptr, *aabbMax = nullptr;
     int* smallSlot = nullptr;      // body -> slot in the hash arrays, -1 = large
@@ -133,6 +135,7 @@ struct b3World_t {
     std::vector<b3Collidable> cols;
     std::vector<b3ConvexPolyhedron> polys;
     std::vector<float> verts4, edges4, localAabb8;
+    std::vector<float> polyInradius;
     std::vector<b3Face> faces;
     std::vector<int> indices;
     std::vector<int> worldIds;

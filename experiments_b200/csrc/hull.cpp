@@ -299,6 +299,19 @@ bool compute_polyhedron(const float* pts_in, int n, Polyhedron& out, std::string
     out.localCenter[1] = acc[1] * inv;
     out.localCenter[2] = acc[2] * inv;
     (void)cx; (void)cy; (void)cz;
+    // inradius about the (float) local centre over the unwelded facets: the
+    // support in each facet direction minus the centre's projection
+    {
+        const V3 lc{out.localCenter[0], out.localCenter[1], out.localCenter[2]};
+        double r = 1e30;
+        for (auto& t : tmp) {
+            const V3 nn{t.plane[0], t.plane[1], t.plane[2]};
+            double h = -1e30;
+            for (auto& v : verts) h = std::max(h, dot(v, nn));
+            r = std::min(r, h - dot(lc, nn));
+        }
+        out.inradius = r < 0.0 ? 0.0 : r;
+    }
     for (int q = 0; q < 3; ++q) {
         out.aabbMin[q] = mn[q];
         out.aabbMax[q] = mx[q];

@@ -17,6 +17,10 @@ struct Polyhedron {
     float localCenter[3] = {0, 0, 0};
     float aabbMin[3] = {0, 0, 0}, aabbMax[3] = {0, 0, 0};
     float mC[3] = {0, 0, 0}, mE[3] = {0, 0, 0};
+    // distance from localCenter to the nearest facet of the exact hull
+    // (before the coplanar weld): the hull's support about its local centre
+    // is at least this in every direction
+    double inradius = 0.0;
 };
 
 bool compute_polyhedron(const float* pts, int n, Polyhedron& out, std::string* err);

@@ -61,6 +61,36 @@ struct NpParams {
     int maxPairs;
 };
 
+// Per-pair context. The clip and float-float stages keep it in the warp's
+// shared scratch (one copy per warp, written by lane 0): the functions that
+// take it by reference are not inlined, and a per-thread copy would live in
+// local memory, which at full occupancy does not fit L1.
+struct PairCtx {
+    int A, B;
+    float invMassA, invMassB;
+    const b3ConvexPolyhedron* pa;
+    const b3ConvexPolyhedron* pb;
+    float4 qA, qB;
+    Mat3 RA, RB;
+    ffmat FA, FB;  // float-float rotation matrices
+    bool haveFF;   // FA/FB valid
+    float3 posA, posB;
+};
+
+// Geometry of one FP32 clip (reference face side planes, incident face).
+struct ClipGeom {
+    const float4* sideN;   // per side plane k: normal (not unit)
+    const float4* sideP;   // per side plane k: a point on it
+    const float4* incV;    // incident face vertices, A frame
+    b3Face fA, fB;
+    Mat3 RA, RB;
+    float3 rel;      // posB - posA
+    float3 nAw;      // reference face normal (world)
+    float3 nIn;      // incident face normal (world)
+    float hIn;       // incident plane: nIn . x = hIn (A frame)
+    float eIn;       // error bound of hIn
+};
+
 // Per-warp shared scratch: two float-float polygons (x, y, z, depth).
 struct __align__(16) FfVert {
     float xh, xl, yh, yl, zh, zl, wh, wl;
@@ -71,6 +101,8 @@ struct __align__(16) WarpScratch {
     float4 sideN[kMaxPoly];   // FP32 clip: side plane normals of the reference face
     float4 sideP[kMaxPoly];   // FP32 clip: a point on each side plane
     float4 incV[kMaxPoly];    // FP32 clip: incident face vertices (A frame)
+    PairCtx ctx;
+    ClipGeom geom;
     int cand[kMaxCand];
     int refinedAxes, refinedClips;  // float-float fallbacks taken by this warp
 };
@@ -111,18 +143,6 @@ __device__ __forceinline__ void warp_argmin_ff(ff& v, int& idx) {
     }
 }
 
-struct PairCtx {
-    int A, B;
-    float invMassA, invMassB;
-    const b3ConvexPolyhedron* pa;
-    const b3ConvexPolyhedron* pb;
-    float4 qA, qB;
-    Mat3 RA, RB;
-    ffmat FA, FB;  // float-float rotation matrices
-    bool haveFF;   // FA/FB valid
-    float3 posA, posB;
-};
-
 // FP32 projection of a hull onto world axis dir, relative to the hull's own
 // position (the caller adds the position offset)
 __device__ __forceinline__ void project_rel(const float4* __restrict__ verts, int off, int nv, const Mat3& R,
@@ -141,17 +161,33 @@ __device__ __forceinline__ void project_rel(const float4* __restrict__ verts, in
 
 // Axis index space (sequential order of the reference): faces of A
 // [0, FA), faces of B [FA, FA+FB), edge pairs e0*EB+e1 after that.
-__device__ __forceinline__ bool axis_f32(const PairCtx& c, const b3::ShapesDev& S, int idx, float3 D,
-                                         float3 rel, float delta, float3& n, float& d, float& err, bool& isFace) {
+//
+// Oriented world direction of axis idx and its FP32 depth error bound;
+// false for a degenerate edge pair (|e0 x e1| components all <= 1e-6).
+// lb: a lower bound of the axis' depth that the sweep compares against its
+// depth windows. With D = cA - cB (the local centres in world space) and
+// rin the hull's inradius about its local centre (ShapesDev.inradius),
+// every axis n has
+//   depth = min(maxA - minB, maxB - minA) >= rinA + rinB - |n . D|,
+// since each hull's support about its centre is at least rin in every
+// direction. rinSum carries a margin for the radii; the FP32 error of n . D
+// and twice the axis' own depth error are subtracted too, so an axis whose
+// bound exceeds the window can neither be the first minimum nor enter the
+// near-minimum candidates (depth - err <= the minimum's depth + err).
+__device__ __forceinline__ bool axis_dir(const PairCtx& c, const b3::ShapesDev& S, int idx, float3 D, float delta,
+                                         float rinSum, float3& n, float& err, float& lb, bool& isFace,
+                                         bool wantLb = true) {
     const b3ConvexPolyhedron& pa = *c.pa;
     const b3ConvexPolyhedron& pb = *c.pb;
     const int FA = pa.numFaces, FB = pb.numFaces;
+    const float lD = wantLb ? length(D) : 0.f;
     if (idx < FA + FB) {
         isFace = true;
         const bool onA = idx < FA;
         const float4 pl = __ldg((const float4*)&S.faces[onA ? pa.faceOffset + idx : pb.faceOffset + idx - FA].plane[0]);
         n = mul(onA ? c.RA : c.RB, make_float3(pl.x, pl.y, pl.z));
         err = delta;
+        lb = wantLb ? rinSum - fabsf(dot(D, n)) - 1e-5f * (1.f + lD) - 2.f * err : -FLT_MAX;
     } else {
         isFace = false;
         const int e = idx - FA - FB;
@@ -166,21 +202,40 @@ __device__ __forceinline__ bool axis_f32(const PairCtx& c, const b3::ShapesDev& 
         // direction error of the normalised FP32 cross product is ~ulp/cl;
         // its depth error scales with the projected extents (delta / 1e-6)
         err = delta + 0.3f * delta / cl;
+        lb = wantLb ? rinSum - fabsf(dot(D, n)) - 1e-5f * (1.f + lD) - 1e-6f * lD / cl - 2.f * err : -FLT_MAX;
     }
     if (dot(D, n) < 0.f) n = -n;
+    return true;
+}
+
+// FP32 depth along the oriented axis n (P2/sat.cl:227-252, relative to
+// body A's position).
+__device__ __forceinline__ float axis_depth(const PairCtx& c, const b3::ShapesDev& S, float3 rel, float3 n) {
+    const b3ConvexPolyhedron& pa = *c.pa;
+    const b3ConvexPolyhedron& pb = *c.pb;
     float mn0, mx0, mn1, mx1;
     project_rel(S.verts, pa.vertexOffset, pa.numVertices, c.RA, n, mn0, mx0);
     project_rel(S.verts, pb.vertexOffset, pb.numVertices, c.RB, n, mn1, mx1);
     const float off = dot(rel, n);  // posB - posA along n
     mn1 += off;
     mx1 += off;
-    d = fminf(mx0 - mn1, mx1 - mn0);
+    return fminf(mx0 - mn1, mx1 - mn0);
+}
+
+// Direction and depth of axis idx; false for a degenerate edge pair.
+__device__ __forceinline__ bool axis_f32(const PairCtx& c, const b3::ShapesDev& S, int idx, float3 D,
+                                         float3 rel, float delta, float3& n, float& d, float& err, bool& isFace) {
+    float lb;
+    if (!axis_dir(c, S, idx, D, delta, 0.f, n, err, lb, isFace, false)) return false;
+    d = axis_depth(c, S, rel, n);
     return true;
 }
 
 // float-float evaluation of one axis: oriented axis and depth; false if
-// the edge pair is degenerate
-__device__ __noinline__ bool axis_ff(const PairCtx& c, const b3::ShapesDev& S, int idx, ff3 Dff, ff3& n, ff& d, bool& isFace) {
+// the edge pair is degenerate. vA / vB: the hulls' vertices (staged in
+// shared memory by the caller, or the global tables).
+__device__ __noinline__ bool axis_ff(const PairCtx& c, const b3::ShapesDev& S, const float4* vA, const float4* vB,
+                                     int idx, ff3 Dff, ff3& n, ff& d, bool& isFace) {
     const b3ConvexPolyhedron& pa = *c.pa;
     const b3ConvexPolyhedron& pb = *c.pb;
     const int FA = pa.numFaces, FB = pb.numFaces;
@@ -207,11 +262,13 @@ __device__ __noinline__ bool axis_ff(const PairCtx& c, const b3::ShapesDev& S, i
     ff lo[2], hi[2];
     for (int h = 0; h < 2; ++h) {
         const b3ConvexPolyhedron& p = h == 0 ? pa : pb;
+        const float4* verts = h == 0 ? vA : vB;
         const float3 pos = h == 0 ? c.posA : c.posB;
         const ff3 ld = mrot_t(h == 0 ? c.FA : c.FB, n);
         ff mn = mk(FLT_MAX), mx = mk(-FLT_MAX);
+#pragma unroll 2
         for (int i = 0; i < p.numVertices; ++i) {
-            const float4 v = __ldg(&S.verts[p.vertexOffset + i]);
+            const float4 v = verts[i];
             const ff dp = add(add(mulf(ld.x, v.x), mulf(ld.y, v.y)), mulf(ld.z, v.z));
             if (lt(dp, mn)) mn = dp;
             if (lt(mx, dp)) mx = dp;
@@ -260,6 +317,12 @@ __device__ __forceinline__ int sweep_axes(PairCtx& c, const b3::ShapesDev& S, in
     bool ambOverflow = false;
     float sepMin = FLT_MAX;
     float upper = FLT_MAX;  // min over axes of (d + err): bounds the true minimum depth
+    // Edge pairs are projected only when a lower bound of their depth
+    // (axis_dir) reaches the best face axis (d + err): the others can
+    // neither be the minimum nor a near-minimum candidate. The radii lose
+    // 1e-4 m for their own rounding.
+    float lbHi = FLT_MAX;
+    const float rinSum = fmaxf(0.f, S.inradius[c.pa - S.polys] + S.inradius[c.pb - S.polys] - 1e-4f);
     // faces of A and B first; a separating face axis ends the search before
     // the edge pairs, as the reference returns early (P2/sat.cl:527-530)
     for (int pass = 0; pass < 2; ++pass) {
@@ -267,9 +330,10 @@ __device__ __forceinline__ int sweep_axes(PairCtx& c, const b3::ShapesDev& S, in
         const int i1 = pass == 0 ? nFace : nAxes;
         for (int idx = i0 + lane; idx < i1; idx += 32) {
             float3 n;
-            float d, err;
+            float err, lb;
             bool isFace;
-            if (!axis_f32(c, S, idx, D, rel, delta, n, d, err, isFace)) continue;
+            if (!axis_dir(c, S, idx, D, delta, rinSum, n, err, lb, isFace, pass == 1) || lb > lbHi) continue;
+            const float d = axis_depth(c, S, rel, n);
             if (isFace) {
                 sepMin = fminf(sepMin, d);
                 if (fabsf(d) <= delta) {
@@ -284,7 +348,7 @@ __device__ __forceinline__ int sweep_axes(PairCtx& c, const b3::ShapesDev& S, in
             // insertion into the lane's sorted keep list (indices increase)
             float cd = lo;
             int ci = idx;
-    #pragma unroll
+#pragma unroll
             for (int k = 0; k < kKeep; ++k) {
                 if (cd < kd[k]) {
                     const float td = kd[k];
@@ -301,6 +365,10 @@ __device__ __forceinline__ int sweep_axes(PairCtx& c, const b3::ShapesDev& S, in
             int dz = 0;
             warp_argmin(sm0, dz);
             if (sm0 < -delta) return 0;
+            float uf = upper;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) uf = fminf(uf, __shfl_xor_sync(0xffffffffu, uf, o));
+            lbHi = uf;
         }
     }
     // clearly separated by a face axis
@@ -399,6 +467,22 @@ __device__ __forceinline__ int sweep_axes(PairCtx& c, const b3::ShapesDev& S, in
     return 2;
 }
 
+// Float-float rotation matrices of the pair, computed once per pair (the
+// context is warp-shared: lane 0 stores, the warp synchronises).
+__device__ __forceinline__ void ensure_ff(PairCtx& c) {
+    const bool have = c.haveFF;
+    __syncwarp();
+    if (!have) {
+        const ffmat a = quat_mat(c.qA), b = quat_mat(c.qB);
+        if ((threadIdx.x & 31) == 0) {
+            c.FA = a;
+            c.FB = b;
+            c.haveFF = true;
+        }
+        __syncwarp();
+    }
+}
+
 // float-float re-ranking of the sweep's candidates
 __device__ __noinline__ bool refine_axes(PairCtx& c, const b3::ShapesDev& S, WarpScratch& W, int count, ff3& sep) {
     const int lane = threadIdx.x & 31;
@@ -408,12 +492,24 @@ __device__ __noinline__ bool refine_axes(PairCtx& c, const b3::ShapesDev& S, War
     const float3 lcB = make_float3(pb.localCenter[0], pb.localCenter[1], pb.localCenter[2]);
     // float-float refinement of the candidates (matrices built only for
     // pairs that got this far)
-    c.FA = quat_mat(c.qA);
-    c.FB = quat_mat(c.qB);
-    c.haveFF = true;
+    ensure_ff(c);
     const ff3 lcAw = mrot(c.FA, make_float3(lcA.x, lcA.y, lcA.z));
     const ff3 lcBw = mrot(c.FB, make_float3(lcB.x, lcB.y, lcB.z));
     const ff3 Dff = sub3(add3(lcAw, mk3(c.posA.x, c.posA.y, c.posA.z)), add3(lcBw, mk3(c.posB.x, c.posB.y, c.posB.z)));
+    // both hulls' vertices staged in shared memory (the polygon buffers are
+    // free until the clip): every candidate lane loops over them, and
+    // dependent L2 loads would dominate the float-float projections
+    const float4* vA = S.verts + pa.vertexOffset;
+    const float4* vB = S.verts + pb.vertexOffset;
+    constexpr int kStage = (int)(sizeof(W.poly) / sizeof(float4));
+    if (pa.numVertices + pb.numVertices <= kStage) {
+        float4* st = reinterpret_cast<float4*>(&W.poly[0][0]);
+        for (int k = lane; k < pa.numVertices; k += 32) st[k] = __ldg(&vA[k]);
+        for (int k = lane; k < pb.numVertices; k += 32) st[pa.numVertices + k] = __ldg(&vB[k]);
+        __syncwarp();
+        vA = st;
+        vB = st + pa.numVertices;
+    }
     ff bd = mk(FLT_MAX);
     int bidx = kNone;
     ff3 bn = mk3(0.f, 0.f, 0.f);
@@ -423,7 +519,7 @@ __device__ __noinline__ bool refine_axes(PairCtx& c, const b3::ShapesDev& S, War
         ff3 n;
         ff d;
         bool isFace;
-        if (axis_ff(c, S, idx, Dff, n, d, isFace)) {
+        if (axis_ff(c, S, vA, vB, idx, Dff, n, d, isFace)) {
             if (isFace && d.hi < 0.f) fsep = true;
             bd = d;
             bidx = idx;
@@ -456,7 +552,6 @@ __device__ __noinline__ bool find_axis(PairCtx& c, const b3::ShapesDev& S, WarpS
     if (r == 0) return false;
     if (r == 1) {
         sep = mk3(sepf.x, sepf.y, sepf.z);
-        c.haveFF = false;
         return true;
     }
     if ((threadIdx.x & 31) == 0) ++W.refinedAxes;
@@ -554,18 +649,6 @@ constexpr int kPlaneTag = 64;
 // contact tolerance against the FP64 restatement
 constexpr float kCutBudget = 4e-6f;
 
-struct ClipGeom {
-    const float4* sideN;   // per side plane k: normal (not unit)
-    const float4* sideP;   // per side plane k: a point on it
-    const float4* incV;    // incident face vertices, A frame
-    b3Face fA, fB;
-    Mat3 RA, RB;
-    float3 rel;      // posB - posA
-    float3 nAw;      // reference face normal (world)
-    float3 nIn;      // incident face normal (world)
-    float hIn;       // incident plane: nIn . x = hIn (A frame)
-    float eIn;       // error bound of hIn
-};
 
 // a . b with TwoProd / TwoSum compensation (Ogita-Rump-Oishi Dot2): the
 // error is that of the rounded inputs only
@@ -726,24 +809,29 @@ __device__ __noinline__ int clip_f32(const PairCtx& c, const b3::ShapesDev& S, c
     const b3ConvexPolyhedron& pa = *c.pa;
     const b3ConvexPolyhedron& pb = *c.pb;
     if (ai == kNone || bi == kNone) return 0;
-    ClipGeom G;
-    G.sideN = W.sideN;
-    G.sideP = W.sideP;
-    G.incV = W.incV;
-    G.fB = S.faces[pb.faceOffset + bi];
-    G.fA = S.faces[pa.faceOffset + ai];
-    G.fB.numIndices = min(G.fB.numIndices, kMaxPoly);
-    G.fA.numIndices = min(G.fA.numIndices, kMaxPoly);
-    G.RA = c.RA;
-    G.RB = c.RB;
-    G.rel = c.posB - c.posA;
-    G.nAw = mul(c.RA, make_float3(G.fA.plane[0], G.fA.plane[1], G.fA.plane[2]));
-    G.nIn = mul(c.RB, make_float3(G.fB.plane[0], G.fB.plane[1], G.fB.plane[2]));
-    // incident plane in A's frame: nIn . x = -d_B + nIn . (posB - posA);
-    // rel is exact for nearby bodies, the dot is compensated, and the
-    // rounding of nIn only matters when B is rotated (times |rel|)
-    G.hIn = -G.fB.plane[3] + dot2(G.nIn, G.rel);
-    G.eIn = 2.5e-7f * (fabsf(G.fB.plane[3]) + fabsf(G.hIn)) + (exact_axes(c.RB) ? 0.f : 2.4e-7f * length(G.rel));
+    {
+        ClipGeom g;
+        g.sideN = W.sideN;
+        g.sideP = W.sideP;
+        g.incV = W.incV;
+        g.fB = S.faces[pb.faceOffset + bi];
+        g.fA = S.faces[pa.faceOffset + ai];
+        g.fB.numIndices = min(g.fB.numIndices, kMaxPoly);
+        g.fA.numIndices = min(g.fA.numIndices, kMaxPoly);
+        g.RA = c.RA;
+        g.RB = c.RB;
+        g.rel = c.posB - c.posA;
+        g.nAw = mul(c.RA, make_float3(g.fA.plane[0], g.fA.plane[1], g.fA.plane[2]));
+        g.nIn = mul(c.RB, make_float3(g.fB.plane[0], g.fB.plane[1], g.fB.plane[2]));
+        // incident plane in A's frame: nIn . x = -d_B + nIn . (posB - posA);
+        // rel is exact for nearby bodies, the dot is compensated, and the
+        // rounding of nIn only matters when B is rotated (times |rel|)
+        g.hIn = -g.fB.plane[3] + dot2(g.nIn, g.rel);
+        g.eIn = 2.5e-7f * (fabsf(g.fB.plane[3]) + fabsf(g.hIn)) + (exact_axes(c.RB) ? 0.f : 2.4e-7f * length(g.rel));
+        if (lane == 0) W.geom = g;
+        __syncwarp();
+    }
+    const ClipGeom& G = W.geom;
     int nIn = G.fB.numIndices;
     const int nvA = G.fA.numIndices;
     // per-pair tables in shared memory: incident vertices and side planes
@@ -894,11 +982,7 @@ __device__ __noinline__ int select_face(const b3::ShapesDev& S, PairCtx& c, bool
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) inWin += __shfl_xor_sync(0xffffffffu, inWin, o);
     if (inWin <= 1) return wi;
-    if (!c.haveFF) {
-        c.FA = quat_mat(c.qA);
-        c.FB = quat_mat(c.qB);
-        c.haveFF = true;
-    }
+    ensure_ff(c);
     const ffmat& F = sideA ? c.FA : c.FB;
     ff rv = mk(FLT_MAX);
     int ri = kNone;
@@ -919,11 +1003,7 @@ __device__ __noinline__ int select_face(const b3::ShapesDev& S, PairCtx& c, bool
 // W.poly[*outBuf].
 __device__ __noinline__ int clip_hull_hull(PairCtx& c, const b3::ShapesDev& S, const NpParams& P, ff3 sep,
                               int ai, int bi, WarpScratch& W, int* outBuf, int* ovf) {
-    if (!c.haveFF) {
-        c.FA = quat_mat(c.qA);
-        c.FB = quat_mat(c.qB);
-        c.haveFF = true;
-    }
+    ensure_ff(c);
     const int lane = threadIdx.x & 31;
     const b3ConvexPolyhedron& pa = *c.pa;
     const b3ConvexPolyhedron& pb = *c.pb;
@@ -1045,6 +1125,31 @@ __device__ __forceinline__ bool pair_setup(PairCtx& c, int2 pr, const b3::Bodies
     return true;
 }
 
+// pair_setup into the warp-shared context: every lane computes, lane 0
+// stores, the warp synchronises.
+__device__ __forceinline__ void pair_setup_shared(PairCtx& c, int2 pr, const b3::BodiesDev& Bd,
+                                                  const b3::ShapesDev& S) {
+    PairCtx t;
+    pair_setup(t, pr, Bd, S);
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) {
+        c.A = t.A;
+        c.B = t.B;
+        c.invMassA = t.invMassA;
+        c.invMassB = t.invMassB;
+        c.pa = t.pa;
+        c.pb = t.pb;
+        c.qA = t.qA;
+        c.qB = t.qB;
+        c.RA = t.RA;
+        c.RB = t.RB;
+        c.haveFF = false;
+        c.posA = t.posA;
+        c.posB = t.posB;
+    }
+    __syncwarp();
+}
+
 // Contact4 of pair p from the kept points pts[0..nOut) and the chosen
 // indices (newContactReductionKernel, P2/satClipHullContacts.cl:1958-2039).
 __device__ __forceinline__ void emit_contact(int p, const PairCtx& c, const FfVert* pts, int nRed, int4 idx,
@@ -1090,7 +1195,7 @@ __device__ __forceinline__ int push(int* queue, int32_t* count, int p) {
 // finished here; pairs whose axis the sweep decides go to the FP32 clip
 // queue with that axis; pairs with near-minimum candidates go to the
 // float-float queue.
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 5)
 k_np_sweep(const int2* __restrict__ pairs, const int32_t* __restrict__ numPairsDev, b3::BodiesDev Bd,
            b3::ShapesDev S, uint32_t* __restrict__ manifoldFlag, float4* __restrict__ pairSep,
            int* __restrict__ fastQ, int* __restrict__ slowQ, int* __restrict__ cand, int candSlots,
@@ -1129,7 +1234,7 @@ k_np_sweep(const int2* __restrict__ pairs, const int32_t* __restrict__ numPairsD
 // Stage 2, pairs with an FP32 axis: face selection, clipping and reduction
 // in FP32 with error bounds; any doubt sends the pair to the float-float
 // queue instead.
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 5)
 k_np_clip(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, NpParams P,
           float4* __restrict__ pairSep, const int* __restrict__ fastQ, int* __restrict__ slowQ,
           b3Contact4* __restrict__ contacts, uint32_t* __restrict__ manifoldFlag, int32_t* __restrict__ scalars,
@@ -1144,8 +1249,8 @@ k_np_clip(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, NpP
         const int chunkEnd = min(chunk + kChunk, nFast);
         for (int q = chunk; q < chunkEnd; ++q) {
             const int p = fastQ[q];
-            PairCtx c;
-            pair_setup(c, pairs[p], Bd, S);
+            PairCtx& c = W.ctx;
+            pair_setup_shared(c, pairs[p], Bd, S);
             const float4 s4 = pairSep[p];
             const float3 sepf = make_float3(s4.x, s4.y, s4.z);
             const ff3 sep = mk3(sepf.x, sepf.y, sepf.z);
@@ -1178,7 +1283,7 @@ k_np_clip(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, NpP
 
 // Stage 3, the pairs either stage handed on: the whole chain with
 // float-float refinement of the axis, the faces, the clip and the reduction.
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 4)
 k_np_exact(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, NpParams P,
            const float4* __restrict__ pairSep, const int* __restrict__ slowQ, const int* __restrict__ cand,
            b3Contact4* __restrict__ contacts,
@@ -1199,8 +1304,8 @@ k_np_exact(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, Np
         const int chunkEnd = min(chunk + 1, nSlow);
         for (int q = chunk; q < chunkEnd; ++q) {
             const int p = slowQ[q];
-            PairCtx c;
-            pair_setup(c, pairs[p], Bd, S);
+            PairCtx& c = W.ctx;
+            pair_setup_shared(c, pairs[p], Bd, S);
             int nOut = 0, buf = 0;
             ff3 sep = mk3(0.f, 0.f, 0.f);
             const float4 s4 = pairSep[p];

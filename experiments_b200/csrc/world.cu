@@ -66,7 +66,7 @@ int dalloc(T*& p, size_t count) {
 void free_all(b3::DevBuffers& d) {
     void* ptrs[] = {d.pos, d.quat, d.linVel, d.angVel, d.invMass, d.friction, d.restitution,
                     d.invInertia, d.collidable, d.worldId, d.cols, d.polys, d.verts, d.faces,
-                    d.indices, d.edges, d.localAabb, d.aabbMin, d.aabbMax, d.smallSlot,
+                    d.indices, d.edges, d.localAabb, d.polyInradius, d.aabbMin, d.aabbMax, d.smallSlot,
                     d.largeStart, d.largeList, d.keys, d.vals, d.keysAlt, d.valsAlt, d.cellTable,
                     d.pairs, d.contacts, d.manifoldFlag, d.pairSep, d.npFast, d.npSlow, d.npCand, d.manifoldScan,
                     d.manifoldPair,
@@ -133,6 +133,7 @@ b3::ShapesDev b3World_t::shapesDev() const {
     S.indices = d.indices;
     S.edges = d.edges;
     S.localAabb = d.localAabb;
+    S.inradius = d.polyInradius;
     S.numPolys = (int)polys.size();
     S.numVerts = (int)verts4.size() / 4;
     S.numFaces = (int)faces.size();
@@ -251,6 +252,10 @@ extern "C" int b3_register_convex_hull(b3World w, const float* vertices, int num
         r = std::min(r, std::fabs(f.plane[0] * P.localCenter[0] + f.plane[1] * P.localCenter[1] +
                                   f.plane[2] * P.localCenter[2] + f.plane[3]));
     poly.radius = r;
+    // rounded down to float: a lower bound stays a lower bound
+    float rin = (float)P.inradius;
+    if ((double)rin > P.inradius) rin = std::nextafter(rin, 0.f);
+    w->polyInradius.push_back(rin);
     poly.numVertices = (int)P.vertices.size() / 3;
     poly.vertexOffset = (int)w->verts4.size() / 4;
     for (int i = 0; i < poly.numVertices; ++i) {
@@ -454,6 +459,7 @@ static int upload_shapes(b3World w, cudaStream_t st) {
     B3_TRY(dalloc(d.indices, w->indices.size()));
     B3_TRY(dalloc(d.edges, w->edges4.size() / 4 + 1));
     B3_TRY(dalloc(d.localAabb, w->localAabb8.size() / 4));
+    B3_TRY(dalloc(d.polyInradius, w->polyInradius.size()));
     B3_CUDA(cudaMemcpyAsync(d.cols, w->cols.data(), sizeof(b3Collidable) * w->cols.size(), cudaMemcpyHostToDevice, st));
     B3_CUDA(cudaMemcpyAsync(d.polys, w->polys.data(), sizeof(b3ConvexPolyhedron) * w->polys.size(), cudaMemcpyHostToDevice, st));
     B3_CUDA(cudaMemcpyAsync(d.verts, w->verts4.data(), sizeof(float) * w->verts4.size(), cudaMemcpyHostToDevice, st));
@@ -462,6 +468,8 @@ static int upload_shapes(b3World w, cudaStream_t st) {
     if (!w->edges4.empty())
         B3_CUDA(cudaMemcpyAsync(d.edges, w->edges4.data(), sizeof(float) * w->edges4.size(), cudaMemcpyHostToDevice, st));
     B3_CUDA(cudaMemcpyAsync(d.localAabb, w->localAabb8.data(), sizeof(float) * w->localAabb8.size(), cudaMemcpyHostToDevice, st));
+    B3_CUDA(cudaMemcpyAsync(d.polyInradius, w->polyInradius.data(), sizeof(float) * w->polyInradius.size(),
+                            cudaMemcpyHostToDevice, st));
     w->shapesDirty = false;
     return B3_OK;
 }
