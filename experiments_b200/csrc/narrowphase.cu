@@ -44,9 +44,11 @@ namespace {
 using namespace b3ff;
 
 constexpr int kMaxPoly = 64;  // capacityWorldVerts (satClipHullContacts.cl:1027)
-constexpr int kChunk = 4;     // pairs per work grab
 constexpr int kKeep = 4;      // near-minimum axis candidates kept per lane
 constexpr int kMaxCand = 32;  // candidates refined in float-float per pair
+constexpr int kPreChunk = 4;  // pairs per work grab of the sweep and the clip, prefetched by lanes
+// shared memory of one sweep warp: the prefetched chunk and the candidates
+constexpr int kSweepWarpSmem = 128 * kPreChunk + 4 * kMaxCand;
 constexpr int kNone = 0x7fffffff;
 // pairSep[p].w: how the pair reached the exact stage
 constexpr int kSepRefine = 0;      // near-minimum axes: float-float re-ranking
@@ -1125,6 +1127,60 @@ __device__ __forceinline__ bool pair_setup(PairCtx& c, int2 pr, const b3::Bodies
     return true;
 }
 
+// Setup data of one pair, loaded by one lane for a chunk of pairs: the
+// chain of dependent loads (pair -> collidables -> shapes, poses) is paid
+// once per chunk instead of once per pair.
+struct __align__(16) PairPre {
+    float4 qA, qB, pA, pB;
+    float4 aux;        // the clip stage: the pair's separating axis
+    int A, B;
+    int shapeA, shapeB;  // shapeA < 0: a pair the narrowphase skips
+    float invMassA, invMassB;
+    int p;
+    int pad[5];
+};
+static_assert(sizeof(PairPre) == 128, "PairPre: 128 bytes");
+static_assert(sizeof(WarpScratch::planes) >= sizeof(PairPre) * kPreChunk, "clip chunk in the plane table");
+
+__device__ __forceinline__ void pair_prefetch(PairPre& q, int p, int2 pr, const b3::BodiesDev& Bd,
+                                              const b3::ShapesDev& S) {
+    q.p = p;
+    q.A = pr.x;
+    q.B = pr.y;
+    q.invMassA = Bd.invMass[pr.x];
+    q.invMassB = Bd.invMass[pr.y];
+    const b3Collidable colA = S.cols[Bd.collidable[pr.x]];
+    const b3Collidable colB = S.cols[Bd.collidable[pr.y]];
+    const bool ok = !(q.invMassA == 0.f && q.invMassB == 0.f) && colA.shapeType == B3_SHAPE_CONVEX_HULL &&
+                    colB.shapeType == B3_SHAPE_CONVEX_HULL;
+    q.shapeA = ok ? colA.shapeIndex : -1;
+    q.shapeB = colB.shapeIndex;
+    q.qA = Bd.quat[pr.x];
+    q.qB = Bd.quat[pr.y];
+    q.pA = Bd.pos[pr.x];
+    q.pB = Bd.pos[pr.y];
+}
+
+// PairCtx of a prefetched pair (pair_setup's result); false for a skipped
+// pair.
+__device__ __forceinline__ bool pair_from_pre(PairCtx& c, const PairPre& q, const b3::ShapesDev& S) {
+    if (q.shapeA < 0) return false;
+    c.A = q.A;
+    c.B = q.B;
+    c.invMassA = q.invMassA;
+    c.invMassB = q.invMassB;
+    c.pa = &S.polys[q.shapeA];
+    c.pb = &S.polys[q.shapeB];
+    c.qA = q.qA;
+    c.qB = q.qB;
+    c.RA = quat_to_mat(c.qA);
+    c.RB = quat_to_mat(c.qB);
+    c.posA = f3(q.pA);
+    c.posB = f3(q.pB);
+    c.haveFF = false;
+    return true;
+}
+
 // pair_setup into the warp-shared context: every lane computes, lane 0
 // stores, the warp synchronises.
 __device__ __forceinline__ void pair_setup_shared(PairCtx& c, int2 pr, const b3::BodiesDev& Bd,
@@ -1175,7 +1231,7 @@ __device__ __forceinline__ void emit_contact(int p, const PairCtx& c, const FfVe
     }
 }
 
-__device__ __forceinline__ int next_work(int32_t* counter, int limit, int chunk = kChunk) {
+__device__ __forceinline__ int next_work(int32_t* counter, int limit, int chunk) {
     int w = 0;
     if ((threadIdx.x & 31) == 0) w = atomicAdd(counter, chunk);
     w = __shfl_sync(0xffffffffu, w, 0);
@@ -1202,17 +1258,22 @@ k_np_sweep(const int2* __restrict__ pairs, const int32_t* __restrict__ numPairsD
            int32_t* __restrict__ scalars, b3Counters* __restrict__ counters) {
     extern __shared__ __align__(16) unsigned char np_smem[];
     const int lane = threadIdx.x & 31;
-    int* wcand = reinterpret_cast<int*>(np_smem) + kMaxCand * (threadIdx.x >> 5);
+    unsigned char* wbase = np_smem + (size_t)(threadIdx.x >> 5) * kSweepWarpSmem;
+    PairPre* pre = reinterpret_cast<PairPre*>(wbase);
+    int* wcand = reinterpret_cast<int*>(wbase + sizeof(PairPre) * kPreChunk);
     const int numPairs = *numPairsDev;
     for (;;) {
-        const int chunk = next_work(scalars + b3::S_NP_WORK, numPairs);
+        const int chunk = next_work(scalars + b3::S_NP_WORK, numPairs, kPreChunk);
         if (chunk < 0) break;
-        const int chunkEnd = min(chunk + kChunk, numPairs);
-        for (int p = chunk; p < chunkEnd; ++p) {
+        const int n = min(kPreChunk, numPairs - chunk);
+        if (lane < n) pair_prefetch(pre[lane], chunk + lane, pairs[chunk + lane], Bd, S);
+        __syncwarp();
+        for (int i = 0; i < n; ++i) {
+            const int p = chunk + i;
             PairCtx c;
             int r = 0, count = 0;
             float3 sepf = make_float3(0.f, 0.f, 0.f);
-            if (pair_setup(c, pairs[p], Bd, S)) r = sweep_axes(c, S, wcand, sepf, count, &counters->clipOverflow);
+            if (pair_from_pre(c, pre[i], S)) r = sweep_axes(c, S, wcand, sepf, count, &counters->clipOverflow);
             if (r == 0) {
                 if (lane == 0) manifoldFlag[p] = 0u;
             } else if (r == 1) {
@@ -1243,15 +1304,29 @@ k_np_clip(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, NpP
     const int lane = threadIdx.x & 31;
     WarpScratch& W = reinterpret_cast<WarpScratch*>(np_smem)[threadIdx.x >> 5];
     const int nFast = scalars[b3::S_NP_FAST];
+    // the prefetched chunk lives in the float-float plane table, which only
+    // the exact stage uses
+    PairPre* pre = reinterpret_cast<PairPre*>(W.planes);
     for (;;) {
-        const int chunk = next_work(scalars + b3::S_NP_WORK2, nFast);
+        const int chunk = next_work(scalars + b3::S_NP_WORK2, nFast, kPreChunk);
         if (chunk < 0) break;
-        const int chunkEnd = min(chunk + kChunk, nFast);
-        for (int q = chunk; q < chunkEnd; ++q) {
-            const int p = fastQ[q];
+        const int n = min(kPreChunk, nFast - chunk);
+        if (lane < n) {
+            const int p = fastQ[chunk + lane];
+            pair_prefetch(pre[lane], p, pairs[p], Bd, S);
+            pre[lane].aux = pairSep[p];
+        }
+        __syncwarp();
+        for (int i = 0; i < n; ++i) {
+            const int p = pre[i].p;
             PairCtx& c = W.ctx;
-            pair_setup_shared(c, pairs[p], Bd, S);
-            const float4 s4 = pairSep[p];
+            {
+                PairCtx t;
+                pair_from_pre(t, pre[i], S);
+                if (lane == 0) c = t;
+                __syncwarp();
+            }
+            const float4 s4 = pre[i].aux;
             const float3 sepf = make_float3(s4.x, s4.y, s4.z);
             const ff3 sep = mk3(sepf.x, sepf.y, sepf.z);
             // incident face of B: max dot(nB, sep); reference face of A: min dot(nA, sep)
@@ -1393,7 +1468,7 @@ int launch_narrowphase(b3World_t* w, cudaStream_t st) {
     const b3::BodiesDev Bd = w->bodiesDev();
     const b3::ShapesDev S = w->shapesDev();
     int32_t* sc = w->d.scalars;
-    const size_t smemSweep = sizeof(int) * kMaxCand * w->npWarpsPerBlock;
+    const size_t smemSweep = (size_t)kSweepWarpSmem * w->npWarpsPerBlock;
     int occS = 1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occS, k_np_sweep, threads, smemSweep) != cudaSuccess || occS < 1)
         occS = 1;
