@@ -14,6 +14,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
 LIB_F32 = os.path.join(HERE, "liboracle_f32.so")
+LIB_DUAL = os.path.join(HERE, "liboracle_dual.so")
 REF_LIB = os.path.join(HERE, "_ref", "libb3ref.so")
 BULLET_LIB = os.path.join(HERE, "_ref", "libb3bullet.so")
 
@@ -31,8 +32,6 @@ class OrContact(C.Structure):
                 ("pairIndex", C.c_int), ("bodyA", C.c_int), ("bodyB", C.c_int), ("pad", C.c_int)]
 
 
-_lib = None
-_lib32 = None
 _ref = None
 _bullet = None
 _D = C.POINTER(C.c_double)
@@ -42,12 +41,16 @@ _U = C.POINTER(C.c_uint32)
 _VP = C.c_void_p
 
 
-def lib(f32=False):
-    """The FP64 oracle, or with f32=True the same restatement in FP32 (used
-    to tell precision effects from logic differences)."""
-    global _lib, _lib32
-    if (_lib32 if f32 else _lib) is None:
-        path = LIB_F32 if f32 else LIB
+_libs = {}
+
+
+def lib(f32=False, dual=False):
+    """The FP64 oracle; with f32=True the same restatement in FP32 (used to
+    tell precision effects from logic differences); with dual=True the FP64
+    restatement carrying forward-mode derivatives (tangent-linear build)."""
+    kind = "dual" if dual else ("f32" if f32 else "f64")
+    if kind not in _libs:
+        path = {"f64": LIB, "f32": LIB_F32, "dual": LIB_DUAL}[kind]
         if not os.path.exists(path):
             from . import build
             build.build_oracle()
@@ -76,11 +79,11 @@ def lib(f32=False):
         L.or_reset_active.argtypes = [_VP]
         L.or_set_params_f64.argtypes = [_VP, _D, _D, _D]
         L.or_clip_face_world.argtypes = [_D, C.c_int, _D, _D, C.c_int, C.c_double, C.c_double, _D]
-        if f32:
-            _lib32 = L
-        else:
-            _lib = L
-    return _lib32 if f32 else _lib
+        L.or_set_tangent.argtypes = [_VP, _D, _D, _D, _D, _D]
+        L.or_get_tangent.argtypes = [_VP, _D, _D, _D, _D]
+        L.or_real_kind.restype = C.c_int
+        _libs[kind] = L
+    return _libs[kind]
 
 
 def ref_lib():
@@ -173,8 +176,8 @@ class OracleWorld:
     """Oracle world built from a registered product world's shape tables
     (hull construction is checked separately against btConvexUtility)."""
 
-    def __init__(self, scene, shapes, cfg, inv_inertia, is_large, f32=False):
-        L = lib(f32)
+    def __init__(self, scene, shapes, cfg, inv_inertia, is_large, f32=False, dual=False):
+        L = lib(f32, dual)
         self.n = scene.n
         c = OrConfig()
         c.cellSize = cfg.cellSize
@@ -298,6 +301,27 @@ class OracleWorld:
         self.L.or_get_overflow(self.h, C.byref(a), C.byref(b))
         return a.value, b.value
 
+    def set_tangent(self, lin=None, ang=None, inv_mass=None, inv_inertia3=None, friction=None):
+        """Derivative seeds (tangent-linear build): initial linear / angular
+        velocities (n x 3), inverse masses, local inverse inertia diagonals
+        (n x 3) and friction coefficients; None means zero."""
+        keep = []
+        for a, cols in ((lin, 4), (ang, 4), (inv_mass, 1), (inv_inertia3, 3), (friction, 1)):
+            if a is None:
+                keep.append(None)
+                continue
+            a = np.asarray(a, np.float64).reshape(self.n, -1)
+            b = np.zeros((self.n, cols))
+            b[:, :a.shape[1]] = a
+            keep.append(np.ascontiguousarray(b))
+        self.L.or_set_tangent(self.h, *[None if a is None else _d(a) for a in keep])
+
+    def tangent(self):
+        """Derivatives of (pos, quat, lin, ang), each n x 4."""
+        out = [np.zeros((self.n, 4), np.float64) for _ in range(4)]
+        self.L.or_get_tangent(self.h, *[_d(a) for a in out])
+        return out
+
     def solve_velocities(self):
         lin = np.zeros((self.n, 4))
         ang = np.zeros((self.n, 4))
@@ -334,7 +358,7 @@ class OracleWorld:
             pass
 
 
-def oracle_from_world(world, scene, cfg=None, f32=False):
+def oracle_from_world(world, scene, cfg=None, f32=False, dual=False):
     """Build an OracleWorld from a registered PhysicsWorld (host-only
     context suffices) and its scene."""
     cfg = cfg or world.cfg
@@ -346,7 +370,7 @@ def oracle_from_world(world, scene, cfg=None, f32=False):
     inv_inertia = world.inertias()
     # large-body classification rule (half-diagonal of the registration AABB)
     is_large = large_flags(world, scene, cfg)
-    return OracleWorld(scene, sh, cfg, inv_inertia, is_large, f32=f32)
+    return OracleWorld(scene, sh, cfg, inv_inertia, is_large, f32=f32, dual=dual)
 
 
 def large_flags(world, scene, cfg):

@@ -36,10 +36,34 @@
 #include <limits>
 #include <vector>
 
+#ifdef ORACLE_DUAL
+// tangent-linear build: every Real carries a derivative along one direction
+#include "b3_dual.h"
+#define ORACLE_REAL b3dual::Dual
+#endif
 #ifndef ORACLE_REAL
 #define ORACLE_REAL double
 #endif
 typedef ORACLE_REAL Real;
+
+// value and tangent of a Real, the same source for every build
+inline double rval(double x) { return x; }
+inline double rval(float x) { return x; }
+inline double rtan(double) { return 0.0; }
+inline double rtan(float) { return 0.0; }
+inline void set_tan(double&, double) {}
+inline void set_tan(float&, double) {}
+#ifdef ORACLE_DUAL
+inline double rval(const b3dual::Dual& x) { return x.v; }
+inline double rtan(const b3dual::Dual& x) { return x.d; }
+inline void set_tan(b3dual::Dual& x, double d) { x.d = d; }
+#endif
+// unqualified calls: the std overloads for double / float, the dual ones
+// by argument-dependent lookup
+using std::cos;
+using std::fabs;
+using std::sin;
+using std::sqrt;
 
 namespace {
 
@@ -56,7 +80,7 @@ inline Real dot(V a, V b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 inline V cross(V a, V b) { return V(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
 inline V mulv(V a, V b) { return V(a.x * b.x, a.y * b.y, a.z * b.z); }
 inline V normalize(V a) {
-    Real l = std::sqrt(dot(a, a));
+    Real l = sqrt(dot(a, a));
     return l > 0 ? a * (1.0 / l) : a;
 }
 struct Q {
@@ -95,10 +119,16 @@ struct or_face {
     float plane[4];
     int indexOffset, numIndices, pad[2];
 };
-struct or_contact {  // Contact4-like, FP64
+struct or_contact {  // Contact4-like, FP64 (the exported layout)
     double pos[4][4];
     double normal[4];  // w = nPoints
     double friction;
+    int pairIndex, bodyA, bodyB, pad;
+};
+struct or_contact_r {  // the same in Real (internal storage)
+    Real pos[4][4];
+    Real normal[4];
+    Real friction;
     int pairIndex, bodyA, bodyB, pad;
 };
 
@@ -140,7 +170,7 @@ struct or_world {
     std::vector<float> aabb;                 // 8 per body
     std::vector<uint32_t> keys, vals;        // sorted (small bodies)
     std::vector<int> pairs;                  // 2 per pair
-    std::vector<or_contact> contacts;        // manifolds in pair order
+    std::vector<or_contact_r> contacts;      // manifolds in pair order
     std::vector<Real> avgLin, avgAng;        // 3 per body (sum/count after the last average)
     std::vector<int> count;                  // copies per body
     // per-world signature of the discrete choices (pairs with manifolds,
@@ -378,7 +408,7 @@ void edge_axes(const or_world* w, const or_poly& hA, const or_poly& hB, const Bo
             const float* eb = &w->edges4[4 * (hB.uniqueEdgesOffset + e1)];
             const V wb = qrot(B.q, V(eb[0], eb[1], eb[2]));
             V c = cross(wa, wb);
-            if (!(std::fabs(c.x) > 1e-6 || std::fabs(c.y) > 1e-6 || std::fabs(c.z) > 1e-6)) continue;
+            if (!(fabs(c.x) > 1e-6 || fabs(c.y) > 1e-6 || fabs(c.z) > 1e-6)) continue;
             c = normalize(c);
             if (dot(D, c) < 0) c = -c;
             Real mn0, mx0, mn1, mx1;
@@ -580,9 +610,9 @@ int reduce_manifold(const std::vector<P4>& p, V nearNormal, int idx[4]) {
     return 4;
 }
 
-Real combine_friction(Real a, Real b, int mode) { return mode == 1 ? a * b : std::sqrt(a * b); }
+Real combine_friction(Real a, Real b, int mode) { return mode == 1 ? a * b : sqrt(a * b); }
 
-bool contact_for_pair(const or_world* w, int pairIndex, int A, int B, or_contact& out) {
+bool contact_for_pair(const or_world* w, int pairIndex, int A, int B, or_contact_r& out) {
     if (w->invMass[A] == 0.f && w->invMass[B] == 0.f) return false;  // sat.cl:944-948
     const or_poly& hA = w->polys[w->colShape[w->col[A]]];
     const or_poly& hB = w->polys[w->colShape[w->col[B]]];
@@ -612,7 +642,7 @@ bool contact_for_pair(const or_world* w, int pairIndex, int A, int B, or_contact
     const V nrm = -sep;
     int idx[4];
     const int nr = reduce_manifold(pts, nrm, idx);
-    memset(&out, 0, sizeof(out));
+    out = or_contact_r();
     out.pad = (int)std::min<size_t>(pts.size(), 127) | (idx[0] << 7) | (idx[1] << 13) | (idx[2] << 19) | (idx[3] << 25);
     for (int k = 0; k < nr; ++k) {
         const P4& q = pts[idx[k]];
@@ -630,7 +660,7 @@ void stage_narrowphase(or_world* w) {
     w->contacts.clear();
     const int np = (int)w->pairs.size() / 2;
     for (int p = 0; p < np; ++p) {
-        or_contact c;
+        or_contact_r c;
         if (contact_for_pair(w, p, w->pairs[2 * p], w->pairs[2 * p + 1], c)) {
             w->contacts.push_back(c);
             const int A = std::abs(c.bodyA), B = std::abs(c.bodyB);
@@ -663,14 +693,14 @@ struct MRows {
 
 void plane_space(V n, V& p, V& q) {
     const Real SQRT12 = 0.7071067811865475244008443621048490;
-    if (std::fabs(n.z) > SQRT12) {
+    if (fabs(n.z) > SQRT12) {
         const Real a = n.y * n.y + n.z * n.z;
-        const Real k = 1.0 / std::sqrt(a);
+        const Real k = 1.0 / sqrt(a);
         p = V(0, -n.z * k, n.y * k);
         q = V(a * k, -n.x * p.z, n.x * p.y);
     } else {
         const Real a = n.x * n.x + n.y * n.y;
-        const Real k = 1.0 / std::sqrt(a);
+        const Real k = 1.0 / sqrt(a);
         p = V(-n.y * k, n.x * k, 0);
         q = V(-n.z * p.y, n.z * p.x, a * k);
     }
@@ -708,7 +738,7 @@ void stage_solve(or_world* w) {
     const Real dt = w->cfg.dt;
     // m_bodyCount (:1105-1129)
     w->count.assign(N, 0);
-    for (const or_contact& c : w->contacts) {
+    for (const or_contact_r& c : w->contacts) {
         const int A = std::abs(c.bodyA), B = std::abs(c.bodyB);
         if (w->invMass[A] != 0.f) w->count[A]++;
         if (w->invMass[B] != 0.f) w->count[B]++;
@@ -728,7 +758,7 @@ void stage_solve(or_world* w) {
     };
     std::vector<MRows> ms;
     ms.reserve(M);
-    for (const or_contact& c : w->contacts) {
+    for (const or_contact_r& c : w->contacts) {
         MRows m;
         m.A = std::abs(c.bodyA);
         m.B = std::abs(c.bodyB);
@@ -751,7 +781,7 @@ void stage_solve(or_world* w) {
         const V wB = dynB ? V(w->ang[4 * m.B], w->ang[4 * m.B + 1], w->ang[4 * m.B + 2]) : V();
         const Real restitution = (Real)w->restitution[m.A] * (Real)w->restitution[m.B];
         const V n = normalize(V(-c.normal[0], -c.normal[1], -c.normal[2]));
-        const int npts = (int)c.normal[3];
+        const int npts = (int)rval(c.normal[3]);
         for (int j = 0; j < npts; ++j) {
             const Real dist = c.pos[j][3] + (Real)w->cfg.slopOffset;
             if (!(dist <= (Real)w->cfg.contactProcessing)) continue;
@@ -792,7 +822,7 @@ void stage_solve(or_world* w) {
                                                    16 + (penetration > 0 ? 1 : 0) + (rest > 0 ? 2 : 0) +
                                                        (lat > (Real)FLT_EPSILON ? 4 : 0) + 8 * j);
             if (lat > (Real)FLT_EPSILON) {
-                d1v = d1v * (1.0 / std::sqrt(lat));
+                d1v = d1v * (1.0 / sqrt(lat));
                 d2v = normalize(cross(d1v, n));
             } else {
                 plane_space(n, d1v, d2v);
@@ -901,19 +931,19 @@ void stage_integrate(or_world* w) {
                 }
         }
         for (int k = 0; k < 3; ++k) a[k] *= (Real)w->cfg.angularDamping;
-        Real fAngle = std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+        Real fAngle = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
         if (fAngle * dt > thr) fAngle = thr / dt;
         Real s;
         if (fAngle < 0.001) s = 0.5 * dt - (dt * dt * dt) * 0.020833333333 * fAngle * fAngle;
-        else s = std::sin(0.5 * fAngle * dt) / fAngle;
-        const Real dq[4] = {a[0] * s, a[1] * s, a[2] * s, std::cos(fAngle * dt * 0.5)};
+        else s = sin(0.5 * fAngle * dt) / fAngle;
+        const Real dq[4] = {a[0] * s, a[1] * s, a[2] * s, cos(fAngle * dt * 0.5)};
         Real* q = &w->quat[4 * i];
         Real r[4];
         r[0] = dq[3] * q[0] + dq[0] * q[3] + dq[1] * q[2] - dq[2] * q[1];
         r[1] = dq[3] * q[1] + dq[1] * q[3] + dq[2] * q[0] - dq[0] * q[2];
         r[2] = dq[3] * q[2] + dq[2] * q[3] + dq[0] * q[1] - dq[1] * q[0];
         r[3] = dq[3] * q[3] - dq[0] * q[0] - dq[1] * q[1] - dq[2] * q[2];
-        const Real len = std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2] + r[3] * r[3]);
+        const Real len = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2] + r[3] * r[3]);
         if (len > 0) for (int k = 0; k < 4; ++k) q[k] = r[k] / len;
         else { q[0] = q[1] = q[2] = 0; q[3] = 1; }
         for (int k = 0; k < 3; ++k) w->pos[4 * i + k] += v[k] * dt;
@@ -1010,11 +1040,46 @@ void or_set_state_f64(or_world* w, const double* pos4, const double* quat4, cons
 }
 void or_get_state(or_world* w, double* pos4, double* quat4, double* lin4, double* ang4) {
     for (size_t i = 0; i < 4 * (size_t)w->n; ++i) {
-        if (pos4) pos4[i] = w->pos[i];
-        if (quat4) quat4[i] = w->quat[i];
-        if (lin4) lin4[i] = w->lin[i];
-        if (ang4) ang4[i] = w->ang[i];
+        if (pos4) pos4[i] = rval(w->pos[i]);
+        if (quat4) quat4[i] = rval(w->quat[i]);
+        if (lin4) lin4[i] = rval(w->lin[i]);
+        if (ang4) ang4[i] = rval(w->ang[i]);
     }
+}
+
+// Tangent-linear build: derivative seeds of the initial velocities and of
+// the body parameters (NULL leaves a set at zero derivative), and the
+// derivatives of the state after the steps. The FP64 and FP32 builds carry
+// no derivatives (set is a no-op, get returns zeros).
+void or_set_tangent(or_world* w, const double* dlin4, const double* dang4, const double* dInvMass,
+                    const double* dInvInertia3, const double* dFriction) {
+    for (int i = 0; i < w->n; ++i) {
+        for (int k = 0; k < 4; ++k) {
+            set_tan(w->pos[4 * i + k], 0.0);
+            set_tan(w->quat[4 * i + k], 0.0);
+            set_tan(w->lin[4 * i + k], dlin4 ? dlin4[4 * i + k] : 0.0);
+            set_tan(w->ang[4 * i + k], dang4 ? dang4[4 * i + k] : 0.0);
+        }
+        set_tan(w->invMass[i], dInvMass ? dInvMass[i] : 0.0);
+        set_tan(w->friction[i], dFriction ? dFriction[i] : 0.0);
+        for (int k = 0; k < 3; ++k) set_tan(w->invInertia[3 * i + k], dInvInertia3 ? dInvInertia3[3 * i + k] : 0.0);
+    }
+}
+void or_get_tangent(or_world* w, double* dpos4, double* dquat4, double* dlin4, double* dang4) {
+    for (size_t i = 0; i < 4 * (size_t)w->n; ++i) {
+        if (dpos4) dpos4[i] = rtan(w->pos[i]);
+        if (dquat4) dquat4[i] = rtan(w->quat[i]);
+        if (dlin4) dlin4[i] = rtan(w->lin[i]);
+        if (dang4) dang4[i] = rtan(w->ang[i]);
+    }
+}
+// 0 = FP64, 1 = FP32, 2 = FP64 with tangents
+int or_real_kind() {
+#ifdef ORACLE_DUAL
+    return 2;
+#else
+    return sizeof(Real) == 4 ? 1 : 0;
+#endif
 }
 
 void or_stage_aabbs(or_world* w) { stage_aabbs(w); }
@@ -1048,9 +1113,23 @@ int or_get_pairs(or_world* w, int* pairs2, int max) {
     if (pairs2) memcpy(pairs2, w->pairs.data(), 8 * (size_t)n);
     return (int)w->pairs.size() / 2;
 }
+or_contact export_contact(const or_contact_r& c) {
+    or_contact o;
+    for (int j = 0; j < 4; ++j) {
+        for (int k = 0; k < 4; ++k) o.pos[j][k] = rval(c.pos[j][k]);
+        o.normal[j] = rval(c.normal[j]);
+    }
+    o.friction = rval(c.friction);
+    o.pairIndex = c.pairIndex;
+    o.bodyA = c.bodyA;
+    o.bodyB = c.bodyB;
+    o.pad = c.pad;
+    return o;
+}
 int or_get_contacts(or_world* w, or_contact* out, int max) {
     const int n = std::min((int)w->contacts.size(), max);
-    if (out) memcpy(out, w->contacts.data(), sizeof(or_contact) * (size_t)n);
+    if (out)
+        for (int i = 0; i < n; ++i) out[i] = export_contact(w->contacts[i]);
     return (int)w->contacts.size();
 }
 void or_get_overflow(or_world* w, long long* pairOverflow, long long* cellOverflow) {
@@ -1058,16 +1137,30 @@ void or_get_overflow(or_world* w, long long* pairOverflow, long long* cellOverfl
     *cellOverflow = w->cellOverflow;
 }
 // Inject contacts (e.g. from the device) before or_stage_solve.
-void or_set_contacts(or_world* w, const or_contact* c, int n) { w->contacts.assign(c, c + n); }
+void or_set_contacts(or_world* w, const or_contact* c, int n) {
+    w->contacts.assign((size_t)n, or_contact_r());
+    for (int i = 0; i < n; ++i) {
+        or_contact_r& r = w->contacts[i];
+        for (int j = 0; j < 4; ++j) {
+            for (int k = 0; k < 4; ++k) r.pos[j][k] = c[i].pos[j][k];
+            r.normal[j] = c[i].normal[j];
+        }
+        r.friction = c[i].friction;
+        r.pairIndex = c[i].pairIndex;
+        r.bodyA = c[i].bodyA;
+        r.bodyB = c[i].bodyB;
+        r.pad = c[i].pad;
+    }
+}
 // Inject pairs before or_stage_narrowphase.
 void or_set_pairs(or_world* w, const int* pairs2, int n) { w->pairs.assign(pairs2, pairs2 + 2 * (size_t)n); }
 
 // Single-pair narrowphase for known-answer tests: returns nPoints (0 = none).
 int or_pair_contact(or_world* w, int A, int B, or_contact* out) {
-    or_contact c;
+    or_contact_r c;
     if (!contact_for_pair(w, 0, A, B, c)) return 0;
-    *out = c;
-    return (int)c.normal[3];
+    *out = export_contact(c);
+    return (int)rval(c.normal[3]);
 }
 
 // Clipping + reduction entry for the pin against the reference host port:
@@ -1101,7 +1194,8 @@ int or_clip_reduce(or_world* w, int polyA, int faceA, const double* posA, const 
         if (depth <= maxDist) pts.push_back({p.x, p.y, p.z, depth});
     }
     for (size_t i = 0; i < pts.size(); ++i) {
-        out4[4 * i] = pts[i].x; out4[4 * i + 1] = pts[i].y; out4[4 * i + 2] = pts[i].z; out4[4 * i + 3] = pts[i].w;
+        out4[4 * i] = rval(pts[i].x); out4[4 * i + 1] = rval(pts[i].y);
+        out4[4 * i + 2] = rval(pts[i].z); out4[4 * i + 3] = rval(pts[i].w);
     }
     reduce_manifold(pts, V(nearNormal[0], nearNormal[1], nearNormal[2]), idx4);
     return (int)pts.size();
@@ -1134,7 +1228,8 @@ int or_clip_face_world(const double* vertsA4, int nA, const double* normalA, con
         Real depth = n.x * p.x + n.y * p.y + n.z * p.z + eqA;
         if (depth <= minDist) depth = minDist;
         if (depth <= maxDist) {
-            out4[4 * k] = p.x; out4[4 * k + 1] = p.y; out4[4 * k + 2] = p.z; out4[4 * k + 3] = depth;
+            out4[4 * k] = rval(p.x); out4[4 * k + 1] = rval(p.y); out4[4 * k + 2] = rval(p.z);
+            out4[4 * k + 3] = rval(depth);
             ++k;
         }
     }
@@ -1155,8 +1250,8 @@ void or_solve_velocities(or_world* w, double* lin4, double* ang4) {
             }
     }
     for (size_t i = 0; i < 4 * (size_t)w->n; ++i) {
-        lin4[i] = w->lin[i];
-        ang4[i] = w->ang[i];
+        lin4[i] = rval(w->lin[i]);
+        ang4[i] = rval(w->ang[i]);
     }
 }
 

@@ -16,6 +16,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
 LIB_F32 = os.path.join(HERE, "liboracle_f32.so")
+LIB_DUAL = os.path.join(HERE, "liboracle_dual.so")
 REF_LIB = os.path.join(HERE, "_ref", "libb3ref.so")
 BULLET_LIB = os.path.join(HERE, "_ref", "libb3bullet.so")
 REFERENCE = "/root/reference"
@@ -41,8 +42,9 @@ def _stale(out, srcs):
 
 def build_oracle(force=False):
     src = os.path.join(HERE, "b3_oracle.cpp")
-    for out, extra in ((LIB, []), (LIB_F32, ["-DORACLE_REAL=float"])):
-        if force or _stale(out, [src]):
+    dual = os.path.join(HERE, "b3_dual.h")
+    for out, extra in ((LIB, []), (LIB_F32, ["-DORACLE_REAL=float"]), (LIB_DUAL, ["-DORACLE_DUAL"])):
+        if force or _stale(out, [src, dual]):
             cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off", "-fno-fast-math"] + \
                 extra + [src, "-o", out]
             r = subprocess.run(cmd, capture_output=True, text=True)

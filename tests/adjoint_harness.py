@@ -9,12 +9,12 @@ import oracle
 from experiments_b200 import b3, scenes
 
 
-def make_oracle(host_ctx, scene):
+def make_oracle(host_ctx, scene, dual=False):
     """Oracle world of a scene plus the per-body inverse inertia diagonal of
-    the registration (FP64 copy)."""
+    the registration (FP64 copy); dual=True: the tangent-linear build."""
     w = b3.PhysicsWorld(host_ctx, scenes.world_config(scene))
     scenes.register_scene(w, scene)
-    o = oracle.oracle_from_world(w, scene)
+    o = oracle.oracle_from_world(w, scene, dual=dual)
     ii = w.inertias()[:, :3].astype(np.float64)
     w.close()
     return o, ii
@@ -67,6 +67,58 @@ def oracle_run(host_ctx, scene, state, steps, seeds, kind=None, delta=None, eps=
     h = o.active_hash()
     o.close()
     return world_functional(scene, st, seeds), h
+
+
+def oracle_tangent(host_ctx, scene, state, steps, seeds, kind, delta):
+    """Directional derivative of the per-world functional along delta (one
+    parameter set: "lin" / "ang" n x 3, "mass" / "friction" n), from the
+    FP64 tangent-linear oracle: exact derivatives of the FP64 step with its
+    discrete choices held at the value path's. Returns the per-world
+    derivatives and the per-world active-set signatures."""
+    o, ii = make_oracle(host_ctx, scene, dual=True)
+    o.set_state_f64(*[a.copy() for a in state])
+    m = np.asarray(scene.mass, np.float64)
+    dyn = m > 0
+    im = np.where(dyn, 1.0 / np.where(dyn, m, 1), 0.0)
+    delta = np.asarray(delta, np.float64)
+    if kind == "lin":
+        o.set_tangent(lin=delta)
+    elif kind == "ang":
+        o.set_tangent(ang=delta)
+    elif kind == "mass":
+        # invMass = 1/m and the inverse inertia is invMass times a shape factor
+        dim = np.where(dyn, -delta / np.where(dyn, m, 1) ** 2, 0.0)
+        o.set_tangent(inv_mass=dim, inv_inertia3=ii * np.where(dyn, dim / np.where(dyn, im, 1), 0.0)[:, None])
+    elif kind == "friction":
+        o.set_tangent(friction=delta)
+    o.reset_active()
+    o.step(steps)
+    d = o.tangent()
+    h = o.active_hash()
+    o.close()
+    return world_functional(scene, d, seeds), h
+
+
+def tangent_vectors(host_ctx, scene, state, steps, seeds, kind, per):
+    """Whole FP64 gradient vectors of the per-world functional with respect
+    to one parameter set, one tangent-linear run per body slot and
+    component (worlds are independent, so a run seeds the same slot in
+    every world). Returns (n x comps gradient, per-world signatures)."""
+    dyn = np.asarray(scene.mass) > 0
+    wid = np.asarray(scene.world)
+    comps = 3 if kind in ("lin", "ang") else 1
+    g = np.zeros((scene.n, comps))
+    slots = np.where(dyn)[0].reshape(scene.num_worlds, per)
+    h0 = None
+    for j in range(per):
+        bodies = slots[:, j]
+        for c in range(comps):
+            d = np.zeros((scene.n, comps))
+            d[bodies, c] = 1.0
+            t, h = oracle_tangent(host_ctx, scene, state, steps, seeds, kind, d if comps == 3 else d[:, 0])
+            g[bodies, c] = t[wid[bodies]]
+            h0 = h if h0 is None else h0
+    return g, h0
 
 
 def gpu_adjoint(ctx, scene, state, steps, seeds, checkpoint_every=16):
