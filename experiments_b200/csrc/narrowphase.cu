@@ -290,6 +290,7 @@ __device__ __noinline__ bool axis_ff(const PairCtx& c, const b3::ShapesDev& S, c
 // face axis separates or no axis exists.
 // FP32 part: 0 = separated (or no axis), 1 = decided in FP32 (sepf),
 // 2 = near-minimum candidates left in W.cand[0..count) for float-float.
+template <bool kEarlyFaces>
 __device__ __forceinline__ int sweep_axes(PairCtx& c, const b3::ShapesDev& S, int* cand, float3& sepf,
                                           int& count, int* ovfCounter) {
     const int lane = threadIdx.x & 31;
@@ -307,6 +308,64 @@ __device__ __forceinline__ int sweep_axes(PairCtx& c, const b3::ShapesDev& S, in
     // largest projected coordinate); edge axes add a term inversely
     // proportional to |e0 x e1| (their normalisation amplifies rounding)
     const float delta = 1e-6f * scale;
+    // kEarlyFaces, hulls with more than two lane-rounds of faces: first
+    // test the face of A and the face of B best aligned with D (the
+    // likeliest separating axes), with the warp splitting the vertices. A
+    // separating face axis rejects the pair whichever face it is, and each
+    // test computes the same FP32 depth as the full pass below, so an early
+    // rejection here is the full pass' own verdict. (A template switch: the
+    // launch picks it only for shape sets with such hulls, as its code
+    // costs the cube-only sweeps a few per cent.)
+    if (kEarlyFaces && nFace > 64) {
+        const int FA = pa.numFaces;
+        float bA = -1.f, bB = -1.f;
+        int iA = kNone, iB = kNone;
+        for (int f = lane; f < nFace; f += 32) {
+            const bool onA = f < FA;
+            const float4 pl = __ldg((const float4*)&S.faces[onA ? pa.faceOffset + f : pb.faceOffset + f - FA].plane[0]);
+            const float a = fabsf(dot(D, mul(onA ? c.RA : c.RB, make_float3(pl.x, pl.y, pl.z))));
+            if (onA) {
+                if (a > bA) { bA = a; iA = f; }
+            } else if (a > bB) {
+                bB = a;
+                iB = f;
+            }
+        }
+        bA = -bA;
+        bB = -bB;
+        warp_argmin(bA, iA);
+        warp_argmin(bB, iB);
+        for (int t = 0; t < 2; ++t) {
+            const int f = t == 0 ? iA : iB;
+            if (f == kNone) continue;
+            const bool onA = f < FA;
+            const float4 pl = __ldg((const float4*)&S.faces[onA ? pa.faceOffset + f : pb.faceOffset + f - FA].plane[0]);
+            float3 n = mul(onA ? c.RA : c.RB, make_float3(pl.x, pl.y, pl.z));
+            if (dot(D, n) < 0.f) n = -n;
+            float mn[2], mx[2];
+            for (int h = 0; h < 2; ++h) {
+                const b3ConvexPolyhedron& p = h == 0 ? pa : pb;
+                const float3 ld = mul_t(h == 0 ? c.RA : c.RB, n);
+                float lo = FLT_MAX, hi = -FLT_MAX;
+                for (int i = lane; i < p.numVertices; i += 32) {
+                    const float4 v = __ldg(&S.verts[p.vertexOffset + i]);
+                    const float dp = v.x * ld.x + v.y * ld.y + v.z * ld.z;
+                    lo = fminf(lo, dp);
+                    hi = fmaxf(hi, dp);
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+                    hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+                }
+                mn[h] = lo;
+                mx[h] = hi;
+            }
+            const float off = dot(rel, n);
+            const float d = fminf(mx[0] - (mn[1] + off), (mx[1] + off) - mn[0]);
+            if (d < -delta) return 0;
+        }
+    }
     float kd[kKeep];
     int ki[kKeep];
 #pragma unroll
@@ -550,7 +609,7 @@ __device__ __noinline__ bool refine_axes(PairCtx& c, const b3::ShapesDev& S, War
 __device__ __noinline__ bool find_axis(PairCtx& c, const b3::ShapesDev& S, WarpScratch& W, ff3& sep, int* ovfCounter) {
     float3 sepf;
     int count = 0;
-    const int r = sweep_axes(c, S, W.cand, sepf, count, ovfCounter);
+    const int r = sweep_axes<false>(c, S, W.cand, sepf, count, ovfCounter);
     if (r == 0) return false;
     if (r == 1) {
         sep = mk3(sepf.x, sepf.y, sepf.z);
@@ -1251,6 +1310,7 @@ __device__ __forceinline__ int push(int* queue, int32_t* count, int p) {
 // finished here; pairs whose axis the sweep decides go to the FP32 clip
 // queue with that axis; pairs with near-minimum candidates go to the
 // float-float queue.
+template <bool kEarlyFaces>
 __global__ void __launch_bounds__(128, 5)
 k_np_sweep(const int2* __restrict__ pairs, const int32_t* __restrict__ numPairsDev, b3::BodiesDev Bd,
            b3::ShapesDev S, uint32_t* __restrict__ manifoldFlag, float4* __restrict__ pairSep,
@@ -1273,7 +1333,8 @@ k_np_sweep(const int2* __restrict__ pairs, const int32_t* __restrict__ numPairsD
             PairCtx c;
             int r = 0, count = 0;
             float3 sepf = make_float3(0.f, 0.f, 0.f);
-            if (pair_from_pre(c, pre[i], S)) r = sweep_axes(c, S, wcand, sepf, count, &counters->clipOverflow);
+            if (pair_from_pre(c, pre[i], S))
+                r = sweep_axes<kEarlyFaces>(c, S, wcand, sepf, count, &counters->clipOverflow);
             if (r == 0) {
                 if (lane == 0) manifoldFlag[p] = 0u;
             } else if (r == 1) {
@@ -1469,10 +1530,16 @@ int launch_narrowphase(b3World_t* w, cudaStream_t st) {
     const b3::ShapesDev S = w->shapesDev();
     int32_t* sc = w->d.scalars;
     const size_t smemSweep = (size_t)kSweepWarpSmem * w->npWarpsPerBlock;
+    // the early face test only where some pair can have more than 64 faces
+    // (a hull may pair with another instance of itself)
+    int maxFaces = 0;
+    for (const b3ConvexPolyhedron& h : w->polys) maxFaces = std::max(maxFaces, h.numFaces);
+    const bool early = 2 * maxFaces > 64;
+    auto sweep = early ? k_np_sweep<true> : k_np_sweep<false>;
     int occS = 1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occS, k_np_sweep, threads, smemSweep) != cudaSuccess || occS < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occS, sweep, threads, smemSweep) != cudaSuccess || occS < 1)
         occS = 1;
-    k_np_sweep<<<w->ctx->numSMs * occS, threads, smemSweep, st>>>(
+    sweep<<<w->ctx->numSMs * occS, threads, smemSweep, st>>>(
         w->d.pairs, sc + S_NUM_PAIRS, Bd, S, w->d.manifoldFlag, w->d.pairSep, w->d.npFast, w->d.npSlow,
         w->d.npCand, std::min(w->cfg.maxPairs, kNpCandSlots), sc, w->d.counters);
     B3_CHECK_LAUNCH();
