@@ -243,7 +243,7 @@ def run_b3(args, world_size, local_rank):
     # per-stage CUDA-event breakdown on an identical world advanced to the
     # same step (eager launches; timing only, not part of `value`)
     w2 = scenes.build_world(ctx, sc, useGraph=0)
-    w2.set_tuning(tuning[:5])
+    w2.set_tuning(tuning)
     w2.stepSimulation(args.warmup + args.steps - 3)
     w2.set_stage_timing(True)
     acc = np.zeros(len(STAGES))
@@ -559,6 +559,7 @@ def main():
                 "tuning": {"np_warps_per_cta": res["tuning"][0], "pair_cta": res["tuning"][1],
                            "jacobi_cta": res["tuning"][2], "jacobi_blocks_per_sm": res["tuning"][4],
                            "autotune_trials": res["tuning"][5], "jacobi_per_world_blocks": res["tuning"][6],
+                           "jacobi_gather4": res["tuning"][7],
                            "kernels_per_step": int(res["kernels"])},
                 "parallelism": (f"worlds sharded x{world_size}" if res["sharded"] else f"replicas x{world_size}")
                 if world_size > 1 else "single GPU",

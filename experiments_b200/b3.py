@@ -478,7 +478,8 @@ class PhysicsWorld:
 
     def tuning(self):
         """(narrowphase warps/CTA, pair CTA size, solver CTA size, kernels per
-        captured step, Jacobi blocks per SM cap, configurations timed)."""
+        captured step, Jacobi blocks per SM cap, configurations timed,
+        Jacobi mode, Jacobi gather)."""
         v = (C.c_int * 8)()
         cnt = C.c_int()
         _check(self.lib.b3_get_tuning(self.h, v, 8, C.byref(cnt)), "b3_get_tuning")

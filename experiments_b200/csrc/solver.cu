@@ -210,7 +210,7 @@ __global__ void k_setup_rows(b3::BodiesDev Bd, SolverView V, const int* __restri
 // the previous phase (zero in the first phase), solve the manifold's normal
 // or friction rows in order, store both copies in buffer outBuf. A copy of a
 // manifold without rows keeps the average, as in the reference.
-template <bool TAPE>
+template <bool TAPE, bool GATHER4>
 __device__ __forceinline__ void solve_manifold(const SolverView& V, int m, bool friction, bool first, int inBuf,
                                                int outBuf, const b3::JacobiTape& T, int phase) {
     {
@@ -220,8 +220,24 @@ __device__ __forceinline__ void solve_manifold(const SolverView& V, int m, bool 
         const int dyn = __float_as_int(h0.w);
         float3 dvA = make_float3(0.f, 0.f, 0.f), dwA = dvA, dvB = dvA, dwB = dvA;
         if (!first) {
-            if (dyn & 1) body_average(V, A, inBuf, dvA, dwA);
-            if (dyn & 2) body_average(V, B, inBuf, dvB, dwB);
+            if (GATHER4) {
+                // both bodies' incidence ranges in one round of loads, then
+                // their copies four at a time (same sums as body_average)
+                uint32_t sA = 0, eA = 0, sB = 0, eB = 0;
+                if (dyn & 1) {
+                    sA = V.incStart[A];
+                    eA = V.incEnd[A];
+                }
+                if (dyn & 2) {
+                    sB = V.incStart[B];
+                    eB = V.incEnd[B];
+                }
+                if (dyn & 1) body_average_range(V, sA, eA, inBuf, dvA, dwA);
+                if (dyn & 2) body_average_range(V, sB, eB, inBuf, dvB, dwB);
+            } else {
+                if (dyn & 1) body_average(V, A, inBuf, dvA, dwA);
+                if (dyn & 2) body_average(V, B, inBuf, dvB, dwB);
+            }
         }
         float lam[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         if (nRows > 0) {
@@ -288,18 +304,22 @@ __device__ __forceinline__ void solve_manifold(const SolverView& V, int m, bool 
     }
 }
 
-template <bool TAPE>
+template <bool TAPE, bool GATHER4>
 __device__ void manifold_phase(const SolverView& V, int M, bool friction, bool first, int inBuf, int outBuf,
                                const b3::JacobiTape& T, int phase) {
     for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x)
-        solve_manifold<TAPE>(V, m, friction, first, inBuf, outBuf, T, phase);
+        solve_manifold<TAPE, GATHER4>(V, m, friction, first, inBuf, outBuf, T, phase);
 }
 
 // Phases p = 0 .. 2*iterations-1 alternate normal (even) and friction (odd)
 // rows; the averaging of the reference happens at the start of the next
 // phase from the double-buffered copies, so phases are separated by one
 // bounded grid barrier each.
-template <bool TAPE>
+//
+// GATHER4 (a tuning choice): each copy's body averages are gathered with
+// their loads issued four at a time. Shorter dependent-load chains per
+// phase, more registers per thread: the autotuner weighs the two.
+template <bool TAPE, bool GATHER4>
 __global__ void __launch_bounds__(256)
 k_jacobi(SolverView V, int iterations, uint32_t* bar, int32_t* err, b3Counters* counters, b3::JacobiTape T) {
     const int M = *V.numManifolds;
@@ -307,7 +327,7 @@ k_jacobi(SolverView V, int iterations, uint32_t* bar, int32_t* err, b3Counters* 
     const int phases = 2 * iterations;
     for (int p = 0; p < phases; ++p) {
         if (p > 0 && !grid_barrier(bar, bar + 1, nb, err, counters)) return;
-        manifold_phase<TAPE>(V, M, (p & 1) != 0, p == 0, (p - 1) & 1, p & 1, T, p);
+        manifold_phase<TAPE, GATHER4>(V, M, (p & 1) != 0, p == 0, (p - 1) & 1, p & 1, T, p);
     }
 }
 
@@ -330,7 +350,7 @@ __global__ void k_world_ranges(SolverView V, const int* __restrict__ worldId, in
     }
 }
 
-template <bool TAPE>
+template <bool TAPE, bool GATHER4>
 __global__ void __launch_bounds__(256)
 k_jacobi_worlds(SolverView V, int iterations, const int* __restrict__ start, const int* __restrict__ end,
                 int numWorlds, const int* __restrict__ worldId, b3::JacobiTape T) {
@@ -342,7 +362,7 @@ k_jacobi_worlds(SolverView V, int iterations, const int* __restrict__ start, con
             if (p > 0) __syncthreads();
             for (int m = s + (int)threadIdx.x; m < e; m += blockDim.x)
                 if (worldId[__float_as_int(R(V, 0, m).x)] == w)
-                    solve_manifold<TAPE>(V, m, (p & 1) != 0, p == 0, (p - 1) & 1, p & 1, T, p);
+                    solve_manifold<TAPE, GATHER4>(V, m, (p & 1) != 0, p == 0, (p - 1) & 1, p & 1, T, p);
         }
         __syncthreads();
     }
@@ -479,7 +499,10 @@ int launch_solver_taped(b3World_t* w, cudaStream_t st, const JacobiTape* tape) {
         k_world_ranges<<<w->ctx->numSMs * 4, 256, 0, st>>>(V, w->d.worldId, w->d.worldMStart, w->d.worldMEnd);
         B3_CHECK_LAUNCH();
         const int threads = w->solverThreads;
-        const void* kw = tape ? (const void*)k_jacobi_worlds<true> : (const void*)k_jacobi_worlds<false>;
+        // the taped forward keeps the plain gather (same results either way)
+        const void* kw = tape ? (const void*)k_jacobi_worlds<true, false>
+                              : (w->solverGather ? (const void*)k_jacobi_worlds<false, true>
+                                                 : (const void*)k_jacobi_worlds<false, false>);
         int occ = 1;
         B3_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kw, threads, 0));
         occ = occ < 1 ? 1 : occ;
@@ -498,7 +521,8 @@ int launch_solver_taped(b3World_t* w, cudaStream_t st, const JacobiTape* tape) {
     B3_CUDA(cudaMemsetAsync(w->d.scalars + S_BAR_COUNT, 0, sizeof(int32_t) * 2, st));
     const int threads = w->solverThreads;
     int occ = 1;
-    const void* kern = tape ? (const void*)k_jacobi<true> : (const void*)k_jacobi<false>;
+    const void* kern = tape ? (const void*)k_jacobi<true, false>
+                            : (w->solverGather ? (const void*)k_jacobi<false, true> : (const void*)k_jacobi<false, false>);
     B3_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, 0));
     occ = occ < 1 ? 1 : occ;
     occ = occ > w->solverOccCap ? w->solverOccCap : occ;

@@ -133,6 +133,38 @@ __device__ __forceinline__ void body_average(const SolverView& V, int b, int buf
     ang = sa * factor;
 }
 
+// One body's average given its incidence range, with the loads issued four
+// copies at a time (copy ids, then the copies): the same copies, order and
+// operations as body_average, hence the same result.
+__device__ __forceinline__ void body_average_range(const SolverView& V, uint32_t s, uint32_t e, int buf, float3& lin,
+                                                   float3& ang) {
+    float3 sl = make_float3(0.f, 0.f, 0.f), sa = sl;
+    for (uint32_t i0 = s; i0 < e; i0 += 4) {
+        uint32_t cid[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) cid[u] = i0 + u < e ? V.incVals[i0 + u] : 0u;
+        float4 cl[4], ca[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (i0 + u < e) {
+                const size_t at = (size_t)(buf * 2 + (int)(cid[u] & 1u)) * V.cap + (cid[u] >> 1);
+                cl[u] = V.copyLin[at];
+                ca[u] = V.copyAng[at];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (i0 + u < e) {
+                sl += f3(cl[u]);
+                sa += f3(ca[u]);
+            }
+        }
+    }
+    const float factor = 1.f / (float)(e - s);
+    lin = sl * factor;
+    ang = sa * factor;
+}
+
 SolverView solver_view(b3World_t* w);
 
 }  // namespace b3solver

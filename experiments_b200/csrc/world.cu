@@ -1038,8 +1038,9 @@ extern "C" int b3_autotune(b3World w, int trialSteps, void* stream) {
         int cand[3];
     };
     Knob knobs[] = {{&w->npWarpsPerBlock, {1, 2, 4}}, {&w->solverThreads, {64, 128, 256}},
-                    {&w->solverOccCap, {1, 2, 4}}, {&w->solverMode, {0, 1, 0}}};
-    const int numKnobs = w->cfg.numWorlds > 1 ? 4 : 3;  // per-world solver only for batched worlds
+                    {&w->solverOccCap, {1, 2, 4}},      {&w->solverGather, {0, 1, 0}},
+                    {&w->solverMode, {0, 1, 0}}};
+    const int numKnobs = w->cfg.numWorlds > 1 ? 5 : 4;  // per-world solver only for batched worlds
     do {
         for (int k = 0; k < 4 && rc == B3_OK; ++k)
             if (cudaMemcpyAsync(save + k * N, bufs[k], N * sizeof(float4), cudaMemcpyDeviceToDevice, st) !=
@@ -1082,23 +1083,25 @@ extern "C" int b3_set_tuning(b3World w, const int* values, int count) {
     if (!w || !values || count < 3) return B3_ERR_INVALID_ARG;
     const int np = values[0], st = values[2], cap = count >= 5 ? values[4] : w->solverOccCap;
     const int mode = count >= 7 ? values[6] : w->solverMode;
+    const int gather = count >= 8 ? values[7] : w->solverGather;
     if ((np != 1 && np != 2 && np != 4) || (st != 64 && st != 128 && st != 256) || cap < 1 || cap > 8 ||
-        (mode != 0 && mode != 1))
+        (mode != 0 && mode != 1) || (gather != 0 && gather != 1))
         return B3_ERR_INVALID_ARG;
     w->npWarpsPerBlock = np;
     w->solverThreads = st;
     w->solverOccCap = cap;
     w->solverMode = mode;
+    w->solverGather = gather;
     w->graphValid = false;
     return B3_OK;
 }
 
 extern "C" int b3_get_tuning(b3World w, int* values, int max, int* count) {
     if (!w || !count) return B3_ERR_INVALID_ARG;
-    int v[7] = {w->npWarpsPerBlock, w->pairThreads, w->solverThreads, w->kernelsPerStep, w->solverOccCap,
-                w->tunedTrials, w->solverMode};
-    *count = 7;
-    for (int i = 0; i < std::min(7, max); ++i) values[i] = v[i];
+    int v[8] = {w->npWarpsPerBlock, w->pairThreads, w->solverThreads, w->kernelsPerStep, w->solverOccCap,
+                w->tunedTrials, w->solverMode, w->solverGather};
+    *count = 8;
+    for (int i = 0; i < std::min(8, max); ++i) values[i] = v[i];
     return B3_OK;
 }
 

@@ -357,8 +357,9 @@ int b3_batch_world_stats(b3World w, float* out4, int numWorlds, void* stream);
 int b3_batch_world_offsets(b3World w, int* offsets, int maxWorlds, int* numWorlds);
 /* Autotuner: coordinate descent over the launch shapes of the tunable
  * kernels on the current scene (narrowphase warps per CTA 1/2/4, Jacobi
- * CTA size 64/128/256, Jacobi persistent blocks per SM 1/2/4, and for
- * batched worlds the Jacobi mode grid-barrier / block-per-world); each trial
+ * CTA size 64/128/256, Jacobi persistent blocks per SM 1/2/4, Jacobi
+ * body-average gather one-at-a-time / four-wide, and for batched worlds
+ * the Jacobi mode grid-barrier / block-per-world); each trial
  * runs trialSteps eager steps from the same saved state, timed with CUDA
  * events; the fastest value of each knob is kept, the body state and
  * counters are restored, and the step graph is recaptured on the next
@@ -368,13 +369,15 @@ int b3_autotune(b3World w, int trialSteps, void* stream);
  * kernel launches per step of the captured step graph (0 before capture),
  * Jacobi blocks per SM cap, configurations timed by the autotuner, Jacobi
  * mode (0 = persistent grid with grid barriers, 1 = one block per world
- * with block barriers; batched worlds only, bit-identical results). */
+ * with block barriers; batched worlds only, bit-identical results), Jacobi
+ * body-average gather (0 = one copy at a time, 1 = four loads in flight;
+ * bit-identical results). */
 int b3_get_tuning(b3World w, int* values, int max, int* count);
 /* Set the tunables in b3_get_tuning's order (count >= 3; the pair-search
- * CTA size, the launch count and the trial count are read-only, indices 4
- * and 6 are optional):
+ * CTA size, the launch count and the trial count are read-only, indices 4,
+ * 6 and 7 are optional):
  * narrowphase warps per CTA 1/2/4, Jacobi CTA size 64/128/256, Jacobi
- * blocks per SM cap 1..8. */
+ * blocks per SM cap 1..8, Jacobi mode 0/1, Jacobi gather 0/1. */
 int b3_set_tuning(b3World w, const int* values, int count);
 
 /* ------------------------------------------------------------------ */

@@ -167,9 +167,30 @@ def test_autotune_keeps_state_and_results(ctx):
     for x, y in zip(before, after):
         assert np.array_equal(x, y)
     t = a.tuning()
-    assert t[5] == 12 and t[0] in (1, 2, 4) and t[6] in (0, 1) and t[2] in (64, 128, 256) and t[4] in (1, 2, 4)
+    assert t[5] == 15 and t[0] in (1, 2, 4) and t[6] in (0, 1) and t[2] in (64, 128, 256) and t[4] in (1, 2, 4)
+    assert t[7] in (0, 1)
     a.stepSimulation(10)
     b.stepSimulation(10)
+    for x, y in zip(a.read_state(), b.read_state()):
+        assert np.array_equal(x, y)
+    a.close()
+    b.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", [0, 1])
+def test_gathered_averages_match_one_at_a_time(ctx, mode):
+    """The Jacobi variant that gathers each body's copies four loads at a
+    time gives the one-at-a-time results bit for bit, in both solver
+    modes."""
+    sc = scenes.random_pile(47, n=48, worlds=6, hull_frac=0.5)
+    a = scenes.build_world(ctx, sc, useGraph=1)
+    b = scenes.build_world(ctx, sc, useGraph=1)
+    t = a.tuning()
+    a.set_tuning([t[0], t[1], t[2], t[3], t[4], t[5], mode, 0])
+    b.set_tuning([t[0], t[1], t[2], t[3], t[4], t[5], mode, 1])
+    a.stepSimulation(30)
+    b.stepSimulation(30)
     for x, y in zip(a.read_state(), b.read_state()):
         assert np.array_equal(x, y)
     a.close()
