@@ -216,7 +216,8 @@ def run_b3(args, world_size, local_rank):
         from experiments_b200 import sharding
         sc, _ = sharding.shard_scene(full, int(os.environ.get("RANK", "0")), world_size)
         sharded = True
-    w = scenes.build_world(ctx, sc, useGraph=1)
+    bp = {"flags": 1} if getattr(args, "sap", False) else {}  # sweep-and-prune broadphase
+    w = scenes.build_world(ctx, sc, useGraph=1, **bp)
     st = torch.cuda.current_stream()
     flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > 126 MB L2
     # launch shapes chosen by the autotuner on this scene (state restored)
@@ -242,7 +243,7 @@ def run_b3(args, world_size, local_rank):
     kernels = w.tuning()[3]
     # per-stage CUDA-event breakdown on an identical world advanced to the
     # same step (eager launches; timing only, not part of `value`)
-    w2 = scenes.build_world(ctx, sc, useGraph=0)
+    w2 = scenes.build_world(ctx, sc, useGraph=0, **bp)
     w2.set_tuning(tuning)
     w2.stepSimulation(args.warmup + args.steps - 3)
     w2.set_stage_timing(True)
@@ -488,12 +489,18 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true")
     ap.add_argument("--scale", action="store_true", help="also run the 1,048,576-body plain and adjoint steps")
+    ap.add_argument("--sap", action="store_true",
+                    help="sweep-and-prune broadphase (pipeline2's default) in place of the grid; single-world workloads")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world_size = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     args.warmup = max(3, args.warmup)
     cfg = {"workload": WORKLOADS[args.workload]}
+    if args.sap:
+        if args.workload in ("c3", "c3s"):
+            ap.error("--sap takes a single-world workload (c1, c2, c2s, c5)")
+        cfg["workload"] += ", sweep-and-prune broadphase"
 
     if args.impl == "reference":
         if rank != 0:

@@ -22,6 +22,7 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "libb3gpu.so")
+B3_WORLD_SAP_BROADPHASE = 1  # b3WorldConfig.flags: sweep-and-prune broadphase
 
 B3_OK = 0
 STATUS = {0: "OK", 1: "INVALID_ARG", 2: "CUDA", 3: "CAPACITY", 4: "NO_DEVICE", 5: "STATE",
@@ -136,6 +137,8 @@ SIGNATURES = [
     ("b3_stage_solve", _I, [_P, _P]),
     ("b3_stage_integrate", _I, [_P, _P]),
     ("b3_grid_broadphase_calculate_overlapping_pairs", _I, [_P, _P]),
+    ("b3_sap_broadphase_calculate_overlapping_pairs", _I, [_P, _P]),
+    ("b3_sap_compute_pairs", _I, [_P, _P, _I, _I, _P, _I, _P, _P]),
     ("b3_grid_broadphase_get_pair_count", _I, [_P, _IP, _P]),
     ("b3_narrowphase_compute_contacts", _I, [_P, _P, _I, _P]),
     ("b3_solver_solve_jacobi", _I, [_P, _P]),
@@ -285,6 +288,21 @@ class RadixSort32:
         else:
             _check(self.ctx.lib.b3_radix_sort32_kv(self.ctx.h, _dptr(keys), _dptr(values), n, key_bits,
                                                    _stream(stream)), "b3_radix_sort32_kv")
+
+
+class SapPairs:
+    """computePairsKernel (BB/sapFast.cl:48-150) on caller-sorted device
+    AABBs in btAabbCL layout (n x 8 float32: min xyz, id bits, max xyz, w)."""
+
+    def __init__(self, ctx):
+        self.ctx = ctx
+
+    def execute(self, sorted_aabbs, pairs, count, n=None, axis=0, max_pairs=None, stream=None):
+        n = sorted_aabbs.shape[0] if n is None else n
+        max_pairs = pairs.shape[0] if max_pairs is None else max_pairs
+        _check(self.ctx.lib.b3_sap_compute_pairs(self.ctx.h, _dptr(sorted_aabbs), n, axis, _dptr(pairs),
+                                                 max_pairs, _dptr(count), _stream(stream)),
+               "b3_sap_compute_pairs")
 
 
 class BoundSearch:
@@ -510,6 +528,12 @@ class PhysicsWorld:
         out = np.zeros(nw.value + 1, np.int32)
         _check(self.lib.b3_batch_world_offsets(self.h, iptr(out), len(out), C.byref(nw)), "b3_batch_world_offsets")
         return out
+
+    def sap_calculate_overlapping_pairs(self, stream=None):
+        """btGpuSapBroadphase::calculateOverlappingPairs on a world created
+        with flags=B3_WORLD_SAP_BROADPHASE (from the current AABBs)."""
+        _check(self.lib.b3_sap_broadphase_calculate_overlapping_pairs(self.h, _stream(stream)),
+               "b3_sap_broadphase_calculate_overlapping_pairs")
 
     def compute_contacts(self, d_pairs=None, num_pairs=0, stream=None):
         """Narrowphase on caller device pairs (int2) or, with None, on the

@@ -70,6 +70,12 @@ struct DevBuffers {
     int* smallSlot = nullptr;      // body -> slot in the hash arrays, -1 = large
     int* largeStart = nullptr;     // per world CSR over largeList
     int* largeList = nullptr;
+    // sweep-and-prune broadphase (B3_WORLD_SAP_BROADPHASE)
+    int* sapSmall = nullptr;          // dynamic bodies (small proxies), body order
+    int* sapLarge = nullptr;          // static bodies (large proxies), body order
+    float4* sapSorted = nullptr;      // small AABBs sorted by min x: (min, max) per proxy
+    uint32_t* sapCount = nullptr;     // pairs per sorted proxy, then their offsets
+    uint32_t* sapOffset = nullptr;
     uint32_t *keys = nullptr, *vals = nullptr, *keysAlt = nullptr, *valsAlt = nullptr;
     uint2* cellTable = nullptr;    // (stamp, first sorted index) per (world, cell)
     int2* pairs = nullptr;
@@ -142,6 +148,8 @@ struct b3World_t {
     std::vector<float> regAabb;   // registration AABB per body (6 floats)
     std::vector<int> smallSlotHost, largeStartHost, largeListHost;
     int numSmall = 0;
+    bool sap = false;    // sweep-and-prune broadphase in place of the grid
+    std::vector<int> sapSmallHost, sapLargeHost;
     int capBodies = 0;   // allocated body capacity on device
     int capInc = 0;
     bool written = false;
@@ -194,6 +202,9 @@ struct JacobiTape {
 int launch_aabb_hash(b3World_t* w, cudaStream_t st);
 int launch_sort_and_cells(b3World_t* w, cudaStream_t st);
 int launch_find_pairs(b3World_t* w, cudaStream_t st);
+// sweep-and-prune counterparts (sap.cu), called by the two above in SAP mode
+int launch_sap_sort(b3World_t* w, cudaStream_t st);
+int launch_sap_pairs(b3World_t* w, cudaStream_t st);
 int launch_narrowphase(b3World_t* w, cudaStream_t st);
 int launch_manifolds(b3World_t* w, cudaStream_t st);
 int launch_solver(b3World_t* w, cudaStream_t st);

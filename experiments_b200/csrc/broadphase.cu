@@ -318,6 +318,7 @@ int launch_aabb_hash(b3World_t* w, cudaStream_t st) {
 }
 
 int launch_sort_and_cells(b3World_t* w, cudaStream_t st) {
+    if (w->sap) return launch_sap_sort(w, st);
     const int ns = w->numSmall;
     if (ns == 0) return B3_OK;
     bool alt = false;
@@ -338,6 +339,7 @@ int launch_sort_and_cells(b3World_t* w, cudaStream_t st) {
 }
 
 int launch_find_pairs(b3World_t* w, cudaStream_t st) {
+    if (w->sap) return launch_sap_pairs(w, st);
     const int ns = w->numSmall;
     // numPairs = 0, tile counter = 0, status cleared
     B3_CUDA(cudaMemsetAsync(w->d.scalars + S_NUM_PAIRS, 0, sizeof(int32_t), st));

@@ -67,7 +67,7 @@ void free_all(b3::DevBuffers& d) {
     void* ptrs[] = {d.pos, d.quat, d.linVel, d.angVel, d.invMass, d.friction, d.restitution,
                     d.invInertia, d.collidable, d.worldId, d.cols, d.polys, d.verts, d.faces,
                     d.indices, d.edges, d.localAabb, d.polyInradius, d.aabbMin, d.aabbMax, d.smallSlot,
-                    d.largeStart, d.largeList, d.keys, d.vals, d.keysAlt, d.valsAlt, d.cellTable,
+                    d.largeStart, d.largeList, d.sapSmall, d.sapLarge, d.sapSorted, d.sapCount, d.sapOffset, d.keys, d.vals, d.keysAlt, d.valsAlt, d.cellTable,
                     d.pairs, d.contacts, d.manifoldFlag, d.pairSep, d.npFast, d.npSlow, d.npCand, d.manifoldScan,
                     d.manifoldPair,
                     d.incKeys, d.incVals, d.incKeysAlt, d.incValsAlt, d.bodyIncStart,
@@ -188,13 +188,18 @@ extern "C" int b3_world_create(b3Context ctx, const b3WorldConfig* cfg, b3World*
         b3_set_error("world id + cell hash need %d > 32 key bits", cellBits + worldBits);
         return B3_ERR_INVALID_ARG;
     }
+    if ((c.flags & ~B3_WORLD_SAP_BROADPHASE) != 0 || ((c.flags & B3_WORLD_SAP_BROADPHASE) && c.numWorlds != 1)) {
+        b3_set_error("invalid world flags (the SAP broadphase takes one world)");
+        return B3_ERR_INVALID_ARG;
+    }
     b3World w = new b3World_t();
     w->ctx = ctx;
     w->cfg = c;
+    w->sap = (c.flags & B3_WORLD_SAP_BROADPHASE) != 0;
     if (w->cfg.maxPairs <= 0) w->cfg.maxPairs = 8 * c.maxBodies;
     w->cellBits = cellBits;
     w->worldBits = worldBits;
-    w->keyBits = std::max(1, cellBits + worldBits);
+    w->keyBits = w->sap ? 32 : std::max(1, cellBits + worldBits);
     w->invCell = 1.f / c.cellSize;
     w->sim.gravity = make_float3(c.gravity[0], c.gravity[1], c.gravity[2]);
     w->sim.dt = c.dt;
@@ -401,6 +406,13 @@ static int ensure_capacity(b3World w) {
         B3_TRY(dalloc(d.aabbMin, nb));
         B3_TRY(dalloc(d.aabbMax, nb));
         B3_TRY(dalloc(d.smallSlot, nb));
+        if (w->sap) {
+            B3_TRY(dalloc(d.sapSmall, nb));
+            B3_TRY(dalloc(d.sapLarge, nb));
+            B3_TRY(dalloc(d.sapSorted, 2 * (size_t)nb));
+            B3_TRY(dalloc(d.sapCount, (size_t)nb + 1));
+            B3_TRY(dalloc(d.sapOffset, (size_t)nb + 1));
+        }
         B3_TRY(dalloc(d.keys, nb));
         B3_TRY(dalloc(d.vals, nb));
         B3_TRY(dalloc(d.keysAlt, nb));
@@ -432,7 +444,8 @@ static int ensure_capacity(b3World w) {
         B3_TRY(dalloc(d.incLin, 4 * c));  // [2 phase buffers][2 sides][capacity]
         B3_TRY(dalloc(d.incAng, 4 * c));
         const size_t tiles = (w->cfg.maxBodies + 127) / 128 + 16;
-        d.scanScratchBytes = std::max(b3::scan_scratch_bytes(cap), tiles * 8 + 256);
+        d.scanScratchBytes = std::max(b3::scan_scratch_bytes(std::max<int64_t>(cap, w->cfg.maxBodies + 1)),
+                                      tiles * 8 + 256);
         B3_TRY(dalloc((unsigned char*&)d.scanScratch, d.scanScratchBytes));
     }
     // body-id key bits for the copy sort must cover the sentinel numBodies
@@ -514,6 +527,17 @@ extern "C" int b3_write_bodies(b3World w, void* stream) {
         if (r > 0.5 * w->cfg.maxSmallProxySize) large[w->worldIds[i]].push_back(i);
         else w->smallSlotHost[i] = ns++;
     }
+    if (w->sap) {
+        // sweep and prune: dynamic bodies are the sorted small proxies,
+        // static ones the large proxies (P2/CLPhysicsDemo.cpp:558-568); no
+        // grid hashing
+        w->smallSlotHost.assign(N, -1);
+        for (auto& l : large) l.clear();
+        w->sapSmallHost.clear();
+        w->sapLargeHost.clear();
+        for (int i = 0; i < N; ++i) (w->bodies[i].invMass != 0.f ? w->sapSmallHost : w->sapLargeHost).push_back(i);
+        ns = (int)w->sapSmallHost.size();
+    }
     w->numSmall = ns;
     w->largeStartHost.assign(w->cfg.numWorlds + 1, 0);
     w->largeListHost.clear();
@@ -529,6 +553,14 @@ extern "C" int b3_write_bodies(b3World w, void* stream) {
     if (!w->largeListHost.empty())
         B3_CUDA(cudaMemcpyAsync(d.largeList, w->largeListHost.data(), sizeof(int) * w->largeListHost.size(), cudaMemcpyHostToDevice, st));
     B3_CUDA(cudaMemcpyAsync(d.smallSlot, w->smallSlotHost.data(), sizeof(int) * N, cudaMemcpyHostToDevice, st));
+    if (w->sap) {
+        if (!w->sapSmallHost.empty())
+            B3_CUDA(cudaMemcpyAsync(d.sapSmall, w->sapSmallHost.data(), sizeof(int) * w->sapSmallHost.size(),
+                                    cudaMemcpyHostToDevice, st));
+        if (!w->sapLargeHost.empty())
+            B3_CUDA(cudaMemcpyAsync(d.sapLarge, w->sapLargeHost.data(), sizeof(int) * w->sapLargeHost.size(),
+                                    cudaMemcpyHostToDevice, st));
+    }
     B3_CUDA(cudaMemcpyAsync(d.pos, pos.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, st));
     B3_CUDA(cudaMemcpyAsync(d.quat, quat.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, st));
     B3_CUDA(cudaMemcpyAsync(d.linVel, lv.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, st));

@@ -221,8 +221,15 @@ typedef struct b3WorldConfig {
     float   angularDamping;       /* per-step factor (0.99, BB/integrateKernel.cl:124-126) */
     int32_t frictionCombine;      /* B3_FRICTION_* */
     int32_t useGraph;             /* capture the step as a CUDA graph */
-    int32_t flags;                /* reserved, 0 */
+    int32_t flags;                /* B3_WORLD_* bits, 0 = defaults */
 } b3WorldConfig;
+
+/* flags: B3_WORLD_SAP_BROADPHASE selects the sweep-and-prune broadphase of
+ * gpu_rigidbody_pipeline2 (its default, P2/CLPhysicsDemo.cpp:17) in place of
+ * the uniform grid: dynamic bodies are the sorted small proxies, static
+ * bodies the large proxies (P2/CLPhysicsDemo.cpp:558-568). One world only
+ * (numWorlds = 1), as in the reference. */
+enum { B3_WORLD_SAP_BROADPHASE = 1 };
 
 /* Defaults: reference constants (P2/CLPhysicsDemo.cpp:603-653,
  * BB/integrateKernel.cl:102-158, P2/btPgsJacobiSolver.cpp:171-191). */
@@ -237,6 +244,33 @@ int b3_world_destroy(b3World w);
  * P1/btGpuNarrowPhaseAndSolver.cpp:423-490): convex hull of the scaled
  * points, coplanar face weld, unique edges; local centre = vertex average
  * (P2/CLPhysicsDemo.cpp:360-366). Returns the collidable index. */
+/* btGpuSapBroadphase::calculateOverlappingPairs (P2/btGpuSapBroadphase.cpp:
+ * 97-485) for a world created with B3_WORLD_SAP_BROADPHASE, from the world
+ * AABBs of b3_stage_aabbs (initializeGpuAabbsFull); b3_stage_broadphase of
+ * such a world runs the same. Steps: FloatFlip keys
+ * of the small proxies' minimum x (flipFloatKernel, BB/sap.cl:301-311),
+ * stable 32-bit radix sort, sorted copy (scatterKernel :313-320), then the
+ * pairs: for each sorted small proxy i, first every large proxy whose AABB
+ * overlaps it (computePairsKernelTwoArrays :65-90; pair = (large id, small
+ * id)), then every later proxy j whose minimum x does not exceed i's
+ * maximum x and whose AABB overlaps (computePairsKernel, BB/sapFast.cl:
+ * 48-150; pair = (id_i, id_j)). The reference appends both sets with
+ * atomics in an unspecified order; here the order is the one just given
+ * (deterministic). Pairs beyond maxPairs are counted in pairOverflow. The
+ * pair list replaces the world's (b3_get_device_buffer B3_BUF_PAIRS). */
+int b3_sap_broadphase_calculate_overlapping_pairs(b3World w, void* stream);
+
+/* computePairsKernel (BB/sapFast.cl:48-150) on a caller-sorted array of
+ * n AABBs in the reference's btAabbCL layout (8 floats per AABB: min xyz,
+ * min w = proxy id as int bits, max xyz, max w), sorted by minimum along
+ * axis (0..2): for each i, every later j whose minimum along axis does not
+ * exceed i's maximum and whose AABB overlaps (inclusive, x, z, y) gives the
+ * pair (id_i, id_j), in order of i then j. Writes min(count, maxPairs) pairs
+ * to d_pairs (int2) and the full count to *d_count (device int). Takes the
+ * context for its scratch (allocated per call); synchronises the stream. */
+int b3_sap_compute_pairs(b3Context ctx, const float* d_sortedAabbs, int n, int axis, int32_t* d_pairs,
+                         int maxPairs, int32_t* d_count, void* stream);
+
 int b3_register_convex_hull(b3World w, const float* vertices, int numVertices, int strideBytes,
                             const float scaling[3], int* collidableOut);
 

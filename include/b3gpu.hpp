@@ -11,6 +11,7 @@
  *   b3::World                    CLPhysicsDemo          (P2/CLPhysicsDemo.cpp:603-943):
  *                                registration, writeBodiesToGpu, stepSimulation
  *   b3::GridBroadphase           btGridBroadphaseCl     (BB/btGridBroadphaseCL.h:54-63)
+ *   b3::GpuSapBroadphase         btGpuSapBroadphase     (P2/btGpuSapBroadphase.h)
  *   b3::GpuNarrowphaseAndSolver  btGpuNarrowphaseAndSolver (P1/btGpuNarrowPhaseAndSolver.h:82-111)
  *
  * Device buffers are raw CUDA device pointers (the reference's cl_mem);
@@ -200,6 +201,30 @@ public:
         return n;
     }
     /* int2 (self, other) pairs on the device. */
+    int32_t* getOverlappingPairBuffer() const { return (int32_t*)w_.deviceBuffer(B3_BUF_PAIRS); }
+    float* getAabbMinBuffer() const { return (float*)w_.deviceBuffer(B3_BUF_AABB_MIN); }
+    float* getAabbMaxBuffer() const { return (float*)w_.deviceBuffer(B3_BUF_AABB_MAX); }
+
+private:
+    World& w_;
+};
+
+/* btGpuSapBroadphase (P2/btGpuSapBroadphase.h) over a world created with
+ * B3_WORLD_SAP_BROADPHASE: dynamic bodies are its small proxies, static
+ * bodies its large proxies. */
+class GpuSapBroadphase {
+public:
+    explicit GpuSapBroadphase(World& w) : w_(w) {}
+    void calculateOverlappingPairs(void* stream = nullptr) {
+        check(b3_sap_broadphase_calculate_overlapping_pairs(w_.handle(), stream), "calculateOverlappingPairs");
+    }
+    int getNumOverlap(void* stream = nullptr) const {
+        int n = 0;
+        check(b3_grid_broadphase_get_pair_count(w_.handle(), &n, stream), "getNumOverlap");
+        return n;
+    }
+    /* int2 pairs on the device: (static id, dynamic id) or (id_i, id_j) in
+     * sorted order. */
     int32_t* getOverlappingPairBuffer() const { return (int32_t*)w_.deviceBuffer(B3_BUF_PAIRS); }
     float* getAabbMinBuffer() const { return (float*)w_.deviceBuffer(B3_BUF_AABB_MIN); }
     float* getAabbMaxBuffer() const { return (float*)w_.deviceBuffer(B3_BUF_AABB_MAX); }

@@ -82,6 +82,9 @@ def lib(f32=False, dual=False):
         L.or_set_tangent.argtypes = [_VP, _D, _D, _D, _D, _D]
         L.or_get_tangent.argtypes = [_VP, _D, _D, _D, _D]
         L.or_real_kind.restype = C.c_int
+        L.or_set_broadphase.argtypes = [_VP, C.c_int]
+        L.or_sap_sorted_pairs.restype = C.c_int
+        L.or_sap_sorted_pairs.argtypes = [_F, C.c_int, C.c_int, _I, C.c_int]
         _libs[kind] = L
     return _libs[kind]
 
@@ -222,6 +225,8 @@ class OracleWorld:
                                    C.cast(shapes["faces"], _VP), ni, _i(k["idx"]), ne, _f(k["edges"]),
                                    _f(k["laabb"]))
         self.L = L
+        if int(getattr(cfg, "flags", 0)) & 1:
+            L.or_set_broadphase(self.h, 1)  # sweep and prune
         pos4 = np.zeros((n, 4), np.float32)
         pos4[:, :3] = scene.pos
         lin4 = np.zeros((n, 4), np.float32)
@@ -390,3 +395,14 @@ def large_flags(world, scene, cfg):
     e = np.einsum("nij,nj->ni", np.abs(R), he)
     r = np.linalg.norm(e, axis=1)
     return (r > 0.5 * cfg.maxSmallProxySize).astype(np.int32)
+
+
+def sap_sorted_pairs(sorted_aabbs, axis=0):
+    """computePairsKernel restatement on caller-sorted n x 8 float32 AABB
+    records; returns the pairs (n_pairs x 2 int32) in the device order."""
+    a = np.ascontiguousarray(np.asarray(sorted_aabbs, np.float32).reshape(-1, 8))
+    L = lib()
+    n = L.or_sap_sorted_pairs(_f(a), a.shape[0], axis, None, 0)
+    out = np.zeros((max(n, 1), 2), np.int32)
+    L.or_sap_sorted_pairs(_f(a), a.shape[0], axis, _i(out), n)
+    return out[:n]

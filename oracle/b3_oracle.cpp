@@ -179,6 +179,7 @@ struct or_world {
     std::vector<uint64_t> activeHash;   // row clamp states
     std::vector<uint64_t> topoHash;     // pairs with manifolds, clip sizes, reduced points
     long long pairOverflow, cellOverflow;
+    int sap;  // broadphase: 0 = uniform grid, 1 = sweep and prune
 };
 
 }  // extern "C"
@@ -246,7 +247,104 @@ void stage_aabbs(or_world* w) {
     }
 }
 
+// Sweep-and-prune pairs over small proxies sorted by min along axis, each
+// record (min x, y, z, id | max x, y, z, max.w) as float bits: per sorted
+// proxy i, every large proxy overlapping it (pair (large id, id_i)), then
+// every later j whose min along axis does not exceed i's max and whose AABB
+// overlaps (pair (id_i, id_j)); computePairsKernelTwoArrays (BB/sap.cl:
+// 65-90) and computePairsKernel (BB/sapFast.cl:48-150), with the device
+// build's deterministic order. The overlap test is inclusive, x, z, y; the
+// small-small test skips two max.w both 0 (BB/sapFast.cl:39-41).
+inline bool sap_overlap(const float* a, const float* b) {
+    bool o = true;
+    o = (a[0] > b[4] || a[4] < b[0]) ? false : o;
+    o = (a[2] > b[6] || a[6] < b[2]) ? false : o;
+    o = (a[1] > b[5] || a[5] < b[1]) ? false : o;
+    return o;
+}
+inline int fbits(float f) {
+    int i;
+    memcpy(&i, &f, 4);
+    return i;
+}
+void sap_pairs(const std::vector<float>& sorted8, int n, int axis, const std::vector<float>& large8, int numLarge,
+               std::vector<int>& pairs) {
+    for (int i = 0; i < n; ++i) {
+        const float* a = &sorted8[8 * (size_t)i];
+        for (int l = 0; l < numLarge; ++l) {
+            const float* L = &large8[8 * (size_t)l];
+            if (sap_overlap(L, a)) {
+                pairs.push_back(fbits(L[3]));
+                pairs.push_back(fbits(a[3]));
+            }
+        }
+        const float test = a[4 + axis];
+        for (int j = i + 1; j < n; ++j) {
+            const float* b = &sorted8[8 * (size_t)j];
+            if (test < b[axis]) break;
+            if (fbits(a[7]) == 0 && fbits(b[7]) == 0) continue;
+            if (sap_overlap(a, b)) {
+                pairs.push_back(fbits(a[3]));
+                pairs.push_back(fbits(b[3]));
+            }
+        }
+    }
+}
+
+// FloatFlip (BB/sap.cl:272-278)
+inline uint32_t float_flip(float f) {
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    const uint32_t mask = (uint32_t)(-(int32_t)(u >> 31)) | 0x80000000u;
+    return u ^ mask;
+}
+
+// btGpuSapBroadphase::calculateOverlappingPairs (P2/btGpuSapBroadphase.cpp:
+// 97-485): dynamic bodies are the small proxies, sorted stably by
+// FloatFlip(min.x); static bodies the large ones (P2/CLPhysicsDemo.cpp:
+// 558-568). A small proxy's max.w is its body index (copyAabbsKernel,
+// BB/sap.cl:290-299).
+void stage_broadphase_sap(or_world* w) {
+    const int N = w->n;
+    std::vector<std::pair<uint32_t, int>> kv;
+    std::vector<float> large8;
+    int numLarge = 0;
+    for (int i = 0; i < N; ++i) {
+        if (w->invMass[i] != 0.f) {
+            kv.push_back({float_flip(w->aabb[8 * (size_t)i]), i});
+        } else {
+            large8.insert(large8.end(), &w->aabb[8 * (size_t)i], &w->aabb[8 * (size_t)i] + 8);
+            ++numLarge;
+        }
+    }
+    std::stable_sort(kv.begin(), kv.end(), [](const std::pair<uint32_t, int>& a, const std::pair<uint32_t, int>& b) {
+        return a.first < b.first;
+    });
+    std::vector<float> sorted8(8 * kv.size());
+    w->keys.clear();
+    w->vals.clear();
+    for (size_t s = 0; s < kv.size(); ++s) {
+        const int b = kv[s].second;
+        memcpy(&sorted8[8 * s], &w->aabb[8 * (size_t)b], 8 * sizeof(float));
+        memcpy(&sorted8[8 * s + 7], &b, 4);
+        w->keys.push_back(kv[s].first);
+        w->vals.push_back((uint32_t)b);
+    }
+    w->pairs.clear();
+    w->pairOverflow = 0;
+    w->cellOverflow = 0;
+    sap_pairs(sorted8, (int)kv.size(), 0, large8, numLarge, w->pairs);
+    if (w->cfg.maxPairs > 0 && (long long)w->pairs.size() / 2 > w->cfg.maxPairs) {
+        w->pairOverflow += (long long)w->pairs.size() / 2 - w->cfg.maxPairs;
+        w->pairs.resize(2 * (size_t)w->cfg.maxPairs);
+    }
+}
+
 void stage_broadphase(or_world* w) {
+    if (w->sap) {
+        stage_broadphase_sap(w);
+        return;
+    }
     const int N = w->n;
     const float inv = 1.f / w->cfg.cellSize;
     const int dx = w->cfg.dims[0], dy = w->cfg.dims[1], dz = w->cfg.dims[2];
@@ -1083,6 +1181,18 @@ int or_real_kind() {
 }
 
 void or_stage_aabbs(or_world* w) { stage_aabbs(w); }
+// 0 = uniform grid (default), 1 = sweep and prune
+void or_set_broadphase(or_world* w, int kind) { w->sap = kind == 1 ? 1 : 0; }
+// computePairsKernel restatement on caller-sorted records (8 floats each):
+// writes up to max pairs, returns the full count
+int or_sap_sorted_pairs(const float* sorted8, int n, int axis, int* pairs2, int max) {
+    std::vector<float> s(sorted8, sorted8 + 8 * (size_t)n), none;
+    std::vector<int> p;
+    sap_pairs(s, n, axis, none, 0, p);
+    const int np = (int)p.size() / 2;
+    if (pairs2) memcpy(pairs2, p.data(), 8 * (size_t)std::min(np, max));
+    return np;
+}
 void or_stage_broadphase(or_world* w) { stage_broadphase(w); }
 void or_stage_narrowphase(or_world* w) { stage_narrowphase(w); }
 void or_stage_solve(or_world* w) { stage_solve(w); }

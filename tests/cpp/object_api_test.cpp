@@ -143,6 +143,23 @@ static int gpu_mode() {
     EXPECT(maxSpeed < 0.5f);    // settled
     b3Counters c = w.counters();
     EXPECT(c.timeouts == 0 && c.pairOverflow == 0);
+
+    // --- the sweep-and-prune broadphase (pipeline2's default) ---
+    b3WorldConfig sapCfg = stack_config();
+    sapCfg.flags = B3_WORLD_SAP_BROADPHASE;
+    b3::World ws(ctx, sapCfg);
+    build_stack(ws);
+    b3::GpuSapBroadphase sap(ws);
+    b3::GpuNarrowphaseAndSolver nps(ws);
+    nps.writeAllBodiesToGpu();
+    ws.computeAabbs();
+    sap.calculateOverlappingPairs();
+    EXPECT(sap.getNumOverlap() == pairs);  // the same stack, the same overlaps
+    ws.stepSimulation(120);
+    std::vector<b3Body> sb = ws.readBodies();
+    float sapMinY = 1e9f;
+    for (size_t i = 1; i < sb.size(); ++i) sapMinY = std::min(sapMinY, sb[i].pos[1]);
+    EXPECT(sapMinY > 0.4f);
     return 0;
 }
 

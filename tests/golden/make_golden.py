@@ -21,6 +21,15 @@ jacobi_pins.npz
     (random_pile seeds 21-23, 40 bodies, 40 oracle steps): the Body /
     Inertia / Contact4 arrays it was given and the velocities it returned.
 
+sap_kernel_args.npz
+    The reference's recorded arguments of its sweep-and-prune pair kernel:
+    testdata/m_sapKernelArgs.zip holds m_sapKernelArgs.bin, the btLauncherCL
+    dump of computePairsKernel (BB/sapFast.cl:48-150) taken before a launch
+    (P2/btGpuSapBroadphase.cpp:349-371), the file opencl/tests/main.cpp:
+    110-190 replays: the sorted AABB array (btAabbCL records), the pair and
+    count buffers, numObjects, axis and maxPairs. The fixture keeps the
+    sorted AABBs and the scalars (the output buffers were not yet written).
+
 hull_pins.npz
     btConvexUtility::initializePolyhedralFeatures
     (P1/btConvexUtility.cpp:31-270) on every distinct shape of the plain and
@@ -289,6 +298,18 @@ def make_jacobi():
     return rec
 
 
+def make_sap():
+    import zipfile
+    blob = zipfile.ZipFile(os.path.join(REFERENCE, "testdata", "m_sapKernelArgs.zip")).read("m_sapKernelArgs.bin")
+    args, work = launcher_args(blob)
+    scalar = lambda k: struct.unpack("<i", args[k][1][:4])[0]
+    aabbs = np.frombuffer(args[0][1], np.float32).reshape(-1, 8).copy()
+    rec = dict(sorted_aabbs=aabbs, numObjects=np.int32(scalar(3)), axis=np.int32(scalar(4)),
+               maxPairs=np.int32(scalar(5)), numWorkItems=np.int32(work))
+    np.savez_compressed(os.path.join(HERE, "sap_kernel_args.npz"), **rec)
+    return rec
+
+
 def make_hulls():
     _import_tests()
     import test_cpu_pins as pins
@@ -315,3 +336,5 @@ if __name__ == "__main__":
     r = make_jacobi()
     print("jacobi_pins.npz:", len(r) // 7, "piles")
     print("hull_pins.npz:", make_hulls(), "shapes")
+    r = make_sap()
+    print("sap_kernel_args.npz:", int(r["numObjects"]), "sorted AABBs")
