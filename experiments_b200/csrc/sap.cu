@@ -125,14 +125,16 @@ k_sap_pairs(const float4* __restrict__ sorted, const int32_t* __restrict__ nDev,
     }
 }
 
-// total pairs (from the scan) -> stored count, capped, with the overflow
+// total pairs (from the scan) -> stored count, capped, with the overflow;
+// the step's pair counter as the grid broadphase reports it
 __global__ void k_sap_finalize(int32_t* __restrict__ total, int cap, b3Counters* __restrict__ counters) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         const uint32_t t = (uint32_t)*total;
         if (t > (uint32_t)cap) {
-            if (counters) atomicAdd(&counters->pairOverflow, (int)(t - (uint32_t)cap));
+            atomicAdd(&counters->pairOverflow, (int)(t - (uint32_t)cap));
             *total = cap;
         }
+        counters->numPairs = *total;
     }
 }
 

@@ -43,6 +43,7 @@ def test_sap_pairs_bit_exact(ctx, name):
     assert len(gp) > 0 and np.array_equal(gp, op)
     c = w.counters()
     assert c["pairOverflow"] == o.overflow()[0] == 0 and c["timeouts"] == 0
+    assert c["numPairs"] == len(op)
     # the reference object API's name runs the same
     w.sap_calculate_overlapping_pairs()
     assert np.array_equal(w.pairs(), op)
