@@ -772,7 +772,11 @@ __device__ float3 exact_cut(const ClipGeom& G, int tag, int k, float3 pn, float3
         const float base = length(G.rel) + length(ap) + 0.5f;
         const float ea = 2.4e-7f * pnl * (length(a) + base);
         const float eb = 2.4e-7f * pnl * (length(b) + base);
-        if (!(fabsf(den) > 0.f) || length(b - a) * (ea + eb) > kCutBudget * fabsf(den)) *bad = true;
+        // position error along the edge: t = da / (da - db) moves by
+        // (|db| ea + |da| eb) / den^2 (at most max(ea, eb) / |den| when
+        // da and db have opposite signs, as for a crossing edge)
+        if (!(fabsf(den) > 0.f) || length(b - a) * (fabsf(db) * ea + fabsf(da) * eb) > kCutBudget * den * den)
+            *bad = true;
         const float t = da / den;
         return a + (b - a) * t;
     }
