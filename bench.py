@@ -558,6 +558,10 @@ def main():
     roof["traffic_source"] = "ncu dram bytes per pair on the 16,384-body case, scaled by pairs" \
         if dom == "narrowphase" else None
     roof["peak_kind"] = "nominal FP32 CUDA-core peak" if roof["bound"] == "fp32" else peak_kind
+    if roof["bound"] == "fp32":
+        roof["work"] = ("FLOPs of the reference algorithm (every axis projected, 8 (VA+VB)(FA+FB+EA*EB) per pair "
+                        "+ 64 V_inc V_ref per clip); the sweep skips axes that provably cannot separate or be the "
+                        "minimum, so the FLOPs executed are fewer")
     cfg.update({"bodies": int(sc.n), "worlds": int(sc.num_worlds), "pairs": res["counters"]["numPairs"],
                 "manifolds": res["counters"]["numManifolds"],
                 "contact_points": res["counters"]["numContactPoints"], "iterations": 10, "dt": 1 / 60,
