@@ -124,6 +124,7 @@ enum ScalarSlot {
     S_NP_SLOW = 11,       // pairs queued for the float-float path
     S_NP_WORK2 = 12,
     S_NP_WORK3 = 13,
+    S_NP_WORK4 = 14,
     S_NUM_SCALARS = 16
 };
 

@@ -1421,6 +1421,50 @@ k_np_clip(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, NpP
     }
 }
 
+// Stage 1b, the sweep's near-minimum pairs with stored candidates: the
+// float-float ranking of the candidates only. A pair with an axis then
+// joins the FP32 clip queue with that axis (rounded to FP32, as the contact
+// normal reports it); a pair without one is finished. Its slow-queue entry
+// is cleared, so stage 3 only sees what is left. Pairs whose candidates
+// did not fit the store keep their entry for stage 3's full search.
+__global__ void __launch_bounds__(128, 4)
+k_np_refine(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, float4* __restrict__ pairSep,
+            int* __restrict__ fastQ, int* __restrict__ slowQ, const int* __restrict__ cand,
+            uint32_t* __restrict__ manifoldFlag, int32_t* __restrict__ scalars, b3Counters* __restrict__ counters) {
+    extern __shared__ __align__(16) unsigned char np_smem[];
+    const int lane = threadIdx.x & 31;
+    WarpScratch& W = reinterpret_cast<WarpScratch*>(np_smem)[threadIdx.x >> 5];
+    const int nSlow = scalars[b3::S_NP_SLOW];  // the sweep's entries: the clip has not run
+    int refined = 0;
+    for (;;) {
+        const int q = next_work(scalars + b3::S_NP_WORK4, nSlow, 1);
+        if (q < 0) break;
+        const int p = slowQ[q];
+        const float4 s4 = pairSep[p];
+        const int count = __float_as_int(s4.x);
+        if ((int)s4.w != kSepRefine || count <= 0) continue;
+        PairCtx& c = W.ctx;
+        pair_setup_shared(c, pairs[p], Bd, S);
+        if (lane < count) W.cand[lane] = cand[(size_t)q * kMaxCand + lane];
+        __syncwarp();
+        ff3 sep = mk3(0.f, 0.f, 0.f);
+        const bool haveAxis = refine_axes(c, S, W, count, sep);
+        ++refined;
+        if (lane == 0) {
+            slowQ[q] = -1;
+            if (haveAxis) {
+                const float3 sf = to_f3(sep);
+                pairSep[p] = make_float4(sf.x, sf.y, sf.z, (float)kSepDecided);
+            } else {
+                manifoldFlag[p] = 0u;
+            }
+        }
+        if (haveAxis) push(fastQ, scalars + b3::S_NP_FAST, p);
+        __syncwarp();
+    }
+    if (lane == 0 && refined) atomicAdd(&counters->refinedAxes, refined);
+}
+
 // Stage 3, the pairs either stage handed on: the whole chain with
 // float-float refinement of the axis, the faces, the clip and the reduction.
 __global__ void __launch_bounds__(128, 4)
@@ -1444,6 +1488,7 @@ k_np_exact(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, Np
         const int chunkEnd = min(chunk + 1, nSlow);
         for (int q = chunk; q < chunkEnd; ++q) {
             const int p = slowQ[q];
+            if (p < 0) continue;  // settled by the ranking stage
             PairCtx& c = W.ctx;
             pair_setup_shared(c, pairs[p], Bd, S);
             int nOut = 0, buf = 0;
@@ -1509,7 +1554,7 @@ namespace b3 {
 
 int launch_narrowphase(b3World_t* w, cudaStream_t st) {
     // work counters and queue lengths S_NP_WORK .. S_NP_WORK3
-    B3_CUDA(cudaMemsetAsync(w->d.scalars + S_NP_WORK, 0, sizeof(int32_t) * 5, st));
+    B3_CUDA(cudaMemsetAsync(w->d.scalars + S_NP_WORK, 0, sizeof(int32_t) * 6, st));
     if (w->cfg.maxPairs == 0 || w->bodies.empty()) return B3_OK;
     NpParams P;
     P.minDist = -1e30f;
@@ -1524,6 +1569,7 @@ int launch_narrowphase(b3World_t* w, cudaStream_t st) {
         w->npSmemAttr = (int)smem;
         B3_CUDA(cudaFuncSetAttribute(k_np_clip, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         B3_CUDA(cudaFuncSetAttribute(k_np_exact, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        B3_CUDA(cudaFuncSetAttribute(k_np_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     }
     auto grid_of = [&](const void* k) -> int {
         int occ = 1;
@@ -1546,6 +1592,9 @@ int launch_narrowphase(b3World_t* w, cudaStream_t st) {
     sweep<<<w->ctx->numSMs * occS, threads, smemSweep, st>>>(
         w->d.pairs, sc + S_NUM_PAIRS, Bd, S, w->d.manifoldFlag, w->d.pairSep, w->d.npFast, w->d.npSlow,
         w->d.npCand, std::min(w->cfg.maxPairs, kNpCandSlots), sc, w->d.counters);
+    B3_CHECK_LAUNCH();
+    k_np_refine<<<grid_of((const void*)k_np_refine), threads, smem, st>>>(
+        w->d.pairs, Bd, S, w->d.pairSep, w->d.npFast, w->d.npSlow, w->d.npCand, w->d.manifoldFlag, sc, w->d.counters);
     B3_CHECK_LAUNCH();
     k_np_clip<<<grid_of((const void*)k_np_clip), threads, smem, st>>>(
         w->d.pairs, Bd, S, P, w->d.pairSep, w->d.npFast, w->d.npSlow, w->d.contacts, w->d.manifoldFlag, sc,
