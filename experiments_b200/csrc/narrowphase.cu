@@ -119,30 +119,39 @@ __device__ __forceinline__ float combine_friction(float a, float b, int mode) {
     return mode == B3_FRICTION_PRODUCT ? a * b : sqrtf(a * b);
 }
 
-// lexicographic (value, index) minimum across the warp
-__device__ __forceinline__ void warp_argmin(float& v, int& idx) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        const float ov = __shfl_xor_sync(0xffffffffu, v, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
-        if (ov < v || (ov == v && (unsigned)oi < (unsigned)idx)) {
-            v = ov;
-            idx = oi;
-        }
-    }
+// Integer key whose signed order is the float order: -0 and +0 share a key
+// (the sum with +0 turns -0 into +0) and a NaN never wins a minimum (or a
+// maximum, with kNanMax).
+constexpr int kNanMin = 0x7fffffff, kNanMax = (int)0x80000000;
+__device__ __forceinline__ int fkey(float v, int nanKey) {
+    const int k = __float_as_int(v + 0.f);
+    return v != v ? nanKey : k ^ ((k >> 31) & 0x7fffffff);
 }
+__device__ __forceinline__ float fkey_inv(int k) { return __int_as_float(k ^ ((k >> 31) & 0x7fffffff)); }
+__device__ __forceinline__ float warp_min(float v) {
+    return fkey_inv(__reduce_min_sync(0xffffffffu, fkey(v, kNanMin)));
+}
+__device__ __forceinline__ float warp_max(float v) {
+    return fkey_inv(__reduce_max_sync(0xffffffffu, fkey(v, kNanMax)));
+}
+
+// lexicographic (value, index) minimum across the warp: the minimum value,
+// then the smallest index (as unsigned) among the lanes holding it
+__device__ __forceinline__ void warp_argmin(float& v, int& idx) {
+    const int k = fkey(v, kNanMin);
+    const int km = __reduce_min_sync(0xffffffffu, k);
+    idx = (int)__reduce_min_sync(0xffffffffu, k == km ? (unsigned)idx : 0xffffffffu);
+    v = fkey_inv(km);
+}
+// the same for float-float values, ordered by (hi, lo)
 __device__ __forceinline__ void warp_argmin_ff(ff& v, int& idx) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        ff ov;
-        ov.hi = __shfl_xor_sync(0xffffffffu, v.hi, o);
-        ov.lo = __shfl_xor_sync(0xffffffffu, v.lo, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
-        if (lt(ov, v) || (eq(ov, v) && (unsigned)oi < (unsigned)idx)) {
-            v = ov;
-            idx = oi;
-        }
-    }
+    const int kh = fkey(v.hi, kNanMin);
+    const int mh = __reduce_min_sync(0xffffffffu, kh);
+    const int kl = kh == mh ? fkey(v.lo, kNanMin) : kNanMin;
+    const int ml = __reduce_min_sync(0xffffffffu, kl);
+    idx = (int)__reduce_min_sync(0xffffffffu, kh == mh && kl == ml ? (unsigned)idx : 0xffffffffu);
+    v.hi = fkey_inv(mh);
+    v.lo = fkey_inv(ml);
 }
 
 // FP32 projection of a hull onto world axis dir, relative to the hull's own
@@ -353,13 +362,8 @@ __device__ __forceinline__ int sweep_axes(PairCtx& c, const b3::ShapesDev& S, in
                     lo = fminf(lo, dp);
                     hi = fmaxf(hi, dp);
                 }
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-                    hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
-                }
-                mn[h] = lo;
-                mx[h] = hi;
+                mn[h] = warp_min(lo);
+                mx[h] = warp_max(hi);
             }
             const float off = dot(rel, n);
             const float d = fminf(mx[0] - (mn[1] + off), (mx[1] + off) - mn[0]);
@@ -426,10 +430,7 @@ __device__ __forceinline__ int sweep_axes(PairCtx& c, const b3::ShapesDev& S, in
             int dz = 0;
             warp_argmin(sm0, dz);
             if (sm0 < -delta) return 0;
-            float uf = upper;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) uf = fminf(uf, __shfl_xor_sync(0xffffffffu, uf, o));
-            lbHi = uf;
+            lbHi = warp_min(upper);
         }
     }
     // clearly separated by a face axis
@@ -665,20 +666,16 @@ __device__ __noinline__ int clip_poly_ff(const FfVert* in, int nin, const FfVert
                 }
             }
         }
-        int x = cnt;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
-        }
-        const int pos = total + x - cnt;
+        const unsigned b1 = __ballot_sync(0xffffffffu, cnt >= 1), b2 = __ballot_sync(0xffffffffu, cnt == 2);
+        const unsigned below = b3dev::lanemask_lt();
+        const int pos = total + __popc(b1 & below) + __popc(b2 & below);
         if (cnt >= 1) {
             if (pos < kMaxPoly) out[pos] = vput(o0, mk(0.f)); else atomicAdd(ovf, 1);
         }
         if (cnt == 2) {
             if (pos + 1 < kMaxPoly) out[pos + 1] = vput(o1, mk(0.f)); else atomicAdd(ovf, 1);
         }
-        total += __shfl_sync(0xffffffffu, x, 31);
+        total += __popc(b1) + __popc(b2);
     }
     __syncwarp();
     return min(total, kMaxPoly);
@@ -849,20 +846,17 @@ __device__ __noinline__ int clip_poly_f32(const ClipGeom& G, const FfVert* in, i
                 }
             }
         }
-        int x = cnt;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
-        }
-        const int pos = total + x - cnt;
+        // output slots: exclusive prefix of cnt (0, 1 or 2) from two ballots
+        const unsigned b1 = __ballot_sync(0xffffffffu, cnt >= 1), b2 = __ballot_sync(0xffffffffu, cnt == 2);
+        const unsigned below = b3dev::lanemask_lt();
+        const int pos = total + __popc(b1 & below) + __popc(b2 & below);
         if (cnt >= 1) {
             if (pos < kMaxPoly) put_tagged(out[pos], o0, t0); else atomicAdd(ovf, 1);
         }
         if (cnt == 2) {
             if (pos + 1 < kMaxPoly) put_tagged(out[pos + 1], o1, t1); else atomicAdd(ovf, 1);
         }
-        total += __shfl_sync(0xffffffffu, x, 31);
+        total += __popc(b1) + __popc(b2);
     }
     __syncwarp();
     return min(total, kMaxPoly);
@@ -952,10 +946,7 @@ __device__ __noinline__ int clip_f32(const PairCtx& c, const b3::ShapesDev& S, c
 
 // count of lanes' values within gap of the warp minimum (near-tie test)
 __device__ __forceinline__ int near_count(float best, float v, bool valid, float gap) {
-    int c = (valid && v <= best + gap) ? 1 : 0;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-    return c;
+    return __popc(__ballot_sync(0xffffffffu, valid && v <= best + gap));
 }
 
 // FP32 extractManifoldSequentialGlobal; *tie set when an arg-min is within
@@ -1044,8 +1035,7 @@ __device__ __noinline__ int select_face(const b3::ShapesDev& S, PairCtx& c, bool
         const float4 pl = __ldg((const float4*)&S.faces[h.faceOffset + f].plane[0]);
         if (sign * dot(mul(R, make_float3(pl.x, pl.y, pl.z)), sepf) <= lim) ++inWin;
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) inWin += __shfl_xor_sync(0xffffffffu, inWin, o);
+    inWin = __reduce_add_sync(0xffffffffu, inWin);
     if (inWin <= 1) return wi;
     ensure_ff(c);
     const ffmat& F = sideA ? c.FA : c.FB;
