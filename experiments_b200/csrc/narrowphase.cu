@@ -119,6 +119,13 @@ __device__ __forceinline__ float combine_friction(float a, float b, int mode) {
     return mode == B3_FRICTION_PRODUCT ? a * b : sqrtf(a * b);
 }
 
+// |a| for error bounds and thresholds, rounded up: the approximate
+// reciprocal square root is within a few ulps, which the factor covers
+__device__ __forceinline__ float len_ub(float3 a) {
+    const float d = dot(a, a);
+    return d * rsqrtf(fmaxf(d, FLT_MIN)) * 1.000002f;
+}
+
 // Integer key whose signed order is the float order: -0 and +0 share a key
 // (the sum with +0 turns -0 into +0) and a NaN never wins a minimum (or a
 // maximum, with kNanMax).
@@ -191,7 +198,7 @@ __device__ __forceinline__ bool axis_dir(const PairCtx& c, const b3::ShapesDev& 
     const b3ConvexPolyhedron& pa = *c.pa;
     const b3ConvexPolyhedron& pb = *c.pb;
     const int FA = pa.numFaces, FB = pb.numFaces;
-    const float lD = wantLb ? length(D) : 0.f;
+    const float lD = wantLb ? len_ub(D) : 0.f;
     if (idx < FA + FB) {
         isFace = true;
         const bool onA = idx < FA;
@@ -312,7 +319,7 @@ __device__ __forceinline__ int sweep_axes(PairCtx& c, const b3::ShapesDev& S, in
     const int nFace = pa.numFaces + pb.numFaces;
     const int nAxes = nFace + pa.numUniqueEdges * pb.numUniqueEdges;
     const float scale = 1.f + sqrtf(pa.mE[0] * pa.mE[0] + pa.mE[1] * pa.mE[1] + pa.mE[2] * pa.mE[2]) +
-                        sqrtf(pb.mE[0] * pb.mE[0] + pb.mE[1] * pb.mE[1] + pb.mE[2] * pb.mE[2]) + length(rel);
+                        sqrtf(pb.mE[0] * pb.mE[0] + pb.mE[1] * pb.mE[1] + pb.mE[2] * pb.mE[2]) + len_ub(rel);
     // FP32 depth error bound for well-conditioned axes (a few ulps of the
     // largest projected coordinate); edge axes add a term inversely
     // proportional to |e0 x e1| (their normalisation amplifies rounding)
@@ -485,7 +492,7 @@ __device__ __forceinline__ int sweep_axes(PairCtx& c, const b3::ShapesDev& S, in
         float d, err;
         bool isFace;
         if (axis_f32(c, S, idx, D, rel, delta, n, d, err, isFace) && err <= 31.f * delta &&
-            fabsf(dot(D, n)) > 1e-5f * (length(D) + 1e-3f)) {
+            fabsf(dot(D, n)) > 1e-5f * (len_ub(D) + 1e-3f)) {
             if (dot(-D, n) > 0.f) n = -n;
             sepf = n;
             return 1;
@@ -504,7 +511,7 @@ __device__ __forceinline__ int sweep_axes(PairCtx& c, const b3::ShapesDev& S, in
         if (lane < count) {
             myIdx = cand[lane];
             ok = axis_f32(c, S, myIdx, D, rel, delta, n, d, err, isFace) && err <= 31.f * delta &&
-                 !(isFace && fabsf(d) <= delta) && fabsf(dot(D, n)) > 1e-5f * (length(D) + 1e-3f);
+                 !(isFace && fabsf(d) <= delta) && fabsf(dot(D, n)) > 1e-5f * (len_ub(D) + 1e-3f);
             if (!ok) myIdx = kNone;
         }
         const float3 n0 = make_float3(__shfl_sync(0xffffffffu, n.x, 0), __shfl_sync(0xffffffffu, n.y, 0),
@@ -758,7 +765,7 @@ __device__ __forceinline__ void side_plane(const ClipGeom& G, int k, float3& pn,
 // *bad when its FP32 error bound exceeds the budget.
 __device__ float3 exact_cut(const ClipGeom& G, int tag, int k, float3 pn, float3 ap, float3 sv, float3 ev,
                             bool* bad) {
-    const float pnl = length(pn);
+    const float pnl = len_ub(pn);
     if (tag >= 0 && tag < kPlaneTag) {
         // incident edge j cut by plane k, from its original end points
         const float3 a = inc_vertex(G, tag), b = inc_vertex(G, tag + 1);
@@ -766,13 +773,13 @@ __device__ float3 exact_cut(const ClipGeom& G, int tag, int k, float3 pn, float3
         const float den = da - db;
         // FP32 error of da, db: the end points' transform (|R v| + |rel|)
         // and the anchor, a few ulps each
-        const float base = length(G.rel) + length(ap) + 0.5f;
-        const float ea = 2.4e-7f * pnl * (length(a) + base);
-        const float eb = 2.4e-7f * pnl * (length(b) + base);
+        const float base = len_ub(G.rel) + len_ub(ap) + 0.5f;
+        const float ea = 2.4e-7f * pnl * (len_ub(a) + base);
+        const float eb = 2.4e-7f * pnl * (len_ub(b) + base);
         // position error along the edge: t = da / (da - db) moves by
         // (|db| ea + |da| eb) / den^2 (at most max(ea, eb) / |den| when
         // da and db have opposite signs, as for a crossing edge)
-        if (!(fabsf(den) > 0.f) || length(b - a) * (fabsf(db) * ea + fabsf(da) * eb) > kCutBudget * den * den)
+        if (!(fabsf(den) > 0.f) || len_ub(b - a) * (fabsf(db) * ea + fabsf(da) * eb) > kCutBudget * den * den)
             *bad = true;
         const float t = da / den;
         return a + (b - a) * t;
@@ -787,7 +794,7 @@ __device__ float3 exact_cut(const ClipGeom& G, int tag, int k, float3 pn, float3
         const float3 c23 = cross(n2, n3), c31 = cross(n3, n1), c12 = cross(n1, n2);
         const float det = dot(n1, c23);
         const float3 p = (c23 * h1 + c31 * h2 + c12 * h3) * (1.f / det);
-        const float err = 3.6e-7f * (fabsf(h1) + fabsf(h2) + fabsf(h3) + length(p)) + G.eIn;
+        const float err = 3.6e-7f * (fabsf(h1) + fabsf(h2) + fabsf(h3) + len_ub(p)) + G.eIn;
         if (!(fabsf(det) > 0.f) || err > kCutBudget * fabsf(det)) *bad = true;
         return p;
     }
@@ -797,9 +804,9 @@ __device__ float3 exact_cut(const ClipGeom& G, int tag, int k, float3 pn, float3
     if (tag < 0) *bad = true;
     const float ds = dot(pn, sv - ap), de = dot(pn, ev - ap);
     const float den = ds - de;
-    const float apl = length(ap);
-    const float es = 2.5e-7f * pnl * (1.f + length(sv) + apl), ee = 2.5e-7f * pnl * (1.f + length(ev) + apl);
-    if (!(fabsf(den) > 0.f) || length(ev - sv) * (es + ee) > kCutBudget * fabsf(den)) *bad = true;
+    const float apl = len_ub(ap);
+    const float es = 2.5e-7f * pnl * (1.f + len_ub(sv) + apl), ee = 2.5e-7f * pnl * (1.f + len_ub(ev) + apl);
+    if (!(fabsf(den) > 0.f) || len_ub(ev - sv) * (es + ee) > kCutBudget * fabsf(den)) *bad = true;
     return sv + (ev - sv) * (ds / den);
 }
 
@@ -808,8 +815,8 @@ __device__ __noinline__ int clip_poly_f32(const ClipGeom& G, const FfVert* in, i
     const int lane = threadIdx.x & 31;
     float3 pn, ap;
     side_plane(G, k, pn, ap);
-    const float pnl = length(pn);
-    const float apl = length(ap);
+    const float pnl = len_ub(pn);
+    const float apl = len_ub(ap);
     const unsigned newTag = (unsigned)(kPlaneTag + k);
     int total = 0;
     for (int base = 0; base < nin; base += 32) {
@@ -824,8 +831,8 @@ __device__ __noinline__ int clip_poly_f32(const ClipGeom& G, const FfVert* in, i
             const float ds = dot(pn, sv - ap);
             const float de = dot(pn, ev - ap);
             // inside / outside decisions: FP32 error of ds, de
-            const float es = 2.5e-7f * pnl * (1.f + length(sv) + apl);
-            const float ee = 2.5e-7f * pnl * (1.f + length(ev) + apl);
+            const float es = 2.5e-7f * pnl * (1.f + len_ub(sv) + apl);
+            const float ee = 2.5e-7f * pnl * (1.f + len_ub(ev) + apl);
             if (fabsf(ds) <= es || fabsf(de) <= ee) *bad = true;
             const bool sNeg = ds < 0.f, eNeg = de < 0.f;
             if (sNeg || eNeg) {
@@ -886,7 +893,7 @@ __device__ __noinline__ int clip_f32(const PairCtx& c, const b3::ShapesDev& S, c
         // rel is exact for nearby bodies, the dot is compensated, and the
         // rounding of nIn only matters when B is rotated (times |rel|)
         g.hIn = -g.fB.plane[3] + dot2(g.nIn, g.rel);
-        g.eIn = 2.5e-7f * (fabsf(g.fB.plane[3]) + fabsf(g.hIn)) + (exact_axes(c.RB) ? 0.f : 2.4e-7f * length(g.rel));
+        g.eIn = 2.5e-7f * (fabsf(g.fB.plane[3]) + fabsf(g.hIn)) + (exact_axes(c.RB) ? 0.f : 2.4e-7f * len_ub(g.rel));
         if (lane == 0) W.geom = g;
         __syncwarp();
     }
@@ -929,7 +936,7 @@ __device__ __noinline__ int clip_f32(const PairCtx& c, const b3::ShapesDev& S, c
         if (k < nIn) {
             p = get_f32(W.poly[cur][k]);
             depth = dot(nAw, p) + fA.plane[3];
-            if (fabsf(depth - P.maxDist) <= 5e-7f * (1.f + length(p))) bad = true;
+            if (fabsf(depth - P.maxDist) <= 5e-7f * (1.f + len_ub(p))) bad = true;
             if (depth <= P.minDist) depth = P.minDist;
             keep = depth <= P.maxDist;
         }
@@ -971,10 +978,13 @@ __device__ __noinline__ int4 reduce_f32(const FfVert* p, int n, float3 nearNorma
     float fw[2], fu[2], fv[2];
     float mw = FLT_MAX, f0 = FLT_MIN, f1 = FLT_MIN, f2 = FLT_MIN, f3v = FLT_MIN;
     int iw = kNone, i0 = kNone, i1 = kNone, i2 = kNone, i3 = kNone;
+    // a second point per lane only past 32 points (n is warp-uniform)
+    const int nj = n > 32 ? 2 : 1;
+#pragma unroll
     for (int j = 0; j < 2; ++j) {
         const int k = lane + 32 * j;
         fw[j] = FLT_MAX; fu[j] = 0.f; fv[j] = 0.f;
-        if (k < n) {
+        if (j < nj && k < n) {
             const float3 r = (get_f32(p[k]) - o) - cr;
             fw[j] = p[k].wh;
             fu[j] = dot(u, r);
@@ -993,7 +1003,9 @@ __device__ __noinline__ int4 reduce_f32(const FfVert* p, int n, float3 nearNorma
     warp_argmin(f3v, i3);
     const float gap = 2e-6f, gapw = 1e-6f;
     int worst = 0;
+#pragma unroll
     for (int j = 0; j < 2; ++j) {
+        if (j >= nj) break;
         const bool ok = lane + 32 * j < n;
         worst = max(worst, near_count(mw, fw[j], ok, gapw));
         worst = max(worst, near_count(f0, fu[j], ok, gap));
@@ -1019,9 +1031,11 @@ __device__ __noinline__ int select_face(const b3::ShapesDev& S, PairCtx& c, bool
     const int lane = threadIdx.x & 31;
     float bv = FLT_MAX;
     int bi = kNone;
+    float d0 = FLT_MAX;  // this lane's first face
     for (int f = lane; f < h.numFaces; f += 32) {
         const float4 pl = __ldg((const float4*)&S.faces[h.faceOffset + f].plane[0]);
         const float d = sign * dot(mul(R, make_float3(pl.x, pl.y, pl.z)), sepf);
+        if (f == lane) d0 = d;
         if (d < bv) { bv = d; bi = f; }
     }
     float wv = bv;
@@ -1030,12 +1044,17 @@ __device__ __noinline__ int select_face(const b3::ShapesDev& S, PairCtx& c, bool
     if (wi == kNone) return kNone;
     const float lim = wv + 4e-6f;
     // near-ties only: count faces inside the window
-    int inWin = 0;
-    for (int f = lane; f < h.numFaces; f += 32) {
-        const float4 pl = __ldg((const float4*)&S.faces[h.faceOffset + f].plane[0]);
-        if (sign * dot(mul(R, make_float3(pl.x, pl.y, pl.z)), sepf) <= lim) ++inWin;
+    int inWin;
+    if (h.numFaces <= 32) {
+        inWin = __popc(__ballot_sync(0xffffffffu, d0 <= lim));
+    } else {
+        inWin = 0;
+        for (int f = lane; f < h.numFaces; f += 32) {
+            const float4 pl = __ldg((const float4*)&S.faces[h.faceOffset + f].plane[0]);
+            if (sign * dot(mul(R, make_float3(pl.x, pl.y, pl.z)), sepf) <= lim) ++inWin;
+        }
+        inWin = __reduce_add_sync(0xffffffffu, inWin);
     }
-    inWin = __reduce_add_sync(0xffffffffu, inWin);
     if (inWin <= 1) return wi;
     ensure_ff(c);
     const ffmat& F = sideA ? c.FA : c.FB;
