@@ -23,6 +23,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "libb3gpu.so")
 B3_WORLD_SAP_BROADPHASE = 1  # b3WorldConfig.flags: sweep-and-prune broadphase
+B3_WORLD_BATCHED_GS_SOLVER = 2  # b3WorldConfig.flags: the reference GPU solver (batched Gauss-Seidel)
 
 B3_OK = 0
 STATUS = {0: "OK", 1: "INVALID_ARG", 2: "CUDA", 3: "CAPACITY", 4: "NO_DEVICE", 5: "STATE",
@@ -66,6 +67,13 @@ class Contact4(C.Structure):
     _fields_ = [("worldPos", (C.c_float * 4) * 4), ("worldNormal", C.c_float * 4),
                 ("friction", C.c_float), ("pairIndex", C.c_int), ("bodyAPtrAndSignBit", C.c_int),
                 ("bodyBPtrAndSignBit", C.c_int)]
+
+
+class Constraint4(C.Structure):
+    _fields_ = [("linear", C.c_float * 4), ("worldPos", (C.c_float * 4) * 4), ("center", C.c_float * 4),
+                ("jacCoeffInv", C.c_float * 4), ("b", C.c_float * 4), ("appliedRambdaDt", C.c_float * 4),
+                ("fJacCoeffInv", C.c_float * 2), ("fAppliedRambdaDt", C.c_float * 2), ("bodyA", C.c_uint32),
+                ("bodyB", C.c_uint32), ("batchIdx", C.c_int32), ("padding", C.c_uint32)]
 
 
 class Counters(C.Structure):
@@ -142,6 +150,9 @@ SIGNATURES = [
     ("b3_grid_broadphase_get_pair_count", _I, [_P, _IP, _P]),
     ("b3_narrowphase_compute_contacts", _I, [_P, _P, _I, _P]),
     ("b3_solver_solve_jacobi", _I, [_P, _P]),
+    ("b3_solver_solve_batched_gs", _I, [_P, _P]),
+    ("b3_get_gs_batches", _I, [_P, _IP, _I, _IP, _P]),
+    ("b3_get_gs_constraints", _I, [_P, C.POINTER(Constraint4), _I, _IP, _P]),
     ("b3_integrate", _I, [_P, _P]),
     ("b3_get_aabbs", _I, [_P, _FP, _I, _P]),
     ("b3_get_sorted_hash", _I, [_P, _U32P, _U32P, _I, _IP, _P]),
@@ -534,6 +545,33 @@ class PhysicsWorld:
         with flags=B3_WORLD_SAP_BROADPHASE (from the current AABBs)."""
         _check(self.lib.b3_sap_broadphase_calculate_overlapping_pairs(self.h, _stream(stream)),
                "b3_sap_broadphase_calculate_overlapping_pairs")
+
+    def solve_batched_gs(self, stream=None):
+        """Solver::batchContacts + convertToConstraints + solveContactConstraint
+        on a world created with flags=B3_WORLD_BATCHED_GS_SOLVER."""
+        _check(self.lib.b3_solver_solve_batched_gs(self.h, _stream(stream)), "b3_solver_solve_batched_gs")
+
+    def gs_batches(self):
+        """(cell, batch) per manifold from the last batched Gauss-Seidel solve (M x 2)."""
+        cnt = C.c_int()
+        _check(self.lib.b3_get_gs_batches(self.h, None, 0, C.byref(cnt), None), "b3_get_gs_batches")
+        out = np.zeros((max(cnt.value, 1), 2), np.int32)
+        _check(self.lib.b3_get_gs_batches(self.h, iptr(out), cnt.value, C.byref(cnt), None), "b3_get_gs_batches")
+        return out[:cnt.value]
+
+    def gs_constraints(self):
+        """Constraint4 per manifold after the last batched Gauss-Seidel solve:
+        dict of arrays (applied impulses included)."""
+        cnt = C.c_int()
+        _check(self.lib.b3_get_gs_constraints(self.h, None, 0, C.byref(cnt), None), "b3_get_gs_constraints")
+        n = cnt.value
+        arr = (Constraint4 * max(n, 1))()
+        _check(self.lib.b3_get_gs_constraints(self.h, arr, n, C.byref(cnt), None), "b3_get_gs_constraints")
+        raw = np.frombuffer(arr, np.float32).reshape(-1, 44)[:n]
+        ints = raw.view(np.int32)
+        return dict(linear=raw[:, 0:4], worldPos=raw[:, 4:20].reshape(-1, 4, 4), center=raw[:, 20:24],
+                    jacCoeffInv=raw[:, 24:28], b=raw[:, 28:32], applied=raw[:, 32:36], fJacCoeffInv=raw[:, 36:38],
+                    fApplied=raw[:, 38:40], bodyA=ints[:, 40], bodyB=ints[:, 41], batchIdx=ints[:, 42])
 
     def compute_contacts(self, d_pairs=None, num_pairs=0, stream=None):
         """Narrowphase on caller device pairs (int2) or, with None, on the

@@ -1065,6 +1065,10 @@ extern "C" int b3_adjoint_create(b3World w, int numSteps, int checkpointEvery, b
     if (!w || !out || numSteps <= 0 || checkpointEvery <= 0) return B3_ERR_INVALID_ARG;
     *out = nullptr;
     if (!w->written) return B3_ERR_STATE;
+    if (w->gs) {
+        b3_set_error("the adjoint form differentiates the Jacobi solver; this world runs batched Gauss-Seidel");
+        return B3_ERR_UNSUPPORTED;
+    }
     B3_CUDA(cudaSetDevice(w->ctx->device));
     b3Adjoint_t* a = new b3Adjoint_t();
     a->w = w;

@@ -107,6 +107,20 @@ struct DevBuffers {
     size_t scanScratchBytes = 0;
     float4* worldStats = nullptr;
     int *worldMStart = nullptr, *worldMEnd = nullptr;  // per world: manifold range (batched solver)
+    // batched Gauss-Seidel solver (B3_WORLD_BATCHED_GS_SOLVER); the
+    // Constraint4 records live in the Jacobi row storage, which that solver
+    // does not use
+    int* gsCell = nullptr;            // per manifold: cell x + 16 z
+    int* gsSlotBatch = nullptr;       // per sorted slot: batch
+    int* gsSlotOfManifold = nullptr;  // per manifold: index of its Constraint4
+    int* gsMinRank = nullptr;         // [4][bodies]
+    int* gsTaken = nullptr;           // [4][bodies]
+    int* gsBatchCount = nullptr;      // [4] batches per class, then 5 round counters
+    uint32_t* gsGroupCount = nullptr; // [4 * kGsMaxBatch]
+    uint32_t* gsGroupFill = nullptr;  // [4 * kGsMaxBatch]
+    uint32_t* gsGroupOffset = nullptr;  // [4 * kGsMaxBatch + 1]
+    float4* gsInertia = nullptr;      // [3][bodies] world inverse inertia rows
+    b3Constraint4* gsConstraints = nullptr;
 };
 
 enum ScalarSlot {
@@ -150,6 +164,7 @@ struct b3World_t {
     std::vector<int> smallSlotHost, largeStartHost, largeListHost;
     int numSmall = 0;
     bool sap = false;    // sweep-and-prune broadphase in place of the grid
+    bool gs = false;     // batched Gauss-Seidel solver in place of Jacobi
     std::vector<int> sapSmallHost, sapLargeHost;
     int capBodies = 0;   // allocated body capacity on device
     int capInc = 0;
@@ -189,6 +204,7 @@ namespace b3 {
 // slots of the narrowphase candidate store (pairs queued for float-float
 // axis ranking beyond this recompute their FP32 sweep)
 constexpr int kNpCandSlots = 1 << 20;
+constexpr int kGsMaxBatch = 1024;  // batches per parity class (batched Gauss-Seidel)
 
 // Record of one Jacobi solve for the reverse sweep: every phase's solver-body
 // copies (both sides of every manifold) and the row impulses after it.
@@ -211,6 +227,7 @@ int launch_manifolds(b3World_t* w, cudaStream_t st);
 int launch_solver(b3World_t* w, cudaStream_t st);
 int launch_solver_taped(b3World_t* w, cudaStream_t st, const JacobiTape* tape);
 int launch_integrate(b3World_t* w, cudaStream_t st);
+int launch_gs_solver(b3World_t* w, cudaStream_t st);
 int launch_world_stats(b3World_t* w, cudaStream_t st);
 // one eager step (world.cu); tape may be null
 int run_step(b3World_t* w, cudaStream_t st, const JacobiTape* tape);

@@ -462,6 +462,7 @@ int launch_manifolds(b3World_t* w, cudaStream_t st) {
                                       w->d.contacts, w->d.invMass, N, w->d.manifoldPair, w->d.incKeys,
                                       w->d.incVals, w->d.scalars, w->d.counters);
     B3_CHECK_LAUNCH();
+    if (w->gs) return B3_OK;  // body incidences serve the Jacobi averaging only
     bool alt = false;
     B3_TRY(radix_sort_pairs(w->d.incKeys, w->d.incVals, w->d.incKeysAlt, w->d.incValsAlt,
                             w->d.scalars + S_NUM_INC, 2LL * cap, w->bodyBits, w->d.incSortScratch,
@@ -482,6 +483,13 @@ int launch_solver(b3World_t* w, cudaStream_t st) { return launch_solver_taped(w,
 
 int launch_solver_taped(b3World_t* w, cudaStream_t st, const JacobiTape* tape) {
     if (w->cfg.maxPairs == 0 || w->bodies.empty()) return B3_OK;
+    if (w->gs) {
+        if (tape) {
+            b3_set_error("the adjoint form runs the Jacobi solver only");
+            return B3_ERR_UNSUPPORTED;
+        }
+        return launch_gs_solver(w, st);
+    }
     SolverView V = solver_view(w);
     SetupParams SP;
     SP.dt = w->sim.dt;
@@ -559,8 +567,9 @@ int launch_integrate(b3World_t* w, cudaStream_t st) {
     P.damping = w->sim.angularDamping;
     P.threshold = 0.25f * 3.14159254f;
     const int iters = w->sim.iterations;
+    // the batched Gauss-Seidel solver leaves final velocities in the bodies
     k_integrate<<<(N + 255) / 256, 256, 0, st>>>(w->bodiesDev(), solver_view(w), (2 * iters - 1) & 1, P,
-                                                iters > 0 ? 1 : 0);
+                                                iters > 0 && !w->gs ? 1 : 0);
     B3_CHECK_LAUNCH();
     return B3_OK;
 }

@@ -188,7 +188,8 @@ extern "C" int b3_world_create(b3Context ctx, const b3WorldConfig* cfg, b3World*
         b3_set_error("world id + cell hash need %d > 32 key bits", cellBits + worldBits);
         return B3_ERR_INVALID_ARG;
     }
-    if ((c.flags & ~B3_WORLD_SAP_BROADPHASE) != 0 || ((c.flags & B3_WORLD_SAP_BROADPHASE) && c.numWorlds != 1)) {
+    if ((c.flags & ~(B3_WORLD_SAP_BROADPHASE | B3_WORLD_BATCHED_GS_SOLVER)) != 0 ||
+        ((c.flags & B3_WORLD_SAP_BROADPHASE) && c.numWorlds != 1)) {
         b3_set_error("invalid world flags (the SAP broadphase takes one world)");
         return B3_ERR_INVALID_ARG;
     }
@@ -196,6 +197,7 @@ extern "C" int b3_world_create(b3Context ctx, const b3WorldConfig* cfg, b3World*
     w->ctx = ctx;
     w->cfg = c;
     w->sap = (c.flags & B3_WORLD_SAP_BROADPHASE) != 0;
+    w->gs = (c.flags & B3_WORLD_BATCHED_GS_SOLVER) != 0;
     if (w->cfg.maxPairs <= 0) w->cfg.maxPairs = 8 * c.maxBodies;
     w->cellBits = cellBits;
     w->worldBits = worldBits;
@@ -421,6 +423,11 @@ static int ensure_capacity(b3World w) {
         B3_TRY(dalloc(d.bodyIncEnd, nb));
         B3_TRY(dalloc(d.avgLin, nb));
         B3_TRY(dalloc(d.avgAng, nb));
+        if (w->gs) {
+            B3_TRY(dalloc(d.gsMinRank, 4 * (size_t)nb));
+            B3_TRY(dalloc(d.gsTaken, 4 * (size_t)nb));
+            B3_TRY(dalloc(d.gsInertia, 3 * (size_t)nb));
+        }
         d.sortScratchBytes = b3::radix_scratch_bytes(nb, w->keyBits);
         B3_TRY(dalloc((unsigned char*&)d.sortScratch, d.sortScratchBytes));
         w->capBodies = nb;
@@ -443,6 +450,17 @@ static int ensure_capacity(b3World w) {
         B3_TRY(dalloc(d.rows, 40 * c));
         B3_TRY(dalloc(d.incLin, 4 * c));  // [2 phase buffers][2 sides][capacity]
         B3_TRY(dalloc(d.incAng, 4 * c));
+        if (w->gs) {
+            static_assert(sizeof(b3Constraint4) <= 40 * sizeof(float4), "Constraint4 fits a manifold's rows");
+            d.gsConstraints = reinterpret_cast<b3Constraint4*>(d.rows);
+            B3_TRY(dalloc(d.gsCell, c));
+            B3_TRY(dalloc(d.gsSlotBatch, c));
+            B3_TRY(dalloc(d.gsSlotOfManifold, c));
+            B3_TRY(dalloc(d.gsBatchCount, 16));
+            B3_TRY(dalloc(d.gsGroupCount, 4 * (size_t)b3::kGsMaxBatch));
+            B3_TRY(dalloc(d.gsGroupFill, 4 * (size_t)b3::kGsMaxBatch));
+            B3_TRY(dalloc(d.gsGroupOffset, 4 * (size_t)b3::kGsMaxBatch + 1));
+        }
         const size_t tiles = (w->cfg.maxBodies + 127) / 128 + 16;
         d.scanScratchBytes = std::max(b3::scan_scratch_bytes(std::max<int64_t>(cap, w->cfg.maxBodies + 1)),
                                       tiles * 8 + 256);
@@ -450,7 +468,8 @@ static int ensure_capacity(b3World w) {
     }
     // body-id key bits for the copy sort must cover the sentinel numBodies
     w->bodyBits = std::max(1, ilog2((uint64_t)N + 1));
-    const size_t incBytes = b3::radix_scratch_bytes(2LL * cap, w->bodyBits);
+    const size_t incBytes = std::max(b3::radix_scratch_bytes(2LL * cap, w->bodyBits),
+                                     w->gs ? b3::radix_scratch_bytes(cap, 10) : (size_t)0);
     if (incBytes > d.incSortScratchBytes) {
         d.incSortScratchBytes = incBytes;
         B3_TRY(dalloc((unsigned char*&)d.incSortScratch, incBytes));

@@ -113,6 +113,28 @@ typedef struct b3Contact4 {
     int bodyBPtrAndSignBit;
 } b3Contact4;
 
+/* Constraint4, ST/AdlConstraint4.h:23-47 (176 bytes, same layout): one
+ * manifold as the batched Gauss-Seidel solver holds it. linear = -normal
+ * (w = friction coefficient), jacCoeffInv = -1 / effective mass per point
+ * (0 for an unused point), b = position correction per point, appliedRambdaDt
+ * = accumulated normal impulses, center and fJacCoeffInv / fAppliedRambdaDt
+ * the two friction directions at the manifold centre. bodyA / bodyB are
+ * body indices (no sign), batchIdx the batch within the parity class. */
+typedef struct b3Constraint4 {
+    float linear[4];
+    float worldPos[4][4];
+    float center[4];
+    float jacCoeffInv[4];
+    float b[4];
+    float appliedRambdaDt[4];
+    float fJacCoeffInv[2];
+    float fAppliedRambdaDt[2];
+    uint32_t bodyA;
+    uint32_t bodyB;
+    int32_t batchIdx;
+    uint32_t padding;
+} b3Constraint4;
+
 /* Step diagnostics (the reference truncates silently; the build counts). */
 typedef struct b3Counters {
     int32_t numPairs;            /* broadphase pairs this step */
@@ -230,6 +252,21 @@ typedef struct b3WorldConfig {
  * bodies the large proxies (P2/CLPhysicsDemo.cpp:558-568). One world only
  * (numWorlds = 1), as in the reference. */
 enum { B3_WORLD_SAP_BROADPHASE = 1 };
+/* flags: B3_WORLD_BATCHED_GS_SOLVER selects the reference's GPU solver
+ * (btGpuNarrowphaseAndSolver::solveContacts, P1/btGpuNarrowPhaseAndSolver.cpp:
+ * 1073-1353, with ST/Solver.cpp) in place of pipeline2's Jacobi solver:
+ * manifolds binned to a 16 x 16 grid of 2 m xz cells by their dynamic body
+ * (SetSortDataKernel, ST/solverSetup2.cl:457-478), cells taken in four
+ * parity classes (ST/solveContact.cl:418-426), each class coloured into
+ * batches without a shared dynamic body, Constraint4 set up per manifold
+ * (ST/solverSetup.cl:520-609), then 4 contact and 4 friction Gauss-Seidel
+ * iterations, batch after batch (ST/Solver.cpp:561-700), writing body
+ * velocities directly. The colouring is the greedy pass of the reference's
+ * CPU batching (sortConstraintByBatch, P1/btGpuNarrowPhaseAndSolver.cpp:
+ * 752-852) over each class in (cell, manifold) order with exact body
+ * identities: deterministic, and free of the reference GPU colouring's
+ * races between concurrently solved cells. */
+enum { B3_WORLD_BATCHED_GS_SOLVER = 2 };
 
 /* Defaults: reference constants (P2/CLPhysicsDemo.cpp:603-653,
  * BB/integrateKernel.cl:102-158, P2/btPgsJacobiSolver.cpp:171-191). */
@@ -342,11 +379,20 @@ int b3_narrowphase_compute_contacts(b3World w, const int32_t* d_pairs, int numPa
 /* btPgsJacobiSolver::solveContacts (P2/btPgsJacobiSolver.cpp:171-189) on the
  * device: same as b3_stage_solve. */
 int b3_solver_solve_jacobi(b3World w, void* stream);
+/* Solver::batchContacts + convertToConstraints + solveContactConstraint
+ * (ST/Solver.cpp:561-761, 842-925) for a world created with
+ * B3_WORLD_BATCHED_GS_SOLVER: same as b3_stage_solve of such a world. */
+int b3_solver_solve_batched_gs(b3World w, void* stream);
 /* integrateTransformsKernel2 (BB/integrateKernel.cl:102-158): same as
  * b3_stage_integrate. */
 int b3_integrate(b3World w, void* stream);
 
 /* --- stage outputs (host copies, synchronising) --- */
+/* Batched Gauss-Seidel solver: per manifold (manifold order of
+ * b3_get_contacts) its cell (x + 16 z) and batch, 2 ints each, and its
+ * Constraint4 after the last solve (applied impulses included). */
+int b3_get_gs_batches(b3World w, int32_t* cellBatch2, int max, int* count, void* stream);
+int b3_get_gs_constraints(b3World w, b3Constraint4* out, int max, int* count, void* stream);
 /* World AABBs, 2 float4 per body (min.w = body id bits, max.w = dynamic flag). */
 int b3_get_aabbs(b3World w, float* out8, int maxBodies, void* stream);
 /* Sorted (cell key, body id) of the small bodies; returns count. */

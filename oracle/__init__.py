@@ -83,6 +83,12 @@ def lib(f32=False, dual=False):
         L.or_get_tangent.argtypes = [_VP, _D, _D, _D, _D]
         L.or_real_kind.restype = C.c_int
         L.or_set_broadphase.argtypes = [_VP, C.c_int]
+        L.or_set_solver.argtypes = [_VP, C.c_int]
+        L.or_gs_batches.restype = C.c_int
+        L.or_gs_batches.argtypes = [_VP, _I, C.c_int]
+        L.or_gs_applied.restype = C.c_int
+        L.or_gs_applied.argtypes = [_VP, _D, C.c_int]
+        L.or_gs_constraint.argtypes = [_D, _D, _D, _D, C.c_double, C.c_double, _D, _D, C.c_double, _D]
         L.or_sap_sorted_pairs.restype = C.c_int
         L.or_sap_sorted_pairs.argtypes = [_F, C.c_int, C.c_int, _I, C.c_int]
         _libs[kind] = L
@@ -227,6 +233,8 @@ class OracleWorld:
         self.L = L
         if int(getattr(cfg, "flags", 0)) & 1:
             L.or_set_broadphase(self.h, 1)  # sweep and prune
+        if int(getattr(cfg, "flags", 0)) & 2:
+            L.or_set_solver(self.h, 1)  # batched Gauss-Seidel
         pos4 = np.zeros((n, 4), np.float32)
         pos4[:, :3] = scene.pos
         lin4 = np.zeros((n, 4), np.float32)
@@ -327,6 +335,21 @@ class OracleWorld:
         self.L.or_get_tangent(self.h, *[_d(a) for a in out])
         return out
 
+    def gs_batches(self):
+        """(cell, batch) per manifold from the last batched Gauss-Seidel solve (M x 2)."""
+        m = self.L.or_gs_batches(self.h, None, 0)
+        out = np.zeros((max(m, 1), 2), np.int32)
+        self.L.or_gs_batches(self.h, _i(out), m)
+        return out[:m]
+
+    def gs_applied(self):
+        """Accumulated impulses per manifold from the last batched Gauss-Seidel
+        solve: M x 6 (normal [4], friction [2])."""
+        m = self.L.or_gs_applied(self.h, None, 0)
+        out = np.zeros((max(m, 1), 6))
+        self.L.or_gs_applied(self.h, _d(out), m)
+        return out[:m]
+
     def solve_velocities(self):
         lin = np.zeros((self.n, 4))
         ang = np.zeros((self.n, 4))
@@ -406,3 +429,14 @@ def sap_sorted_pairs(sorted_aabbs, axis=0):
     out = np.zeros((max(n, 1), 2), np.int32)
     L.or_sap_sorted_pairs(_f(a), a.shape[0], axis, _i(out), n)
     return out[:n]
+
+
+def gs_constraint(pos4x4, normal4, posA, posB, inv_mass_a, inv_mass_b, inv_inertia_a, inv_inertia_b, dt):
+    """setConstraint4 of the batched Gauss-Seidel restatement on one manifold:
+    (jacCoeffInv[4], b[4], center[3], fJacCoeffInv[2])."""
+    out = np.zeros(13)
+    arr = [np.ascontiguousarray(np.asarray(a, np.float64).reshape(-1))
+           for a in (pos4x4, normal4, posA, posB, inv_inertia_a, inv_inertia_b)]
+    lib().or_gs_constraint(_d(arr[0]), _d(arr[1]), _d(arr[2]), _d(arr[3]), float(inv_mass_a), float(inv_mass_b),
+                           _d(arr[4]), _d(arr[5]), float(dt), _d(out))
+    return out[:4], out[4:8], out[8:11], out[11:13]

@@ -180,6 +180,10 @@ struct or_world {
     std::vector<uint64_t> topoHash;     // pairs with manifolds, clip sizes, reduced points
     long long pairOverflow, cellOverflow;
     int sap;  // broadphase: 0 = uniform grid, 1 = sweep and prune
+    int gs;   // solver: 0 = Jacobi (pipeline2), 1 = batched Gauss-Seidel (the reference GPU solver)
+    // batched Gauss-Seidel: per manifold its cell (xz, 16 x 16) and batch
+    std::vector<int> gsCell, gsBatch;
+    std::vector<double> gsApplied;  // per manifold: normal impulses [4], friction impulses [2]
 };
 
 }  // extern "C"
@@ -830,7 +834,296 @@ int solve_row(Row& c, Copy& A, Copy& B, Real imA, Real imB, V iiA, V iiB) {
     return state;
 }
 
+
+// ---------------------------------------------------------------------------
+// Batched Gauss-Seidel solver: the reference's GPU solver
+// (P1/btGpuNarrowPhaseAndSolver.cpp:1073-1353 driving ST/Solver.cpp), in
+// FP64. Structure followed: contacts binned to a 16 x 16 xz grid of cells
+// (SetSortDataKernel, ST/solverSetup2.cl:457-478), cells solved in four
+// parity classes (BatchSolveKernelContact, ST/solveContact.cl:418-426),
+// batches of constraints without a shared dynamic body solved one after
+// another, four contact iterations then four friction iterations
+// (ST/Solver.cpp:561-700), Constraint4 set up by setConstraint4
+// (ST/solverSetup.cl:520-609). The colouring is the sequential greedy pass
+// of the reference's CPU batching (sortConstraintByBatch,
+// P1/btGpuNarrowPhaseAndSolver.cpp:752-852) run over each parity class in
+// (cell, manifold) order with exact body identities, so that no dynamic
+// body appears twice in a batch anywhere in the class (the reference's GPU
+// colouring is per cell, with atomics, and races on bodies shared by
+// concurrently solved cells). Static means inverse mass 0.
+// ---------------------------------------------------------------------------
+namespace gs {
+
+constexpr int kSplit = 16;          // SolverBase::N_SPLIT
+constexpr int kIterations = 4;      // m_nIterations (:1330)
+constexpr float kScale = 0.5f;      // 1 / (N_OBJ_PER_SPLIT * m_averageExtent) = 1 / (10 * 0.2)
+constexpr double kFriction = 0.7;   // m_linear.w (solverSetup.cl:541), solveFriction.cl:319
+constexpr double kDrift = 0.005;    // ConstraintCfg::m_positionDrift
+constexpr double kPosCoeff = 0.2;   // ConstraintCfg::m_positionConstraintCoeff
+
+struct M3 {
+    V r[3];
+};
+inline V mul(const M3& m, V v) { return V(dot(m.r[0], v), dot(m.r[1], v), dot(m.r[2], v)); }
+
+struct C4 {  // Constraint4 (ST/AdlConstraint4.h:23-47) in Real
+    V linear;
+    V worldPos[4];
+    V center;
+    Real jacCoeffInv[4], b[4], applied[4];
+    Real fJacCoeffInv[2], fApplied[2];
+    int A, B;
+};
+
+// world inverse inertia R diag(I^-1) R^T (setupBodiesKernel,
+// broadphaseKernel.cl:189-201); static bodies have none
+M3 world_inv_inertia(const or_world* w, int i) {
+    M3 m;
+    if (w->invMass[i] == 0.f) return m;
+    const Q q = {w->quat[4 * i], w->quat[4 * i + 1], w->quat[4 * i + 2], w->quat[4 * i + 3]};
+    const V c0 = qrot(q, V(1, 0, 0)), c1 = qrot(q, V(0, 1, 0)), c2 = qrot(q, V(0, 0, 1));
+    const V d(w->invInertia[3 * i], w->invInertia[3 * i + 1], w->invInertia[3 * i + 2]);
+    const V rows[3] = {V(c0.x, c1.x, c2.x), V(c0.y, c1.y, c2.y), V(c0.z, c1.z, c2.z)};
+    for (int a = 0; a < 3; ++a) m.r[a] = V(dot(mulv(rows[a], d), rows[0]), dot(mulv(rows[a], d), rows[1]),
+                                          dot(mulv(rows[a], d), rows[2]));
+    return m;
+}
+
+// btPlaneSpace1 (solverSetup.cl:477-501)
+void plane_space1(V n, V& p, V& q) {
+    if (fabs(n.z) > 0.70710678) {
+        const Real a = n.y * n.y + n.z * n.z;
+        const Real k = 1.0 / sqrt(a);
+        p = V(0, -n.z * k, n.y * k);
+        q = V(a * k, -n.x * p.z, n.x * p.y);
+    } else {
+        const Real a = n.x * n.x + n.y * n.y;
+        const Real k = 1.0 / sqrt(a);
+        p = V(-n.y * k, n.x * k, 0);
+        q = V(-n.z * p.y, n.z * p.x, a * k);
+    }
+}
+
+// calcJacCoeff (solverSetup.cl:445-454) with setLinearAndAngular's angular
+// parts; the inverse inertias are symmetric, so a^T I = I a
+Real jac_coeff(V ang0, V ang1, Real imA, const M3& IA, Real imB, const M3& IB) {
+    return -1.0 / (imA + dot(mul(IA, ang0), ang0) + imB + dot(mul(IB, ang1), ang1));
+}
+
+// setConstraint4 (solverSetup.cl:520-609), restitution 0
+C4 set_constraint(const or_contact_r& c, V posA, V linA, V angA, Real imA, const M3& IA, V posB, V linB, V angB,
+                  Real imB, const M3& IB, Real dt) {
+    C4 d;
+    d.A = std::abs(c.bodyA);
+    d.B = std::abs(c.bodyB);
+    const V n(c.normal[0], c.normal[1], c.normal[2]);
+    const int np = (int)rval(c.normal[3]);
+    d.linear = -n;
+    for (int i = 0; i < 4; ++i) {
+        d.applied[i] = 0;
+        d.jacCoeffInv[i] = 0;
+        d.b[i] = 0;
+        d.worldPos[i] = V();
+    }
+    d.fJacCoeffInv[0] = d.fJacCoeffInv[1] = 0;
+    d.fApplied[0] = d.fApplied[1] = 0;
+    for (int ic = 0; ic < 4 && ic < np; ++ic) {
+        const V p(c.pos[ic][0], c.pos[ic][1], c.pos[ic][2]);
+        const V r0 = p - posA, r1 = p - posB;
+        const V ang0 = -cross(r0, n), ang1 = cross(r1, n);
+        d.jacCoeffInv[ic] = jac_coeff(ang0, ang1, imA, IA, imB, IB);
+        // restitution e = 0: m_b is the position term alone
+        d.b[ic] = (c.pos[ic][3] + kDrift) * kPosCoeff / dt;
+        d.worldPos[ic] = p;
+    }
+    V center;
+    for (int i = 0; i < np; ++i) center = center + V(c.pos[i][0], c.pos[i][1], c.pos[i][2]);
+    center = center * (1.0 / (Real)np);
+    V t[2];
+    plane_space1(n, t[0], t[1]);
+    for (int i = 0; i < 2; ++i) {
+        const V ang0 = -cross(center - posA, t[i]), ang1 = cross(center - posB, t[i]);
+        d.fJacCoeffInv[i] = jac_coeff(ang0, ang1, imA, IA, imB, IB);
+    }
+    d.center = center;
+    (void)linA; (void)angA; (void)linB; (void)angB;
+    return d;
+}
+
+struct BodyVel {
+    V lin, ang;
+};
+
+// solveContact (solveContact.cl:272-309), accumulated impulse clamped to [0, inf)
+void solve_contact(C4& cs, V posA, BodyVel& a, Real imA, const M3& IA, V posB, BodyVel& b, Real imB, const M3& IB) {
+    const V n = -cs.linear;  // the argument -m_linear of setLinearAndAngular
+    for (int ic = 0; ic < 4; ++ic) {
+        if (cs.jacCoeffInv[ic] == 0) continue;
+        const V r0 = cs.worldPos[ic] - posA, r1 = cs.worldPos[ic] - posB;
+        const V lin = -n, ang0 = -cross(r0, n), ang1 = cross(r1, n);
+        Real l = dot(cs.linear, a.lin) + dot(ang0, a.ang) + dot(-cs.linear, b.lin) + dot(ang1, b.ang) + cs.b[ic];
+        l = l * cs.jacCoeffInv[ic];
+        const Real prev = cs.applied[ic];
+        Real upd = prev + l;
+        if (upd < 0) upd = 0;
+        l = upd - prev;
+        cs.applied[ic] = upd;
+        a.lin = a.lin + lin * (imA * l);
+        b.lin = b.lin + (-lin) * (imB * l);
+        a.ang = a.ang + mul(IA, ang0) * l;
+        b.ang = b.ang + mul(IB, ang1) * l;
+    }
+}
+
+// solveFrictionConstraint (solveFriction.cl:297-391): limits 0.7 times the
+// sum of the contact impulses, then the angular damping about the normal
+void solve_friction(C4& cs, V posA, BodyVel& a, Real imA, const M3& IA, V posB, BodyVel& b, Real imB, const M3& IB) {
+    Real sum = 0;
+    for (int j = 0; j < 4; ++j) sum = sum + cs.applied[j];
+    const Real maxR = kFriction * sum, minR = -maxR;
+    const V n = -cs.linear;
+    V t[2];
+    plane_space1(n, t[0], t[1]);
+    const V r0 = cs.center - posA, r1 = cs.center - posB;
+    for (int i = 0; i < 2; ++i) {
+        const V lin = -t[i], ang0 = -cross(r0, t[i]), ang1 = cross(r1, t[i]);
+        Real l = dot(lin, a.lin) + dot(ang0, a.ang) + dot(-lin, b.lin) + dot(ang1, b.ang);
+        l = l * cs.fJacCoeffInv[i];
+        const Real prev = cs.fApplied[i];
+        Real upd = prev + l;
+        if (upd < minR) upd = minR;
+        if (upd > maxR) upd = maxR;
+        l = upd - prev;
+        cs.fApplied[i] = upd;
+        a.lin = a.lin + lin * (imA * l);
+        b.lin = b.lin + (-lin) * (imB * l);
+        a.ang = a.ang + mul(IA, ang0) * l;
+        b.ang = b.ang + mul(IB, ang1) * l;
+    }
+    const V ab = normalize(posB - posA), ac = normalize(cs.center - posA);
+    if (dot(ab, ac) > 0.95 || imA == 0 || imB == 0) {
+        const Real angNA = dot(n, a.ang), angNB = dot(n, b.ang);
+        a.ang = a.ang - n * (angNA * 0.1);
+        b.ang = b.ang - n * (angNB * 0.1);
+    }
+}
+
+// cell of a manifold: the xz position of its dynamic body (A unless A is
+// static), in FP32 as SetSortDataKernel computes it
+int cell_of(const or_world* w, const or_contact_r& c) {
+    const int A = std::abs(c.bodyA), B = std::abs(c.bodyB);
+    const int body = w->invMass[A] != 0.f ? A : B;
+    const float px = (float)w->pos[4 * body], pz = (float)w->pos[4 * body + 2];
+    const int xi = (int)((px - (px < 0.f ? 1.f : 0.f)) * kScale) & (kSplit - 1);
+    const int zi = (int)((pz - (pz < 0.f ? 1.f : 0.f)) * kScale) & (kSplit - 1);
+    return xi + zi * kSplit;
+}
+inline int class_of(int cell) { return (cell & 1) + 2 * ((cell / kSplit) & 1); }
+
+}  // namespace gs
+
+void stage_solve_gs(or_world* w) {
+    using namespace gs;
+    const int N = w->n;
+    const int M = (int)w->contacts.size();
+    w->count.clear();  // integration applies no Jacobi averages
+    w->gsCell.assign(M, 0);
+    w->gsBatch.assign(M, -1);
+    for (int m = 0; m < M; ++m) w->gsCell[m] = cell_of(w, w->contacts[m]);
+    // each parity class in (cell, manifold) order
+    std::vector<int> order(M);
+    for (int m = 0; m < M; ++m) order[m] = m;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        const int ka = class_of(w->gsCell[a]) * 256 + w->gsCell[a];
+        const int kb = class_of(w->gsCell[b]) * 256 + w->gsCell[b];
+        return ka < kb;
+    });
+    // greedy colouring per class (sortConstraintByBatch's pass, exact bodies)
+    int nb[4] = {0, 0, 0, 0};
+    std::vector<int> stamp(N, -1);
+    for (int cls = 0; cls < 4; ++cls) {
+        std::vector<int> rem;
+        for (int m : order)
+            if (class_of(w->gsCell[m]) == cls) rem.push_back(m);
+        int b = 0;
+        while (!rem.empty()) {
+            std::vector<int> next;
+            for (int m : rem) {
+                const int A = std::abs(w->contacts[m].bodyA), B = std::abs(w->contacts[m].bodyB);
+                const bool dA = w->invMass[A] != 0.f, dB = w->invMass[B] != 0.f;
+                if ((!dA || stamp[A] != b) && (!dB || stamp[B] != b)) {
+                    w->gsBatch[m] = b;
+                    if (dA) stamp[A] = b;
+                    if (dB) stamp[B] = b;
+                } else {
+                    next.push_back(m);
+                }
+            }
+            rem.swap(next);
+            ++b;
+            // stamps of this pass must not alias the next class' batch 0
+            if (rem.empty()) std::fill(stamp.begin(), stamp.end(), -1);
+        }
+        nb[cls] = b;
+    }
+    if (M == 0) return;
+    // constraints, bodies' state at the solve
+    std::vector<M3> Iw(N);
+    for (int i = 0; i < N; ++i) Iw[i] = world_inv_inertia(w, i);
+    auto posv = [&](int i) { return V(w->pos[4 * i], w->pos[4 * i + 1], w->pos[4 * i + 2]); };
+    std::vector<BodyVel> vel(N);
+    for (int i = 0; i < N; ++i) {
+        if (w->invMass[i] == 0.f) continue;  // static bodies move with zero velocity
+        vel[i].lin = V(w->lin[4 * i], w->lin[4 * i + 1], w->lin[4 * i + 2]);
+        vel[i].ang = V(w->ang[4 * i], w->ang[4 * i + 1], w->ang[4 * i + 2]);
+    }
+    std::vector<C4> cs(M);
+    for (int m = 0; m < M; ++m) {
+        const or_contact_r& c = w->contacts[m];
+        const int A = std::abs(c.bodyA), B = std::abs(c.bodyB);
+        cs[m] = set_constraint(c, posv(A), vel[A].lin, vel[A].ang, (Real)w->invMass[A], Iw[A], posv(B), vel[B].lin,
+                               vel[B].ang, (Real)w->invMass[B], Iw[B], (Real)w->cfg.dt);
+    }
+    // (class, batch) lists in class order
+    std::vector<std::vector<int>> lists;
+    for (int cls = 0; cls < 4; ++cls)
+        for (int b = 0; b < nb[cls]; ++b) {
+            std::vector<int> l;
+            for (int m : order)
+                if (class_of(w->gsCell[m]) == cls && w->gsBatch[m] == b) l.push_back(m);
+            lists.push_back(l);
+        }
+    for (int phase = 0; phase < 2; ++phase)
+        for (int it = 0; it < kIterations; ++it)
+            for (const std::vector<int>& l : lists)
+                for (int m : l) {
+                    C4& c = cs[m];
+                    const int A = c.A, B = c.B;
+                    const Real imA = w->invMass[A], imB = w->invMass[B];
+                    BodyVel a = vel[A], b = vel[B];
+                    if (phase == 0) solve_contact(c, posv(A), a, imA, Iw[A], posv(B), b, imB, Iw[B]);
+                    else solve_friction(c, posv(A), a, imA, Iw[A], posv(B), b, imB, Iw[B]);
+                    // a static body's velocity is written as zero
+                    vel[A] = imA != 0 ? a : BodyVel();
+                    vel[B] = imB != 0 ? b : BodyVel();
+                }
+    w->gsApplied.assign(6 * (size_t)M, 0.0);
+    for (int m = 0; m < M; ++m) {
+        for (int k = 0; k < 4; ++k) w->gsApplied[6 * m + k] = rval(cs[m].applied[k]);
+        for (int k = 0; k < 2; ++k) w->gsApplied[6 * m + 4 + k] = rval(cs[m].fApplied[k]);
+    }
+    for (int i = 0; i < N; ++i) {
+        if (w->invMass[i] == 0.f) continue;
+        w->lin[4 * i] = vel[i].lin.x; w->lin[4 * i + 1] = vel[i].lin.y; w->lin[4 * i + 2] = vel[i].lin.z;
+        w->ang[4 * i] = vel[i].ang.x; w->ang[4 * i + 1] = vel[i].ang.y; w->ang[4 * i + 2] = vel[i].ang.z;
+    }
+}
+
 void stage_solve(or_world* w) {
+    if (w->gs) {
+        stage_solve_gs(w);
+        return;
+    }
     const int N = w->n;
     const int M = (int)w->contacts.size();
     const Real dt = w->cfg.dt;
@@ -1183,6 +1476,53 @@ int or_real_kind() {
 void or_stage_aabbs(or_world* w) { stage_aabbs(w); }
 // 0 = uniform grid (default), 1 = sweep and prune
 void or_set_broadphase(or_world* w, int kind) { w->sap = kind == 1 ? 1 : 0; }
+// solver: 0 = Jacobi with velocity averaging, 1 = batched Gauss-Seidel
+void or_set_solver(or_world* w, int kind) { w->gs = kind == 1 ? 1 : 0; }
+// per manifold (in contact order) its cell and batch from the last
+// batched Gauss-Seidel solve; returns the manifold count
+int or_gs_batches(or_world* w, int* cellBatch2, int max) {
+    const int n = (int)w->gsBatch.size();
+    for (int m = 0; m < n && m < max; ++m) {
+        cellBatch2[2 * m] = w->gsCell[m];
+        cellBatch2[2 * m + 1] = w->gsBatch[m];
+    }
+    return n;
+}
+// per manifold the accumulated impulses of the last batched Gauss-Seidel
+// solve: normal [4], friction [2]; returns the manifold count
+int or_gs_applied(or_world* w, double* out6, int max) {
+    const int n = (int)w->gsApplied.size() / 6;
+    for (int m = 0; m < n && m < max; ++m)
+        for (int k = 0; k < 6; ++k) out6[6 * m + k] = w->gsApplied[6 * m + k];
+    return n;
+}
+// setConstraint4 on one manifold given the bodies' state (for pinning the
+// restatement against recorded constraints): out = jacCoeffInv[4], b[4],
+// center[3], fJacCoeffInv[2]
+void or_gs_constraint(const double* pos4x4, const double* normal4, const double* posA3, const double* posB3,
+                      double invMassA, double invMassB, const double* invInertiaA9, const double* invInertiaB9,
+                      double dt, double* out13) {
+    or_contact_r c = {};
+    for (int i = 0; i < 4; ++i)
+        for (int k = 0; k < 4; ++k) c.pos[i][k] = pos4x4[4 * i + k];
+    for (int k = 0; k < 4; ++k) c.normal[k] = normal4[k];
+    gs::M3 IA, IB;
+    for (int r = 0; r < 3; ++r) {
+        IA.r[r] = V(invInertiaA9[3 * r], invInertiaA9[3 * r + 1], invInertiaA9[3 * r + 2]);
+        IB.r[r] = V(invInertiaB9[3 * r], invInertiaB9[3 * r + 1], invInertiaB9[3 * r + 2]);
+    }
+    const gs::C4 d = gs::set_constraint(c, V(posA3[0], posA3[1], posA3[2]), V(), V(), invMassA, IA,
+                                        V(posB3[0], posB3[1], posB3[2]), V(), V(), invMassB, IB, dt);
+    for (int i = 0; i < 4; ++i) {
+        out13[i] = rval(d.jacCoeffInv[i]);
+        out13[4 + i] = rval(d.b[i]);
+    }
+    out13[8] = rval(d.center.x);
+    out13[9] = rval(d.center.y);
+    out13[10] = rval(d.center.z);
+    out13[11] = rval(d.fJacCoeffInv[0]);
+    out13[12] = rval(d.fJacCoeffInv[1]);
+}
 // computePairsKernel restatement on caller-sorted records (8 floats each):
 // writes up to max pairs, returns the full count
 int or_sap_sorted_pairs(const float* sorted8, int n, int axis, int* pairs2, int max) {

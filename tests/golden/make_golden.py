@@ -30,6 +30,20 @@ sap_kernel_args.npz
     count buffers, numObjects, axis and maxPairs. The fixture keeps the
     sorted AABBs and the scalars (the output buffers were not yet written).
 
+gs_solve_args.npz
+    The reference's recorded arguments of its batched Gauss-Seidel solve
+    kernel: testdata/m_batchSolveKernel.7z holds m_batchSolveKernel.bin, the
+    btLauncherCL dump of one BatchSolveKernelContact launch
+    (ST/solveContact.cl:400-476; ST/Solver.cpp:561-640 sets its arguments):
+    the Body array (96-byte records of that revision: position, orientation,
+    linear and angular velocity, then inverse mass at float 18), the Shape
+    array (world and local inverse inertia), the Constraint4 array (176
+    bytes, ST/AdlConstraint4.h:23-47) as ContactToConstraintKernel
+    (ST/solverSetup.cl:614-655) and the batching kernel left it, and the
+    per-cell counts and offsets of the 16 x 16 grid; maxBatch, the parity
+    class and N_SPLIT. The fixture keeps the used constraints, the bodies'
+    positions, inverse masses and world inverse inertias, and the grid.
+
 hull_pins.npz
     btConvexUtility::initializePolyhedralFeatures
     (P1/btConvexUtility.cpp:31-270) on every distinct shape of the plain and
@@ -310,6 +324,31 @@ def make_sap():
     return rec
 
 
+def make_gs():
+    files = read_7z(os.path.join(REFERENCE, "testdata", "m_batchSolveKernel.7z"))
+    args, work = launcher_args(files["m_batchSolveKernel.bin"])
+    scalar = lambda k: struct.unpack("<i", args[k][1][:4])[0]
+    gN = np.frombuffer(args[3][1], np.int32).copy()
+    gO = np.frombuffer(args[4][1], np.int32).copy()
+    n = int(gN.sum())
+    cf = np.frombuffer(args[2][1], np.float32)[:44 * n].reshape(n, 44)
+    ci = np.frombuffer(args[2][1], np.int32)[:44 * n].reshape(n, 44)
+    bodies = np.frombuffer(args[0][1], np.float32).reshape(-1, 24)
+    shapes = np.frombuffer(args[1][1], np.float32).reshape(-1, 24)
+    used = np.unique(ci[:, 40:42])
+    rec = dict(cellCount=gN, cellOffset=gO, numWorkItems=np.int32(work), maxBatch=np.int32(scalar(6)),
+               classIdx=np.int32(scalar(7)), nSplit=np.int32(scalar(8)),
+               linear=cf[:, 0:4].copy(), worldPos=cf[:, 4:20].reshape(n, 4, 4).copy(), center=cf[:, 20:24].copy(),
+               jacCoeffInv=cf[:, 24:28].copy(), b=cf[:, 28:32].copy(), applied=cf[:, 32:36].copy(),
+               fJacCoeffInv=cf[:, 36:38].copy(), fApplied=cf[:, 38:40].copy(), bodyAB=ci[:, 40:42].copy(),
+               batchIdx=ci[:, 42].copy(), bodies=used.astype(np.int32),
+               bodyPos=bodies[used, 0:4].copy(), bodyLinVel=bodies[used, 8:12].copy(),
+               bodyAngVel=bodies[used, 12:16].copy(), bodyInvMass=bodies[used, 18].copy(),
+               bodyInvInertiaWorld=shapes[used, 0:12].reshape(-1, 3, 4)[:, :, :3].copy())
+    np.savez_compressed(os.path.join(HERE, "gs_solve_args.npz"), **rec)
+    return rec
+
+
 def make_hulls():
     _import_tests()
     import test_cpu_pins as pins
@@ -338,3 +377,5 @@ if __name__ == "__main__":
     print("hull_pins.npz:", make_hulls(), "shapes")
     r = make_sap()
     print("sap_kernel_args.npz:", int(r["numObjects"]), "sorted AABBs")
+    r = make_gs()
+    print("gs_solve_args.npz:", len(r["batchIdx"]), "constraints")

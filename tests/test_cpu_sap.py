@@ -85,6 +85,7 @@ def test_sap_flag_rules(host_ctx):
     with pytest.raises(b3.B3Error):
         b3.PhysicsWorld(host_ctx, scenes.world_config(sc, flags=1))
     with pytest.raises(b3.B3Error):
-        b3.PhysicsWorld(host_ctx, scenes.world_config(scenes.random_pile(5, n=20), flags=2))
-    w = b3.PhysicsWorld(host_ctx, scenes.world_config(scenes.random_pile(5, n=20), flags=1))
-    w.close()
+        b3.PhysicsWorld(host_ctx, scenes.world_config(scenes.random_pile(5, n=20), flags=4))
+    for flags in (1, 2, 3):  # SAP, batched Gauss-Seidel, both
+        w = b3.PhysicsWorld(host_ctx, scenes.world_config(scenes.random_pile(5, n=20), flags=flags))
+        w.close()
