@@ -216,7 +216,9 @@ def run_b3(args, world_size, local_rank):
         from experiments_b200 import sharding
         sc, _ = sharding.shard_scene(full, int(os.environ.get("RANK", "0")), world_size)
         sharded = True
-    bp = {"flags": 1} if getattr(args, "sap", False) else {}  # sweep-and-prune broadphase
+    # world flags: 1 = sweep-and-prune broadphase, 2 = batched Gauss-Seidel solver
+    flags = (1 if getattr(args, "sap", False) else 0) | (2 if getattr(args, "solver", "jacobi") == "gs" else 0)
+    bp = {"flags": flags} if flags else {}
     w = scenes.build_world(ctx, sc, useGraph=1, **bp)
     st = torch.cuda.current_stream()
     flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > 126 MB L2
@@ -491,6 +493,9 @@ def main():
     ap.add_argument("--scale", action="store_true", help="also run the 1,048,576-body plain and adjoint steps")
     ap.add_argument("--sap", action="store_true",
                     help="sweep-and-prune broadphase (pipeline2's default) in place of the grid; single-world workloads")
+    ap.add_argument("--solver", default="jacobi", choices=["jacobi", "gs"],
+                    help="jacobi: pipeline2's Jacobi solver (default); gs: the reference GPU solver, batched "
+                         "Gauss-Seidel (4 contact + 4 friction iterations)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world_size = int(os.environ.get("WORLD_SIZE", "1"))
@@ -501,6 +506,10 @@ def main():
         if args.workload in ("c3", "c3s"):
             ap.error("--sap takes a single-world workload (c1, c2, c2s, c5)")
         cfg["workload"] += ", sweep-and-prune broadphase"
+    if args.solver == "gs":
+        cfg["workload"] += ", batched Gauss-Seidel solver"
+        # the CPU port times the Jacobi pipeline; no baseline for this form
+        args.no_cpu_baseline = True
 
     if args.impl == "reference":
         if rank != 0:

@@ -189,7 +189,8 @@ struct b3World_t {
     int pairThreads = 128;     // pair-search CTA size
     int solverThreads = 256;   // Jacobi CTA size
     int solverOccCap = 4;      // Jacobi persistent blocks per SM (at most)
-    int solverMode = 0;        // Jacobi: 0 = grid barriers, 1 = one block per world (batched)
+    int solverMode = 0;        // Jacobi: 0 = grid barriers, 1 = one block per world (batched);
+                               // batched Gauss-Seidel: grid width 0 = manifolds / 8, 1 = manifolds / 64
     int solverGather = 0;      // Jacobi body averages: 0 = one copy at a time, 1 = four loads in flight
     int tunedTrials = 0;       // configurations the autotuner timed
     int npSmemAttr = 0;        // dynamic shared memory attribute set on the narrowphase kernels

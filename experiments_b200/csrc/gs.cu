@@ -567,11 +567,13 @@ int launch_gs_solver(b3World_t* w, cudaStream_t st) {
     SV.err = d.scalars + S_ERR;
     SV.counters = d.counters;
     {
-        // batches are a fraction of the manifolds: a smaller grid keeps
-        // each barrier cheap
-        const int grid = cooperative_grid((const void*)k_gs_solve, 256, w->ctx->numSMs, estM / 8);
+        // a batch holds a fraction of the manifolds, and fewer blocks make
+        // each grid barrier cheaper: the autotuner picks the width
+        // (solverMode 0: manifolds / 8 threads, 1: manifolds / 64)
+        const void* kg = (const void*)k_gs_solve;
+        const int grid = cooperative_grid(kg, 256, w->ctx->numSMs, estM / (w->solverMode == 1 ? 64 : 8));
         void* args[] = {&SV};
-        B3_TRY(launch_cooperative((const void*)k_gs_solve, grid, 256, args, st));
+        B3_TRY(launch_cooperative(kg, grid, 256, args, st));
     }
     return B3_OK;
 }

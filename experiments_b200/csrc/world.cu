@@ -1091,7 +1091,13 @@ extern "C" int b3_autotune(b3World w, int trialSteps, void* stream) {
     Knob knobs[] = {{&w->npWarpsPerBlock, {1, 2, 4}}, {&w->solverThreads, {64, 128, 256}},
                     {&w->solverOccCap, {1, 2, 4}},      {&w->solverGather, {0, 1, 0}},
                     {&w->solverMode, {0, 1, 0}}};
-    const int numKnobs = w->cfg.numWorlds > 1 ? 5 : 4;  // per-world solver only for batched worlds
+    int numKnobs = w->cfg.numWorlds > 1 ? 5 : 4;  // per-world solver only for batched worlds
+    if (w->gs) {
+        // the Jacobi launch shapes do not apply: narrowphase CTA size, then
+        // the Gauss-Seidel grid width
+        knobs[1] = knobs[4];
+        numKnobs = 2;
+    }
     do {
         for (int k = 0; k < 4 && rc == B3_OK; ++k)
             if (cudaMemcpyAsync(save + k * N, bufs[k], N * sizeof(float4), cudaMemcpyDeviceToDevice, st) !=

@@ -8,7 +8,7 @@ accumulated impulses within 1e-4 of the restatement's, relative to the
 largest. The device colouring is valid and greedy on a workload scene, and
 graph replays are bitwise deterministic (the counting sort places each
 batch's constraints in any order; batches share no dynamic body, so the
-result cannot depend on it)."""
+result cannot depend on it), whatever the width of the cooperative grid."""
 import numpy as np
 import pytest
 
@@ -136,6 +136,25 @@ def test_graph_replay_is_bitwise_deterministic(ctx):
         w, _ = make_pair(ctx, sc, flags=GS)
         w.stepSimulation(8)
         states.append(w.read_state())
+        w.close()
+    for a, b in zip(*states):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+@pytest.mark.parametrize("name", ["pile_hulls", "c2_small"])
+def test_grid_widths_agree_bitwise(ctx, scene_cache, name):
+    """The two cooperative grid widths of the solve (solverMode 0 and 1) run
+    the same batches in the same order: the same bits."""
+    sc = scene_cache[name]
+    states = []
+    for mode in (0, 1):
+        w, _ = make_pair(ctx, sc, flags=GS)
+        t = w.tuning()
+        t[6] = mode
+        w.set_tuning(t)
+        w.stepSimulation(6)
+        states.append(w.read_state())
+        assert w.counters()["timeouts"] == 0
         w.close()
     for a, b in zip(*states):
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
