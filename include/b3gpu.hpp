@@ -233,6 +233,32 @@ private:
     World& w_;
 };
 
+/* Solver (ST/Solver.h:104-158), the reference's batched Gauss-Seidel GPU
+ * solver, over a world created with B3_WORLD_BATCHED_GS_SOLVER:
+ * solveContactConstraint runs batching, convertToConstraints and the 4 + 4
+ * iterations (the world's solve stage); getBatches / getConstraints read
+ * each manifold's (cell, batch) and Constraint4 after it. */
+class BatchedSolver {
+public:
+    explicit BatchedSolver(World& w) : w_(w) {}
+    void solveContactConstraint(void* stream = nullptr) {
+        check(b3_solver_solve_batched_gs(w_.handle(), stream), "solveContactConstraint");
+    }
+    int getBatches(int32_t* cellBatch2, int max, void* stream = nullptr) const {
+        int n = 0;
+        check(b3_get_gs_batches(w_.handle(), cellBatch2, max, &n, stream), "getBatches");
+        return n;
+    }
+    int getConstraints(b3Constraint4* out, int max, void* stream = nullptr) const {
+        int n = 0;
+        check(b3_get_gs_constraints(w_.handle(), out, max, &n, stream), "getConstraints");
+        return n;
+    }
+
+private:
+    World& w_;
+};
+
 /* btGpuNarrowphaseAndSolver over a world: contacts, Jacobi solve, integrate. */
 class GpuNarrowphaseAndSolver {
 public:

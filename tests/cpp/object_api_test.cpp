@@ -160,6 +160,36 @@ static int gpu_mode() {
     float sapMinY = 1e9f;
     for (size_t i = 1; i < sb.size(); ++i) sapMinY = std::min(sapMinY, sb[i].pos[1]);
     EXPECT(sapMinY > 0.4f);
+
+    // --- the reference's GPU solver (batched Gauss-Seidel) ---
+    b3WorldConfig gsCfg = stack_config();
+    gsCfg.flags = B3_WORLD_BATCHED_GS_SOLVER;
+    b3::World wg(ctx, gsCfg);
+    build_stack(wg);
+    b3::GpuNarrowphaseAndSolver npg(wg);
+    b3::BatchedSolver gs(wg);
+    npg.writeAllBodiesToGpu();
+    wg.computeAabbs();
+    b3::GridBroadphase bpg(wg);
+    bpg.calculateOverlappingPairs();
+    npg.computeContacts();
+    gs.solveContactConstraint();
+    npg.integrate();
+    const int nm = gs.getConstraints(nullptr, 0);
+    EXPECT(nm >= 16);
+    std::vector<b3Constraint4> cs(nm);
+    std::vector<int32_t> cb(2 * (size_t)nm);
+    EXPECT(gs.getConstraints(cs.data(), nm) == nm && gs.getBatches(cb.data(), nm) == nm);
+    for (int m = 0; m < nm; ++m) {
+        EXPECT(cs[m].batchIdx == cb[2 * m + 1] && cs[m].batchIdx >= 0);
+        EXPECT(cs[m].jacCoeffInv[0] < 0.f && cs[m].linear[3] == 0.7f);
+    }
+    wg.stepSimulation(120);
+    std::vector<b3Body> gb = wg.readBodies();
+    float gsMinY = 1e9f;
+    for (size_t i = 1; i < gb.size(); ++i) gsMinY = std::min(gsMinY, gb[i].pos[1]);
+    EXPECT(gsMinY > 0.4f);
+    EXPECT(wg.counters().timeouts == 0);
     return 0;
 }
 
