@@ -73,7 +73,9 @@ void free_all(b3::DevBuffers& d) {
                     d.incKeys, d.incVals, d.incKeysAlt, d.incValsAlt, d.bodyIncStart,
                     d.bodyIncEnd, d.rows, d.manifoldHdr, d.incLin, d.incAng, d.avgLin, d.avgAng,
                     d.scalars, d.counters, d.sortScratch, d.incSortScratch, d.scanScratch,
-                    d.worldStats, d.worldMStart, d.worldMEnd};
+                    d.worldStats, d.worldMStart, d.worldMEnd, d.gsCell, d.gsSlotBatch,
+                    d.gsSlotOfManifold, d.gsMinRank, d.gsTaken, d.gsBatchCount, d.gsGroupCount, d.gsGroupFill,
+                    d.gsGroupOffset, d.gsInertia};  // gsConstraints shares the row storage
     for (void* p : ptrs)
         if (p) cudaFree(p);
     d = b3::DevBuffers();
