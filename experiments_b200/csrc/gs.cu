@@ -378,21 +378,56 @@ __device__ __forceinline__ float3 ldv(const float4* p) {
     return make_float3(v.x, v.y, v.z);
 }
 
-// one constraint, contact (phase 0) or friction (phase 1); a static
+// One constraint with the data that does not change during the solve:
+// its Constraint4 record and its bodies' positions, inverse masses and world
+// inverse inertias. The solve fetches the next batch's before each barrier,
+// so that after it only the velocities are still to be loaded.
+struct Pending {
+    int q;  // constraint index, -1 for none
+    union {
+        b3Constraint4 c;
+        float4 raw[11];
+    };
+    int A, B;
+    float imA, imB;
+    float3 posA, posB;
+    M3 IA, IB;
+};
+static_assert(sizeof(b3Constraint4) == 11 * sizeof(float4), "Constraint4 is 176 bytes");
+
+__device__ __forceinline__ void fetch(const SolveView& V, int q, Pending& P) {
+    P.q = q;
+    if (q < 0) return;
+    const float4* src = reinterpret_cast<const float4*>(V.cs + q);
+#pragma unroll
+    for (int k = 0; k < 11; ++k) P.raw[k] = src[k];
+    P.A = (int)P.c.bodyA;
+    P.B = (int)P.c.bodyB;
+    P.imA = V.invMass[P.A];
+    P.imB = V.invMass[P.B];
+    P.posA = f3(V.pos[P.A]);
+    P.posB = f3(V.pos[P.B]);
+    P.IA = load_iw(V.Iw, P.A);
+    P.IB = load_iw(V.Iw, P.B);
+}
+
+// the constraint, contact (phase 0) or friction (phase 1); a static
 // body's velocity is read and written as zero
-__device__ void solve_one(const SolveView& V, int q, int phase) {
-    b3Constraint4& c = V.cs[q];
-    const int A = (int)c.bodyA, B = (int)c.bodyB;
-    const float imA = V.invMass[A], imB = V.invMass[B];
+__device__ void solve_one(const SolveView& V, Pending& P, int phase) {
+    b3Constraint4& c = P.c;
+    const int A = P.A, B = P.B;
+    const float imA = P.imA, imB = P.imB;
     const bool dA = imA != 0.f, dB = imB != 0.f;
     float3 vA = dA ? ldv(&V.linVel[A]) : make_float3(0.f, 0.f, 0.f);
     float3 wA = dA ? ldv(&V.angVel[A]) : make_float3(0.f, 0.f, 0.f);
     float3 vB = dB ? ldv(&V.linVel[B]) : make_float3(0.f, 0.f, 0.f);
     float3 wB = dB ? ldv(&V.angVel[B]) : make_float3(0.f, 0.f, 0.f);
-    const float3 posA = f3(V.pos[A]), posB = f3(V.pos[B]);
-    const M3 IA = load_iw(V.Iw, A), IB = load_iw(V.Iw, B);
+    const float3 posA = P.posA, posB = P.posB;
+    const M3& IA = P.IA;
+    const M3& IB = P.IB;
     const float3 lin = make_float3(c.linear[0], c.linear[1], c.linear[2]);
     const float3 n = -lin;
+    float4* dst = reinterpret_cast<float4*>(V.cs + P.q);
     if (phase == 0) {
         // solveContact (ST/solveContact.cl:272-309): impulses clamped to [0, inf)
 #pragma unroll
@@ -411,6 +446,7 @@ __device__ void solve_one(const SolveView& V, int q, int phase) {
             wA += mul(IA, ang0) * l;
             wB += mul(IB, ang1) * l;
         }
+        dst[8] = P.raw[8];  // appliedRambdaDt
     } else {
         // solveFrictionConstraint (ST/solveFriction.cl:297-391)
         if (c.fJacCoeffInv[0] == 0.f && c.fJacCoeffInv[1] == 0.f) return;
@@ -441,11 +477,23 @@ __device__ void solve_one(const SolveView& V, int q, int phase) {
             wA -= n * (angNA * 0.1f);
             wB -= n * (angNB * 0.1f);
         }
+        dst[9] = P.raw[9];  // fJacCoeffInv, fAppliedRambdaDt
     }
     __stcg(&V.linVel[A], dA ? make_float4(vA.x, vA.y, vA.z, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f));
     __stcg(&V.angVel[A], dA ? make_float4(wA.x, wA.y, wA.z, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f));
     __stcg(&V.linVel[B], dB ? make_float4(vB.x, vB.y, vB.z, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f));
     __stcg(&V.angVel[B], dB ? make_float4(wB.x, wB.y, wB.z, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f));
+}
+
+// (class, batch) group of step j of an iteration (classes in order, their
+// batches in order)
+__device__ __forceinline__ int group_of(int j, const int nb[4], int maxBatch) {
+    int cls = 0;
+    while (cls < 3 && j >= nb[cls]) {
+        j -= nb[cls];
+        ++cls;
+    }
+    return cls * maxBatch + j;
 }
 
 __global__ void __launch_bounds__(256) k_gs_solve(SolveView V) {
@@ -454,15 +502,31 @@ __global__ void __launch_bounds__(256) k_gs_solve(SolveView V) {
     int nb[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) nb[c] = min(__ldcg(&V.batchCount[c]), V.maxBatch);
-    for (int phase = 0; phase < 2; ++phase)
-        for (int it = 0; it < kIterations; ++it)
-            for (int cls = 0; cls < 4; ++cls)
-                for (int b = 0; b < nb[cls]; ++b) {
-                    const int g = cls * V.maxBatch + b;
-                    const int q0 = (int)V.groupOffset[g], q1 = (int)V.groupOffset[g + 1];
-                    for (int q = q0 + tid; q < q1; q += stride) solve_one(V, q, phase);
-                    if (!grid_barrier(V.bar, V.bar + 1, gridDim.x, V.err, V.counters)) return;
-                }
+    const int G = nb[0] + nb[1] + nb[2] + nb[3];  // batch steps per iteration
+    const int steps = 2 * kIterations * G;        // contact iterations, then friction
+    if (steps == 0) return;
+    int g = group_of(0, nb, V.maxBatch);
+    int q0 = (int)V.groupOffset[g], q1 = (int)V.groupOffset[g + 1];
+    Pending P;
+    fetch(V, q0 + tid < q1 ? q0 + tid : -1, P);
+    for (int k = 0; k < steps; ++k) {
+        const int phase = k / (kIterations * G);
+        if (P.q >= 0) solve_one(V, P, phase);
+        for (int q = q0 + tid + stride; q < q1; q += stride) {
+            Pending T;
+            fetch(V, q, T);
+            solve_one(V, T, phase);
+        }
+        // the next batch's records and static body data: no thread of this
+        // batch writes them (a record belongs to its own thread)
+        if (k + 1 < steps) {
+            g = group_of((k + 1) % G, nb, V.maxBatch);
+            q0 = (int)V.groupOffset[g];
+            q1 = (int)V.groupOffset[g + 1];
+            fetch(V, q0 + tid < q1 ? q0 + tid : -1, P);
+        }
+        if (!grid_barrier(V.bar, V.bar + 1, gridDim.x, V.err, V.counters)) return;
+    }
 }
 
 int cooperative_grid(const void* kern, int threads, int numSMs, long long work) {
