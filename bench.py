@@ -56,9 +56,9 @@ WORKLOADS = {
     "c5": "plain step, 1,048,576 unit cubes, 128x64x128 lattice, 10 Jacobi iterations",
 }
 STAGES = ["aabb_hash", "sort_cells", "find_pairs", "narrowphase", "manifolds", "solve", "integrate"]
-# DRAM bytes per pair of the three narrowphase kernels (read + write) from the ncu capture in
+# DRAM bytes per pair of the four narrowphase kernels (read + write) from the ncu capture in
 # profiles/kernels_c2s_plain_step.md, scaled by the timed workload's pair count
-NARROWPHASE_DRAM_BYTES_PER_PAIR = 4.604e6 / 36735
+NARROWPHASE_DRAM_BYTES_PER_PAIR = 4.352e6 / 36735
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 148 SMs x 128 FP32 lanes x FMA x 1.965 GHz
 
 
