@@ -594,7 +594,11 @@ int launch_gs_solver(b3World_t* w, cudaStream_t st) {
     CV.maxBatch = maxBatch;
     const long long estM = std::min<long long>((long long)cap, 3LL * N);
     {
-        const int grid = cooperative_grid((const void*)k_gs_colour, 256, w->ctx->numSMs, estM);
+        // the narrow width of the solve (solverMode 1) also narrows the
+        // colouring: each round passes over every slot, but costs three
+        // barriers
+        const int grid = cooperative_grid((const void*)k_gs_colour, 256, w->ctx->numSMs,
+                                          w->solverMode == 1 ? estM / 8 : estM);
         void* args[] = {&CV};
         B3_TRY(launch_cooperative((const void*)k_gs_colour, grid, 256, args, st));
     }
