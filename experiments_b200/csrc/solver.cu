@@ -206,37 +206,53 @@ __global__ void k_setup_rows(b3::BodiesDev Bd, SolverView V, const int* __restri
 // ---------------------------------------------------------------------------
 // Persistent Jacobi kernel
 // ---------------------------------------------------------------------------
-// One phase for every manifold: start each copy from its body's average of
+constexpr int kJacobiHeads = 4;         // manifolds per thread whose headers stay in shared memory
+constexpr int kJacobiMaxThreads = 256;  // k_jacobi's largest CTA
+
+// What a manifold's solve reads that no phase changes: its header (bodies,
+// row count, dynamic flags) and its bodies' incidence ranges.
+struct MHead {
+    int A, B, nRows, dyn;
+    uint32_t sA, eA, sB, eB;
+};
+
+__device__ __forceinline__ void load_head(const SolverView& V, int m, MHead& H) {
+    const float4 h0 = R(V, 0, m);
+    H.nRows = __float_as_int(h0.z);
+    H.A = __float_as_int(h0.x);
+    H.B = __float_as_int(h0.y);
+    H.dyn = __float_as_int(h0.w);
+    H.sA = H.eA = H.sB = H.eB = 0u;
+    if (H.dyn & 1) {
+        H.sA = V.incStart[H.A];
+        H.eA = V.incEnd[H.A];
+    }
+    if (H.dyn & 2) {
+        H.sB = V.incStart[H.B];
+        H.eB = V.incEnd[H.B];
+    }
+}
+
+// One phase for one manifold: start each copy from its body's average of
 // the previous phase (zero in the first phase), solve the manifold's normal
 // or friction rows in order, store both copies in buffer outBuf. A copy of a
 // manifold without rows keeps the average, as in the reference.
 template <bool TAPE, bool GATHER4>
-__device__ __forceinline__ void solve_manifold(const SolverView& V, int m, bool friction, bool first, int inBuf,
-                                               int outBuf, const b3::JacobiTape& T, int phase) {
+__device__ __forceinline__ void solve_manifold_h(const SolverView& V, int m, const MHead& H, bool friction,
+                                                 bool first, int inBuf, int outBuf, const b3::JacobiTape& T,
+                                                 int phase) {
     {
-        const float4 h0 = R(V, 0, m);
-        const int nRows = __float_as_int(h0.z);
-        const int A = __float_as_int(h0.x), B = __float_as_int(h0.y);
-        const int dyn = __float_as_int(h0.w);
+        const int nRows = H.nRows;
+        const int dyn = H.dyn;
         float3 dvA = make_float3(0.f, 0.f, 0.f), dwA = dvA, dvB = dvA, dwB = dvA;
         if (!first) {
             if (GATHER4) {
-                // both bodies' incidence ranges in one round of loads, then
-                // their copies four at a time (same sums as body_average)
-                uint32_t sA = 0, eA = 0, sB = 0, eB = 0;
-                if (dyn & 1) {
-                    sA = V.incStart[A];
-                    eA = V.incEnd[A];
-                }
-                if (dyn & 2) {
-                    sB = V.incStart[B];
-                    eB = V.incEnd[B];
-                }
-                if (dyn & 1) body_average_range(V, sA, eA, inBuf, dvA, dwA);
-                if (dyn & 2) body_average_range(V, sB, eB, inBuf, dvB, dwB);
+                // the copies four at a time (same sums as body_average)
+                if (dyn & 1) body_average_range(V, H.sA, H.eA, inBuf, dvA, dwA);
+                if (dyn & 2) body_average_range(V, H.sB, H.eB, inBuf, dvB, dwB);
             } else {
-                if (dyn & 1) body_average(V, A, inBuf, dvA, dwA);
-                if (dyn & 2) body_average(V, B, inBuf, dvB, dwB);
+                if (dyn & 1) body_average_se(V, H.sA, H.eA, inBuf, dvA, dwA);
+                if (dyn & 2) body_average_se(V, H.sB, H.eB, inBuf, dvB, dwB);
             }
         }
         float lam[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -305,6 +321,14 @@ __device__ __forceinline__ void solve_manifold(const SolverView& V, int m, bool 
 }
 
 template <bool TAPE, bool GATHER4>
+__device__ __forceinline__ void solve_manifold(const SolverView& V, int m, bool friction, bool first, int inBuf,
+                                               int outBuf, const b3::JacobiTape& T, int phase) {
+    MHead H;
+    load_head(V, m, H);
+    solve_manifold_h<TAPE, GATHER4>(V, m, H, friction, first, inBuf, outBuf, T, phase);
+}
+
+template <bool TAPE, bool GATHER4>
 __device__ void manifold_phase(const SolverView& V, int M, bool friction, bool first, int inBuf, int outBuf,
                                const b3::JacobiTape& T, int phase) {
     for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x)
@@ -325,9 +349,25 @@ k_jacobi(SolverView V, int iterations, uint32_t* bar, int32_t* err, b3Counters* 
     const int M = *V.numManifolds;
     const uint32_t nb = gridDim.x;
     const int phases = 2 * iterations;
+    const int m0 = blockIdx.x * blockDim.x + threadIdx.x;
+    const int stride = gridDim.x * blockDim.x;
+    // the headers and incidence ranges of this thread's first kJacobiHeads
+    // manifolds stay in shared memory for every phase: after each barrier
+    // only the copy ids and the copies remain to be loaded from L2
+    __shared__ MHead heads[kJacobiHeads][kJacobiMaxThreads];
+    for (int k = 0; k < kJacobiHeads; ++k)
+        if (m0 + k * stride < M) load_head(V, m0 + k * stride, heads[k][threadIdx.x]);
     for (int p = 0; p < phases; ++p) {
         if (p > 0 && !grid_barrier(bar, bar + 1, nb, err, counters)) return;
-        manifold_phase<TAPE, GATHER4>(V, M, (p & 1) != 0, p == 0, (p - 1) & 1, p & 1, T, p);
+        const bool friction = (p & 1) != 0, first = p == 0;
+        const int inBuf = (p - 1) & 1, outBuf = p & 1;
+        int k = 0;
+        for (int m = m0; m < M; m += stride, ++k) {
+            MHead H;
+            if (k < kJacobiHeads) H = heads[k][threadIdx.x];
+            else load_head(V, m, H);
+            solve_manifold_h<TAPE, GATHER4>(V, m, H, friction, first, inBuf, outBuf, T, p);
+        }
     }
 }
 

@@ -119,8 +119,8 @@ __device__ __forceinline__ void solve_row(const float4 r0, const float4 r1, floa
 // Averaged delta velocity of body b over its copies in buffer buf
 // (averageVelocities, P2/btPgsJacobiSolver.cpp:1683-1720): copies in
 // manifold order, sum then multiply by 1/count.
-__device__ __forceinline__ void body_average(const SolverView& V, int b, int buf, float3& lin, float3& ang) {
-    const uint32_t s = V.incStart[b], e = V.incEnd[b];
+__device__ __forceinline__ void body_average_se(const SolverView& V, uint32_t s, uint32_t e, int buf, float3& lin,
+                                                float3& ang) {
     float3 sl = make_float3(0.f, 0.f, 0.f), sa = sl;
     for (uint32_t i = s; i < e; ++i) {
         const uint32_t cid = V.incVals[i];
@@ -131,6 +131,9 @@ __device__ __forceinline__ void body_average(const SolverView& V, int b, int buf
     const float factor = 1.f / (float)(e - s);
     lin = sl * factor;
     ang = sa * factor;
+}
+__device__ __forceinline__ void body_average(const SolverView& V, int b, int buf, float3& lin, float3& ang) {
+    body_average_se(V, V.incStart[b], V.incEnd[b], buf, lin, ang);
 }
 
 // One body's average given its incidence range, with the loads issued four
