@@ -151,6 +151,7 @@ SIGNATURES = [
     ("b3_narrowphase_compute_contacts", _I, [_P, _P, _I, _P]),
     ("b3_solver_solve_jacobi", _I, [_P, _P]),
     ("b3_solver_solve_batched_gs", _I, [_P, _P]),
+    ("b3_load_bullet_file", _I, [_P, C.c_char_p, _I, _IP]),
     ("b3_get_gs_batches", _I, [_P, _IP, _I, _IP, _P]),
     ("b3_get_gs_constraints", _I, [_P, C.POINTER(Constraint4), _I, _IP, _P]),
     ("b3_integrate", _I, [_P, _P]),
@@ -545,6 +546,18 @@ class PhysicsWorld:
         with flags=B3_WORLD_SAP_BROADPHASE (from the current AABBs)."""
         _check(self.lib.b3_sap_broadphase_calculate_overlapping_pairs(self.h, _stream(stream)),
                "b3_sap_broadphase_calculate_overlapping_pairs")
+
+    def load_bullet_file(self, path, keep_static_objects=False):
+        """btBulletDataExtractor::convertAllObjects on a .bullet scene file:
+        registers its box and convex-hull shapes and its rigid bodies (see
+        b3_load_bullet_file); returns the number of bodies added."""
+        n = C.c_int()
+        _check(self.lib.b3_load_bullet_file(self.h, os.fsencode(path), 1 if keep_static_objects else 0, C.byref(n)),
+               "b3_load_bullet_file")
+        total = C.c_int()
+        _check(self.lib.b3_get_num_bodies(self.h, C.byref(total)), "b3_get_num_bodies")
+        self.n = total.value
+        return n.value
 
     def solve_batched_gs(self, stream=None):
         """Solver::batchContacts + convertToConstraints + solveContactConstraint

@@ -849,8 +849,12 @@ extern "C" int b3_write_state(b3World w, const float* pos4, const float* quat4, 
 
 extern "C" int b3_read_bodies(b3World w, b3Body* out, int maxBodies, void* stream) {
     if (!w || !out) return B3_ERR_INVALID_ARG;
-    if (!w->written) return B3_ERR_STATE;
     const int N = std::min((int)w->bodies.size(), maxBodies);
+    if (!w->written) {
+        // before the first write: the records as registered (host only)
+        for (int i = 0; i < N; ++i) out[i] = w->bodies[i];
+        return B3_OK;
+    }
     std::vector<float4> p(w->bodies.size()), q(p.size()), l(p.size()), a(p.size());
     B3_TRY(b3_read_state(w, (float*)p.data(), (float*)q.data(), (float*)l.data(), (float*)a.data(), stream));
     for (int i = 0; i < N; ++i) {

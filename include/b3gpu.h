@@ -319,6 +319,21 @@ int b3_register_convex_hull(b3World w, const float* vertices, int numVertices, i
 int b3_register_body(b3World w, float mass, const float position[3], const float orientation[4],
                      int collidable, float friction, float restitution, int worldId, int* bodyOut);
 
+/* btBulletDataExtractor::convertAllObjects (P2/BulletDataExtractor.cpp:
+ * 456-721) on a .bullet scene file as bullet2's btDefaultSerializer writes it
+ * (single precision, little endian), read by this library's own parser of
+ * the format (chunks and the DNA1 struct catalogue, fields found by name as
+ * bParse's btBulletFile does). Registers, in file order, the box shapes (the
+ * unit cube scaled by halfDimensions * localScaling + margin) and convex
+ * hulls (points times localScaling); spheres, planes and other shapes are
+ * skipped, as there. Then the rigid bodies, grouped by shape in shape order:
+ * mass 1 / inverseMass, position and orientation from the world transform,
+ * friction 1 (registerRigidBody, P1/btGpuNarrowPhaseAndSolver.cpp:577).
+ * Static bodies are dropped unless keepStaticObjects, and then, as the demo
+ * does, a 50 x 50 grid of static ground tiles is added. Call before
+ * b3_write_bodies; *numBodiesOut = bodies added. */
+int b3_load_bullet_file(b3World w, const char* path, int keepStaticObjects, int* numBodiesOut);
+
 /* Bulk form of b3_register_body for n bodies (arrays of n, xyz / xyzw
  * packed); writes the id of the first new body. */
 int b3_register_bodies(b3World w, int n, const float* masses, const float* positions3,
@@ -337,7 +352,8 @@ int b3_write_velocities(b3World w, const float* linVel3, const float* angVel3, v
  * setup, Jacobi solve with velocity averaging, integrate; n steps. */
 int b3_step(b3World w, int numSteps, void* stream);
 
-/* Read bodies back in the reference Body layout (host, synchronising). */
+/* Read bodies back in the reference Body layout (host, synchronising);
+ * before the first b3_write_bodies, the records as registered. */
 int b3_read_bodies(b3World w, b3Body* out, int maxBodies, void* stream);
 /* Read SoA state (host float4 arrays, NULL to skip; synchronising). */
 int b3_read_state(b3World w, float* pos4, float* quat4, float* linVel4, float* angVel4, void* stream);

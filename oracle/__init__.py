@@ -120,6 +120,8 @@ def bullet_lib():
         B.rb_step.argtypes = [_VP, C.c_int]
         B.rb_positions.argtypes = [_VP, _F]
         B.rb_destroy.argtypes = [_VP]
+        B.rb_write_bullet.restype = C.c_int
+        B.rb_write_bullet.argtypes = [_VP, C.c_char_p]
         _bullet = B
     return _bullet
 
@@ -156,6 +158,11 @@ class ReferenceCpuWorld:
         out = np.zeros((self.n, 3), np.float32)
         self.B.rb_positions(self.h, _f(out))
         return out
+
+    def write_bullet(self, path):
+        """The first world written by bullet2's btDefaultSerializer (a .bullet file)."""
+        if self.B.rb_write_bullet(self.h, os.fsencode(path)) != 0:
+            raise RuntimeError(f"could not write {path}")
 
     def close(self):
         if self.h:

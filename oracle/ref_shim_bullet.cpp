@@ -9,6 +9,7 @@
 #include "btBulletDynamicsCommon.h"
 
 #include <cmath>
+#include <cstdio>
 #include <vector>
 
 namespace {
@@ -115,6 +116,23 @@ void rb_positions(void* h, float* pos3) {
         pos3[3 * i + 1] = o.y();
         pos3[3 * i + 2] = o.z();
     }
+}
+
+// The first world serialised by bullet2's own btDefaultSerializer into a
+// .bullet file at path (the reference's scene file format); 0 on success.
+int rb_write_bullet(void* h, const char* path) {
+    RefScene* s = (RefScene*)h;
+    btDefaultSerializer* ser = new btDefaultSerializer();
+    s->worlds[0].world->serialize(ser);
+    FILE* f = fopen(path, "wb");
+    if (!f) {
+        delete ser;
+        return 1;
+    }
+    const size_t n = fwrite(ser->getBufferPointer(), ser->getCurrentBufferSize(), 1, f);
+    fclose(f);
+    delete ser;
+    return n == 1 ? 0 : 1;
 }
 
 void rb_destroy(void* h) {

@@ -44,6 +44,16 @@ gs_solve_args.npz
     class and N_SPLIT. The fixture keeps the used constraints, the bodies'
     positions, inverse masses and world inverse inertias, and the grid.
 
+pile.bullet, pile_bullet.npz
+    A .bullet scene file written by the reference's own serializer: a seeded
+    pile (random_pile seed 61, 40 bodies: unit cubes, which the reference
+    CPU pipeline builds as btBoxShape, and 12-point hulls as
+    btConvexHullShape) on a static ground box, put into bullet2's
+    btDiscreteDynamicsWorld (oracle/_ref/libb3bullet.so, compiled from the
+    reference's bullet2 sources) and written by btDefaultSerializer. The npz
+    keeps the scene it was made from (positions, orientations, masses,
+    shape of each body and the shapes' points).
+
 hull_pins.npz
     btConvexUtility::initializePolyhedralFeatures
     (P1/btConvexUtility.cpp:31-270) on every distinct shape of the plain and
@@ -349,6 +359,23 @@ def make_gs():
     return rec
 
 
+def make_bullet_scene():
+    _import_tests()
+    import oracle
+    from experiments_b200 import scenes
+    sc = scenes.random_pile(61, n=40, hull_frac=0.5, pool=4)
+    ref = oracle.ReferenceCpuWorld(sc)
+    ref.write_bullet(os.path.join(HERE, "pile.bullet"))
+    ref.close()
+    pts = [np.asarray(v, np.float32).reshape(-1, 3) for v in sc.shapes]
+    offs = np.concatenate([[0], np.cumsum([len(p) for p in pts])]).astype(np.int32)
+    rec = dict(pos=np.asarray(sc.pos, np.float32), quat=np.asarray(sc.quat, np.float32),
+               mass=np.asarray(sc.mass, np.float32), shape=np.asarray(sc.shape, np.int32),
+               points=np.concatenate(pts).astype(np.float32), shapeOffsets=offs)
+    np.savez_compressed(os.path.join(HERE, "pile_bullet.npz"), **rec)
+    return sc.n
+
+
 def make_hulls():
     _import_tests()
     import test_cpu_pins as pins
@@ -379,3 +406,4 @@ if __name__ == "__main__":
     print("sap_kernel_args.npz:", int(r["numObjects"]), "sorted AABBs")
     r = make_gs()
     print("gs_solve_args.npz:", len(r["batchIdx"]), "constraints")
+    print("pile.bullet:", make_bullet_scene(), "bodies")
