@@ -139,6 +139,14 @@ public:
     b3World handle() const { return h_; }
 
     /* CLPhysicsDemo::registerConvexPolyhedron: returns the collidable id. */
+    /* createScene's file path (P2/BulletDataExtractor.cpp:456-721): the
+     * shapes and rigid bodies of a .bullet file (b3_load_bullet_file);
+     * returns the bodies added. */
+    int loadBulletFile(const char* path, bool keepStaticObjects = false) {
+        int n = 0;
+        check(b3_load_bullet_file(h_, path, keepStaticObjects ? 1 : 0, &n), "loadBulletFile");
+        return n;
+    }
     int registerConvexPolyhedron(const float* vertices, int numVertices, int strideBytes = 16,
                                  const float* scaling3 = nullptr) {
         int c = -1;

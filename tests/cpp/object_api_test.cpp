@@ -56,8 +56,15 @@ static b3WorldConfig stack_config() {
     return cfg;
 }
 
-static int host_mode() {
+static int host_mode(const char* bulletFile) {
     b3::Context ctx(-1);
+    if (bulletFile) {
+        // createScene's file path: the shapes and bodies of a .bullet scene
+        b3WorldConfig cfg = stack_config();
+        cfg.maxBodies = 64;
+        b3::World wf(ctx, cfg);
+        EXPECT(wf.loadBulletFile(bulletFile, true) == 41 && wf.numBodies() == 41);
+    }
     b3::World w(ctx, stack_config());
     EXPECT(build_stack(w) == w.numBodies());
     b3::GpuNarrowphaseAndSolver np(w);
@@ -197,7 +204,7 @@ int main(int argc, char** argv) {
     const bool gpu = argc > 1 && std::strcmp(argv[1], "gpu") == 0;
     int rc = 1;
     try {
-        rc = gpu ? gpu_mode() : host_mode();
+        rc = gpu ? gpu_mode() : host_mode(argc > 2 ? argv[2] : nullptr);
     } catch (const std::exception& e) {
         std::printf("FAILED: %s\n", e.what());
         return 1;

@@ -24,7 +24,8 @@ def program():
 
 
 def test_object_api_host(program):
-    r = subprocess.run([program, "host"], capture_output=True, text=True, timeout=120)
+    bullet = os.path.join(ROOT, "tests", "golden", "pile.bullet")  # a .bullet scene of 41 bodies
+    r = subprocess.run([program, "host", bullet], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0 and "OK" in r.stdout, r.stdout + r.stderr
 
 
