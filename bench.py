@@ -5,29 +5,43 @@ python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2] [--impl b3|r
 Prints one JSON line on rank 0.
 
 * value: whole-job body-steps/s of the plain step on the workload (default
-  the 131,072-body mixed-hull scene), the scene resident in HBM. Each of
-  the K timed steps is one replay of the captured step graph bracketed by
-  CUDA events on the launching stream; a 256 MiB write flushes L2 between
-  steps, outside the events. Max over ranks; for N > 1 every rank steps its
-  own replica (weak scaling, no collective on the data path).
-* e2e: the same metric through the C ABI with host buffers: every step
-  uploads the body state from pinned host memory, steps, and reads the
-  state back (H2D + D2H inside the timed region).
-* roofline: the dominant kernel of the step from live per-stage CUDA-event
-  times. The narrowphase is FP32-ALU bound (SAT projections), so its
-  roofline is FP32 FLOP/s against the CUDA-core peak; the other stages are
-  HBM bound and use the measured copy bandwidth. All stages are listed in
-  stage_roofline.
+  the 131,072-body mixed-hull scene), the scene resident in HBM, timed in
+  the contact-rich part of the run: the scene is stepped to the settle step
+  (300 of c2's 1,000: every layer has landed), then W warm-up steps, then K
+  timed steps. Each timed step is one replay of the captured step graph
+  bracketed by CUDA events on the launching stream; a 256 MiB write
+  flushes L2 between steps, outside the events. `early` holds the same
+  measurement over the free-fall start (steps W+1..W+K). Max over ranks;
+  for N > 1 every rank steps its own replica (weak scaling, no collective
+  on the data path).
+* e2e: the same metric through the C ABI with host buffers, in the settled
+  window: every step uploads the body state from pinned host memory,
+  steps, and reads the state back (H2D + D2H inside the timed region).
+* error: one step of the timed state checked against the oracle, stage by
+  stage (oracle/parity.py), measured in this run.
+* roofline: the kernel that takes the most time in the settled step, from
+  live per-kernel CUDA-event times: the separating-axis sweep and the FP32
+  clip against the FP32 CUDA-core peak at the sampled SM clock, with the
+  FP32 work they execute (per pair, from the ncu capture summarised in
+  profiles/); the other kernels against the measured HBM copy bandwidth
+  with their compulsory bytes. step_roofline is the whole step's
+  compulsory bytes against HBM; stage_roofline lists every stage.
 * cpu_baseline: the reference's CPU rigid-body pipeline (bullet2
-  btDiscreteDynamicsWorld built from the reference's sources; the oracle port
-  where that library is absent) on one host thread, a bounded sample of the
-  same scene.
-* forms: the batched 4,096-world step against the plain per-world step on
-  the same GPU (body-steps/s of each; per-world time sampled on a subset),
-  and the adjoint form (forward with checkpoints + reverse sweep) on the
-  256-world differentiable throw against its plain forward.
---impl reference: the same CPU pipeline on all host cores (independent
-  replicas, one process per core), same metric and workload.
+  btDiscreteDynamicsWorld built from the reference's sources; the oracle
+  port where that library is absent) on one host thread, timed in the
+  settled window of one column of the scene (a 1/16 block of the lattice
+  footprint, all layers, with the ground), stepped alone to the same settle
+  step.
+* forms: the batched 4,096-world step against the plain step run world by
+  world on the same GPU, both at the settle step (body-steps/s of each;
+  per-world time sampled on a subset), with the batched step's one-step
+  error against the oracle; and the adjoint form (forward with checkpoints
+  + reverse sweep) on the 256-world differentiable throw against its plain
+  forward.
+* scale: the 1,048,576-cube plain step and adjoint.
+--impl reference: the same CPU pipeline on all host cores: one replica per
+  core, each one column block of the scene stepped to the settle step and
+  then timed (the 16 blocks tile the whole scene), same metric.
 """
 import argparse
 import json
@@ -56,10 +70,32 @@ WORKLOADS = {
     "c5": "plain step, 1,048,576 unit cubes, 128x64x128 lattice, 10 Jacobi iterations",
 }
 STAGES = ["aabb_hash", "sort_cells", "find_pairs", "narrowphase", "manifolds", "solve", "integrate"]
-# DRAM bytes per pair of the four narrowphase kernels (read + write) from the ncu capture in
-# profiles/kernels_c2s_plain_step.md, scaled by the timed workload's pair count
-NARROWPHASE_DRAM_BYTES_PER_PAIR = 4.352e6 / 36735
-FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 148 SMs x 128 FP32 lanes x FMA x 1.965 GHz
+# per-kernel CUDA-event times that b3_get_stage_times appends after the 7 stages
+KERNELS = ["k_np_sweep", "k_np_refine", "k_np_clip", "k_np_exact", "k_setup_rows", "k_jacobi"]
+# The settle step of each workload: the timed window starts there (the
+# contact-rich part of the configuration's run); c5 runs 32 steps in all.
+SETTLE = {"c1": 150, "c2": 300, "c2s": 300, "c3": 300, "c3s": 300, "c5": 24}
+# Lattice dimensions of the single-world lattice workloads (CPU column blocks).
+LATTICE = {"c1": (16, 16, 16), "c2": (64, 32, 64), "c2s": (32, 16, 32), "c5": (128, 64, 128)}
+
+
+def fp32_peak_tflops(sm_mhz):
+    """FP32 CUDA-core peak at an SM clock: 148 SMs x 128 FP32 lanes x 2
+    (FMA) x clock. No FP32 figure is measured on this pool, so this is the
+    nominal peak at the clock sampled during the timed region."""
+    return 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+
+
+def profile_constants():
+    """Per-unit figures read from ncu captures (profiles/ncu_constants.json):
+    FP32 operations each kernel executes per unit (2 per FFMA + FADD + FMUL,
+    per thread, from smsp__sass_thread_inst_executed_op_*_pred_on.sum) and
+    its DRAM bytes per unit, on the settled 16,384-body case."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_constants.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
 
 
 def peaks():
@@ -203,6 +239,14 @@ def time_steps(w, steps, stream, flush):
     return sum(e0.elapsed_time(e1) for e0, e1 in evs)
 
 
+def window_counts(c, n, steps_done):
+    """N, P, C and contact points of the last step, for the record."""
+    return {"step": int(steps_done), "bodies": int(n), "pairs": int(c["numPairs"]),
+            "manifolds": int(c["numManifolds"]), "contact_points": int(c["numContactPoints"]),
+            "manifolds_per_body": c["numManifolds"] / max(n, 1), "iterations": 10,
+            "refined_axes": int(c["refinedAxes"]), "refined_clips": int(c["refinedClips"])}
+
+
 def run_b3(args, world_size, local_rank):
     import torch
     from experiments_b200 import b3, scenes
@@ -222,42 +266,63 @@ def run_b3(args, world_size, local_rank):
     w = scenes.build_world(ctx, sc, useGraph=1, **bp)
     st = torch.cuda.current_stream()
     flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > 126 MB L2
-    # launch shapes chosen by the autotuner on this scene (state restored)
+    settle = max(args.settle, args.warmup + args.steps)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world_size > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world_size > 1:
+            import torch.distributed as dist
+            t = torch.tensor([x], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+        return x
+
+    # early window: the free-fall start of the run, launch shapes tuned there
+    w.autotune(3, stream=st.cuda_stream)
+    for _ in range(args.warmup):
+        w.stepSimulation(1, stream=st.cuda_stream)
+    barrier()
+    early_ms = max_over_ranks(time_steps(w, args.steps, st, flush))
+    early = window_counts(w.counters(), sc.n, args.warmup + args.steps)
+    early["ms_per_step"] = early_ms / args.steps
+    done = args.warmup + args.steps
+    # settled window: step on to the settle step, retune there, warm up, time
+    if settle - args.warmup > done:
+        w.stepSimulation(settle - args.warmup - done, stream=st.cuda_stream)
+        done = settle - args.warmup
     w.autotune(3, stream=st.cuda_stream)
     tuning = w.tuning()
     for _ in range(args.warmup):
         w.stepSimulation(1, stream=st.cuda_stream)
-    torch.cuda.synchronize()
-    if world_size > 1:
-        import torch.distributed as dist
-        dist.barrier()
-    torch.cuda.synchronize()
+    done += args.warmup
+    barrier()
     with ClockSampler(local_rank) as clk:
         ms = time_steps(w, args.steps, st, flush)
-    torch.cuda.synchronize()
-    if world_size > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        dist.barrier()
+    barrier()
+    ms = max_over_ranks(ms)
+    done += args.steps
     counters = w.counters()
     kernels = w.tuning()[3]
-    # per-stage CUDA-event breakdown on an identical world advanced to the
-    # same step (eager launches; timing only, not part of `value`)
-    w2 = scenes.build_world(ctx, sc, useGraph=0, **bp)
-    w2.set_tuning(tuning)
-    w2.stepSimulation(args.warmup + args.steps - 3)
-    w2.set_stage_timing(True)
-    acc = np.zeros(len(STAGES))
+    # per-stage and per-kernel CUDA events on three more eager steps of the
+    # same world (timing only, not part of `value`)
+    w.set_stage_timing(True)
+    acc = None
     for _ in range(3):
         flush_l2(flush)
-        w2.stepSimulation(1)
-        acc += np.array(w2.stage_times()[:len(STAGES)])
+        w.stepSimulation(1, stream=st.cuda_stream)
+        t = np.array(w.stage_times(), np.float64)
+        acc = t if acc is None else acc + t
+    w.set_stage_timing(False)
+    done += 3
     stage_ms = acc / 3
-    c2 = w2.counters()
-    flops = sat_flops(w2, sc)
-    w2.close()
+    c2 = w.counters()
+    flops = sat_flops(w, sc)
     # e2e through the C ABI with pinned host buffers
     pos, quat, lin, ang = w.read_state()
     hp = torch.from_numpy(pos).pin_memory().numpy()
@@ -265,7 +330,7 @@ def run_b3(args, world_size, local_rank):
     hl = torch.from_numpy(lin).pin_memory().numpy()
     ha = torch.from_numpy(ang).pin_memory().numpy()
     e2e_steps = max(3, min(args.steps, 20))
-    torch.cuda.synchronize()
+    barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         # H2D of the step's input state from pinned memory, the step, and the
@@ -274,32 +339,56 @@ def run_b3(args, world_size, local_rank):
         w.stepSimulation(1, stream=st.cuda_stream)
         w.read_state(stream=st.cuda_stream, out=(hp, hq, hl, ha))
     torch.cuda.synchronize()
-    e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / e2e_steps)
+    done += e2e_steps
     contact_points = counters["numContactPoints"]
     if world_size > 1:
         import torch.distributed as dist
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
         t = torch.tensor([contact_points], device="cuda", dtype=torch.int64)
         dist.all_reduce(t, op=dist.ReduceOp.SUM)
         contact_points = int(t.item())
-    return dict(sc=sc, full=full, sharded=sharded, ms=ms, contact_points=contact_points, tuning=tuning, counters=counters, stage_ms=stage_ms, c2=c2, clocks=clk.summary(), e2e_ms=e2e_ms,
-                w=w, kernels=kernels, flops=flops, ctx=ctx)
+    settled = window_counts(counters, sc.n, settle + args.steps)
+    settled["ms_per_step"] = ms / args.steps
+    return dict(sc=sc, full=full, sharded=sharded, ms=ms, contact_points=contact_points, tuning=tuning,
+                counters=counters, stage_ms=stage_ms, c2=c2, clocks=clk.summary(), e2e_ms=e2e_ms, w=w,
+                kernels=kernels, flops=flops, ctx=ctx, early=early, settled=settled, early_ms=early_ms,
+                steps_done=done)
 
 
-def forms_comparison(ctx, steps=10, sample_worlds=32):
-    """Batched 4,096-world step vs the plain step run world by world."""
+def oracle_check(w, sc):
+    """One step of the device world's current state against the oracle
+    (the checker: oracle/parity.py), reported next to the throughput."""
+    import oracle
+    from oracle import parity
+    o = oracle.oracle_from_world(w, sc)
+    rep = parity.one_step_report(w, o, dynamic=np.asarray(sc.mass) > 0)
+    o.close()
+    keep = ["pos_err_m", "lin_vel_err_mps", "ang_vel_err_radps", "quat_err", "contact_point_err_m", "normal_err",
+            "aabbs_bit_exact", "keys_bit_exact", "permutation_bit_exact", "pairs_bit_exact", "manifold_set_equal",
+            "pairs", "manifolds", "within_bars", "check_s"]
+    out = {k: rep[k] for k in keep}
+    out["bars"] = "pairs/keys/permutation bit-exact; contacts 1e-5 m, normals 1e-4; one step 1e-5 m, 1e-4 m/s"
+    return out
+
+
+def forms_comparison(ctx, steps=10, sample_worlds=32, settle=SETTLE["c3"], check=True):
+    """Batched 4,096-world step vs the plain step run world by world, both
+    from the batched scene's state at the settle step (piles in contact)."""
     import torch
     from experiments_b200 import scenes
     sc = scenes.c3()
     wb = scenes.build_world(ctx, sc, useGraph=1)
     st = torch.cuda.current_stream()
+    wb.stepSimulation(settle, stream=st.cuda_stream)
     wb.autotune(3, stream=st.cuda_stream)
     for _ in range(3):
         wb.stepSimulation(1, stream=st.cuda_stream)
     ms_b = time_steps(wb, steps, st, None)
     batched = sc.n * steps / (ms_b / 1e3)
+    cb = wb.counters()
+    # the state the batched timing started from is gone; take the current
+    # one for the per-world worlds and time them over the same count of steps
+    pos, quat, lin, ang = wb.read_state()
     # plain per-world step: each world in its own plain world, stepped one
     # world at a time (the reference's one-scene-per-pipeline usage)
     counts = sc.extra["counts"]
@@ -309,7 +398,9 @@ def forms_comparison(ctx, steps=10, sample_worlds=32):
     bodies = 0
     for wid in pick:
         sub = scenes.select_worlds(sc, [int(wid)])
+        idx = np.nonzero(np.asarray(sc.world) == int(wid))[0]
         wp = scenes.build_world(ctx, sub, useGraph=1)
+        wp.write_state(pos[idx], quat[idx], lin[idx], ang[idx])
         for _ in range(3):
             wp.stepSimulation(1, stream=st.cuda_stream)
         total_ms += time_steps(wp, steps, st, None)
@@ -318,11 +409,15 @@ def forms_comparison(ctx, steps=10, sample_worlds=32):
     # extrapolate the sampled per-world times to all worlds
     per_body_ms = total_ms / max(bodies, 1)
     plain = sc.n * steps / (per_body_ms * sc.n / 1e3)
+    out = {"batched_body_steps_per_s": batched, "plain_per_world_body_steps_per_s": plain,
+           "speedup": batched / plain, "worlds": int(sc.num_worlds), "bodies": int(sc.n),
+           "plain_sample": f"{len(pick)} of {sc.num_worlds} worlds, {steps} steps each, graph replay, "
+                           f"from the batched scene's state at step {settle + 3 + steps}",
+           "steps": steps, "window": window_counts(cb, sc.n, settle + 3 + steps)}
+    if check:
+        out["error"] = oracle_check(wb, sc)
     wb.close()
-    return {"batched_body_steps_per_s": batched, "plain_per_world_body_steps_per_s": plain,
-            "speedup": batched / plain, "worlds": int(sc.num_worlds), "bodies": int(sc.n),
-            "plain_sample": f"{len(pick)} of {sc.num_worlds} worlds, {steps} steps each, graph replay",
-            "steps": steps}
+    return out
 
 
 def adjoint_form(ctx, worlds=256, steps=120, checkpoint_every=16):
@@ -434,14 +529,18 @@ def scale_run(ctx, steps=32, checkpoint_every=8):
 
 
 def _cpu_worker(args):
-    """One CPU replica of the workload for `budget_s` seconds: the reference's
-    CPU pipeline (bullet2 btDiscreteDynamicsWorld) when built, else the
-    oracle port."""
-    name, budget_s = args
+    """One CPU replica: the reference's CPU pipeline (bullet2
+    btDiscreteDynamicsWorld) when built, else the oracle port, on one column
+    block of a lattice workload (or the whole scene of a batched one). It is
+    stepped untimed to the settle step, then timed for up to `budget_s`
+    seconds (at least one step)."""
+    name, block, settle, budget_s = args
     sys.path.insert(0, ROOT)
     import oracle
     from experiments_b200 import b3, scenes
     sc = make_scene(name)
+    if block is not None and name in LATTICE:
+        sc = scenes.lattice_block(sc, LATTICE[name], block)
     if oracle.bullet_lib() is not None:
         wld = oracle.ReferenceCpuWorld(sc)
         kind = "reference"
@@ -451,12 +550,15 @@ def _cpu_worker(args):
         scenes.register_scene(w, sc)
         wld = oracle.oracle_from_world(w, sc)
         kind = "port"
+    ts = time.perf_counter()
+    wld.step(settle)
+    settle_s = time.perf_counter() - ts
     t0 = time.perf_counter()
     steps = 0
-    while time.perf_counter() - t0 < budget_s and steps < 1000:
+    while steps < 1 or (time.perf_counter() - t0 < budget_s and steps < 1000):
         wld.step(1)
         steps += 1
-    return sc.n, steps, time.perf_counter() - t0, kind
+    return sc.n, steps, time.perf_counter() - t0, kind, settle_s
 
 
 CPU_KIND = {"reference": "bullet2 btDiscreteDynamicsWorld (btDbvtBroadphase + btSequentialImpulseConstraintSolver, "
@@ -464,21 +566,85 @@ CPU_KIND = {"reference": "bullet2 btDiscreteDynamicsWorld (btDbvtBroadphase + bt
             "port": "the oracle (single-threaded C++ restatement of the reference step, FP64)"}
 
 
-def cpu_baseline_port(name, budget_s=12.0, procs=1):
+def cpu_baseline_port(name, budget_s=10.0, procs=1, settle=None):
     """The reference's CPU pipeline (or the oracle port) on `procs` host
-    cores (independent replicas, one process each)."""
+    cores, one replica per core. For a lattice workload replica r runs
+    column block r mod 16 of the scene (the 16 blocks tile the footprint),
+    stepped alone to the settle step and then timed; a batched workload runs
+    whole, timed from the start."""
+    settle = SETTLE.get(name, 0) if settle is None else settle
+    lattice = name in LATTICE
+    blocks = [k % 16 if lattice else None for k in range(max(1, procs))]
+    st = settle if lattice else 0
     if procs <= 1:
-        n, steps, dt, kind = _cpu_worker((name, budget_s))
-        return {"value": n * steps / dt, "unit": "body-steps/s", "cores": 1, "kind": kind,
-                "sample": f"first {steps} steps of the full {n}-body scene ({dt:.1f} s), 1 thread; {CPU_KIND[kind]}"}
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(procs) as pool:
-        res = pool.map(_cpu_worker, [(name, budget_s)] * procs)
-    total = sum(n * s / dt for n, s, dt, _ in res)
-    n, s, dt, kind = res[0]
-    return {"value": total, "unit": "body-steps/s", "cores": procs, "kind": kind,
-            "sample": f"{procs} independent replicas, each the first ~{s} steps of the full {n}-body scene "
-                      f"(~{dt:.0f} s); {CPU_KIND[kind]}"}
+        res = [_cpu_worker((name, blocks[0], st, budget_s))]
+    else:
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(procs) as pool:
+            res = pool.map(_cpu_worker, [(name, b, st, budget_s) for b in blocks])
+    total = sum(n * s / dt for n, s, dt, _, _ in res)
+    n, s, dt, kind, settle_s = res[0]
+    if lattice:
+        what = (f"{len(res)} replica(s), each one 1/16 column block of the scene ({n} bodies with the ground; the "
+                f"16 blocks tile the footprint) stepped alone to step {st} ({settle_s:.0f} s untimed), then ~{s} "
+                f"steps timed (~{dt:.0f} s)")
+    else:
+        what = f"{len(res)} replica(s), each the first ~{s} steps of the full {n}-body scene (~{dt:.0f} s)"
+    return {"value": total, "unit": "body-steps/s", "cores": len(res), "kind": kind,
+            "sample": f"{what}; {CPU_KIND[kind]}"}
+
+
+def kernel_roofline(name, ms, sc, counters, key_bits, body_bits, hbm_peak, peak_kind, sm_mhz, consts):
+    """Roofline of one kernel or stage from its CUDA-event time. The sweep
+    and the FP32 clip are FP32-issue bound: achieved = the FP32 operations
+    they execute (per unit, from the ncu capture) / time, against the FP32
+    CUDA-core peak at the sampled clock. Everything else is HBM bound:
+    compulsory bytes / time against the measured copy bandwidth."""
+    n = sc.n
+    P = counters["numPairs"]
+    C = counters["numManifolds"]
+    iters = 10
+    sb = stage_bytes(n, counters, key_bits, body_bits, iters)
+    hbm_bytes = dict(sb)
+    hbm_bytes["k_setup_rows"] = C * (96 + 368)
+    hbm_bytes["k_jacobi"] = iters * (200 * C + 64 * n)
+    hbm_bytes["k_np_refine"] = None
+    hbm_bytes["k_np_exact"] = None
+    units = {"k_np_sweep": ("pair", P), "k_np_clip": ("manifold", C)}
+    if name in units:
+        unit, count = units[name]
+        c = consts.get(name, {})
+        ops = c.get("fp32_ops_per_" + unit)
+        peak = fp32_peak_tflops(sm_mhz or 1965.0)
+        r = {"kernel": name, "bound": "fp32", "unit": "TFLOP/s", "peak": peak, "ms": ms,
+             "peak_kind": f"nominal FP32 CUDA-core peak at the sampled SM clock ({sm_mhz} MHz); no measured FP32 peak"}
+        if ops is not None:
+            r["achieved"] = ops * count / (ms / 1e3) / 1e12
+            r["frac"] = r["achieved"] / peak
+            r["work"] = (f"executed FP32 operations: {ops:.0f} per {unit} (2 per FFMA + FADD + FMUL, per thread) "
+                         f"from {c.get('source')}, times {count} {unit}s")
+        else:
+            r["achieved"] = None
+            r["frac"] = None
+            r["work"] = "no ncu capture of this kernel's executed FP32 operations"
+        dram = c.get("dram_bytes_per_" + unit)
+        r["traffic"] = dram * count if dram is not None else None
+        r["traffic_source"] = c.get("source") if dram is not None else None
+        return r
+    b = hbm_bytes.get(name)
+    r = {"kernel": name, "bound": "hbm", "unit": "GB/s", "peak": hbm_peak, "ms": ms, "peak_kind": peak_kind}
+    if b is None:
+        r.update(achieved=None, frac=None, traffic=None, work="latency-bound minority path; no byte model")
+        return r
+    r["achieved"] = b / (ms / 1e3) / 1e9
+    r["frac"] = r["achieved"] / hbm_peak
+    r["bytes"] = b
+    c = consts.get(name, {})
+    unit = "manifold" if name in ("k_setup_rows", "k_jacobi") else "body"
+    dram = c.get("dram_bytes_per_" + unit)
+    r["traffic"] = dram * (C if unit == "manifold" else n) if dram is not None else None
+    r["traffic_source"] = c.get("source") if dram is not None else None
+    return r
 
 
 def main():
@@ -488,9 +654,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="b3", choices=["b3", "reference"])
+    ap.add_argument("--settle", type=int, default=None,
+                    help="step at which the timed window starts (default: per workload, c2 300)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true")
-    ap.add_argument("--scale", action="store_true", help="also run the 1,048,576-body plain and adjoint steps")
+    ap.add_argument("--no-scale", action="store_true", help="skip the 1,048,576-body plain and adjoint steps")
+    ap.add_argument("--no-check", action="store_true", help="skip the one-step oracle checks")
     ap.add_argument("--sap", action="store_true",
                     help="sweep-and-prune broadphase (pipeline2's default) in place of the grid; single-world workloads")
     ap.add_argument("--solver", default="jacobi", choices=["jacobi", "gs"],
@@ -501,6 +670,8 @@ def main():
     world_size = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     args.warmup = max(3, args.warmup)
+    if args.settle is None:
+        args.settle = SETTLE[args.workload]
     cfg = {"workload": WORKLOADS[args.workload]}
     if args.sap:
         if args.workload in ("c3", "c3s"):
@@ -515,7 +686,8 @@ def main():
         if rank != 0:
             return
         procs = max(1, os.cpu_count() or 1)
-        r = cpu_baseline_port(args.workload, budget_s=20.0, procs=procs)
+        r = cpu_baseline_port(args.workload, budget_s=15.0, procs=procs, settle=args.settle)
+        cfg["window"] = f"settled: timed from step {args.settle}" if args.workload in LATTICE else "from the start"
         line = {"metric": "body-steps/s", "value": r["value"], "unit": "body-steps/s", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32" if r["kind"] == "reference" else "f64",
@@ -544,37 +716,53 @@ def main():
     key_bits = sum(int(d).bit_length() - 1 for d in dims) + \
         ((int(sc.num_worlds) - 1).bit_length() if sc.num_worlds > 1 else 0)
     body_bits = max(1, int(sc.n).bit_length())
+    sm_mhz = res["clocks"].get("sm_mhz")
+    consts = profile_constants()
     sb = stage_bytes(sc.n, res["c2"], key_bits, body_bits, 10)
-    sm = dict(zip(STAGES, res["stage_ms"].tolist()))
+    stage_ms = res["stage_ms"].tolist()
+    sm = dict(zip(STAGES, stage_ms[:len(STAGES)]))
+    km = dict(zip(KERNELS, stage_ms[len(STAGES):len(STAGES) + len(KERNELS)]))
     stage_roof = {}
     for k in STAGES:
         if k == "narrowphase":
             ach = res["flops"] / (sm[k] / 1e3) / 1e12
-            stage_roof[k] = {"bound": "fp32", "achieved": ach, "peak": FP32_PEAK_TFLOPS, "unit": "TFLOP/s",
-                             "frac": ach / FP32_PEAK_TFLOPS, "ms": sm[k]}
+            pk = fp32_peak_tflops(sm_mhz or 1965.0)
+            stage_roof[k] = {"bound": "fp32", "algorithmic_tflops": ach, "peak": pk, "unit": "TFLOP/s",
+                             "ms": sm[k],
+                             "work": "FLOPs of the reference algorithm (every axis projected: 8 (VA+VB)(FA+FB+EA*EB) "
+                                     "per pair + 64 V_inc V_ref per clip); the kernels skip axes that provably cannot "
+                                     "separate or be the minimum, so they execute fewer (see roofline)"}
         else:
             ach = sb[k] / (sm[k] / 1e3) / 1e9
             stage_roof[k] = {"bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
                              "frac": ach / hbm_peak, "ms": sm[k]}
+    kernel_roof = {}
+    for k, t in list(km.items()) + [(s_, sm[s_]) for s_ in ("aabb_hash", "sort_cells", "find_pairs", "manifolds",
+                                                            "integrate")]:
+        if t > 0:
+            kernel_roof[k] = kernel_roofline(k, t, sc, res["c2"], key_bits, body_bits, hbm_peak, peak_kind, sm_mhz,
+                                             consts)
     b_step = step_bytes(sc.n, res["counters"], key_bits, 10)
     step_roof = {"bound": "hbm", "achieved": b_step / (ms_per_step / 1e3) / 1e9, "peak": hbm_peak,
-                 "unit": "GB/s", "bytes_per_step": b_step, "peak_kind": peak_kind}
+                 "unit": "GB/s", "bytes_per_step": b_step, "peak_kind": peak_kind,
+                 "model": "N (128 + 20 + 8 + S + 12 + 32) + 80 P + 368 C + I (200 C + 64 N)"}
     step_roof["frac"] = step_roof["achieved"] / hbm_peak
-    dom = max(sm, key=lambda k: sm[k])
-    roof = dict(stage_roof[dom])
-    roof["kernel"] = dom
-    roof["traffic"] = NARROWPHASE_DRAM_BYTES_PER_PAIR * res["c2"]["numPairs"] if dom == "narrowphase" else None
-    roof["traffic_source"] = "ncu dram bytes per pair on the 16,384-body case, scaled by pairs" \
-        if dom == "narrowphase" else None
-    roof["peak_kind"] = "nominal FP32 CUDA-core peak" if roof["bound"] == "fp32" else peak_kind
-    if roof["bound"] == "fp32":
-        roof["work"] = ("FLOPs of the reference algorithm (every axis projected, 8 (VA+VB)(FA+FB+EA*EB) per pair "
-                        "+ 64 V_inc V_ref per clip); the sweep skips axes that provably cannot separate or be the "
-                        "minimum, so the FLOPs executed are fewer")
-    cfg.update({"bodies": int(sc.n), "worlds": int(sc.num_worlds), "pairs": res["counters"]["numPairs"],
-                "manifolds": res["counters"]["numManifolds"],
-                "contact_points": res["counters"]["numContactPoints"], "iterations": 10, "dt": 1 / 60,
-                "refined_axes": res["counters"]["refinedAxes"], "refined_clips": res["counters"]["refinedClips"],
+    # the dominant kernel of the settled step
+    dom = max(kernel_roof, key=lambda k: kernel_roof[k]["ms"])
+    roof = dict(kernel_roof[dom])
+    roof["share_of_step"] = roof["ms"] / max(sum(sm.values()), 1e-9)
+    early_bytes = step_bytes(sc.n, {"numPairs": res["early"]["pairs"], "numManifolds": res["early"]["manifolds"]},
+                             key_bits, 10)
+    early = dict(res["early"])
+    early["body_steps_per_s"] = job_bodies / (early["ms_per_step"] / 1e3)
+    early["step_roofline_frac"] = early_bytes / (early["ms_per_step"] / 1e3) / 1e9 / hbm_peak
+    settled = dict(res["settled"])
+    settled["step_roofline_frac"] = step_roof["frac"]
+    cfg.update({"bodies": int(sc.n), "worlds": int(sc.num_worlds), "iterations": 10, "dt": 1 / 60,
+                "window": f"steps {args.settle + 1}..{args.settle + args.steps} of the run (settle step "
+                          f"{args.settle}, {args.warmup} warm-up steps before it)",
+                "pairs": res["counters"]["numPairs"], "manifolds": res["counters"]["numManifolds"],
+                "contact_points": res["counters"]["numContactPoints"],
                 "l2": "flushed between timed steps (256 MiB write outside the events)",
                 "tuning": {"np_warps_per_cta": res["tuning"][0], "pair_cta": res["tuning"][1],
                            "jacobi_cta": res["tuning"][2], "jacobi_blocks_per_sm": res["tuning"][4],
@@ -582,9 +770,7 @@ def main():
                            "jacobi_gather4": res["tuning"][7],
                            "kernels_per_step": int(res["kernels"])},
                 "parallelism": (f"worlds sharded x{world_size}" if res["sharded"] else f"replicas x{world_size}")
-                if world_size > 1 else "single GPU",
-                "error": "pairs/keys bit-exact; contacts 1e-5 m / normals 1e-4; one step 1e-5 m, 1e-4 m/s "
-                         "(tests/test_gpu_parity.py)"})
+                if world_size > 1 else "single GPU"})
     line = {
         "metric": "body-steps/s", "value": value, "unit": "body-steps/s", "n_gpus": world_size,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
@@ -593,18 +779,22 @@ def main():
         "config": cfg,
         # contact points of every rank (summed), per timed second
         "contacts_per_s": res["contact_points"] * args.steps / (res["ms"] / 1e3),
-        "roofline": roof, "step_roofline": step_roof, "stage_roofline": stage_roof, "clocks": res["clocks"],
+        "settled": settled, "early": early,
+        "roofline": roof, "step_roofline": step_roof, "kernel_roofline": kernel_roof,
+        "stage_roofline": stage_roof, "clocks": res["clocks"],
         "e2e": {"value": job_bodies / (res["e2e_ms"] / 1e3), "unit": "body-steps/s",
                 "h2d_bytes_per_step": 64 * sc.n, "d2h_bytes_per_step": 64 * sc.n},
         "gpu_launches": int(res["kernels"]) * args.steps,
     }
+    if rank == 0 and world_size == 1 and not args.no_check:
+        line["error"] = oracle_check(w, sc)
     if rank == 0 and world_size == 1 and not args.no_forms:
-        line["forms"] = forms_comparison(res["ctx"])
+        line["forms"] = forms_comparison(res["ctx"], check=not args.no_check)
         line["forms"]["adjoint"] = adjoint_form(res["ctx"])
-    if rank == 0 and world_size == 1 and args.scale:
+    if rank == 0 and world_size == 1 and not args.no_scale:
         line["scale"] = scale_run(res["ctx"])
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_port(args.workload)
+        line["cpu_baseline"] = cpu_baseline_port(args.workload, settle=args.settle)
     if rank == 0:
         print(json.dumps(line))
     if world_size > 1:

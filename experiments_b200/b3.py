@@ -120,7 +120,7 @@ SIGNATURES = [
     ("b3_fill_u32", _I, [_P, _P, C.c_uint32, _I64, _I64, _P]),
     ("b3_fill_int2", _I, [_P, _P, C.c_int32, C.c_int32, _I64, _I64, _P]),
     ("b3_prefix_scan_u32", _I, [_P, _P, _P, _I64, _P, _U32P, _P]),
-    ("b3_prefix_scan_u32_static", _I, [_P, _P, _I64, _P, _P]),
+    ("b3_prefix_scan_u32_static", _I, [_P, _P, _I64, _P, _P, _P]),
     ("b3_radix_sort32_kv", _I, [_P, _P, _P, _I64, _I, _P]),
     ("b3_radix_sort32_keys", _I, [_P, _P, _I64, _I, _P]),
     ("b3_bound_search", _I, [_P, _P, _I64, _P, _I64, _I, _P]),

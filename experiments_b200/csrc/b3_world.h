@@ -179,9 +179,13 @@ struct b3World_t {
     cudaStream_t graphStream = nullptr;
     bool graphValid = false;
 
-    // stage timing
+    // stage timing; with it on, the narrowphase also records one event
+    // after each of its four kernels (npEv[0] before the sweep) and the
+    // Jacobi solve one after its row setup (setupEv)
     bool timing = false;
     std::vector<float> stageMs;
+    cudaEvent_t npEv[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t setupEv = nullptr;
 
     // tunables (autotuner)
     int npWarpsPerBlock = 4;   // narrowphase warps per CTA

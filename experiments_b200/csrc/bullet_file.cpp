@@ -20,6 +20,8 @@
 #include <vector>
 
 #include "b3_internal.h"
+#include "b3_world.h"
+#include "hull.h"
 
 namespace {
 
@@ -312,6 +314,18 @@ void basis_to_quat(const double r[3][3], float q[4]) {
 // (P2/BulletDataExtractor.cpp:529-577)
 constexpr int kBoxShape = 0;
 constexpr int kConvexHullShape = 4;
+// most points a convex hull record of a file may hold
+constexpr int64_t kMaxFileHullPoints = 1 << 16;
+
+// A shape or body of the file, read and checked before anything registers.
+struct ShapeRec {
+    uint64_t oldPtr;
+    std::vector<float> points;  // xyz triples, final scale applied
+};
+struct BodyRec {
+    int shape;  // index into the shape records
+    float mass, pos[3], quat[4];
+};
 
 }  // namespace
 
@@ -323,10 +337,11 @@ extern "C" int b3_load_bullet_file(b3World w, const char* path, int keepStaticOb
         b3_set_error("%s: %s", path, err.c_str());
         return B3_ERR_INVALID_ARG;
     }
-    // shapes in file order (convertCollisionShape :723-840): boxes and
-    // convex hulls; spheres, planes and the rest are skipped, as there
-    std::vector<uint64_t> shapePtr;
-    std::vector<int> shapeCol;
+    // Pass 1 reads and checks every record; nothing is registered unless
+    // the whole file is usable, so a failed load leaves the world as it was.
+    // Shapes in file order (convertCollisionShape :723-840): boxes and
+    // convex hulls; spheres, planes and the rest are skipped, as there.
+    std::vector<ShapeRec> shapes;
     for (const Chunk& c : F.chunks) {
         if (c.code != code4("SHAP")) continue;
         // a convex hull's record nests the convex-internal part
@@ -335,7 +350,8 @@ extern "C" int b3_load_bullet_file(b3World w, const char* path, int keepStaticOb
         const int stype = F.i32(c, (in + "m_collisionShapeData.m_shapeType").c_str());
         float scale[3];
         for (int k = 0; k < 3; ++k) scale[k] = F.f32(c, (in + "m_localScaling.m_floats").c_str(), k);
-        int col = -1;
+        ShapeRec r;
+        r.oldPtr = c.oldPtr;
         if (stype == kBoxShape && !hull) {
             // createBoxShape (:969-997): the unit cube scaled by
             // halfDimensions * localScaling + margin
@@ -343,61 +359,86 @@ extern "C" int b3_load_bullet_file(b3World w, const char* path, int keepStaticOb
             const float margin = F.f32(c, "m_collisionMargin");
             float he[3];
             for (int k = 0; k < 3; ++k) he[k] = F.f32(c, "m_implicitShapeDimensions.m_floats", k) * scale[k] + margin;
-            float corners[24];
             for (int i = 0; i < 8; ++i) {
-                corners[3 * i] = (i & 1) ? 1.f : -1.f;
-                corners[3 * i + 1] = (i & 2) ? 1.f : -1.f;
-                corners[3 * i + 2] = (i & 4) ? 1.f : -1.f;
+                r.points.push_back((i & 1) ? he[0] : -he[0]);
+                r.points.push_back((i & 2) ? he[1] : -he[1]);
+                r.points.push_back((i & 4) ? he[2] : -he[2]);
             }
-            const int rc = b3_register_convex_hull(w, corners, 8, 12, he, &col);
-            if (rc != B3_OK) return rc;
         } else if (stype == kConvexHullShape && hull) {
             // the points times localScaling (:757-787)
-            const int n = F.i32(c, "m_numUnscaledPoints");
+            const int64_t n = F.i32(c, "m_numUnscaledPoints");
             const Chunk* pts = F.chunk_at(F.ptr(c, "m_unscaledPointsFloatPtr"));
-            if (n < 4 || !pts || pts->length < 16 * n) {
+            if (n < 4 || !pts || (int64_t)pts->length < 16 * n) {
                 b3_set_error("%s: convex hull without its points", path);
                 return B3_ERR_INVALID_ARG;
             }
-            std::vector<float> p(3 * (size_t)n);
-            for (int i = 0; i < n; ++i)
+            if (n > kMaxFileHullPoints) {
+                b3_set_error("%s: convex hull of %lld points (at most %lld)", path, (long long)n,
+                             (long long)kMaxFileHullPoints);
+                return B3_ERR_CAPACITY;
+            }
+            r.points.resize(3 * (size_t)n);
+            for (int64_t i = 0; i < n; ++i)
                 for (int k = 0; k < 3; ++k) {
                     float v;
                     std::memcpy(&v, pts->data + 16 * i + 4 * k, 4);
-                    p[3 * i + k] = v * scale[k];
+                    r.points[3 * i + k] = v * scale[k];
                 }
-            const float unit[3] = {1.f, 1.f, 1.f};
-            const int rc = b3_register_convex_hull(w, p.data(), n, 12, unit, &col);
-            if (rc != B3_OK) return rc;
+        } else {
+            continue;
         }
-        if (col >= 0) {
-            shapePtr.push_back(c.oldPtr);
-            shapeCol.push_back(col);
+        // the same hull construction registration runs: a point set it
+        // refuses fails the load here, before anything is registered
+        b3hull::Polyhedron P;
+        std::string herr;
+        if (!b3hull::compute_polyhedron(r.points.data(), (int)(r.points.size() / 3), P, &herr)) {
+            b3_set_error("%s: convex hull: %s", path, herr.c_str());
+            return B3_ERR_INVALID_ARG;
         }
+        shapes.push_back(std::move(r));
     }
     // bodies grouped by shape, shapes in order, file order inside a group
     // (:614-666); mass 1 / inverseMass, friction 1 (registerRigidBody,
     // P1/btGpuNarrowPhaseAndSolver.cpp:577); static bodies only when kept
-    int count = 0;
-    for (size_t g = 0; g < shapePtr.size(); ++g) {
+    std::vector<BodyRec> bodies;
+    for (size_t g = 0; g < shapes.size(); ++g) {
         for (const Chunk& c : F.chunks) {
             if (c.code != code4("RBDY")) continue;
-            if (F.ptr(c, "m_collisionObjectData.m_collisionShape") != shapePtr[g]) continue;
+            if (F.ptr(c, "m_collisionObjectData.m_collisionShape") != shapes[g].oldPtr) continue;
             const float invMass = F.f32(c, "m_inverseMass");
             if (!keepStaticObjects && invMass == 0.f) continue;
             double r[3][3];
             for (int row = 0; row < 3; ++row)
                 for (int k = 0; k < 3; ++k)
                     r[row][k] = F.f32(c, "m_collisionObjectData.m_worldTransform.m_basis.m_el", 4 * row + k);
-            float q[4], pos[3];
-            basis_to_quat(r, q);
-            for (int k = 0; k < 3; ++k) pos[k] = F.f32(c, "m_collisionObjectData.m_worldTransform.m_origin.m_floats", k);
-            int body;
-            const int rc = b3_register_body(w, invMass == 0.f ? 0.f : 1.f / invMass, pos, q, shapeCol[g], 1.f, 0.f, 0,
-                                            &body);
-            if (rc != B3_OK) return rc;
-            ++count;
+            BodyRec b;
+            b.shape = (int)g;
+            b.mass = invMass == 0.f ? 0.f : 1.f / invMass;
+            basis_to_quat(r, b.quat);
+            for (int k = 0; k < 3; ++k) b.pos[k] = F.f32(c, "m_collisionObjectData.m_worldTransform.m_origin.m_floats", k);
+            bodies.push_back(b);
         }
+    }
+    const int64_t extra = keepStaticObjects ? 0 : 50 * 50;
+    if ((int64_t)w->bodies.size() + (int64_t)bodies.size() + extra > (int64_t)w->cfg.maxBodies) {
+        b3_set_error("%s: %lld bodies do not fit the world (capacity %d, %d registered)", path,
+                     (long long)(bodies.size() + extra), w->cfg.maxBodies, (int)w->bodies.size());
+        return B3_ERR_CAPACITY;
+    }
+    // Pass 2: register.
+    std::vector<int> shapeCol(shapes.size(), -1);
+    const float unit[3] = {1.f, 1.f, 1.f};
+    for (size_t g = 0; g < shapes.size(); ++g) {
+        const int rc = b3_register_convex_hull(w, shapes[g].points.data(), (int)(shapes[g].points.size() / 3), 12,
+                                               unit, &shapeCol[g]);
+        if (rc != B3_OK) return rc;
+    }
+    int count = 0;
+    for (const BodyRec& b : bodies) {
+        int body;
+        const int rc = b3_register_body(w, b.mass, b.pos, b.quat, shapeCol[b.shape], 1.f, 0.f, 0, &body);
+        if (rc != B3_OK) return rc;
+        ++count;
     }
     if (!keepStaticObjects) {
         // the demo's replacement ground: 50 x 50 static tiles, an inverted

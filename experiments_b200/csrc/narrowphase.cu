@@ -59,6 +59,10 @@ constexpr int kSepReduceTie = 3;   // FP32 axis and clip, reduction tie
 struct NpParams {
     float minDist;
     float maxDist;
+    // depth above which the solver skips a point (contactProcessing -
+    // slopOffset, btPgsJacobiSolver.cpp:961): a depth this close to it in
+    // FP32 is a decision in doubt as well
+    float skipDist;
     int frictionCombine;
     int maxPairs;
 };
@@ -936,7 +940,8 @@ __device__ __noinline__ int clip_f32(const PairCtx& c, const b3::ShapesDev& S, c
         if (k < nIn) {
             p = get_f32(W.poly[cur][k]);
             depth = dot(nAw, p) + fA.plane[3];
-            if (fabsf(depth - P.maxDist) <= 5e-7f * (1.f + len_ub(p))) bad = true;
+            const float eb = 5e-7f * (1.f + len_ub(p));
+            if (fabsf(depth - P.maxDist) <= eb || fabsf(depth - P.skipDist) <= eb) bad = true;
             if (depth <= P.minDist) depth = P.minDist;
             keep = depth <= P.maxDist;
         }
@@ -1568,6 +1573,7 @@ int launch_narrowphase(b3World_t* w, cudaStream_t st) {
     NpParams P;
     P.minDist = -1e30f;
     P.maxDist = w->sim.contactBreaking;
+    P.skipDist = (float)((double)w->sim.contactProcessing - (double)w->sim.slopOffset);
     P.frictionCombine = w->sim.frictionCombine;
     P.maxPairs = w->cfg.maxPairs;
     const int threads = 32 * w->npWarpsPerBlock;
@@ -1598,21 +1604,28 @@ int launch_narrowphase(b3World_t* w, cudaStream_t st) {
     int occS = 1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occS, sweep, threads, smemSweep) != cudaSuccess || occS < 1)
         occS = 1;
+    // per-kernel events only in eagerly timed steps (never inside a capture)
+    const bool tk = w->timing && w->npEv[0] != nullptr;
+    if (tk) B3_CUDA(cudaEventRecord(w->npEv[0], st));
     sweep<<<w->ctx->numSMs * occS, threads, smemSweep, st>>>(
         w->d.pairs, sc + S_NUM_PAIRS, Bd, S, w->d.manifoldFlag, w->d.pairSep, w->d.npFast, w->d.npSlow,
         w->d.npCand, std::min(w->cfg.maxPairs, kNpCandSlots), sc, w->d.counters);
     B3_CHECK_LAUNCH();
+    if (tk) B3_CUDA(cudaEventRecord(w->npEv[1], st));
     k_np_refine<<<grid_of((const void*)k_np_refine), threads, smem, st>>>(
         w->d.pairs, Bd, S, w->d.pairSep, w->d.npFast, w->d.npSlow, w->d.npCand, w->d.manifoldFlag, sc, w->d.counters);
     B3_CHECK_LAUNCH();
+    if (tk) B3_CUDA(cudaEventRecord(w->npEv[2], st));
     k_np_clip<<<grid_of((const void*)k_np_clip), threads, smem, st>>>(
         w->d.pairs, Bd, S, P, w->d.pairSep, w->d.npFast, w->d.npSlow, w->d.contacts, w->d.manifoldFlag, sc,
         w->d.counters);
     B3_CHECK_LAUNCH();
+    if (tk) B3_CUDA(cudaEventRecord(w->npEv[3], st));
     k_np_exact<<<grid_of((const void*)k_np_exact), threads, smem, st>>>(
         w->d.pairs, Bd, S, P, w->d.pairSep, w->d.npSlow, w->d.npCand, w->d.contacts, w->d.manifoldFlag, sc,
         w->d.counters);
     B3_CHECK_LAUNCH();
+    if (tk) B3_CUDA(cudaEventRecord(w->npEv[4], st));
     return B3_OK;
 }
 

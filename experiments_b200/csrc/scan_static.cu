@@ -14,7 +14,11 @@
 //   * the array lives on every GPU that loads the library, until exit;
 //   * every call on a device uses the same array, and the array keeps the
 //     last call's contents; each call clears the parts that must start at
-//     zero (tile counter, tile status words, error flag) before the scan;
+//     zero (tile counter, tile status words, error flag, total) on the
+//     stream before the scan, with a set-up kernel that takes n by value;
+//   * the scan's look-back waits are bounded; a wait that gives up sets the
+//     array's error flag, which the call copies to the caller's d_err
+//     (1 = the result is not valid, 0 = a valid scan);
 //   * two calls whose work overlaps on the GPU (different streams, or
 //     different host threads) race on the array and give wrong results;
 //     serialise them on one stream;
@@ -64,10 +68,23 @@ int static_scratch(int dev, void** ptr, int* sms) {
     return B3_OK;
 }
 
+// Writes n and clears the error flag and the total (header words 0, 1, 2).
+__global__ void k_static_scan_begin(int32_t* hdr, int32_t n) {
+    hdr[0] = n;
+    hdr[1] = 0;
+    hdr[2] = 0;
+}
+
+// Copies the total and the error flag out of the array to the caller.
+__global__ void k_static_scan_end(const int32_t* hdr, uint32_t* d_sum, int32_t* d_err) {
+    if (d_sum) *d_sum = (uint32_t)hdr[2];
+    if (d_err) *d_err = hdr[1] != 0 ? 1 : 0;
+}
+
 }  // namespace
 
 extern "C" int b3_prefix_scan_u32_static(const uint32_t* d_src, uint32_t* d_dst, int64_t n, uint32_t* d_sum,
-                                         void* stream) {
+                                         int32_t* d_err, void* stream) {
     if (n < 0 || (n > 0 && (!d_src || !d_dst))) return B3_ERR_INVALID_ARG;
     if (n > kStaticScanMaxN) {
         b3_set_error("b3_prefix_scan_u32_static: n = %lld exceeds the static limit of %lld elements",
@@ -86,9 +103,12 @@ extern "C" int b3_prefix_scan_u32_static(const uint32_t* d_src, uint32_t* d_dst,
     uint32_t* total = (uint32_t*)(b + 8);
     void* body = b + kHeaderBytes;
     const size_t body_bytes = kStaticScanBytes - kHeaderBytes;
-    const int32_t hv[3] = {(int32_t)n, 0, 0};  // n, cleared error flag, cleared total
-    B3_CUDA(cudaMemcpyAsync(b, hv, sizeof(hv), cudaMemcpyHostToDevice, st));
+    k_static_scan_begin<<<1, 1, 0, st>>>(n_dev, (int32_t)n);
+    B3_CHECK_LAUNCH();
     B3_TRY(b3::exclusive_scan_u32(d_src, d_dst, n_dev, n, total, body, body_bytes, err, st, sms));
-    if (d_sum) B3_CUDA(cudaMemcpyAsync(d_sum, total, sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+    if (d_sum || d_err) {
+        k_static_scan_end<<<1, 1, 0, st>>>(n_dev, d_sum, d_err);
+        B3_CHECK_LAUNCH();
+    }
     return B3_OK;
 }

@@ -539,6 +539,7 @@ int launch_solver_taped(b3World_t* w, cudaStream_t st, const JacobiTape* tape) {
     const int g = w->ctx->numSMs * 8;
     k_setup_rows<<<g, 128, 0, st>>>(w->bodiesDev(), V, w->d.manifoldPair, w->d.contacts, SP);
     B3_CHECK_LAUNCH();
+    if (w->timing && w->setupEv) B3_CUDA(cudaEventRecord(w->setupEv, st));
     if (w->solverMode == 1 && w->cfg.numWorlds > 1) {
         // one block per world at a time, block barriers between phases
         const int nw = w->cfg.numWorlds;

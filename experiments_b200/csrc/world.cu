@@ -654,6 +654,8 @@ static int run_one_step(b3World w, cudaStream_t st) { return b3::run_step(w, st,
 static int run_one_step_timed(b3World w, cudaStream_t st) {
     cudaEvent_t ev[9];
     for (auto& e : ev) B3_CUDA(cudaEventCreate(&e));
+    for (auto& e : w->npEv) B3_CUDA(cudaEventCreate(&e));
+    B3_CUDA(cudaEventCreate(&w->setupEv));
     B3_CUDA(cudaEventRecord(ev[0], st));
     B3_TRY(step_begin(w, st));
     B3_TRY(b3::launch_aabb_hash(w, st));
@@ -671,9 +673,24 @@ static int run_one_step_timed(b3World w, cudaStream_t st) {
     B3_TRY(b3::launch_integrate(w, st));
     B3_CUDA(cudaEventRecord(ev[7], st));
     B3_CUDA(cudaEventSynchronize(ev[7]));
-    w->stageMs.assign(7, 0.f);
+    // 7 stages, the narrowphase's four kernels (sweep, refine, clip, exact),
+    // then the Jacobi solve's row setup and its iterations
+    w->stageMs.assign(13, 0.f);
     for (int k = 0; k < 7; ++k) cudaEventElapsedTime(&w->stageMs[k], ev[k], ev[k + 1]);
+    if (w->cfg.maxPairs > 0 && !w->bodies.empty()) {
+        for (int k = 0; k < 4; ++k) cudaEventElapsedTime(&w->stageMs[7 + k], w->npEv[k], w->npEv[k + 1]);
+        if (!w->gs) {
+            cudaEventElapsedTime(&w->stageMs[11], ev[5], w->setupEv);
+            cudaEventElapsedTime(&w->stageMs[12], w->setupEv, ev[6]);
+        }
+    }
     for (auto& e : ev) cudaEventDestroy(e);
+    for (auto& e : w->npEv) {
+        cudaEventDestroy(e);
+        e = nullptr;
+    }
+    cudaEventDestroy(w->setupEv);
+    w->setupEv = nullptr;
     return B3_OK;
 }
 

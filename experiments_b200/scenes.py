@@ -324,3 +324,21 @@ def select_worlds(scene, world_ids):
     cfg.pop("maxPairs", None)
     return Scene(name=f"{scene.name}_sel{len(world_ids)}", shapes=scene.shapes, num_worlds=len(world_ids),
                  config=cfg, steps=scene.steps, **b)
+
+
+def lattice_block(scene, dims, block, blocks=(4, 4)):
+    """Sub-scene of a lattice scene: the static ground plus the column of
+    bodies whose lattice x and z indices fall in block `block` of a
+    blocks[0] x blocks[1] tiling of the footprint (all layers). The blocks
+    tile the scene, so running every block covers every body once."""
+    nx, ny, nz = dims
+    bx, bz = nx // blocks[0], nz // blocks[1]
+    ix, iy, iz = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    ix, iz = ix.ravel(), iz.ravel()
+    x0, z0 = (block // blocks[1]) * bx, (block % blocks[1]) * bz
+    sel = (ix >= x0) & (ix < x0 + bx) & (iz >= z0) & (iz < z0 + bz)
+    idx = np.concatenate([[0], 1 + np.nonzero(sel)[0]])  # body 0 is the ground
+    b = dict(shape=scene.shape[idx], mass=scene.mass[idx], pos=scene.pos[idx], quat=scene.quat[idx],
+             friction=scene.friction[idx], world=scene.world[idx], lin=scene.lin[idx], ang=scene.ang[idx])
+    return Scene(name=f"{scene.name}_block{block}", shapes=scene.shapes, num_worlds=1, config=dict(scene.config),
+                 steps=scene.steps, **b)

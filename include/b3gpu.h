@@ -193,9 +193,11 @@ int b3_prefix_scan_u32(b3Context ctx, const uint32_t* d_src, uint32_t* d_dst, in
  * a device share that array: calls that overlap on the GPU race, so keep
  * them on one stream. The first call on a device looks up the array's
  * address; make it before any stream capture. The total goes to d_sum
- * (device, may be NULL). */
+ * (device, may be NULL). d_err (device, may be NULL) receives 0 after a
+ * valid scan and 1 if a bounded wait inside the scan gave up, in which case
+ * d_dst and d_sum are not valid. */
 int b3_prefix_scan_u32_static(const uint32_t* d_src, uint32_t* d_dst, int64_t n, uint32_t* d_sum,
-                              void* stream);
+                              int32_t* d_err, void* stream);
 
 /* btRadixSort32CL::execute (BB/btRadixSort32CL.cpp:161-535): stable LSD
  * key-value sort of n (key, value) pairs, in place. Only the low key_bits
@@ -331,7 +333,11 @@ int b3_register_body(b3World w, float mass, const float position[3], const float
  * friction 1 (registerRigidBody, P1/btGpuNarrowPhaseAndSolver.cpp:577).
  * Static bodies are dropped unless keepStaticObjects, and then, as the demo
  * does, a 50 x 50 grid of static ground tiles is added. Call before
- * b3_write_bodies; *numBodiesOut = bodies added. */
+ * b3_write_bodies; *numBodiesOut = bodies added. The whole file is read and
+ * checked before anything is registered: a file that fails (truncated or
+ * inconsistent records, a degenerate hull, a hull record of more than 65,536
+ * points, more bodies than the world's capacity) returns an error and leaves
+ * the world as it was. */
 int b3_load_bullet_file(b3World w, const char* path, int keepStaticObjects, int* numBodiesOut);
 
 /* Bulk form of b3_register_body for n bodies (arrays of n, xyz / xyzw
@@ -433,7 +439,11 @@ enum {
 };
 int b3_get_device_buffer(b3World w, int which, void** d_ptr, int64_t* bytes);
 
-/* CUDA-event timing of each stage of the last timed step (ms). */
+/* CUDA-event timing of each stage of the last timed step (ms): 13 values,
+ * the 7 stages (AABB + hash, cell sort, pair search, narrowphase, manifolds,
+ * solve, integrate), the narrowphase's 4 kernels (separating-axis sweep,
+ * float-float ranking, FP32 clip, float-float path), then the Jacobi
+ * solve's row setup and its iterations (0 for the Gauss-Seidel solver). */
 int b3_set_stage_timing(b3World w, int enable);
 int b3_get_stage_times(b3World w, float* ms, int max, int* count);
 

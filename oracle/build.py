@@ -19,7 +19,8 @@ LIB_F32 = os.path.join(HERE, "liboracle_f32.so")
 LIB_DUAL = os.path.join(HERE, "liboracle_dual.so")
 REF_LIB = os.path.join(HERE, "_ref", "libb3ref.so")
 BULLET_LIB = os.path.join(HERE, "_ref", "libb3bullet.so")
-REFERENCE = "/root/reference"
+# the reference tree; B3_REFERENCE_ROOT overrides the default location
+REFERENCE = os.environ.get("B3_REFERENCE_ROOT", "/root/reference")
 
 # Reference sources compiled for the pins (paths relative to the reference root).
 REF_SOURCES = [

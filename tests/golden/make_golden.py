@@ -73,7 +73,8 @@ import struct
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REFERENCE = "/root/reference"
+# the reference tree; B3_REFERENCE_ROOT overrides the default location
+REFERENCE = os.environ.get("B3_REFERENCE_ROOT", "/root/reference")
 
 
 def _num(b, i):

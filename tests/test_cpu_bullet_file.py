@@ -127,3 +127,53 @@ def test_loaded_file_steps_on_the_device(ctx):
     assert np.abs(lin[dyn, :3]).max() < 1.0
     assert w.counters()["timeouts"] == 0
     w.close()
+
+
+def _hull_count_offsets(raw):
+    """Byte offsets of m_numUnscaledPoints in the file's convex hull shape
+    records (64-bit pointers, little endian): a chunk header is code, length,
+    old pointer (8), struct index, count; btConvexHullShapeData holds the
+    convex-internal part (56 bytes: name pointer, shape type, padding,
+    scaling, dimensions, margin, padding), two point pointers, then the
+    count."""
+    out, o = [], 12
+    while o + 24 <= len(raw):
+        code = bytes(raw[o:o + 4])
+        length = int.from_bytes(raw[o + 4:o + 8], "little")
+        data = o + 24
+        if code == b"ENDB":
+            break
+        if code == b"SHAP" and int.from_bytes(raw[data + 8:data + 12], "little") == 4:
+            out.append(data + 72)
+        o = data + length
+    return out
+
+
+@pytest.mark.parametrize("count", [100, 0x10000000, 1 << 20])
+def test_hull_point_counts_are_checked_before_anything_registers(host_ctx, tmp_path, count):
+    """A hull record whose point count exceeds its point data (100), whose
+    byte size overflows 32-bit arithmetic (2^28 points x 16 bytes = 2^32) or
+    exceeds the 65,536-point limit is refused, and the world is left with
+    nothing registered."""
+    raw = bytearray(open(FILE, "rb").read())
+    offs = _hull_count_offsets(raw)
+    assert offs and all(int.from_bytes(raw[o:o + 4], "little") == 12 for o in offs)
+    raw[offs[-1]:offs[-1] + 4] = int(count).to_bytes(4, "little")
+    bad = tmp_path / "corrupt.bullet"
+    bad.write_bytes(bytes(raw))
+    w = _world(host_ctx, 3000)
+    with pytest.raises(b3.B3Error):
+        w.load_bullet_file(str(bad), keep_static_objects=False)
+    assert w.n == 0 and w.shapes()["counts"][:2] == (0, 0)
+    # the intact file still loads into the same world afterwards
+    assert w.load_bullet_file(FILE, keep_static_objects=True) == w.n > 0
+    w.close()
+
+
+def test_a_file_that_does_not_fit_registers_nothing(host_ctx):
+    g = np.load(os.path.join(GOLDEN, "pile_bullet.npz"))
+    w = _world(host_ctx, len(g["mass"]) - 1)
+    with pytest.raises(b3.B3Error):
+        w.load_bullet_file(FILE, keep_static_objects=True)
+    assert w.n == 0 and w.shapes()["counts"][:2] == (0, 0)
+    w.close()

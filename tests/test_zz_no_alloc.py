@@ -35,11 +35,15 @@ def test_static_scan_matches_allocating_scan_twice(ctx):
         ref = _dev(np.zeros(n, np.uint32))
         out = _dev(np.full(n, 0xFFFFFFFF, np.uint32))
         dsum = _dev(np.zeros(1, np.uint32))
+        # the error flag comes back 0 after a valid scan (set to 7 first so a
+        # call that never writes it would show)
+        derr = _dev(np.full(1, 7, np.uint32))
         total_ref = b3.PrefixScan(ctx).execute(src, ref)
         rc = lib.b3_prefix_scan_u32_static(C.c_void_p(src.data_ptr()), C.c_void_p(out.data_ptr()), n,
-                                           C.c_void_p(dsum.data_ptr()), None)
+                                           C.c_void_p(dsum.data_ptr()), C.c_void_p(derr.data_ptr()), None)
         assert rc == 0, lib.b3_last_error()
         torch.cuda.synchronize()
+        assert int(derr.cpu().numpy()[0]) == 0
         got = out.cpu().numpy().view(np.uint32)
         want = ref.cpu().numpy().view(np.uint32)
         assert np.array_equal(got, want)
@@ -48,6 +52,6 @@ def test_static_scan_matches_allocating_scan_twice(ctx):
 
 def test_static_scan_rejects_oversized_input(ctx):
     lib = b3.load()
-    rc = lib.b3_prefix_scan_u32_static(C.c_void_p(16), C.c_void_p(16), (1 << 24) + 1, None, None)
+    rc = lib.b3_prefix_scan_u32_static(C.c_void_p(16), C.c_void_p(16), (1 << 24) + 1, None, None, None)
     assert rc == 3  # B3_ERR_CAPACITY, nothing launched
     assert b"exceeds the static limit" in lib.b3_last_error()
