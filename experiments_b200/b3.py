@@ -124,6 +124,9 @@ SIGNATURES = [
     ("b3_radix_sort32_kv", _I, [_P, _P, _P, _I64, _I, _P]),
     ("b3_radix_sort32_keys", _I, [_P, _P, _I64, _I, _P]),
     ("b3_bound_search", _I, [_P, _P, _I64, _P, _I64, _I, _P]),
+    ("b3_radix_sort32_kv_out", _I, [_P, _P, _P, _P, _P, _I64, _I, _P]),
+    ("b3_radix_sort32_sortdata", _I, [_P, _P, _I64, _I, _P]),
+    ("b3_bound_search_sortdata", _I, [_P, _P, _I64, _P, _I64, _I, _P]),
     ("b3_world_config_default", None, [C.POINTER(WorldConfig)]),
     ("b3_world_create", _I, [_P, C.POINTER(WorldConfig), C.POINTER(_P)]),
     ("b3_world_destroy", _I, [_P]),
@@ -253,7 +256,7 @@ class Context:
 # Primitive objects (device pointers are torch CUDA tensors)
 # ---------------------------------------------------------------------------
 def _dptr(t):
-    return C.c_void_p(t.data_ptr())
+    return None if t is None else C.c_void_p(t.data_ptr())
 
 
 class Fill:
@@ -301,6 +304,19 @@ class RadixSort32:
             _check(self.ctx.lib.b3_radix_sort32_kv(self.ctx.h, _dptr(keys), _dptr(values), n, key_bits,
                                                    _stream(stream)), "b3_radix_sort32_kv")
 
+    def execute_out(self, keys_in, keys_out, values_in=None, values_out=None, n=None, key_bits=32, stream=None):
+        """execute(keysIn, keysOut, valuesIn, valuesOut, n, sortBits): out of place."""
+        n = keys_in.numel() if n is None else n
+        _check(self.ctx.lib.b3_radix_sort32_kv_out(self.ctx.h, _dptr(keys_in), _dptr(keys_out), _dptr(values_in),
+                                                   _dptr(values_out), n, key_bits, _stream(stream)),
+               "b3_radix_sort32_kv_out")
+
+    def execute_sortdata(self, key_values, n=None, key_bits=32, stream=None):
+        """execute(btOpenCLArray<btSortData>&, sortBits): (n, 2) int32 records in place."""
+        n = key_values.shape[0] if n is None else n
+        _check(self.ctx.lib.b3_radix_sort32_sortdata(self.ctx.h, _dptr(key_values), n, key_bits, _stream(stream)),
+               "b3_radix_sort32_sortdata")
+
 
 class SapPairs:
     """computePairsKernel (BB/sapFast.cl:48-150) on caller-sorted device
@@ -327,6 +343,11 @@ class BoundSearch:
     def execute(self, sorted_keys, n_src, dst, n_dst, mode, stream=None):
         _check(self.ctx.lib.b3_bound_search(self.ctx.h, _dptr(sorted_keys), n_src, _dptr(dst), n_dst, mode,
                                             _stream(stream)), "b3_bound_search")
+
+    def execute_sortdata(self, sorted_key_values, n_src, dst, n_dst, mode=0, stream=None):
+        """execute(btOpenCLArray<btSortData>& src, nSrc, dst, nDst, option)."""
+        _check(self.ctx.lib.b3_bound_search_sortdata(self.ctx.h, _dptr(sorted_key_values), n_src, _dptr(dst), n_dst,
+                                                     mode, _stream(stream)), "b3_bound_search_sortdata")
 
 
 # ---------------------------------------------------------------------------

@@ -191,6 +191,58 @@ extern "C" int b3_radix_sort32_keys(b3Context ctx, uint32_t* d_keys, int64_t n, 
     return sort_impl(ctx, d_keys, nullptr, n, key_bits, stream);
 }
 
+extern "C" int b3_radix_sort32_kv_out(b3Context ctx, const uint32_t* d_keys_in, uint32_t* d_keys_out,
+                                      const uint32_t* d_values_in, uint32_t* d_values_out, int64_t n, int key_bits,
+                                      void* stream) {
+    if (!ctx || n < 0 || n > (int64_t)0x3fffffff || key_bits < 1 || key_bits > 32 ||
+        (n > 0 && (!d_keys_in || !d_keys_out)) || (n > 0 && (d_values_in == nullptr) != (d_values_out == nullptr)))
+        return B3_ERR_INVALID_ARG;
+    if (d_keys_in == d_keys_out || (d_values_in && d_values_in == d_values_out)) {
+        b3_set_error("b3_radix_sort32_kv_out: the outputs must not be the inputs (use b3_radix_sort32_kv)");
+        return B3_ERR_INVALID_ARG;
+    }
+    if (ctx->device < 0) return B3_ERR_NO_DEVICE;
+    if (n == 0) return B3_OK;
+    cudaStream_t st = as_stream(stream);
+    if (n == 1) {
+        B3_CUDA(cudaMemcpyAsync(d_keys_out, d_keys_in, 4, cudaMemcpyDeviceToDevice, st));
+        if (d_values_in) B3_CUDA(cudaMemcpyAsync(d_values_out, d_values_in, 4, cudaMemcpyDeviceToDevice, st));
+        return B3_OK;
+    }
+    const size_t rb = b3::radix_scratch_bytes(n, key_bits);
+    const size_t alt = ((size_t)n * 4 + 255) / 256 * 256;
+    int32_t *n_dev, *err;
+    void* body;
+    B3_TRY(prim_scratch(ctx, rb + 2 * alt, n, st, &n_dev, &err, &body));
+    uint32_t* ktmp = (uint32_t*)((unsigned char*)body + rb);
+    uint32_t* vtmp = d_values_in ? (uint32_t*)((unsigned char*)body + rb + alt) : nullptr;
+    return b3::radix_sort_kv_out(d_keys_in, d_values_in, d_keys_out, d_values_out, ktmp, vtmp, n_dev, n, key_bits,
+                                 body, rb, err, st, ctx->numSMs);
+}
+
+extern "C" int b3_radix_sort32_sortdata(b3Context ctx, int32_t* d_key_values, int64_t n, int key_bits,
+                                        void* stream) {
+    if (!ctx || n < 0 || n > (int64_t)0x3fffffff || key_bits < 1 || key_bits > 32 || (n > 0 && !d_key_values))
+        return B3_ERR_INVALID_ARG;
+    if (((uintptr_t)d_key_values & 7) != 0) {
+        b3_set_error("b3_radix_sort32_sortdata: the (key, value) array must be 8-byte aligned");
+        return B3_ERR_INVALID_ARG;
+    }
+    if (ctx->device < 0) return B3_ERR_NO_DEVICE;
+    if (n <= 1) return B3_OK;
+    cudaStream_t st = as_stream(stream);
+    const size_t rb = b3::radix_scratch_bytes(n, key_bits);
+    int32_t *n_dev, *err;
+    void* body;
+    B3_TRY(prim_scratch(ctx, rb + 8 * (size_t)n, n, st, &n_dev, &err, &body));
+    uint2* kv = reinterpret_cast<uint2*>(d_key_values);
+    uint2* alt = (uint2*)((unsigned char*)body + rb);  // rb is a multiple of 256
+    bool in_alt = false;
+    B3_TRY(b3::radix_sort_interleaved(kv, alt, n_dev, n, key_bits, body, rb, err, st, &in_alt, ctx->numSMs));
+    if (in_alt) B3_CUDA(cudaMemcpyAsync(kv, alt, 8 * (size_t)n, cudaMemcpyDeviceToDevice, st));
+    return B3_OK;
+}
+
 extern "C" int b3_bound_search(b3Context ctx, const uint32_t* d_sorted_keys, int64_t n_src,
                                uint32_t* d_dst, int64_t n_dst, int mode, void* stream) {
     if (!ctx || n_src < 0 || n_dst < 0 || mode < 0 || mode > 2 || (n_src > 0 && !d_sorted_keys) ||
@@ -204,4 +256,20 @@ extern "C" int b3_bound_search(b3Context ctx, const uint32_t* d_sorted_keys, int
     void* body;
     B3_TRY(prim_scratch(ctx, 0, n_src, st, &n_dev, &err, &body));
     return b3::bound_search(d_sorted_keys, n_dev, n_src, d_dst, n_dst, mode, st);
+}
+
+extern "C" int b3_bound_search_sortdata(b3Context ctx, const int32_t* d_sorted_key_values, int64_t n_src,
+                                        uint32_t* d_dst, int64_t n_dst, int mode, void* stream) {
+    if (!ctx || n_src < 0 || n_dst < 0 || mode < 0 || mode > 2 || (n_src > 0 && !d_sorted_key_values) ||
+        (n_dst > 0 && !d_dst) || n_src > (int64_t)0x7fffffff || ((uintptr_t)d_sorted_key_values & 7) != 0)
+        return B3_ERR_INVALID_ARG;
+    if (ctx->device < 0) return B3_ERR_NO_DEVICE;
+    cudaStream_t st = as_stream(stream);
+    if (mode == 2) B3_TRY(b3::fill_u32(d_dst, 0u, n_dst, st));
+    if (n_src == 0) return B3_OK;
+    int32_t *n_dev, *err;
+    void* body;
+    B3_TRY(prim_scratch(ctx, 0, n_src, st, &n_dev, &err, &body));
+    return b3::bound_search_interleaved(reinterpret_cast<const uint2*>(d_sorted_key_values), n_dev, n_src, d_dst,
+                                        n_dst, mode, st);
 }

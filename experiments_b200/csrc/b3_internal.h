@@ -68,6 +68,18 @@ int radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_
                      size_t scratch_bytes, int32_t* err_flag, cudaStream_t st, bool* result_in_alt,
                      int numSMs);
 
+// Out-of-place sort: (keys_in, vals_in) are only read; the sorted result
+// lands in (keys_out, vals_out); (keys_tmp, vals_tmp) hold the passes in
+// between (unused for one pass). vals_in may be null (keys only).
+int radix_sort_kv_out(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out,
+                      uint32_t* keys_tmp, uint32_t* vals_tmp, const int32_t* n_dev, int64_t n_max, int key_bits,
+                      void* scratch, size_t scratch_bytes, int32_t* err_flag, cudaStream_t st, int numSMs);
+// Interleaved (key, value) pairs (btSortData): result in kv_alt when
+// *result_in_alt, else in kv.
+int radix_sort_interleaved(uint2* kv, uint2* kv_alt, const int32_t* n_dev, int64_t n_max, int key_bits,
+                           void* scratch, size_t scratch_bytes, int32_t* err_flag, cudaStream_t st,
+                           bool* result_in_alt, int numSMs);
+
 size_t scan_scratch_bytes(int64_t n_max);
 // Exclusive scan of n_dev u32 values; total to d_total (may be null).
 int exclusive_scan_u32(const uint32_t* src, uint32_t* dst, const int32_t* n_dev, int64_t n_max,
@@ -77,6 +89,8 @@ int exclusive_scan_u32(const uint32_t* src, uint32_t* dst, const int32_t* n_dev,
 int fill_u32(uint32_t* dst, uint32_t v, int64_t n, cudaStream_t st);
 int bound_search(const uint32_t* keys, const int32_t* n_dev, int64_t n_max, uint32_t* dst,
                  int64_t n_dst, int mode, cudaStream_t st);
+int bound_search_interleaved(const uint2* kv, const int32_t* n_dev, int64_t n_max, uint32_t* dst, int64_t n_dst,
+                             int mode, cudaStream_t st);
 
 }  // namespace b3
 

@@ -83,6 +83,16 @@ __global__ void k_fill_int2(int2* __restrict__ dst, int2 v, int64_t n) {
 // ---------------------------------------------------------------------------
 // Radix sort: one-read histogram for all passes
 // ---------------------------------------------------------------------------
+// Key i of a sort input: split arrays hold the keys contiguously; the
+// interleaved form (btSortData, BB/btRadixSort32CL.h:7-11) holds (key, value)
+// pairs, key first.
+template <bool kPairs>
+__device__ __forceinline__ uint32_t sort_key(const uint32_t* __restrict__ keys, int64_t i) {
+    if (kPairs) return reinterpret_cast<const uint2*>(keys)[i].x;
+    return keys[i];
+}
+
+template <bool kPairs>
 __global__ void __launch_bounds__(kSortThreads)
 k_radix_histogram(const uint32_t* __restrict__ keys, const int32_t* n_dev, int passes,
                   uint32_t* __restrict__ ghist /* [passes][256] */) {
@@ -94,7 +104,7 @@ k_radix_histogram(const uint32_t* __restrict__ keys, const int32_t* n_dev, int p
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
          i < ((int64_t)n + 31) / 32 * 32; i += stride) {
         const bool valid = i < n;
-        const uint32_t k = valid ? keys[i] : 0u;
+        const uint32_t k = valid ? sort_key<kPairs>(keys, i) : 0u;
         for (int p = 0; p < passes; ++p) {
             const uint32_t d = valid ? ((k >> (8 * p)) & 0xFFu) : 0x100u;
             const uint32_t peers = __match_any_sync(0xffffffffu, d);
@@ -122,6 +132,9 @@ struct SortSmem {
     int tile;
 };
 
+// kPairs: keys_in / keys_out hold interleaved (key, value) pairs and the
+// value pointers are unused.
+template <bool kPairs>
 __global__ void __launch_bounds__(kSortThreads)
 k_onesweep_pass(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                 uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out,
@@ -133,7 +146,7 @@ k_onesweep_pass(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict
     const int n = dev_n(n_dev);
     const int num_tiles = (n + kSortTile - 1) / kSortTile;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const bool has_vals = vals_in != nullptr;
+    const bool has_vals = kPairs || vals_in != nullptr;
 
     for (;;) {
         if (threadIdx.x == 0) S.tile = atomicAdd(tile_counter, 1);
@@ -154,8 +167,14 @@ k_onesweep_pass(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict
         for (int i = 0; i < kSortItems; ++i) {
             const int idx = warp * 32 * kSortItems + i * 32 + lane;
             if (idx < tile_n) {
-                k[i] = keys_in[tile_base + idx];
-                v[i] = has_vals ? vals_in[tile_base + idx] : 0u;
+                if (kPairs) {
+                    const uint2 kv = reinterpret_cast<const uint2*>(keys_in)[tile_base + idx];
+                    k[i] = kv.x;
+                    v[i] = kv.y;
+                } else {
+                    k[i] = keys_in[tile_base + idx];
+                    v[i] = has_vals ? vals_in[tile_base + idx] : 0u;
+                }
             } else {
                 k[i] = 0xFFFFFFFFu;
                 v[i] = 0u;
@@ -236,8 +255,12 @@ k_onesweep_pass(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict
             const uint32_t kk = S.keys[j];
             const uint32_t dd = (kk >> shift) & 0xFFu;
             const uint32_t dst = S.gbase[dd] + (j - S.tileStart[dd]);
-            keys_out[dst] = kk;
-            if (has_vals) vals_out[dst] = S.vals[j];
+            if (kPairs) {
+                reinterpret_cast<uint2*>(keys_out)[dst] = make_uint2(kk, S.vals[j]);
+            } else {
+                keys_out[dst] = kk;
+                if (has_vals) vals_out[dst] = S.vals[j];
+            }
         }
         __syncthreads();
     }
@@ -335,37 +358,45 @@ __global__ void k_scan_empty_total(const int32_t* n_dev, uint32_t* d_total) {
 // ---------------------------------------------------------------------------
 // Bound search over sorted keys
 // ---------------------------------------------------------------------------
+// kPairs: the sorted input is interleaved (key, value) pairs (btSortData).
+template <bool kPairs>
 __global__ void k_bound_lower(const uint32_t* __restrict__ keys, const int32_t* n_dev,
                               uint32_t* __restrict__ dst, int64_t n_dst) {
     const int n = dev_n(n_dev);
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t k = keys[i];
-        if ((i == 0 || keys[i - 1] != k) && k < (uint64_t)n_dst) dst[k] = (uint32_t)i;
+        const uint32_t k = sort_key<kPairs>(keys, i);
+        if ((i == 0 || sort_key<kPairs>(keys, i - 1) != k) && k < (uint64_t)n_dst) dst[k] = (uint32_t)i;
     }
 }
+// kPairs also follows SearchSortDataUpperKernel (PR/Search/BoundSearchKernels.cl:66-86)
+// where no key 0 is present: its first work item compares the first key
+// with 0 and writes dst[0] = 0.
+template <bool kPairs>
 __global__ void k_bound_upper(const uint32_t* __restrict__ keys, const int32_t* n_dev,
                               uint32_t* __restrict__ dst, int64_t n_dst) {
     const int n = dev_n(n_dev);
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t k = keys[i];
-        if ((i == n - 1 || keys[i + 1] != k) && k < (uint64_t)n_dst) dst[k] = (uint32_t)(i + 1);
+        const uint32_t k = sort_key<kPairs>(keys, i);
+        if ((i == n - 1 || sort_key<kPairs>(keys, i + 1) != k) && k < (uint64_t)n_dst) dst[k] = (uint32_t)(i + 1);
+        if (kPairs && i == 0 && k != 0u && n_dst > 0) dst[0] = 0u;
     }
 }
+template <bool kPairs>
 __global__ void k_bound_count(const uint32_t* __restrict__ keys, const int32_t* n_dev,
                               uint32_t* __restrict__ dst, int64_t n_dst) {
     const int n = dev_n(n_dev);
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t k = keys[i];
-        if ((i == 0 || keys[i - 1] != k) && k < (uint64_t)n_dst) {
+        const uint32_t k = sort_key<kPairs>(keys, i);
+        if ((i == 0 || sort_key<kPairs>(keys, i - 1) != k) && k < (uint64_t)n_dst) {
             int64_t j = i;
             // run length by binary search for the first index with a larger key
             int64_t lo = i + 1, hi = n;
             while (lo < hi) {
                 int64_t mid = (lo + hi) >> 1;
-                if (keys[mid] == k) lo = mid + 1; else hi = mid;
+                if (sort_key<kPairs>(keys, mid) == k) lo = mid + 1; else hi = mid;
             }
             dst[k] = (uint32_t)(lo - j);
         }
@@ -391,10 +422,13 @@ size_t radix_scratch_bytes(int64_t n_max, int key_bits) {
     return 256 + (size_t)P * kRadix * 4 + (size_t)P * (size_t)std::max<int64_t>(tiles, 1) * kRadix * 4;
 }
 
-int radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt,
-                     const int32_t* n_dev, int64_t n_max, int key_bits, void* scratch,
-                     size_t scratch_bytes, int32_t* err_flag, cudaStream_t st, bool* result_in_alt,
-                     int numSMs) {
+// Passes of one sort: pass 0 reads (kin, vin) and writes buffer A, pass 1
+// reads A and writes B, and so on; the result is in A when the pass count
+// is odd, else in B. The input may be A or B itself (in-place sorts).
+template <bool kPairs>
+static int radix_sort_core(const uint32_t* kin, const uint32_t* vin, uint32_t* kA, uint32_t* vA, uint32_t* kB,
+                           uint32_t* vB, const int32_t* n_dev, int64_t n_max, int key_bits, void* scratch,
+                           size_t scratch_bytes, int32_t* err_flag, cudaStream_t st, int numSMs) {
     if (key_bits < 1 || key_bits > 32) return B3_ERR_INVALID_ARG;
     const int P = sort_passes(key_bits);
     const size_t need = radix_scratch_bytes(n_max, key_bits);
@@ -405,39 +439,68 @@ int radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_
     uint32_t* ghist = (uint32_t*)(s + 256);             // P x 256
     uint32_t* status = ghist + (size_t)P * kRadix;      // P x tiles x 256
     B3_CUDA(cudaMemsetAsync(scratch, 0, need, st));
-    if (n_max <= 0) {
-        *result_in_alt = false;
-        return B3_OK;
-    }
+    if (n_max <= 0) return B3_OK;
     const int hgrid = grid_for(n_max, kSortThreads, numSMs, 4);
-    k_radix_histogram<<<hgrid, kSortThreads, 0, st>>>(keys, n_dev, P, ghist);
+    k_radix_histogram<kPairs><<<hgrid, kSortThreads, 0, st>>>(kin, n_dev, P, ghist);
     B3_CHECK_LAUNCH();
     const size_t smem = sizeof(SortSmem);
     static bool attr_set = false;
     if (!attr_set) {
-        B3_CUDA(cudaFuncSetAttribute(k_onesweep_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        B3_CUDA(cudaFuncSetAttribute(k_onesweep_pass<kPairs>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem));
         attr_set = true;
     }
     // Persistent grid: resident blocks only, so every tile whose result a
     // later tile waits for is held by a running block.
     int occ = 1;
-    B3_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_onesweep_pass, kSortThreads, smem));
+    B3_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_onesweep_pass<kPairs>, kSortThreads, smem));
     occ = std::max(1, occ);
     const int pgrid = (int)std::min<int64_t>(tiles, (int64_t)numSMs * occ);
-    uint32_t* kin = keys; uint32_t* vin = vals;
-    uint32_t* kout = keys_alt; uint32_t* vout = vals;
-    vout = vals ? vals_alt : nullptr;
+    const uint32_t* ki = kin;
+    const uint32_t* vi = vin;
     for (int p = 0; p < P; ++p) {
-        k_onesweep_pass<<<pgrid, kSortThreads, smem, st>>>(
-            kin, vin, kout, vout, n_dev, 8 * p, ghist + (size_t)p * kRadix,
-            status + (size_t)p * tiles * kRadix, counters + p, err_flag);
+        uint32_t* ko = (p & 1) ? kB : kA;
+        uint32_t* vo = (p & 1) ? vB : vA;
+        k_onesweep_pass<kPairs><<<pgrid, kSortThreads, smem, st>>>(
+            ki, vi, ko, vo, n_dev, 8 * p, ghist + (size_t)p * kRadix, status + (size_t)p * tiles * kRadix,
+            counters + p, err_flag);
         B3_CHECK_LAUNCH();
-        std::swap(kin, kout);
-        std::swap(vin, vout);
+        ki = ko;
+        vi = vo;
     }
-    *result_in_alt = (P & 1) != 0;
     return B3_OK;
+}
+
+int radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt,
+                     const int32_t* n_dev, int64_t n_max, int key_bits, void* scratch,
+                     size_t scratch_bytes, int32_t* err_flag, cudaStream_t st, bool* result_in_alt,
+                     int numSMs) {
+    *result_in_alt = n_max > 0 && (sort_passes(key_bits) & 1) != 0;
+    return radix_sort_core<false>(keys, vals, keys_alt, vals ? vals_alt : nullptr, keys, vals, n_dev, n_max,
+                                  key_bits, scratch, scratch_bytes, err_flag, st, numSMs);
+}
+
+int radix_sort_kv_out(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out,
+                      uint32_t* keys_tmp, uint32_t* vals_tmp, const int32_t* n_dev, int64_t n_max, int key_bits,
+                      void* scratch, size_t scratch_bytes, int32_t* err_flag, cudaStream_t st, int numSMs) {
+    // the first pass writes the buffer that makes the last pass land in out
+    const bool odd = (sort_passes(key_bits) & 1) != 0;
+    uint32_t* kA = odd ? keys_out : keys_tmp;
+    uint32_t* vA = odd ? vals_out : vals_tmp;
+    uint32_t* kB = odd ? keys_tmp : keys_out;
+    uint32_t* vB = odd ? vals_tmp : vals_out;
+    return radix_sort_core<false>(keys_in, vals_in, kA, vals_in ? vA : nullptr, kB, vals_in ? vB : nullptr,
+                                  n_dev, n_max, key_bits, scratch, scratch_bytes, err_flag, st, numSMs);
+}
+
+int radix_sort_interleaved(uint2* kv, uint2* kv_alt, const int32_t* n_dev, int64_t n_max, int key_bits,
+                           void* scratch, size_t scratch_bytes, int32_t* err_flag, cudaStream_t st,
+                           bool* result_in_alt, int numSMs) {
+    *result_in_alt = n_max > 0 && (sort_passes(key_bits) & 1) != 0;
+    uint32_t* a = reinterpret_cast<uint32_t*>(kv_alt);
+    uint32_t* b = reinterpret_cast<uint32_t*>(kv);
+    return radix_sort_core<true>(b, nullptr, a, nullptr, b, nullptr, n_dev, n_max, key_bits, scratch, scratch_bytes,
+                                 err_flag, st, numSMs);
 }
 
 size_t scan_scratch_bytes(int64_t n_max) {
@@ -475,15 +538,26 @@ int fill_u32(uint32_t* dst, uint32_t v, int64_t n, cudaStream_t st) {
     return B3_OK;
 }
 
-int bound_search(const uint32_t* keys, const int32_t* n_dev, int64_t n_max, uint32_t* dst,
-                 int64_t n_dst, int mode, cudaStream_t st) {
+template <bool kPairs>
+static int bound_search_t(const uint32_t* keys, const int32_t* n_dev, int64_t n_max, uint32_t* dst,
+                          int64_t n_dst, int mode, cudaStream_t st) {
     if (n_max <= 0) return B3_OK;
     const int g = grid_for(n_max, 256, 148, 16);
-    if (mode == 0) k_bound_lower<<<g, 256, 0, st>>>(keys, n_dev, dst, n_dst);
-    else if (mode == 1) k_bound_upper<<<g, 256, 0, st>>>(keys, n_dev, dst, n_dst);
-    else k_bound_count<<<g, 256, 0, st>>>(keys, n_dev, dst, n_dst);
+    if (mode == 0) k_bound_lower<kPairs><<<g, 256, 0, st>>>(keys, n_dev, dst, n_dst);
+    else if (mode == 1) k_bound_upper<kPairs><<<g, 256, 0, st>>>(keys, n_dev, dst, n_dst);
+    else k_bound_count<kPairs><<<g, 256, 0, st>>>(keys, n_dev, dst, n_dst);
     B3_CHECK_LAUNCH();
     return B3_OK;
+}
+
+int bound_search(const uint32_t* keys, const int32_t* n_dev, int64_t n_max, uint32_t* dst,
+                 int64_t n_dst, int mode, cudaStream_t st) {
+    return bound_search_t<false>(keys, n_dev, n_max, dst, n_dst, mode, st);
+}
+
+int bound_search_interleaved(const uint2* kv, const int32_t* n_dev, int64_t n_max, uint32_t* dst, int64_t n_dst,
+                             int mode, cudaStream_t st) {
+    return bound_search_t<true>(reinterpret_cast<const uint32_t*>(kv), n_dev, n_max, dst, n_dst, mode, st);
 }
 
 int fill_int2(int2* dst, int2 v, int64_t n, cudaStream_t st) {

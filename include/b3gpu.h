@@ -208,6 +208,21 @@ int b3_radix_sort32_kv(b3Context ctx, uint32_t* d_keys, uint32_t* d_values, int6
 /* Keys-only variant (RadixSort32 keys-only benchmark,
  * opencl/primitives/AdlTest/RadixSortBenchmark.h:64). */
 int b3_radix_sort32_keys(b3Context ctx, uint32_t* d_keys, int64_t n, int key_bits, void* stream);
+/* btRadixSort32CL::execute(keysIn, keysOut, valuesIn, valuesOut, n, sortBits)
+ * (BB/btRadixSort32CL.h:67-68): out of place. The inputs are only read; the
+ * stably sorted keys and values land in the outputs, which must not be the
+ * inputs. d_values_in / d_values_out may both be NULL (keys only). The
+ * reference declares this form with an empty body
+ * (BB/btRadixSort32CL.cpp:151-155); this is the sort its signature names. */
+int b3_radix_sort32_kv_out(b3Context ctx, const uint32_t* d_keys_in, uint32_t* d_keys_out,
+                           const uint32_t* d_values_in, uint32_t* d_values_out, int64_t n, int key_bits,
+                           void* stream);
+/* btRadixSort32CL::execute(btOpenCLArray<btSortData>& keyValuesInOut,
+ * sortBits) (BB/btRadixSort32CL.h:70): the grid broadphase's and the batched
+ * solver's form. d_key_values holds n btSortData records (BB/btRadixSort32CL.h:
+ * 7-11: int m_key, int m_value; 8 bytes, 8-byte aligned), sorted in place
+ * by the low key_bits bits of m_key taken as unsigned, stably. */
+int b3_radix_sort32_sortdata(b3Context ctx, int32_t* d_key_values, int64_t n, int key_bits, void* stream);
 
 /* btBoundSearchCL::execute (BB/btBoundSearchCL.cpp:78-136,
  * PR/Search/BoundSearchKernels.cl:42-104) over sorted keys.
@@ -217,6 +232,15 @@ int b3_radix_sort32_keys(b3Context ctx, uint32_t* d_keys, int64_t n, int key_bit
  * Keys >= n_dst are ignored (the reference would write out of range). */
 int b3_bound_search(b3Context ctx, const uint32_t* d_sorted_keys, int64_t n_src,
                     uint32_t* d_dst, int64_t n_dst, int mode, void* stream);
+/* btBoundSearchCL::execute(btOpenCLArray<btSortData>& src, nSrc, dst, nDst,
+ * option) (BB/btBoundSearchCL.h:60): the same search over btSortData records
+ * sorted by m_key (8-byte aligned), modes as b3_bound_search. One difference
+ * follows the reference's SearchSortDataUpperKernel
+ * (PR/Search/BoundSearchKernels.cl:66-86): in UPPER mode, when no record has
+ * key 0, d_dst[0] is set to 0. Keys >= n_dst are skipped (the reference
+ * writes past d_dst for them). */
+int b3_bound_search_sortdata(b3Context ctx, const int32_t* d_sorted_key_values, int64_t n_src, uint32_t* d_dst,
+                             int64_t n_dst, int mode, void* stream);
 
 /* ------------------------------------------------------------------ */
 /* World: rigid-body & collidable arrays, grid broadphase,              */

@@ -64,6 +64,14 @@ private:
 
 /* btRadixSort32CL::execute(keyValues, sortBits): stable LSD sort of
  * (key, value) pairs by the low sortBits bits of the key. */
+/* btSortData (BB/btRadixSort32CL.h:7-11): one (key, value) record of the
+ * sorts and bound searches, 8 bytes. */
+struct SortData {
+    int m_key;
+    int m_value;
+};
+static_assert(sizeof(SortData) == 8, "btSortData is 8 bytes");
+
 class RadixSort32 {
 public:
     explicit RadixSort32(Context& ctx) : ctx_(ctx) {}
@@ -72,6 +80,17 @@ public:
     }
     void executeKeys(uint32_t* d_keys, int64_t n, int sortBits = 32, void* stream = nullptr) {
         check(b3_radix_sort32_keys(ctx_.handle(), d_keys, n, sortBits, stream), "RadixSort32::executeKeys");
+    }
+    /* execute(keysIn, keysOut, valuesIn, valuesOut, n, sortBits): out of place. */
+    void execute(const uint32_t* d_keysIn, uint32_t* d_keysOut, const uint32_t* d_valuesIn, uint32_t* d_valuesOut,
+                 int64_t n, int sortBits = 32, void* stream = nullptr) {
+        check(b3_radix_sort32_kv_out(ctx_.handle(), d_keysIn, d_keysOut, d_valuesIn, d_valuesOut, n, sortBits, stream),
+              "RadixSort32::execute");
+    }
+    /* execute(keyValuesInOut, sortBits): n btSortData records in place. */
+    void execute(SortData* d_keyValues, int64_t n, int sortBits = 32, void* stream = nullptr) {
+        check(b3_radix_sort32_sortdata(ctx_.handle(), reinterpret_cast<int32_t*>(d_keyValues), n, sortBits, stream),
+              "RadixSort32::execute");
     }
 
 private:
@@ -115,6 +134,13 @@ public:
     void execute(const uint32_t* d_sortedKeys, int64_t nSrc, uint32_t* d_dst, int64_t nDst, Option option,
                  void* stream = nullptr) {
         check(b3_bound_search(ctx_.handle(), d_sortedKeys, nSrc, d_dst, nDst, (int)option, stream),
+              "BoundSearch::execute");
+    }
+    /* execute(src, nSrc, dst, nDst, option) over btSortData records. */
+    void execute(const SortData* d_src, int64_t nSrc, uint32_t* d_dst, int64_t nDst, Option option = BOUND_LOWER,
+                 void* stream = nullptr) {
+        check(b3_bound_search_sortdata(ctx_.handle(), reinterpret_cast<const int32_t*>(d_src), nSrc, d_dst, nDst,
+                                       (int)option, stream),
               "BoundSearch::execute");
     }
 

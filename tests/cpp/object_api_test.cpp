@@ -118,6 +118,34 @@ static int gpu_mode() {
     uint64_t sum = 0;
     for (uint32_t c : cnt) sum += c;
     EXPECT(sum == (uint64_t)n);
+    // btSortData form: the same keys and values interleaved, sorted in place,
+    // then bound-searched; and the out-of-place four-array form
+    std::vector<b3::SortData> kv(n);
+    for (int i = 0; i < n; ++i) kv[i] = {(int)keys[i], (int)vals[i]};
+    b3::SortData* dkv = nullptr;
+    uint32_t *dko = nullptr, *dvo = nullptr, *dlo = nullptr;
+    EXPECT(cudaMalloc(&dkv, n * 8) == cudaSuccess && cudaMalloc(&dko, n * 4) == cudaSuccess &&
+           cudaMalloc(&dvo, n * 4) == cudaSuccess && cudaMalloc(&dlo, 4 << 20) == cudaSuccess);
+    cudaMemcpy(dkv, kv.data(), n * 8, cudaMemcpyHostToDevice);
+    sort.execute(dkv, n, 20);
+    cudaMemcpy(kv.data(), dkv, n * 8, cudaMemcpyDeviceToHost);
+    for (int i = 0; i < n; ++i) EXPECT((uint32_t)kv[i].m_key == sk[i] && (uint32_t)kv[i].m_value == sv[i]);
+    bs.execute(dkv, n, dlo, 1 << 20, b3::BoundSearch::COUNT);
+    std::vector<uint32_t> cnt2(1 << 20);
+    cudaMemcpy(cnt2.data(), dlo, 4 << 20, cudaMemcpyDeviceToHost);
+    EXPECT(cnt2 == cnt);
+    cudaMemcpy(dk, keys.data(), n * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(dv, vals.data(), n * 4, cudaMemcpyHostToDevice);
+    sort.execute(dk, dko, dv, dvo, n, 20);
+    std::vector<uint32_t> ok(n), ov(n), ik(n);
+    cudaMemcpy(ok.data(), dko, n * 4, cudaMemcpyDeviceToHost);
+    cudaMemcpy(ov.data(), dvo, n * 4, cudaMemcpyDeviceToHost);
+    cudaMemcpy(ik.data(), dk, n * 4, cudaMemcpyDeviceToHost);
+    EXPECT(ok == sk && ov == sv && ik == keys);
+    cudaFree(dkv);
+    cudaFree(dko);
+    cudaFree(dvo);
+    cudaFree(dlo);
     cudaFree(dk);
     cudaFree(dv);
     cudaFree(ds);

@@ -121,3 +121,73 @@ def test_fill(ctx):
     b3.Fill(ctx).execute(d2, (7, -3), n=32, offset=16)
     h2 = d2.cpu().numpy()
     assert np.all(h2[16:48] == [7, -3]) and np.all(h2[:16] == 0) and np.all(h2[48:] == 0)
+
+
+# --- the btSortData and out-of-place forms (BB/btRadixSort32CL.h:67-70,
+# BB/btBoundSearchCL.h:60), each against the split-array form
+
+
+@pytest.mark.parametrize("n,bits", [(2, 32), (4097, 32), (1000003, 32), (300000, 13), (70000, 8), (5, 4)])
+def test_sortdata_sort_matches_split_form(ctx, n, bits):
+    rng = np.random.default_rng(n + bits)
+    keys = rng.integers(0, 1 << bits, n, dtype=np.uint64).astype(np.uint32)
+    vals = np.arange(n, dtype=np.uint32)
+    kv = np.stack([keys, vals], 1).view(np.int32).copy()
+    dkv = torch.from_numpy(kv).cuda()
+    dk, dv = _dev(keys), _dev(vals)
+    s = b3.RadixSort32(ctx)
+    s.execute_sortdata(dkv, key_bits=bits)
+    s.execute(dk, dv, key_bits=bits)
+    torch.cuda.synchronize()
+    out = dkv.cpu().numpy().view(np.uint32)
+    assert np.array_equal(out[:, 0], _host(dk)) and np.array_equal(out[:, 1], _host(dv))
+    # stable: the numpy stable order
+    order = np.argsort(keys, kind="stable")
+    assert np.array_equal(out[:, 1], order.astype(np.uint32))
+
+
+@pytest.mark.parametrize("n,bits,with_values", [(3, 32, True), (65537, 32, True), (500000, 24, True),
+                                                (200000, 16, False), (9999, 7, True)])
+def test_out_of_place_sort_leaves_inputs(ctx, n, bits, with_values):
+    rng = np.random.default_rng(7 * n + bits)
+    keys = rng.integers(0, 1 << bits, n, dtype=np.uint64).astype(np.uint32)
+    vals = rng.integers(0, 1 << 32, n, dtype=np.uint64).astype(np.uint32)
+    ki, ko = _dev(keys), _dev(np.zeros(n, np.uint32))
+    vi = _dev(vals) if with_values else None
+    vo = _dev(np.zeros(n, np.uint32)) if with_values else None
+    b3.RadixSort32(ctx).execute_out(ki, ko, vi, vo, key_bits=bits)
+    torch.cuda.synchronize()
+    order = np.argsort(keys, kind="stable")
+    assert np.array_equal(_host(ko), keys[order])
+    assert np.array_equal(_host(ki), keys)
+    if with_values:
+        assert np.array_equal(_host(vo), vals[order]) and np.array_equal(_host(vi), vals)
+
+
+def test_out_of_place_sort_rejects_aliased_outputs(ctx):
+    k = _dev(np.arange(10, dtype=np.uint32))
+    with pytest.raises(b3.B3Error):
+        b3.RadixSort32(ctx).execute_out(k, k)
+
+
+@pytest.mark.parametrize("n", [1, 100, 4096, 65537])
+def test_sortdata_bound_search(ctx, n):
+    rng = np.random.default_rng(n + 11)
+    keys = np.sort(rng.integers(1 if n == 100 else 0, 256, n)).astype(np.uint32)
+    kv = np.stack([keys, np.arange(n, dtype=np.uint32)], 1).view(np.int32).copy()
+    dkv = torch.from_numpy(kv).cuda()
+    dk = _dev(keys)
+    nd = 256
+    bs = b3.BoundSearch(ctx)
+    for mode in (bs.LOWER, bs.UPPER, bs.COUNT):
+        a = _dev(np.full(nd, 0xFFFFFFFF, np.uint32))
+        b = _dev(np.full(nd, 0xFFFFFFFF, np.uint32))
+        bs.execute_sortdata(dkv, n, a, nd, mode)
+        bs.execute(dk, n, b, nd, mode)
+        torch.cuda.synchronize()
+        A, B = _host(a), _host(b)
+        if mode == bs.UPPER and keys[0] != 0:
+            # SearchSortDataUpperKernel: upper bound of an absent key 0 is 0
+            assert A[0] == 0
+            A[0] = B[0]
+        assert np.array_equal(A, B), mode
