@@ -124,6 +124,7 @@ SIGNATURES = [
     ("b3_radix_sort32_kv", _I, [_P, _P, _P, _I64, _I, _P]),
     ("b3_radix_sort32_keys", _I, [_P, _P, _I64, _I, _P]),
     ("b3_bound_search", _I, [_P, _P, _I64, _P, _I64, _I, _P]),
+    ("b3_set_wait_limits", _I, [_P, _I, _I]),
     ("b3_radix_sort32_kv_out", _I, [_P, _P, _P, _P, _P, _I64, _I, _P]),
     ("b3_radix_sort32_sortdata", _I, [_P, _P, _I64, _I, _P]),
     ("b3_bound_search_sortdata", _I, [_P, _P, _I64, _P, _I64, _I, _P]),
@@ -469,6 +470,18 @@ class PhysicsWorld:
         c = Counters()
         _check(self.lib.b3_get_counters(self.h, C.byref(c), None), "b3_get_counters")
         return c.as_dict()
+
+    def counters_status(self):
+        """(status, counters): b3_get_counters without raising on
+        B3_ERR_TIMEOUT (a bounded device wait gave up)."""
+        c = Counters()
+        rc = self.lib.b3_get_counters(self.h, C.byref(c), None)
+        if rc not in (0, 6):
+            _check(rc, "b3_get_counters")
+        return rc, c.as_dict()
+
+    def set_wait_limits(self, spin_limit=0, hold_micros=0):
+        _check(self.lib.b3_set_wait_limits(self.h, int(spin_limit), int(hold_micros)), "b3_set_wait_limits")
 
     def reset_counters(self):
         _check(self.lib.b3_reset_counters(self.h, None), "b3_reset_counters")

@@ -58,6 +58,10 @@ static inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStre
 // ---------------------------------------------------------------------------
 namespace b3 {
 
+// Polls of a device-side wait before it gives up (the Jacobi grid barrier's
+// limit can be changed per world, b3_set_wait_limits).
+constexpr int kDefaultSpinLimit = 1 << 22;
+
 // Onesweep radix sort scratch: returns bytes for n_max elements.
 size_t radix_scratch_bytes(int64_t n_max, int key_bits);
 // Sort (keys, vals) of device count *n_dev (<= n_max). The sorted result
@@ -120,7 +124,7 @@ __device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned l
 // Bounded spin budget for every device-side wait: about 4M polls with a
 // short back-off (well under a second), after which the waiter records an
 // error and proceeds instead of hanging the GPU.
-constexpr int kSpinLimit = 1 << 22;
+constexpr int kSpinLimit = b3::kDefaultSpinLimit;
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;

@@ -201,6 +201,10 @@ struct b3World_t {
 
     int cooperativeOk = 1;
 
+    // bounded waits of the persistent Jacobi kernel (b3_set_wait_limits)
+    int waitSpinLimit = b3::kDefaultSpinLimit;
+    int waitHoldMicros = 0;
+
     b3::BodiesDev bodiesDev() const;
     b3::ShapesDev shapesDev() const;
 };

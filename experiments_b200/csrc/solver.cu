@@ -358,7 +358,11 @@ k_jacobi(SolverView V, int iterations, uint32_t* bar, int32_t* err, b3Counters* 
     for (int k = 0; k < kJacobiHeads; ++k)
         if (m0 + k * stride < M) load_head(V, m0 + k * stride, heads[k][threadIdx.x]);
     for (int p = 0; p < phases; ++p) {
-        if (p > 0 && !grid_barrier(bar, bar + 1, nb, err, counters)) return;
+        if (p == 1 && V.holdMicros > 0 && blockIdx.x == 0 && threadIdx.x == 0) {
+            // test of the give-up path: block 0 arrives late (bounded sleep)
+            for (int i = 0; i < V.holdMicros; ++i) __nanosleep(1000);
+        }
+        if (p > 0 && !grid_barrier(bar, bar + 1, nb, err, counters, V.spinLimit)) return;
         const bool friction = (p & 1) != 0, first = p == 0;
         const int inBuf = (p - 1) & 1, outBuf = p & 1;
         int k = 0;
@@ -482,6 +486,8 @@ SolverView b3solver::solver_view(b3World_t* w) {
     V.incEnd = w->d.bodyIncEnd;
     V.numManifolds = w->d.scalars + b3::S_NUM_MANIFOLDS;
     V.numBodies = (int)w->bodies.size();
+    V.spinLimit = w->waitSpinLimit;
+    V.holdMicros = w->waitHoldMicros;
     return V;
 }
 

@@ -31,6 +31,11 @@ struct SolverView {
     const uint32_t* incEnd;
     const int32_t* numManifolds;
     int numBodies;
+    // bounded waits of the persistent Jacobi kernel: polls of a grid
+    // barrier before it gives up, and (testing the give-up path only) how
+    // long block 0 holds back before its first barrier, in microseconds
+    int spinLimit;
+    int holdMicros;
 };
 
 __device__ __forceinline__ float4& R(const SolverView& v, int slot, int m) {
@@ -57,8 +62,13 @@ __device__ __forceinline__ void plane_space(float3 n, float3& p, float3& q) {
 // ---------------------------------------------------------------------------
 // Persistent-kernel helpers
 // ---------------------------------------------------------------------------
+// Every block arrives, the last one releases the others. A waiter gives up
+// after spinLimit polls: it sets *err, counts a timeout and the kernel's
+// blocks leave at this or their next barrier (an error set by anyone makes
+// every barrier fail), so the launch always ends.
 __device__ __forceinline__ bool grid_barrier(uint32_t* count, uint32_t* gen, uint32_t nblocks,
-                                             int32_t* err, b3Counters* counters) {
+                                             int32_t* err, b3Counters* counters,
+                                             int spinLimit = b3dev::kSpinLimit) {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -73,7 +83,7 @@ __device__ __forceinline__ bool grid_barrier(uint32_t* count, uint32_t* gen, uin
         } else {
             int spins = 0;
             while (b3dev::ld_acquire_u32(gen) == g) {
-                if (++spins > b3dev::kSpinLimit) {
+                if (++spins > spinLimit) {
                     atomicExch(err, 1);
                     atomicAdd(&counters->timeouts, 1);
                     ok = 0;

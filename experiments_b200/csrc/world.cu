@@ -847,10 +847,19 @@ extern "C" int b3_read_state(b3World w, float* pos4, float* quat4, float* linVel
     if (quat4) B3_CUDA(cudaMemcpyAsync(quat4, w->d.quat, 16 * N, cudaMemcpyDeviceToHost, st));
     if (linVel4) B3_CUDA(cudaMemcpyAsync(linVel4, w->d.linVel, 16 * N, cudaMemcpyDeviceToHost, st));
     if (angVel4) B3_CUDA(cudaMemcpyAsync(angVel4, w->d.angVel, 16 * N, cudaMemcpyDeviceToHost, st));
+    int32_t err = 0;
+    B3_CUDA(cudaMemcpyAsync(&err, w->d.scalars + b3::S_ERR, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     B3_CUDA(cudaStreamSynchronize(st));
+    if (err) {
+        b3_set_error("a bounded device wait gave up; the state read is not valid");
+        return B3_ERR_TIMEOUT;
+    }
     return B3_OK;
 }
 
+// Asynchronous on the stream: the copies read pinned host buffers when the
+// stream reaches them (keep them unchanged until then); pageable buffers are
+// staged before the call returns.
 extern "C" int b3_write_state(b3World w, const float* pos4, const float* quat4, const float* linVel4,
                               const float* angVel4, void* stream) {
     if (!w || !w->written) return B3_ERR_STATE;
@@ -860,7 +869,6 @@ extern "C" int b3_write_state(b3World w, const float* pos4, const float* quat4, 
     if (quat4) B3_CUDA(cudaMemcpyAsync(w->d.quat, quat4, 16 * N, cudaMemcpyHostToDevice, st));
     if (linVel4) B3_CUDA(cudaMemcpyAsync(w->d.linVel, linVel4, 16 * N, cudaMemcpyHostToDevice, st));
     if (angVel4) B3_CUDA(cudaMemcpyAsync(w->d.angVel, angVel4, 16 * N, cudaMemcpyHostToDevice, st));
-    B3_CUDA(cudaStreamSynchronize(st));
     return B3_OK;
 }
 
@@ -895,6 +903,19 @@ extern "C" int b3_get_counters(b3World w, b3Counters* out, void* stream) {
     B3_CUDA(cudaMemcpyAsync(&err, w->d.scalars + b3::S_ERR, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     B3_CUDA(cudaStreamSynchronize(st));
     if (err && out->timeouts == 0) out->timeouts = 1;
+    if (err) {
+        b3_set_error("a bounded device wait gave up (%d timeouts); results since are not valid",
+                     (int)out->timeouts);
+        return B3_ERR_TIMEOUT;
+    }
+    return B3_OK;
+}
+
+extern "C" int b3_set_wait_limits(b3World w, int spinLimit, int holdMicros) {
+    if (!w || spinLimit < 0 || holdMicros < 0 || holdMicros > 1000000) return B3_ERR_INVALID_ARG;
+    w->waitSpinLimit = spinLimit == 0 ? b3::kDefaultSpinLimit : spinLimit;
+    w->waitHoldMicros = holdMicros;
+    w->graphValid = false;  // the limits are launch arguments of the captured step
     return B3_OK;
 }
 

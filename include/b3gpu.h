@@ -383,15 +383,33 @@ int b3_write_velocities(b3World w, const float* linVel3, const float* angVel3, v
 int b3_step(b3World w, int numSteps, void* stream);
 
 /* Read bodies back in the reference Body layout (host, synchronising);
- * before the first b3_write_bodies, the records as registered. */
+ * before the first b3_write_bodies, the records as registered. Reports
+ * B3_ERR_TIMEOUT as b3_read_state does. */
 int b3_read_bodies(b3World w, b3Body* out, int maxBodies, void* stream);
-/* Read SoA state (host float4 arrays, NULL to skip; synchronising). */
+/* Read SoA state (host float4 arrays, NULL to skip; synchronising).
+ * Returns B3_ERR_TIMEOUT (arrays filled) when a bounded device wait has
+ * given up since the last b3_reset_counters: the state is not valid. */
 int b3_read_state(b3World w, float* pos4, float* quat4, float* linVel4, float* angVel4, void* stream);
-/* Write SoA state (host float4 arrays, NULL to skip). */
+/* Write SoA state (host float4 arrays, NULL to skip). Asynchronous on the
+ * stream: pinned host buffers are read when the stream reaches the copies
+ * and must stay unchanged until then; pageable buffers are staged before
+ * the call returns. */
 int b3_write_state(b3World w, const float* pos4, const float* quat4, const float* linVel4,
                    const float* angVel4, void* stream);
 int b3_get_num_bodies(b3World w, int* n);
+/* Step diagnostics (synchronising). Returns B3_ERR_TIMEOUT, with *out
+ * filled and out->timeouts >= 1, when a bounded device wait has given up
+ * since the last b3_reset_counters; the step results since are not valid.
+ * The error stays set (later solves stop at their first grid barrier) until
+ * b3_reset_counters. */
 int b3_get_counters(b3World w, b3Counters* out, void* stream);
+/* Bounded waits of the persistent Jacobi solve (its grid barriers): a
+ * waiter gives up after spinLimit polls (0 = the default, 4,194,304 polls
+ * of about 64 ns each). holdMicros > 0 makes block 0 of the solve arrive at
+ * its first grid barrier that many microseconds late, which, with a small
+ * spinLimit, exercises the give-up path (tests only; at most 1 s).
+ * No reference counterpart: the reference's waits are clFinish calls. */
+int b3_set_wait_limits(b3World w, int spinLimit, int holdMicros);
 int b3_reset_counters(b3World w, void* stream);
 
 /* --- stage entry points (each one stage of stepSimulation) --- */
