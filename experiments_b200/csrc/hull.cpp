@@ -1,25 +1,39 @@
 // Convex-hull polyhedral features for registration (host side).
 //
 // Behaviour follows btConvexUtility::initializePolyhedralFeatures and
-// ::initialize (P1/btConvexUtility.cpp:31-270, 339-513):
-//   * hull of the point cloud; hull vertices keep their input order,
-//   * faces wound counter-clockwise seen from outside, plane
-//     (n, -min_v n.v) over the face's vertices,
-//   * faces whose normals agree to dot > 0.999 are welded into one polygon
-//     (2D hull of their points, plane of the group's reference face), unless
-//     a dropped point is used by a face outside the group,
+// ::initialize (P1/btConvexUtility.cpp:31-270, 339-513) over the hull that
+// bullet2's btConvexHullComputer returns for the same points:
+//   * the points are quantised to btConvexHullComputer's integer grid
+//     (btConvexHullInternal::compute, bullet2/LinearMath/
+//     btConvexHullComputer.cpp:1940-2030: per-axis extent / 10216, axes
+//     ordered medium, largest, smallest, coordinates truncated toward zero)
+//     and the hull is computed exactly on the grid points; its vertices are
+//     the grid points mapped back (getCoordinates, :2075-2082: point *
+//     scaling + center, in float), so they sit where the reference's do;
+//   * faces are the hull's maximal planar polygons, wound counter-clockwise
+//     seen from outside; each face's plane is computed from its first two
+//     normalised edges and its lowest vertex in float, as btConvexUtility
+//     does (:56-108);
+//   * faces whose normals agree to dot > 0.999 (in float) are welded into
+//     one polygon (2D hull of their points, plane of the group's reference
+//     face), unless a dropped point is used by a face outside the group;
 //   * unique edge directions: normalised (v[smaller] - v[larger]) deduped
-//     by +/- within 1e-6 per component,
+//     by +/- within 1e-6 per component;
 //   * local centre = average of the hull vertices
 //     (CLPhysicsDemo::registerConvexPolyhedron, P2/CLPhysicsDemo.cpp:360-366).
-// The hull itself is computed here by exhaustive plane search, which is exact
-// for the few-dozen-point shapes this pipeline registers (the reference uses
-// Bullet's btConvexHullComputer); faces, vertices and edges agree as sets.
+// The hull itself is this file's own incremental construction with exact
+// 64-bit integer predicates on the grid (O(points x faces)); vertices are
+// listed in the order of their first input point, faces by their vertex
+// indices (the reference lists both in its hull traversal order).
 #include "hull.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
+#include <cstdint>
 #include <map>
+#include <numeric>
+#include <unordered_map>
 
 namespace b3hull {
 
@@ -41,14 +55,242 @@ inline V3 norm(V3 a) {
     return l > 0 ? mul(a, 1.0 / l) : a;
 }
 
-struct RawFace {
-    V3 n;
-    double d;                 // plane: n.x = d
-    std::vector<int> idx;     // CCW seen from outside (indices into input points)
+// float vector arithmetic in btVector3's operation order
+struct F3 {
+    float x, y, z;
+};
+inline F3 fsub(F3 a, F3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline float fdot(F3 a, F3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline F3 fcross(F3 a, F3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+inline F3 fnormalized(F3 a) {
+    // btVector3::normalize: *this /= length(), the division as a multiply
+    // by the reciprocal
+    const float r = 1.f / std::sqrt(fdot(a, a));
+    return {a.x * r, a.y * r, a.z * r};
+}
+
+// ---------------------------------------------------------------------------
+// btConvexHullComputer's integer grid
+// ---------------------------------------------------------------------------
+struct Grid {
+    int medAxis = 0, maxAxis = 0, minAxis = 0;
+    float scaling[3] = {0, 0, 0}, center[3] = {0, 0, 0}, inv[3] = {0, 0, 0};
 };
 
+Grid make_grid(const float* p, int n) {
+    Grid g;
+    float mn[3] = {1e30f, 1e30f, 1e30f}, mx[3] = {-1e30f, -1e30f, -1e30f};
+    for (int i = 0; i < n; ++i)
+        for (int k = 0; k < 3; ++k) {
+            const float v = p[3 * i + k];
+            if (v < mn[k]) mn[k] = v;   // btSetMin
+            if (mx[k] < v) mx[k] = v;   // btSetMax
+        }
+    float s[3] = {mx[0] - mn[0], mx[1] - mn[1], mx[2] - mn[2]};
+    // btVector3::maxAxis / minAxis (bullet2/LinearMath/btVector3.h:453-463)
+    g.maxAxis = s[0] < s[1] ? (s[1] < s[2] ? 2 : 1) : (s[0] < s[2] ? 2 : 0);
+    g.minAxis = s[0] < s[1] ? (s[0] < s[2] ? 0 : 2) : (s[1] < s[2] ? 1 : 2);
+    if (g.minAxis == g.maxAxis) g.minAxis = (g.maxAxis + 1) % 3;
+    g.medAxis = 3 - g.maxAxis - g.minAxis;
+    const volatile float div = 10216.f;
+    const float r = 1.f / div;  // s /= 10216: a multiply by the reciprocal
+    for (int k = 0; k < 3; ++k) s[k] *= r;
+    if (((g.medAxis + 1) % 3) != g.maxAxis)
+        for (int k = 0; k < 3; ++k) s[k] *= -1.f;
+    for (int k = 0; k < 3; ++k) {
+        g.scaling[k] = s[k];
+        g.inv[k] = s[k] != 0.f ? 1.f / s[k] : s[k];
+        g.center[k] = (mn[k] + mx[k]) * 0.5f;
+    }
+    return g;
+}
+
+struct IV {
+    int64_t x, y, z;
+    bool operator==(const IV& o) const { return x == o.x && y == o.y && z == o.z; }
+};
+inline IV isub(IV a, IV b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline IV icross(IV a, IV b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+inline int64_t idot(IV a, IV b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+// grid coordinates of one point: x along the medium axis, y the largest,
+// z the smallest, truncated toward zero
+IV quantize(const Grid& g, const float* p) {
+    float q[3];
+    for (int k = 0; k < 3; ++k) q[k] = (p[k] - g.center[k]) * g.inv[k];
+    return {(int64_t)(int32_t)q[g.medAxis], (int64_t)(int32_t)q[g.maxAxis], (int64_t)(int32_t)q[g.minAxis]};
+}
+
+// the grid point mapped back: getCoordinates (p * scaling + center, float)
+V3 dequantize(const Grid& g, IV v) {
+    float p[3];
+    p[g.medAxis] = (float)v.x;
+    p[g.maxAxis] = (float)v.y;
+    p[g.minAxis] = (float)v.z;
+    float o[3];
+    for (int k = 0; k < 3; ++k) o[k] = p[k] * g.scaling[k] + g.center[k];
+    return {o[0], o[1], o[2]};
+}
+
+// ---------------------------------------------------------------------------
+// Exact incremental hull of grid points (|coordinate| <= 2^13, so every
+// cross product and plane test below is exact in 64-bit integers)
+// ---------------------------------------------------------------------------
+struct HTri {
+    int a, b, c;
+    IV n;       // outward normal (b - a) x (c - a)
+    int64_t d;  // plane n . x = d
+    bool alive;
+};
+
+HTri make_tri(const std::vector<IV>& Q, int a, int b, int c) {
+    HTri t;
+    t.a = a;
+    t.b = b;
+    t.c = c;
+    t.n = icross(isub(Q[b], Q[a]), isub(Q[c], Q[a]));
+    t.d = idot(t.n, Q[a]);
+    t.alive = true;
+    return t;
+}
+
+bool exact_hull(const std::vector<IV>& Q, std::vector<HTri>& tris) {
+    const int m = (int)Q.size();
+    tris.clear();
+    if (m < 4) return false;
+    // initial tetrahedron: farthest point, largest triangle, largest volume
+    const int i0 = 0;
+    int i1 = -1, i2 = -1, i3 = -1;
+    int64_t best = 0;
+    for (int j = 1; j < m; ++j) {
+        const IV d = isub(Q[j], Q[i0]);
+        const int64_t l2 = idot(d, d);
+        if (l2 > best) best = l2, i1 = j;
+    }
+    if (i1 < 0) return false;
+    best = 0;
+    for (int j = 1; j < m; ++j) {
+        const IV c = icross(isub(Q[i1], Q[i0]), isub(Q[j], Q[i0]));
+        const int64_t l2 = idot(c, c);
+        if (l2 > best) best = l2, i2 = j;
+    }
+    if (i2 < 0) return false;
+    const IV nrm = icross(isub(Q[i1], Q[i0]), isub(Q[i2], Q[i0]));
+    best = 0;
+    for (int j = 1; j < m; ++j) {
+        const int64_t v = idot(nrm, isub(Q[j], Q[i0]));
+        const int64_t av = v < 0 ? -v : v;
+        if (av > best) best = av, i3 = j;
+    }
+    if (i3 < 0) return false;
+    if (idot(nrm, isub(Q[i3], Q[i0])) > 0) {
+        tris.push_back(make_tri(Q, i0, i2, i1));
+        tris.push_back(make_tri(Q, i0, i1, i3));
+        tris.push_back(make_tri(Q, i1, i2, i3));
+        tris.push_back(make_tri(Q, i2, i0, i3));
+    } else {
+        tris.push_back(make_tri(Q, i0, i1, i2));
+        tris.push_back(make_tri(Q, i0, i3, i1));
+        tris.push_back(make_tri(Q, i1, i3, i2));
+        tris.push_back(make_tri(Q, i2, i3, i0));
+    }
+    // the remaining points in a fixed pseudo-random order (an odd-step walk
+    // through the indices), which keeps the visible sets small on average
+    std::vector<int> order;
+    order.reserve(m);
+    uint64_t step = 0x9E3779B97F4A7C15ull % (uint64_t)m;
+    while (step == 0 || std::gcd(step, (uint64_t)m) != 1) step = (step + 1) % (uint64_t)m;
+    for (uint64_t k = 0, j = 0; k < (uint64_t)m; ++k, j = (j + step) % (uint64_t)m)
+        if ((int)j != i0 && (int)j != i1 && (int)j != i2 && (int)j != i3) order.push_back((int)j);
+    std::vector<int> visible;
+    std::vector<std::pair<int, int>> edges;
+    int alive = 4;
+    for (int p : order) {
+        visible.clear();
+        for (int t = 0; t < (int)tris.size(); ++t)
+            if (tris[t].alive && idot(tris[t].n, Q[p]) > tris[t].d) visible.push_back(t);
+        if (visible.empty()) continue;  // inside the hull or on its surface
+        edges.clear();
+        for (int t : visible) {
+            edges.push_back({tris[t].a, tris[t].b});
+            edges.push_back({tris[t].b, tris[t].c});
+            edges.push_back({tris[t].c, tris[t].a});
+            tris[t].alive = false;
+        }
+        alive -= (int)visible.size();
+        std::vector<std::pair<int, int>> sorted = edges;
+        std::sort(sorted.begin(), sorted.end());
+        // horizon: edges of the visible region whose reverse is not in it;
+        // each gets a new triangle to p with the visible face's winding
+        for (const auto& e : edges)
+            if (!std::binary_search(sorted.begin(), sorted.end(), std::make_pair(e.second, e.first))) {
+                tris.push_back(make_tri(Q, e.first, e.second, p));
+                ++alive;
+            }
+        if ((int)tris.size() > 4 * alive + 64) {
+            std::vector<HTri> keep;
+            keep.reserve(alive);
+            for (const HTri& t : tris)
+                if (t.alive) keep.push_back(t);
+            tris.swap(keep);
+        }
+    }
+    std::vector<HTri> keep;
+    for (const HTri& t : tris)
+        if (t.alive) keep.push_back(t);
+    tris.swap(keep);
+    return true;
+}
+
+int64_t gcd64(int64_t a, int64_t b) {
+    a = a < 0 ? -a : a;
+    b = b < 0 ? -b : b;
+    while (b) {
+        const int64_t t = a % b;
+        a = b;
+        b = t;
+    }
+    return a;
+}
+
+// Vertices of one planar face, strictly convex and counter-clockwise about
+// the outward normal n, by a monotone chain on the two axes other than n's
+// largest component (exact).
+std::vector<int> planar_polygon(const std::vector<IV>& Q, const std::vector<int>& ids, IV n) {
+    const int64_t ax = std::llabs(n.x), ay = std::llabs(n.y), az = std::llabs(n.z);
+    const int k = (ax >= ay && ax >= az) ? 0 : (ay >= az ? 1 : 2);
+    const int64_t nk = k == 0 ? n.x : (k == 1 ? n.y : n.z);
+    auto coord = [&](const IV& v, int c) { return c == 0 ? v.x : (c == 1 ? v.y : v.z); };
+    struct P2 {
+        int64_t u, v;
+        int id;
+    };
+    std::vector<P2> q;
+    for (int id : ids) q.push_back({coord(Q[id], (k + 1) % 3), coord(Q[id], (k + 2) % 3), id});
+    std::sort(q.begin(), q.end(), [](const P2& a, const P2& b) { return a.u < b.u || (a.u == b.u && a.v < b.v); });
+    auto crs = [](const P2& o, const P2& a, const P2& b) { return (a.u - o.u) * (b.v - o.v) - (a.v - o.v) * (b.u - o.u); };
+    std::vector<P2> h(2 * q.size() + 1);
+    size_t t = 0;
+    for (size_t i = 0; i < q.size(); ++i) {
+        while (t >= 2 && crs(h[t - 2], h[t - 1], q[i]) <= 0) --t;
+        h[t++] = q[i];
+    }
+    for (size_t i = q.size() - 1, lo = t + 1; i > 0; --i) {
+        while (t >= lo && crs(h[t - 2], h[t - 1], q[i - 1]) <= 0) --t;
+        h[t++] = q[i - 1];
+    }
+    h.resize(t > 0 ? t - 1 : 0);
+    // (axis k+1, axis k+2, axis k) is right-handed: counter-clockwise in
+    // (u, v) is counter-clockwise about +axis k
+    std::vector<int> r;
+    for (const P2& e : h) r.push_back(e.id);
+    if (nk < 0) std::reverse(r.begin(), r.end());
+    return r;
+}
+
 // Order coplanar points counter-clockwise around normal n, keeping only the
-// extreme points of their 2D convex hull (monotone chain).
+// extreme points of their 2D convex hull (monotone chain); for the welded
+// faces, whose points are not exactly coplanar.
 std::vector<int> ccw_hull_2d(const std::vector<V3>& P, const std::vector<int>& ids, V3 n) {
     V3 a = std::fabs(n.x) < 0.9 ? V3{1, 0, 0} : V3{0, 1, 0};
     V3 u = norm(cross(n, a));
@@ -87,6 +329,10 @@ std::vector<int> ccw_hull_2d(const std::vector<V3>& P, const std::vector<int>& i
     return r;
 }
 
+struct RawFace {
+    std::vector<int> idx;  // CCW seen from outside (indices into the grid points)
+};
+
 }  // namespace
 
 bool compute_polyhedron(const float* pts_in, int n, Polyhedron& out, std::string* err) {
@@ -95,62 +341,56 @@ bool compute_polyhedron(const float* pts_in, int n, Polyhedron& out, std::string
         if (err) *err = "need at least 4 points";
         return false;
     }
-    std::vector<V3> P(n);
-    double scale = 0;
-    for (int i = 0; i < n; ++i) {
-        P[i] = {pts_in[3 * i], pts_in[3 * i + 1], pts_in[3 * i + 2]};
-        scale = std::max(scale, std::max(std::fabs(P[i].x), std::max(std::fabs(P[i].y), std::fabs(P[i].z))));
+    // 1. Grid points, duplicates merged (numbered by their first input point).
+    const Grid G = make_grid(pts_in, n);
+    std::vector<IV> Q;
+    {
+        std::unordered_map<uint64_t, int> seen;
+        seen.reserve(2 * (size_t)n);
+        for (int i = 0; i < n; ++i) {
+            const IV v = quantize(G, pts_in + 3 * i);
+            const uint64_t key = ((uint64_t)(v.x + 32768) << 32) | ((uint64_t)(v.y + 32768) << 16) |
+                                 (uint64_t)(v.z + 32768);
+            if (seen.emplace(key, (int)Q.size()).second) Q.push_back(v);
+        }
     }
-    const double eps = 1e-7 * std::max(1.0, scale);
-    // 1. Exhaustive supporting-plane search.
+    std::vector<HTri> tris;
+    if (!exact_hull(Q, tris)) {
+        if (err) *err = "degenerate point set";
+        return false;
+    }
+    // 2. Maximal planar faces: the triangles of one supporting plane.
+    std::map<std::array<int64_t, 4>, std::vector<int>> byPlane;
+    for (const HTri& t : tris) {
+        const int64_t g = gcd64(gcd64(t.n.x, t.n.y), t.n.z);
+        const std::array<int64_t, 4> key = {t.n.x / g, t.n.y / g, t.n.z / g, t.d / g};
+        std::vector<int>& ids = byPlane[key];
+        for (int id : {t.a, t.b, t.c})
+            if (std::find(ids.begin(), ids.end(), id) == ids.end()) ids.push_back(id);
+    }
+    // the grid-to-world map is a per-axis scaling after an axis permutation;
+    // when it reverses orientation the counter-clockwise order flips
+    int perm[3] = {G.medAxis, G.maxAxis, G.minAxis};
+    int inversions = 0;
+    for (int a = 0; a < 3; ++a)
+        for (int b = a + 1; b < 3; ++b)
+            if (perm[a] > perm[b]) ++inversions;
+    const double det = (inversions & 1 ? -1.0 : 1.0) * (double)G.scaling[0] * G.scaling[1] * G.scaling[2];
     std::vector<RawFace> planes;
-    for (int i = 0; i < n; ++i)
-        for (int j = i + 1; j < n; ++j)
-            for (int k = j + 1; k < n; ++k) {
-                V3 nn = cross(sub(P[j], P[i]), sub(P[k], P[i]));
-                double l = len(nn);
-                if (l < 1e-12 * std::max(1.0, scale * scale)) continue;
-                nn = mul(nn, 1.0 / l);
-                double d = dot(nn, P[i]);
-                double mx = -1e300, mn = 1e300;
-                for (int m = 0; m < n; ++m) {
-                    double s = dot(nn, P[m]) - d;
-                    mx = std::max(mx, s);
-                    mn = std::min(mn, s);
-                }
-                if (mx <= eps) {
-                } else if (mn >= -eps) {
-                    nn = mul(nn, -1.0);
-                    d = -d;
-                } else {
-                    continue;
-                }
-                bool dup = false;
-                for (auto& f : planes)
-                    if (dot(f.n, nn) > 1.0 - 1e-9 && std::fabs(f.d - d) < 4 * eps) {
-                        dup = true;
-                        break;
-                    }
-                if (!dup) planes.push_back({nn, d, {}});
-            }
+    for (const auto& kv : byPlane) {
+        const IV nn = {kv.first[0], kv.first[1], kv.first[2]};
+        RawFace f;
+        f.idx = planar_polygon(Q, kv.second, nn);
+        if (det < 0) std::reverse(f.idx.begin(), f.idx.end());
+        if (f.idx.size() >= 3) planes.push_back(f);
+    }
     if (planes.size() < 4) {
         if (err) *err = "degenerate point set";
         return false;
     }
-    for (auto& f : planes) {
-        std::vector<int> on;
-        for (int m = 0; m < n; ++m)
-            if (std::fabs(dot(f.n, P[m]) - f.d) <= 4 * eps) on.push_back(m);
-        // drop duplicate input points (keep first)
-        std::vector<int> uniq;
-        for (int m : on) {
-            bool same = false;
-            for (int u : uniq)
-                if (len(sub(P[m], P[u])) <= eps) same = true;
-            if (!same) uniq.push_back(m);
-        }
-        f.idx = ccw_hull_2d(P, uniq, f.n);
-    }
+    std::vector<V3> P(Q.size());
+    for (size_t i = 0; i < Q.size(); ++i) P[i] = dequantize(G, Q[i]);
+    n = (int)Q.size();
     // Deterministic face order: by the sorted smallest vertex index, then normal.
     std::sort(planes.begin(), planes.end(), [](const RawFace& a, const RawFace& b) {
         std::vector<int> sa = a.idx, sb = b.idx;
@@ -170,20 +410,26 @@ bool compute_polyhedron(const float* pts_in, int n, Polyhedron& out, std::string
             verts.push_back(P[i]);
         }
     // Faces with hull-vertex indices; plane from the first two edges of the
-    // polygon (btConvexUtility: normal = e0 x e1, w = -min over face verts).
+    // polygon, in float as btConvexUtility computes it (:56-108): normal =
+    // normalized(normalized(e0) x normalized(e1)), w = -min over the face's
+    // vertices of v . normal.
     struct TF {
         double plane[4];
         std::vector<int> idx;
     };
+    auto fv = [&](int id) { return F3{(float)verts[id].x, (float)verts[id].y, (float)verts[id].z}; };
     std::vector<TF> tmp;
     for (auto& f : planes) {
         TF t;
         for (int id : f.idx) t.idx.push_back(remap[id]);
-        V3 e0 = norm(sub(verts[t.idx[1]], verts[t.idx[0]]));
-        V3 e1 = norm(sub(verts[t.idx[2]], verts[t.idx[1]]));
-        V3 nn = norm(cross(e0, e1));
-        double pe = 1e30;
-        for (int id : t.idx) pe = std::min(pe, dot(verts[id], nn));
+        const F3 e0 = fnormalized(fsub(fv(t.idx[1]), fv(t.idx[0])));
+        const F3 e1 = fnormalized(fsub(fv(t.idx[2]), fv(t.idx[1])));
+        const F3 nn = fnormalized(fcross(e0, e1));
+        float pe = 1e30f;
+        for (int id : t.idx) {
+            const float eq = fdot(fv(id), nn);
+            if (pe > eq) pe = eq;
+        }
         t.plane[0] = nn.x;
         t.plane[1] = nn.y;
         t.plane[2] = nn.z;
@@ -198,11 +444,11 @@ bool compute_polyhedron(const float* pts_in, int n, Polyhedron& out, std::string
         int ref = todo.back();
         todo.pop_back();
         std::vector<int> group{ref};
-        V3 na{tmp[ref].plane[0], tmp[ref].plane[1], tmp[ref].plane[2]};
+        const F3 na{(float)tmp[ref].plane[0], (float)tmp[ref].plane[1], (float)tmp[ref].plane[2]};
         for (int j = (int)todo.size() - 1; j >= 0; --j) {
             int i = todo[j];
-            V3 nb{tmp[i].plane[0], tmp[i].plane[1], tmp[i].plane[2]};
-            if (dot(na, nb) > 0.999) {
+            const F3 nb{(float)tmp[i].plane[0], (float)tmp[i].plane[1], (float)tmp[i].plane[2]};
+            if (fdot(na, nb) > 0.999f) {
                 group.push_back(i);
                 todo.erase(todo.begin() + j);
             }

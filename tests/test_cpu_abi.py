@@ -149,3 +149,26 @@ def test_adjoint_call_order(host_ctx):
     assert lib.b3_adjoint_forward(None, None) == 1
     assert lib.b3_adjoint_gradients(None, None, None, None, None) == 1
     w.close()
+
+
+def test_large_hull_registers_quickly(host_ctx):
+    """Registration builds the hull in O(points x faces) on the integer
+    grid: 65,536 points of a shell register in well under the time an
+    exhaustive plane search would take, and every point lies inside every
+    face plane of the result."""
+    import time
+    rng = np.random.default_rng(5)
+    p = rng.normal(size=(65536, 3))
+    p /= np.linalg.norm(p, axis=1, keepdims=True)
+    p = (p * rng.uniform(0.5, 1.0, (65536, 1))).astype(np.float32)
+    w = b3.PhysicsWorld(host_ctx, b3.default_config(maxBodies=4))
+    t0 = time.perf_counter()
+    w.registerConvexPolyhedron(p)
+    assert time.perf_counter() - t0 < 10.0
+    sh = w.shapes()
+    poly = sh["polys"][0]
+    assert poly.numVertices > 100 and poly.numFaces > 100
+    planes = np.array([list(sh["faces"][f].plane) for f in range(poly.faceOffset, poly.faceOffset + poly.numFaces)])
+    # grid vertices sit within one grid step (extent / 10216) of the input
+    assert (p @ planes[:, :3].T + planes[:, 3]).max() < 2.0 / 10216 * 2
+    w.close()
