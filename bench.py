@@ -86,16 +86,21 @@ def fp32_peak_tflops(sm_mhz):
     return 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
 
 
+# Per-unit figures from the ncu capture summarised in
+# profiles/kernels_c2s_settled_step.md (settled 16,384-body case, same
+# kernels): FP32 operations each kernel executes (2 per FFMA + FADD + FMUL,
+# per thread) and DRAM bytes (read + write), per pair or per manifold.
+NCU_SOURCE = "profiles/kernels_c2s_settled_step.md (ncu, settled 16,384-body case)"
+NCU_PER_UNIT = {
+    "k_np_sweep": {"fp32_ops_per_pair": 25737.0, "dram_bytes_per_pair": 13.2, "source": NCU_SOURCE},
+    "k_np_clip": {"fp32_ops_per_manifold": 8940.0, "dram_bytes_per_manifold": 154.5, "source": NCU_SOURCE},
+    "k_setup_rows": {"dram_bytes_per_manifold": 288.9, "source": NCU_SOURCE},
+    "k_jacobi": {"dram_bytes_per_manifold": 605.6, "source": NCU_SOURCE},
+}
+
+
 def profile_constants():
-    """Per-unit figures read from ncu captures (profiles/ncu_constants.json):
-    FP32 operations each kernel executes per unit (2 per FFMA + FADD + FMUL,
-    per thread, from smsp__sass_thread_inst_executed_op_*_pred_on.sum) and
-    its DRAM bytes per unit, on the settled 16,384-body case."""
-    try:
-        with open(os.path.join(ROOT, "profiles", "ncu_constants.json")) as f:
-            return json.load(f)
-    except Exception:
-        return {}
+    return NCU_PER_UNIT
 
 
 def peaks():
@@ -361,13 +366,18 @@ def oracle_check(w, sc):
     import oracle
     from oracle import parity
     o = oracle.oracle_from_world(w, sc)
-    rep = parity.one_step_report(w, o, dynamic=np.asarray(sc.mass) > 0)
+    rep = parity.one_step_report(w, o, dynamic=np.asarray(sc.mass) > 0,
+                                 make_oracle=lambda f32: oracle.oracle_from_world(w, sc, f32=f32))
     o.close()
     keep = ["pos_err_m", "lin_vel_err_mps", "ang_vel_err_radps", "quat_err", "contact_point_err_m", "normal_err",
             "aabbs_bit_exact", "keys_bit_exact", "permutation_bit_exact", "pairs_bit_exact", "manifold_set_equal",
-            "pairs", "manifolds", "within_bars", "check_s"]
+            "pairs", "manifolds", "pair_overflow", "narrowphase_within_bars", "solver_err", "fp32_envelope",
+            "bars_used", "within_bars", "check_s"]
     out = {k: rep[k] for k in keep}
-    out["bars"] = "pairs/keys/permutation bit-exact; contacts 1e-5 m, normals 1e-4; one step 1e-5 m, 1e-4 m/s"
+    out["bars"] = ("pairs/keys/permutation bit-exact; contacts 1e-5 m, normals 1e-4; one step 1e-5 m, 1e-4 m/s, or "
+                   "twice the FP32 envelope (the oracle's FP32 build against its FP64 build from the same contacts) "
+                   "where that is larger; solver_err: the device's solve against the FP64 oracle's from the "
+                   "device's contacts")
     return out
 
 

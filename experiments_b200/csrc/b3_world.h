@@ -33,6 +33,7 @@ struct ShapesDev {
     const float4* edges;
     const float4* localAabb;  // 2 per collidable (min, max)
     const float* inradius;    // per polyhedron: lower bound of its support about localCenter
+    const float2* faceExt;    // per face: (min, max) over its hull's vertices of n . v (local frame)
     int numPolys, numVerts, numFaces, numIndices, numEdges;
     int tableBytes;           // packed size for shared-memory staging
 };
@@ -65,6 +66,7 @@ struct DevBuffers {
     float4* edges = nullptr;
     float4* localAabb = nullptr;
     float* polyInradius = nullptr;
+    float2* faceExt = nullptr;  // per face: the hull's extent along the face normal
     // broadphase
     float4 *aabbMin = nullptr, *aabbMax = nullptr;
     int* smallSlot = nullptr;      // body -> slot in the hash arrays, -1 = large
@@ -157,6 +159,7 @@ struct b3World_t {
     std::vector<b3ConvexPolyhedron> polys;
     std::vector<float> verts4, edges4, localAabb8;
     std::vector<float> polyInradius;
+    std::vector<float> faceExt;   // 2 per face: min, max of n . v over the face's hull
     std::vector<b3Face> faces;
     std::vector<int> indices;
     std::vector<int> worldIds;

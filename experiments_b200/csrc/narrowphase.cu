@@ -51,10 +51,11 @@ constexpr int kPreChunk = 4;  // pairs per work grab of the sweep and the clip, 
 constexpr int kSweepWarpSmem = 128 * kPreChunk + 4 * kMaxCand;
 constexpr int kNone = 0x7fffffff;
 // pairSep[p].w: how the pair reached the exact stage
+// pairSep[p].w: how the pair reached the exact stage
 constexpr int kSepRefine = 0;      // near-minimum axes: float-float re-ranking
 constexpr int kSepDecided = 1;     // FP32 axis (FP32 clip stage)
-constexpr int kSepClipDoubt = 2;   // FP32 axis, clipping in doubt
-constexpr int kSepReduceTie = 3;   // FP32 axis and clip, reduction tie
+constexpr int kSepClipDoubt = 2;   // FP32 axis, clip or reduction in doubt: float-float clip
+constexpr int kSepFaceTie = 3;     // FP32 axis, clip faces near-tied: float-float axis, then clip
 
 struct NpParams {
     float minDist;
@@ -198,7 +199,7 @@ __device__ __forceinline__ void project_rel(const float4* __restrict__ verts, in
 // near-minimum candidates (depth - err <= the minimum's depth + err).
 __device__ __forceinline__ bool axis_dir(const PairCtx& c, const b3::ShapesDev& S, int idx, float3 D, float delta,
                                          float rinSum, float3& n, float& err, float& lb, bool& isFace,
-                                         bool wantLb = true) {
+                                         bool wantLb = true, bool* flipped = nullptr) {
     const b3ConvexPolyhedron& pa = *c.pa;
     const b3ConvexPolyhedron& pb = *c.pb;
     const int FA = pa.numFaces, FB = pb.numFaces;
@@ -226,7 +227,9 @@ __device__ __forceinline__ bool axis_dir(const PairCtx& c, const b3::ShapesDev& 
         err = delta + 0.3f * delta / cl;
         lb = wantLb ? rinSum - fabsf(dot(D, n)) - 1e-5f * (1.f + lD) - 1e-6f * lD / cl - 2.f * err : -FLT_MAX;
     }
-    if (dot(D, n) < 0.f) n = -n;
+    const bool f = dot(D, n) < 0.f;
+    if (f) n = -n;
+    if (flipped) *flipped = f;
     return true;
 }
 
@@ -238,6 +241,33 @@ __device__ __forceinline__ float axis_depth(const PairCtx& c, const b3::ShapesDe
     float mn0, mx0, mn1, mx1;
     project_rel(S.verts, pa.vertexOffset, pa.numVertices, c.RA, n, mn0, mx0);
     project_rel(S.verts, pb.vertexOffset, pb.numVertices, c.RB, n, mn1, mx1);
+    const float off = dot(rel, n);  // posB - posA along n
+    mn1 += off;
+    mx1 += off;
+    return fminf(mx0 - mn1, mx1 - mn0);
+}
+
+// FP32 depth along the oriented face axis n of face idx (flipped: n is
+// the negated face normal). The face's own hull projects onto its normal
+// over the registered extent (faceExt, exact and rounded outward), so only
+// the other hull's vertices are projected.
+__device__ __forceinline__ float face_axis_depth(const PairCtx& c, const b3::ShapesDev& S, int idx, float3 rel,
+                                                 float3 n, bool flipped) {
+    const b3ConvexPolyhedron& pa = *c.pa;
+    const b3ConvexPolyhedron& pb = *c.pb;
+    const bool onA = idx < pa.numFaces;
+    const float2 ext = __ldg(&S.faceExt[onA ? pa.faceOffset + idx : pb.faceOffset + idx - pa.numFaces]);
+    const float lo = flipped ? -ext.y : ext.x, hi = flipped ? -ext.x : ext.y;
+    float mn0, mx0, mn1, mx1;
+    if (onA) {
+        mn0 = lo;
+        mx0 = hi;
+        project_rel(S.verts, pb.vertexOffset, pb.numVertices, c.RB, n, mn1, mx1);
+    } else {
+        project_rel(S.verts, pa.vertexOffset, pa.numVertices, c.RA, n, mn0, mx0);
+        mn1 = lo;
+        mx1 = hi;
+    }
     const float off = dot(rel, n);  // posB - posA along n
     mn1 += off;
     mx1 += off;
@@ -407,9 +437,10 @@ __device__ __forceinline__ int sweep_axes(PairCtx& c, const b3::ShapesDev& S, in
         for (int idx = i0 + lane; idx < i1; idx += 32) {
             float3 n;
             float err, lb;
-            bool isFace;
-            if (!axis_dir(c, S, idx, D, delta, rinSum, n, err, lb, isFace, pass == 1) || lb > lbHi) continue;
-            const float d = axis_depth(c, S, rel, n);
+            bool isFace, flipped;
+            if (!axis_dir(c, S, idx, D, delta, rinSum, n, err, lb, isFace, pass == 1, &flipped) || lb > lbHi)
+                continue;
+            const float d = isFace ? face_axis_depth(c, S, idx, rel, n, flipped) : axis_depth(c, S, rel, n);
             if (isFace) {
                 sepMin = fminf(sepMin, d);
                 if (fabsf(d) <= delta) {
@@ -617,13 +648,16 @@ __device__ __noinline__ bool refine_axes(PairCtx& c, const b3::ShapesDev& S, War
 }
 
 // Separating-axis search: the FP32 sweep, then the float-float re-ranking
-// when the sweep leaves near-minimum candidates.
-__device__ __noinline__ bool find_axis(PairCtx& c, const b3::ShapesDev& S, WarpScratch& W, ff3& sep, int* ovfCounter) {
+// when the sweep leaves near-minimum candidates. exact: the axis is needed
+// to float-float accuracy (clip faces near-tied along it), so a winner the
+// FP32 sweep decided is re-evaluated in float-float too.
+__device__ __noinline__ bool find_axis(PairCtx& c, const b3::ShapesDev& S, WarpScratch& W, ff3& sep, int* ovfCounter,
+                                       bool exact = false) {
     float3 sepf;
     int count = 0;
     const int r = sweep_axes<false>(c, S, W.cand, sepf, count, ovfCounter);
     if (r == 0) return false;
-    if (r == 1) {
+    if (r == 1 && !(exact && count >= 1)) {
         sep = mk3(sepf.x, sepf.y, sepf.z);
         return true;
     }
@@ -962,7 +996,11 @@ __device__ __forceinline__ int near_count(float best, float v, bool valid, float
 }
 
 // FP32 extractManifoldSequentialGlobal; *tie set when an arg-min is within
-// FP32 error of another candidate or of the FLT_MIN threshold.
+// the error of its inputs of another candidate or of the FLT_MIN threshold.
+// The points carry the FP32 clip's error (the 4e-6 m cut budget plus the
+// rounding of world coordinates); the directions u and v come from the
+// first point minus the centre, so their error grows as that vector
+// shortens. A tie sends the pair to the float-float clip and reduction.
 __device__ __noinline__ int4 reduce_f32(const FfVert* p, int n, float3 nearNormal, bool* tie) {
     const int lane = threadIdx.x & 31;
     const float3 o = get_f32(p[0]);  // subtract a point first: world magnitudes cancel
@@ -977,9 +1015,21 @@ __device__ __noinline__ int4 reduce_f32(const FfVert* p, int n, float3 nearNorma
     const float3 cr = s * (1.f / (float)n);  // centre relative to o
     const float3 aV = -cr;
     float3 u = cross(nearNormal, aV);
+    const float ul = length(u);
     float3 v = cross(nearNormal, u);
     u = normalize(u);
     v = normalize(v);
+    // error bounds of the points (eP) and of the directions (du)
+    float pm = 0.f, rm = 0.f;
+    for (int k = lane; k < n; k += 32) {
+        const float3 q = get_f32(p[k]);
+        pm = fmaxf(pm, len_ub(q));
+        rm = fmaxf(rm, len_ub((q - o) - cr));
+    }
+    pm = warp_max(pm);
+    rm = warp_max(rm);
+    const float eP = 4e-6f + 1.2e-7f * pm;
+    const float du = 2.f * eP / fmaxf(ul, 1e-30f) + 4e-7f;
     float fw[2], fu[2], fv[2];
     float mw = FLT_MAX, f0 = FLT_MIN, f1 = FLT_MIN, f2 = FLT_MIN, f3v = FLT_MIN;
     int iw = kNone, i0 = kNone, i1 = kNone, i2 = kNone, i3 = kNone;
@@ -1006,7 +1056,7 @@ __device__ __noinline__ int4 reduce_f32(const FfVert* p, int n, float3 nearNorma
     warp_argmin(f1, i1);
     warp_argmin(f2, i2);
     warp_argmin(f3v, i3);
-    const float gap = 2e-6f, gapw = 1e-6f;
+    const float gap = 2.f * (2.f * eP + rm * du) + 1e-6f, gapw = 2.f * eP + 1e-6f;
     int worst = 0;
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
@@ -1030,7 +1080,7 @@ __device__ __noinline__ int4 reduce_f32(const FfVert* p, int n, float3 nearNorma
 // comparisons: the first extreme face wins). FP32 sweep, then faces within
 // a small window of the FP32 extreme are re-ranked in float-float.
 __device__ __noinline__ int select_face(const b3::ShapesDev& S, PairCtx& c, bool sideA, float3 sepf, ff3 sep,
-                                        float sign) {
+                                        float sign, bool* tied = nullptr) {
     const b3ConvexPolyhedron& h = sideA ? *c.pa : *c.pb;
     const Mat3& R = sideA ? c.RA : c.RB;
     const int lane = threadIdx.x & 31;
@@ -1061,6 +1111,9 @@ __device__ __noinline__ int select_face(const b3::ShapesDev& S, PairCtx& c, bool
         inWin = __reduce_add_sync(0xffffffffu, inWin);
     }
     if (inWin <= 1) return wi;
+    // faces within the window: the choice follows the axis to float-float
+    // accuracy, which the caller may have only to FP32
+    if (tied) *tied = true;
     ensure_ff(c);
     const ffmat& F = sideA ? c.FA : c.FB;
     ff rv = mk(FLT_MAX);
@@ -1409,21 +1462,25 @@ k_np_clip(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, NpP
             const float3 sepf = make_float3(s4.x, s4.y, s4.z);
             const ff3 sep = mk3(sepf.x, sepf.y, sepf.z);
             // incident face of B: max dot(nB, sep); reference face of A: min dot(nA, sep)
-            const int bi = select_face(S, c, false, sepf, sep, -1.f);
-            const int ai = select_face(S, c, true, sepf, sep, 1.f);
+            bool faceTie = false;
+            const int bi = select_face(S, c, false, sepf, sep, -1.f, &faceTie);
+            const int ai = select_face(S, c, true, sepf, sep, 1.f, &faceTie);
             int buf = 0;
             bool slow = false;
-            const int nOut = clip_f32(c, S, P, ai, bi, W, &buf, &slow, &counters->clipOverflow);
+            int nOut = 0;
+            if (!faceTie) nOut = clip_f32(c, S, P, ai, bi, W, &buf, &slow, &counters->clipOverflow);
             int4 idx = make_int4(0, 1, 2, 3);
             int nRed = nOut;
             bool tie = false;
-            if (!slow && nOut > 4) {
+            if (!faceTie && !slow && nOut > 4) {
                 idx = reduce_f32(W.poly[buf], min(nOut, kMaxPoly), -sepf, &tie);
                 nRed = 4;
             }
-            if (slow || tie) {
-                // the exact stage redoes only the part in doubt
-                if (lane == 0) pairSep[p].w = (float)(slow ? kSepClipDoubt : kSepReduceTie);
+            if (faceTie || slow || tie) {
+                // the exact stage redoes the part in doubt: the axis (faces
+                // near-tied along it), or the clip (its own doubt, or a
+                // reduction decided by points within their error bound)
+                if (lane == 0) pairSep[p].w = (float)(faceTie ? kSepFaceTie : kSepClipDoubt);
                 push(slowQ, scalars + b3::S_NP_SLOW, p);
             } else if (nOut > 0) {
                 emit_contact(p, c, W.poly[buf], nRed, idx, -sepf, Bd, P, contacts, manifoldFlag);
@@ -1510,6 +1567,7 @@ k_np_exact(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, Np
             const float4 s4 = pairSep[p];
             const int why = (int)s4.w;
             bool haveAxis;
+            bool exactAxis = false;  // sep known to float-float accuracy
             if (why == kSepRefine) {
                 const int count = __float_as_int(s4.x);
                 if (count > 0) {
@@ -1518,20 +1576,36 @@ k_np_exact(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, Np
                     __syncwarp();
                     if (lane == 0) ++W.refinedAxes;
                     haveAxis = refine_axes(c, S, W, count, sep);
+                    exactAxis = true;
                 } else {
                     haveAxis = find_axis(c, S, W, sep, &counters->clipOverflow);
                 }
+            } else if (why == kSepFaceTie) {
+                // clip faces near-tied along the FP32 axis: the axis in float-float
+                if (lane == 0) ++W.refinedAxes;
+                haveAxis = find_axis(c, S, W, sep, &counters->clipOverflow, true);
+                exactAxis = true;
             } else {
                 // axis decided by the FP32 sweep
                 sep = mk3(s4.x, s4.y, s4.z);
                 haveAxis = true;
             }
+            int ai = kNone, bi = kNone;
             if (haveAxis) {
-                const float3 sepf = to_f3(sep);
                 // incident face of B: max dot(nB, sep); reference face of A: min dot(nA, sep)
-                const int bi = select_face(S, c, false, sepf, sep, -1.f);
-                const int ai = select_face(S, c, true, sepf, sep, 1.f);
-                bool doubt = why == kSepClipDoubt;
+                bool faceTie = false;
+                bi = select_face(S, c, false, to_f3(sep), sep, -1.f, &faceTie);
+                ai = select_face(S, c, true, to_f3(sep), sep, 1.f, &faceTie);
+                if (faceTie && !exactAxis) {
+                    haveAxis = find_axis(c, S, W, sep, &counters->clipOverflow, true);
+                    if (haveAxis) {
+                        bi = select_face(S, c, false, to_f3(sep), sep, -1.f);
+                        ai = select_face(S, c, true, to_f3(sep), sep, 1.f);
+                    }
+                }
+            }
+            if (haveAxis) {
+                bool doubt = why == kSepClipDoubt || why == kSepFaceTie;
                 if (!doubt) nOut = clip_f32(c, S, P, ai, bi, W, &buf, &doubt, &counters->clipOverflow);
                 if (doubt) {
                     if (lane == 0) ++W.refinedClips;

@@ -35,6 +35,9 @@ __global__ void k_step_begin(int32_t* scalars, b3Counters* counters) {
         counters->numPairs = 0;
         counters->refinedAxes = 0;
         counters->refinedClips = 0;
+        counters->pairOverflow = 0;
+        counters->cellOverflow = 0;
+        counters->clipOverflow = 0;
     }
 }
 
@@ -66,7 +69,7 @@ int dalloc(T*& p, size_t count) {
 void free_all(b3::DevBuffers& d) {
     void* ptrs[] = {d.pos, d.quat, d.linVel, d.angVel, d.invMass, d.friction, d.restitution,
                     d.invInertia, d.collidable, d.worldId, d.cols, d.polys, d.verts, d.faces,
-                    d.indices, d.edges, d.localAabb, d.polyInradius, d.aabbMin, d.aabbMax, d.smallSlot,
+                    d.indices, d.edges, d.localAabb, d.polyInradius, d.faceExt, d.aabbMin, d.aabbMax, d.smallSlot,
                     d.largeStart, d.largeList, d.sapSmall, d.sapLarge, d.sapSorted, d.sapCount, d.sapOffset, d.keys, d.vals, d.keysAlt, d.valsAlt, d.cellTable,
                     d.pairs, d.contacts, d.manifoldFlag, d.pairSep, d.npFast, d.npSlow, d.npCand, d.manifoldScan,
                     d.manifoldPair,
@@ -136,6 +139,7 @@ b3::ShapesDev b3World_t::shapesDev() const {
     S.edges = d.edges;
     S.localAabb = d.localAabb;
     S.inradius = d.polyInradius;
+    S.faceExt = d.faceExt;
     S.numPolys = (int)polys.size();
     S.numVerts = (int)verts4.size() / 4;
     S.numFaces = (int)faces.size();
@@ -292,6 +296,20 @@ extern "C" int b3_register_convex_hull(b3World w, const float* vertices, int num
         ff.pad[0] = off <= 1e-6 * mag ? 1 : 0;
         for (int id : f.indices) w->indices.push_back(id);
         w->faces.push_back(ff);
+        // the hull's extent along the face normal: every face axis of this
+        // hull needs only the other hull's projection (rounded outward)
+        double lo = 1e300, hi = -1e300;
+        for (int i = 0; i < (int)P.vertices.size() / 3; ++i) {
+            const double d = (double)ff.plane[0] * P.vertices[3 * i] + (double)ff.plane[1] * P.vertices[3 * i + 1] +
+                             (double)ff.plane[2] * P.vertices[3 * i + 2];
+            lo = std::min(lo, d);
+            hi = std::max(hi, d);
+        }
+        float flo = (float)lo, fhi = (float)hi;
+        if ((double)flo > lo) flo = std::nextafter(flo, -1e30f);
+        if ((double)fhi < hi) fhi = std::nextafter(fhi, 1e30f);
+        w->faceExt.push_back(flo);
+        w->faceExt.push_back(fhi);
     }
     poly.numUniqueEdges = (int)P.uniqueEdges.size() / 3;
     poly.uniqueEdgesOffset = (int)w->edges4.size() / 4;
@@ -494,6 +512,7 @@ static int upload_shapes(b3World w, cudaStream_t st) {
     B3_TRY(dalloc(d.edges, w->edges4.size() / 4 + 1));
     B3_TRY(dalloc(d.localAabb, w->localAabb8.size() / 4));
     B3_TRY(dalloc(d.polyInradius, w->polyInradius.size()));
+    B3_TRY(dalloc(d.faceExt, w->faceExt.size() / 2));
     B3_CUDA(cudaMemcpyAsync(d.cols, w->cols.data(), sizeof(b3Collidable) * w->cols.size(), cudaMemcpyHostToDevice, st));
     B3_CUDA(cudaMemcpyAsync(d.polys, w->polys.data(), sizeof(b3ConvexPolyhedron) * w->polys.size(), cudaMemcpyHostToDevice, st));
     B3_CUDA(cudaMemcpyAsync(d.verts, w->verts4.data(), sizeof(float) * w->verts4.size(), cudaMemcpyHostToDevice, st));
@@ -504,6 +523,9 @@ static int upload_shapes(b3World w, cudaStream_t st) {
     B3_CUDA(cudaMemcpyAsync(d.localAabb, w->localAabb8.data(), sizeof(float) * w->localAabb8.size(), cudaMemcpyHostToDevice, st));
     B3_CUDA(cudaMemcpyAsync(d.polyInradius, w->polyInradius.data(), sizeof(float) * w->polyInradius.size(),
                             cudaMemcpyHostToDevice, st));
+    if (!w->faceExt.empty())
+        B3_CUDA(cudaMemcpyAsync(d.faceExt, w->faceExt.data(), sizeof(float) * w->faceExt.size(),
+                                cudaMemcpyHostToDevice, st));
     w->shapesDirty = false;
     return B3_OK;
 }

@@ -135,15 +135,17 @@ typedef struct b3Constraint4 {
     uint32_t padding;
 } b3Constraint4;
 
-/* Step diagnostics (the reference truncates silently; the build counts). */
+/* Step diagnostics (the reference truncates silently; the build counts).
+ * Every count is of the last step, except timeouts and steps, which
+ * accumulate until b3_reset_counters. */
 typedef struct b3Counters {
     int32_t numPairs;            /* broadphase pairs this step */
     int32_t numManifolds;        /* contact manifolds this step */
     int32_t numContactPoints;    /* sum of manifold points */
-    int32_t pairOverflow;        /* pairs dropped: per-body or global cap */
-    int32_t cellOverflow;        /* candidates skipped by the per-cell cap */
+    int32_t pairOverflow;        /* pairs dropped this step: per-body or global cap */
+    int32_t cellOverflow;        /* candidates skipped by the per-cell cap this step */
     int32_t timeouts;            /* bounded device waits that gave up */
-    int32_t clipOverflow;        /* clipped polygons truncated to 64 verts */
+    int32_t clipOverflow;        /* clipped polygons truncated to 64 verts this step */
     int32_t steps;               /* steps executed since write_bodies */
     int32_t refinedAxes;         /* pairs whose axis choice was re-ranked in float-float */
     int32_t refinedClips;        /* pairs whose clipping was redone in float-float */

@@ -32,6 +32,11 @@ class OrContact(C.Structure):
                 ("pairIndex", C.c_int), ("bodyA", C.c_int), ("bodyB", C.c_int), ("pad", C.c_int)]
 
 
+# OrContact as a numpy record (same field order and packing)
+_OR_CONTACT_DTYPE = np.dtype([("pos", "<f8", (4, 4)), ("normal", "<f8", 4), ("friction", "<f8"),
+                              ("pairIndex", "<i4"), ("bodyA", "<i4"), ("bodyB", "<i4"), ("pad", "<i4")])
+assert _OR_CONTACT_DTYPE.itemsize == C.sizeof(OrContact)
+
 _ref = None
 _bullet = None
 _D = C.POINTER(C.c_double)
@@ -304,17 +309,15 @@ class OracleWorld:
 
     def set_contacts(self, c):
         n = len(c["normal"])
-        arr = (OrContact * max(n, 1))()
-        for j in range(n):
-            for a in range(4):
-                for b in range(4):
-                    arr[j].pos[a][b] = float(c["pos"][j][a][b])
-                arr[j].normal[a] = float(c["normal"][j][a])
-            arr[j].friction = float(c["friction"][j])
-            arr[j].pairIndex = int(c["pairIndex"][j])
-            arr[j].bodyA = int(c["bodyA"][j])
-            arr[j].bodyB = int(c["bodyB"][j])
-        self.L.or_set_contacts(self.h, arr, n)
+        rec = np.zeros(max(n, 1), dtype=_OR_CONTACT_DTYPE)
+        if n:
+            rec["pos"][:n] = np.asarray(c["pos"], np.float64).reshape(n, 4, 4)
+            rec["normal"][:n] = np.asarray(c["normal"], np.float64).reshape(n, 4)
+            rec["friction"][:n] = np.asarray(c["friction"], np.float64)
+            rec["pairIndex"][:n] = np.asarray(c["pairIndex"], np.int32)
+            rec["bodyA"][:n] = np.asarray(c["bodyA"], np.int32)
+            rec["bodyB"][:n] = np.asarray(c["bodyB"], np.int32)
+        self.L.or_set_contacts(self.h, C.cast(rec.ctypes.data, C.POINTER(OrContact)), n)
 
     def overflow(self):
         a, b = C.c_longlong(), C.c_longlong()
