@@ -51,6 +51,14 @@ class Collidable(C.Structure):
                 ("shapeIndex", C.c_int)]
 
 
+class ChildShape(C.Structure):
+    _fields_ = [("childPosition", C.c_float * 4), ("childOrientation", C.c_float * 4), ("shapeIndex", C.c_int),
+                ("unused", C.c_int * 3)]
+
+
+SHAPE_CONVEX_HULL, SHAPE_PLANE, SHAPE_CONCAVE_TRIMESH, SHAPE_COMPOUND, SHAPE_SPHERE = 3, 4, 5, 6, 7
+
+
 class ConvexPolyhedron(C.Structure):
     _fields_ = [("localCenter", C.c_float * 4), ("extents", C.c_float * 4), ("mC", C.c_float * 4),
                 ("mE", C.c_float * 4), ("radius", C.c_float), ("faceOffset", C.c_int),
@@ -125,6 +133,11 @@ SIGNATURES = [
     ("b3_radix_sort32_keys", _I, [_P, _P, _I64, _I, _P]),
     ("b3_bound_search", _I, [_P, _P, _I64, _P, _I64, _I, _P]),
     ("b3_set_wait_limits", _I, [_P, _I, _I]),
+    ("b3_register_sphere", _I, [_P, C.c_float, _IP]),
+    ("b3_register_plane", _I, [_P, _FP, C.c_float, _IP]),
+    ("b3_register_compound", _I, [_P, _P, _I, _IP]),
+    ("b3_register_concave_mesh", _I, [_P, _FP, _I, _IP, _I, _FP, _IP]),
+    ("b3_get_child_shapes", _I, [_P, _P, _I, _IP]),
     ("b3_radix_sort32_kv_out", _I, [_P, _P, _P, _P, _P, _I64, _I, _P]),
     ("b3_radix_sort32_sortdata", _I, [_P, _P, _I64, _I, _P]),
     ("b3_bound_search_sortdata", _I, [_P, _P, _I64, _P, _I64, _I, _P]),
@@ -392,6 +405,46 @@ class PhysicsWorld:
         _check(self.lib.b3_register_convex_hull(self.h, fptr(v), v.shape[0], 12, fptr(s), C.byref(out)),
                "b3_register_convex_hull")
         return out.value
+
+    def registerSphereShape(self, radius):
+        out = C.c_int()
+        _check(self.lib.b3_register_sphere(self.h, float(radius), C.byref(out)), "b3_register_sphere")
+        return out.value
+
+    def registerPlaneShape(self, normal, constant):
+        n = np.ascontiguousarray(np.asarray(normal, np.float32).reshape(3))
+        out = C.c_int()
+        _check(self.lib.b3_register_plane(self.h, fptr(n), float(constant), C.byref(out)), "b3_register_plane")
+        return out.value
+
+    def registerCompoundShape(self, children):
+        """children: list of (convex hull collidable, position xyz, orientation xyzw)."""
+        arr = (ChildShape * len(children))()
+        for k, (col, pos, orn) in enumerate(children):
+            arr[k].shapeIndex = int(col)
+            for i in range(3):
+                arr[k].childPosition[i] = float(pos[i])
+            for i in range(4):
+                arr[k].childOrientation[i] = float(orn[i])
+        out = C.c_int()
+        _check(self.lib.b3_register_compound(self.h, arr, len(children), C.byref(out)), "b3_register_compound")
+        return out.value
+
+    def registerConcaveMesh(self, vertices, indices, scaling=(1.0, 1.0, 1.0)):
+        v = np.ascontiguousarray(np.asarray(vertices, np.float32).reshape(-1, 3))
+        ix = np.ascontiguousarray(np.asarray(indices, np.int32).reshape(-1))
+        sc = np.ascontiguousarray(np.asarray(scaling, np.float32).reshape(3))
+        out = C.c_int()
+        _check(self.lib.b3_register_concave_mesh(self.h, fptr(v), v.shape[0], iptr(ix), ix.shape[0], fptr(sc),
+                                                 C.byref(out)), "b3_register_concave_mesh")
+        return out.value
+
+    def child_shapes(self):
+        cnt = C.c_int()
+        _check(self.lib.b3_get_child_shapes(self.h, None, 0, C.byref(cnt)), "b3_get_child_shapes")
+        arr = (ChildShape * max(cnt.value, 1))()
+        _check(self.lib.b3_get_child_shapes(self.h, arr, cnt.value, C.byref(cnt)), "b3_get_child_shapes")
+        return arr, cnt.value
 
     def registerPhysicsInstance(self, mass, position, orientation, collidable, friction=1.0,
                                 restitution=0.0, world_id=0):

@@ -67,6 +67,7 @@ struct DevBuffers {
     float4* localAabb = nullptr;
     float* polyInradius = nullptr;
     float2* faceExt = nullptr;  // per face: the hull's extent along the face normal
+    b3ChildShape* childShapes = nullptr;
     // broadphase
     float4 *aabbMin = nullptr, *aabbMax = nullptr;
     int* smallSlot = nullptr;      // body -> slot in the hash arrays, -1 = large
@@ -160,6 +161,8 @@ struct b3World_t {
     std::vector<float> verts4, edges4, localAabb8;
     std::vector<float> polyInradius;
     std::vector<float> faceExt;   // 2 per face: min, max of n . v over the face's hull
+    std::vector<b3ChildShape> childShapes;  // children of the compounds
+    int numSpheres = 0, numPlanes = 0, numCompounds = 0, numMeshes = 0;
     std::vector<b3Face> faces;
     std::vector<int> indices;
     std::vector<int> worldIds;

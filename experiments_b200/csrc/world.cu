@@ -14,6 +14,7 @@
 #include "b3_world.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 
@@ -69,7 +70,7 @@ int dalloc(T*& p, size_t count) {
 void free_all(b3::DevBuffers& d) {
     void* ptrs[] = {d.pos, d.quat, d.linVel, d.angVel, d.invMass, d.friction, d.restitution,
                     d.invInertia, d.collidable, d.worldId, d.cols, d.polys, d.verts, d.faces,
-                    d.indices, d.edges, d.localAabb, d.polyInradius, d.faceExt, d.aabbMin, d.aabbMax, d.smallSlot,
+                    d.indices, d.edges, d.localAabb, d.polyInradius, d.faceExt, d.childShapes, d.aabbMin, d.aabbMax, d.smallSlot,
                     d.largeStart, d.largeList, d.sapSmall, d.sapLarge, d.sapSorted, d.sapCount, d.sapOffset, d.keys, d.vals, d.keysAlt, d.valsAlt, d.cellTable,
                     d.pairs, d.contacts, d.manifoldFlag, d.pairSep, d.npFast, d.npSlow, d.npCand, d.manifoldScan,
                     d.manifoldPair,
@@ -335,6 +336,242 @@ extern "C" int b3_register_convex_hull(b3World w, const float* vertices, int num
     return B3_OK;
 }
 
+// Appends a collidable with its local AABB; returns its index.
+static int add_collidable(b3World w, int type, int shapeIndex, float radius, int numChildren, const float mn[3],
+                          const float mx[3]) {
+    b3Collidable col;
+    col.numChildShapes = numChildren;
+    col.radius = radius;
+    col.shapeType = type;
+    col.shapeIndex = shapeIndex;
+    w->cols.push_back(col);
+    for (int k = 0; k < 3; ++k) w->localAabb8.push_back(mn[k]);
+    w->localAabb8.push_back(0.f);
+    for (int k = 0; k < 3; ++k) w->localAabb8.push_back(mx[k]);
+    w->localAabb8.push_back(0.f);
+    w->shapesDirty = true;
+    return (int)w->cols.size() - 1;
+}
+
+extern "C" int b3_register_sphere(b3World w, float radius, int* collidableOut) {
+    if (!w || !collidableOut || !(radius > 0.f)) return B3_ERR_INVALID_ARG;
+    const float mn[3] = {-radius, -radius, -radius}, mx[3] = {radius, radius, radius};
+    // registerSphereShape: shapeIndex 0, the radius in the collidable
+    *collidableOut = add_collidable(w, B3_SHAPE_SPHERE, 0, radius, 0, mn, mx);
+    ++w->numSpheres;
+    return B3_OK;
+}
+
+extern "C" int b3_register_plane(b3World w, const float normal[3], float planeConstant, int* collidableOut) {
+    if (!w || !normal || !collidableOut) return B3_ERR_INVALID_ARG;
+    // registerFace: the plane as one face of the shared face table
+    b3Face f;
+    memset(&f, 0, sizeof(f));
+    for (int k = 0; k < 3; ++k) f.plane[k] = normal[k];
+    f.plane[3] = planeConstant;
+    const int face = (int)w->faces.size();
+    w->faces.push_back(f);
+    w->faceExt.push_back(0.f);
+    w->faceExt.push_back(0.f);
+    const float mn[3] = {-1e30f, -1e30f, -1e30f}, mx[3] = {1e30f, 1e30f, 1e30f};
+    *collidableOut = add_collidable(w, B3_SHAPE_PLANE, face, planeConstant, 0, mn, mx);
+    ++w->numPlanes;
+    return B3_OK;
+}
+
+extern "C" int b3_register_compound(b3World w, const b3ChildShape* children, int numChildren, int* collidableOut) {
+    if (!w || !children || numChildren <= 0 || !collidableOut) return B3_ERR_INVALID_ARG;
+    float mn[3] = {1e30f, 1e30f, 1e30f}, mx[3] = {-1e30f, -1e30f, -1e30f};
+    for (int i = 0; i < numChildren; ++i) {
+        const int c = children[i].shapeIndex;
+        if (c < 0 || c >= (int)w->cols.size() || w->cols[c].shapeType != B3_SHAPE_CONVEX_HULL) {
+            b3_set_error("compound child %d: collidable %d is not a convex hull", i, c);
+            return B3_ERR_INVALID_ARG;
+        }
+    }
+    // the union of the children's local AABBs at their poses (btTransformAabb, margin 0)
+    for (int i = 0; i < numChildren; ++i) {
+        const float* la = &w->localAabb8[8 * (size_t)children[i].shapeIndex];
+        float a[3], b[3];
+        transform_aabb(la, la + 4, 0.f, children[i].childPosition, children[i].childOrientation, a, b);
+        for (int k = 0; k < 3; ++k) {
+            mn[k] = std::min(mn[k], a[k]);
+            mx[k] = std::max(mx[k], b[k]);
+        }
+    }
+    const int first = (int)w->childShapes.size();
+    for (int i = 0; i < numChildren; ++i) w->childShapes.push_back(children[i]);
+    *collidableOut = add_collidable(w, B3_SHAPE_COMPOUND_OF_CONVEX_HULLS, first, 0.f, numChildren, mn, mx);
+    ++w->numCompounds;
+    return B3_OK;
+}
+
+// float helpers in btVector3's operation order (the mesh's face planes)
+static inline void fcross3(const float a[3], const float b[3], float r[3]) {
+    r[0] = a[1] * b[2] - a[2] * b[1];
+    r[1] = a[2] * b[0] - a[0] * b[2];
+    r[2] = a[0] * b[1] - a[1] * b[0];
+}
+static inline float fdot3(const float a[3], const float b[3]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+static inline void fnormalize3(float a[3]) {
+    const float r = 1.f / std::sqrt(fdot3(a, a));
+    for (int k = 0; k < 3; ++k) a[k] *= r;
+}
+
+extern "C" int b3_register_concave_mesh(b3World w, const float* vertices3, int numVertices, const int* indices,
+                                        int numIndices, const float scaling[3], int* collidableOut) {
+    if (!w || !vertices3 || numVertices < 3 || !indices || numIndices < 3 || numIndices % 3 != 0 || !collidableOut)
+        return B3_ERR_INVALID_ARG;
+    for (int i = 0; i < numIndices; ++i)
+        if (indices[i] < 0 || indices[i] >= numVertices) {
+            b3_set_error("mesh index %d out of range", i);
+            return B3_ERR_INVALID_ARG;
+        }
+    const int numTri = numIndices / 3;
+    std::vector<float> v(3 * (size_t)numVertices);
+    for (int i = 0; i < numVertices; ++i)
+        for (int k = 0; k < 3; ++k) v[3 * i + k] = vertices3[3 * i + k] * (scaling ? scaling[k] : 1.f);
+    auto V = [&](int i) { return &v[3 * (size_t)i]; };
+    // the mesh's own table entry (registerConcaveMeshShape): its vertices,
+    // one face per triangle with the reference's plane, no unique edges
+    b3ConvexPolyhedron mesh;
+    memset(&mesh, 0, sizeof(mesh));
+    mesh.numVertices = numVertices;
+    mesh.vertexOffset = (int)w->verts4.size() / 4;
+    for (int i = 0; i < numVertices; ++i) {
+        for (int k = 0; k < 3; ++k) w->verts4.push_back(V(i)[k]);
+        w->verts4.push_back(0.f);
+    }
+    mesh.faceOffset = (int)w->faces.size();
+    mesh.numFaces = numTri;
+    mesh.uniqueEdgesOffset = (int)w->edges4.size() / 4;
+    mesh.numUniqueEdges = 0;
+    std::vector<std::array<float, 4>> triPlane(numTri);
+    for (int t = 0; t < numTri; ++t) {
+        const float* a = V(indices[3 * t]);
+        const float* b = V(indices[3 * t + 1]);
+        const float* c = V(indices[3 * t + 2]);
+        const float e0[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+        const float e1[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+        float n[3];
+        fcross3(e0, e1, n);
+        if (!(fdot3(n, n) > 0.f)) {
+            b3_set_error("mesh triangle %d is degenerate", t);
+            return B3_ERR_INVALID_ARG;
+        }
+        fnormalize3(n);
+        triPlane[t] = {n[0], n[1], n[2], -fdot3(n, a)};
+        b3Face f;
+        memset(&f, 0, sizeof(f));
+        for (int k = 0; k < 4; ++k) f.plane[k] = triPlane[t][k];
+        f.indexOffset = (int)w->indices.size();
+        f.numIndices = 3;
+        f.pad[0] = 1;
+        for (int k = 0; k < 3; ++k) w->indices.push_back(indices[3 * t + k]);
+        w->faces.push_back(f);
+        w->faceExt.push_back(0.f);
+        w->faceExt.push_back(0.f);
+    }
+    const int meshPoly = (int)w->polys.size();
+    mesh.unused = meshPoly + 1;  // the first triangle polytope
+    w->polys.push_back(mesh);
+    w->polyInradius.push_back(0.f);
+    // one polytope per triangle, as findSeparatingAxisKernel builds it
+    // (P2/sat.cl:970-1100): vertices 0, 1, 2; faces front (the triangle's
+    // plane; indices 0 1 2), back (-n, n . v0; 2 1 0), and for i = 0, 1, 2
+    // the edge plane of vertices i and i-1 (normalize(n x (v[i-1] - v[i])),
+    // -e . v[i]; indices i, i-1); unique edges v1-v0, v2-v1, v0-v2 as they
+    // are (not normalised); local centre (v0 + v1 + v2) / 3
+    for (int t = 0; t < numTri; ++t) {
+        const float* tv[3] = {V(indices[3 * t]), V(indices[3 * t + 1]), V(indices[3 * t + 2])};
+        const float n[3] = {triPlane[t][0], triPlane[t][1], triPlane[t][2]};
+        b3ConvexPolyhedron tp;
+        memset(&tp, 0, sizeof(tp));
+        tp.numVertices = 3;
+        tp.vertexOffset = (int)w->verts4.size() / 4;
+        float lc[3] = {0.f, 0.f, 0.f}, mn[3] = {1e30f, 1e30f, 1e30f}, mx[3] = {-1e30f, -1e30f, -1e30f};
+        for (int i = 0; i < 3; ++i) {
+            for (int k = 0; k < 3; ++k) {
+                w->verts4.push_back(tv[i][k]);
+                lc[k] += tv[i][k];
+                mn[k] = std::min(mn[k], tv[i][k]);
+                mx[k] = std::max(mx[k], tv[i][k]);
+            }
+            w->verts4.push_back(0.f);
+        }
+        for (int k = 0; k < 3; ++k) {
+            tp.localCenter[k] = lc[k] * (1.f / 3.f);
+            tp.mC[k] = mx[k] + mn[k];
+            tp.mE[k] = mx[k] - mn[k];
+            tp.extents[k] = 0.5f * tp.mE[k];
+        }
+        tp.faceOffset = (int)w->faces.size();
+        tp.numFaces = 5;
+        auto add_face = [&](const float pl[4], std::initializer_list<int> ids) {
+            b3Face f;
+            memset(&f, 0, sizeof(f));
+            for (int k = 0; k < 4; ++k) f.plane[k] = pl[k];
+            f.indexOffset = (int)w->indices.size();
+            f.numIndices = (int)ids.size();
+            f.pad[0] = 1;
+            for (int id : ids) w->indices.push_back(id);
+            w->faces.push_back(f);
+            double lo = 1e300, hi = -1e300;
+            for (int i = 0; i < 3; ++i) {
+                const double d = (double)pl[0] * tv[i][0] + (double)pl[1] * tv[i][1] + (double)pl[2] * tv[i][2];
+                lo = std::min(lo, d);
+                hi = std::max(hi, d);
+            }
+            float flo = (float)lo, fhi = (float)hi;
+            if ((double)flo > lo) flo = std::nextafter(flo, -1e30f);
+            if ((double)fhi < hi) fhi = std::nextafter(fhi, 1e30f);
+            w->faceExt.push_back(flo);
+            w->faceExt.push_back(fhi);
+        };
+        const float front[4] = {n[0], n[1], n[2], triPlane[t][3]};
+        add_face(front, {0, 1, 2});
+        const float back[4] = {-n[0], -n[1], -n[2], fdot3(n, tv[0])};
+        add_face(back, {2, 1, 0});
+        int prev = 2;
+        for (int i = 0; i < 3; ++i) {
+            const float d[3] = {tv[prev][0] - tv[i][0], tv[prev][1] - tv[i][1], tv[prev][2] - tv[i][2]};
+            float e[3];
+            fcross3(n, d, e);
+            fnormalize3(e);
+            const float pl[4] = {e[0], e[1], e[2], -fdot3(e, tv[i])};
+            add_face(pl, {i, prev});
+            prev = i;
+        }
+        tp.uniqueEdgesOffset = (int)w->edges4.size() / 4;
+        tp.numUniqueEdges = 3;
+        for (int i = 0; i < 3; ++i) {
+            const float* a = tv[i];
+            const float* b = tv[(i + 1) % 3];
+            for (int k = 0; k < 3; ++k) w->edges4.push_back(b[k] - a[k]);
+            w->edges4.push_back(0.f);
+        }
+        tp.radius = 0.f;
+        w->polys.push_back(tp);
+        w->polyInradius.push_back(0.f);
+    }
+    float mn[3] = {1e30f, 1e30f, 1e30f}, mx[3] = {-1e30f, -1e30f, -1e30f};
+    for (int i = 0; i < numVertices; ++i)
+        for (int k = 0; k < 3; ++k) {
+            mn[k] = std::min(mn[k], V(i)[k]);
+            mx[k] = std::max(mx[k], V(i)[k]);
+        }
+    *collidableOut = add_collidable(w, B3_SHAPE_CONCAVE_TRIMESH, meshPoly, 0.f, numTri, mn, mx);
+    ++w->numMeshes;
+    return B3_OK;
+}
+
+extern "C" int b3_get_child_shapes(b3World w, b3ChildShape* out, int max, int* count) {
+    if (!w || !count) return B3_ERR_INVALID_ARG;
+    *count = (int)w->childShapes.size();
+    if (out) memcpy(out, w->childShapes.data(), sizeof(b3ChildShape) * std::min(max, *count));
+    return B3_OK;
+}
+
 extern "C" int b3_register_body(b3World w, float mass, const float position[3], const float orientation[4],
                                 int collidable, float friction, float restitution, int worldId, int* bodyOut) {
     if (!w || !position || !orientation || !bodyOut) return B3_ERR_INVALID_ARG;
@@ -525,6 +762,10 @@ static int upload_shapes(b3World w, cudaStream_t st) {
                             cudaMemcpyHostToDevice, st));
     if (!w->faceExt.empty())
         B3_CUDA(cudaMemcpyAsync(d.faceExt, w->faceExt.data(), sizeof(float) * w->faceExt.size(),
+                                cudaMemcpyHostToDevice, st));
+    B3_TRY(dalloc(d.childShapes, w->childShapes.size()));
+    if (!w->childShapes.empty())
+        B3_CUDA(cudaMemcpyAsync(d.childShapes, w->childShapes.data(), sizeof(b3ChildShape) * w->childShapes.size(),
                                 cudaMemcpyHostToDevice, st));
     w->shapesDirty = false;
     return B3_OK;

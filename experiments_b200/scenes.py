@@ -292,9 +292,30 @@ def world_config(scene, **over):
     return b3.default_config(**kw)
 
 
+def register_shape(w, entry):
+    """Register one scene shape: an array of points (a convex hull), or a
+    dict {"kind": "sphere", "radius"}, {"kind": "plane", "normal",
+    "constant"}, {"kind": "compound", "children": [(shape index, position,
+    orientation), ...]} (children are earlier shapes of the scene, which are
+    collidables in registration order) or {"kind": "mesh", "vertices",
+    "indices", "scaling"}."""
+    if not isinstance(entry, dict):
+        return w.registerConvexPolyhedron(entry)
+    kind = entry["kind"]
+    if kind == "sphere":
+        return w.registerSphereShape(entry["radius"])
+    if kind == "plane":
+        return w.registerPlaneShape(entry["normal"], entry["constant"])
+    if kind == "compound":
+        return w.registerCompoundShape(entry["children"])
+    if kind == "mesh":
+        return w.registerConcaveMesh(entry["vertices"], entry["indices"], entry.get("scaling", (1.0, 1.0, 1.0)))
+    raise ValueError(f"unknown shape kind {kind}")
+
+
 def register_scene(w, scene):
     """Register the scene's shapes and bodies on a PhysicsWorld (host only)."""
-    cols = np.array([w.registerConvexPolyhedron(v) for v in scene.shapes], np.int32)
+    cols = np.array([register_shape(w, v) for v in scene.shapes], np.int32)
     w.register_bodies(scene.mass, scene.pos, scene.quat, cols[scene.shape], friction=scene.friction,
                       world=scene.world)
     return cols

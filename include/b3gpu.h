@@ -66,11 +66,39 @@ typedef struct b3Inertia {
 typedef struct b3Collidable {
     int numChildShapes;
     float radius;
-    int shapeType;         /* B3_SHAPE_CONVEX_HULL = 3 */
+    int shapeType;         /* B3_SHAPE_* */
     int shapeIndex;
 } b3Collidable;
 
-enum { B3_SHAPE_CONVEX_HULL = 3 };
+/* Shape types, the values of the reference's CollisionShape enum
+ * (P2/sat.cl:1-5, P2/satClipHullContacts.cl:4-5). What shapeIndex, radius
+ * and numChildShapes hold for each:
+ *   CONVEX_HULL: shapeIndex = its b3ConvexPolyhedron;
+ *   PLANE: shapeIndex = its b3Face (normal, constant), radius = constant;
+ *   CONCAVE_TRIMESH: shapeIndex = its b3ConvexPolyhedron, whose faces are
+ *     the triangles and whose `unused` field holds the first of the
+ *     per-triangle polytopes (see b3_register_concave_mesh),
+ *     numChildShapes = number of triangles;
+ *   COMPOUND_OF_CONVEX_HULLS: shapeIndex = first b3ChildShape,
+ *     numChildShapes = number of children;
+ *   SPHERE: radius. */
+enum {
+    B3_SHAPE_CONVEX_HULL = 3,
+    B3_SHAPE_PLANE = 4,
+    B3_SHAPE_CONCAVE_TRIMESH = 5,
+    B3_SHAPE_COMPOUND_OF_CONVEX_HULLS = 6,
+    B3_SHAPE_SPHERE = 7
+};
+
+/* btGpuChildShape (P2/sat.cl:21-29, 48 bytes, same layout): a child of a
+ * compound, a convex hull collidable at a pose relative to the compound's
+ * body (position xyz, orientation quaternion xyzw). */
+typedef struct b3ChildShape {
+    float childPosition[4];
+    float childOrientation[4];
+    int shapeIndex;        /* collidable of a convex hull */
+    int unused[3];
+} b3ChildShape;
 
 /* ConvexPolyhedronCL, P2/ConvexPolyhedronCL.h:15-31 (96 bytes, same layout). */
 typedef struct b3ConvexPolyhedron {
@@ -339,6 +367,45 @@ int b3_sap_compute_pairs(b3Context ctx, const float* d_sortedAabbs, int n, int a
 int b3_register_convex_hull(b3World w, const float* vertices, int numVertices, int strideBytes,
                             const float scaling[3], int* collidableOut);
 
+/* CLPhysicsDemo::registerSphereShape (P2/CLPhysicsDemo.cpp:420-456): a
+ * sphere of the given radius (> 0); local AABB +-radius. Spheres collide
+ * with spheres and planes (clipHullHullKernel, P2/satClipHullContacts.cl:
+ * 1057-1124); the reference has no sphere-hull contact, nor has this. */
+int b3_register_sphere(b3World w, float radius, int* collidableOut);
+/* CLPhysicsDemo::registerPlaneShape (:459-490) -> registerFace
+ * (P1/btGpuNarrowPhaseAndSolver.cpp:252-262): the plane n . x = constant
+ * in the body's frame (n of unit length), unbounded (local AABB +-1e30).
+ * Planes collide with spheres only, as there. */
+int b3_register_plane(b3World w, const float normal[3], float planeConstant, int* collidableOut);
+/* CLPhysicsDemo::registerCompoundShape (P2/CLPhysicsDemo.cpp:217-285) ->
+ * registerCompoundShape (P1/btGpuNarrowPhaseAndSolver.cpp:237-250): a
+ * compound of n convex hull children (each child's shapeIndex a
+ * convex-hull collidable registered before). Local AABB: the union of the
+ * children's AABBs at their poses. A compound pair expands into one pair
+ * per child (per child pair for compound-compound) with no culling between
+ * children (findCompoundPairsKernel, P2/sat.cl:747-926), each tested and
+ * clipped as two hulls at the composed poses; every child pair with
+ * contact points gives its own manifold. Compounds collide with hulls and
+ * compounds. */
+int b3_register_compound(b3World w, const b3ChildShape* children, int numChildren, int* collidableOut);
+/* CLPhysicsDemo::registerConcaveMesh (P2/CLPhysicsDemo.cpp:288-330) ->
+ * registerConcaveMeshShape (P1/btGpuNarrowPhaseAndSolver.cpp:264-333): a
+ * triangle mesh (numIndices / 3 triangles, vertices scaled by scaling),
+ * normally the shape of a static body. Each triangle's plane is
+ * normalize((v1 - v0) x (v2 - v0)), -n . v0. Against a convex hull, every
+ * triangle whose local AABB overlaps the hull's world AABB is tested as the
+ * reference builds it in findSeparatingAxisKernel (P2/sat.cl:970-1191): a
+ * polytope of the 3 vertices, the front and back faces, 3 edge planes and
+ * the 3 edges, clipped as a hull (clipHullHullConcaveConvexKernel,
+ * P2/satClipHullContacts.cl:1387); each triangle with contact points gives
+ * its own manifold. These polytopes are registered here, after the mesh's
+ * own table entry. The reference's test takes the mesh's local triangle
+ * AABBs as world ones (a mesh body at the origin, unrotated), and so does
+ * this. The reference tests a mesh only when it is the pair's first body;
+ * here either order is tested, the mesh body taking the manifold's A side. */
+int b3_register_concave_mesh(b3World w, const float* vertices3, int numVertices, const int* indices,
+                             int numIndices, const float scaling[3], int* collidableOut);
+
 /* CLPhysicsDemo::registerPhysicsInstance (P2/CLPhysicsDemo.cpp:533-599) ->
  * btGpuNarrowphaseAndSolver::registerRigidBody (P1/...cpp:566-657):
  * mass 0 = static. Inverse inertia from the registration AABB (margin
@@ -472,6 +539,9 @@ int b3_get_shape_sizes(b3World w, int* numCollidables, int* numPolys, int* numVe
                        int* numFaces, int* numIndices, int* numEdges);
 int b3_get_shapes(b3World w, b3Collidable* cols, b3ConvexPolyhedron* polys, float* vertices4,
                   b3Face* faces, int* indices, float* edges4, float* localAabbs8);
+/* The compounds' child shapes (all of them, in registration order);
+ * *count = their number. */
+int b3_get_child_shapes(b3World w, b3ChildShape* out, int max, int* count);
 int b3_get_inertias(b3World w, b3Inertia* out, int maxBodies);
 
 /* --- device buffers (borrowed views, like getBodiesGpu / getContactsGpu,

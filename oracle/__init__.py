@@ -64,6 +64,7 @@ def lib(f32=False, dual=False):
         L.or_world_create.argtypes = [C.POINTER(OrConfig), C.c_int, _F, _F, _F, _I, _I, _I, _F, C.c_int, _I,
                                       C.c_int, _VP, C.c_int, _F, C.c_int, _VP, C.c_int, _I, C.c_int, _F, _F]
         L.or_world_destroy.argtypes = [_VP]
+        L.or_set_collidables.argtypes = [_VP, C.c_int, _I, _F, _I, _I, C.c_int, _F, _I]
         L.or_set_state_f32.argtypes = [_VP, _F, _F, _F, _F]
         L.or_set_state_f64.argtypes = [_VP, _D, _D, _D, _D]
         L.or_get_state.argtypes = [_VP, _D, _D, _D, _D]
@@ -243,6 +244,25 @@ class OracleWorld:
                                    C.cast(shapes["faces"], _VP), ni, _i(k["idx"]), ne, _f(k["edges"]),
                                    _f(k["laabb"]))
         self.L = L
+        # the collidable table (types other than hulls, compound children)
+        cols = shapes["cols"]
+        nc = shapes["counts"][0]
+        ch = shapes.get("children", [])
+        self._keep["colType"] = np.ascontiguousarray(np.array([cols[k].shapeType for k in range(nc)], np.int32))
+        self._keep["colRadius"] = np.ascontiguousarray(np.array([cols[k].radius for k in range(nc)], np.float32))
+        self._keep["colNum"] = np.ascontiguousarray(np.array([cols[k].numChildShapes for k in range(nc)], np.int32))
+        self._keep["colIndex"] = np.ascontiguousarray(np.array([cols[k].shapeIndex for k in range(nc)], np.int32))
+        pose = np.zeros((max(len(ch), 1), 8), np.float32)
+        ccol = np.zeros(max(len(ch), 1), np.int32)
+        for j, c in enumerate(ch):
+            pose[j, :4] = list(c.childPosition)
+            pose[j, 4:] = list(c.childOrientation)
+            ccol[j] = c.shapeIndex
+        self._keep["childPose"] = np.ascontiguousarray(pose)
+        self._keep["childCol"] = np.ascontiguousarray(ccol)
+        k = self._keep
+        L.or_set_collidables(self.h, nc, _i(k["colType"]), _f(k["colRadius"]), _i(k["colNum"]), _i(k["colIndex"]),
+                             len(ch), _f(k["childPose"]), _i(k["childCol"]))
         if int(getattr(cfg, "flags", 0)) & 1:
             L.or_set_broadphase(self.h, 1)  # sweep and prune
         if int(getattr(cfg, "flags", 0)) & 2:
@@ -405,6 +425,8 @@ def oracle_from_world(world, scene, cfg=None, f32=False, dual=False):
     # body collidable index = scene.shape (shapes are registered in scene order)
     sh["col_of_body"] = np.asarray(scene.shape, np.int32)
     assert sh["counts"][0] == n_shapes
+    arr, cnt = world.child_shapes()
+    sh["children"] = [arr[j] for j in range(cnt)]
     inv_inertia = world.inertias()
     # large-body classification rule (half-diagonal of the registration AABB)
     is_large = large_flags(world, scene, cfg)

@@ -179,6 +179,12 @@ struct or_world {
     std::vector<uint64_t> activeHash;   // row clamp states
     std::vector<uint64_t> topoHash;     // pairs with manifolds, clip sizes, reduced points
     long long pairOverflow, cellOverflow;
+    // collidable table beyond the hulls (or_set_collidables): type, radius,
+    // child count and shape index per collidable; the compounds' children
+    std::vector<int> colType, colNum, colIndex;
+    std::vector<float> colRadius;
+    std::vector<float> childPose;   // 8 per child: position xyzw, orientation xyzw
+    std::vector<int> childCol;
     int sap;  // broadphase: 0 = uniform grid, 1 = sweep and prune
     int gs;   // solver: 0 = Jacobi (pipeline2), 1 = batched Gauss-Seidel (the reference GPU solver)
     // batched Gauss-Seidel: per manifold its cell (xz, 16 x 16) and batch
@@ -714,15 +720,26 @@ int reduce_manifold(const std::vector<P4>& p, V nearNormal, int idx[4]) {
 
 Real combine_friction(Real a, Real b, int mode) { return mode == 1 ? a * b : sqrt(a * b); }
 
+Body body_pose(const or_world* w, int i) {
+    Body b;
+    b.pos = V(w->pos[4 * i], w->pos[4 * i + 1], w->pos[4 * i + 2]);
+    b.q = Q{w->quat[4 * i], w->quat[4 * i + 1], w->quat[4 * i + 2], w->quat[4 * i + 3]};
+    return b;
+}
+
+// SAT, clip and reduction of hull hA at pose a against hull hB at pose b;
+// the manifold is reported for bodies A and B.
+bool contact_for_shapes(const or_world* w, int pairIndex, int A, int B, const or_poly& hA, const Body& a,
+                        const or_poly& hB, const Body& b, or_contact_r& out);
+
 bool contact_for_pair(const or_world* w, int pairIndex, int A, int B, or_contact_r& out) {
     if (w->invMass[A] == 0.f && w->invMass[B] == 0.f) return false;  // sat.cl:944-948
-    const or_poly& hA = w->polys[w->colShape[w->col[A]]];
-    const or_poly& hB = w->polys[w->colShape[w->col[B]]];
-    Body a, b;
-    a.pos = V(w->pos[4 * A], w->pos[4 * A + 1], w->pos[4 * A + 2]);
-    a.q = Q{w->quat[4 * A], w->quat[4 * A + 1], w->quat[4 * A + 2], w->quat[4 * A + 3]};
-    b.pos = V(w->pos[4 * B], w->pos[4 * B + 1], w->pos[4 * B + 2]);
-    b.q = Q{w->quat[4 * B], w->quat[4 * B + 1], w->quat[4 * B + 2], w->quat[4 * B + 3]};
+    return contact_for_shapes(w, pairIndex, A, B, w->polys[w->colShape[w->col[A]]], body_pose(w, A),
+                              w->polys[w->colShape[w->col[B]]], body_pose(w, B), out);
+}
+
+bool contact_for_shapes(const or_world* w, int pairIndex, int A, int B, const or_poly& hA, const Body& a,
+                        const or_poly& hB, const Body& b, or_contact_r& out) {
     const V c0 = qrot(a.q, V(hA.localCenter[0], hA.localCenter[1], hA.localCenter[2])) + a.pos;
     const V c1 = qrot(b.q, V(hB.localCenter[0], hB.localCenter[1], hB.localCenter[2])) + b.pos;
     const V D = c0 - c1;
@@ -758,18 +775,195 @@ bool contact_for_pair(const or_world* w, int pairIndex, int A, int B, or_contact
     return true;
 }
 
+// The pair's manifold goes into the per-world signature of discrete choices.
+void record_topology(or_world* w, const or_contact_r& c) {
+    const int A = std::abs(c.bodyA), B = std::abs(c.bodyB);
+    uint64_t& h = w->topoHash[w->worldId[A]];
+    h = mix64(h, ((uint64_t)A << 32) | (uint32_t)B);
+    h = mix64(h, (uint32_t)c.pad);
+    h = mix64(h, (uint64_t)(int64_t)g_axisId);
+}
+
+int col_type(const or_world* w, int col) { return w->colType.empty() ? 3 : w->colType[col]; }
+
+inline int ibits(float f) {
+    int i;
+    memcpy(&i, &f, 4);
+    return i;
+}
+
+// sphere-sphere branch of clipHullHullKernel (satClipHullContacts.cl:1078-1124)
+bool sphere_sphere(const or_world* w, int slot, int A, int B, or_contact_r& out) {
+    const Real rA = w->colRadius[w->col[A]], rB = w->colRadius[w->col[B]];
+    const V pA = body_pose(w, A).pos, pB = body_pose(w, B).pos;
+    const V diff = pA - pB;
+    const Real len = sqrt(dot(diff, diff));
+    if (!(len <= rA + rB)) return false;
+    const Real dist = len - (rA + rB);
+    V nB(1, 0, 0);
+    if (len > 0.00001) nB = diff * (1 / len);
+    const V cp = pB + nB * rB;
+    out = or_contact_r();
+    out.pos[0][0] = cp.x; out.pos[0][1] = cp.y; out.pos[0][2] = cp.z; out.pos[0][3] = dist;
+    out.normal[0] = -nB.x; out.normal[1] = -nB.y; out.normal[2] = -nB.z; out.normal[3] = 1;
+    out.friction = combine_friction(w->friction[A], w->friction[B], w->cfg.frictionCombine);
+    out.pairIndex = slot;
+    out.bodyA = w->invMass[A] == 0.f ? -A : A;
+    out.bodyB = w->invMass[B] == 0.f ? -B : B;
+    return true;
+}
+
+// computeContactPlaneConvex (satClipHullContacts.cl:957-1016) for a sphere:
+// the sphere's point deepest along -n, its distance to the plane
+// n . x = constant in the plane body's frame; a contact when below it. The
+// manifold's A side is the plane's body, B the sphere's.
+bool plane_sphere(const or_world* w, int slot, int P, int Sb, or_contact_r& out) {
+    const float* pl = w->faces[w->colIndex[w->col[P]]].plane;
+    const Real r = w->colRadius[w->col[Sb]];
+    const Body bp = body_pose(w, P), bs = body_pose(w, Sb);
+    const V n(pl[0], pl[1], pl[2]);
+    const V cLocal = qinvrot(bp.q, bs.pos - bp.pos);
+    const Real distance = dot(n, cLocal) - r - (Real)pl[3];
+    if (!(distance < 0)) return false;
+    const V nw = qrot(bp.q, n);
+    const V pOnB = bs.pos - nw * r;
+    out = or_contact_r();
+    out.pos[0][0] = pOnB.x; out.pos[0][1] = pOnB.y; out.pos[0][2] = pOnB.z; out.pos[0][3] = distance;
+    out.normal[0] = nw.x; out.normal[1] = nw.y; out.normal[2] = nw.z; out.normal[3] = 1;
+    out.friction = combine_friction(w->friction[P], w->friction[Sb], w->cfg.frictionCombine);
+    out.pairIndex = slot;
+    out.bodyA = w->invMass[P] == 0.f ? -P : P;
+    out.bodyB = w->invMass[Sb] == 0.f ? -Sb : Sb;
+    return true;
+}
+
+// A sub-pair of a compound or mesh pair: bodies A and B (the manifold's
+// sides) and per side either a compound child (>= 0) or, as -(poly + 1), a
+// polytope at the body's own pose.
+struct SubPair {
+    int A, B, sa, sb;
+};
+
+// The child's pose: qtRotate(orn, childPos) + pos and qtMul(orn, childOrn)
+// in FP32 (findCompoundPairsKernel, sat.cl:774-781), in the operation order
+// the device uses, from the body's FP32 pose.
+Body child_pose(const or_world* w, int body, int child) {
+    const float p[4] = {(float)rval(w->pos[4 * body]), (float)rval(w->pos[4 * body + 1]),
+                        (float)rval(w->pos[4 * body + 2]), 0.f};
+    const float q[4] = {(float)rval(w->quat[4 * body]), (float)rval(w->quat[4 * body + 1]),
+                        (float)rval(w->quat[4 * body + 2]), (float)rval(w->quat[4 * body + 3])};
+    const float* cp = &w->childPose[8 * (size_t)child];
+    const float* cq = cp + 4;
+    const float v[4] = {cp[0], cp[1], cp[2], 0.f};
+    const float qi[4] = {-q[0], -q[1], -q[2], q[3]};
+    float t[4], r[4], o[4];
+    qmul_f(q, v, t);
+    qmul_f(t, qi, r);
+    qmul_f(q, cq, o);
+    Body b;
+    b.pos = V(r[0] + p[0], r[1] + p[1], r[2] + p[2]);
+    b.q = Q{o[0], o[1], o[2], o[3]};
+    return b;
+}
+
+void side_of(const or_world* w, int body, int s, const or_poly*& h, Body& pose) {
+    if (s >= 0) {
+        h = &w->polys[w->colIndex[w->childCol[s]]];
+        pose = child_pose(w, body, s);
+    } else {
+        h = &w->polys[-s - 1];
+        pose = body_pose(w, body);
+    }
+}
+
+// Sub-pairs of broadphase pair (A, B) in order: compound children (child
+// of A outer, child of B inner; findCompoundPairsKernel, sat.cl:747-926,
+// with no culling between children), or a mesh's triangles whose local AABB
+// overlaps the hull's world AABB (findSeparatingAxisKernel, sat.cl:970-1012),
+// the mesh taking side A whichever order the pair has.
+void sub_pairs_of(const or_world* w, int A, int B, std::vector<SubPair>& out) {
+    if (w->invMass[A] == 0.f && w->invMass[B] == 0.f) return;
+    const int tA = col_type(w, w->col[A]), tB = col_type(w, w->col[B]);
+    if (tA == 6 || tB == 6) {
+        if ((tA != 6 && tA != 3) || (tB != 6 && tB != 3)) return;
+        const int nA = tA == 6 ? w->colNum[w->col[A]] : 1;
+        const int nB = tB == 6 ? w->colNum[w->col[B]] : 1;
+        for (int i = 0; i < nA; ++i)
+            for (int j = 0; j < nB; ++j) {
+                const int sa = tA == 6 ? w->colIndex[w->col[A]] + i : -(w->colShape[w->col[A]] + 1);
+                const int sb = tB == 6 ? w->colIndex[w->col[B]] + j : -(w->colShape[w->col[B]] + 1);
+                out.push_back({A, B, sa, sb});
+            }
+        return;
+    }
+    int M = -1, H = -1;
+    if (tA == 5 && tB == 3) M = A, H = B;
+    else if (tB == 5 && tA == 3) M = B, H = A;
+    if (M < 0) return;
+    const or_poly& mesh = w->polys[w->colIndex[w->col[M]]];
+    const float* bb = &w->aabb[8 * (size_t)H];
+    for (int f = 0; f < mesh.numFaces; ++f) {
+        const int tp = mesh.unused + f;
+        const or_poly& t = w->polys[tp];
+        float mn[3] = {1e30f, 1e30f, 1e30f}, mx[3] = {-1e30f, -1e30f, -1e30f};
+        for (int i = 0; i < 3; ++i)
+            for (int k = 0; k < 3; ++k) {
+                const float v = w->verts4[4 * (size_t)(t.vertexOffset + i) + k];
+                mn[k] = std::min(mn[k], v);
+                mx[k] = std::max(mx[k], v);
+            }
+        bool overlap = true;
+        overlap = (mn[0] > bb[4] || mx[0] < bb[0]) ? false : overlap;
+        overlap = (mn[2] > bb[6] || mx[2] < bb[2]) ? false : overlap;
+        overlap = (mn[1] > bb[5] || mx[1] < bb[1]) ? false : overlap;
+        if (overlap) out.push_back({M, H, -(tp + 1), -(w->colShape[w->col[H]] + 1)});
+    }
+}
+
 void stage_narrowphase(or_world* w) {
     w->contacts.clear();
     const int np = (int)w->pairs.size() / 2;
+    std::vector<SubPair> subs;
     for (int p = 0; p < np; ++p) {
+        const int A = w->pairs[2 * p], B = w->pairs[2 * p + 1];
+        const int tA = col_type(w, w->col[A]), tB = col_type(w, w->col[B]);
         or_contact_r c;
-        if (contact_for_pair(w, p, w->pairs[2 * p], w->pairs[2 * p + 1], c)) {
+        bool have = false;
+        if (tA == 3 && tB == 3) {
+            have = contact_for_pair(w, p, A, B, c);
+        } else if (w->invMass[A] == 0.f && w->invMass[B] == 0.f) {
+        } else if (tA == 7 && tB == 7) {
+            have = sphere_sphere(w, p, A, B, c);
+        } else if (tA == 7 && tB == 4) {
+            have = plane_sphere(w, p, B, A, c);
+        } else if (tA == 4 && tB == 7) {
+            have = plane_sphere(w, p, A, B, c);
+        } else {
+            sub_pairs_of(w, A, B, subs);
+        }
+        if (have) {
             w->contacts.push_back(c);
-            const int A = std::abs(c.bodyA), B = std::abs(c.bodyB);
-            uint64_t& h = w->topoHash[w->worldId[A]];
-            h = mix64(h, ((uint64_t)A << 32) | (uint32_t)B);
-            h = mix64(h, (uint32_t)c.pad);
-            h = mix64(h, (uint64_t)(int64_t)g_axisId);
+            record_topology(w, c);
+        }
+    }
+    // the sub-pairs' slots follow the pairs' within the pair capacity
+    long long room = w->cfg.maxPairs > 0 ? (long long)w->cfg.maxPairs - np : (long long)subs.size();
+    if (room < 0) room = 0;
+    if ((long long)subs.size() > room) {
+        w->pairOverflow += (long long)subs.size() - room;
+        subs.resize((size_t)room);
+    }
+    for (size_t s = 0; s < subs.size(); ++s) {
+        const SubPair& sp = subs[s];
+        const or_poly* hA;
+        const or_poly* hB;
+        Body a, b;
+        side_of(w, sp.A, sp.sa, hA, a);
+        side_of(w, sp.B, sp.sb, hB, b);
+        or_contact_r c;
+        if (contact_for_shapes(w, np + (int)s, sp.A, sp.B, *hA, a, *hB, b, c)) {
+            w->contacts.push_back(c);
+            record_topology(w, c);
         }
     }
 }
@@ -1387,6 +1581,20 @@ or_world* or_world_create(const or_config* cfg, int n, const float* invMass, con
 }
 
 void or_world_destroy(or_world* w) { delete w; }
+
+// The collidable table of a scene with shapes other than hulls: per
+// collidable its type (B3_SHAPE_*), radius, child count and shape index,
+// and the compounds' children (pose: position xyzw, orientation xyzw; the
+// child's collidable).
+void or_set_collidables(or_world* w, int numCols, const int* type, const float* radius, const int* numChildren,
+                        const int* shapeIndex, int numChild, const float* childPose8, const int* childCol) {
+    w->colType.assign(type, type + numCols);
+    w->colRadius.assign(radius, radius + numCols);
+    w->colNum.assign(numChildren, numChildren + numCols);
+    w->colIndex.assign(shapeIndex, shapeIndex + numCols);
+    w->childPose.assign(childPose8, childPose8 + 8 * (size_t)numChild);
+    w->childCol.assign(childCol, childCol + numChild);
+}
 
 // FP64 body parameters (finite differences need perturbations finer than
 // FP32 inputs resolve): inverse masses, friction coefficients and local
