@@ -372,7 +372,7 @@ def oracle_check(w, sc):
     keep = ["pos_err_m", "lin_vel_err_mps", "ang_vel_err_radps", "quat_err", "contact_point_err_m", "normal_err",
             "aabbs_bit_exact", "keys_bit_exact", "permutation_bit_exact", "pairs_bit_exact", "manifold_set_equal",
             "pairs", "manifolds", "pair_overflow", "narrowphase_within_bars", "solver_err", "fp32_envelope",
-            "bars_used", "within_bars", "check_s"]
+            "contact_sensitivity", "bars_used", "step_bars_used", "within_bars", "check_s"]
     out = {k: rep[k] for k in keep}
     out["bars"] = ("pairs/keys/permutation bit-exact; contacts 1e-5 m, normals 1e-4; one step 1e-5 m, 1e-4 m/s, or "
                    "twice the FP32 envelope (the oracle's FP32 build against its FP64 build from the same contacts) "

@@ -1069,6 +1069,11 @@ extern "C" int b3_adjoint_create(b3World w, int numSteps, int checkpointEvery, b
         b3_set_error("the adjoint form differentiates the Jacobi solver; this world runs batched Gauss-Seidel");
         return B3_ERR_UNSUPPORTED;
     }
+    if (w->numSpheres || w->numPlanes || w->numCompounds || w->numMeshes) {
+        b3_set_error("the adjoint form differentiates hull-hull contact geometry; this world has spheres, planes, "
+                     "compounds or meshes");
+        return B3_ERR_UNSUPPORTED;
+    }
     B3_CUDA(cudaSetDevice(w->ctx->device));
     b3Adjoint_t* a = new b3Adjoint_t();
     a->w = w;

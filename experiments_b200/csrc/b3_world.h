@@ -34,6 +34,7 @@ struct ShapesDev {
     const float4* localAabb;  // 2 per collidable (min, max)
     const float* inradius;    // per polyhedron: lower bound of its support about localCenter
     const float2* faceExt;    // per face: (min, max) over its hull's vertices of n . v (local frame)
+    const b3ChildShape* children;  // the compounds' children
     int numPolys, numVerts, numFaces, numIndices, numEdges;
     int tableBytes;           // packed size for shared-memory staging
 };
@@ -68,6 +69,12 @@ struct DevBuffers {
     float* polyInradius = nullptr;
     float2* faceExt = nullptr;  // per face: the hull's extent along the face normal
     b3ChildShape* childShapes = nullptr;
+    // compound and mesh pairs: sub-pair records (body A, body B, side A,
+    // side B; a side is a child shape >= 0 or -(polytope + 1)), per pair
+    // counts and their exclusive scan
+    int4* subPairs = nullptr;
+    uint32_t* subCount = nullptr;
+    uint32_t* subOffset = nullptr;
     // broadphase
     float4 *aabbMin = nullptr, *aabbMax = nullptr;
     int* smallSlot = nullptr;      // body -> slot in the hash arrays, -1 = large
@@ -142,7 +149,10 @@ enum ScalarSlot {
     S_NP_WORK2 = 12,
     S_NP_WORK3 = 13,
     S_NP_WORK4 = 14,
-    S_NUM_SCALARS = 16
+    S_NUM_SUB = 15,       // sub-pairs of compound and mesh pairs this step (after the capacity cut)
+    S_NUM_SLOTS = 16,     // manifold slots: pairs, then sub-pairs
+    S_SUB_TOTAL = 17,     // sub-pairs before the capacity cut
+    S_NUM_SCALARS = 24
 };
 
 }  // namespace b3
@@ -163,6 +173,8 @@ struct b3World_t {
     std::vector<float> faceExt;   // 2 per face: min, max of n . v over the face's hull
     std::vector<b3ChildShape> childShapes;  // children of the compounds
     int numSpheres = 0, numPlanes = 0, numCompounds = 0, numMeshes = 0;
+    bool hasSpheresPlanes() const { return numSpheres > 0 && (numSpheres > 1 || numPlanes > 0); }
+    bool hasSubPairs() const { return numCompounds + numMeshes > 0; }
     std::vector<b3Face> faces;
     std::vector<int> indices;
     std::vector<int> worldIds;

@@ -250,27 +250,25 @@ __device__ __forceinline__ float axis_depth(const PairCtx& c, const b3::ShapesDe
 // FP32 depth along the oriented face axis n of face idx (flipped: n is
 // the negated face normal). The face's own hull projects onto its normal
 // over the registered extent (faceExt, exact and rounded outward), so only
-// the other hull's vertices are projected.
+// the other hull's vertices are projected. Lanes on faces of A and of B run
+// the same code on selected data (the other hull and its rotation), so a
+// warp holding both kinds does not serialise two loops.
 __device__ __forceinline__ float face_axis_depth(const PairCtx& c, const b3::ShapesDev& S, int idx, float3 rel,
                                                  float3 n, bool flipped) {
-    const b3ConvexPolyhedron& pa = *c.pa;
-    const b3ConvexPolyhedron& pb = *c.pb;
-    const bool onA = idx < pa.numFaces;
-    const float2 ext = __ldg(&S.faceExt[onA ? pa.faceOffset + idx : pb.faceOffset + idx - pa.numFaces]);
+    const bool onA = idx < c.pa->numFaces;
+    const b3ConvexPolyhedron* own = onA ? c.pa : c.pb;
+    const b3ConvexPolyhedron* oth = onA ? c.pb : c.pa;
+    const float2 ext = __ldg(&S.faceExt[own->faceOffset + (onA ? idx : idx - c.pa->numFaces)]);
+    Mat3 R;
+    R.r0 = onA ? c.RB.r0 : c.RA.r0;
+    R.r1 = onA ? c.RB.r1 : c.RA.r1;
+    R.r2 = onA ? c.RB.r2 : c.RA.r2;
+    float mo, xo;
+    project_rel(S.verts, oth->vertexOffset, oth->numVertices, R, n, mo, xo);
     const float lo = flipped ? -ext.y : ext.x, hi = flipped ? -ext.x : ext.y;
-    float mn0, mx0, mn1, mx1;
-    if (onA) {
-        mn0 = lo;
-        mx0 = hi;
-        project_rel(S.verts, pb.vertexOffset, pb.numVertices, c.RB, n, mn1, mx1);
-    } else {
-        project_rel(S.verts, pa.vertexOffset, pa.numVertices, c.RA, n, mn0, mx0);
-        mn1 = lo;
-        mx1 = hi;
-    }
     const float off = dot(rel, n);  // posB - posA along n
-    mn1 += off;
-    mx1 += off;
+    const float mn0 = onA ? lo : mo, mx0 = onA ? hi : xo;
+    const float mn1 = (onA ? mo : lo) + off, mx1 = (onA ? xo : hi) + off;
     return fminf(mx0 - mn1, mx1 - mn0);
 }
 
@@ -1336,6 +1334,83 @@ __device__ __forceinline__ void pair_setup_shared(PairCtx& c, int2 pr, const b3:
     __syncwarp();
 }
 
+// One side of a sub-pair: a compound child (s >= 0: its hull at the pose
+// qtRotate(q, childPos) + pos, qtMul(q, childOrn) in FP32,
+// findCompoundPairsKernel P2/sat.cl:774-781, in the order the oracle
+// evaluates) or a polytope at the body's pose (s = -(polytope + 1)).
+__device__ __forceinline__ void sub_side(const b3::BodiesDev& Bd, const b3::ShapesDev& S, int body, int s, int& poly,
+                                         float4& q, float4& pos) {
+    const float4 bq = Bd.quat[body], bp = Bd.pos[body];
+    if (s >= 0) {
+        const b3ChildShape& ch = S.children[s];
+        poly = S.cols[ch.shapeIndex].shapeIndex;
+        const float4 cp = make_float4(ch.childPosition[0], ch.childPosition[1], ch.childPosition[2], 0.f);
+        const float4 cq = make_float4(ch.childOrientation[0], ch.childOrientation[1], ch.childOrientation[2],
+                                      ch.childOrientation[3]);
+        const float4 r = b3m::qt_rotate_rn(bq, cp);
+        pos = make_float4(b3m::arn(r.x, bp.x), b3m::arn(r.y, bp.y), b3m::arn(r.z, bp.z), 0.f);
+        q = b3m::qt_mul_rn(bq, cq);
+    } else {
+        poly = -s - 1;
+        q = bq;
+        pos = bp;
+    }
+}
+
+// Setup of the item in slot `slot`: a broadphase pair (slot = pair index),
+// or with kSub the sub-pair slot - base of a compound or mesh pair.
+template <bool kSub>
+__device__ __forceinline__ void item_prefetch(PairPre& q, int slot, const int2* __restrict__ pairs,
+                                              const int4* __restrict__ subs, int base, const b3::BodiesDev& Bd,
+                                              const b3::ShapesDev& S) {
+    if (!kSub) {
+        pair_prefetch(q, slot, pairs[slot], Bd, S);
+        return;
+    }
+    const int4 sp = subs[slot - base];
+    q.p = slot;
+    q.A = sp.x;
+    q.B = sp.y;
+    q.invMassA = Bd.invMass[sp.x];
+    q.invMassB = Bd.invMass[sp.y];
+    int pa, pb;
+    sub_side(Bd, S, sp.x, sp.z, pa, q.qA, q.pA);
+    sub_side(Bd, S, sp.y, sp.w, pb, q.qB, q.pB);
+    q.shapeA = pa;
+    q.shapeB = pb;
+}
+
+template <bool kSub>
+__device__ __forceinline__ void item_setup_shared(PairCtx& c, int slot, const int2* __restrict__ pairs,
+                                                  const int4* __restrict__ subs, int base, const b3::BodiesDev& Bd,
+                                                  const b3::ShapesDev& S) {
+    if (!kSub) {
+        pair_setup_shared(c, pairs[slot], Bd, S);
+        return;
+    }
+    PairPre q;
+    item_prefetch<true>(q, slot, pairs, subs, base, Bd, S);
+    PairCtx t;
+    pair_from_pre(t, q, S);
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) {
+        c.A = t.A;
+        c.B = t.B;
+        c.invMassA = t.invMassA;
+        c.invMassB = t.invMassB;
+        c.pa = t.pa;
+        c.pb = t.pb;
+        c.qA = t.qA;
+        c.qB = t.qB;
+        c.RA = t.RA;
+        c.RB = t.RB;
+        c.haveFF = false;
+        c.posA = t.posA;
+        c.posB = t.posB;
+    }
+    __syncwarp();
+}
+
 // Contact4 of pair p from the kept points pts[0..nOut) and the chosen
 // indices (newContactReductionKernel, P2/satClipHullContacts.cl:1958-2039).
 __device__ __forceinline__ void emit_contact(int p, const PairCtx& c, const FfVert* pts, int nRed, int4 idx,
@@ -1381,10 +1456,12 @@ __device__ __forceinline__ int push(int* queue, int32_t* count, int p) {
 // finished here; pairs whose axis the sweep decides go to the FP32 clip
 // queue with that axis; pairs with near-minimum candidates go to the
 // float-float queue.
-template <bool kEarlyFaces>
+// kSub: the items are the sub-pairs of compound and mesh pairs, in the
+// slots after the pairs' (slot = numPairs + sub-pair).
+template <bool kEarlyFaces, bool kSub>
 __global__ void __launch_bounds__(128, 5)
-k_np_sweep(const int2* __restrict__ pairs, const int32_t* __restrict__ numPairsDev, b3::BodiesDev Bd,
-           b3::ShapesDev S, uint32_t* __restrict__ manifoldFlag, float4* __restrict__ pairSep,
+k_np_sweep(const int2* __restrict__ pairs, const int4* __restrict__ subs, const int32_t* __restrict__ numPairsDev,
+           b3::BodiesDev Bd, b3::ShapesDev S, uint32_t* __restrict__ manifoldFlag, float4* __restrict__ pairSep,
            int* __restrict__ fastQ, int* __restrict__ slowQ, int* __restrict__ cand, int candSlots,
            int32_t* __restrict__ scalars, b3Counters* __restrict__ counters) {
     extern __shared__ __align__(16) unsigned char np_smem[];
@@ -1392,15 +1469,16 @@ k_np_sweep(const int2* __restrict__ pairs, const int32_t* __restrict__ numPairsD
     unsigned char* wbase = np_smem + (size_t)(threadIdx.x >> 5) * kSweepWarpSmem;
     PairPre* pre = reinterpret_cast<PairPre*>(wbase);
     int* wcand = reinterpret_cast<int*>(wbase + sizeof(PairPre) * kPreChunk);
-    const int numPairs = *numPairsDev;
+    const int numItems = kSub ? scalars[b3::S_NUM_SUB] : *numPairsDev;
+    const int base = kSub ? *numPairsDev : 0;
     for (;;) {
-        const int chunk = next_work(scalars + b3::S_NP_WORK, numPairs, kPreChunk);
+        const int chunk = next_work(scalars + b3::S_NP_WORK, numItems, kPreChunk);
         if (chunk < 0) break;
-        const int n = min(kPreChunk, numPairs - chunk);
-        if (lane < n) pair_prefetch(pre[lane], chunk + lane, pairs[chunk + lane], Bd, S);
+        const int n = min(kPreChunk, numItems - chunk);
+        if (lane < n) item_prefetch<kSub>(pre[lane], base + chunk + lane, pairs, subs, base, Bd, S);
         __syncwarp();
         for (int i = 0; i < n; ++i) {
-            const int p = chunk + i;
+            const int p = base + chunk + i;
             PairCtx c;
             int r = 0, count = 0;
             float3 sepf = make_float3(0.f, 0.f, 0.f);
@@ -1427,8 +1505,9 @@ k_np_sweep(const int2* __restrict__ pairs, const int32_t* __restrict__ numPairsD
 // Stage 2, pairs with an FP32 axis: face selection, clipping and reduction
 // in FP32 with error bounds; any doubt sends the pair to the float-float
 // queue instead.
+template <bool kSub>
 __global__ void __launch_bounds__(128, 5)
-k_np_clip(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, NpParams P,
+k_np_clip(const int2* __restrict__ pairs, const int4* __restrict__ subs, b3::BodiesDev Bd, b3::ShapesDev S, NpParams P,
           float4* __restrict__ pairSep, const int* __restrict__ fastQ, int* __restrict__ slowQ,
           b3Contact4* __restrict__ contacts, uint32_t* __restrict__ manifoldFlag, int32_t* __restrict__ scalars,
           b3Counters* __restrict__ counters) {
@@ -1445,7 +1524,7 @@ k_np_clip(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, NpP
         const int n = min(kPreChunk, nFast - chunk);
         if (lane < n) {
             const int p = fastQ[chunk + lane];
-            pair_prefetch(pre[lane], p, pairs[p], Bd, S);
+            item_prefetch<kSub>(pre[lane], p, pairs, subs, scalars[b3::S_NUM_PAIRS], Bd, S);
             pre[lane].aux = pairSep[p];
         }
         __syncwarp();
@@ -1498,8 +1577,10 @@ k_np_clip(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, NpP
 // normal reports it); a pair without one is finished. Its slow-queue entry
 // is cleared, so stage 3 only sees what is left. Pairs whose candidates
 // did not fit the store keep their entry for stage 3's full search.
+template <bool kSub>
 __global__ void __launch_bounds__(128, 4)
-k_np_refine(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, float4* __restrict__ pairSep,
+k_np_refine(const int2* __restrict__ pairs, const int4* __restrict__ subs, b3::BodiesDev Bd, b3::ShapesDev S,
+            float4* __restrict__ pairSep,
             int* __restrict__ fastQ, int* __restrict__ slowQ, const int* __restrict__ cand,
             uint32_t* __restrict__ manifoldFlag, int32_t* __restrict__ scalars, b3Counters* __restrict__ counters) {
     extern __shared__ __align__(16) unsigned char np_smem[];
@@ -1515,7 +1596,7 @@ k_np_refine(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, f
         const int count = __float_as_int(s4.x);
         if ((int)s4.w != kSepRefine || count <= 0) continue;
         PairCtx& c = W.ctx;
-        pair_setup_shared(c, pairs[p], Bd, S);
+        item_setup_shared<kSub>(c, p, pairs, subs, scalars[b3::S_NUM_PAIRS], Bd, S);
         if (lane < count) W.cand[lane] = cand[(size_t)q * kMaxCand + lane];
         __syncwarp();
         ff3 sep = mk3(0.f, 0.f, 0.f);
@@ -1538,8 +1619,10 @@ k_np_refine(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, f
 
 // Stage 3, the pairs either stage handed on: the whole chain with
 // float-float refinement of the axis, the faces, the clip and the reduction.
+template <bool kSub>
 __global__ void __launch_bounds__(128, 4)
-k_np_exact(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, NpParams P,
+k_np_exact(const int2* __restrict__ pairs, const int4* __restrict__ subs, b3::BodiesDev Bd, b3::ShapesDev S,
+           NpParams P,
            const float4* __restrict__ pairSep, const int* __restrict__ slowQ, const int* __restrict__ cand,
            b3Contact4* __restrict__ contacts,
            uint32_t* __restrict__ manifoldFlag, int32_t* __restrict__ scalars, b3Counters* __restrict__ counters) {
@@ -1561,7 +1644,7 @@ k_np_exact(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, Np
             const int p = slowQ[q];
             if (p < 0) continue;  // settled by the ranking stage
             PairCtx& c = W.ctx;
-            pair_setup_shared(c, pairs[p], Bd, S);
+            item_setup_shared<kSub>(c, p, pairs, subs, scalars[b3::S_NUM_PAIRS], Bd, S);
             int nOut = 0, buf = 0;
             ff3 sep = mk3(0.f, 0.f, 0.f);
             const float4 s4 = pairSep[p];
@@ -1636,30 +1719,215 @@ k_np_exact(const int2* __restrict__ pairs, b3::BodiesDev Bd, b3::ShapesDev S, Np
     }
 }
 
+// ---------------------------------------------------------------------------
+// Spheres and planes (clipHullHullKernel's sphere branches,
+// P2/satClipHullContacts.cl:957-1124): one manifold of one point per pair,
+// decided in float-float (a body resting on a plane or a sphere sits at the
+// contact threshold, where FP32 and FP64 decide apart)
+// ---------------------------------------------------------------------------
+__device__ void write_point_contact(b3Contact4* __restrict__ out, int slot, int A, int B, float3 pt, float depth,
+                                    float3 n, const b3::BodiesDev& Bd, const NpParams& P) {
+    *reinterpret_cast<float4*>(&out->worldPos[0][0]) = make_float4(pt.x, pt.y, pt.z, depth);
+    for (int k = 1; k < 4; ++k) *reinterpret_cast<float4*>(&out->worldPos[k][0]) = make_float4(0.f, 0.f, 0.f, 0.f);
+    *reinterpret_cast<float4*>(&out->worldNormal[0]) = make_float4(n.x, n.y, n.z, 1.f);
+    out->friction = combine_friction(Bd.friction[A], Bd.friction[B], P.frictionCombine);
+    out->pairIndex = slot;
+    out->bodyAPtrAndSignBit = Bd.invMass[A] == 0.f ? -A : A;
+    out->bodyBPtrAndSignBit = Bd.invMass[B] == 0.f ? -B : B;
+}
+
+__global__ void k_np_special(const int2* __restrict__ pairs, const int32_t* __restrict__ numPairsDev, b3::BodiesDev Bd,
+                             b3::ShapesDev S, NpParams P, b3Contact4* __restrict__ contacts,
+                             uint32_t* __restrict__ manifoldFlag) {
+    const int np = *numPairsDev;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < np; p += gridDim.x * blockDim.x) {
+        const int2 pr = pairs[p];
+        const int A = pr.x, B = pr.y;
+        const b3Collidable cA = S.cols[Bd.collidable[A]], cB = S.cols[Bd.collidable[B]];
+        const int tA = cA.shapeType, tB = cB.shapeType;
+        if (!((tA == B3_SHAPE_SPHERE && (tB == B3_SHAPE_SPHERE || tB == B3_SHAPE_PLANE)) ||
+              (tA == B3_SHAPE_PLANE && tB == B3_SHAPE_SPHERE)))
+            continue;
+        if (Bd.invMass[A] == 0.f && Bd.invMass[B] == 0.f) continue;
+        const float4 pA4 = Bd.pos[A], pB4 = Bd.pos[B];
+        bool hit = false;
+        if (tA == B3_SHAPE_SPHERE && tB == B3_SHAPE_SPHERE) {
+            // len = |posA - posB| <= rA + rB; normalOnSurfaceB = (posA - posB) / len
+            const ff3 d = {two_sum(pA4.x, -pB4.x), two_sum(pA4.y, -pB4.y), two_sum(pA4.z, -pB4.z)};
+            const ff rs = two_sum(cA.radius, cB.radius);
+            const ff l2 = dot3(d, d);
+            if (le(l2, mul(rs, rs))) {
+                const ff len = sqrt_ff(l2);
+                const float dist = val(sub(len, rs));
+                float3 nB = make_float3(1.f, 0.f, 0.f);
+                if (val(len) > 0.00001f) nB = to_f3(scale3(d, div(mk(1.f), len)));
+                const float3 pt = make_float3(pB4.x, pB4.y, pB4.z) + nB * cB.radius;
+                write_point_contact(&contacts[p], p, A, B, pt, dist, -nB, Bd, P);
+                hit = true;
+            }
+        } else {
+            // computeContactPlaneConvex with the plane's body on side A
+            const int Pl = tA == B3_SHAPE_PLANE ? A : B, Sp = tA == B3_SHAPE_PLANE ? B : A;
+            const b3Collidable cP = tA == B3_SHAPE_PLANE ? cA : cB, cS = tA == B3_SHAPE_PLANE ? cB : cA;
+            const float4 pl = *reinterpret_cast<const float4*>(&S.faces[cP.shapeIndex].plane[0]);
+            const float4 pP = Bd.pos[Pl], pS = Bd.pos[Sp];
+            const ffmat R = quat_mat(Bd.quat[Pl]);
+            const ff3 rel = {two_sum(pS.x, -pP.x), two_sum(pS.y, -pP.y), two_sum(pS.z, -pP.z)};
+            const ff3 cl = mrot_t(R, rel);
+            const ff dist = sub(sub(dot3(mk3(pl.x, pl.y, pl.z), cl), mk(cS.radius)), mk(pl.w));
+            if (lt(dist, mk(0.f))) {
+                const float3 nw = to_f3(mrot(R, make_float3(pl.x, pl.y, pl.z)));
+                const float3 pt = make_float3(pS.x, pS.y, pS.z) - nw * cS.radius;
+                write_point_contact(&contacts[p], p, Pl, Sp, pt, val(dist), nw, Bd, P);
+                hit = true;
+            }
+        }
+        if (hit) manifoldFlag[p] = 1u;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Compound and mesh pairs: sub-pairs in pair order (count, scan, write)
+// ---------------------------------------------------------------------------
+// A mesh triangle's local AABB against a body's world AABB (the reference
+// culls so, P2/sat.cl:985-1012; inclusive)
+__device__ __forceinline__ bool tri_overlaps(const float4* __restrict__ tv, float4 mn, float4 mx) {
+    const float4 a = __ldg(&tv[0]), b = __ldg(&tv[1]), c = __ldg(&tv[2]);
+    const float x0 = fminf(fminf(a.x, b.x), c.x), x1 = fmaxf(fmaxf(a.x, b.x), c.x);
+    const float y0 = fminf(fminf(a.y, b.y), c.y), y1 = fmaxf(fmaxf(a.y, b.y), c.y);
+    const float z0 = fminf(fminf(a.z, b.z), c.z), z1 = fmaxf(fmaxf(a.z, b.z), c.z);
+    return !(x0 > mx.x || x1 < mn.x) && !(z0 > mx.z || z1 < mn.z) && !(y0 > mx.y || y1 < mn.y);
+}
+
+// What a pair expands into: compound x compound / hull (n child pairs), or
+// mesh x hull (the mesh's triangles). kind 0 = nothing.
+struct SubPlan {
+    int kind;       // 1 compound, 2 mesh
+    int A, B;       // manifold sides (the mesh body takes side A)
+    int nA, nB;     // children per side (1 for a hull)
+    int sA, sB;     // first child, or -(polytope + 1)
+    int triBase;    // mesh: first triangle polytope
+    int numTri, triVerts;
+};
+
+__device__ __forceinline__ SubPlan sub_plan(int2 pr, const b3::BodiesDev& Bd, const b3::ShapesDev& S) {
+    SubPlan pl{};
+    const int A = pr.x, B = pr.y;
+    if (Bd.invMass[A] == 0.f && Bd.invMass[B] == 0.f) return pl;
+    const b3Collidable cA = S.cols[Bd.collidable[A]], cB = S.cols[Bd.collidable[B]];
+    const int tA = cA.shapeType, tB = cB.shapeType;
+    if (tA == B3_SHAPE_COMPOUND_OF_CONVEX_HULLS || tB == B3_SHAPE_COMPOUND_OF_CONVEX_HULLS) {
+        const bool okA = tA == B3_SHAPE_COMPOUND_OF_CONVEX_HULLS || tA == B3_SHAPE_CONVEX_HULL;
+        const bool okB = tB == B3_SHAPE_COMPOUND_OF_CONVEX_HULLS || tB == B3_SHAPE_CONVEX_HULL;
+        if (!okA || !okB) return pl;
+        pl.kind = 1;
+        pl.A = A;
+        pl.B = B;
+        pl.nA = tA == B3_SHAPE_COMPOUND_OF_CONVEX_HULLS ? cA.numChildShapes : 1;
+        pl.nB = tB == B3_SHAPE_COMPOUND_OF_CONVEX_HULLS ? cB.numChildShapes : 1;
+        pl.sA = tA == B3_SHAPE_COMPOUND_OF_CONVEX_HULLS ? cA.shapeIndex : -(cA.shapeIndex + 1);
+        pl.sB = tB == B3_SHAPE_COMPOUND_OF_CONVEX_HULLS ? cB.shapeIndex : -(cB.shapeIndex + 1);
+        return pl;
+    }
+    int M = -1, H = -1;
+    b3Collidable cM{}, cH{};
+    if (tA == B3_SHAPE_CONCAVE_TRIMESH && tB == B3_SHAPE_CONVEX_HULL) M = A, H = B, cM = cA, cH = cB;
+    else if (tB == B3_SHAPE_CONCAVE_TRIMESH && tA == B3_SHAPE_CONVEX_HULL) M = B, H = A, cM = cB, cH = cA;
+    if (M < 0) return pl;
+    const b3ConvexPolyhedron& mesh = S.polys[cM.shapeIndex];
+    pl.kind = 2;
+    pl.A = M;
+    pl.B = H;
+    pl.numTri = mesh.numFaces;
+    pl.triBase = mesh.unused;
+    pl.triVerts = S.polys[mesh.unused].vertexOffset;
+    pl.sB = -(cH.shapeIndex + 1);
+    return pl;
+}
+
+// one warp per pair
+__global__ void k_sub_count(const int2* __restrict__ pairs, const int32_t* __restrict__ numPairsDev, b3::BodiesDev Bd,
+                            b3::ShapesDev S, const float4* __restrict__ aabbMin, const float4* __restrict__ aabbMax,
+                            uint32_t* __restrict__ subCount) {
+    const int np = *numPairsDev;
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < np; p += warps) {
+        const SubPlan pl = sub_plan(pairs[p], Bd, S);
+        uint32_t cnt = 0;
+        if (pl.kind == 1) {
+            cnt = (uint32_t)(pl.nA * pl.nB);
+        } else if (pl.kind == 2) {
+            const float4 mn = aabbMin[pl.B], mx = aabbMax[pl.B];
+            for (int base = 0; base < pl.numTri; base += 32) {
+                const int f = base + lane;
+                const bool ov = f < pl.numTri && tri_overlaps(S.verts + pl.triVerts + 3 * f, mn, mx);
+                cnt += __popc(__ballot_sync(0xffffffffu, ov));
+            }
+        }
+        if (lane == 0) subCount[p] = cnt;
+    }
+}
+
+// the sub-pairs that fit the slots after the pairs'; the rest are counted
+// as dropped pairs
+__global__ void k_sub_total(int32_t* __restrict__ scalars, b3Counters* __restrict__ counters, int maxSlots) {
+    const int P = scalars[b3::S_NUM_PAIRS];
+    const uint32_t total = (uint32_t)scalars[b3::S_SUB_TOTAL];
+    const uint32_t room = (uint32_t)max(0, maxSlots - P);
+    const uint32_t n = min(total, room);
+    if (total > n) atomicAdd(&counters->pairOverflow, (int)(total - n));
+    scalars[b3::S_NUM_SUB] = (int32_t)n;
+    scalars[b3::S_NUM_SLOTS] = P + (int32_t)n;
+}
+
+// one warp per pair, sub-pairs in order (children of A outer, of B inner;
+// triangles in mesh order)
+__global__ void k_sub_write(const int2* __restrict__ pairs, const int32_t* __restrict__ numPairsDev, b3::BodiesDev Bd,
+                            b3::ShapesDev S, const float4* __restrict__ aabbMin, const float4* __restrict__ aabbMax,
+                            const uint32_t* __restrict__ subOffset, const int32_t* __restrict__ scalars,
+                            int4* __restrict__ subs) {
+    const int np = *numPairsDev;
+    const int n = scalars[b3::S_NUM_SUB];
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < np; p += warps) {
+        const int off = (int)subOffset[p];
+        if (off >= n) continue;
+        const SubPlan pl = sub_plan(pairs[p], Bd, S);
+        if (pl.kind == 1) {
+            const int total = pl.nA * pl.nB;
+            for (int k = lane; k < total && off + k < n; k += 32) {
+                const int i = k / pl.nB, j = k - i * pl.nB;
+                subs[off + k] = make_int4(pl.A, pl.B, pl.sA >= 0 ? pl.sA + i : pl.sA, pl.sB >= 0 ? pl.sB + j : pl.sB);
+            }
+        } else if (pl.kind == 2) {
+            const float4 mn = aabbMin[pl.B], mx = aabbMax[pl.B];
+            int run = 0;
+            for (int base = 0; base < pl.numTri; base += 32) {
+                const int f = base + lane;
+                const bool ov = f < pl.numTri && tri_overlaps(S.verts + pl.triVerts + 3 * f, mn, mx);
+                const unsigned m = __ballot_sync(0xffffffffu, ov);
+                const int pos = off + run + __popc(m & b3dev::lanemask_lt());
+                if (ov && pos < n) subs[pos] = make_int4(pl.A, pl.B, -(pl.triBase + f + 1), pl.sB);
+                run += __popc(m);
+            }
+        }
+    }
+}
+
 }  // namespace
 
 namespace b3 {
 
-int launch_narrowphase(b3World_t* w, cudaStream_t st) {
-    // work counters and queue lengths S_NP_WORK .. S_NP_WORK3
+// The four narrowphase stages over the pairs (kSub false) or the sub-pairs
+// of compound and mesh pairs (kSub true).
+template <bool kSub>
+static int launch_np_stages(b3World_t* w, cudaStream_t st, const NpParams& P, bool early) {
+    // work counters and queue lengths S_NP_WORK .. S_NP_WORK4
     B3_CUDA(cudaMemsetAsync(w->d.scalars + S_NP_WORK, 0, sizeof(int32_t) * 6, st));
-    if (w->cfg.maxPairs == 0 || w->bodies.empty()) return B3_OK;
-    NpParams P;
-    P.minDist = -1e30f;
-    P.maxDist = w->sim.contactBreaking;
-    P.skipDist = (float)((double)w->sim.contactProcessing - (double)w->sim.slopOffset);
-    P.frictionCombine = w->sim.frictionCombine;
-    P.maxPairs = w->cfg.maxPairs;
     const int threads = 32 * w->npWarpsPerBlock;
     const size_t smem = sizeof(WarpScratch) * w->npWarpsPerBlock;
-    if (smem > 48 * 1024 && (size_t)w->npSmemAttr < smem) {
-        // more than the default dynamic shared memory per block (8 warps);
-        // set once per size, before any capture (the first step is eager)
-        w->npSmemAttr = (int)smem;
-        B3_CUDA(cudaFuncSetAttribute(k_np_clip, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        B3_CUDA(cudaFuncSetAttribute(k_np_exact, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        B3_CUDA(cudaFuncSetAttribute(k_np_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    }
     auto grid_of = [&](const void* k) -> int {
         int occ = 1;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, threads, smem) != cudaSuccess || occ < 1) occ = 1;
@@ -1669,37 +1937,91 @@ int launch_narrowphase(b3World_t* w, cudaStream_t st) {
     const b3::ShapesDev S = w->shapesDev();
     int32_t* sc = w->d.scalars;
     const size_t smemSweep = (size_t)kSweepWarpSmem * w->npWarpsPerBlock;
-    // the early face test only where some pair can have more than 64 faces
-    // (a hull may pair with another instance of itself)
-    int maxFaces = 0;
-    for (const b3ConvexPolyhedron& h : w->polys) maxFaces = std::max(maxFaces, h.numFaces);
-    const bool early = 2 * maxFaces > 64;
-    auto sweep = early ? k_np_sweep<true> : k_np_sweep<false>;
+    auto sweep = early ? k_np_sweep<true, kSub> : k_np_sweep<false, kSub>;
     int occS = 1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occS, sweep, threads, smemSweep) != cudaSuccess || occS < 1)
         occS = 1;
-    // per-kernel events only in eagerly timed steps (never inside a capture)
-    const bool tk = w->timing && w->npEv[0] != nullptr;
+    // per-kernel events only in eagerly timed steps of the pairs (never inside a capture)
+    const bool tk = !kSub && w->timing && w->npEv[0] != nullptr;
     if (tk) B3_CUDA(cudaEventRecord(w->npEv[0], st));
     sweep<<<w->ctx->numSMs * occS, threads, smemSweep, st>>>(
-        w->d.pairs, sc + S_NUM_PAIRS, Bd, S, w->d.manifoldFlag, w->d.pairSep, w->d.npFast, w->d.npSlow,
-        w->d.npCand, std::min(w->cfg.maxPairs, kNpCandSlots), sc, w->d.counters);
+        w->d.pairs, w->d.subPairs, sc + S_NUM_PAIRS, Bd, S, w->d.manifoldFlag, w->d.pairSep, w->d.npFast,
+        w->d.npSlow, w->d.npCand, std::min(w->cfg.maxPairs, kNpCandSlots), sc, w->d.counters);
     B3_CHECK_LAUNCH();
     if (tk) B3_CUDA(cudaEventRecord(w->npEv[1], st));
-    k_np_refine<<<grid_of((const void*)k_np_refine), threads, smem, st>>>(
-        w->d.pairs, Bd, S, w->d.pairSep, w->d.npFast, w->d.npSlow, w->d.npCand, w->d.manifoldFlag, sc, w->d.counters);
+    k_np_refine<kSub><<<grid_of((const void*)k_np_refine<kSub>), threads, smem, st>>>(
+        w->d.pairs, w->d.subPairs, Bd, S, w->d.pairSep, w->d.npFast, w->d.npSlow, w->d.npCand, w->d.manifoldFlag,
+        sc, w->d.counters);
     B3_CHECK_LAUNCH();
     if (tk) B3_CUDA(cudaEventRecord(w->npEv[2], st));
-    k_np_clip<<<grid_of((const void*)k_np_clip), threads, smem, st>>>(
-        w->d.pairs, Bd, S, P, w->d.pairSep, w->d.npFast, w->d.npSlow, w->d.contacts, w->d.manifoldFlag, sc,
-        w->d.counters);
+    k_np_clip<kSub><<<grid_of((const void*)k_np_clip<kSub>), threads, smem, st>>>(
+        w->d.pairs, w->d.subPairs, Bd, S, P, w->d.pairSep, w->d.npFast, w->d.npSlow, w->d.contacts,
+        w->d.manifoldFlag, sc, w->d.counters);
     B3_CHECK_LAUNCH();
     if (tk) B3_CUDA(cudaEventRecord(w->npEv[3], st));
-    k_np_exact<<<grid_of((const void*)k_np_exact), threads, smem, st>>>(
-        w->d.pairs, Bd, S, P, w->d.pairSep, w->d.npSlow, w->d.npCand, w->d.contacts, w->d.manifoldFlag, sc,
-        w->d.counters);
+    k_np_exact<kSub><<<grid_of((const void*)k_np_exact<kSub>), threads, smem, st>>>(
+        w->d.pairs, w->d.subPairs, Bd, S, P, w->d.pairSep, w->d.npSlow, w->d.npCand, w->d.contacts,
+        w->d.manifoldFlag, sc, w->d.counters);
     B3_CHECK_LAUNCH();
     if (tk) B3_CUDA(cudaEventRecord(w->npEv[4], st));
+    return B3_OK;
+}
+
+int launch_narrowphase(b3World_t* w, cudaStream_t st) {
+    B3_CUDA(cudaMemsetAsync(w->d.scalars + S_NP_WORK, 0, sizeof(int32_t) * 6, st));
+    if (w->cfg.maxPairs == 0 || w->bodies.empty()) return B3_OK;
+    NpParams P;
+    P.minDist = -1e30f;
+    P.maxDist = w->sim.contactBreaking;
+    P.skipDist = (float)((double)w->sim.contactProcessing - (double)w->sim.slopOffset);
+    P.frictionCombine = w->sim.frictionCombine;
+    P.maxPairs = w->cfg.maxPairs;
+    // the early face test only where some pair can have more than 64 faces
+    // (a hull may pair with another instance of itself); mesh triangles are
+    // polytopes of 5 faces
+    int maxFaces = 0;
+    for (const b3Collidable& c : w->cols)
+        if (c.shapeType == B3_SHAPE_CONVEX_HULL) maxFaces = std::max(maxFaces, w->polys[c.shapeIndex].numFaces);
+    if (w->numMeshes) maxFaces = std::max(maxFaces, 5);
+    const bool early = 2 * maxFaces > 64;
+    const size_t smem = sizeof(WarpScratch) * w->npWarpsPerBlock;
+    if (smem > 48 * 1024 && (size_t)w->npSmemAttr < smem) {
+        // more than the default dynamic shared memory per block (8 warps);
+        // set once per size, before any capture (the first step is eager)
+        w->npSmemAttr = (int)smem;
+        B3_CUDA(cudaFuncSetAttribute(k_np_clip<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        B3_CUDA(cudaFuncSetAttribute(k_np_exact<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        B3_CUDA(cudaFuncSetAttribute(k_np_refine<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        B3_CUDA(cudaFuncSetAttribute(k_np_clip<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        B3_CUDA(cudaFuncSetAttribute(k_np_exact<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        B3_CUDA(cudaFuncSetAttribute(k_np_refine<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+    {
+        B3_TRY(launch_np_stages<false>(w, st, P, early));
+        if (w->hasSubPairs()) {
+            // expand compound and mesh pairs into sub-pairs, then their stages
+            const b3::BodiesDev Bd = w->bodiesDev();
+            const b3::ShapesDev S = w->shapesDev();
+            const int g = w->ctx->numSMs * 4;
+            k_sub_count<<<g, 256, 0, st>>>(w->d.pairs, w->d.scalars + S_NUM_PAIRS, Bd, S, w->d.aabbMin,
+                                          w->d.aabbMax, w->d.subCount);
+            B3_CHECK_LAUNCH();
+            B3_TRY(exclusive_scan_u32(w->d.subCount, w->d.subOffset, w->d.scalars + S_NUM_PAIRS, w->cfg.maxPairs,
+                                      (uint32_t*)(w->d.scalars + S_SUB_TOTAL), w->d.scanScratch,
+                                      w->d.scanScratchBytes, w->d.scalars + S_ERR, st, w->ctx->numSMs));
+            k_sub_total<<<1, 1, 0, st>>>(w->d.scalars, w->d.counters, w->cfg.maxPairs);
+            B3_CHECK_LAUNCH();
+            k_sub_write<<<g, 256, 0, st>>>(w->d.pairs, w->d.scalars + S_NUM_PAIRS, Bd, S, w->d.aabbMin, w->d.aabbMax,
+                                          w->d.subOffset, w->d.scalars, w->d.subPairs);
+            B3_CHECK_LAUNCH();
+            B3_TRY(launch_np_stages<true>(w, st, P, early));
+        }
+    }
+    if (w->hasSpheresPlanes()) {
+        k_np_special<<<w->ctx->numSMs * 4, 256, 0, st>>>(w->d.pairs, w->d.scalars + S_NUM_PAIRS, w->bodiesDev(),
+                                                          w->shapesDev(), P, w->d.contacts, w->d.manifoldFlag);
+        B3_CHECK_LAUNCH();
+    }
     return B3_OK;
 }
 

@@ -500,11 +500,13 @@ int launch_manifolds(b3World_t* w, cudaStream_t st) {
     B3_CUDA(cudaMemsetAsync(w->d.bodyIncStart, 0, sizeof(uint32_t) * N, st));
     B3_CUDA(cudaMemsetAsync(w->d.bodyIncEnd, 0, sizeof(uint32_t) * N, st));
     if (cap == 0 || N == 0) return B3_OK;
-    B3_TRY(exclusive_scan_u32(w->d.manifoldFlag, w->d.manifoldScan, w->d.scalars + S_NUM_PAIRS, cap,
+    // manifold slots: the pairs', then (compound and mesh worlds) the sub-pairs'
+    const int32_t* slots = w->d.scalars + (w->hasSubPairs() ? S_NUM_SLOTS : S_NUM_PAIRS);
+    B3_TRY(exclusive_scan_u32(w->d.manifoldFlag, w->d.manifoldScan, slots, cap,
                               (uint32_t*)(w->d.scalars + S_NUM_MANIFOLDS), w->d.scanScratch,
                               w->d.scanScratchBytes, w->d.scalars + S_ERR, st, w->ctx->numSMs));
     const int g = w->ctx->numSMs * 8;
-    k_manifold_emit<<<g, 256, 0, st>>>(w->d.manifoldFlag, w->d.manifoldScan, w->d.scalars + S_NUM_PAIRS,
+    k_manifold_emit<<<g, 256, 0, st>>>(w->d.manifoldFlag, w->d.manifoldScan, slots,
                                       w->d.contacts, w->d.invMass, N, w->d.manifoldPair, w->d.incKeys,
                                       w->d.incVals, w->d.scalars, w->d.counters);
     B3_CHECK_LAUNCH();

@@ -70,7 +70,7 @@ int dalloc(T*& p, size_t count) {
 void free_all(b3::DevBuffers& d) {
     void* ptrs[] = {d.pos, d.quat, d.linVel, d.angVel, d.invMass, d.friction, d.restitution,
                     d.invInertia, d.collidable, d.worldId, d.cols, d.polys, d.verts, d.faces,
-                    d.indices, d.edges, d.localAabb, d.polyInradius, d.faceExt, d.childShapes, d.aabbMin, d.aabbMax, d.smallSlot,
+                    d.indices, d.edges, d.localAabb, d.polyInradius, d.faceExt, d.childShapes, d.subPairs, d.subCount, d.subOffset, d.aabbMin, d.aabbMax, d.smallSlot,
                     d.largeStart, d.largeList, d.sapSmall, d.sapLarge, d.sapSorted, d.sapCount, d.sapOffset, d.keys, d.vals, d.keysAlt, d.valsAlt, d.cellTable,
                     d.pairs, d.contacts, d.manifoldFlag, d.pairSep, d.npFast, d.npSlow, d.npCand, d.manifoldScan,
                     d.manifoldPair,
@@ -141,6 +141,7 @@ b3::ShapesDev b3World_t::shapesDev() const {
     S.localAabb = d.localAabb;
     S.inradius = d.polyInradius;
     S.faceExt = d.faceExt;
+    S.children = d.childShapes;
     S.numPolys = (int)polys.size();
     S.numVerts = (int)verts4.size() / 4;
     S.numFaces = (int)faces.size();
@@ -730,6 +731,12 @@ static int ensure_capacity(b3World w) {
     if (incBytes > d.incSortScratchBytes) {
         d.incSortScratchBytes = incBytes;
         B3_TRY(dalloc((unsigned char*&)d.incSortScratch, incBytes));
+    }
+    if (w->hasSubPairs() && !d.subPairs) {
+        const size_t c = std::max(cap, 1);
+        B3_TRY(dalloc(d.subPairs, c));
+        B3_TRY(dalloc(d.subCount, c));
+        B3_TRY(dalloc(d.subOffset, c));
     }
     if (!d.worldStats) B3_TRY(dalloc(d.worldStats, 2 * (size_t)w->cfg.numWorlds));
     if (!d.worldMStart) {

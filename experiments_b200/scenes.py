@@ -363,3 +363,75 @@ def lattice_block(scene, dims, block, blocks=(4, 4)):
              friction=scene.friction[idx], world=scene.world[idx], lin=scene.lin[idx], ang=scene.ang[idx])
     return Scene(name=f"{scene.name}_block{block}", shapes=scene.shapes, num_worlds=1, config=dict(scene.config),
                  steps=scene.steps, **b)
+
+
+def spheres_on_plane(seed=81, n=200, box=6.0):
+    """Spheres of radius U(0.2, 0.5) dropped as a random pile onto a static
+    plane y = 0 (the reference's sphere and plane shapes)."""
+    radii = uniform(seed, 1, n, 0.2, 0.5)
+    shapes = [{"kind": "plane", "normal": [0.0, 1.0, 0.0], "constant": 0.0}] + \
+        [{"kind": "sphere", "radius": float(r)} for r in radii]
+    u = uniform(seed, 2, 3 * n).reshape(n, 3)
+    pos = np.stack([u[:, 0] * box - box / 2, 0.6 + u[:, 1] * box, u[:, 2] * box - box / 2], 1)
+    lin = normal(seed, 3, 3 * n, 0.5).reshape(n, 3)
+    parts = [_bodies([0], [0.0], [[0, 0, 0]], [[0, 0, 0, 1.0]], [0.6], [0]),
+             _bodies(np.arange(1, n + 1), uniform(seed, 4, n, 0.5, 2.0), pos, np.tile([0, 0, 0, 1.0], (n, 1)),
+                     uniform(seed, 5, n, 0.3, 0.9), np.zeros(n), lin=lin)]
+    b = _concat(parts)
+    return Scene(name=f"spheres_{n}", shapes=shapes, num_worlds=1,
+                 config=dict(cellSize=1.0, gridDims=(32, 32, 32)), steps=1, **b)
+
+
+def compound_pile(seed=82, n=120, spacing=4.0):
+    """Compounds of unit cubes (two-cube bars and three-cube L shapes,
+    children at fixed offsets and turns) mixed with 12-point hulls, in
+    random orientations on a jittered 4 x k x 4 lattice (spacing beyond any
+    two bodies' reach, so nothing starts interpenetrating), dropped onto a
+    static ground box."""
+    q90 = [0.0, np.sin(np.pi / 4), 0.0, np.cos(np.pi / 4)]
+    shapes = [box_vertices(10.0, 0.5, 10.0), box_vertices(0.5, 0.5, 0.5)] + hull_pool(seed, 4)
+    shapes.append({"kind": "compound", "children": [(1, (0.55, 0.0, 0.0), [0, 0, 0, 1.0]),
+                                                    (1, (-0.55, 0.0, 0.0), [0, 0, 0, 1.0])]})
+    shapes.append({"kind": "compound", "children": [(1, (0.0, 0.0, 0.0), [0, 0, 0, 1.0]),
+                                                    (1, (1.05, 0.0, 0.0), q90), (1, (0.0, 0.0, 1.05), q90)]})
+    k = uniform(seed, 1, n)
+    sid = np.where(k < 0.35, 6, np.where(k < 0.7, 7, 2 + (uniform(seed, 2, n) * 4).astype(np.int32) % 4))
+    i = np.arange(n)
+    lat = np.stack([i % 4, i // 16, (i // 4) % 4], 1).astype(np.float64)
+    pos = (lat - [1.5, 0.0, 1.5]) * spacing + [0.0, 2.0, 0.0] + uniform(seed, 3, 3 * n, -0.2, 0.2).reshape(n, 3)
+    q = normal(seed, 4, 4 * n).reshape(n, 4)
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    parts = [ground(), _bodies(sid, uniform(seed, 5, n, 0.5, 2.0), pos, q, uniform(seed, 6, n, 0.3, 0.9), np.zeros(n),
+                               lin=normal(seed, 7, 3 * n, 0.5).reshape(n, 3))]
+    b = _concat(parts)
+    return Scene(name=f"compounds_{n}", shapes=shapes, num_worlds=1,
+                 config=dict(cellSize=1.5, gridDims=(32, 32, 32)), steps=1, **b)
+
+
+def mesh_terrain(seed=83, n=150, cells=16, size=16.0, box=6.0):
+    """A static triangle-mesh terrain (cells x cells squares of two
+    triangles, heights U(0, 0.3)) at the origin, with unit cubes and
+    12-point hulls dropped as a random pile onto it."""
+    g = cells + 1
+    hx = (np.arange(g) / cells - 0.5) * size
+    X, Z = np.meshgrid(hx, hx, indexing="ij")
+    Y = uniform(seed, 1, g * g, 0.0, 0.3).reshape(g, g)
+    verts = np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1).astype(np.float32)
+    idx = []
+    for i in range(cells):
+        for j in range(cells):
+            a, b_, c, d = i * g + j, (i + 1) * g + j, i * g + j + 1, (i + 1) * g + j + 1
+            idx += [a, c, b_, b_, c, d]  # counter-clockwise seen from above (+y)
+    shapes = [{"kind": "mesh", "vertices": verts, "indices": np.array(idx, np.int32)},
+              box_vertices(0.5, 0.5, 0.5)] + hull_pool(seed, 4)
+    k = uniform(seed, 2, n)
+    sid = np.where(k < 0.5, 1, 2 + (uniform(seed, 3, n) * 4).astype(np.int32) % 4)
+    u = uniform(seed, 4, 3 * n).reshape(n, 3)
+    pos = np.stack([u[:, 0] * box - box / 2, 1.2 + u[:, 1] * 2 * box, u[:, 2] * box - box / 2], 1)
+    q = normal(seed, 5, 4 * n).reshape(n, 4)
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    parts = [_bodies([0], [0.0], [[0, 0, 0]], [[0, 0, 0, 1.0]], [0.6], [0]),
+             _bodies(sid, uniform(seed, 6, n, 0.5, 2.0), pos, q, uniform(seed, 7, n, 0.3, 0.9), np.zeros(n))]
+    b = _concat(parts)
+    return Scene(name=f"terrain_{n}", shapes=shapes, num_worlds=1,
+                 config=dict(cellSize=1.0, gridDims=(32, 32, 32)), steps=1, **b)

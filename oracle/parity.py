@@ -123,14 +123,22 @@ def one_step_report(w, o, dynamic=None, make_oracle=None):
             ox.close()
         solver = _state_errors(gs, solved[0], sel)
         env = _state_errors(solved[1], solved[0], sel)
+        # how far the FP64 solve moves when given the device's contacts
+        # instead of its own (both within the contact bars): the problem's
+        # sensitivity to those differences, not an arithmetic error
+        sens = _state_errors(solved[0], os_, sel)
         rep["solver_err"] = solver
         rep["fp32_envelope"] = env
-        # the bar: the stated tolerance, or twice what FP32 arithmetic of the
-        # same algorithm shows on this state, whichever is larger
+        rep["contact_sensitivity"] = sens
+        # the bars: the stated tolerance, or twice what FP32 arithmetic of the
+        # same algorithm shows on this state, whichever is larger; the whole
+        # step also carries the sensitivity to the contact differences
         bars = {k: max(tol[k], 2.0 * env[k]) for k in tol}
+        step_bars = {k: max(tol[k], 2.0 * (env[k] + sens[k])) for k in tol}
         rep["bars_used"] = bars
+        rep["step_bars_used"] = step_bars
         rep["solver_within_bars"] = all(solver[k] <= bars[k] for k in tol)
-        rep["step_within_bars"] = all(rep[k] <= bars[k] for k in tol)
+        rep["step_within_bars"] = all(rep[k] <= step_bars[k] for k in tol)
     else:
         rep["step_within_bars"] = all(rep[k] <= tol[k] for k in tol)
     rep["within_bars"] = bool(narrow_ok and rep["step_within_bars"] and rep.get("solver_within_bars", True)
