@@ -216,16 +216,21 @@ __device__ __forceinline__ bool axis_dir(const PairCtx& c, const b3::ShapesDev& 
         const int e = idx - FA - FB;
         const int EB = pb.numUniqueEdges;
         const int e0 = e / EB, e1 = e - e0 * EB;
-        const float3 wa = mul(c.RA, f3(__ldg(&S.edges[pa.uniqueEdgesOffset + e0])));
-        const float3 wb = mul(c.RB, f3(__ldg(&S.edges[pb.uniqueEdgesOffset + e1])));
+        const float4 ea = __ldg(&S.edges[pa.uniqueEdgesOffset + e0]);
+        const float4 eb = __ldg(&S.edges[pb.uniqueEdgesOffset + e1]);
+        const float3 wa = mul(c.RA, f3(ea));
+        const float3 wb = mul(c.RB, f3(eb));
         float3 cr = cross(wa, wb);
         if (!(fabsf(cr.x) > 1e-6f || fabsf(cr.y) > 1e-6f || fabsf(cr.z) > 1e-6f)) return false;
         const float cl = length(cr);
         n = cr * (1.f / cl);
-        // direction error of the normalised FP32 cross product is ~ulp/cl;
-        // its depth error scales with the projected extents (delta / 1e-6)
-        err = delta + 0.3f * delta / cl;
-        lb = wantLb ? rinSum - fabsf(dot(D, n)) - 1e-5f * (1.f + lD) - 1e-6f * lD / cl - 2.f * err : -FLT_MAX;
+        // direction error of the normalised FP32 cross product is ~ulp/sin,
+        // sin = cl over the edges' lengths (w: 1 for a hull's unit edges, the
+        // length of a mesh triangle's edge); its depth error scales with the
+        // projected extents (delta / 1e-6)
+        const float isin = ea.w * eb.w / cl;
+        err = delta + 0.3f * delta * isin;
+        lb = wantLb ? rinSum - fabsf(dot(D, n)) - 1e-5f * (1.f + lD) - 1e-6f * lD * isin - 2.f * err : -FLT_MAX;
     }
     const bool f = dot(D, n) < 0.f;
     if (f) n = -n;

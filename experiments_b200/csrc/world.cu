@@ -319,7 +319,7 @@ extern "C" int b3_register_convex_hull(b3World w, const float* vertices, int num
         w->edges4.push_back(P.uniqueEdges[3 * i]);
         w->edges4.push_back(P.uniqueEdges[3 * i + 1]);
         w->edges4.push_back(P.uniqueEdges[3 * i + 2]);
-        w->edges4.push_back(0.f);
+        w->edges4.push_back(1.f);  // w: the edge's length (unit edges)
     }
     b3Collidable col;
     col.numChildShapes = 0;
@@ -548,8 +548,12 @@ extern "C" int b3_register_concave_mesh(b3World w, const float* vertices3, int n
         for (int i = 0; i < 3; ++i) {
             const float* a = tv[i];
             const float* b = tv[(i + 1) % 3];
-            for (int k = 0; k < 3; ++k) w->edges4.push_back(b[k] - a[k]);
-            w->edges4.push_back(0.f);
+            float e[3];
+            for (int k = 0; k < 3; ++k) e[k] = b[k] - a[k];
+            for (int k = 0; k < 3; ++k) w->edges4.push_back(e[k]);
+            // w: the edge's length, rounded up (scales the sweep's error bound)
+            w->edges4.push_back(std::nextafter((float)std::sqrt((double)e[0] * e[0] + (double)e[1] * e[1] +
+                                                                (double)e[2] * e[2]), 1e30f));
         }
         tp.radius = 0.f;
         w->polys.push_back(tp);
