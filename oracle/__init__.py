@@ -87,6 +87,7 @@ def lib(f32=False, dual=False):
         L.or_clip_face_world.argtypes = [_D, C.c_int, _D, _D, C.c_int, C.c_double, C.c_double, _D]
         L.or_set_tangent.argtypes = [_VP, _D, _D, _D, _D, _D]
         L.or_get_tangent.argtypes = [_VP, _D, _D, _D, _D]
+        L.or_set_tangent_pose.argtypes = [_VP, _D, _D]
         L.or_real_kind.restype = C.c_int
         L.or_set_broadphase.argtypes = [_VP, C.c_int]
         L.or_set_solver.argtypes = [_VP, C.c_int]
@@ -358,6 +359,13 @@ class OracleWorld:
             b[:, :a.shape[1]] = a
             keep.append(np.ascontiguousarray(b))
         self.L.or_set_tangent(self.h, *[None if a is None else _d(a) for a in keep])
+
+    def set_tangent_pose(self, pos=None, quat=None):
+        """Derivative seeds of the positions and quaternions (n x 4; None
+        leaves zero), after set_tangent, which zeroes them."""
+        arrs = [None if a is None else np.ascontiguousarray(np.asarray(a, np.float64).reshape(self.n, 4))
+                for a in (pos, quat)]
+        self.L.or_set_tangent_pose(self.h, *[None if a is None else _d(a) for a in arrs])
 
     def tangent(self):
         """Derivatives of (pos, quat, lin, ang), each n x 4."""

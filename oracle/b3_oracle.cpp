@@ -1664,6 +1664,15 @@ void or_set_tangent(or_world* w, const double* dlin4, const double* dang4, const
         for (int k = 0; k < 3; ++k) set_tan(w->invInertia[3 * i + k], dInvInertia3 ? dInvInertia3[3 * i + k] : 0.0);
     }
 }
+// Derivative seeds of the pose (position and quaternion, n x 4 each), set
+// after or_set_tangent (which zeroes them): with them a run continues a
+// tangent from any state, e.g. one step at a time along another trajectory.
+void or_set_tangent_pose(or_world* w, const double* dpos4, const double* dquat4) {
+    for (size_t i = 0; i < 4 * (size_t)w->n; ++i) {
+        if (dpos4) set_tan(w->pos[i], dpos4[i]);
+        if (dquat4) set_tan(w->quat[i], dquat4[i]);
+    }
+}
 void or_get_tangent(or_world* w, double* dpos4, double* dquat4, double* dlin4, double* dang4) {
     for (size_t i = 0; i < 4 * (size_t)w->n; ++i) {
         if (dpos4) dpos4[i] = rtan(w->pos[i]);

@@ -7,6 +7,8 @@ import numpy as np
 
 import oracle
 from experiments_b200 import b3, scenes
+from oracle import tangent_chain
+from oracle.tangent_chain import com_seeds, param_tangents, world_functional  # noqa: F401
 
 
 def make_oracle(host_ctx, scene, dual=False):
@@ -28,17 +30,6 @@ def oracle_state_at(host_ctx, scene, steps):
     st = [a.astype(np.float32).astype(np.float64) for a in o.state()]
     o.close()
     return st
-
-
-def world_functional(scene, state, seeds):
-    """Per-world linear functional sum <seed, state> over (pos, quat, lin, ang)."""
-    wid = np.asarray(scene.world)
-    out = np.zeros(scene.num_worlds)
-    for k in range(4):
-        cols = 4 if k == 1 else 3
-        contrib = np.sum(seeds[k][:, :cols] * state[k][:, :cols], axis=1)
-        np.add.at(out, wid, contrib)
-    return out
 
 
 def oracle_run(host_ctx, scene, state, steps, seeds, kind=None, delta=None, eps=0.0):
@@ -77,26 +68,29 @@ def oracle_tangent(host_ctx, scene, state, steps, seeds, kind, delta):
     derivatives and the per-world active-set signatures."""
     o, ii = make_oracle(host_ctx, scene, dual=True)
     o.set_state_f64(*[a.copy() for a in state])
-    m = np.asarray(scene.mass, np.float64)
-    dyn = m > 0
-    im = np.where(dyn, 1.0 / np.where(dyn, m, 1), 0.0)
     delta = np.asarray(delta, np.float64)
     if kind == "lin":
         o.set_tangent(lin=delta)
     elif kind == "ang":
         o.set_tangent(ang=delta)
-    elif kind == "mass":
-        # invMass = 1/m and the inverse inertia is invMass times a shape factor
-        dim = np.where(dyn, -delta / np.where(dyn, m, 1) ** 2, 0.0)
-        o.set_tangent(inv_mass=dim, inv_inertia3=ii * np.where(dyn, dim / np.where(dyn, im, 1), 0.0)[:, None])
-    elif kind == "friction":
-        o.set_tangent(friction=delta)
+    else:
+        o.set_tangent(**param_tangents(scene, ii, kind, delta))
     o.reset_active()
     o.step(steps)
     d = o.tangent()
     h = o.active_hash()
     o.close()
     return world_functional(scene, d, seeds), h
+
+
+def chained_tangent(host_ctx, scene, traj, seeds, kind, delta):
+    """The FP64 tangent chained along a recorded trajectory
+    (oracle.tangent_chain.chained_tangent) with a fresh tangent-linear
+    oracle of the scene."""
+    o, ii = make_oracle(host_ctx, scene, dual=True)
+    out = tangent_chain.chained_tangent(o, ii, scene, traj, seeds, kind, delta)
+    o.close()
+    return out
 
 
 def tangent_vectors(host_ctx, scene, state, steps, seeds, kind, per):
@@ -119,6 +113,19 @@ def tangent_vectors(host_ctx, scene, state, steps, seeds, kind, per):
             g[bodies, c] = t[wid[bodies]]
             h0 = h if h0 is None else h0
     return g, h0
+
+
+def device_trajectory(ctx, scene, state, steps):
+    """The device's states s_0 .. s_steps (FP32 values as FP64), one step
+    at a time from `state`."""
+    w = scenes.build_world(ctx, scene, useGraph=1)
+    w.write_state(*[np.asarray(a, np.float32) for a in state])
+    traj = [[a.astype(np.float64) for a in w.read_state()]]
+    for _ in range(steps):
+        w.stepSimulation(1)
+        traj.append([a.astype(np.float64) for a in w.read_state()])
+    w.close()
+    return traj
 
 
 def gpu_adjoint(ctx, scene, state, steps, seeds, checkpoint_every=16):

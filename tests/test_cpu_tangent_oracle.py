@@ -37,3 +37,32 @@ def test_tangent_matches_fp64_central_differences(host_ctx, t0, steps):
         assert np.all(rel[same] < 1e-5), (kind, rel, same)
         checked += int(same.sum())
     assert checked >= 8
+
+
+def test_chained_one_step_tangents_equal_the_multi_step_tangent(host_ctx):
+    """Carrying the tangent from step to step through the pose and velocity
+    seeds reproduces the tangent of one multi-step run when the recorded
+    trajectory is the oracle's own: the machinery that linearises the FP64
+    step along another (the device's) trajectory."""
+    from adjoint_harness import chained_tangent, make_oracle
+    sc = scenes.c4(worlds=4)
+    steps = 12
+    st = oracle_state_at(host_ctx, sc, 20)
+    o, _ = make_oracle(host_ctx, sc)
+    o.set_state_f64(*st)
+    traj = [[a.copy() for a in st]]
+    for _ in range(steps):
+        o.step(1)
+        traj.append(o.state())
+    o.close()
+    rng = np.random.default_rng(17)
+    seeds = random_seeds(sc, rng)
+    dyn = np.asarray(sc.mass) > 0
+    for kind in ("lin", "ang", "mass", "friction"):
+        comps = 3 if kind in ("lin", "ang") else 1
+        d = rng.normal(size=(sc.n, comps)) * dyn[:, None]
+        dd = d if comps == 3 else d[:, 0]
+        whole, _ = oracle_tangent(host_ctx, sc, st, steps, seeds, kind, dd)
+        chained, dev_pos, dev_vel = chained_tangent(host_ctx, sc, traj, seeds, kind, dd)
+        assert dev_pos.max() == 0 and dev_vel.max() == 0
+        assert np.allclose(chained, whole, rtol=1e-10, atol=1e-12 * np.abs(whole).max()), (kind, chained, whole)

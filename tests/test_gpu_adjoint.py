@@ -8,7 +8,9 @@ signs them) is the same for the +eps and -eps runs."""
 import numpy as np
 import pytest
 
-from adjoint_harness import Rollout, gpu_adjoint, oracle_run, oracle_state_at, random_seeds, tangent_vectors
+from adjoint_harness import (Rollout, com_seeds, device_trajectory, gpu_adjoint, make_oracle, oracle_run,
+                             oracle_state_at, random_seeds, tangent_vectors)
+from oracle import tangent_chain
 from experiments_b200 import scenes
 
 pytestmark = pytest.mark.gpu
@@ -114,6 +116,31 @@ def test_multi_step_gradients_against_fp64_tangent_oracle(ctx, host_ctx, throw, 
         ref, _ = tangent_vectors(host_ctx, sc, st, steps, seeds, kind, PER)
         rels += list(_world_rel(sc, g[kind].reshape(sc.n, -1), ref))
     assert np.median(rels) < median_bound, rels
+
+
+def test_throw_gradients_along_the_device_trajectory(ctx, host_ctx, throw):
+    """The throw at its full length: the loss (sum over worlds of the
+    squared distance of the centre of mass from its target) after 120 steps,
+    checkpoints every 16. The FP64 reference is the tangent-linear step
+    chained along the device's own FP32 trajectory, so the trajectory's
+    sensitivity (chaotic over 120 steps) cancels and what remains is the
+    adjoint's own error: within 1e-3 relative on every stable world."""
+    sc = throw
+    st = oracle_state_at(host_ctx, sc, 0)
+    traj = device_trajectory(ctx, sc, st, 120)
+    seeds = com_seeds(sc, traj[-1][0])
+    g = gpu_adjoint(ctx, sc, st, 120, seeds, checkpoint_every=16)
+    assert g["unclassified"] == 0
+    # the checkpointed forward is the recorded trajectory, bit for bit
+    for a, b in zip(g["final"], traj[-1]):
+        assert np.array_equal(a, b)
+    o, ii = make_oracle(host_ctx, sc, dual=True)
+    rel, stable = tangent_chain.gradient_errors(o, ii, sc, traj, g, seeds)
+    o.close()
+    print({k: v.tolist() for k, v in rel.items()}, stable.tolist())
+    assert stable.sum() >= W // 2, stable
+    for kind, r in rel.items():
+        assert np.all(r[stable] < 1e-3), (kind, r, stable)
 
 
 def test_checkpoint_interval_does_not_change_gradients(ctx, host_ctx, throw):
