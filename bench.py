@@ -374,6 +374,7 @@ def oracle_check(w, sc):
             "pairs", "manifolds", "pair_overflow", "narrowphase_within_bars", "solver_err", "fp32_envelope",
             "contact_sensitivity", "bars_used", "step_bars_used", "within_bars", "check_s"]
     out = {k: rep[k] for k in keep}
+    out["manifolds_differing"] = len(rep["manifold_differences"])
     out["bars"] = ("pairs/keys/permutation bit-exact; contacts 1e-5 m, normals 1e-4; one step 1e-5 m, 1e-4 m/s, or "
                    "twice the FP32 envelope (the oracle's FP32 build against its FP64 build from the same contacts) "
                    "where that is larger; solver_err: the device's solve against the FP64 oracle's from the "

@@ -33,7 +33,6 @@ struct ShapesDev {
     const float4* edges;
     const float4* localAabb;  // 2 per collidable (min, max)
     const float* inradius;    // per polyhedron: lower bound of its support about localCenter
-    const float2* faceExt;    // per face: (min, max) over its hull's vertices of n . v (local frame)
     const b3ChildShape* children;  // the compounds' children
     int numPolys, numVerts, numFaces, numIndices, numEdges;
     int tableBytes;           // packed size for shared-memory staging
@@ -67,7 +66,6 @@ struct DevBuffers {
     float4* edges = nullptr;
     float4* localAabb = nullptr;
     float* polyInradius = nullptr;
-    float2* faceExt = nullptr;  // per face: the hull's extent along the face normal
     b3ChildShape* childShapes = nullptr;
     // compound and mesh pairs: sub-pair records (body A, body B, side A,
     // side B; a side is a child shape >= 0 or -(polytope + 1)), per pair
@@ -170,7 +168,6 @@ struct b3World_t {
     std::vector<b3ConvexPolyhedron> polys;
     std::vector<float> verts4, edges4, localAabb8;
     std::vector<float> polyInradius;
-    std::vector<float> faceExt;   // 2 per face: min, max of n . v over the face's hull
     std::vector<b3ChildShape> childShapes;  // children of the compounds
     int numSpheres = 0, numPlanes = 0, numCompounds = 0, numMeshes = 0;
     bool hasSpheresPlanes() const { return numSpheres > 0 && (numSpheres > 1 || numPlanes > 0); }

@@ -199,7 +199,7 @@ __device__ __forceinline__ void project_rel(const float4* __restrict__ verts, in
 // near-minimum candidates (depth - err <= the minimum's depth + err).
 __device__ __forceinline__ bool axis_dir(const PairCtx& c, const b3::ShapesDev& S, int idx, float3 D, float delta,
                                          float rinSum, float3& n, float& err, float& lb, bool& isFace,
-                                         bool wantLb = true, bool* flipped = nullptr) {
+                                         bool wantLb = true) {
     const b3ConvexPolyhedron& pa = *c.pa;
     const b3ConvexPolyhedron& pb = *c.pb;
     const int FA = pa.numFaces, FB = pb.numFaces;
@@ -232,9 +232,7 @@ __device__ __forceinline__ bool axis_dir(const PairCtx& c, const b3::ShapesDev& 
         err = delta + 0.3f * delta * isin;
         lb = wantLb ? rinSum - fabsf(dot(D, n)) - 1e-5f * (1.f + lD) - 1e-6f * lD * isin - 2.f * err : -FLT_MAX;
     }
-    const bool f = dot(D, n) < 0.f;
-    if (f) n = -n;
-    if (flipped) *flipped = f;
+    if (dot(D, n) < 0.f) n = -n;
     return true;
 }
 
@@ -249,31 +247,6 @@ __device__ __forceinline__ float axis_depth(const PairCtx& c, const b3::ShapesDe
     const float off = dot(rel, n);  // posB - posA along n
     mn1 += off;
     mx1 += off;
-    return fminf(mx0 - mn1, mx1 - mn0);
-}
-
-// FP32 depth along the oriented face axis n of face idx (flipped: n is
-// the negated face normal). The face's own hull projects onto its normal
-// over the registered extent (faceExt, exact and rounded outward), so only
-// the other hull's vertices are projected. Lanes on faces of A and of B run
-// the same code on selected data (the other hull and its rotation), so a
-// warp holding both kinds does not serialise two loops.
-__device__ __forceinline__ float face_axis_depth(const PairCtx& c, const b3::ShapesDev& S, int idx, float3 rel,
-                                                 float3 n, bool flipped) {
-    const bool onA = idx < c.pa->numFaces;
-    const b3ConvexPolyhedron* own = onA ? c.pa : c.pb;
-    const b3ConvexPolyhedron* oth = onA ? c.pb : c.pa;
-    const float2 ext = __ldg(&S.faceExt[own->faceOffset + (onA ? idx : idx - c.pa->numFaces)]);
-    Mat3 R;
-    R.r0 = onA ? c.RB.r0 : c.RA.r0;
-    R.r1 = onA ? c.RB.r1 : c.RA.r1;
-    R.r2 = onA ? c.RB.r2 : c.RA.r2;
-    float mo, xo;
-    project_rel(S.verts, oth->vertexOffset, oth->numVertices, R, n, mo, xo);
-    const float lo = flipped ? -ext.y : ext.x, hi = flipped ? -ext.x : ext.y;
-    const float off = dot(rel, n);  // posB - posA along n
-    const float mn0 = onA ? lo : mo, mx0 = onA ? hi : xo;
-    const float mn1 = (onA ? mo : lo) + off, mx1 = (onA ? xo : hi) + off;
     return fminf(mx0 - mn1, mx1 - mn0);
 }
 
@@ -440,10 +413,9 @@ __device__ __forceinline__ int sweep_axes(PairCtx& c, const b3::ShapesDev& S, in
         for (int idx = i0 + lane; idx < i1; idx += 32) {
             float3 n;
             float err, lb;
-            bool isFace, flipped;
-            if (!axis_dir(c, S, idx, D, delta, rinSum, n, err, lb, isFace, pass == 1, &flipped) || lb > lbHi)
-                continue;
-            const float d = isFace ? face_axis_depth(c, S, idx, rel, n, flipped) : axis_depth(c, S, rel, n);
+            bool isFace;
+            if (!axis_dir(c, S, idx, D, delta, rinSum, n, err, lb, isFace, pass == 1) || lb > lbHi) continue;
+            const float d = axis_depth(c, S, rel, n);
             if (isFace) {
                 sepMin = fminf(sepMin, d);
                 if (fabsf(d) <= delta) {

@@ -70,7 +70,7 @@ int dalloc(T*& p, size_t count) {
 void free_all(b3::DevBuffers& d) {
     void* ptrs[] = {d.pos, d.quat, d.linVel, d.angVel, d.invMass, d.friction, d.restitution,
                     d.invInertia, d.collidable, d.worldId, d.cols, d.polys, d.verts, d.faces,
-                    d.indices, d.edges, d.localAabb, d.polyInradius, d.faceExt, d.childShapes, d.subPairs, d.subCount, d.subOffset, d.aabbMin, d.aabbMax, d.smallSlot,
+                    d.indices, d.edges, d.localAabb, d.polyInradius, d.childShapes, d.subPairs, d.subCount, d.subOffset, d.aabbMin, d.aabbMax, d.smallSlot,
                     d.largeStart, d.largeList, d.sapSmall, d.sapLarge, d.sapSorted, d.sapCount, d.sapOffset, d.keys, d.vals, d.keysAlt, d.valsAlt, d.cellTable,
                     d.pairs, d.contacts, d.manifoldFlag, d.pairSep, d.npFast, d.npSlow, d.npCand, d.manifoldScan,
                     d.manifoldPair,
@@ -140,7 +140,6 @@ b3::ShapesDev b3World_t::shapesDev() const {
     S.edges = d.edges;
     S.localAabb = d.localAabb;
     S.inradius = d.polyInradius;
-    S.faceExt = d.faceExt;
     S.children = d.childShapes;
     S.numPolys = (int)polys.size();
     S.numVerts = (int)verts4.size() / 4;
@@ -298,20 +297,6 @@ extern "C" int b3_register_convex_hull(b3World w, const float* vertices, int num
         ff.pad[0] = off <= 1e-6 * mag ? 1 : 0;
         for (int id : f.indices) w->indices.push_back(id);
         w->faces.push_back(ff);
-        // the hull's extent along the face normal: every face axis of this
-        // hull needs only the other hull's projection (rounded outward)
-        double lo = 1e300, hi = -1e300;
-        for (int i = 0; i < (int)P.vertices.size() / 3; ++i) {
-            const double d = (double)ff.plane[0] * P.vertices[3 * i] + (double)ff.plane[1] * P.vertices[3 * i + 1] +
-                             (double)ff.plane[2] * P.vertices[3 * i + 2];
-            lo = std::min(lo, d);
-            hi = std::max(hi, d);
-        }
-        float flo = (float)lo, fhi = (float)hi;
-        if ((double)flo > lo) flo = std::nextafter(flo, -1e30f);
-        if ((double)fhi < hi) fhi = std::nextafter(fhi, 1e30f);
-        w->faceExt.push_back(flo);
-        w->faceExt.push_back(fhi);
     }
     poly.numUniqueEdges = (int)P.uniqueEdges.size() / 3;
     poly.uniqueEdgesOffset = (int)w->edges4.size() / 4;
@@ -372,8 +357,6 @@ extern "C" int b3_register_plane(b3World w, const float normal[3], float planeCo
     f.plane[3] = planeConstant;
     const int face = (int)w->faces.size();
     w->faces.push_back(f);
-    w->faceExt.push_back(0.f);
-    w->faceExt.push_back(0.f);
     const float mn[3] = {-1e30f, -1e30f, -1e30f}, mx[3] = {1e30f, 1e30f, 1e30f};
     *collidableOut = add_collidable(w, B3_SHAPE_PLANE, face, planeConstant, 0, mn, mx);
     ++w->numPlanes;
@@ -470,8 +453,6 @@ extern "C" int b3_register_concave_mesh(b3World w, const float* vertices3, int n
         f.pad[0] = 1;
         for (int k = 0; k < 3; ++k) w->indices.push_back(indices[3 * t + k]);
         w->faces.push_back(f);
-        w->faceExt.push_back(0.f);
-        w->faceExt.push_back(0.f);
     }
     const int meshPoly = (int)w->polys.size();
     mesh.unused = meshPoly + 1;  // the first triangle polytope
@@ -517,17 +498,6 @@ extern "C" int b3_register_concave_mesh(b3World w, const float* vertices3, int n
             f.pad[0] = 1;
             for (int id : ids) w->indices.push_back(id);
             w->faces.push_back(f);
-            double lo = 1e300, hi = -1e300;
-            for (int i = 0; i < 3; ++i) {
-                const double d = (double)pl[0] * tv[i][0] + (double)pl[1] * tv[i][1] + (double)pl[2] * tv[i][2];
-                lo = std::min(lo, d);
-                hi = std::max(hi, d);
-            }
-            float flo = (float)lo, fhi = (float)hi;
-            if ((double)flo > lo) flo = std::nextafter(flo, -1e30f);
-            if ((double)fhi < hi) fhi = std::nextafter(fhi, 1e30f);
-            w->faceExt.push_back(flo);
-            w->faceExt.push_back(fhi);
         };
         const float front[4] = {n[0], n[1], n[2], triPlane[t][3]};
         add_face(front, {0, 1, 2});
@@ -760,7 +730,6 @@ static int upload_shapes(b3World w, cudaStream_t st) {
     B3_TRY(dalloc(d.edges, w->edges4.size() / 4 + 1));
     B3_TRY(dalloc(d.localAabb, w->localAabb8.size() / 4));
     B3_TRY(dalloc(d.polyInradius, w->polyInradius.size()));
-    B3_TRY(dalloc(d.faceExt, w->faceExt.size() / 2));
     B3_CUDA(cudaMemcpyAsync(d.cols, w->cols.data(), sizeof(b3Collidable) * w->cols.size(), cudaMemcpyHostToDevice, st));
     B3_CUDA(cudaMemcpyAsync(d.polys, w->polys.data(), sizeof(b3ConvexPolyhedron) * w->polys.size(), cudaMemcpyHostToDevice, st));
     B3_CUDA(cudaMemcpyAsync(d.verts, w->verts4.data(), sizeof(float) * w->verts4.size(), cudaMemcpyHostToDevice, st));
@@ -771,9 +740,6 @@ static int upload_shapes(b3World w, cudaStream_t st) {
     B3_CUDA(cudaMemcpyAsync(d.localAabb, w->localAabb8.data(), sizeof(float) * w->localAabb8.size(), cudaMemcpyHostToDevice, st));
     B3_CUDA(cudaMemcpyAsync(d.polyInradius, w->polyInradius.data(), sizeof(float) * w->polyInradius.size(),
                             cudaMemcpyHostToDevice, st));
-    if (!w->faceExt.empty())
-        B3_CUDA(cudaMemcpyAsync(d.faceExt, w->faceExt.data(), sizeof(float) * w->faceExt.size(),
-                                cudaMemcpyHostToDevice, st));
     B3_TRY(dalloc(d.childShapes, w->childShapes.size()));
     if (!w->childShapes.empty())
         B3_CUDA(cudaMemcpyAsync(d.childShapes, w->childShapes.data(), sizeof(b3ChildShape) * w->childShapes.size(),
@@ -1250,10 +1216,12 @@ extern "C" int b3_get_contacts(b3World w, b3Contact4* out, int max, int* count, 
     if (!w || !count) return B3_ERR_INVALID_ARG;
     if (!w->written) return B3_ERR_STATE;
     cudaStream_t st = as_stream(stream);
-    int32_t s[3] = {0, 0, 0};
-    B3_CUDA(cudaMemcpyAsync(s, w->d.scalars + b3::S_NUM_PAIRS, 12, cudaMemcpyDeviceToHost, st));
+    int32_t s[b3::S_NUM_SCALARS] = {};
+    B3_CUDA(cudaMemcpyAsync(s, w->d.scalars, sizeof(s), cudaMemcpyDeviceToHost, st));
     B3_CUDA(cudaStreamSynchronize(st));
-    const int np = s[0], nm = s[1];
+    // manifold slots: the pairs', then the sub-pairs' of compound and mesh pairs
+    const int np = w->hasSubPairs() ? s[b3::S_NUM_SLOTS] : s[b3::S_NUM_PAIRS];
+    const int nm = s[b3::S_NUM_MANIFOLDS];
     *count = nm;
     if (!out || nm <= 0 || max <= 0) return B3_OK;
     std::vector<uint32_t> flag(np);

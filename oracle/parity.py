@@ -47,6 +47,45 @@ def _contact_errors(gc, oc):
     return same_set, same_counts, worst_p, worst_n
 
 
+def manifold_differences(gc, oc, limit=20):
+    """The manifolds (by pair slot) where the device and the oracle differ:
+    present on one side only, other point counts or bodies, or points or
+    normal beyond the bars. Each entry holds the slot, the kind and both
+    records (bodies, normal with its count in w, points with depth in w)."""
+    gi = {int(p): k for k, p in enumerate(gc["pairIndex"])}
+    oi = {int(p): k for k, p in enumerate(oc["pairIndex"])}
+
+    def rec(c, k):
+        if k is None:
+            return None
+        n = int(c["normal"][k, 3])
+        return {"bodies": [int(c["bodyA"][k]), int(c["bodyB"][k])], "normal": c["normal"][k].tolist(),
+                "points": c["pos"][k][:n].tolist()}
+
+    out = []
+    for p in sorted(set(gi) | set(oi)):
+        kg, ko = gi.get(p), oi.get(p)
+        kind = None
+        if kg is None:
+            kind = "oracle only"
+        elif ko is None:
+            kind = "device only"
+        else:
+            ng, no = int(gc["normal"][kg, 3]), int(oc["normal"][ko, 3])
+            if ng != no or gc["bodyA"][kg] != oc["bodyA"][ko] or gc["bodyB"][kg] != oc["bodyB"][ko]:
+                kind = "counts or bodies"
+            else:
+                dp = float(np.abs(gc["pos"][kg][:ng] - oc["pos"][ko][:ng]).max()) if ng else 0.0
+                dn = float(np.abs(gc["normal"][kg, :3] - oc["normal"][ko, :3]).max())
+                if dp > POS_TOL or dn > NRM_TOL:
+                    kind = "points %.3g m, normal %.3g" % (dp, dn)
+        if kind:
+            out.append({"slot": p, "kind": kind, "device": rec(gc, kg), "oracle": rec(oc, ko)})
+            if len(out) >= limit:
+                break
+    return out
+
+
 def _state_errors(a, b, sel):
     return {"pos_err_m": float(np.abs(a[0][sel, :3] - b[0][sel, :3]).max()),
             "lin_vel_err_mps": float(np.abs(a[2][sel, :3] - b[2][sel, :3]).max()),
@@ -94,6 +133,7 @@ def one_step_report(w, o, dynamic=None, make_oracle=None):
     same_set, same_counts, wp, wn = _contact_errors(gc, oc)
     rep["manifolds"] = int(len(gc["normal"]))
     rep["manifold_set_equal"] = same_set and same_counts
+    rep["manifold_differences"] = manifold_differences(gc, oc)
     rep["contact_point_err_m"] = wp
     rep["normal_err"] = wn
     w.stage("solve")
