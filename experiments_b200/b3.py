@@ -23,6 +23,8 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "libb3gpu.so")
 B3_WORLD_SAP_BROADPHASE = 1  # b3WorldConfig.flags: sweep-and-prune broadphase
+BULLET_KEEP_STATIC_OBJECTS = 1  # b3_load_bullet_file_ex flags (B3_BULLET_*)
+BULLET_SPHERES_AND_PLANES = 2
 B3_WORLD_BATCHED_GS_SOLVER = 2  # b3WorldConfig.flags: the reference GPU solver (batched Gauss-Seidel)
 
 B3_OK = 0
@@ -169,6 +171,7 @@ SIGNATURES = [
     ("b3_solver_solve_jacobi", _I, [_P, _P]),
     ("b3_solver_solve_batched_gs", _I, [_P, _P]),
     ("b3_load_bullet_file", _I, [_P, C.c_char_p, _I, _IP]),
+    ("b3_load_bullet_file_ex", _I, [_P, C.c_char_p, _I, _IP]),
     ("b3_get_gs_batches", _I, [_P, _IP, _I, _IP, _P]),
     ("b3_get_gs_constraints", _I, [_P, C.POINTER(Constraint4), _I, _IP, _P]),
     ("b3_integrate", _I, [_P, _P]),
@@ -634,13 +637,20 @@ class PhysicsWorld:
         _check(self.lib.b3_sap_broadphase_calculate_overlapping_pairs(self.h, _stream(stream)),
                "b3_sap_broadphase_calculate_overlapping_pairs")
 
-    def load_bullet_file(self, path, keep_static_objects=False):
+    def load_bullet_file(self, path, keep_static_objects=False, spheres_and_planes=False):
         """btBulletDataExtractor::convertAllObjects on a .bullet scene file:
         registers its box and convex-hull shapes and its rigid bodies (see
-        b3_load_bullet_file); returns the number of bodies added."""
+        b3_load_bullet_file); with spheres_and_planes also its sphere and
+        static plane shapes (b3_load_bullet_file_ex,
+        B3_BULLET_SPHERES_AND_PLANES). Returns the number of bodies added."""
         n = C.c_int()
-        _check(self.lib.b3_load_bullet_file(self.h, os.fsencode(path), 1 if keep_static_objects else 0, C.byref(n)),
-               "b3_load_bullet_file")
+        if spheres_and_planes:
+            flags = BULLET_SPHERES_AND_PLANES | (BULLET_KEEP_STATIC_OBJECTS if keep_static_objects else 0)
+            _check(self.lib.b3_load_bullet_file_ex(self.h, os.fsencode(path), flags, C.byref(n)),
+                   "b3_load_bullet_file_ex")
+        else:
+            _check(self.lib.b3_load_bullet_file(self.h, os.fsencode(path), 1 if keep_static_objects else 0,
+                                                C.byref(n)), "b3_load_bullet_file")
         total = C.c_int()
         _check(self.lib.b3_get_num_bodies(self.h, C.byref(total)), "b3_get_num_bodies")
         self.n = total.value

@@ -314,13 +314,18 @@ void basis_to_quat(const double r[3][3], float q[4]) {
 // (P2/BulletDataExtractor.cpp:529-577)
 constexpr int kBoxShape = 0;
 constexpr int kConvexHullShape = 4;
+constexpr int kSphereShape = 8;
+constexpr int kStaticPlaneShape = 28;
 // most points a convex hull record of a file may hold
 constexpr int64_t kMaxFileHullPoints = 1 << 16;
 
 // A shape or body of the file, read and checked before anything registers.
 struct ShapeRec {
     uint64_t oldPtr;
-    std::vector<float> points;  // xyz triples, final scale applied
+    int kind = 0;               // 0 convex hull, 1 sphere, 2 static plane
+    std::vector<float> points;  // hull: xyz triples, final scale applied
+    float radius = 0.f;         // sphere
+    float plane[4] = {};        // static plane: normal, constant
 };
 struct BodyRec {
     int shape;  // index into the shape records
@@ -330,7 +335,14 @@ struct BodyRec {
 }  // namespace
 
 extern "C" int b3_load_bullet_file(b3World w, const char* path, int keepStaticObjects, int* numBodiesOut) {
+    return b3_load_bullet_file_ex(w, path, keepStaticObjects ? B3_BULLET_KEEP_STATIC_OBJECTS : 0, numBodiesOut);
+}
+
+extern "C" int b3_load_bullet_file_ex(b3World w, const char* path, int flags, int* numBodiesOut) {
     if (!w || !path) return B3_ERR_INVALID_ARG;
+    if (flags & ~(B3_BULLET_KEEP_STATIC_OBJECTS | B3_BULLET_SPHERES_AND_PLANES)) return B3_ERR_INVALID_ARG;
+    const bool keepStaticObjects = (flags & B3_BULLET_KEEP_STATIC_OBJECTS) != 0;
+    const bool spheresPlanes = (flags & B3_BULLET_SPHERES_AND_PLANES) != 0;
     File F;
     std::string err;
     if (!read_file(path, F, err)) {
@@ -340,7 +352,10 @@ extern "C" int b3_load_bullet_file(b3World w, const char* path, int keepStaticOb
     // Pass 1 reads and checks every record; nothing is registered unless
     // the whole file is usable, so a failed load leaves the world as it was.
     // Shapes in file order (convertCollisionShape :723-840): boxes and
-    // convex hulls; spheres, planes and the rest are skipped, as there.
+    // convex hulls; spheres, planes and the rest are skipped, as there
+    // (createSphereShape and createPlaneShape return -1, :999-1010), unless
+    // B3_BULLET_SPHERES_AND_PLANES asks for this library's sphere and plane
+    // shapes.
     std::vector<ShapeRec> shapes;
     for (const Chunk& c : F.chunks) {
         if (c.code != code4("SHAP")) continue;
@@ -352,6 +367,33 @@ extern "C" int b3_load_bullet_file(b3World w, const char* path, int keepStaticOb
         for (int k = 0; k < 3; ++k) scale[k] = F.f32(c, (in + "m_localScaling.m_floats").c_str(), k);
         ShapeRec r;
         r.oldPtr = c.oldPtr;
+        if (spheresPlanes && stype == kSphereShape && !hull) {
+            // btSphereShape: radius = implicitShapeDimensions.x * localScaling.x
+            if (!F.has(c, "m_implicitShapeDimensions")) continue;
+            r.kind = 1;
+            r.radius = F.f32(c, "m_implicitShapeDimensions.m_floats", 0) * scale[0];
+            if (!(r.radius > 0.f) || !std::isfinite(r.radius)) {
+                b3_set_error("%s: sphere of radius %g", path, (double)r.radius);
+                return B3_ERR_INVALID_ARG;
+            }
+            shapes.push_back(std::move(r));
+            continue;
+        }
+        if (spheresPlanes && stype == kStaticPlaneShape && !hull) {
+            // btStaticPlaneShape: the plane n . x = constant (its local
+            // scaling changes only its bounding box)
+            if (!F.has(c, "m_planeNormal") || !F.has(c, "m_planeConstant")) continue;
+            r.kind = 2;
+            for (int k = 0; k < 3; ++k) r.plane[k] = F.f32(c, "m_planeNormal.m_floats", k);
+            r.plane[3] = F.f32(c, "m_planeConstant");
+            const float len2 = r.plane[0] * r.plane[0] + r.plane[1] * r.plane[1] + r.plane[2] * r.plane[2];
+            if (!(len2 > 0.f) || !std::isfinite(len2) || !std::isfinite(r.plane[3])) {
+                b3_set_error("%s: static plane without a normal", path);
+                return B3_ERR_INVALID_ARG;
+            }
+            shapes.push_back(std::move(r));
+            continue;
+        }
         if (stype == kBoxShape && !hull) {
             // createBoxShape (:969-997): the unit cube scaled by
             // halfDimensions * localScaling + margin
@@ -429,8 +471,11 @@ extern "C" int b3_load_bullet_file(b3World w, const char* path, int keepStaticOb
     std::vector<int> shapeCol(shapes.size(), -1);
     const float unit[3] = {1.f, 1.f, 1.f};
     for (size_t g = 0; g < shapes.size(); ++g) {
-        const int rc = b3_register_convex_hull(w, shapes[g].points.data(), (int)(shapes[g].points.size() / 3), 12,
-                                               unit, &shapeCol[g]);
+        const ShapeRec& r = shapes[g];
+        int rc;
+        if (r.kind == 1) rc = b3_register_sphere(w, r.radius, &shapeCol[g]);
+        else if (r.kind == 2) rc = b3_register_plane(w, r.plane, r.plane[3], &shapeCol[g]);
+        else rc = b3_register_convex_hull(w, r.points.data(), (int)(r.points.size() / 3), 12, unit, &shapeCol[g]);
         if (rc != B3_OK) return rc;
     }
     int count = 0;

@@ -433,6 +433,22 @@ int b3_register_body(b3World w, float mass, const float position[3], const float
  * the world as it was. */
 int b3_load_bullet_file(b3World w, const char* path, int keepStaticObjects, int* numBodiesOut);
 
+/* Flags of b3_load_bullet_file_ex. */
+enum {
+    B3_BULLET_KEEP_STATIC_OBJECTS = 1, /* keepStaticObjects of b3_load_bullet_file */
+    /* also convert sphere shapes (radius = implicitShapeDimensions.x *
+     * localScaling.x) and static plane shapes (n . x = constant) into this
+     * library's sphere and plane shapes, where the reference's extractor
+     * skips them (createSphereShape / createPlaneShape return -1,
+     * P2/BulletDataExtractor.cpp:999-1010); their bodies register like the
+     * others. A plane body is static, so it is kept only with
+     * B3_BULLET_KEEP_STATIC_OBJECTS. */
+    B3_BULLET_SPHERES_AND_PLANES = 2
+};
+/* b3_load_bullet_file with flags (B3_BULLET_*); flags 0 or
+ * B3_BULLET_KEEP_STATIC_OBJECTS give exactly b3_load_bullet_file. */
+int b3_load_bullet_file_ex(b3World w, const char* path, int flags, int* numBodiesOut);
+
 /* Bulk form of b3_register_body for n bodies (arrays of n, xyz / xyzw
  * packed); writes the id of the first new body. */
 int b3_register_bodies(b3World w, int n, const float* masses, const float* positions3,

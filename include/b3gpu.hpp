@@ -173,6 +173,14 @@ public:
         check(b3_load_bullet_file(h_, path, keepStaticObjects ? 1 : 0, &n), "loadBulletFile");
         return n;
     }
+    /* The same with B3_BULLET_* flags (b3_load_bullet_file_ex): e.g. with
+     * B3_BULLET_SPHERES_AND_PLANES the file's spheres and static planes
+     * register too. */
+    int loadBulletFileFlags(const char* path, int flags) {
+        int n = 0;
+        check(b3_load_bullet_file_ex(h_, path, flags, &n), "loadBulletFileFlags");
+        return n;
+    }
     int registerConvexPolyhedron(const float* vertices, int numVertices, int strideBytes = 16,
                                  const float* scaling3 = nullptr) {
         int c = -1;

@@ -133,6 +133,18 @@ def bullet_lib():
     return _bullet
 
 
+def _bullet_points(shape):
+    """A scene shape as the shim's point list: hull points, one point
+    (radius, 0, 0) for a sphere, two (normal; constant, 0, 0) for a plane."""
+    if isinstance(shape, dict):
+        if shape["kind"] == "sphere":
+            return np.array([[shape["radius"], 0.0, 0.0]], np.float32)
+        if shape["kind"] == "plane":
+            return np.array([shape["normal"], [shape["constant"], 0.0, 0.0]], np.float32)
+        raise NotImplementedError(f"{shape['kind']} shapes in the reference CPU pipeline")
+    return np.asarray(shape, np.float32).reshape(-1, 3)
+
+
 class ReferenceCpuWorld:
     """A scene in the reference's CPU pipeline (btDiscreteDynamicsWorld:
     btDbvtBroadphase + btSequentialImpulseConstraintSolver, 10 iterations);
@@ -145,7 +157,7 @@ class ReferenceCpuWorld:
             raise RuntimeError("oracle/_ref/libb3bullet.so not built")
         self.B = B
         self.n = scene.n
-        pts = [np.asarray(v, np.float32).reshape(-1, 3) for v in scene.shapes]
+        pts = [_bullet_points(v) for v in scene.shapes]
         offs = np.zeros(len(pts) + 1, np.int32)
         offs[1:] = np.cumsum([len(p) for p in pts])
         allp = np.ascontiguousarray(np.concatenate(pts).astype(np.float32))

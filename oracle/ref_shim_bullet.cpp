@@ -32,7 +32,11 @@ struct RefScene {
 };
 
 // An axis-aligned box given by its 8 corner points becomes a btBoxShape.
+// One point (r, 0, 0) is a btSphereShape of radius r; two points (normal,
+// then (constant, 0, 0)) a btStaticPlaneShape n . x = constant.
 btCollisionShape* make_shape(const float* p, int n) {
+    if (n == 1) return new btSphereShape(p[0]);
+    if (n == 2) return new btStaticPlaneShape(btVector3(p[0], p[1], p[2]), p[3]);
     if (n == 8) {
         float lo[3] = {p[0], p[1], p[2]}, hi[3] = {p[0], p[1], p[2]};
         for (int i = 1; i < 8; ++i)

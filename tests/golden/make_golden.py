@@ -54,6 +54,12 @@ pile.bullet, pile_bullet.npz
     keeps the scene it was made from (positions, orientations, masses,
     shape of each body and the shapes' points).
 
+spheres.bullet, spheres_bullet.npz
+    The same writer on 24 spheres (spheres_on_plane seed 84: radii
+    U(0.2, 0.5), btSphereShape) above a static plane y = 0
+    (btStaticPlaneShape); the npz keeps each body's position, orientation,
+    mass and radius and the plane.
+
 hull_pins.npz
     btConvexUtility::initializePolyhedralFeatures
     (P1/btConvexUtility.cpp:31-270) on every distinct shape of the plain and
@@ -377,6 +383,25 @@ def make_bullet_scene():
     return sc.n
 
 
+def make_bullet_spheres():
+    """spheres.bullet: 24 spheres on a static plane written by the
+    reference's serializer (btSphereShape, btStaticPlaneShape)."""
+    _import_tests()
+    import oracle
+    from experiments_b200 import scenes
+    sc = scenes.spheres_on_plane(84, n=24)
+    ref = oracle.ReferenceCpuWorld(sc)
+    ref.write_bullet(os.path.join(HERE, "spheres.bullet"))
+    ref.close()
+    radius = np.array([sc.shapes[k]["radius"] if sc.shapes[k]["kind"] == "sphere" else 0.0 for k in sc.shape],
+                      np.float32)
+    rec = dict(pos=np.asarray(sc.pos, np.float32), quat=np.asarray(sc.quat, np.float32),
+               mass=np.asarray(sc.mass, np.float32), shape=np.asarray(sc.shape, np.int32), radius=radius,
+               plane=np.array(list(sc.shapes[0]["normal"]) + [sc.shapes[0]["constant"]], np.float32))
+    np.savez_compressed(os.path.join(HERE, "spheres_bullet.npz"), **rec)
+    return sc.n
+
+
 def make_hulls():
     _import_tests()
     import test_cpu_pins as pins
@@ -408,3 +433,4 @@ if __name__ == "__main__":
     r = make_gs()
     print("gs_solve_args.npz:", len(r["batchIdx"]), "constraints")
     print("pile.bullet:", make_bullet_scene(), "bodies")
+    print("spheres.bullet:", make_bullet_spheres(), "bodies")

@@ -177,3 +177,83 @@ def test_a_file_that_does_not_fit_registers_nothing(host_ctx):
         w.load_bullet_file(FILE, keep_static_objects=True)
     assert w.n == 0 and w.shapes()["counts"][:2] == (0, 0)
     w.close()
+
+
+SPHERES = os.path.join(GOLDEN, "spheres.bullet")
+
+
+def test_spheres_and_planes_are_skipped_as_in_the_reference(host_ctx):
+    """The reference's extractor skips sphere and plane shapes
+    (createSphereShape / createPlaneShape return -1), and so does the
+    default load: of the spheres-on-a-plane file only the replacement
+    ground registers."""
+    w = _world(host_ctx, 2600)
+    assert w.load_bullet_file(SPHERES) == 2500
+    w.close()
+
+
+@pytest.mark.parametrize("keep_static", [True, False])
+def test_spheres_and_planes_load_on_request(host_ctx, keep_static):
+    """With B3_BULLET_SPHERES_AND_PLANES every sphere registers as a sphere
+    of its radius (implicit dimension x times scaling x) at its position and
+    mass; the static plane body registers with keepStaticObjects."""
+    g = np.load(os.path.join(GOLDEN, "spheres_bullet.npz"))
+    n = len(g["mass"])
+    dyn = g["mass"] > 0
+    w = _world(host_ctx, n + 2600)
+    added = w.load_bullet_file(SPHERES, keep_static_objects=keep_static, spheres_and_planes=True)
+    assert added == (n if keep_static else int(dyn.sum()) + 2500) == w.n
+    bodies = w.read_bodies()
+    cols = w.shapes()["cols"]
+    spheres = planes = 0
+    for i in range(w.n):
+        b = bodies[i]
+        c = cols[int(b.collidableIdx)]
+        if c.shapeType == 7:  # sphere
+            p = np.array(b.pos[:3])
+            j = int(np.argmin(np.linalg.norm(g["pos"] - p, axis=1)))
+            assert np.abs(g["pos"][j] - p).max() == 0.0
+            assert c.radius == pytest.approx(float(g["radius"][j]), rel=1e-6)
+            assert 1.0 / b.invMass == pytest.approx(float(g["mass"][j]), rel=2e-6)
+            spheres += 1
+        elif c.shapeType == 4:  # plane
+            assert b.invMass == 0 and c.radius == pytest.approx(float(g["plane"][3]))
+            face = w.shapes()["faces"][int(c.shapeIndex)]
+            assert np.allclose(np.array(face.plane[:3]), g["plane"][:3])
+            planes += 1
+    assert spheres == int(dyn.sum())
+    assert planes == (1 if keep_static else 0)
+    w.close()
+
+
+def test_spheres_fixture_is_the_seeded_scene():
+    g = np.load(os.path.join(GOLDEN, "spheres_bullet.npz"))
+    sc = scenes.spheres_on_plane(84, n=24)
+    assert np.array_equal(np.asarray(sc.pos, np.float32), g["pos"])
+    assert np.array_equal(np.asarray(sc.mass, np.float32), g["mass"])
+
+
+@pytest.mark.gpu
+def test_loaded_spheres_rest_on_the_plane(ctx):
+    """The spheres-on-a-plane file loaded with its spheres and plane steps
+    on the device: no sphere passes through the plane, nearly all of them
+    come to rest on it (a few may rest on others) and everything is still."""
+    g = np.load(os.path.join(GOLDEN, "spheres_bullet.npz"))
+    w = b3.PhysicsWorld(ctx, scenes.world_config(scenes.spheres_on_plane(84, n=24)))
+    w.load_bullet_file(SPHERES, keep_static_objects=True, spheres_and_planes=True)
+    w.writeBodiesToGpu()
+    w.stepSimulation(300)
+    pos, _, lin, _ = w.read_state()
+    bodies = w.read_bodies()
+    cols = w.shapes()["cols"]
+    on_plane = 0
+    for i in range(w.n):
+        if bodies[i].invMass == 0:
+            continue
+        r = cols[int(bodies[i].collidableIdx)].radius
+        assert pos[i, 1] > r - 0.03
+        on_plane += abs(pos[i, 1] - r) < 0.03
+    assert on_plane >= 0.8 * (w.n - 1)
+    assert np.abs(lin[[b.invMass != 0 for b in bodies], :3]).max() < 0.1
+    assert w.counters()["timeouts"] == 0
+    w.close()
