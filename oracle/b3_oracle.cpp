@@ -648,6 +648,12 @@ int clip_hull_hull(const or_world* w, V sep, const or_poly& hA, const or_poly& h
     if (closestA < 0) return 0;
     const or_face& fa = w->faces[hA.faceOffset + closestA];
     const int nvA = fa.numIndices;
+    // A reference face of two vertices (a mesh triangle's edge plane,
+    // sat.cl:1083-1105) has two side planes that are one plane with opposite
+    // orientations; clipFace keeps only points strictly inside (ds < 0), so
+    // in exact arithmetic nothing is kept. The reference's FP32 outcome
+    // there is rounding noise; the exact result is taken.
+    if (nvA < 3) return 0;
     const V nA = V(fa.plane[0], fa.plane[1], fa.plane[2]);
     const V nAw = qrot(A.q, nA);
     for (int e0 = 0; e0 < nvA; ++e0) {

