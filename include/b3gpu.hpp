@@ -188,6 +188,37 @@ public:
               "registerConvexPolyhedron");
         return c;
     }
+    /* CLPhysicsDemo::registerSphereShape / registerPlaneShape /
+     * registerCompoundShape / registerConcaveMesh: return the collidable
+     * id (b3_register_sphere, _plane, _compound, _concave_mesh). */
+    int registerSphereShape(float radius) {
+        int c = -1;
+        check(b3_register_sphere(h_, radius, &c), "registerSphereShape");
+        return c;
+    }
+    int registerPlaneShape(const float* normal3, float planeConstant) {
+        int c = -1;
+        check(b3_register_plane(h_, normal3, planeConstant, &c), "registerPlaneShape");
+        return c;
+    }
+    int registerCompoundShape(const b3ChildShape* children, int numChildren) {
+        int c = -1;
+        check(b3_register_compound(h_, children, numChildren, &c), "registerCompoundShape");
+        return c;
+    }
+    int registerConcaveMesh(const float* vertices3, int numVertices, const int* indices, int numIndices,
+                            const float* scaling3 = nullptr) {
+        const float one[3] = {1.f, 1.f, 1.f};
+        int c = -1;
+        check(b3_register_concave_mesh(h_, vertices3, numVertices, indices, numIndices, scaling3 ? scaling3 : one,
+                                       &c),
+              "registerConcaveMesh");
+        return c;
+    }
+    /* Bounded waits of the persistent solve (b3_set_wait_limits). */
+    void setWaitLimits(int spinLimit, int holdMicros = 0) {
+        check(b3_set_wait_limits(h_, spinLimit, holdMicros), "setWaitLimits");
+    }
     /* CLPhysicsDemo::registerPhysicsInstance: mass 0 = static. */
     int registerPhysicsInstance(float mass, const float* position3, const float* orientation4, int collidable,
                                 float friction = 0.6f, float restitution = 0.f, int worldId = 0) {

@@ -65,6 +65,33 @@ static int host_mode(const char* bulletFile) {
         b3::World wf(ctx, cfg);
         EXPECT(wf.loadBulletFile(bulletFile, true) == 41 && wf.numBodies() == 41);
     }
+    {
+        // the other shape kinds: sphere, plane, a compound of two cubes, a
+        // two-triangle mesh; each is a collidable of its reference shape type
+        b3::World ws(ctx, stack_config());
+        const float one[3] = {1.f, 1.f, 1.f};
+        const int cube = ws.registerConvexPolyhedron(&kCube[0][0], 8, 16, one);
+        const int sphere = ws.registerSphereShape(0.5f);
+        const float up[3] = {0.f, 1.f, 0.f};
+        const int plane = ws.registerPlaneShape(up, 0.f);
+        b3ChildShape kids[2] = {};
+        kids[0].childPosition[0] = 0.55f;
+        kids[1].childPosition[0] = -0.55f;
+        kids[0].childOrientation[3] = kids[1].childOrientation[3] = 1.f;
+        kids[0].shapeIndex = kids[1].shapeIndex = cube;
+        const int compound = ws.registerCompoundShape(kids, 2);
+        const float sq[12] = {-5, 0, 5, 5, 0, 5, -5, 0, -5, 5, 0, -5};
+        const int tris[6] = {0, 1, 2, 2, 1, 3};
+        const int mesh = ws.registerConcaveMesh(sq, 4, tris, 6);
+        std::vector<b3Collidable> cols(8);
+        EXPECT(b3_get_shapes(ws.handle(), cols.data(), nullptr, nullptr, nullptr, nullptr, nullptr, nullptr) == 0);
+        EXPECT(cols[sphere].shapeType == B3_SHAPE_SPHERE && cols[sphere].radius == 0.5f);
+        EXPECT(cols[plane].shapeType == B3_SHAPE_PLANE);
+        EXPECT(cols[compound].shapeType == B3_SHAPE_COMPOUND_OF_CONVEX_HULLS && cols[compound].numChildShapes == 2);
+        EXPECT(cols[mesh].shapeType == B3_SHAPE_CONCAVE_TRIMESH && cols[mesh].numChildShapes == 2);
+        ws.setWaitLimits(1000);
+        ws.setWaitLimits(0);
+    }
     b3::World w(ctx, stack_config());
     EXPECT(build_stack(w) == w.numBodies());
     b3::GpuNarrowphaseAndSolver np(w);
