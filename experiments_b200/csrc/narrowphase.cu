@@ -47,11 +47,13 @@ constexpr int kMaxPoly = 64;  // capacityWorldVerts (satClipHullContacts.cl:1027
 constexpr int kKeep = 4;      // near-minimum axis candidates kept per lane
 constexpr int kMaxCand = 32;  // candidates refined in float-float per pair
 constexpr int kPreChunk = 4;  // pairs per work grab of the sweep and the clip, prefetched by lanes
-// shared memory of one sweep warp: the prefetched chunk, the candidates and
-// the queue of edge axes that pass the lower bound (64 directions with
-// their errors, 64 indices)
-constexpr int kSweepWarpSmem = 128 * kPreChunk + 4 * kMaxCand + 16 * 64 + 4 * 64;
+// shared memory of one sweep warp: the prefetched chunk and the candidates
+constexpr int kSweepWarpSmem = 128 * kPreChunk + 4 * kMaxCand;
 constexpr int kNone = 0x7fffffff;
+// clip faces whose products with the axis differ by no more than this are
+// tied (the lowest index wins), in the device's float-float ranking and in
+// the oracle's FP64 one alike
+constexpr float kFaceTieTol = 1e-10f;
 // pairSep[p].w: how the pair reached the exact stage
 // pairSep[p].w: how the pair reached the exact stage
 constexpr int kSepRefine = 0;      // near-minimum axes: float-float re-ranking
@@ -319,8 +321,8 @@ __device__ __noinline__ bool axis_ff(const PairCtx& c, const b3::ShapesDev& S, c
 // FP32 part: 0 = separated (or no axis), 1 = decided in FP32 (sepf),
 // 2 = near-minimum candidates left in W.cand[0..count) for float-float.
 template <bool kEarlyFaces>
-__device__ __forceinline__ int sweep_axes(PairCtx& c, const b3::ShapesDev& S, int* cand, float4* qAxis, int* qIdx,
-                                          float3& sepf, int& count, int* ovfCounter) {
+__device__ __forceinline__ int sweep_axes(PairCtx& c, const b3::ShapesDev& S, int* cand, float3& sepf,
+                                          int& count, int* ovfCounter) {
     const int lane = threadIdx.x & 31;
     const b3ConvexPolyhedron& pa = *c.pa;
     const b3ConvexPolyhedron& pb = *c.pb;
@@ -407,97 +409,51 @@ __device__ __forceinline__ int sweep_axes(PairCtx& c, const b3::ShapesDev& S, in
     // 1e-4 m for their own rounding.
     float lbHi = FLT_MAX;
     const float rinSum = fmaxf(0.f, S.inradius[c.pa - S.polys] + S.inradius[c.pb - S.polys] - 1e-4f);
-    // One projected axis into the lane's state: the face-separation minimum
-    // and its ambiguous axes, the upper bound of the minimum depth, and the
-    // lane's sorted keep list of near-minimum lower bounds (each lane sees
-    // its axes in increasing index order, so ties keep the earlier axis).
-    auto take = [&](int idx, float d, float err, bool isFace) {
-        if (isFace) {
-            sepMin = fminf(sepMin, d);
-            if (fabsf(d) <= delta) {
-                if (amb[0] == kNone) amb[0] = idx;
-                else if (amb[1] == kNone) amb[1] = idx;
-                else ambOverflow = true;
-            }
-        }
-        upper = fminf(upper, d + err);
-        const float lo = d - err;  // lower bound of this axis' depth
-        if (!(lo < kd[kKeep - 1])) return;  // also drops NaN
-        float cd = lo;
-        int ci = idx;
-#pragma unroll
-        for (int k = 0; k < kKeep; ++k) {
-            if (cd < kd[k]) {
-                const float td = kd[k];
-                const int ti = ki[k];
-                kd[k] = cd;
-                ki[k] = ci;
-                cd = td;
-                ci = ti;
-            }
-        }
-    };
     // faces of A and B first; a separating face axis ends the search before
     // the edge pairs, as the reference returns early (P2/sat.cl:527-530)
-    for (int idx = lane; idx < nFace; idx += 32) {
-        float3 n;
-        float err, lb;
-        bool isFace;
-        axis_dir(c, S, idx, D, delta, rinSum, n, err, lb, isFace, false);
-        take(idx, axis_depth(c, S, rel, n), err, true);
-    }
-    {
-        float sm0 = sepMin;
-        int dz = 0;
-        warp_argmin(sm0, dz);
-        if (sm0 < -delta) return 0;
-        lbHi = warp_min(upper);
-    }
-    // Edge pairs: the lanes bound 32 axes at a time and queue those whose
-    // lower bound reaches lbHi (with direction and error) in the warp's
-    // queue; every 32 queued axes are projected by the whole warp, so the
-    // projections keep every lane busy however few axes pass the bound.
-    int qn = 0;
-    for (int base = nFace; base < nAxes; base += 32) {
-        const int idx = base + lane;
-        float3 n = make_float3(0.f, 0.f, 0.f);
-        float err = 0.f, lb = 0.f;
-        bool isFace;
-        const bool keep = idx < nAxes && axis_dir(c, S, idx, D, delta, rinSum, n, err, lb, isFace, true) &&
-                          !(lb > lbHi);
-        const unsigned m = __ballot_sync(0xffffffffu, keep);
-        if (keep) {
-            const int pos = qn + __popc(m & b3dev::lanemask_lt());
-            qAxis[pos] = make_float4(n.x, n.y, n.z, err);
-            qIdx[pos] = idx;
+    for (int pass = 0; pass < 2; ++pass) {
+        const int i0 = pass == 0 ? 0 : nFace;
+        const int i1 = pass == 0 ? nFace : nAxes;
+        for (int idx = i0 + lane; idx < i1; idx += 32) {
+            float3 n;
+            float err, lb;
+            bool isFace;
+            if (!axis_dir(c, S, idx, D, delta, rinSum, n, err, lb, isFace, pass == 1) || lb > lbHi) continue;
+            const float d = axis_depth(c, S, rel, n);
+            if (isFace) {
+                sepMin = fminf(sepMin, d);
+                if (fabsf(d) <= delta) {
+                    if (amb[0] == kNone) amb[0] = idx;
+                    else if (amb[1] == kNone) amb[1] = idx;
+                    else ambOverflow = true;
+                }
+            }
+            upper = fminf(upper, d + err);
+            const float lo = d - err;  // lower bound of this axis' depth
+            if (!(lo < kd[kKeep - 1])) continue;  // also drops NaN
+            // insertion into the lane's sorted keep list (indices increase)
+            float cd = lo;
+            int ci = idx;
+#pragma unroll
+            for (int k = 0; k < kKeep; ++k) {
+                if (cd < kd[k]) {
+                    const float td = kd[k];
+                    const int ti = ki[k];
+                    kd[k] = cd;
+                    ki[k] = ci;
+                    cd = td;
+                    ci = ti;
+                }
+            }
         }
-        qn += __popc(m);
-        if (qn >= 32) {
-            __syncwarp();
-            const float4 e = qAxis[lane];
-            take(qIdx[lane], axis_depth(c, S, rel, f3(e)), e.w, false);
-            const int rest = qn - 32;
-            float4 te;
-            int ti = 0;
-            if (lane < rest) {
-                te = qAxis[32 + lane];
-                ti = qIdx[32 + lane];
-            }
-            __syncwarp();
-            if (lane < rest) {
-                qAxis[lane] = te;
-                qIdx[lane] = ti;
-            }
-            __syncwarp();
-            qn = rest;
+        if (pass == 0) {
+            float sm0 = sepMin;
+            int dz = 0;
+            warp_argmin(sm0, dz);
+            if (sm0 < -delta) return 0;
+            lbHi = warp_min(upper);
         }
     }
-    __syncwarp();
-    if (lane < qn) {
-        const float4 e = qAxis[lane];
-        take(qIdx[lane], axis_depth(c, S, rel, f3(e)), e.w, false);
-    }
-    __syncwarp();
     // clearly separated by a face axis
     float sm = sepMin;
     int dummy = 0;
@@ -572,12 +528,8 @@ __device__ __forceinline__ int sweep_axes(PairCtx& c, const b3::ShapesDev& S, in
                  !(isFace && fabsf(d) <= delta) && fabsf(dot(D, n)) > 1e-5f * (len_ub(D) + 1e-3f);
             if (!ok) myIdx = kNone;
         }
-        // compared with the candidate of the lowest index (the candidates'
-        // order in the list depends on which lanes found them)
-        const unsigned lowIdx = __reduce_min_sync(0xffffffffu, lane < count ? (unsigned)cand[lane] : 0xffffffffu);
-        const int src0 = __ffs(__ballot_sync(0xffffffffu, lane < count && (unsigned)cand[lane] == lowIdx)) - 1;
-        const float3 n0 = make_float3(__shfl_sync(0xffffffffu, n.x, src0), __shfl_sync(0xffffffffu, n.y, src0),
-                                      __shfl_sync(0xffffffffu, n.z, src0));
+        const float3 n0 = make_float3(__shfl_sync(0xffffffffu, n.x, 0), __shfl_sync(0xffffffffu, n.y, 0),
+                                      __shfl_sync(0xffffffffu, n.z, 0));
         if (lane < count && ok) {
             const float3 dd = n - n0;
             if (fmaxf(fabsf(dd.x), fmaxf(fabsf(dd.y), fabsf(dd.z))) > 1e-5f) ok = false;
@@ -691,8 +643,7 @@ __device__ __noinline__ bool find_axis(PairCtx& c, const b3::ShapesDev& S, WarpS
                                        bool exact = false) {
     float3 sepf;
     int count = 0;
-    // the clip's side-plane buffers are free until the clip: the edge queue
-    const int r = sweep_axes<false>(c, S, W.cand, W.sideN, reinterpret_cast<int*>(W.sideP), sepf, count, ovfCounter);
+    const int r = sweep_axes<false>(c, S, W.cand, sepf, count, ovfCounter);
     if (r == 0) return false;
     if (r == 1 && !(exact && count >= 1)) {
         sep = mk3(sepf.x, sepf.y, sepf.z);
@@ -1164,7 +1115,20 @@ __device__ __noinline__ int select_face(const b3::ShapesDev& S, PairCtx& c, bool
         if (lt(d, rv)) { rv = d; ri = f; }
     }
     warp_argmin_ff(rv, ri);
-    return ri == kNone ? wi : ri;
+    if (ri == kNone) return wi;
+    // faces within kFaceTieTol of the extreme count as tied, and the lowest
+    // index wins: the reference's first extreme for faces tied in exact
+    // arithmetic, whose FP64 values differ only by rounding
+    int lowest = ri;
+    for (int f = lane; f < h.numFaces; f += 32) {
+        const float4 pl = __ldg((const float4*)&S.faces[h.faceOffset + f].plane[0]);
+        const float3 nl = make_float3(pl.x, pl.y, pl.z);
+        if (f >= lowest || !(sign * dot(mul(R, nl), sepf) <= lim)) continue;
+        ff d = dot3(mrot(F, nl), sep);
+        if (sign < 0.f) d = neg(d);
+        if (sub(d, rv).hi <= kFaceTieTol) lowest = f;
+    }
+    return (int)__reduce_min_sync(0xffffffffu, (unsigned)lowest);
 }
 
 // clipHullAgainstHull (satClipHullContacts.cl:556-611 + clipFaceAgainstHull
@@ -1508,8 +1472,6 @@ k_np_sweep(const int2* __restrict__ pairs, const int4* __restrict__ subs, const 
     unsigned char* wbase = np_smem + (size_t)(threadIdx.x >> 5) * kSweepWarpSmem;
     PairPre* pre = reinterpret_cast<PairPre*>(wbase);
     int* wcand = reinterpret_cast<int*>(wbase + sizeof(PairPre) * kPreChunk);
-    float4* wqAxis = reinterpret_cast<float4*>(wbase + sizeof(PairPre) * kPreChunk + 4 * kMaxCand);
-    int* wqIdx = reinterpret_cast<int*>(wqAxis + 64);
     const int numItems = kSub ? scalars[b3::S_NUM_SUB] : *numPairsDev;
     const int base = kSub ? *numPairsDev : 0;
     for (;;) {
@@ -1524,7 +1486,7 @@ k_np_sweep(const int2* __restrict__ pairs, const int4* __restrict__ subs, const 
             int r = 0, count = 0;
             float3 sepf = make_float3(0.f, 0.f, 0.f);
             if (pair_from_pre(c, pre[i], S))
-                r = sweep_axes<kEarlyFaces>(c, S, wcand, wqAxis, wqIdx, sepf, count, &counters->clipOverflow);
+                r = sweep_axes<kEarlyFaces>(c, S, wcand, sepf, count, &counters->clipOverflow);
             if (r == 0) {
                 if (lane == 0) manifoldFlag[p] = 0u;
             } else if (r == 1) {

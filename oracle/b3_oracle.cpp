@@ -602,21 +602,32 @@ int clip_face_pt(const std::vector<P4>& in, V pn, V a, std::vector<P4>& out) {
 }
 #endif
 
+constexpr double kFaceTieTol = 1e-10;
+
+// The face of h (posed b) with the smallest sign * (n . sep), ties within
+// kFaceTieTol to the lowest index; -1 for a hull without faces.
+int extreme_face(const or_world* w, const or_poly& h, const Body& b, V sep, double sign) {
+    std::vector<Real> d(h.numFaces);
+    Real best = std::numeric_limits<Real>::max();
+    for (int f = 0; f < h.numFaces; ++f) {
+        const or_face& fc = w->faces[h.faceOffset + f];
+        d[f] = (Real)sign * dot(qrot(b.q, V(fc.plane[0], fc.plane[1], fc.plane[2])), sep);
+        if (d[f] < best) best = d[f];
+    }
+    for (int f = 0; f < h.numFaces; ++f)
+        if (d[f] - best <= (Real)kFaceTieTol) return f;
+    return -1;
+}
+
 // clipHullAgainstHull (satClipHullContacts.cl:556-611 with clipFaceAgainstHull :353-452)
 int clip_hull_hull(const or_world* w, V sep, const or_poly& hA, const or_poly& hB, const Body& A, const Body& B,
                    Real minDist, Real maxDist, std::vector<P4>& out) {
     out.clear();
-    int closestB = -1;
-    Real dmax = -std::numeric_limits<Real>::max();
-    for (int f = 0; f < hB.numFaces; ++f) {
-        const or_face& fc = w->faces[hB.faceOffset + f];
-        const V n = qrot(B.q, V(fc.plane[0], fc.plane[1], fc.plane[2]));
-        const Real d = dot(n, sep);
-        if (d > dmax) {
-            dmax = d;
-            closestB = f;
-        }
-    }
+    // incident face of B: the largest n . sep; reference face of A: the
+    // smallest. Faces within kFaceTieTol of the extreme are tied and the
+    // lowest index wins, the reference's first extreme for faces tied in
+    // exact arithmetic (their FP64 products differ only by rounding).
+    const int closestB = extreme_face(w, hB, B, sep, -1.0);
     if (closestB < 0) return 0;
     std::vector<P4> in, tmp;
 #ifdef ORACLE_LOCAL_FRAME
@@ -634,17 +645,7 @@ int clip_hull_hull(const or_world* w, V sep, const or_poly& hA, const or_poly& h
             in.push_back({wv.x, wv.y, wv.z, 0});
         }
     }
-    int closestA = -1;
-    Real dmin = std::numeric_limits<Real>::max();
-    for (int f = 0; f < hA.numFaces; ++f) {
-        const or_face& fc = w->faces[hA.faceOffset + f];
-        const V n = qrot(A.q, V(fc.plane[0], fc.plane[1], fc.plane[2]));
-        const Real d = dot(n, sep);
-        if (d < dmin) {
-            dmin = d;
-            closestA = f;
-        }
-    }
+    const int closestA = extreme_face(w, hA, A, sep, 1.0);
     if (closestA < 0) return 0;
     const or_face& fa = w->faces[hA.faceOffset + closestA];
     const int nvA = fa.numIndices;

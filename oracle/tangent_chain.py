@@ -10,8 +10,10 @@ from step to step through the pose and velocity seeds of the tangent-linear
 build (`or_set_tangent` + `or_set_tangent_pose`), each step taken from the
 recorded state. What differs from the device's reverse sweep is then the
 adjoint's own arithmetic, plus any step whose discrete choices (contacts,
-axes, clamp masks) the FP64 step makes differently from the recorded FP32
-state; such worlds are detected from the values of the same FP64 steps.
+axes, clamp masks) the FP64 step makes differently from the device. Such
+worlds are detected two ways: from the values of the same FP64 steps, and
+from choices that flip when the recorded states are perturbed at the size of
+the device's own one-step deviation from FP64.
 """
 import numpy as np
 
@@ -95,17 +97,57 @@ def chained_tangent(o, inv_inertia3, scene, traj, seeds, kind, delta):
 # the next recorded state within ten times the one-step bars
 STABLE_POS_M = 1e-4
 STABLE_VEL_MPS = 1e-3
+# and when the FP64 step's discrete choices at every recorded state stay the
+# same under perturbations of the state at the size of the device's own
+# one-step deviation from FP64 (positions 1e-6 m, velocities 1e-5 m/s,
+# quaternions 1e-7): a choice that flips there is one the FP32 device may
+# make the other way, and the derivative then follows another piece
+PERTURB = (1e-6, 1e-7, 1e-5, 1e-5)
 
 
-def gradient_errors(o, inv_inertia3, scene, traj, grads, seeds, directions=2, rng_seed=0):
+def active_signature(o, scene, traj, rng=None):
+    """Per-world signatures (contact topology, active set) of the FP64
+    steps from the recorded states (each optionally perturbed by PERTURB in
+    uniform noise), accumulated over the trajectory. `o` is an FP64
+    OracleWorld of the scene."""
+    o.reset_active()
+    dyn = (np.asarray(scene.mass) > 0)[:, None]
+    for t in range(len(traj) - 1):
+        st = [np.array(a, np.float64) for a in traj[t]]
+        if rng is not None:
+            for k in range(4):
+                cols = 4 if k == 1 else 3
+                st[k][:, :cols] += rng.uniform(-PERTURB[k], PERTURB[k], (scene.n, cols)) * dyn
+        o.set_state_f64(*st)
+        o.step(1)
+    return o.active_hash()
+
+
+def robust_worlds(o, scene, traj, perturbations=2, rng_seed=1):
+    """Worlds whose FP64 discrete choices along the recorded trajectory are
+    the same for the recorded states and for `perturbations` perturbed
+    copies of them."""
+    base = active_signature(o, scene, traj)
+    rng = np.random.default_rng(rng_seed)
+    ok = np.ones(scene.num_worlds, bool)
+    for _ in range(perturbations):
+        ok &= (active_signature(o, scene, traj, rng) == base).all(1)
+    return ok
+
+
+def gradient_errors(o, inv_inertia3, scene, traj, grads, seeds, directions=2, rng_seed=0, o_value=None):
     """Per parameter set ("lin", "ang", "mass", "friction") and world, the
     relative error (vector norm over `directions` random directions) of the
     device gradients' directional derivatives against the chained FP64
-    tangent, and the per-world stability flags."""
+    tangent, and the per-world stability flags: the value criterion
+    (STABLE_POS_M, STABLE_VEL_MPS) and, with an FP64 OracleWorld o_value,
+    the robustness of the discrete choices (robust_worlds)."""
     rng = np.random.default_rng(rng_seed)
     dyn = np.asarray(scene.mass) > 0
     wid = np.asarray(scene.world)
     rel, stable = {}, np.ones(scene.num_worlds, bool)
+    if o_value is not None:
+        stable &= robust_worlds(o_value, scene, traj)
     for kind in ("lin", "ang", "mass", "friction"):
         comps = 3 if kind in ("lin", "ang") else 1
         ga = np.asarray(grads[kind], np.float64).reshape(scene.n, -1)
