@@ -627,24 +627,108 @@ __device__ bool corner_ok(const b3::ShapesDev& S, const b3ConvexPolyhedron& hA, 
     return fabsf(dot(pk, cross(pl, nb))) > 1e-3f;
 }
 
+// Classify the manifold's points against reference face G.faceA and
+// incident face G.faceB (values only); returns how many points fit neither
+// an incident vertex, an incident edge cut by a side plane, nor a corner of
+// two side planes.
+__device__ int geo_points(Geo& G, const b3::ShapesDev& S, const b3ConvexPolyhedron& hA, const b3ConvexPolyhedron& hB,
+                          const Mat3& RA, const Mat3& RB, float3 xB, const float3* p, int npts) {
+    int miss = 0;
+    // origin at body A's position (p and xB are given relative to it)
+    const b3Face fa = S.faces[hA.faceOffset + G.faceA];
+    const b3Face fb = S.faces[hB.faceOffset + G.faceB];
+    const int nvA = fa.numIndices, nvB = fb.numIndices;
+    const float3 nAw = mul(RA, make_float3(fa.plane[0], fa.plane[1], fa.plane[2]));
+    const float tol = 5e-5f;
+    for (int j = 0; j < npts; ++j) {
+        GeoPoint& g = G.pt[j];
+        g.kind = PK_ATTACHED;
+        g.local = mul_t(RB, p[j] - xB);
+        float bestV = tol;
+        for (int i = 0; i < nvB; ++i) {
+            const float3 w = mul(RB, vtx(S, hB, face_vertex(S, fb, i))) + xB;
+            const float e = length(w - p[j]);
+            if (e < bestV) { bestV = e; g.kind = PK_VERTEX; g.i0 = i; }
+        }
+        if (g.kind == PK_VERTEX) continue;
+        // side planes containing the point
+        int on[2] = {-1, -1};
+        float onErr[2] = {tol, tol};
+        for (int k = 0; k < nvA; ++k) {
+            const float3 va = vtx(S, hA, face_vertex(S, fa, k));
+            const float3 vb = vtx(S, hA, face_vertex(S, fa, (k + 1) % nvA));
+            float3 pn = -cross(mul(RA, va - vb), nAw);
+            const float l = length(pn);
+            if (l <= 0.f) continue;
+            pn = pn * (1.f / l);
+            const float e = fabsf(dot(pn, p[j] - mul(RA, va)));
+            if (e < onErr[0]) { onErr[1] = onErr[0]; on[1] = on[0]; onErr[0] = e; on[0] = k; }
+            else if (e < onErr[1]) { onErr[1] = e; on[1] = k; }
+        }
+        if (on[0] < 0) { ++miss; continue; }
+        // an incident edge through the point, crossing the side plane
+        // (not lying in it: the intersection must be well defined)
+        const float3 vk = vtx(S, hA, face_vertex(S, fa, on[0]));
+        const float3 vk1 = vtx(S, hA, face_vertex(S, fa, (on[0] + 1) % nvA));
+        const float3 pnk = normalize(-cross(mul(RA, vk - vk1), nAw));
+        int edge = -1;
+        float bestE = tol;
+        for (int i = 0; i < nvB; ++i) {
+            const float3 a = mul(RB, vtx(S, hB, face_vertex(S, fb, i))) + xB;
+            const float3 b = mul(RB, vtx(S, hB, face_vertex(S, fb, (i + 1) % nvB))) + xB;
+            const float3 u = b - a;
+            const float uu = dot(u, u);
+            if (uu <= 0.f) continue;
+            if (fabsf(dot(pnk, u)) < 1e-3f * sqrtf(uu)) continue;
+            const float t = dot(p[j] - a, u) / uu;
+            if (t < -1e-4f || t > 1.f + 1e-4f) continue;
+            const float e = length(a + u * t - p[j]);
+            if (e < bestE) { bestE = e; edge = i; }
+        }
+        if (edge >= 0) {
+            g.kind = PK_EDGE;
+            g.i0 = edge;
+            g.i1 = (edge + 1) % nvB;
+            g.k = on[0];
+        } else if (on[1] >= 0 && corner_ok(S, hA, hB, fa, fb, RA, RB, nAw, on[0], on[1])) {
+            g.kind = PK_CORNER;
+            g.i0 = on[0];
+            g.i1 = on[1];
+        } else {
+            ++miss;
+        }
+    }
+    return miss;
+}
+
+// Faces of h whose sign * (n . sep) is within the forward's FP32 window
+// (4e-6) of the extreme, extreme first: clipHullAgainstHull's choice, or
+// its candidates where faces tie within FP32 (the forward decides those in
+// float-float, exact ties to the lowest index).
+__device__ int face_candidates(const b3::ShapesDev& S, const b3ConvexPolyhedron& h, const Mat3& R, float3 sep,
+                               float sign, int* out, int maxOut) {
+    float best = FLT_MAX;
+    int bi = 0;
+    for (int f = 0; f < h.numFaces; ++f) {
+        const b3Face fc = S.faces[h.faceOffset + f];
+        const float d = sign * dot(mul(R, make_float3(fc.plane[0], fc.plane[1], fc.plane[2])), sep);
+        if (d < best) { best = d; bi = f; }
+    }
+    int n = 0;
+    out[n++] = bi;
+    for (int f = 0; f < h.numFaces && n < maxOut; ++f) {
+        if (f == bi) continue;
+        const b3Face fc = S.faces[h.faceOffset + f];
+        const float d = sign * dot(mul(R, make_float3(fc.plane[0], fc.plane[1], fc.plane[2])), sep);
+        if (d <= best + 4e-6f) out[n++] = f;
+    }
+    return n;
+}
+
 // Classify the stored manifold against the forward poses (values only).
 __device__ void geo_classify(Geo& G, const b3::ShapesDev& S, const b3ConvexPolyhedron& hA,
                              const b3ConvexPolyhedron& hB, const Mat3& RA, const Mat3& RB, float3 xB, float3 sep,
                              const float3* p, int npts, int* unclassified) {
-    // reference / incident faces (clipHullAgainstHull's choice)
-    float dmax = -FLT_MAX, dmin = FLT_MAX;
-    G.faceA = 0;
-    G.faceB = 0;
-    for (int f = 0; f < hB.numFaces; ++f) {
-        const b3Face fc = S.faces[hB.faceOffset + f];
-        const float d = dot(mul(RB, make_float3(fc.plane[0], fc.plane[1], fc.plane[2])), sep);
-        if (d > dmax) { dmax = d; G.faceB = f; }
-    }
-    for (int f = 0; f < hA.numFaces; ++f) {
-        const b3Face fc = S.faces[hA.faceOffset + f];
-        const float d = dot(mul(RA, make_float3(fc.plane[0], fc.plane[1], fc.plane[2])), sep);
-        if (d < dmin) { dmin = d; G.faceA = f; }
-    }
     // separating axis: the feature whose direction matches sep best
     float best = 1e-4f;
     G.axisKind = AX_ATTACHED;
@@ -682,70 +766,23 @@ __device__ void geo_classify(Geo& G, const b3::ShapesDev& S, const b3ConvexPolyh
         }
     }
     if (G.axisKind == AX_ATTACHED) atomicAdd(unclassified, 1);
-    // points: origin at body A's position (p and xB are given relative to it)
-    const b3Face fa = S.faces[hA.faceOffset + G.faceA];
-    const b3Face fb = S.faces[hB.faceOffset + G.faceB];
-    const int nvA = fa.numIndices, nvB = fb.numIndices;
-    const float3 nAw = mul(RA, make_float3(fa.plane[0], fa.plane[1], fa.plane[2]));
-    const float tol = 5e-5f;
-    for (int j = 0; j < npts; ++j) {
-        GeoPoint& g = G.pt[j];
-        g.kind = PK_ATTACHED;
-        g.local = mul_t(RB, p[j] - xB);
-        float bestV = tol;
-        for (int i = 0; i < nvB; ++i) {
-            const float3 w = mul(RB, vtx(S, hB, face_vertex(S, fb, i))) + xB;
-            const float e = length(w - p[j]);
-            if (e < bestV) { bestV = e; g.kind = PK_VERTEX; g.i0 = i; }
+    // reference / incident faces: clipHullAgainstHull's choice, trying the
+    // faces tied within FP32 until the points fit one pair of them
+    int candA[4], candB[4];
+    const int nA = face_candidates(S, hA, RA, sep, 1.f, candA, 4);
+    const int nB = face_candidates(S, hB, RB, sep, -1.f, candB, 4);
+    int bestMiss = 1 << 30, bestA = candA[0], bestB = candB[0];
+    for (int ia = 0; ia < nA && bestMiss > 0; ++ia)
+        for (int ib = 0; ib < nB && bestMiss > 0; ++ib) {
+            G.faceA = candA[ia];
+            G.faceB = candB[ib];
+            const int miss = geo_points(G, S, hA, hB, RA, RB, xB, p, npts);
+            if (miss < bestMiss) { bestMiss = miss; bestA = candA[ia]; bestB = candB[ib]; }
         }
-        if (g.kind == PK_VERTEX) continue;
-        // side planes containing the point
-        int on[2] = {-1, -1};
-        float onErr[2] = {tol, tol};
-        for (int k = 0; k < nvA; ++k) {
-            const float3 va = vtx(S, hA, face_vertex(S, fa, k));
-            const float3 vb = vtx(S, hA, face_vertex(S, fa, (k + 1) % nvA));
-            float3 pn = -cross(mul(RA, va - vb), nAw);
-            const float l = length(pn);
-            if (l <= 0.f) continue;
-            pn = pn * (1.f / l);
-            const float e = fabsf(dot(pn, p[j] - mul(RA, va)));
-            if (e < onErr[0]) { onErr[1] = onErr[0]; on[1] = on[0]; onErr[0] = e; on[0] = k; }
-            else if (e < onErr[1]) { onErr[1] = e; on[1] = k; }
-        }
-        if (on[0] < 0) { atomicAdd(unclassified, 1); continue; }
-        // an incident edge through the point, crossing the side plane
-        // (not lying in it: the intersection must be well defined)
-        const float3 vk = vtx(S, hA, face_vertex(S, fa, on[0]));
-        const float3 vk1 = vtx(S, hA, face_vertex(S, fa, (on[0] + 1) % nvA));
-        const float3 pnk = normalize(-cross(mul(RA, vk - vk1), nAw));
-        int edge = -1;
-        float bestE = tol;
-        for (int i = 0; i < nvB; ++i) {
-            const float3 a = mul(RB, vtx(S, hB, face_vertex(S, fb, i))) + xB;
-            const float3 b = mul(RB, vtx(S, hB, face_vertex(S, fb, (i + 1) % nvB))) + xB;
-            const float3 u = b - a;
-            const float uu = dot(u, u);
-            if (uu <= 0.f) continue;
-            if (fabsf(dot(pnk, u)) < 1e-3f * sqrtf(uu)) continue;
-            const float t = dot(p[j] - a, u) / uu;
-            if (t < -1e-4f || t > 1.f + 1e-4f) continue;
-            const float e = length(a + u * t - p[j]);
-            if (e < bestE) { bestE = e; edge = i; }
-        }
-        if (edge >= 0) {
-            g.kind = PK_EDGE;
-            g.i0 = edge;
-            g.i1 = (edge + 1) % nvB;
-            g.k = on[0];
-        } else if (on[1] >= 0 && corner_ok(S, hA, hB, fa, fb, RA, RB, nAw, on[0], on[1])) {
-            g.kind = PK_CORNER;
-            g.i0 = on[0];
-            g.i1 = on[1];
-        } else {
-            atomicAdd(unclassified, 1);
-        }
-    }
+    G.faceA = bestA;
+    G.faceB = bestB;
+    const int miss = geo_points(G, S, hA, hB, RA, RB, xB, p, npts);
+    if (miss) atomicAdd(unclassified, miss);
 }
 
 struct ManifoldArgs {
