@@ -301,7 +301,12 @@ def run_b3(args, world_size, local_rank):
     if settle - args.warmup > done:
         w.stepSimulation(settle - args.warmup - done, stream=st.cuda_stream)
         done = settle - args.warmup
-    w.autotune(3, stream=st.cuda_stream)
+    if args.tuning:
+        # fixed launch shapes (b3_get_tuning order) instead of the autotuner:
+        # a profiler run repeats the shapes the plain run chose
+        w.set_tuning([int(x) for x in args.tuning.split(",")])
+    else:
+        w.autotune(3, stream=st.cuda_stream)
     tuning = w.tuning()
     for _ in range(args.warmup):
         w.stepSimulation(1, stream=st.cuda_stream)
@@ -723,6 +728,10 @@ def main():
     ap.add_argument("--no-forms", action="store_true")
     ap.add_argument("--no-scale", action="store_true", help="skip the 1,048,576-body plain and adjoint steps")
     ap.add_argument("--no-check", action="store_true", help="skip the one-step oracle checks")
+    ap.add_argument("--tuning", default=None,
+                    help="settled-window launch shapes as b3_get_tuning's comma-separated values (np warps per CTA, "
+                         "pair CTA, Jacobi CTA, -, Jacobi blocks per SM, -, Jacobi mode, Jacobi gather) instead of "
+                         "autotuning, e.g. to repeat a plain run's shapes under a profiler")
     ap.add_argument("--sap", action="store_true",
                     help="sweep-and-prune broadphase (pipeline2's default) in place of the grid; single-world workloads")
     ap.add_argument("--solver", default="jacobi", choices=["jacobi", "gs"],
