@@ -735,7 +735,11 @@ __device__ __forceinline__ float3 get_f32(const FfVert& v) { return make_float3(
 // recomputed from its defining primitives, not interpolated between
 // already-rounded points: the original incident edge cut by plane k, or
 // the corner of two side planes on the incident face plane. The output
-// order is that of the sequential clip.
+// order is that of the sequential clip. A vertex also carries its own
+// position error bound (FfVert.wl): later inside / outside decisions on it
+// widen by that bound, and only the vertices that reach the output must
+// keep within kCutBudget (an intermediate vertex that a later plane clips
+// away cleanly may carry more).
 constexpr int kPlaneTag = 64;
 // error budget of one FP32 intersection in metres: with the FP32 rounding
 // of world coordinates (< 4e-6 m up to 100 m) it stays inside the 1e-5 m
@@ -770,9 +774,10 @@ __device__ __forceinline__ bool exact_axes(const Mat3& R) {
 
 __device__ __forceinline__ unsigned tag2(int a, int b) { return (unsigned)a | ((unsigned)b << 16); }
 __device__ __forceinline__ unsigned vtag(const FfVert& v) { return __float_as_uint(v.xl); }
-__device__ __forceinline__ void put_tagged(FfVert& v, float3 p, unsigned tags) {
-    v = {p.x, __uint_as_float(tags), p.y, 0.f, p.z, 0.f, 0.f, 0.f};
+__device__ __forceinline__ void put_tagged(FfVert& v, float3 p, unsigned tags, float err = 0.f) {
+    v = {p.x, __uint_as_float(tags), p.y, 0.f, p.z, 0.f, 0.f, err};
 }
+__device__ __forceinline__ float verr(const FfVert& v) { return v.wl; }
 __device__ __forceinline__ int shared_tag(unsigned s, unsigned e) {
     const int s0 = (int)(s & 0xffffu), s1 = (int)(s >> 16), e0 = (int)(e & 0xffffu), e1 = (int)(e >> 16);
     if (s0 == e0 || s0 == e1) return s0;
@@ -789,10 +794,11 @@ __device__ __forceinline__ void side_plane(const ClipGeom& G, int k, float3& pn,
     ap = f3(G.sideP[k]);
 }
 
-// Intersection of the polygon edge on constraint `tag` with side plane k;
-// *bad when its FP32 error bound exceeds the budget.
+// Intersection of the polygon edge on constraint `tag` with side plane k,
+// and its FP32 position error bound in *err; *bad for a degenerate cut (or
+// an interpolated one over the budget).
 __device__ float3 exact_cut(const ClipGeom& G, int tag, int k, float3 pn, float3 ap, float3 sv, float3 ev,
-                            bool* bad) {
+                            bool* bad, float* err) {
     const float pnl = len_ub(pn);
     if (tag >= 0 && tag < kPlaneTag) {
         // incident edge j cut by plane k, from its original end points
@@ -806,9 +812,11 @@ __device__ float3 exact_cut(const ClipGeom& G, int tag, int k, float3 pn, float3
         const float eb = 2.4e-7f * pnl * (len_ub(b) + base);
         // position error along the edge: t = da / (da - db) moves by
         // (|db| ea + |da| eb) / den^2 (at most max(ea, eb) / |den| when
-        // da and db have opposite signs, as for a crossing edge)
-        if (!(fabsf(den) > 0.f) || len_ub(b - a) * (fabsf(db) * ea + fabsf(da) * eb) > kCutBudget * den * den)
-            *bad = true;
+        // da and db have opposite signs, as for a crossing edge), plus the
+        // rounding of a + (b - a) t
+        if (!(fabsf(den) > 0.f)) *bad = true;
+        const float lba = len_ub(b - a);
+        *err = lba * (fabsf(db) * ea + fabsf(da) * eb) / (den * den) + 2.4e-7f * (len_ub(a) + lba);
         const float t = da / den;
         return a + (b - a) * t;
     }
@@ -822,8 +830,9 @@ __device__ float3 exact_cut(const ClipGeom& G, int tag, int k, float3 pn, float3
         const float3 c23 = cross(n2, n3), c31 = cross(n3, n1), c12 = cross(n1, n2);
         const float det = dot(n1, c23);
         const float3 p = (c23 * h1 + c31 * h2 + c12 * h3) * (1.f / det);
-        const float err = 3.6e-7f * (fabsf(h1) + fabsf(h2) + fabsf(h3) + len_ub(p)) + G.eIn;
-        if (!(fabsf(det) > 0.f) || err > kCutBudget * fabsf(det)) *bad = true;
+        const float e = 3.6e-7f * (fabsf(h1) + fabsf(h2) + fabsf(h3) + len_ub(p)) + G.eIn;
+        if (!(fabsf(det) > 0.f)) *bad = true;
+        *err = e / fabsf(det);
         return p;
     }
     // interpolation between the current end points (an edge along a side
@@ -835,6 +844,7 @@ __device__ float3 exact_cut(const ClipGeom& G, int tag, int k, float3 pn, float3
     const float apl = len_ub(ap);
     const float es = 2.5e-7f * pnl * (1.f + len_ub(sv) + apl), ee = 2.5e-7f * pnl * (1.f + len_ub(ev) + apl);
     if (!(fabsf(den) > 0.f) || len_ub(ev - sv) * (es + ee) > kCutBudget * fabsf(den)) *bad = true;
+    *err = kCutBudget;
     return sv + (ev - sv) * (ds / den);
 }
 
@@ -852,30 +862,34 @@ __device__ __noinline__ int clip_poly_f32(const ClipGeom& G, const FfVert* in, i
         int cnt = 0;
         float3 o0 = make_float3(0.f, 0.f, 0.f), o1 = o0;
         unsigned t0 = 0, t1 = 0;
+        float r0 = 0.f, r1 = 0.f;
         if (ve < nin) {
             const FfVert& S0 = in[ve == 0 ? nin - 1 : ve - 1];
             const FfVert& E0 = in[ve];
             const float3 sv = get_f32(S0), ev = get_f32(E0);
             const float ds = dot(pn, sv - ap);
             const float de = dot(pn, ev - ap);
-            // inside / outside decisions: FP32 error of ds, de
-            const float es = 2.5e-7f * pnl * (1.f + len_ub(sv) + apl);
-            const float ee = 2.5e-7f * pnl * (1.f + len_ub(ev) + apl);
+            // inside / outside decisions: FP32 error of ds, de, and of the
+            // vertices themselves
+            const float es = 2.5e-7f * pnl * (1.f + len_ub(sv) + apl) + pnl * verr(S0);
+            const float ee = 2.5e-7f * pnl * (1.f + len_ub(ev) + apl) + pnl * verr(E0);
             if (fabsf(ds) <= es || fabsf(de) <= ee) *bad = true;
             const bool sNeg = ds < 0.f, eNeg = de < 0.f;
             if (sNeg || eNeg) {
                 if (sNeg && eNeg) {
                     o0 = ev;
                     t0 = vtag(E0);
+                    r0 = verr(E0);
                     cnt = 1;
                 } else {
                     const int tag = shared_tag(vtag(S0), vtag(E0));
-                    o0 = exact_cut(G, tag, k, pn, ap, sv, ev, bad);
+                    o0 = exact_cut(G, tag, k, pn, ap, sv, ev, bad, &r0);
                     t0 = tag2(tag < 0 ? 0 : tag, newTag);
                     cnt = 1;
                     if (!sNeg) {
                         o1 = ev;
                         t1 = vtag(E0);
+                        r1 = verr(E0);
                         cnt = 2;
                     }
                 }
@@ -886,10 +900,10 @@ __device__ __noinline__ int clip_poly_f32(const ClipGeom& G, const FfVert* in, i
         const unsigned below = b3dev::lanemask_lt();
         const int pos = total + __popc(b1 & below) + __popc(b2 & below);
         if (cnt >= 1) {
-            if (pos < kMaxPoly) put_tagged(out[pos], o0, t0); else atomicAdd(ovf, 1);
+            if (pos < kMaxPoly) put_tagged(out[pos], o0, t0, r0); else atomicAdd(ovf, 1);
         }
         if (cnt == 2) {
-            if (pos + 1 < kMaxPoly) put_tagged(out[pos + 1], o1, t1); else atomicAdd(ovf, 1);
+            if (pos + 1 < kMaxPoly) put_tagged(out[pos + 1], o1, t1, r1); else atomicAdd(ovf, 1);
         }
         total += __popc(b1) + __popc(b2);
     }
@@ -963,8 +977,12 @@ __device__ __noinline__ int clip_f32(const PairCtx& c, const b3::ShapesDev& S, c
         float depth = 0.f;
         if (k < nIn) {
             p = get_f32(W.poly[cur][k]);
+            const float pe = verr(W.poly[cur][k]);
+            // an output point keeps within the budget; its depth decisions
+            // widen by its error
+            if (!(pe <= kCutBudget)) bad = true;
             depth = dot(nAw, p) + fA.plane[3];
-            const float eb = 5e-7f * (1.f + len_ub(p));
+            const float eb = 5e-7f * (1.f + len_ub(p)) + pe;
             if (fabsf(depth - P.maxDist) <= eb || fabsf(depth - P.skipDist) <= eb) bad = true;
             if (depth <= P.minDist) depth = P.minDist;
             keep = depth <= P.maxDist;
