@@ -54,6 +54,10 @@ constexpr int kNone = 0x7fffffff;
 // tied (the lowest index wins), in the device's float-float ranking and in
 // the oracle's FP64 one alike
 constexpr float kFaceTieTol = 1e-10f;
+// separating axes whose depths differ by no more than this (metres) are
+// tied and the lowest axis index wins, in the float-float ranking and in the
+// oracle's FP64 one alike
+constexpr float kAxisTieTol = 1e-10f;
 // pairSep[p].w: how the pair reached the exact stage
 // pairSep[p].w: how the pair reached the exact stage
 constexpr int kSepRefine = 0;      // near-minimum axes: float-float re-ranking
@@ -616,6 +620,11 @@ __device__ __noinline__ bool refine_axes(PairCtx& c, const b3::ShapesDev& S, War
     int widx = bidx;
     warp_argmin_ff(wd, widx);
     if (widx == kNone) return false;
+    // depths within kAxisTieTol of the minimum are tied and the lowest axis
+    // index wins: the reference's first minimum for axes tied in exact
+    // arithmetic, whose FP64 depths differ only by rounding
+    widx = (int)__reduce_min_sync(0xffffffffu, bidx != kNone && sub(bd, wd).hi <= kAxisTieTol ? (unsigned)bidx
+                                                                                               : 0xffffffffu);
     const unsigned who = __ballot_sync(0xffffffffu, bidx == widx);
     const int src = __ffs(who) - 1;
     sep.x.hi = __shfl_sync(0xffffffffu, bn.x.hi, src);

@@ -484,6 +484,18 @@ void project(const or_world* w, const or_poly& h, const Body& b, V dir, Real& mn
 // 100000 + 1000 e0 + e1 for an edge pair), for the active-set signature
 int g_axisId = -1;
 
+// Every axis projected by the search (depth, feature id, oriented normal):
+// depths within kAxisTieTol of the minimum are tied and the first axis in
+// the reference's order wins (its first minimum for axes tied in exact
+// arithmetic, whose FP64 depths differ only by rounding).
+constexpr double kAxisTieTol = 1e-10;
+struct AxisRec {
+    Real d;
+    int id;
+    V n;
+};
+thread_local std::vector<AxisRec> g_axes;
+
 bool face_axes(const or_world* w, const or_poly& hA, const or_poly& hB, const Body& A, const Body& B, V D,
                V& sep, Real& dmin, int idBase) {
     for (int i = 0; i < hA.numFaces; ++i) {
@@ -496,6 +508,7 @@ bool face_axes(const or_world* w, const or_poly& hA, const or_poly& hB, const Bo
         if (mx0 < mn1 || mx1 < mn0) return false;
         const Real d0 = mx0 - mn1, d1 = mx1 - mn0;
         const Real d = d0 < d1 ? d0 : d1;
+        g_axes.push_back({d, idBase + i, n});
         if (d < dmin) {
             dmin = d;
             sep = n;
@@ -524,6 +537,7 @@ void edge_axes(const or_world* w, const or_poly& hA, const or_poly& hB, const Bo
             project(w, hB, B, c, mn1, mx1);
             const Real d0 = mx0 - mn1, d1 = mx1 - mn0;
             const Real d = d0 < d1 ? d0 : d1;
+            g_axes.push_back({d, 100000 + 1000 * e0 + e1, c});
             if (d < dmin) {
                 dmin = d;
                 sep = c;
@@ -756,10 +770,19 @@ bool contact_for_shapes(const or_world* w, int pairIndex, int A, int B, const or
     {
         // track whether any axis was accepted (dmin updated)
         g_axisId = -1;
+        g_axes.clear();
         if (!face_axes(w, hA, hB, a, b, D, sep, dmin, 0)) return false;
         if (!face_axes(w, hB, hA, b, a, D, sep, dmin, 1000)) return false;
         edge_axes(w, hA, hB, a, b, D, sep, dmin);
         haveAxis = dmin < std::numeric_limits<Real>::max();
+        // ties: the first axis (in search order) within kAxisTieTol of the minimum
+        for (const AxisRec& r : g_axes)
+            if (r.d - dmin <= (Real)kAxisTieTol) {
+                sep = r.n;
+                g_axisId = r.id;
+                if (dot(-D, sep) > 0) sep = -sep;
+                break;
+            }
     }
     if (!haveAxis) return false;
     std::vector<P4> pts;
