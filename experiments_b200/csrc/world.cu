@@ -1374,16 +1374,24 @@ extern "C" int b3_autotune(b3World w, int trialSteps, void* stream) {
         int* v;
         int cand[3];
     };
-    Knob knobs[] = {{&w->npWarpsPerBlock, {1, 2, 4}}, {&w->solverThreads, {64, 128, 256}},
-                    {&w->solverOccCap, {1, 2, 4}},      {&w->solverGather, {0, 1, 0}},
-                    {&w->solverMode, {0, 1, 0}}};
-    int numKnobs = w->cfg.numWorlds > 1 ? 5 : 4;  // per-world solver only for batched worlds
-    if (w->gs) {
-        // the Jacobi launch shapes do not apply: narrowphase CTA size, then
-        // the Gauss-Seidel grid width
-        knobs[1] = knobs[4];
-        numKnobs = 2;
-    }
+    // the narrowphase CTA size by whole-step trials; with the batched
+    // Gauss-Seidel solver also its grid width (solverMode). The Jacobi
+    // launch shapes interact (a one-knob-at-a-time descent stops in a
+    // local optimum), so they are searched jointly below on the solve alone.
+    Knob knobs[] = {{&w->npWarpsPerBlock, {1, 2, 4}}, {&w->solverMode, {0, 1, 0}}};
+    const int numKnobs = w->gs ? 2 : 1;
+    // one solve from the current contacts, timed (the solve leaves the body
+    // state alone: the finish happens in the integration)
+    auto solve_trial = [&](float* ms) -> int {
+        B3_TRY(b3::launch_solver(w, st));
+        B3_CUDA(cudaEventRecord(e0, st));
+        for (int i = 0; i < 3; ++i) B3_TRY(b3::launch_solver(w, st));
+        B3_CUDA(cudaEventRecord(e1, st));
+        B3_CUDA(cudaEventSynchronize(e1));
+        B3_CUDA(cudaEventElapsedTime(ms, e0, e1));
+        ++w->tunedTrials;
+        return B3_OK;
+    };
     do {
         for (int k = 0; k < 4 && rc == B3_OK; ++k)
             if (cudaMemcpyAsync(save + k * N, bufs[k], N * sizeof(float4), cudaMemcpyDeviceToDevice, st) !=
@@ -1411,6 +1419,37 @@ extern "C" int b3_autotune(b3World w, int trialSteps, void* stream) {
             }
             *kb.v = best;
             if (rc != B3_OK) break;
+        }
+        if (rc == B3_OK && !w->gs) {
+            // Jacobi: CTA size x blocks per SM x gather (x mode for batched
+            // worlds), every combination timed on the same contacts
+            rc = restore();
+            if (rc == B3_OK) rc = step_begin(w, st);
+            if (rc == B3_OK) rc = b3::launch_aabb_hash(w, st);
+            if (rc == B3_OK) rc = b3::launch_sort_and_cells(w, st);
+            if (rc == B3_OK) rc = b3::launch_find_pairs(w, st);
+            if (rc == B3_OK) rc = b3::launch_narrowphase(w, st);
+            if (rc == B3_OK) rc = b3::launch_manifolds(w, st);
+            int bt = w->solverThreads, bo = w->solverOccCap, bg = w->solverGather, bm = w->solverMode;
+            float bestMs = 1e30f;
+            const int modes = w->cfg.numWorlds > 1 ? 2 : 1;  // per-world solver only for batched worlds
+            for (int m = 0; m < modes && rc == B3_OK; ++m)
+                for (int t : {64, 128, 256})
+                    for (int o : {1, 2, 4, 8})
+                        for (int g = 0; g < 2 && rc == B3_OK; ++g) {
+                            if (m == 1 && o > 1) continue;  // the per-world grid ignores the cap
+                            w->solverMode = m;
+                            w->solverThreads = t;
+                            w->solverOccCap = o;
+                            w->solverGather = g;
+                            float ms = 0.f;
+                            if ((rc = solve_trial(&ms)) != B3_OK) break;
+                            if (ms < bestMs) {
+                                bestMs = ms;
+                                bt = t, bo = o, bg = g, bm = m;
+                            }
+                        }
+            w->solverThreads = bt, w->solverOccCap = bo, w->solverGather = bg, w->solverMode = bm;
         }
         if (rc == B3_OK) rc = restore();
         if (rc == B3_OK && cudaStreamSynchronize(st) != cudaSuccess) rc = B3_ERR_CUDA;

@@ -591,15 +591,17 @@ int b3_batch_world_stats(b3World w, float* out4, int numWorlds, void* stream);
  * [offsets[k], offsets[k+1])). offsets NULL = query numWorlds only. Used to
  * partition worlds across GPUs by body count. */
 int b3_batch_world_offsets(b3World w, int* offsets, int maxWorlds, int* numWorlds);
-/* Autotuner: coordinate descent over the launch shapes of the tunable
- * kernels on the current scene (narrowphase warps per CTA 1/2/4, Jacobi
- * CTA size 64/128/256, Jacobi persistent blocks per SM 1/2/4, Jacobi
- * body-average gather one-at-a-time / four-wide, and for batched worlds
- * the Jacobi mode grid-barrier / block-per-world); each trial
- * runs trialSteps eager steps from the same saved state, timed with CUDA
- * events; the fastest value of each knob is kept, the body state and
- * counters are restored, and the step graph is recaptured on the next
- * b3_step. Synchronises the stream. */
+/* Autotuner over the launch shapes of the tunable kernels on the current
+ * scene: the narrowphase warps per CTA (1/2/4) by trials of trialSteps
+ * eager steps from the same saved state; then the Jacobi launch shapes
+ * jointly, every combination of CTA size (64/128/256), persistent blocks
+ * per SM (1/2/4/8), body-average gather (one-at-a-time / four-wide) and,
+ * for batched worlds, mode (grid-barrier / block-per-world), each timed on
+ * three solves of the same contacts (the knobs interact, so they are not
+ * tuned one at a time). With the batched Gauss-Seidel solver its grid width
+ * is tuned by step trials instead. Timing uses CUDA events; the fastest
+ * shapes are kept, the body state and counters are restored, and the step
+ * graph is recaptured on the next b3_step. Synchronises the stream. */
 int b3_autotune(b3World w, int trialSteps, void* stream);
 /* values: narrowphase warps per CTA, pair-search CTA size, solver CTA size,
  * kernel launches per step of the captured step graph (0 before capture),
