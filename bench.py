@@ -81,21 +81,21 @@ LATTICE = {"c1": (16, 16, 16), "c2": (64, 32, 64), "c2s": (32, 16, 32), "c5": (1
 
 def fp32_peak_tflops(sm_mhz):
     """FP32 CUDA-core peak at an SM clock: 148 SMs x 128 FP32 lanes x 2
-    (FMA) x clock. No FP32 figure is measured on this pool, so this is the
+    (FMA) x clock. No FP32 peak is measured for this device, so this is the
     nominal peak at the clock sampled during the timed region."""
     return 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
 
 
-# Per-unit figures from the ncu capture summarised in
-# profiles/kernels_c2s_settled_step.md (settled 16,384-body case, same
-# kernels): FP32 operations each kernel executes (2 per FFMA + FADD + FMUL,
-# per thread) and DRAM bytes (read + write), per pair or per manifold.
-NCU_SOURCE = "profiles/kernels_c2s_settled_step.md (ncu, settled 16,384-body case)"
+# Per-unit figures from the ncu capture of the settled 16,384-body case (the
+# same kernels; summarised under profiles/): FP32 operations each kernel
+# executes (2 per FFMA + FADD + FMUL, per thread) and DRAM bytes (read +
+# write), per pair or per manifold.
+NCU_SOURCE = "ncu capture of the settled 16,384-body mixed-hull step (profiles/)"
 NCU_PER_UNIT = {
-    "k_np_sweep": {"fp32_ops_per_pair": 25737.0, "dram_bytes_per_pair": 13.2, "source": NCU_SOURCE},
-    "k_np_clip": {"fp32_ops_per_manifold": 8940.0, "dram_bytes_per_manifold": 154.5, "source": NCU_SOURCE},
-    "k_setup_rows": {"dram_bytes_per_manifold": 288.9, "source": NCU_SOURCE},
-    "k_jacobi": {"dram_bytes_per_manifold": 605.6, "source": NCU_SOURCE},
+    "k_np_sweep": {"fp32_ops_per_pair": 25828.0, "dram_bytes_per_pair": 12.9, "source": NCU_SOURCE},
+    "k_np_clip": {"fp32_ops_per_manifold": 8865.0, "dram_bytes_per_manifold": 105.6, "source": NCU_SOURCE},
+    "k_setup_rows": {"dram_bytes_per_manifold": 295.1, "source": NCU_SOURCE},
+    "k_jacobi": {"dram_bytes_per_manifold": 611.4, "source": NCU_SOURCE},
 }
 
 
