@@ -34,6 +34,12 @@ struct ShapesDev {
     const float4* localAabb;  // 2 per collidable (min, max)
     const float* inradius;    // per polyhedron: lower bound of its support about localCenter
     const b3ChildShape* children;  // the compounds' children
+    // the hulls' vertices two at a time for the packed FP32x2 projection:
+    // pair j of polyhedron p at polyPack[p] + j holds (x0, x1, y0, y1) in
+    // vpXY and (z0, z1) in vpZ (an odd count repeats the last vertex)
+    const float4* vpXY;
+    const float2* vpZ;
+    const int* polyPack;
     int numPolys, numVerts, numFaces, numIndices, numEdges;
     int tableBytes;           // packed size for shared-memory staging
 };
@@ -67,6 +73,9 @@ struct DevBuffers {
     float4* localAabb = nullptr;
     float* polyInradius = nullptr;
     b3ChildShape* childShapes = nullptr;
+    float4* vpXY = nullptr;  // vertex pairs (x0, x1, y0, y1)
+    float2* vpZ = nullptr;   // vertex pairs (z0, z1)
+    int* polyPack = nullptr; // per polyhedron: its first vertex pair
     // compound and mesh pairs: sub-pair records (body A, body B, side A,
     // side B; a side is a child shape >= 0 or -(polytope + 1)), per pair
     // counts and their exclusive scan
@@ -168,6 +177,8 @@ struct b3World_t {
     std::vector<b3ConvexPolyhedron> polys;
     std::vector<float> verts4, edges4, localAabb8;
     std::vector<float> polyInradius;
+    std::vector<float> vpXY, vpZ;  // vertex pairs, built at upload
+    std::vector<int> polyPack;
     std::vector<b3ChildShape> childShapes;  // children of the compounds
     int numSpheres = 0, numPlanes = 0, numCompounds = 0, numMeshes = 0;
     bool hasSpheresPlanes() const { return numSpheres > 0 && (numSpheres > 1 || numPlanes > 0); }

@@ -174,24 +174,6 @@ __device__ __forceinline__ void warp_argmin_ff(ff& v, int& idx) {
     v.lo = fkey_inv(ml);
 }
 
-// FP32 projection of a hull onto world axis dir, relative to the hull's own
-// position (the caller adds the position offset)
-__device__ __forceinline__ void project_rel(const float4* __restrict__ verts, int off, int nv, const Mat3& R,
-                                            float3 dir, float& mn, float& mx) {
-    const float3 ld = mul_t(R, dir);
-    float lo = FLT_MAX, hi = -FLT_MAX;
-    // four vertex loads in flight per lane: the loop is latency-bound
-#pragma unroll 4
-    for (int i = 0; i < nv; ++i) {
-        const float4 v = __ldg(&verts[off + i]);
-        const float dp = v.x * ld.x + v.y * ld.y + v.z * ld.z;
-        lo = fminf(lo, dp);
-        hi = fmaxf(hi, dp);
-    }
-    mn = lo;
-    mx = hi;
-}
-
 // Axis index space (sequential order of the reference): faces of A
 // [0, FA), faces of B [FA, FA+FB), edge pairs e0*EB+e1 after that.
 //
@@ -246,14 +228,60 @@ __device__ __forceinline__ bool axis_dir(const PairCtx& c, const b3::ShapesDev& 
     return true;
 }
 
+// Two FP32 lanes in one 64-bit register, and the packed FP32x2 multiply
+// and fused multiply-add (each half rounds as its scalar instruction would).
+__device__ __forceinline__ unsigned long long pack2(float a, float b) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void unpack2(unsigned long long v, float& a, float& b) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ unsigned long long mul2(unsigned long long a, unsigned long long b) {
+    unsigned long long d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigned long long b, unsigned long long c) {
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
+// FP32 projection of polyhedron h (index pi) onto world axis dir relative to
+// its own position, two vertices per packed FP32x2 instruction: x * d.x,
+// then + y * d.y, then + z * d.z, each rounded once.
+__device__ __forceinline__ void project_packed(const b3::ShapesDev& S, const b3ConvexPolyhedron& h, int pi,
+                                               const Mat3& R, float3 dir, float& mn, float& mx) {
+    const float3 ld = mul_t(R, dir);
+    const unsigned long long lx = pack2(ld.x, ld.x), ly = pack2(ld.y, ld.y), lz = pack2(ld.z, ld.z);
+    const int off = __ldg(&S.polyPack[pi]), np = (h.numVertices + 1) >> 1;
+    float lo = FLT_MAX, hi = -FLT_MAX;
+#pragma unroll 4
+    for (int j = 0; j < np; ++j) {
+        const float4 xy = __ldg(&S.vpXY[off + j]);
+        const float2 z = __ldg(&S.vpZ[off + j]);
+        unsigned long long d = mul2(pack2(xy.x, xy.y), lx);
+        d = fma2(pack2(xy.z, xy.w), ly, d);
+        d = fma2(pack2(z.x, z.y), lz, d);
+        float d0, d1;
+        unpack2(d, d0, d1);
+        lo = fminf(lo, fminf(d0, d1));
+        hi = fmaxf(hi, fmaxf(d0, d1));
+    }
+    mn = lo;
+    mx = hi;
+}
+
 // FP32 depth along the oriented axis n (P2/sat.cl:227-252, relative to
 // body A's position).
 __device__ __forceinline__ float axis_depth(const PairCtx& c, const b3::ShapesDev& S, float3 rel, float3 n) {
     const b3ConvexPolyhedron& pa = *c.pa;
     const b3ConvexPolyhedron& pb = *c.pb;
     float mn0, mx0, mn1, mx1;
-    project_rel(S.verts, pa.vertexOffset, pa.numVertices, c.RA, n, mn0, mx0);
-    project_rel(S.verts, pb.vertexOffset, pb.numVertices, c.RB, n, mn1, mx1);
+    project_packed(S, pa, (int)(c.pa - S.polys), c.RA, n, mn0, mx0);
+    project_packed(S, pb, (int)(c.pb - S.polys), c.RB, n, mn1, mx1);
     const float off = dot(rel, n);  // posB - posA along n
     mn1 += off;
     mx1 += off;

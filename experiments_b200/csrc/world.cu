@@ -70,7 +70,7 @@ int dalloc(T*& p, size_t count) {
 void free_all(b3::DevBuffers& d) {
     void* ptrs[] = {d.pos, d.quat, d.linVel, d.angVel, d.invMass, d.friction, d.restitution,
                     d.invInertia, d.collidable, d.worldId, d.cols, d.polys, d.verts, d.faces,
-                    d.indices, d.edges, d.localAabb, d.polyInradius, d.childShapes, d.subPairs, d.subCount, d.subOffset, d.aabbMin, d.aabbMax, d.smallSlot,
+                    d.indices, d.edges, d.localAabb, d.polyInradius, d.childShapes, d.vpXY, d.vpZ, d.polyPack, d.subPairs, d.subCount, d.subOffset, d.aabbMin, d.aabbMax, d.smallSlot,
                     d.largeStart, d.largeList, d.sapSmall, d.sapLarge, d.sapSorted, d.sapCount, d.sapOffset, d.keys, d.vals, d.keysAlt, d.valsAlt, d.cellTable,
                     d.pairs, d.contacts, d.manifoldFlag, d.pairSep, d.npFast, d.npSlow, d.npCand, d.manifoldScan,
                     d.manifoldPair,
@@ -141,6 +141,9 @@ b3::ShapesDev b3World_t::shapesDev() const {
     S.localAabb = d.localAabb;
     S.inradius = d.polyInradius;
     S.children = d.childShapes;
+    S.vpXY = d.vpXY;
+    S.vpZ = d.vpZ;
+    S.polyPack = d.polyPack;
     S.numPolys = (int)polys.size();
     S.numVerts = (int)verts4.size() / 4;
     S.numFaces = (int)faces.size();
@@ -740,6 +743,30 @@ static int upload_shapes(b3World w, cudaStream_t st) {
     B3_CUDA(cudaMemcpyAsync(d.localAabb, w->localAabb8.data(), sizeof(float) * w->localAabb8.size(), cudaMemcpyHostToDevice, st));
     B3_CUDA(cudaMemcpyAsync(d.polyInradius, w->polyInradius.data(), sizeof(float) * w->polyInradius.size(),
                             cudaMemcpyHostToDevice, st));
+    // vertex pairs per polyhedron (the packed projection's layout)
+    w->vpXY.clear();
+    w->vpZ.clear();
+    w->polyPack.assign(w->polys.size(), 0);
+    for (size_t p = 0; p < w->polys.size(); ++p) {
+        const b3ConvexPolyhedron& h = w->polys[p];
+        w->polyPack[p] = (int)(w->vpZ.size() / 2);
+        for (int j = 0; j < h.numVertices; j += 2) {
+            const float* a = &w->verts4[4 * (size_t)(h.vertexOffset + j)];
+            const float* b = &w->verts4[4 * (size_t)(h.vertexOffset + std::min(j + 1, h.numVertices - 1))];
+            w->vpXY.insert(w->vpXY.end(), {a[0], b[0], a[1], b[1]});
+            w->vpZ.insert(w->vpZ.end(), {a[2], b[2]});
+        }
+    }
+    B3_TRY(dalloc(d.vpXY, w->vpXY.size() / 4 + 1));
+    B3_TRY(dalloc(d.vpZ, w->vpZ.size() / 2 + 1));
+    B3_TRY(dalloc(d.polyPack, w->polyPack.size() + 1));
+    if (!w->vpXY.empty()) {
+        B3_CUDA(cudaMemcpyAsync(d.vpXY, w->vpXY.data(), sizeof(float) * w->vpXY.size(), cudaMemcpyHostToDevice, st));
+        B3_CUDA(cudaMemcpyAsync(d.vpZ, w->vpZ.data(), sizeof(float) * w->vpZ.size(), cudaMemcpyHostToDevice, st));
+    }
+    if (!w->polyPack.empty())
+        B3_CUDA(cudaMemcpyAsync(d.polyPack, w->polyPack.data(), sizeof(int) * w->polyPack.size(),
+                                cudaMemcpyHostToDevice, st));
     B3_TRY(dalloc(d.childShapes, w->childShapes.size()));
     if (!w->childShapes.empty())
         B3_CUDA(cudaMemcpyAsync(d.childShapes, w->childShapes.data(), sizeof(b3ChildShape) * w->childShapes.size(),
