@@ -88,14 +88,14 @@ def fp32_peak_tflops(sm_mhz):
 
 # Per-unit figures from the ncu capture of the settled 16,384-body case (the
 # same kernels; summarised under profiles/): FP32 operations each kernel
-# executes (2 per FFMA + FADD + FMUL, per thread) and DRAM bytes (read +
-# write), per pair or per manifold.
+# executes (2 per FFMA + FADD + FMUL, 4 per FFMA2, 2 per FMUL2, per thread)
+# and DRAM bytes (read + write), per pair or per manifold.
 NCU_SOURCE = "ncu capture of the settled 16,384-body mixed-hull step (profiles/)"
 NCU_PER_UNIT = {
-    "k_np_sweep": {"fp32_ops_per_pair": 25828.0, "dram_bytes_per_pair": 12.9, "source": NCU_SOURCE},
-    "k_np_clip": {"fp32_ops_per_manifold": 8865.0, "dram_bytes_per_manifold": 105.6, "source": NCU_SOURCE},
-    "k_setup_rows": {"dram_bytes_per_manifold": 295.1, "source": NCU_SOURCE},
-    "k_jacobi": {"dram_bytes_per_manifold": 611.4, "source": NCU_SOURCE},
+    "k_np_sweep": {"fp32_ops_per_pair": 25977.0, "dram_bytes_per_pair": 13.1, "source": NCU_SOURCE},
+    "k_np_clip": {"fp32_ops_per_manifold": 8889.0, "dram_bytes_per_manifold": 105.0, "source": NCU_SOURCE},
+    "k_setup_rows": {"dram_bytes_per_manifold": 290.4, "source": NCU_SOURCE},
+    "k_jacobi": {"dram_bytes_per_manifold": 605.0, "source": NCU_SOURCE},
 }
 
 
@@ -689,7 +689,8 @@ def kernel_roofline(name, ms, sc, counters, key_bits, body_bits, hbm_peak, peak_
         if ops is not None:
             r["achieved"] = ops * count / (ms / 1e3) / 1e12
             r["frac"] = r["achieved"] / peak
-            r["work"] = (f"executed FP32 operations: {ops:.0f} per {unit} (2 per FFMA + FADD + FMUL, per thread) "
+            r["work"] = (f"executed FP32 operations: {ops:.0f} per {unit} (2 per FFMA + FADD + FMUL, 4 per FFMA2, "
+                         f"2 per FMUL2, per thread) "
                          f"from {c.get('source')}, times {count} {unit}s")
         else:
             r["achieved"] = None
