@@ -41,7 +41,6 @@ struct ShapesDev {
     const float2* vpZ;
     const int* polyPack;
     int numPolys, numVerts, numFaces, numIndices, numEdges;
-    int tableBytes;           // packed size for shared-memory staging
 };
 
 struct SimParams {

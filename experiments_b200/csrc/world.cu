@@ -149,7 +149,6 @@ b3::ShapesDev b3World_t::shapesDev() const {
     S.numFaces = (int)faces.size();
     S.numIndices = (int)indices.size();
     S.numEdges = (int)edges4.size() / 4;
-    S.tableBytes = 0;
     return S;
 }
 
