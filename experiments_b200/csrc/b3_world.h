@@ -221,6 +221,7 @@ struct b3World_t {
     int solverMode = 0;        // Jacobi: 0 = grid barriers, 1 = one block per world (batched);
                                // batched Gauss-Seidel: grid width 0 = manifolds / 8, 1 = manifolds / 64
     int solverGather = 0;      // Jacobi body averages: 0 = one copy at a time, 1 = four loads in flight
+    int pairSearchMode = 0;    // grid pair search: 0 = thread per body, 1 = warp per body
     int tunedTrials = 0;       // configurations the autotuner timed
     int npSmemAttr = 0;        // dynamic shared memory attribute set on the narrowphase kernels
 

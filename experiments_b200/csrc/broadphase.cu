@@ -33,7 +33,9 @@ using namespace b3m;
 namespace {
 
 constexpr int kAabbThreads = 256;
-constexpr int kPairTile = 128;
+constexpr int kPairTile = 128;        // bodies per tile, one thread per body
+constexpr int kWarpPairTile = 32;     // bodies per tile of the warp-per-body search
+constexpr int kWarpPairThreads = 128; // its CTA: four warps of eight bodies each
 
 struct GridParams {
     float invCell;
@@ -152,6 +154,46 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* warp_t
     return r;
 }
 
+// Output offset of one pair tile by decoupled look-back over the tiles before
+// it (flag 1 = aggregate, 2 = inclusive prefix); the last tile publishes the
+// pair count, clamped to maxPairs with the excess counted as pair overflow.
+// Called by one thread of the tile.
+__device__ uint32_t tile_lookback(int tile, int num_tiles, uint32_t agg, const GridParams& g,
+                                  unsigned long long* __restrict__ status, int32_t* __restrict__ numPairs,
+                                  b3Counters* __restrict__ counters, int32_t* __restrict__ err_flag) {
+    const unsigned long long FA = 1ull << 32, FP = 2ull << 32;
+    uint32_t excl = 0;
+    if (tile == 0) {
+        b3dev::st_release_u64(status, FP | agg);
+    } else {
+        b3dev::st_release_u64(status + tile, FA | agg);
+        int t = tile - 1;
+        while (t >= 0) {
+            unsigned long long s = 0;
+            int spins = 0;
+            while (((s = b3dev::ld_acquire_u64(status + t)) >> 32) == 0) {
+                if (++spins > b3dev::kSpinLimit) {
+                    atomicExch(err_flag, 1);
+                    atomicAdd(&counters->timeouts, 1);
+                    break;
+                }
+                __nanosleep(32);
+            }
+            excl += (uint32_t)s;
+            if ((s >> 32) != 1) break;
+            --t;
+        }
+        b3dev::st_release_u64(status + tile, FP | (unsigned long long)(excl + agg));
+    }
+    if (tile == num_tiles - 1) {
+        const uint32_t total = excl + agg;
+        *numPairs = (int32_t)min(total, (uint32_t)g.maxPairs);
+        if (total > (uint32_t)g.maxPairs) atomicAdd(&counters->pairOverflow, (int)(total - (uint32_t)g.maxPairs));
+        counters->numPairs = (int32_t)min(total, (uint32_t)g.maxPairs);
+    }
+    return excl;
+}
+
 __global__ void __launch_bounds__(kPairTile)
 k_find_pairs(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
              const float4* __restrict__ aabbMin, const float4* __restrict__ aabbMax,
@@ -236,41 +278,8 @@ k_find_pairs(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ val
         }
         // tile compaction with decoupled look-back
         const uint32_t texcl = block_excl_scan((uint32_t)cnt, warp_tot, &tile_total);
-        if (threadIdx.x == 0) {
-            const unsigned long long FA = 1ull << 32, FP = 2ull << 32;
-            const uint32_t agg = tile_total;
-            uint32_t excl = 0;
-            if (tile == 0) {
-                b3dev::st_release_u64(status, FP | agg);
-            } else {
-                b3dev::st_release_u64(status + tile, FA | agg);
-                int t = tile - 1;
-                while (t >= 0) {
-                    unsigned long long s = 0;
-                    int spins = 0;
-                    while (((s = b3dev::ld_acquire_u64(status + t)) >> 32) == 0) {
-                        if (++spins > b3dev::kSpinLimit) {
-                            atomicExch(err_flag, 1);
-                            atomicAdd(&counters->timeouts, 1);
-                            break;
-                        }
-                        __nanosleep(32);
-                    }
-                    excl += (uint32_t)s;
-                    if ((s >> 32) != 1) break;
-                    --t;
-                }
-                b3dev::st_release_u64(status + tile, FP | (unsigned long long)(excl + agg));
-            }
-            tile_excl = excl;
-            if (tile == num_tiles - 1) {
-                const uint32_t total = excl + agg;
-                *numPairs = (int32_t)min(total, (uint32_t)g.maxPairs);
-                if (total > (uint32_t)g.maxPairs)
-                    atomicAdd(&counters->pairOverflow, (int)(total - (uint32_t)g.maxPairs));
-                counters->numPairs = (int32_t)min(total, (uint32_t)g.maxPairs);
-            }
-        }
+        if (threadIdx.x == 0)
+            tile_excl = tile_lookback(tile, num_tiles, tile_total, g, status, numPairs, counters, err_flag);
         if (ovf) atomicAdd(&counters->pairOverflow, ovf);
         if (covf) atomicAdd(&counters->cellOverflow, covf);
         __syncthreads();
@@ -280,6 +289,193 @@ k_find_pairs(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ val
             for (int c = 0; c < cnt; ++c) {
                 const uint32_t o = base + c;
                 if (o < (uint32_t)g.maxPairs) pairs[o] = make_int2((int)self, buf[c]);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Warp-cooperative form of k_find_pairs with the same output: one warp per
+// body, lane l < 27 scanning neighbour cell l in findPairsInCell's z, y, x
+// order (G3/bt3dGridBroadphaseOCL.cl:170-206). Each lane counts its cell's
+// candidates (id(other) < id(self), inclusive AABB overlap) over the whole
+// bucket, four entries per load batch; a warp scan of the counts gives every
+// cell the pair count of the cells before it, and from that the sequential
+// cap semantics follow per cell: the cell keeps min(count, cap - before)
+// pairs, counts one pair overflow when it has more, and counts one cell
+// overflow when it has none and its bucket holds more than maxBodiesPerCell
+// bodies. Kept pairs are written from a 64-position candidate mask (a rescan
+// covers candidates further into a bucket). The large bodies follow in
+// 32-wide ballots with the same cap rule. Tiles of 32 bodies (eight per
+// warp) are compacted like k_find_pairs' 128-body tiles, so the pair list,
+// pair count and overflow counters are identical to it bit for bit.
+__global__ void __launch_bounds__(kWarpPairThreads)
+k_find_pairs_warp(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals,
+                  const float4* __restrict__ aabbMin, const float4* __restrict__ aabbMax,
+                  const uint2* __restrict__ table, const int32_t* stamp_dev,
+                  const int* __restrict__ largeStart, const int* __restrict__ largeList, GridParams g,
+                  int2* __restrict__ pairs, int32_t* __restrict__ numPairs,
+                  unsigned long long* __restrict__ status, int32_t* __restrict__ tile_counter,
+                  b3Counters* __restrict__ counters, int32_t* __restrict__ err_flag) {
+    extern __shared__ int pbuf[];  // [kWarpPairTile][maxPairsPerBody]
+    __shared__ uint32_t warp_tot[32];
+    __shared__ uint32_t tile_total, tile_excl;
+    __shared__ int tile_sh;
+    __shared__ int cnts[kWarpPairTile];
+    __shared__ uint32_t offs[kWarpPairTile];
+    constexpr int kPerWarp = kWarpPairTile / (kWarpPairThreads / 32);
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int n = g.numSmall;
+    const int num_tiles = (n + kWarpPairTile - 1) / kWarpPairTile;
+    const uint32_t stamp = (uint32_t)*stamp_dev;
+    const int cap = g.maxPairsPerBody - 1;  // curr_max (G3/bt3dGridBroadphaseOCL.cl:129)
+    const int dz = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dx = lane % 3 - 1;
+    const uint32_t lanes_below = (1u << lane) - 1u;
+    for (;;) {
+        if (threadIdx.x == 0) tile_sh = atomicAdd(tile_counter, 1);
+        __syncthreads();
+        const int tile = tile_sh;
+        if (tile >= num_tiles) break;
+        int ovf = 0, covf = 0;
+        for (int b = 0; b < kPerWarp; ++b) {
+            const int local = warp * kPerWarp + b;
+            const int i = tile * kWarpPairTile + local;
+            int cnt = 0;
+            if (i < n) {  // warp-uniform
+                const uint32_t key = keys[i];
+                const uint32_t self = vals[i];
+                const uint32_t world = key >> g.cellBits;
+                const float4 mn0 = aabbMin[self], mx0 = aabbMax[self];
+                const float cx = mrn(arn(mn0.x, mx0.x), 0.5f);
+                const float cy = mrn(arn(mn0.y, mx0.y), 0.5f);
+                const float cz = mrn(arn(mn0.z, mx0.z), 0.5f);
+                int c = 0, start = 0, end = 0;
+                uint32_t h = 0;
+                bool active = false;
+                unsigned long long mask = 0;  // candidate positions 0..63 of the bucket
+                if (lane < 27) {
+                    const int zz = (grid_coord(cz, g.invCell, g.dimZ) + dz) & (g.dimZ - 1);
+                    const int yy = (grid_coord(cy, g.invCell, g.dimY) + dy) & (g.dimY - 1);
+                    const int xx = (grid_coord(cx, g.invCell, g.dimX) + dx) & (g.dimX - 1);
+                    h = (world << g.cellBits) | (uint32_t)(zz * g.dimY * g.dimX + yy * g.dimX + xx);
+                    const uint2 e = table[h];
+                    if (e.x == stamp) {
+                        active = true;
+                        start = (int)e.y;
+                        end = min(start + g.maxBodiesPerCell, n);
+                        for (int j = start; j < end; j += 4) {
+                            bool in[4], cand[4];
+                            uint32_t oo[4];
+                            float4 amn[4], amx[4];
+#pragma unroll
+                            for (int u = 0; u < 4; ++u) {
+                                const int jj = j + u;
+                                in[u] = false;
+                                oo[u] = 0;
+                                if (jj < end) {
+                                    in[u] = keys[jj] == h;
+                                    oo[u] = vals[jj];
+                                }
+                            }
+#pragma unroll
+                            for (int u = 0; u < 4; ++u) {
+                                cand[u] = in[u] && oo[u] < self;
+                                amn[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+                                amx[u] = amn[u];
+                                if (cand[u]) {
+                                    amn[u] = aabbMin[oo[u]];
+                                    amx[u] = aabbMax[oo[u]];
+                                }
+                            }
+#pragma unroll
+                            for (int u = 0; u < 4; ++u) {
+                                if (cand[u] && aabb_overlap(mn0, mx0, amn[u], amx[u])) {
+                                    const int pos = j + u - start;
+                                    if (pos < 64) mask |= 1ull << pos;
+                                    ++c;
+                                }
+                            }
+                            if (!in[3]) break;  // keys are sorted: the bucket ended in this batch
+                        }
+                    }
+                }
+                // pairs of the cells before this one, and the cap rule per cell
+                int incl = c;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(full, incl, o);
+                    if (lane >= o) incl += y;
+                }
+                const int before = min(incl - c, cap);
+                const int room = cap - before;
+                const int keep = min(c, room);
+                const bool cell_ovf = c > room;
+                ovf += cell_ovf ? 1 : 0;
+                if (active && !cell_ovf && end < n && keys[end] == h) ++covf;
+                cnt = min(__shfl_sync(full, incl, 31), cap);
+                int* buf = pbuf + local * g.maxPairsPerBody;
+                if (keep > 0) {
+                    int w = 0;
+                    unsigned long long m = mask;
+                    while (m && w < keep) {
+                        const int pos = __ffsll((long long)m) - 1;
+                        m &= m - 1;
+                        buf[before + w++] = (int)vals[start + pos];
+                    }
+                    for (int j = start + 64; j < end && w < keep; ++j) {
+                        if (keys[j] != h) break;
+                        const uint32_t other = vals[j];
+                        if (other < self && aabb_overlap(mn0, mx0, aabbMin[other], aabbMax[other]))
+                            buf[before + w++] = (int)other;
+                    }
+                }
+                // large bodies of this world
+                const int l0 = largeStart[world], l1 = largeStart[world + 1];
+                for (int l = l0; l < l1; l += 32) {
+                    const int ll = l + lane;
+                    bool hit = false;
+                    int L = 0;
+                    if (ll < l1) {
+                        L = largeList[ll];
+                        hit = aabb_overlap(mn0, mx0, aabbMin[L], aabbMax[L]);
+                    }
+                    const uint32_t bm = __ballot_sync(full, hit);
+                    const int rank = __popc(bm & lanes_below);
+                    if (hit && cnt + rank < cap) buf[cnt + rank] = L;
+                    const int nb = __popc(bm);
+                    if (cnt + nb > cap) {
+                        if (lane == 0) ++ovf;
+                        cnt = cap;
+                        break;
+                    }
+                    cnt += nb;
+                }
+            }
+            if (lane == 0) cnts[local] = cnt;
+        }
+        __syncthreads();
+        // tile compaction with decoupled look-back
+        const uint32_t v = threadIdx.x < kWarpPairTile ? (uint32_t)cnts[threadIdx.x] : 0u;
+        const uint32_t texcl = block_excl_scan(v, warp_tot, &tile_total);
+        if (threadIdx.x < kWarpPairTile) offs[threadIdx.x] = texcl;
+        if (threadIdx.x == 0)
+            tile_excl = tile_lookback(tile, num_tiles, tile_total, g, status, numPairs, counters, err_flag);
+        ovf = __reduce_add_sync(full, ovf);
+        covf = __reduce_add_sync(full, covf);
+        if (lane == 0 && ovf) atomicAdd(&counters->pairOverflow, ovf);
+        if (lane == 0 && covf) atomicAdd(&counters->cellOverflow, covf);
+        __syncthreads();
+        for (int b = 0; b < kPerWarp; ++b) {
+            const int local = warp * kPerWarp + b;
+            const int i = tile * kWarpPairTile + local;
+            if (i >= n) break;
+            const int self = (int)vals[i];
+            const uint32_t base = tile_excl + offs[local];
+            const int c = cnts[local];
+            for (int k = lane; k < c; k += 32) {
+                const uint32_t o = base + (uint32_t)k;
+                if (o < (uint32_t)g.maxPairs) pairs[o] = make_int2(self, pbuf[local * g.maxPairsPerBody + k]);
             }
         }
         __syncthreads();
@@ -345,25 +541,37 @@ int launch_find_pairs(b3World_t* w, cudaStream_t st) {
     B3_CUDA(cudaMemsetAsync(w->d.scalars + S_NUM_PAIRS, 0, sizeof(int32_t), st));
     B3_CUDA(cudaMemsetAsync(w->d.scalars + S_TILE, 0, sizeof(int32_t), st));
     if (ns == 0) return B3_OK;
-    const int tiles = (ns + kPairTile - 1) / kPairTile;
+    const bool warp = w->pairSearchMode == 1;
+    const int tileBodies = warp ? kWarpPairTile : kPairTile;
+    const int threads = warp ? kWarpPairThreads : kPairTile;
+    const int tiles = (ns + tileBodies - 1) / tileBodies;
     B3_CUDA(cudaMemsetAsync(w->d.scanScratch, 0, sizeof(unsigned long long) * tiles, st));
     const GridParams g = grid_params(w);
-    const size_t smem = (size_t)kPairTile * w->cfg.maxPairsPerBody * sizeof(int);
-    static bool attr = false;
-    if (!attr) {
-        B3_CUDA(cudaFuncSetAttribute(k_find_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     96 * 1024));
-        attr = true;
+    const size_t smem = (size_t)tileBodies * w->cfg.maxPairsPerBody * sizeof(int);
+    const void* fn = warp ? (const void*)k_find_pairs_warp : (const void*)k_find_pairs;
+    // opt in to the per-body pair buffers above 48 KB (128 KB at the
+    // largest cap, 256 pairs per body in 128-body tiles)
+    static size_t optIn[2] = {0, 0};
+    if (smem > 48 * 1024 && smem > optIn[warp]) {
+        B3_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        optIn[warp] = smem;
     }
     int occ = 1;
-    B3_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_find_pairs, kPairTile, smem));
+    B3_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, smem));
     occ = occ < 1 ? 1 : occ;
     const int grid = std::min(tiles, w->ctx->numSMs * occ);
-    k_find_pairs<<<grid, kPairTile, smem, st>>>(
-        w->d.keys, w->d.vals, w->d.aabbMin, w->d.aabbMax, w->d.cellTable, w->d.scalars + S_STAMP,
-        w->d.largeStart, w->d.largeList, g, w->d.pairs, w->d.scalars + S_NUM_PAIRS,
-        (unsigned long long*)w->d.scanScratch, w->d.scalars + S_TILE, w->d.counters,
-        w->d.scalars + S_ERR);
+    if (warp)
+        k_find_pairs_warp<<<grid, threads, smem, st>>>(
+            w->d.keys, w->d.vals, w->d.aabbMin, w->d.aabbMax, w->d.cellTable, w->d.scalars + S_STAMP,
+            w->d.largeStart, w->d.largeList, g, w->d.pairs, w->d.scalars + S_NUM_PAIRS,
+            (unsigned long long*)w->d.scanScratch, w->d.scalars + S_TILE, w->d.counters,
+            w->d.scalars + S_ERR);
+    else
+        k_find_pairs<<<grid, threads, smem, st>>>(
+            w->d.keys, w->d.vals, w->d.aabbMin, w->d.aabbMax, w->d.cellTable, w->d.scalars + S_STAMP,
+            w->d.largeStart, w->d.largeList, g, w->d.pairs, w->d.scalars + S_NUM_PAIRS,
+            (unsigned long long*)w->d.scanScratch, w->d.scalars + S_TILE, w->d.counters,
+            w->d.scalars + S_ERR);
     B3_CHECK_LAUNCH();
     return B3_OK;
 }

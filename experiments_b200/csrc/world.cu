@@ -695,7 +695,7 @@ static int ensure_capacity(b3World w) {
             B3_TRY(dalloc(d.gsGroupFill, 4 * (size_t)b3::kGsMaxBatch));
             B3_TRY(dalloc(d.gsGroupOffset, 4 * (size_t)b3::kGsMaxBatch + 1));
         }
-        const size_t tiles = (w->cfg.maxBodies + 127) / 128 + 16;
+        const size_t tiles = (w->cfg.maxBodies + 31) / 32 + 16;  // pair-search tiles, 32 bodies at the least
         d.scanScratchBytes = std::max(b3::scan_scratch_bytes(std::max<int64_t>(cap, w->cfg.maxBodies + 1)),
                                       tiles * 8 + 256);
         B3_TRY(dalloc((unsigned char*&)d.scanScratch, d.scanScratchBytes));
@@ -1418,6 +1418,17 @@ extern "C" int b3_autotune(b3World w, int trialSteps, void* stream) {
         ++w->tunedTrials;
         return B3_OK;
     };
+    // three pair searches over the same sorted keys, timed
+    auto pair_trial = [&](float* ms) -> int {
+        B3_TRY(b3::launch_find_pairs(w, st));
+        B3_CUDA(cudaEventRecord(e0, st));
+        for (int i = 0; i < 3; ++i) B3_TRY(b3::launch_find_pairs(w, st));
+        B3_CUDA(cudaEventRecord(e1, st));
+        B3_CUDA(cudaEventSynchronize(e1));
+        B3_CUDA(cudaEventElapsedTime(ms, e0, e1));
+        ++w->tunedTrials;
+        return B3_OK;
+    };
     do {
         for (int k = 0; k < 4 && rc == B3_OK; ++k)
             if (cudaMemcpyAsync(save + k * N, bufs[k], N * sizeof(float4), cudaMemcpyDeviceToDevice, st) !=
@@ -1445,6 +1456,26 @@ extern "C" int b3_autotune(b3World w, int trialSteps, void* stream) {
             }
             *kb.v = best;
             if (rc != B3_OK) break;
+        }
+        if (rc == B3_OK && !w->sap) {
+            // grid pair search: thread per body or warp per body, each timed
+            // on three searches over the same sorted keys
+            rc = restore();
+            if (rc == B3_OK) rc = step_begin(w, st);
+            if (rc == B3_OK) rc = b3::launch_aabb_hash(w, st);
+            if (rc == B3_OK) rc = b3::launch_sort_and_cells(w, st);
+            int bp = w->pairSearchMode;
+            float bestMs = 1e30f;
+            for (int m = 0; m < 2 && rc == B3_OK; ++m) {
+                w->pairSearchMode = m;
+                float ms = 0.f;
+                if ((rc = pair_trial(&ms)) != B3_OK) break;
+                if (ms < bestMs) {
+                    bestMs = ms;
+                    bp = m;
+                }
+            }
+            w->pairSearchMode = bp;
         }
         if (rc == B3_OK && !w->gs) {
             // Jacobi: CTA size x blocks per SM x gather (x mode for batched
@@ -1492,24 +1523,26 @@ extern "C" int b3_set_tuning(b3World w, const int* values, int count) {
     const int np = values[0], st = values[2], cap = count >= 5 ? values[4] : w->solverOccCap;
     const int mode = count >= 7 ? values[6] : w->solverMode;
     const int gather = count >= 8 ? values[7] : w->solverGather;
+    const int pairMode = count >= 9 ? values[8] : w->pairSearchMode;
     if ((np != 1 && np != 2 && np != 4) || (st != 64 && st != 128 && st != 256) || cap < 1 || cap > 8 ||
-        (mode != 0 && mode != 1) || (gather != 0 && gather != 1))
+        (mode != 0 && mode != 1) || (gather != 0 && gather != 1) || (pairMode != 0 && pairMode != 1))
         return B3_ERR_INVALID_ARG;
     w->npWarpsPerBlock = np;
     w->solverThreads = st;
     w->solverOccCap = cap;
     w->solverMode = mode;
     w->solverGather = gather;
+    w->pairSearchMode = pairMode;
     w->graphValid = false;
     return B3_OK;
 }
 
 extern "C" int b3_get_tuning(b3World w, int* values, int max, int* count) {
     if (!w || !count) return B3_ERR_INVALID_ARG;
-    int v[8] = {w->npWarpsPerBlock, w->pairThreads, w->solverThreads, w->kernelsPerStep, w->solverOccCap,
-                w->tunedTrials, w->solverMode, w->solverGather};
-    *count = 8;
-    for (int i = 0; i < std::min(8, max); ++i) values[i] = v[i];
+    int v[9] = {w->npWarpsPerBlock, w->pairThreads, w->solverThreads, w->kernelsPerStep, w->solverOccCap,
+                w->tunedTrials, w->solverMode, w->solverGather, w->pairSearchMode};
+    *count = 9;
+    for (int i = 0; i < std::min(9, max); ++i) values[i] = v[i];
     return B3_OK;
 }
 

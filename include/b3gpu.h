@@ -593,7 +593,9 @@ int b3_batch_world_stats(b3World w, float* out4, int numWorlds, void* stream);
 int b3_batch_world_offsets(b3World w, int* offsets, int maxWorlds, int* numWorlds);
 /* Autotuner over the launch shapes of the tunable kernels on the current
  * scene: the narrowphase warps per CTA (1/2/4) by trials of trialSteps
- * eager steps from the same saved state; then the Jacobi launch shapes
+ * eager steps from the same saved state; then the grid pair search form
+ * (thread or warp per body), each timed on three searches over the same
+ * sorted keys; then the Jacobi launch shapes
  * jointly, every combination of CTA size (64/128/256), persistent blocks
  * per SM (1/2/4/8), body-average gather (one-at-a-time / four-wide) and,
  * for batched worlds, mode (grid-barrier / block-per-world), each timed on
@@ -609,13 +611,16 @@ int b3_autotune(b3World w, int trialSteps, void* stream);
  * mode (0 = persistent grid with grid barriers, 1 = one block per world
  * with block barriers; batched worlds only, bit-identical results), Jacobi
  * body-average gather (0 = one copy at a time, 1 = four loads in flight;
- * bit-identical results). */
+ * bit-identical results), grid pair search form (0 = one thread per body
+ * over its 27 cells, 1 = one warp per body, a lane per cell; the same pair
+ * list and overflow counts bit for bit). */
 int b3_get_tuning(b3World w, int* values, int max, int* count);
 /* Set the tunables in b3_get_tuning's order (count >= 3; the pair-search
  * CTA size, the launch count and the trial count are read-only, indices 4,
- * 6 and 7 are optional):
+ * 6, 7 and 8 are optional):
  * narrowphase warps per CTA 1/2/4, Jacobi CTA size 64/128/256, Jacobi
- * blocks per SM cap 1..8, Jacobi mode 0/1, Jacobi gather 0/1. */
+ * blocks per SM cap 1..8, Jacobi mode 0/1, Jacobi gather 0/1, pair search
+ * form 0/1. */
 int b3_set_tuning(b3World w, const int* values, int count);
 
 /* ------------------------------------------------------------------ */
