@@ -732,7 +732,7 @@ def main():
     ap.add_argument("--tuning", default=None,
                     help="settled-window launch shapes as b3_get_tuning's comma-separated values (np warps per CTA, "
                          "pair CTA, Jacobi CTA, -, Jacobi blocks per SM, -, Jacobi mode, Jacobi gather[, pair search "
-                         "form]) instead of "
+                         "form[, clip form]]) instead of "
                          "autotuning, e.g. to repeat a plain run's shapes under a profiler")
     ap.add_argument("--sap", action="store_true",
                     help="sweep-and-prune broadphase (pipeline2's default) in place of the grid; single-world workloads")
@@ -842,6 +842,7 @@ def main():
                            "jacobi_cta": res["tuning"][2], "jacobi_blocks_per_sm": res["tuning"][4],
                            "autotune_trials": res["tuning"][5], "jacobi_per_world_blocks": res["tuning"][6],
                            "jacobi_gather4": res["tuning"][7], "pair_search_warp_per_body": res["tuning"][8],
+                           "clip_lane_groups": res["tuning"][9],
                            "kernels_per_step": int(res["kernels"])},
                 "parallelism": (f"worlds sharded x{world_size}" if res["sharded"] else f"replicas x{world_size}")
                 if world_size > 1 else "single GPU"})

@@ -599,10 +599,10 @@ class PhysicsWorld:
     def tuning(self):
         """(narrowphase warps/CTA, pair CTA size, solver CTA size, kernels per
         captured step, Jacobi blocks per SM cap, configurations timed,
-        Jacobi mode, Jacobi gather, grid pair search form)."""
-        v = (C.c_int * 9)()
+        Jacobi mode, Jacobi gather, grid pair search form, FP32 clip form)."""
+        v = (C.c_int * 10)()
         cnt = C.c_int()
-        _check(self.lib.b3_get_tuning(self.h, v, 9, C.byref(cnt)), "b3_get_tuning")
+        _check(self.lib.b3_get_tuning(self.h, v, 10, C.byref(cnt)), "b3_get_tuning")
         return list(v)[:cnt.value]
 
     def set_tuning(self, values):

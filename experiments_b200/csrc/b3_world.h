@@ -101,6 +101,7 @@ struct DevBuffers {
     float4* pairSep = nullptr;        // per pair: FP32 separating axis of the sweep
     int* npFast = nullptr;            // queue: pairs whose axis the FP32 sweep decided
     int* npSlow = nullptr;            // queue: pairs for the float-float path
+    int* npDefer = nullptr;           // queue: clip pairs the lane groups pass to the warp clip
     int* npCand = nullptr;            // near-minimum axes of queued pairs (kNpCandSlots x 32)
     uint32_t* manifoldScan = nullptr; // exclusive scan of the flags
     int* manifoldPair = nullptr;      // manifold -> pair slot
@@ -158,6 +159,8 @@ enum ScalarSlot {
     S_NUM_SUB = 15,       // sub-pairs of compound and mesh pairs this step (after the capacity cut)
     S_NUM_SLOTS = 16,     // manifold slots: pairs, then sub-pairs
     S_SUB_TOTAL = 17,     // sub-pairs before the capacity cut
+    S_NP_DEFER = 18,      // clip-queue pairs the lane-group clip passed to the warp clip
+    S_NP_WORK5 = 19,
     S_NUM_SCALARS = 24
 };
 
@@ -222,8 +225,10 @@ struct b3World_t {
                                // batched Gauss-Seidel: grid width 0 = manifolds / 8, 1 = manifolds / 64
     int solverGather = 0;      // Jacobi body averages: 0 = one copy at a time, 1 = four loads in flight
     int pairSearchMode = 0;    // grid pair search: 0 = thread per body, 1 = warp per body
+    int clipGroups = 1;        // FP32 clip: 0 = a warp per pair, 1 = 8-lane groups (warp for what does not fit)
     int tunedTrials = 0;       // configurations the autotuner timed
     int npSmemAttr = 0;        // dynamic shared memory attribute set on the narrowphase kernels
+    int npGroupSmemAttr = 0;   // the same for the lane-group clip
 
     int cooperativeOk = 1;
 

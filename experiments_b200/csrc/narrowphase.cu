@@ -1102,17 +1102,19 @@ __device__ __noinline__ int4 reduce_f32(const FfVert* p, int n, float3 nearNorma
     warp_argmin(f2, i2);
     warp_argmin(f3v, i3);
     const float gap = 2.f * (2.f * eP + rm * du) + 1e-6f, gapw = 2.f * eP + 1e-6f;
-    int worst = 0;
+    // points within the gap of each extreme, over both rounds of lanes
+    int cw = 0, c0 = 0, c1 = 0, c2 = 0, c3 = 0;
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
         if (j >= nj) break;
         const bool ok = lane + 32 * j < n;
-        worst = max(worst, near_count(mw, fw[j], ok, gapw));
-        worst = max(worst, near_count(f0, fu[j], ok, gap));
-        worst = max(worst, near_count(f1, -fu[j], ok, gap));
-        worst = max(worst, near_count(f2, fv[j], ok, gap));
-        worst = max(worst, near_count(f3v, -fv[j], ok, gap));
+        cw += near_count(mw, fw[j], ok, gapw);
+        c0 += near_count(f0, fu[j], ok, gap);
+        c1 += near_count(f1, -fu[j], ok, gap);
+        c2 += near_count(f2, fv[j], ok, gap);
+        c3 += near_count(f3v, -fv[j], ok, gap);
     }
+    const int worst = max(max(cw, c0), max(max(c1, c2), c3));
     // values near the FLT_MIN start (i.e. near zero) are ambiguous too
     *tie = worst > 1 || fabsf(f0) <= gap || fabsf(f1) <= gap || fabsf(f2) <= gap || fabsf(f3v) <= gap;
     int4 idx = make_int4(i0 == kNone ? 0 : i0, i1 == kNone ? 1 : i1, i2 == kNone ? 2 : i2, i3 == kNone ? 3 : i3);
@@ -1568,26 +1570,28 @@ k_np_sweep(const int2* __restrict__ pairs, const int4* __restrict__ subs, const 
 // Stage 2, pairs with an FP32 axis: face selection, clipping and reduction
 // in FP32 with error bounds; any doubt sends the pair to the float-float
 // queue instead. (Four blocks per SM, 128 registers, measured 4-5 % faster
-// than five or six on the settled workloads.)
+// than five or six on the settled workloads.) The queue is the clip queue
+// (scalars[countSlot] entries, work counter scalars[workSlot]): every pair
+// with an FP32 axis, or the pairs the lane-group clip passed on.
 template <bool kSub>
 __global__ void __launch_bounds__(128, 4)
 k_np_clip(const int2* __restrict__ pairs, const int4* __restrict__ subs, b3::BodiesDev Bd, b3::ShapesDev S, NpParams P,
-          float4* __restrict__ pairSep, const int* __restrict__ fastQ, int* __restrict__ slowQ,
-          b3Contact4* __restrict__ contacts, uint32_t* __restrict__ manifoldFlag, int32_t* __restrict__ scalars,
-          b3Counters* __restrict__ counters) {
+          float4* __restrict__ pairSep, const int* __restrict__ clipQ, int countSlot, int workSlot,
+          int* __restrict__ slowQ, b3Contact4* __restrict__ contacts, uint32_t* __restrict__ manifoldFlag,
+          int32_t* __restrict__ scalars, b3Counters* __restrict__ counters) {
     extern __shared__ __align__(16) unsigned char np_smem[];
     const int lane = threadIdx.x & 31;
     WarpScratch& W = reinterpret_cast<WarpScratch*>(np_smem)[threadIdx.x >> 5];
-    const int nFast = scalars[b3::S_NP_FAST];
+    const int nFast = scalars[countSlot];
     // the prefetched chunk lives in the float-float plane table, which only
     // the exact stage uses
     PairPre* pre = reinterpret_cast<PairPre*>(W.planes);
     for (;;) {
-        const int chunk = next_work(scalars + b3::S_NP_WORK2, nFast, kPreChunk);
+        const int chunk = next_work(scalars + workSlot, nFast, kPreChunk);
         if (chunk < 0) break;
         const int n = min(kPreChunk, nFast - chunk);
         if (lane < n) {
-            const int p = fastQ[chunk + lane];
+            const int p = clipQ[chunk + lane];
             item_prefetch<kSub>(pre[lane], p, pairs, subs, scalars[b3::S_NUM_PAIRS], Bd, S);
             pre[lane].aux = pairSep[p];
         }
@@ -1633,6 +1637,403 @@ k_np_clip(const int2* __restrict__ pairs, const int4* __restrict__ subs, b3::Bod
             }
             __syncwarp();
         }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Stage 2 by lane groups: kClipGroup lanes per pair, four pairs per warp.
+// A cube face clipped by a cube face keeps 4 to 8 of a warp's 32 lanes busy;
+// a group of 8 lanes runs the same face selection, clip, depth filter,
+// reduction and Contact4 with the same arithmetic in the same order (each
+// per-vertex and per-face value is computed alike; compactions keep the
+// sequential order; the centroid sum of at most 16 points associates as the
+// 32-lane butterfly does, whose first step only adds zeros), so a pair gets
+// the same bits from either. A pair whose faces or clipped polygon exceed
+// the group's 16-vertex tables goes to the clip queue of the warp kernel,
+// which redoes it from the start; a pair whose clip faces tie goes to the
+// float-float stage, as from the warp kernel.
+// ---------------------------------------------------------------------------
+constexpr int kClipGroup = 8;                // lanes per pair
+constexpr int kGroupPoly = 2 * kClipGroup;   // vertex capacity of a group's polygons and face tables
+
+struct __align__(16) GroupScratch {
+    FfVert poly[2][kGroupPoly];
+    float4 sideN[kGroupPoly];
+    float4 sideP[kGroupPoly];
+    float4 incV[kGroupPoly];
+    PairCtx ctx;
+    ClipGeom geom;
+    PairPre pre;
+};
+
+__device__ __forceinline__ int grp_lane() { return threadIdx.x & (kClipGroup - 1); }
+__device__ __forceinline__ unsigned grp_mask() {
+    return ((1u << kClipGroup) - 1u) << ((threadIdx.x & 31) & ~(kClipGroup - 1));
+}
+__device__ __forceinline__ float grp_max(float v, unsigned m) {
+    return fkey_inv(__reduce_max_sync(m, fkey(v, kNanMax)));
+}
+// (value, index) minimum over the group, as warp_argmin
+__device__ __forceinline__ void grp_argmin(float& v, int& idx, unsigned m) {
+    const int k = fkey(v, kNanMin);
+    const int km = __reduce_min_sync(m, k);
+    idx = (int)__reduce_min_sync(m, k == km ? (unsigned)idx : 0xffffffffu);
+    v = fkey_inv(km);
+}
+
+// select_face over the group's lanes; faces within the window of the FP32
+// extreme only set *tied (the pair then goes to the float-float stage,
+// which decides them).
+__device__ __noinline__ int select_face_g(const b3::ShapesDev& S, const PairCtx& c, bool sideA, float3 sepf,
+                                          float sign, bool* tied) {
+    const b3ConvexPolyhedron& h = sideA ? *c.pa : *c.pb;
+    const Mat3& R = sideA ? c.RA : c.RB;
+    const int gl = grp_lane();
+    const unsigned gm = grp_mask();
+    float bv = FLT_MAX;
+    int bi = kNone;
+    float d0 = FLT_MAX;  // this lane's first face
+    for (int f = gl; f < h.numFaces; f += kClipGroup) {
+        const float4 pl = __ldg((const float4*)&S.faces[h.faceOffset + f].plane[0]);
+        const float d = sign * dot(mul(R, make_float3(pl.x, pl.y, pl.z)), sepf);
+        if (f == gl) d0 = d;
+        if (d < bv) { bv = d; bi = f; }
+    }
+    float wv = bv;
+    int wi = bi;
+    grp_argmin(wv, wi, gm);
+    if (wi == kNone) return kNone;
+    const float lim = wv + 4e-6f;
+    int inWin;
+    if (h.numFaces <= kClipGroup) {
+        inWin = __popc(__ballot_sync(gm, d0 <= lim));
+    } else {
+        inWin = 0;
+        for (int f = gl; f < h.numFaces; f += kClipGroup) {
+            const float4 pl = __ldg((const float4*)&S.faces[h.faceOffset + f].plane[0]);
+            if (sign * dot(mul(R, make_float3(pl.x, pl.y, pl.z)), sepf) <= lim) ++inWin;
+        }
+        inWin = __reduce_add_sync(gm, inWin);
+    }
+    if (inWin > 1) *tied = true;
+    return wi;
+}
+
+// clip_poly_f32 over the group; *over when the output exceeds kGroupPoly
+// (nothing past it is written).
+__device__ __noinline__ int clip_poly_f32_g(const ClipGeom& G, const FfVert* in, int nin, int k, FfVert* out,
+                                            bool* bad, bool* over) {
+    const int gl = grp_lane();
+    const unsigned gm = grp_mask();
+    float3 pn, ap;
+    side_plane(G, k, pn, ap);
+    const float pnl = len_ub(pn);
+    const float apl = len_ub(ap);
+    const unsigned newTag = (unsigned)(kPlaneTag + k);
+    int total = 0;
+    for (int base = 0; base < nin; base += kClipGroup) {
+        const int ve = base + gl;
+        int cnt = 0;
+        float3 o0 = make_float3(0.f, 0.f, 0.f), o1 = o0;
+        unsigned t0 = 0, t1 = 0;
+        float r0 = 0.f, r1 = 0.f;
+        if (ve < nin) {
+            const FfVert& S0 = in[ve == 0 ? nin - 1 : ve - 1];
+            const FfVert& E0 = in[ve];
+            const float3 sv = get_f32(S0), ev = get_f32(E0);
+            const float ds = dot(pn, sv - ap);
+            const float de = dot(pn, ev - ap);
+            const float es = 2.5e-7f * pnl * (1.f + len_ub(sv) + apl) + pnl * verr(S0);
+            const float ee = 2.5e-7f * pnl * (1.f + len_ub(ev) + apl) + pnl * verr(E0);
+            if (fabsf(ds) <= es || fabsf(de) <= ee) *bad = true;
+            const bool sNeg = ds < 0.f, eNeg = de < 0.f;
+            if (sNeg || eNeg) {
+                if (sNeg && eNeg) {
+                    o0 = ev;
+                    t0 = vtag(E0);
+                    r0 = verr(E0);
+                    cnt = 1;
+                } else {
+                    const int tag = shared_tag(vtag(S0), vtag(E0));
+                    o0 = exact_cut(G, tag, k, pn, ap, sv, ev, bad, &r0);
+                    t0 = tag2(tag < 0 ? 0 : tag, newTag);
+                    cnt = 1;
+                    if (!sNeg) {
+                        o1 = ev;
+                        t1 = vtag(E0);
+                        r1 = verr(E0);
+                        cnt = 2;
+                    }
+                }
+            }
+        }
+        const unsigned b1 = __ballot_sync(gm, cnt >= 1), b2 = __ballot_sync(gm, cnt == 2);
+        const unsigned below = b3dev::lanemask_lt();
+        const int pos = total + __popc(b1 & below) + __popc(b2 & below);
+        if (cnt >= 1 && pos < kGroupPoly) put_tagged(out[pos], o0, t0, r0);
+        if (cnt == 2 && pos + 1 < kGroupPoly) put_tagged(out[pos + 1], o1, t1, r1);
+        total += __popc(b1) + __popc(b2);
+    }
+    __syncwarp(gm);
+    if (total > kGroupPoly) *over = true;
+    return min(total, kGroupPoly);
+}
+
+// clip_f32 over the group. *defer: a face or the clipped polygon exceeds the
+// group's tables (nothing is decided; the warp kernel redoes the pair).
+__device__ __noinline__ int clip_f32_g(const PairCtx& c, const b3::ShapesDev& S, const NpParams& P, int ai, int bi,
+                                       GroupScratch& W, int* outBuf, bool* doubt, bool* defer) {
+    const int gl = grp_lane();
+    const unsigned gm = grp_mask();
+    const b3ConvexPolyhedron& pa = *c.pa;
+    const b3ConvexPolyhedron& pb = *c.pb;
+    if (ai == kNone || bi == kNone) return 0;
+    {
+        ClipGeom g;
+        g.sideN = W.sideN;
+        g.sideP = W.sideP;
+        g.incV = W.incV;
+        g.fB = S.faces[pb.faceOffset + bi];
+        g.fA = S.faces[pa.faceOffset + ai];
+        g.fB.numIndices = min(g.fB.numIndices, kMaxPoly);
+        g.fA.numIndices = min(g.fA.numIndices, kMaxPoly);
+        g.RA = c.RA;
+        g.RB = c.RB;
+        g.rel = c.posB - c.posA;
+        g.nAw = mul(c.RA, make_float3(g.fA.plane[0], g.fA.plane[1], g.fA.plane[2]));
+        g.nIn = mul(c.RB, make_float3(g.fB.plane[0], g.fB.plane[1], g.fB.plane[2]));
+        g.hIn = -g.fB.plane[3] + dot2(g.nIn, g.rel);
+        g.eIn = 2.5e-7f * (fabsf(g.fB.plane[3]) + fabsf(g.hIn)) + (exact_axes(c.RB) ? 0.f : 2.4e-7f * len_ub(g.rel));
+        if (gl == 0) W.geom = g;
+        __syncwarp(gm);
+    }
+    const ClipGeom& G = W.geom;
+    int nIn = G.fB.numIndices;
+    const int nvA = G.fA.numIndices;
+    if (nIn > kGroupPoly || nvA > kGroupPoly) {
+        *defer = true;
+        return 0;
+    }
+    for (int k = gl; k < nIn; k += kClipGroup) {
+        const float4 v = __ldg(&S.verts[pb.vertexOffset + S.indices[G.fB.indexOffset + k]]);
+        W.incV[k] = f4(mul(c.RB, f3(v)) + G.rel);
+    }
+    for (int k = gl; k < nvA; k += kClipGroup) {
+        const float4 a = __ldg(&S.verts[pa.vertexOffset + S.indices[G.fA.indexOffset + k]]);
+        const float4 b = __ldg(&S.verts[pa.vertexOffset + S.indices[G.fA.indexOffset + (k + 1) % nvA]]);
+        W.sideN[k] = f4(-cross(mul(c.RA, make_float3(a.x - b.x, a.y - b.y, a.z - b.z)), G.nAw));
+        W.sideP[k] = f4(mul(c.RA, f3(a)));
+    }
+    __syncwarp(gm);
+    for (int k = gl; k < nIn; k += kClipGroup)
+        put_tagged(W.poly[0][k], inc_vertex(G, k), tag2((k + nIn - 1) % nIn, k));
+    __syncwarp(gm);
+    bool bad = false, over = false;
+    int cur = 0;
+    for (int e0 = 0; e0 < nvA && !over; ++e0) {
+        nIn = clip_poly_f32_g(G, W.poly[cur], nIn, e0, W.poly[cur ^ 1], &bad, &over);
+        cur ^= 1;
+    }
+    if (over) {
+        *defer = true;
+        return 0;
+    }
+    const float3 nAw = G.nAw;
+    const b3Face& fA = G.fA;
+    int total = 0;
+    for (int base = 0; base < nIn; base += kClipGroup) {
+        const int k = base + gl;
+        bool keep = false;
+        float3 p = make_float3(0.f, 0.f, 0.f);
+        float depth = 0.f;
+        if (k < nIn) {
+            p = get_f32(W.poly[cur][k]);
+            const float pe = verr(W.poly[cur][k]);
+            if (!(pe <= kCutBudget)) bad = true;
+            depth = dot(nAw, p) + fA.plane[3];
+            const float eb = 5e-7f * (1.f + len_ub(p)) + pe;
+            if (fabsf(depth - P.maxDist) <= eb || fabsf(depth - P.skipDist) <= eb) bad = true;
+            if (depth <= P.minDist) depth = P.minDist;
+            keep = depth <= P.maxDist;
+        }
+        const unsigned m = __ballot_sync(gm, keep);
+        const int pos = total + __popc(m & b3dev::lanemask_lt());
+        if (keep) put_f32(W.poly[cur ^ 1][pos], p + c.posA, depth);
+        total += __popc(m);
+    }
+    __syncwarp(gm);
+    *doubt = __any_sync(gm, bad);
+    *outBuf = cur ^ 1;
+    return total;
+}
+
+// reduce_f32 over the group, for n <= kGroupPoly points (two per lane).
+__device__ __noinline__ int4 reduce_f32_g(const FfVert* p, int n, float3 nearNormal, bool* tie) {
+    const int gl = grp_lane();
+    const unsigned gm = grp_mask();
+    const float3 o = get_f32(p[0]);
+    float3 s = make_float3(0.f, 0.f, 0.f);
+    for (int k = gl; k < n; k += kClipGroup) s += get_f32(p[k]) - o;
+#pragma unroll
+    for (int q = kClipGroup / 2; q > 0; q >>= 1) {
+        s.x += __shfl_xor_sync(gm, s.x, q);
+        s.y += __shfl_xor_sync(gm, s.y, q);
+        s.z += __shfl_xor_sync(gm, s.z, q);
+    }
+    const float3 cr = s * (1.f / (float)n);
+    const float3 aV = -cr;
+    float3 u = cross(nearNormal, aV);
+    const float ul = length(u);
+    float3 v = cross(nearNormal, u);
+    u = normalize(u);
+    v = normalize(v);
+    float pm = 0.f, rm = 0.f;
+    for (int k = gl; k < n; k += kClipGroup) {
+        const float3 q = get_f32(p[k]);
+        pm = fmaxf(pm, len_ub(q));
+        rm = fmaxf(rm, len_ub((q - o) - cr));
+    }
+    pm = grp_max(pm, gm);
+    rm = grp_max(rm, gm);
+    const float eP = 4e-6f + 1.2e-7f * pm;
+    const float du = 2.f * eP / fmaxf(ul, 1e-30f) + 4e-7f;
+    float fw[2], fu[2], fv[2];
+    float mw = FLT_MAX, f0 = FLT_MIN, f1 = FLT_MIN, f2 = FLT_MIN, f3v = FLT_MIN;
+    int iw = kNone, i0 = kNone, i1 = kNone, i2 = kNone, i3 = kNone;
+    const int nj = n > kClipGroup ? 2 : 1;
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        const int k = gl + kClipGroup * j;
+        fw[j] = FLT_MAX; fu[j] = 0.f; fv[j] = 0.f;
+        if (j < nj && k < n) {
+            const float3 r = (get_f32(p[k]) - o) - cr;
+            fw[j] = p[k].wh;
+            fu[j] = dot(u, r);
+            fv[j] = dot(v, r);
+            if (fw[j] < mw) { mw = fw[j]; iw = k; }
+            if (fu[j] < f0) { f0 = fu[j]; i0 = k; }
+            if (-fu[j] < f1) { f1 = -fu[j]; i1 = k; }
+            if (fv[j] < f2) { f2 = fv[j]; i2 = k; }
+            if (-fv[j] < f3v) { f3v = -fv[j]; i3 = k; }
+        }
+    }
+    grp_argmin(mw, iw, gm);
+    grp_argmin(f0, i0, gm);
+    grp_argmin(f1, i1, gm);
+    grp_argmin(f2, i2, gm);
+    grp_argmin(f3v, i3, gm);
+    const float gap = 2.f * (2.f * eP + rm * du) + 1e-6f, gapw = 2.f * eP + 1e-6f;
+    int cw = 0, c0 = 0, c1 = 0, c2 = 0, c3 = 0;
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        if (j >= nj) break;
+        const bool ok = gl + kClipGroup * j < n;
+        cw += __popc(__ballot_sync(gm, ok && fw[j] <= mw + gapw));
+        c0 += __popc(__ballot_sync(gm, ok && fu[j] <= f0 + gap));
+        c1 += __popc(__ballot_sync(gm, ok && -fu[j] <= f1 + gap));
+        c2 += __popc(__ballot_sync(gm, ok && fv[j] <= f2 + gap));
+        c3 += __popc(__ballot_sync(gm, ok && -fv[j] <= f3v + gap));
+    }
+    const int worst = max(max(cw, c0), max(max(c1, c2), c3));
+    *tie = worst > 1 || fabsf(f0) <= gap || fabsf(f1) <= gap || fabsf(f2) <= gap || fabsf(f3v) <= gap;
+    int4 idx = make_int4(i0 == kNone ? 0 : i0, i1 == kNone ? 1 : i1, i2 == kNone ? 2 : i2, i3 == kNone ? 3 : i3);
+    const int minIndex = iw == kNone ? -1 : iw;
+    if (idx.x != minIndex && idx.y != minIndex && idx.z != minIndex && idx.w != minIndex) idx.x = minIndex;
+    return idx;
+}
+
+// emit_contact by the group's lanes
+__device__ __forceinline__ void emit_contact_g(int p, const PairCtx& c, const FfVert* pts, int nRed, int4 idx,
+                                               float3 nrm, const b3::BodiesDev& Bd, const NpParams& P,
+                                               b3Contact4* __restrict__ contacts, uint32_t* __restrict__ manifoldFlag) {
+    const int gl = grp_lane();
+    b3Contact4* out = &contacts[p];
+    if (gl < nRed) {
+        const int k = gl == 0 ? idx.x : gl == 1 ? idx.y : gl == 2 ? idx.z : idx.w;
+        const FfVert q = pts[k];
+        *reinterpret_cast<float4*>(&out->worldPos[gl][0]) =
+            make_float4(q.xh + q.xl, q.yh + q.yl, q.zh + q.zl, q.wh + q.wl);
+    } else if (gl < 4) {
+        *reinterpret_cast<float4*>(&out->worldPos[gl][0]) = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    if (gl == 4) {
+        *reinterpret_cast<float4*>(&out->worldNormal[0]) = make_float4(nrm.x, nrm.y, nrm.z, (float)nRed);
+        out->friction = combine_friction(Bd.friction[c.A], Bd.friction[c.B], P.frictionCombine);
+        out->pairIndex = p;
+        out->bodyAPtrAndSignBit = c.invMassA == 0.f ? -c.A : c.A;
+        out->bodyBPtrAndSignBit = c.invMassB == 0.f ? -c.B : c.B;
+        manifoldFlag[p] = 1u;
+    }
+}
+
+// Stage 2 by lane groups over the clip queue: four pairs per warp per work
+// grab, lane l < 4 prefetching group l's pair. Pairs the groups cannot hold
+// go to deferQ for k_np_clip.
+template <bool kSub>
+__global__ void __launch_bounds__(128, 4)
+k_np_clip_groups(const int2* __restrict__ pairs, const int4* __restrict__ subs, b3::BodiesDev Bd, b3::ShapesDev S,
+                 NpParams P, float4* __restrict__ pairSep, const int* __restrict__ fastQ, int* __restrict__ slowQ,
+                 int* __restrict__ deferQ, b3Contact4* __restrict__ contacts, uint32_t* __restrict__ manifoldFlag,
+                 int32_t* __restrict__ scalars) {
+    extern __shared__ __align__(16) unsigned char np_smem[];
+    constexpr int kPerWarp = 32 / kClipGroup;
+    const int lane = threadIdx.x & 31;
+    GroupScratch* Wg = reinterpret_cast<GroupScratch*>(np_smem) + (threadIdx.x >> 5) * kPerWarp;
+    const int g = lane / kClipGroup;
+    const int gl = grp_lane();
+    const unsigned gm = grp_mask();
+    GroupScratch& W = Wg[g];
+    const int nFast = scalars[b3::S_NP_FAST];
+    for (;;) {
+        const int chunk = next_work(scalars + b3::S_NP_WORK2, nFast, kPerWarp);
+        if (chunk < 0) break;
+        const int n = min(kPerWarp, nFast - chunk);
+        if (lane < n) {
+            const int p = fastQ[chunk + lane];
+            item_prefetch<kSub>(Wg[lane].pre, p, pairs, subs, scalars[b3::S_NUM_PAIRS], Bd, S);
+            Wg[lane].pre.aux = pairSep[p];
+        }
+        __syncwarp();
+        if (g < n) {
+            const int p = W.pre.p;
+            PairCtx& c = W.ctx;
+            {
+                PairCtx t;
+                pair_from_pre(t, W.pre, S);
+                __syncwarp(gm);
+                if (gl == 0) c = t;
+                __syncwarp(gm);
+            }
+            const float4 s4 = W.pre.aux;
+            const float3 sepf = make_float3(s4.x, s4.y, s4.z);
+            bool faceTie = false;
+            const int bi = select_face_g(S, c, false, sepf, -1.f, &faceTie);
+            const int ai = select_face_g(S, c, true, sepf, 1.f, &faceTie);
+            int buf = 0;
+            bool slow = false, defer = false;
+            int nOut = 0;
+            if (!faceTie && ref_face_clips(S, c, ai)) nOut = clip_f32_g(c, S, P, ai, bi, W, &buf, &slow, &defer);
+            int4 idx = make_int4(0, 1, 2, 3);
+            int nRed = nOut;
+            bool tie = false;
+            if (!defer && !faceTie && !slow && nOut > 4) {
+                idx = reduce_f32_g(W.poly[buf], nOut, -sepf, &tie);
+                nRed = 4;
+            }
+            if (defer) {
+                if (gl == 0) deferQ[atomicAdd(scalars + b3::S_NP_DEFER, 1)] = p;
+            } else if (faceTie || slow || tie) {
+                if (gl == 0) {
+                    pairSep[p].w = (float)(faceTie ? kSepFaceTie : kSepClipDoubt);
+                    slowQ[atomicAdd(scalars + b3::S_NP_SLOW, 1)] = p;
+                }
+            } else if (nOut > 0) {
+                emit_contact_g(p, c, W.poly[buf], nRed, idx, -sepf, Bd, P, contacts, manifoldFlag);
+            } else if (gl == 0) {
+                manifoldFlag[p] = 0u;
+            }
+        }
+        __syncwarp();
     }
 }
 
@@ -1989,10 +2390,12 @@ namespace b3 {
 // of compound and mesh pairs (kSub true).
 template <bool kSub>
 static int launch_np_stages(b3World_t* w, cudaStream_t st, const NpParams& P, bool early) {
-    // work counters and queue lengths S_NP_WORK .. S_NP_WORK4
+    // work counters and queue lengths S_NP_WORK .. S_NP_WORK4, S_NP_DEFER, S_NP_WORK5
     B3_CUDA(cudaMemsetAsync(w->d.scalars + S_NP_WORK, 0, sizeof(int32_t) * 6, st));
+    B3_CUDA(cudaMemsetAsync(w->d.scalars + S_NP_DEFER, 0, sizeof(int32_t) * 2, st));
     const int threads = 32 * w->npWarpsPerBlock;
     const size_t smem = sizeof(WarpScratch) * w->npWarpsPerBlock;
+    const size_t smemGroups = sizeof(GroupScratch) * (32 / kClipGroup) * w->npWarpsPerBlock;
     auto grid_of = [&](const void* k) -> int {
         int occ = 1;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, threads, smem) != cudaSuccess || occ < 1) occ = 1;
@@ -2019,10 +2422,26 @@ static int launch_np_stages(b3World_t* w, cudaStream_t st, const NpParams& P, bo
         sc, w->d.counters);
     B3_CHECK_LAUNCH();
     if (tk) B3_CUDA(cudaEventRecord(w->npEv[2], st));
-    k_np_clip<kSub><<<grid_of((const void*)k_np_clip<kSub>), threads, smem, st>>>(
-        w->d.pairs, w->d.subPairs, Bd, S, P, w->d.pairSep, w->d.npFast, w->d.npSlow, w->d.contacts,
-        w->d.manifoldFlag, sc, w->d.counters);
-    B3_CHECK_LAUNCH();
+    if (w->clipGroups) {
+        // lane groups over the clip queue; what they pass on, by warps
+        int occG = 1;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occG, k_np_clip_groups<kSub>, threads, smemGroups) !=
+                cudaSuccess || occG < 1)
+            occG = 1;
+        k_np_clip_groups<kSub><<<w->ctx->numSMs * occG, threads, smemGroups, st>>>(
+            w->d.pairs, w->d.subPairs, Bd, S, P, w->d.pairSep, w->d.npFast, w->d.npSlow, w->d.npDefer,
+            w->d.contacts, w->d.manifoldFlag, sc);
+        B3_CHECK_LAUNCH();
+        k_np_clip<kSub><<<grid_of((const void*)k_np_clip<kSub>), threads, smem, st>>>(
+            w->d.pairs, w->d.subPairs, Bd, S, P, w->d.pairSep, w->d.npDefer, S_NP_DEFER, S_NP_WORK5, w->d.npSlow,
+            w->d.contacts, w->d.manifoldFlag, sc, w->d.counters);
+        B3_CHECK_LAUNCH();
+    } else {
+        k_np_clip<kSub><<<grid_of((const void*)k_np_clip<kSub>), threads, smem, st>>>(
+            w->d.pairs, w->d.subPairs, Bd, S, P, w->d.pairSep, w->d.npFast, S_NP_FAST, S_NP_WORK2, w->d.npSlow,
+            w->d.contacts, w->d.manifoldFlag, sc, w->d.counters);
+        B3_CHECK_LAUNCH();
+    }
     if (tk) B3_CUDA(cudaEventRecord(w->npEv[3], st));
     k_np_exact<kSub><<<grid_of((const void*)k_np_exact<kSub>), threads, smem, st>>>(
         w->d.pairs, w->d.subPairs, Bd, S, P, w->d.pairSep, w->d.npSlow, w->d.npCand, w->d.contacts,
@@ -2060,6 +2479,14 @@ int launch_narrowphase(b3World_t* w, cudaStream_t st) {
         B3_CUDA(cudaFuncSetAttribute(k_np_clip<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         B3_CUDA(cudaFuncSetAttribute(k_np_exact<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         B3_CUDA(cudaFuncSetAttribute(k_np_refine<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+    const size_t smemGroups = sizeof(GroupScratch) * (32 / kClipGroup) * w->npWarpsPerBlock;
+    if (smemGroups > 48 * 1024 && (size_t)w->npGroupSmemAttr < smemGroups) {
+        w->npGroupSmemAttr = (int)smemGroups;
+        B3_CUDA(cudaFuncSetAttribute(k_np_clip_groups<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smemGroups));
+        B3_CUDA(cudaFuncSetAttribute(k_np_clip_groups<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smemGroups));
     }
     {
         B3_TRY(launch_np_stages<false>(w, st, P, early));

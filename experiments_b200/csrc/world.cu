@@ -72,7 +72,7 @@ void free_all(b3::DevBuffers& d) {
                     d.invInertia, d.collidable, d.worldId, d.cols, d.polys, d.verts, d.faces,
                     d.indices, d.edges, d.localAabb, d.polyInradius, d.childShapes, d.vpXY, d.vpZ, d.polyPack, d.subPairs, d.subCount, d.subOffset, d.aabbMin, d.aabbMax, d.smallSlot,
                     d.largeStart, d.largeList, d.sapSmall, d.sapLarge, d.sapSorted, d.sapCount, d.sapOffset, d.keys, d.vals, d.keysAlt, d.valsAlt, d.cellTable,
-                    d.pairs, d.contacts, d.manifoldFlag, d.pairSep, d.npFast, d.npSlow, d.npCand, d.manifoldScan,
+                    d.pairs, d.contacts, d.manifoldFlag, d.pairSep, d.npFast, d.npSlow, d.npDefer, d.npCand, d.manifoldScan,
                     d.manifoldPair,
                     d.incKeys, d.incVals, d.incKeysAlt, d.incValsAlt, d.bodyIncStart,
                     d.bodyIncEnd, d.rows, d.manifoldHdr, d.incLin, d.incAng, d.avgLin, d.avgAng,
@@ -674,6 +674,7 @@ static int ensure_capacity(b3World w) {
         B3_TRY(dalloc(d.pairSep, c));
         B3_TRY(dalloc(d.npFast, c));
         B3_TRY(dalloc(d.npSlow, c));
+        B3_TRY(dalloc(d.npDefer, c));
         B3_TRY(dalloc(d.npCand, (size_t)std::min<size_t>(c, b3::kNpCandSlots) * 32));
         B3_TRY(dalloc(d.manifoldScan, c));
         B3_TRY(dalloc(d.manifoldPair, c));
@@ -1398,14 +1399,16 @@ extern "C" int b3_autotune(b3World w, int trialSteps, void* stream) {
     };
     struct Knob {
         int* v;
+        int n;
         int cand[3];
     };
-    // the narrowphase CTA size by whole-step trials; with the batched
-    // Gauss-Seidel solver also its grid width (solverMode). The Jacobi
-    // launch shapes interact (a one-knob-at-a-time descent stops in a
-    // local optimum), so they are searched jointly below on the solve alone.
-    Knob knobs[] = {{&w->npWarpsPerBlock, {1, 2, 4}}, {&w->solverMode, {0, 1, 0}}};
-    const int numKnobs = w->gs ? 2 : 1;
+    // the narrowphase CTA size and the FP32 clip form by whole-step trials;
+    // with the batched Gauss-Seidel solver also its grid width (solverMode).
+    // The Jacobi launch shapes interact (a one-knob-at-a-time descent stops
+    // in a local optimum), so they are searched jointly below on the solve
+    // alone.
+    Knob knobs[] = {{&w->npWarpsPerBlock, 3, {1, 2, 4}}, {&w->clipGroups, 2, {0, 1, 0}}, {&w->solverMode, 2, {0, 1, 0}}};
+    const int numKnobs = w->gs ? 3 : 2;
     // one solve from the current contacts, timed (the solve leaves the body
     // state alone: the finish happens in the integration)
     auto solve_trial = [&](float* ms) -> int {
@@ -1445,7 +1448,8 @@ extern "C" int b3_autotune(b3World w, int trialSteps, void* stream) {
             Knob& kb = knobs[ki];
             int best = *kb.v;
             float bestMs = 1e30f;
-            for (int c : kb.cand) {
+            for (int ci = 0; ci < kb.n; ++ci) {
+                const int c = kb.cand[ci];
                 *kb.v = c;
                 float ms = 0.f;
                 if ((rc = trial(&ms)) != B3_OK) break;
@@ -1524,8 +1528,10 @@ extern "C" int b3_set_tuning(b3World w, const int* values, int count) {
     const int mode = count >= 7 ? values[6] : w->solverMode;
     const int gather = count >= 8 ? values[7] : w->solverGather;
     const int pairMode = count >= 9 ? values[8] : w->pairSearchMode;
+    const int clipG = count >= 10 ? values[9] : w->clipGroups;
     if ((np != 1 && np != 2 && np != 4) || (st != 64 && st != 128 && st != 256) || cap < 1 || cap > 8 ||
-        (mode != 0 && mode != 1) || (gather != 0 && gather != 1) || (pairMode != 0 && pairMode != 1))
+        (mode != 0 && mode != 1) || (gather != 0 && gather != 1) || (pairMode != 0 && pairMode != 1) ||
+        (clipG != 0 && clipG != 1))
         return B3_ERR_INVALID_ARG;
     w->npWarpsPerBlock = np;
     w->solverThreads = st;
@@ -1533,16 +1539,17 @@ extern "C" int b3_set_tuning(b3World w, const int* values, int count) {
     w->solverMode = mode;
     w->solverGather = gather;
     w->pairSearchMode = pairMode;
+    w->clipGroups = clipG;
     w->graphValid = false;
     return B3_OK;
 }
 
 extern "C" int b3_get_tuning(b3World w, int* values, int max, int* count) {
     if (!w || !count) return B3_ERR_INVALID_ARG;
-    int v[9] = {w->npWarpsPerBlock, w->pairThreads, w->solverThreads, w->kernelsPerStep, w->solverOccCap,
-                w->tunedTrials, w->solverMode, w->solverGather, w->pairSearchMode};
-    *count = 9;
-    for (int i = 0; i < std::min(9, max); ++i) values[i] = v[i];
+    int v[10] = {w->npWarpsPerBlock, w->pairThreads, w->solverThreads, w->kernelsPerStep, w->solverOccCap,
+                 w->tunedTrials, w->solverMode, w->solverGather, w->pairSearchMode, w->clipGroups};
+    *count = 10;
+    for (int i = 0; i < std::min(10, max); ++i) values[i] = v[i];
     return B3_OK;
 }
 
