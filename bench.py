@@ -92,10 +92,10 @@ def fp32_peak_tflops(sm_mhz):
 # and DRAM bytes (read + write), per pair or per manifold.
 NCU_SOURCE = "ncu capture of the settled 16,384-body mixed-hull step (profiles/)"
 NCU_PER_UNIT = {
-    "k_np_sweep": {"fp32_ops_per_pair": 25977.0, "dram_bytes_per_pair": 13.1, "source": NCU_SOURCE},
-    "k_np_clip": {"fp32_ops_per_manifold": 8889.0, "dram_bytes_per_manifold": 105.0, "source": NCU_SOURCE},
-    "k_setup_rows": {"dram_bytes_per_manifold": 290.4, "source": NCU_SOURCE},
-    "k_jacobi": {"dram_bytes_per_manifold": 605.0, "source": NCU_SOURCE},
+    "k_np_sweep": {"fp32_ops_per_pair": 26729.0, "dram_bytes_per_pair": 13.2, "source": NCU_SOURCE},
+    "k_np_clip": {"fp32_ops_per_manifold": 4740.0, "dram_bytes_per_manifold": 106.8, "source": NCU_SOURCE},
+    "k_setup_rows": {"dram_bytes_per_manifold": 301.3, "source": NCU_SOURCE},
+    "k_jacobi": {"dram_bytes_per_manifold": 618.5, "source": NCU_SOURCE},
 }
 
 
@@ -699,6 +699,9 @@ def kernel_roofline(name, ms, sc, counters, key_bits, body_bits, hbm_peak, peak_
         dram = c.get("dram_bytes_per_" + unit)
         r["traffic"] = dram * count if dram is not None else None
         r["traffic_source"] = c.get("source") if dram is not None else None
+        if name == "k_np_clip":
+            r["launches"] = ("the FP32 clip stage: k_np_clip_groups (eight-lane groups) when the tuning selects it, "
+                             "then k_np_clip on the pairs it passes on")
         return r
     b = hbm_bytes.get(name)
     r = {"kernel": name, "bound": "hbm", "unit": "GB/s", "peak": hbm_peak, "ms": ms, "peak_kind": peak_kind}
