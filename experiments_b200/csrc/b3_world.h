@@ -102,6 +102,8 @@ struct DevBuffers {
     int* npFast = nullptr;            // queue: pairs whose axis the FP32 sweep decided
     int* npSlow = nullptr;            // queue: pairs for the float-float path
     int* npDefer = nullptr;           // queue: clip pairs the lane groups pass to the warp clip
+    int* npDefer2 = nullptr;          // queue: slow-queue positions for the warp float-float stage
+    int* npDefer3 = nullptr;          // queue: slow-queue positions for the warp ranking
     int* npCand = nullptr;            // near-minimum axes of queued pairs (kNpCandSlots x 32)
     uint32_t* manifoldScan = nullptr; // exclusive scan of the flags
     int* manifoldPair = nullptr;      // manifold -> pair slot
@@ -161,6 +163,10 @@ enum ScalarSlot {
     S_SUB_TOTAL = 17,     // sub-pairs before the capacity cut
     S_NP_DEFER = 18,      // clip-queue pairs the lane-group clip passed to the warp clip
     S_NP_WORK5 = 19,
+    S_NP_DEFER2 = 20,     // slow-queue positions the lane-group float-float clip passed to k_np_exact
+    S_NP_WORK6 = 21,
+    S_NP_DEFER3 = 22,     // slow-queue positions the lane-group ranking passed to k_np_refine
+    S_NP_WORK7 = 23,
     S_NUM_SCALARS = 24
 };
 
@@ -229,6 +235,7 @@ struct b3World_t {
     int tunedTrials = 0;       // configurations the autotuner timed
     int npSmemAttr = 0;        // dynamic shared memory attribute set on the narrowphase kernels
     int npGroupSmemAttr = 0;   // the same for the lane-group clip
+    int npFFSmemAttr = 0;      // and for the lane-group float-float stages
 
     int cooperativeOk = 1;
 

@@ -2037,6 +2037,420 @@ k_np_clip_groups(const int2* __restrict__ pairs, const int4* __restrict__ subs, 
     }
 }
 
+// ---------------------------------------------------------------------------
+// The float-float stages by lane groups, as the FP32 clip above: the ranking
+// of a pair's near-tied axes (at most kClipGroup candidates, one per lane)
+// and the float-float clip of a pair whose FP32 clip was in doubt. Each pair
+// gets the warp kernels' bits (the same per-candidate, per-vertex and
+// per-point arithmetic; order-independent reductions; compactions in the
+// sequential order). Pairs outside the group tables (more candidates, faces
+// or clipped points than they hold, or clip faces tied along the FP32 axis,
+// whose axis the full search must redo) are passed to the warp kernels.
+// ---------------------------------------------------------------------------
+struct __align__(16) GroupScratchFF {
+    FfVert poly[2][kGroupPoly];   // clip polygons; the ranking's staged vertices
+    FfVert planes[kGroupPoly];    // float-float side planes
+    PairCtx ctx;
+    int cand[kClipGroup];
+};
+
+__device__ __forceinline__ void ensure_ff_g(PairCtx& c, unsigned gm) {
+    const bool have = c.haveFF;
+    __syncwarp(gm);
+    if (!have) {
+        const ffmat a = quat_mat(c.qA), b = quat_mat(c.qB);
+        if (grp_lane() == 0) {
+            c.FA = a;
+            c.FB = b;
+            c.haveFF = true;
+        }
+        __syncwarp(gm);
+    }
+}
+
+// (hi, lo, index) minimum over the group, as warp_argmin_ff
+__device__ __forceinline__ void grp_argmin_ff(ff& v, int& idx, unsigned m) {
+    const int kh = fkey(v.hi, kNanMin);
+    const int mh = __reduce_min_sync(m, kh);
+    const int kl = kh == mh ? fkey(v.lo, kNanMin) : kNanMin;
+    const int ml = __reduce_min_sync(m, kl);
+    idx = (int)__reduce_min_sync(m, kh == mh && kl == ml ? (unsigned)idx : 0xffffffffu);
+    v.hi = fkey_inv(mh);
+    v.lo = fkey_inv(ml);
+}
+
+// PairCtx of item p into the group's shared context (every lane computes,
+// the group leader stores)
+template <bool kSub>
+__device__ __forceinline__ void item_setup_group(PairCtx& c, int p, const int2* __restrict__ pairs,
+                                                 const int4* __restrict__ subs, int base, const b3::BodiesDev& Bd,
+                                                 const b3::ShapesDev& S, unsigned gm) {
+    PairPre q;
+    item_prefetch<kSub>(q, p, pairs, subs, base, Bd, S);
+    PairCtx t;
+    pair_from_pre(t, q, S);
+    __syncwarp(gm);
+    if (grp_lane() == 0) {
+        c.A = t.A;
+        c.B = t.B;
+        c.invMassA = t.invMassA;
+        c.invMassB = t.invMassB;
+        c.pa = t.pa;
+        c.pb = t.pb;
+        c.qA = t.qA;
+        c.qB = t.qB;
+        c.RA = t.RA;
+        c.RB = t.RB;
+        c.haveFF = false;
+        c.posA = t.posA;
+        c.posB = t.posB;
+    }
+    __syncwarp(gm);
+}
+
+// refine_axes over the group, count <= kClipGroup candidates in W.cand
+__device__ __noinline__ bool refine_axes_g(PairCtx& c, const b3::ShapesDev& S, GroupScratchFF& W, int count,
+                                           ff3& sep) {
+    const int gl = grp_lane();
+    const unsigned gm = grp_mask();
+    const b3ConvexPolyhedron& pa = *c.pa;
+    const b3ConvexPolyhedron& pb = *c.pb;
+    const float3 lcA = make_float3(pa.localCenter[0], pa.localCenter[1], pa.localCenter[2]);
+    const float3 lcB = make_float3(pb.localCenter[0], pb.localCenter[1], pb.localCenter[2]);
+    ensure_ff_g(c, gm);
+    const ff3 lcAw = mrot(c.FA, make_float3(lcA.x, lcA.y, lcA.z));
+    const ff3 lcBw = mrot(c.FB, make_float3(lcB.x, lcB.y, lcB.z));
+    const ff3 Dff = sub3(add3(lcAw, mk3(c.posA.x, c.posA.y, c.posA.z)), add3(lcBw, mk3(c.posB.x, c.posB.y, c.posB.z)));
+    const float4* vA = S.verts + pa.vertexOffset;
+    const float4* vB = S.verts + pb.vertexOffset;
+    constexpr int kStage = (int)(sizeof(W.poly) / sizeof(float4));
+    if (pa.numVertices + pb.numVertices <= kStage) {
+        float4* st = reinterpret_cast<float4*>(&W.poly[0][0]);
+        for (int k = gl; k < pa.numVertices; k += kClipGroup) st[k] = __ldg(&vA[k]);
+        for (int k = gl; k < pb.numVertices; k += kClipGroup) st[pa.numVertices + k] = __ldg(&vB[k]);
+        __syncwarp(gm);
+        vA = st;
+        vB = st + pa.numVertices;
+    }
+    ff bd = mk(FLT_MAX);
+    int bidx = kNone;
+    ff3 bn = mk3(0.f, 0.f, 0.f);
+    bool fsep = false;
+    if (gl < count) {
+        const int idx = W.cand[gl];
+        ff3 n;
+        ff d;
+        bool isFace;
+        if (axis_ff(c, S, vA, vB, idx, Dff, n, d, isFace)) {
+            if (isFace && d.hi < 0.f) fsep = true;
+            bd = d;
+            bidx = idx;
+            bn = n;
+        }
+    }
+    if (__any_sync(gm, fsep)) return false;
+    ff wd = bd;
+    int widx = bidx;
+    grp_argmin_ff(wd, widx, gm);
+    if (widx == kNone) return false;
+    widx = (int)__reduce_min_sync(gm, bidx != kNone && sub(bd, wd).hi <= kAxisTieTol ? (unsigned)bidx : 0xffffffffu);
+    const unsigned who = __ballot_sync(gm, bidx == widx);
+    const int src = __ffs(who) - 1;
+    sep.x.hi = __shfl_sync(gm, bn.x.hi, src);
+    sep.x.lo = __shfl_sync(gm, bn.x.lo, src);
+    sep.y.hi = __shfl_sync(gm, bn.y.hi, src);
+    sep.y.lo = __shfl_sync(gm, bn.y.lo, src);
+    sep.z.hi = __shfl_sync(gm, bn.z.hi, src);
+    sep.z.lo = __shfl_sync(gm, bn.z.lo, src);
+    if (dot3(neg3(Dff), sep).hi > 0.f) sep = neg3(sep);
+    return true;
+}
+
+// clip_poly_ff over the group; *over when the output exceeds kGroupPoly
+__device__ __noinline__ int clip_poly_ff_g(const FfVert* in, int nin, const FfVert& plane, FfVert* out, bool* over) {
+    const int gl = grp_lane();
+    const unsigned gm = grp_mask();
+    const ff3 pn = vget(plane);
+    const ff eq = wget(plane);
+    int total = 0;
+    for (int base = 0; base < nin; base += kClipGroup) {
+        const int ve = base + gl;
+        const int sv = ve == 0 ? nin - 1 : ve - 1;
+        ff3 e = mk3(0.f, 0.f, 0.f), s = e;
+        ff de = mk(0.f);
+        if (ve < nin) {
+            e = vget(in[ve]);
+            s = vget(in[sv]);
+            de = add(dot3(pn, e), eq);
+        }
+        ff ds;
+        ds.hi = __shfl_up_sync(gm, de.hi, 1, kClipGroup);
+        ds.lo = __shfl_up_sync(gm, de.lo, 1, kClipGroup);
+        if (ve < nin && gl == 0) ds = add(dot3(pn, s), eq);
+        int cnt = 0;
+        ff3 o0 = mk3(0.f, 0.f, 0.f), o1 = o0;
+        if (ve < nin) {
+            const bool sNeg = ds.hi < 0.f, eNeg = de.hi < 0.f;
+            if (sNeg || eNeg) {
+                if (sNeg && eNeg) {
+                    o0 = e;
+                    cnt = 1;
+                } else {
+                    const ff t = div(ds, sub(ds, de));
+                    o0 = add3(s, scale3(sub3(e, s), t));
+                    cnt = 1;
+                    if (!sNeg) {
+                        o1 = e;
+                        cnt = 2;
+                    }
+                }
+            }
+        }
+        const unsigned b1 = __ballot_sync(gm, cnt >= 1), b2 = __ballot_sync(gm, cnt == 2);
+        const unsigned below = b3dev::lanemask_lt();
+        const int pos = total + __popc(b1 & below) + __popc(b2 & below);
+        if (cnt >= 1 && pos < kGroupPoly) out[pos] = vput(o0, mk(0.f));
+        if (cnt == 2 && pos + 1 < kGroupPoly) out[pos + 1] = vput(o1, mk(0.f));
+        total += __popc(b1) + __popc(b2);
+    }
+    __syncwarp(gm);
+    if (total > kGroupPoly) *over = true;
+    return min(total, kGroupPoly);
+}
+
+// clip_hull_hull over the group; *over: a face or the clipped polygon
+// exceeds the group's tables (nothing decided)
+__device__ __noinline__ int clip_hull_hull_g(PairCtx& c, const b3::ShapesDev& S, const NpParams& P, ff3 sep, int ai,
+                                             int bi, GroupScratchFF& W, int* outBuf, bool* over) {
+    const unsigned gm = grp_mask();
+    ensure_ff_g(c, gm);
+    const int gl = grp_lane();
+    const b3ConvexPolyhedron& pa = *c.pa;
+    const b3ConvexPolyhedron& pb = *c.pb;
+    if (ai == kNone || bi == kNone) return 0;
+    const b3Face fB = S.faces[pb.faceOffset + bi];
+    const b3Face fA = S.faces[pa.faceOffset + ai];
+    const ff3 posA = mk3(c.posA.x, c.posA.y, c.posA.z);
+    const ff3 posB = mk3(c.posB.x, c.posB.y, c.posB.z);
+    int nIn = min(fB.numIndices, kMaxPoly);
+    const int nvA = min(fA.numIndices, kMaxPoly);
+    if (nIn > kGroupPoly || nvA > kGroupPoly) {
+        *over = true;
+        return 0;
+    }
+    for (int k = gl; k < nIn; k += kClipGroup) {
+        const float4 v = __ldg(&S.verts[pb.vertexOffset + S.indices[fB.indexOffset + k]]);
+        W.poly[0][k] = vput(add3(mrot(c.FB, make_float3(v.x, v.y, v.z)), posB), mk(0.f));
+    }
+    __syncwarp(gm);
+    int cur = 0;
+    const ff3 nAw = mrot(c.FA, make_float3(fA.plane[0], fA.plane[1], fA.plane[2]));
+    for (int e0 = gl; e0 < nvA; e0 += kClipGroup) {
+        const float4 a = __ldg(&S.verts[pa.vertexOffset + S.indices[fA.indexOffset + e0]]);
+        const float4 b = __ldg(&S.verts[pa.vertexOffset + S.indices[fA.indexOffset + (e0 + 1) % fA.numIndices]]);
+        const ff3 edge = sub3(mk3(a.x, a.y, a.z), mk3(b.x, b.y, b.z));
+        const ff3 we{add(add(mul(c.FA.m[0][0], edge.x), mul(c.FA.m[0][1], edge.y)), mul(c.FA.m[0][2], edge.z)),
+                     add(add(mul(c.FA.m[1][0], edge.x), mul(c.FA.m[1][1], edge.y)), mul(c.FA.m[1][2], edge.z)),
+                     add(add(mul(c.FA.m[2][0], edge.x), mul(c.FA.m[2][1], edge.y)), mul(c.FA.m[2][2], edge.z))};
+        const ff3 pn = neg3(cross3(we, nAw));
+        const ff3 wa = add3(mrot(c.FA, make_float3(a.x, a.y, a.z)), posA);
+        W.planes[e0] = vput(pn, neg(dot3(wa, pn)));
+    }
+    __syncwarp(gm);
+    for (int e0 = 0; e0 < nvA && !*over; ++e0) {
+        nIn = clip_poly_ff_g(W.poly[cur], nIn, W.planes[e0], W.poly[cur ^ 1], over);
+        cur ^= 1;
+    }
+    if (*over) return 0;
+    const ff eqA = sub(mk(fA.plane[3]), dot3(nAw, posA));
+    const ff minD = mk(P.minDist), maxD = mk(P.maxDist);
+    int total = 0;
+    for (int base = 0; base < nIn; base += kClipGroup) {
+        const int k = base + gl;
+        bool keep = false;
+        ff3 p = mk3(0.f, 0.f, 0.f);
+        ff depth = mk(0.f);
+        if (k < nIn) {
+            p = vget(W.poly[cur][k]);
+            depth = add(dot3(nAw, p), eqA);
+            if (le(depth, minD)) depth = minD;
+            keep = le(depth, maxD);
+        }
+        const unsigned m = __ballot_sync(gm, keep);
+        const int pos = total + __popc(m & b3dev::lanemask_lt());
+        if (keep) W.poly[cur ^ 1][pos] = vput(p, depth);
+        total += __popc(m);
+    }
+    __syncwarp(gm);
+    *outBuf = cur ^ 1;
+    return total;
+}
+
+// reduce_manifold over the group
+__device__ __noinline__ int4 reduce_manifold_g(const FfVert* p, int n, ff3 nearNormal) {
+    const int gl = grp_lane();
+    const unsigned gm = grp_mask();
+    ff3 s = mk3(0.f, 0.f, 0.f);
+    for (int k = 0; k < n; ++k) s = add3(s, vget(p[k]));
+    const ff invn = div(mk(1.f), mk((float)n));
+    const ff3 center = scale3(s, invn);
+    const ff3 aV = sub3(vget(p[0]), center);
+    ff3 u = cross3(nearNormal, aV);
+    ff3 v = cross3(nearNormal, u);
+    u = normalize3(u);
+    v = normalize3(v);
+    ff mw = mk(FLT_MAX), f0 = mk(FLT_MIN), f1 = mk(FLT_MIN), f2 = mk(FLT_MIN), f3v = mk(FLT_MIN);
+    int iw = kNone, i0 = kNone, i1 = kNone, i2 = kNone, i3 = kNone;
+    for (int k = gl; k < n; k += kClipGroup) {
+        const ff w = wget(p[k]);
+        if (lt(w, mw)) { mw = w; iw = k; }
+        const ff3 r = sub3(vget(p[k]), center);
+        const ff du = dot3(u, r), dv = dot3(v, r);
+        if (lt(du, f0)) { f0 = du; i0 = k; }
+        if (lt(neg(du), f1)) { f1 = neg(du); i1 = k; }
+        if (lt(dv, f2)) { f2 = dv; i2 = k; }
+        if (lt(neg(dv), f3v)) { f3v = neg(dv); i3 = k; }
+    }
+    grp_argmin_ff(mw, iw, gm);
+    grp_argmin_ff(f0, i0, gm);
+    grp_argmin_ff(f1, i1, gm);
+    grp_argmin_ff(f2, i2, gm);
+    grp_argmin_ff(f3v, i3, gm);
+    int4 idx = make_int4(i0 == kNone ? 0 : i0, i1 == kNone ? 1 : i1, i2 == kNone ? 2 : i2, i3 == kNone ? 3 : i3);
+    const int minIndex = iw == kNone ? -1 : iw;
+    if (idx.x != minIndex && idx.y != minIndex && idx.z != minIndex && idx.w != minIndex) idx.x = minIndex;
+    return idx;
+}
+
+// Stage 1b by lane groups: the sweep's near-tie entries with at most
+// kClipGroup stored candidates; the others (slow-queue positions) go to
+// deferQ for k_np_refine.
+template <bool kSub>
+__global__ void __launch_bounds__(128, 4)
+k_np_refine_groups(const int2* __restrict__ pairs, const int4* __restrict__ subs, b3::BodiesDev Bd, b3::ShapesDev S,
+                   float4* __restrict__ pairSep, int* __restrict__ fastQ, int* __restrict__ slowQ,
+                   const int* __restrict__ cand, int* __restrict__ deferQ, uint32_t* __restrict__ manifoldFlag,
+                   int32_t* __restrict__ scalars, b3Counters* __restrict__ counters) {
+    extern __shared__ __align__(16) unsigned char np_smem[];
+    constexpr int kPerWarp = 32 / kClipGroup;
+    const int lane = threadIdx.x & 31;
+    const int g = lane / kClipGroup;
+    const int gl = grp_lane();
+    const unsigned gm = grp_mask();
+    GroupScratchFF& W = reinterpret_cast<GroupScratchFF*>(np_smem)[(threadIdx.x >> 5) * kPerWarp + g];
+    const int nSlow = scalars[b3::S_NP_SLOW];  // the sweep's entries: the clip has not run
+    int refined = 0;
+    for (;;) {
+        const int chunk = next_work(scalars + b3::S_NP_WORK4, nSlow, kPerWarp);
+        if (chunk < 0) break;
+        const int q = chunk + g;
+        if (q < nSlow) {
+            const int p = slowQ[q];
+            const float4 s4 = pairSep[p];
+            const int count = __float_as_int(s4.x);
+            if ((int)s4.w == kSepRefine && count > 0) {
+                if (count > kClipGroup) {
+                    if (gl == 0) deferQ[atomicAdd(scalars + b3::S_NP_DEFER3, 1)] = q;
+                } else {
+                    PairCtx& c = W.ctx;
+                    item_setup_group<kSub>(c, p, pairs, subs, scalars[b3::S_NUM_PAIRS], Bd, S, gm);
+                    if (gl < count) W.cand[gl] = cand[(size_t)q * kMaxCand + gl];
+                    __syncwarp(gm);
+                    ff3 sep = mk3(0.f, 0.f, 0.f);
+                    const bool haveAxis = refine_axes_g(c, S, W, count, sep);
+                    ++refined;
+                    if (gl == 0) {
+                        slowQ[q] = -1;
+                        if (haveAxis) {
+                            const float3 sf = to_f3(sep);
+                            pairSep[p] = make_float4(sf.x, sf.y, sf.z, (float)kSepDecided);
+                            fastQ[atomicAdd(scalars + b3::S_NP_FAST, 1)] = p;
+                        } else {
+                            manifoldFlag[p] = 0u;
+                        }
+                    }
+                }
+            }
+        }
+        __syncwarp();
+    }
+    if (gl == 0 && refined) atomicAdd(&counters->refinedAxes, refined);
+}
+
+// Stage 3 by lane groups: slow-queue entries whose FP32 clip was in doubt
+// (the axis is the sweep's FP32 axis) get the float-float clip and
+// reduction here; every other entry (slow-queue position) goes to deferQ
+// for k_np_exact.
+template <bool kSub>
+__global__ void __launch_bounds__(128, 4)
+k_np_exact_groups(const int2* __restrict__ pairs, const int4* __restrict__ subs, b3::BodiesDev Bd, b3::ShapesDev S,
+                  NpParams P, const float4* __restrict__ pairSep, const int* __restrict__ slowQ,
+                  int* __restrict__ deferQ, b3Contact4* __restrict__ contacts, uint32_t* __restrict__ manifoldFlag,
+                  int32_t* __restrict__ scalars, b3Counters* __restrict__ counters) {
+    extern __shared__ __align__(16) unsigned char np_smem[];
+    constexpr int kPerWarp = 32 / kClipGroup;
+    const int lane = threadIdx.x & 31;
+    const int g = lane / kClipGroup;
+    const int gl = grp_lane();
+    const unsigned gm = grp_mask();
+    GroupScratchFF& W = reinterpret_cast<GroupScratchFF*>(np_smem)[(threadIdx.x >> 5) * kPerWarp + g];
+    const int nSlow = scalars[b3::S_NP_SLOW];
+    int clips = 0;
+    for (;;) {
+        const int chunk = next_work(scalars + b3::S_NP_WORK3, nSlow, kPerWarp);
+        if (chunk < 0) break;
+        const int q = chunk + g;
+        if (q < nSlow) {
+            const int p = slowQ[q];
+            if (p >= 0) {
+                const float4 s4 = pairSep[p];
+                bool defer = (int)s4.w != kSepClipDoubt;
+                if (!defer) {
+                    PairCtx& c = W.ctx;
+                    item_setup_group<kSub>(c, p, pairs, subs, scalars[b3::S_NUM_PAIRS], Bd, S, gm);
+                    const ff3 sep = mk3(s4.x, s4.y, s4.z);
+                    const float3 sepf = to_f3(sep);
+                    bool faceTie = false;
+                    const int bi = select_face_g(S, c, false, sepf, -1.f, &faceTie);
+                    const int ai = select_face_g(S, c, true, sepf, 1.f, &faceTie);
+                    defer = faceTie;
+                    if (!defer) {
+                        int nOut = 0, buf = 0;
+                        bool over = false, clipped = false;
+                        if (ref_face_clips(S, c, ai)) {
+                            nOut = clip_hull_hull_g(c, S, P, sep, ai, bi, W, &buf, &over);
+                            clipped = true;
+                        }
+                        if (over) {
+                            defer = true;
+                        } else {
+                            if (clipped) ++clips;
+                            if (nOut > 0) {
+                                const FfVert* pts = W.poly[buf];
+                                const ff3 nrm = neg3(sep);
+                                int4 idx = make_int4(0, 1, 2, 3);
+                                int nRed = nOut;
+                                if (nOut > 4) {
+                                    bool tie = false;
+                                    idx = reduce_f32_g(pts, nOut, to_f3(nrm), &tie);
+                                    if (tie) idx = reduce_manifold_g(pts, nOut, nrm);
+                                    nRed = 4;
+                                }
+                                emit_contact_g(p, c, pts, nRed, idx, to_f3(nrm), Bd, P, contacts, manifoldFlag);
+                            } else if (gl == 0) {
+                                manifoldFlag[p] = 0u;
+                            }
+                        }
+                    }
+                }
+                if (defer && gl == 0) deferQ[atomicAdd(scalars + b3::S_NP_DEFER2, 1)] = q;
+            }
+        }
+        __syncwarp();
+    }
+    if (gl == 0 && clips) atomicAdd(&counters->refinedClips, clips);
+}
+
 // Stage 1b, the sweep's near-minimum pairs with stored candidates: the
 // float-float ranking of the candidates only. A pair with an axis then
 // joins the FP32 clip queue with that axis (rounded to FP32, as the contact
@@ -2048,15 +2462,19 @@ __global__ void __launch_bounds__(128, 4)
 k_np_refine(const int2* __restrict__ pairs, const int4* __restrict__ subs, b3::BodiesDev Bd, b3::ShapesDev S,
             float4* __restrict__ pairSep,
             int* __restrict__ fastQ, int* __restrict__ slowQ, const int* __restrict__ cand,
+            const int* __restrict__ idxQ, int countSlot, int workSlot,
             uint32_t* __restrict__ manifoldFlag, int32_t* __restrict__ scalars, b3Counters* __restrict__ counters) {
     extern __shared__ __align__(16) unsigned char np_smem[];
     const int lane = threadIdx.x & 31;
     WarpScratch& W = reinterpret_cast<WarpScratch*>(np_smem)[threadIdx.x >> 5];
-    const int nSlow = scalars[b3::S_NP_SLOW];  // the sweep's entries: the clip has not run
+    // the sweep's entries (the clip has not run), or the slow-queue
+    // positions in idxQ that the lane groups passed on
+    const int nSlow = scalars[idxQ ? countSlot : b3::S_NP_SLOW];
     int refined = 0;
     for (;;) {
-        const int q = next_work(scalars + b3::S_NP_WORK4, nSlow, 1);
-        if (q < 0) break;
+        const int i = next_work(scalars + workSlot, nSlow, 1);
+        if (i < 0) break;
+        const int q = idxQ ? idxQ[i] : i;
         const int p = slowQ[q];
         const float4 s4 = pairSep[p];
         const int count = __float_as_int(s4.x);
@@ -2090,12 +2508,14 @@ __global__ void __launch_bounds__(128, 4)
 k_np_exact(const int2* __restrict__ pairs, const int4* __restrict__ subs, b3::BodiesDev Bd, b3::ShapesDev S,
            NpParams P,
            const float4* __restrict__ pairSep, const int* __restrict__ slowQ, const int* __restrict__ cand,
-           b3Contact4* __restrict__ contacts,
+           const int* __restrict__ idxQ, int countSlot, int workSlot, b3Contact4* __restrict__ contacts,
            uint32_t* __restrict__ manifoldFlag, int32_t* __restrict__ scalars, b3Counters* __restrict__ counters) {
     extern __shared__ __align__(16) unsigned char np_smem[];
     const int lane = threadIdx.x & 31;
     WarpScratch& W = reinterpret_cast<WarpScratch*>(np_smem)[threadIdx.x >> 5];
-    const int nSlow = scalars[b3::S_NP_SLOW];
+    // every slow-queue entry, or the positions in idxQ that the lane groups
+    // passed on
+    const int nSlow = scalars[idxQ ? countSlot : b3::S_NP_SLOW];
     if (lane == 0) {
         W.refinedAxes = 0;
         W.refinedClips = 0;
@@ -2103,10 +2523,11 @@ k_np_exact(const int2* __restrict__ pairs, const int4* __restrict__ subs, b3::Bo
     __syncwarp();
     for (;;) {
         // one pair per grab: the queued pairs differ widely in cost
-        const int chunk = next_work(scalars + b3::S_NP_WORK3, nSlow, 1);
+        const int chunk = next_work(scalars + workSlot, nSlow, 1);
         if (chunk < 0) break;
         const int chunkEnd = min(chunk + 1, nSlow);
-        for (int q = chunk; q < chunkEnd; ++q) {
+        for (int i = chunk; i < chunkEnd; ++i) {
+            const int q = idxQ ? idxQ[i] : i;
             const int p = slowQ[q];
             if (p < 0) continue;  // settled by the ranking stage
             PairCtx& c = W.ctx;
@@ -2390,9 +2811,9 @@ namespace b3 {
 // of compound and mesh pairs (kSub true).
 template <bool kSub>
 static int launch_np_stages(b3World_t* w, cudaStream_t st, const NpParams& P, bool early) {
-    // work counters and queue lengths S_NP_WORK .. S_NP_WORK4, S_NP_DEFER, S_NP_WORK5
+    // work counters and queue lengths S_NP_WORK .. S_NP_WORK4, S_NP_DEFER .. S_NP_WORK7
     B3_CUDA(cudaMemsetAsync(w->d.scalars + S_NP_WORK, 0, sizeof(int32_t) * 6, st));
-    B3_CUDA(cudaMemsetAsync(w->d.scalars + S_NP_DEFER, 0, sizeof(int32_t) * 2, st));
+    B3_CUDA(cudaMemsetAsync(w->d.scalars + S_NP_DEFER, 0, sizeof(int32_t) * 6, st));
     const int threads = 32 * w->npWarpsPerBlock;
     const size_t smem = sizeof(WarpScratch) * w->npWarpsPerBlock;
     const size_t smemGroups = sizeof(GroupScratch) * (32 / kClipGroup) * w->npWarpsPerBlock;
@@ -2417,10 +2838,28 @@ static int launch_np_stages(b3World_t* w, cudaStream_t st, const NpParams& P, bo
         w->d.npSlow, w->d.npCand, std::min(w->cfg.maxPairs, kNpCandSlots), sc, w->d.counters);
     B3_CHECK_LAUNCH();
     if (tk) B3_CUDA(cudaEventRecord(w->npEv[1], st));
-    k_np_refine<kSub><<<grid_of((const void*)k_np_refine<kSub>), threads, smem, st>>>(
-        w->d.pairs, w->d.subPairs, Bd, S, w->d.pairSep, w->d.npFast, w->d.npSlow, w->d.npCand, w->d.manifoldFlag,
-        sc, w->d.counters);
-    B3_CHECK_LAUNCH();
+    const size_t smemFF = sizeof(GroupScratchFF) * (32 / kClipGroup) * w->npWarpsPerBlock;
+    auto grid_ff = [&](const void* k) -> int {
+        int occ = 1;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, threads, smemFF) != cudaSuccess || occ < 1) occ = 1;
+        return w->ctx->numSMs * occ;
+    };
+    if (w->clipGroups) {
+        // lane groups for the rankings of up to 8 candidates; the rest by warps
+        k_np_refine_groups<kSub><<<grid_ff((const void*)k_np_refine_groups<kSub>), threads, smemFF, st>>>(
+            w->d.pairs, w->d.subPairs, Bd, S, w->d.pairSep, w->d.npFast, w->d.npSlow, w->d.npCand, w->d.npDefer3,
+            w->d.manifoldFlag, sc, w->d.counters);
+        B3_CHECK_LAUNCH();
+        k_np_refine<kSub><<<grid_of((const void*)k_np_refine<kSub>), threads, smem, st>>>(
+            w->d.pairs, w->d.subPairs, Bd, S, w->d.pairSep, w->d.npFast, w->d.npSlow, w->d.npCand, w->d.npDefer3,
+            S_NP_DEFER3, S_NP_WORK7, w->d.manifoldFlag, sc, w->d.counters);
+        B3_CHECK_LAUNCH();
+    } else {
+        k_np_refine<kSub><<<grid_of((const void*)k_np_refine<kSub>), threads, smem, st>>>(
+            w->d.pairs, w->d.subPairs, Bd, S, w->d.pairSep, w->d.npFast, w->d.npSlow, w->d.npCand, nullptr, 0,
+            S_NP_WORK4, w->d.manifoldFlag, sc, w->d.counters);
+        B3_CHECK_LAUNCH();
+    }
     if (tk) B3_CUDA(cudaEventRecord(w->npEv[2], st));
     if (w->clipGroups) {
         // lane groups over the clip queue; what they pass on, by warps
@@ -2443,10 +2882,22 @@ static int launch_np_stages(b3World_t* w, cudaStream_t st, const NpParams& P, bo
         B3_CHECK_LAUNCH();
     }
     if (tk) B3_CUDA(cudaEventRecord(w->npEv[3], st));
-    k_np_exact<kSub><<<grid_of((const void*)k_np_exact<kSub>), threads, smem, st>>>(
-        w->d.pairs, w->d.subPairs, Bd, S, P, w->d.pairSep, w->d.npSlow, w->d.npCand, w->d.contacts,
-        w->d.manifoldFlag, sc, w->d.counters);
-    B3_CHECK_LAUNCH();
+    if (w->clipGroups) {
+        // lane groups for the float-float clips of FP32 clips in doubt; the rest by warps
+        k_np_exact_groups<kSub><<<grid_ff((const void*)k_np_exact_groups<kSub>), threads, smemFF, st>>>(
+            w->d.pairs, w->d.subPairs, Bd, S, P, w->d.pairSep, w->d.npSlow, w->d.npDefer2, w->d.contacts,
+            w->d.manifoldFlag, sc, w->d.counters);
+        B3_CHECK_LAUNCH();
+        k_np_exact<kSub><<<grid_of((const void*)k_np_exact<kSub>), threads, smem, st>>>(
+            w->d.pairs, w->d.subPairs, Bd, S, P, w->d.pairSep, w->d.npSlow, w->d.npCand, w->d.npDefer2, S_NP_DEFER2,
+            S_NP_WORK6, w->d.contacts, w->d.manifoldFlag, sc, w->d.counters);
+        B3_CHECK_LAUNCH();
+    } else {
+        k_np_exact<kSub><<<grid_of((const void*)k_np_exact<kSub>), threads, smem, st>>>(
+            w->d.pairs, w->d.subPairs, Bd, S, P, w->d.pairSep, w->d.npSlow, w->d.npCand, nullptr, 0, S_NP_WORK3,
+            w->d.contacts, w->d.manifoldFlag, sc, w->d.counters);
+        B3_CHECK_LAUNCH();
+    }
     if (tk) B3_CUDA(cudaEventRecord(w->npEv[4], st));
     return B3_OK;
 }
@@ -2487,6 +2938,13 @@ int launch_narrowphase(b3World_t* w, cudaStream_t st) {
                                      (int)smemGroups));
         B3_CUDA(cudaFuncSetAttribute(k_np_clip_groups<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smemGroups));
+    }
+    const size_t smemFF = sizeof(GroupScratchFF) * (32 / kClipGroup) * w->npWarpsPerBlock;
+    if (smemFF > 48 * 1024 && (size_t)w->npFFSmemAttr < smemFF) {
+        w->npFFSmemAttr = (int)smemFF;
+        for (const void* k : {(const void*)k_np_refine_groups<false>, (const void*)k_np_refine_groups<true>,
+                              (const void*)k_np_exact_groups<false>, (const void*)k_np_exact_groups<true>})
+            B3_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemFF));
     }
     {
         B3_TRY(launch_np_stages<false>(w, st, P, early));

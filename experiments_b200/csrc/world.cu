@@ -72,7 +72,7 @@ void free_all(b3::DevBuffers& d) {
                     d.invInertia, d.collidable, d.worldId, d.cols, d.polys, d.verts, d.faces,
                     d.indices, d.edges, d.localAabb, d.polyInradius, d.childShapes, d.vpXY, d.vpZ, d.polyPack, d.subPairs, d.subCount, d.subOffset, d.aabbMin, d.aabbMax, d.smallSlot,
                     d.largeStart, d.largeList, d.sapSmall, d.sapLarge, d.sapSorted, d.sapCount, d.sapOffset, d.keys, d.vals, d.keysAlt, d.valsAlt, d.cellTable,
-                    d.pairs, d.contacts, d.manifoldFlag, d.pairSep, d.npFast, d.npSlow, d.npDefer, d.npCand, d.manifoldScan,
+                    d.pairs, d.contacts, d.manifoldFlag, d.pairSep, d.npFast, d.npSlow, d.npDefer, d.npDefer2, d.npDefer3, d.npCand, d.manifoldScan,
                     d.manifoldPair,
                     d.incKeys, d.incVals, d.incKeysAlt, d.incValsAlt, d.bodyIncStart,
                     d.bodyIncEnd, d.rows, d.manifoldHdr, d.incLin, d.incAng, d.avgLin, d.avgAng,
@@ -675,6 +675,8 @@ static int ensure_capacity(b3World w) {
         B3_TRY(dalloc(d.npFast, c));
         B3_TRY(dalloc(d.npSlow, c));
         B3_TRY(dalloc(d.npDefer, c));
+        B3_TRY(dalloc(d.npDefer2, c));
+        B3_TRY(dalloc(d.npDefer3, c));
         B3_TRY(dalloc(d.npCand, (size_t)std::min<size_t>(c, b3::kNpCandSlots) * 32));
         B3_TRY(dalloc(d.manifoldScan, c));
         B3_TRY(dalloc(d.manifoldPair, c));

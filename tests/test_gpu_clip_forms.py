@@ -1,10 +1,13 @@
-"""The FP32 clip by eight-lane groups gives the warp clip's results bit for bit.
+"""The narrowphase stages by eight-lane groups give the warp kernels' results bit for bit.
 
 k_np_clip_groups runs face selection, Sutherland-Hodgman clipping, the
 depth filter, the contact reduction and the Contact4 write of four pairs per
 warp, eight lanes each, with the arithmetic of k_np_clip (warp per pair);
 pairs whose faces or clipped polygon exceed its 16-vertex tables are passed
-to k_np_clip. The two forms (b3_set_tuning index 9) must give the same
+to k_np_clip. k_np_refine_groups and k_np_exact_groups do the same for the
+float-float ranking of up to 8 near-tied axes and for the float-float clip
+of pairs whose FP32 clip was in doubt, passing the rest to k_np_refine and
+k_np_exact. The two forms (b3_set_tuning index 9) must give the same
 state bits step after step, on the parity scenes, on the compound and mesh
 sub-pairs, and on prism columns built to reach the hand-over: 20-gon caps
 resting on 20-gon caps (faces of 20 vertices) and 12-gon caps turned by 15
@@ -68,6 +71,9 @@ CASES = {
     "mesh_terrain": (lambda: scenes.mesh_terrain(), 60),
     "prism_columns": (_prism_columns, 30),
     "prism_columns_aligned": (lambda: _prism_columns(aligned=True), 30),
+    # resting, nearly aligned cubes: the float-float ranking and clip stages
+    # carry many pairs
+    "cube_lattice": (lambda: scenes.c5(dims=(24, 8, 24), steps=24), 24),
 }
 
 
@@ -95,6 +101,8 @@ def test_clip_forms_agree_bitwise(ctx, name):
     assert c0 == c1
     for a, b in zip(s0, s1):
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    if name == "cube_lattice":
+        assert c0["refinedAxes"] > 100 and c0["refinedClips"] > 100
 
 
 def test_prism_contacts_match_oracle_in_both_forms(ctx):
