@@ -312,8 +312,12 @@ def run_b3(args, world_size, local_rank):
         w.stepSimulation(1, stream=st.cuda_stream)
     done += args.warmup
     barrier()
+    if args.profile_window:
+        torch.cuda.profiler.start()
     with ClockSampler(local_rank) as clk:
         ms = time_steps(w, args.steps, st, flush)
+    if args.profile_window:
+        torch.cuda.profiler.stop()
     barrier()
     ms = max_over_ranks(ms)
     done += args.steps
@@ -737,6 +741,9 @@ def main():
                          "pair CTA, Jacobi CTA, -, Jacobi blocks per SM, -, Jacobi mode, Jacobi gather[, pair search "
                          "form[, clip form]]) instead of "
                          "autotuning, e.g. to repeat a plain run's shapes under a profiler")
+    ap.add_argument("--profile-window", action="store_true",
+                    help="bracket the settled window's timed steps with cudaProfilerStart / cudaProfilerStop, so that "
+                         "a profiler started with --profile-from-start off sees those launches only")
     ap.add_argument("--sap", action="store_true",
                     help="sweep-and-prune broadphase (pipeline2's default) in place of the grid; single-world workloads")
     ap.add_argument("--solver", default="jacobi", choices=["jacobi", "gs"],
