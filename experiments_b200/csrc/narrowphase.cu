@@ -372,7 +372,7 @@ __device__ __forceinline__ int sweep_axes(PairCtx& c, const b3::ShapesDev& S, in
     // largest projected coordinate); edge axes add a term inversely
     // proportional to |e0 x e1| (their normalisation amplifies rounding)
     const float delta = 1e-6f * scale;
-    // kEarlyFaces, hulls with more than two lane-rounds of faces: first
+    // kEarlyFaces, pairs with more than one lane-round of faces: first
     // test the face of A and the face of B best aligned with D (the
     // likeliest separating axes), with the warp splitting the vertices. A
     // separating face axis rejects the pair whichever face it is, and each
@@ -380,7 +380,7 @@ __device__ __forceinline__ int sweep_axes(PairCtx& c, const b3::ShapesDev& S, in
     // rejection here is the full pass' own verdict. (A template switch: the
     // launch picks it only for shape sets with such hulls, as its code
     // costs the cube-only sweeps a few per cent.)
-    if (kEarlyFaces && nFace > 64) {
+    if (kEarlyFaces && nFace > 32) {
         const int FA = pa.numFaces;
         float bA = -1.f, bB = -1.f;
         int iA = kNone, iB = kNone;
