@@ -1653,27 +1653,22 @@ k_np_clip(const int2* __restrict__ pairs, const int4* __restrict__ subs, b3::Bod
 // which redoes it from the start; a pair whose clip faces tie goes to the
 // float-float stage, as from the warp kernel.
 // ---------------------------------------------------------------------------
-constexpr int kClipGroup = 8;                // lanes per pair (the float-float stages; the FP32 clip: 8 or 4)
+constexpr int kClipGroup = 8;                // lanes per pair
 constexpr int kGroupPoly = 2 * kClipGroup;   // vertex capacity of a group's polygons and face tables
 
-// Per-group scratch of the FP32 clip by groups of G lanes: tables of 2G
-// vertices.
-template <int G>
-struct __align__(16) GroupScratchT {
-    FfVert poly[2][2 * G];
-    float4 sideN[2 * G];
-    float4 sideP[2 * G];
-    float4 incV[2 * G];
+struct __align__(16) GroupScratch {
+    FfVert poly[2][kGroupPoly];
+    float4 sideN[kGroupPoly];
+    float4 sideP[kGroupPoly];
+    float4 incV[kGroupPoly];
     PairCtx ctx;
     ClipGeom geom;
     PairPre pre;
 };
 
-template <int G = kClipGroup>
-__device__ __forceinline__ int grp_lane() { return threadIdx.x & (G - 1); }
-template <int G = kClipGroup>
+__device__ __forceinline__ int grp_lane() { return threadIdx.x & (kClipGroup - 1); }
 __device__ __forceinline__ unsigned grp_mask() {
-    return ((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1));
+    return ((1u << kClipGroup) - 1u) << ((threadIdx.x & 31) & ~(kClipGroup - 1));
 }
 __device__ __forceinline__ float grp_max(float v, unsigned m) {
     return fkey_inv(__reduce_max_sync(m, fkey(v, kNanMax)));
@@ -1689,17 +1684,16 @@ __device__ __forceinline__ void grp_argmin(float& v, int& idx, unsigned m) {
 // select_face over the group's lanes; faces within the window of the FP32
 // extreme only set *tied (the pair then goes to the float-float stage,
 // which decides them).
-template <int G = kClipGroup>
 __device__ __noinline__ int select_face_g(const b3::ShapesDev& S, const PairCtx& c, bool sideA, float3 sepf,
                                           float sign, bool* tied) {
     const b3ConvexPolyhedron& h = sideA ? *c.pa : *c.pb;
     const Mat3& R = sideA ? c.RA : c.RB;
-    const int gl = grp_lane<G>();
-    const unsigned gm = grp_mask<G>();
+    const int gl = grp_lane();
+    const unsigned gm = grp_mask();
     float bv = FLT_MAX;
     int bi = kNone;
     float d0 = FLT_MAX;  // this lane's first face
-    for (int f = gl; f < h.numFaces; f += G) {
+    for (int f = gl; f < h.numFaces; f += kClipGroup) {
         const float4 pl = __ldg((const float4*)&S.faces[h.faceOffset + f].plane[0]);
         const float d = sign * dot(mul(R, make_float3(pl.x, pl.y, pl.z)), sepf);
         if (f == gl) d0 = d;
@@ -1711,11 +1705,11 @@ __device__ __noinline__ int select_face_g(const b3::ShapesDev& S, const PairCtx&
     if (wi == kNone) return kNone;
     const float lim = wv + 4e-6f;
     int inWin;
-    if (h.numFaces <= G) {
+    if (h.numFaces <= kClipGroup) {
         inWin = __popc(__ballot_sync(gm, d0 <= lim));
     } else {
         inWin = 0;
-        for (int f = gl; f < h.numFaces; f += G) {
+        for (int f = gl; f < h.numFaces; f += kClipGroup) {
             const float4 pl = __ldg((const float4*)&S.faces[h.faceOffset + f].plane[0]);
             if (sign * dot(mul(R, make_float3(pl.x, pl.y, pl.z)), sepf) <= lim) ++inWin;
         }
@@ -1727,18 +1721,17 @@ __device__ __noinline__ int select_face_g(const b3::ShapesDev& S, const PairCtx&
 
 // clip_poly_f32 over the group; *over when the output exceeds kGroupPoly
 // (nothing past it is written).
-template <int GL>
 __device__ __noinline__ int clip_poly_f32_g(const ClipGeom& G, const FfVert* in, int nin, int k, FfVert* out,
                                             bool* bad, bool* over) {
-    const int gl = grp_lane<GL>();
-    const unsigned gm = grp_mask<GL>();
+    const int gl = grp_lane();
+    const unsigned gm = grp_mask();
     float3 pn, ap;
     side_plane(G, k, pn, ap);
     const float pnl = len_ub(pn);
     const float apl = len_ub(ap);
     const unsigned newTag = (unsigned)(kPlaneTag + k);
     int total = 0;
-    for (int base = 0; base < nin; base += GL) {
+    for (int base = 0; base < nin; base += kClipGroup) {
         const int ve = base + gl;
         int cnt = 0;
         float3 o0 = make_float3(0.f, 0.f, 0.f), o1 = o0;
@@ -1777,22 +1770,21 @@ __device__ __noinline__ int clip_poly_f32_g(const ClipGeom& G, const FfVert* in,
         const unsigned b1 = __ballot_sync(gm, cnt >= 1), b2 = __ballot_sync(gm, cnt == 2);
         const unsigned below = b3dev::lanemask_lt();
         const int pos = total + __popc(b1 & below) + __popc(b2 & below);
-        if (cnt >= 1 && pos < 2 * GL) put_tagged(out[pos], o0, t0, r0);
-        if (cnt == 2 && pos + 1 < 2 * GL) put_tagged(out[pos + 1], o1, t1, r1);
+        if (cnt >= 1 && pos < kGroupPoly) put_tagged(out[pos], o0, t0, r0);
+        if (cnt == 2 && pos + 1 < kGroupPoly) put_tagged(out[pos + 1], o1, t1, r1);
         total += __popc(b1) + __popc(b2);
     }
     __syncwarp(gm);
-    if (total > 2 * GL) *over = true;
-    return min(total, 2 * GL);
+    if (total > kGroupPoly) *over = true;
+    return min(total, kGroupPoly);
 }
 
 // clip_f32 over the group. *defer: a face or the clipped polygon exceeds the
 // group's tables (nothing is decided; the warp kernel redoes the pair).
-template <int GL>
 __device__ __noinline__ int clip_f32_g(const PairCtx& c, const b3::ShapesDev& S, const NpParams& P, int ai, int bi,
-                                       GroupScratchT<GL>& W, int* outBuf, bool* doubt, bool* defer) {
-    const int gl = grp_lane<GL>();
-    const unsigned gm = grp_mask<GL>();
+                                       GroupScratch& W, int* outBuf, bool* doubt, bool* defer) {
+    const int gl = grp_lane();
+    const unsigned gm = grp_mask();
     const b3ConvexPolyhedron& pa = *c.pa;
     const b3ConvexPolyhedron& pb = *c.pb;
     if (ai == kNone || bi == kNone) return 0;
@@ -1818,28 +1810,28 @@ __device__ __noinline__ int clip_f32_g(const PairCtx& c, const b3::ShapesDev& S,
     const ClipGeom& G = W.geom;
     int nIn = G.fB.numIndices;
     const int nvA = G.fA.numIndices;
-    if (nIn > 2 * GL || nvA > 2 * GL) {
+    if (nIn > kGroupPoly || nvA > kGroupPoly) {
         *defer = true;
         return 0;
     }
-    for (int k = gl; k < nIn; k += GL) {
+    for (int k = gl; k < nIn; k += kClipGroup) {
         const float4 v = __ldg(&S.verts[pb.vertexOffset + S.indices[G.fB.indexOffset + k]]);
         W.incV[k] = f4(mul(c.RB, f3(v)) + G.rel);
     }
-    for (int k = gl; k < nvA; k += GL) {
+    for (int k = gl; k < nvA; k += kClipGroup) {
         const float4 a = __ldg(&S.verts[pa.vertexOffset + S.indices[G.fA.indexOffset + k]]);
         const float4 b = __ldg(&S.verts[pa.vertexOffset + S.indices[G.fA.indexOffset + (k + 1) % nvA]]);
         W.sideN[k] = f4(-cross(mul(c.RA, make_float3(a.x - b.x, a.y - b.y, a.z - b.z)), G.nAw));
         W.sideP[k] = f4(mul(c.RA, f3(a)));
     }
     __syncwarp(gm);
-    for (int k = gl; k < nIn; k += GL)
+    for (int k = gl; k < nIn; k += kClipGroup)
         put_tagged(W.poly[0][k], inc_vertex(G, k), tag2((k + nIn - 1) % nIn, k));
     __syncwarp(gm);
     bool bad = false, over = false;
     int cur = 0;
     for (int e0 = 0; e0 < nvA && !over; ++e0) {
-        nIn = clip_poly_f32_g<GL>(G, W.poly[cur], nIn, e0, W.poly[cur ^ 1], &bad, &over);
+        nIn = clip_poly_f32_g(G, W.poly[cur], nIn, e0, W.poly[cur ^ 1], &bad, &over);
         cur ^= 1;
     }
     if (over) {
@@ -1849,7 +1841,7 @@ __device__ __noinline__ int clip_f32_g(const PairCtx& c, const b3::ShapesDev& S,
     const float3 nAw = G.nAw;
     const b3Face& fA = G.fA;
     int total = 0;
-    for (int base = 0; base < nIn; base += GL) {
+    for (int base = 0; base < nIn; base += kClipGroup) {
         const int k = base + gl;
         bool keep = false;
         float3 p = make_float3(0.f, 0.f, 0.f);
@@ -1876,15 +1868,14 @@ __device__ __noinline__ int clip_f32_g(const PairCtx& c, const b3::ShapesDev& S,
 }
 
 // reduce_f32 over the group, for n <= kGroupPoly points (two per lane).
-template <int G = kClipGroup>
 __device__ __noinline__ int4 reduce_f32_g(const FfVert* p, int n, float3 nearNormal, bool* tie) {
-    const int gl = grp_lane<G>();
-    const unsigned gm = grp_mask<G>();
+    const int gl = grp_lane();
+    const unsigned gm = grp_mask();
     const float3 o = get_f32(p[0]);
     float3 s = make_float3(0.f, 0.f, 0.f);
-    for (int k = gl; k < n; k += G) s += get_f32(p[k]) - o;
+    for (int k = gl; k < n; k += kClipGroup) s += get_f32(p[k]) - o;
 #pragma unroll
-    for (int q = G / 2; q > 0; q >>= 1) {
+    for (int q = kClipGroup / 2; q > 0; q >>= 1) {
         s.x += __shfl_xor_sync(gm, s.x, q);
         s.y += __shfl_xor_sync(gm, s.y, q);
         s.z += __shfl_xor_sync(gm, s.z, q);
@@ -1897,7 +1888,7 @@ __device__ __noinline__ int4 reduce_f32_g(const FfVert* p, int n, float3 nearNor
     u = normalize(u);
     v = normalize(v);
     float pm = 0.f, rm = 0.f;
-    for (int k = gl; k < n; k += G) {
+    for (int k = gl; k < n; k += kClipGroup) {
         const float3 q = get_f32(p[k]);
         pm = fmaxf(pm, len_ub(q));
         rm = fmaxf(rm, len_ub((q - o) - cr));
@@ -1909,10 +1900,10 @@ __device__ __noinline__ int4 reduce_f32_g(const FfVert* p, int n, float3 nearNor
     float fw[2], fu[2], fv[2];
     float mw = FLT_MAX, f0 = FLT_MIN, f1 = FLT_MIN, f2 = FLT_MIN, f3v = FLT_MIN;
     int iw = kNone, i0 = kNone, i1 = kNone, i2 = kNone, i3 = kNone;
-    const int nj = n > G ? 2 : 1;
+    const int nj = n > kClipGroup ? 2 : 1;
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
-        const int k = gl + G * j;
+        const int k = gl + kClipGroup * j;
         fw[j] = FLT_MAX; fu[j] = 0.f; fv[j] = 0.f;
         if (j < nj && k < n) {
             const float3 r = (get_f32(p[k]) - o) - cr;
@@ -1936,7 +1927,7 @@ __device__ __noinline__ int4 reduce_f32_g(const FfVert* p, int n, float3 nearNor
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
         if (j >= nj) break;
-        const bool ok = gl + G * j < n;
+        const bool ok = gl + kClipGroup * j < n;
         cw += __popc(__ballot_sync(gm, ok && fw[j] <= mw + gapw));
         c0 += __popc(__ballot_sync(gm, ok && fu[j] <= f0 + gap));
         c1 += __popc(__ballot_sync(gm, ok && -fu[j] <= f1 + gap));
@@ -1952,11 +1943,10 @@ __device__ __noinline__ int4 reduce_f32_g(const FfVert* p, int n, float3 nearNor
 }
 
 // emit_contact by the group's lanes
-template <int G = kClipGroup>
 __device__ __forceinline__ void emit_contact_g(int p, const PairCtx& c, const FfVert* pts, int nRed, int4 idx,
                                                float3 nrm, const b3::BodiesDev& Bd, const NpParams& P,
                                                b3Contact4* __restrict__ contacts, uint32_t* __restrict__ manifoldFlag) {
-    const int gl = grp_lane<G>();
+    const int gl = grp_lane();
     b3Contact4* out = &contacts[p];
     if (gl < nRed) {
         const int k = gl == 0 ? idx.x : gl == 1 ? idx.y : gl == 2 ? idx.z : idx.w;
@@ -1966,7 +1956,7 @@ __device__ __forceinline__ void emit_contact_g(int p, const PairCtx& c, const Ff
     } else if (gl < 4) {
         *reinterpret_cast<float4*>(&out->worldPos[gl][0]) = make_float4(0.f, 0.f, 0.f, 0.f);
     }
-    if (gl == (G > 4 ? 4 : 0)) {  // the header: a lane past the points where there is one
+    if (gl == 4) {
         *reinterpret_cast<float4*>(&out->worldNormal[0]) = make_float4(nrm.x, nrm.y, nrm.z, (float)nRed);
         out->friction = combine_friction(Bd.friction[c.A], Bd.friction[c.B], P.frictionCombine);
         out->pairIndex = p;
@@ -1976,23 +1966,23 @@ __device__ __forceinline__ void emit_contact_g(int p, const PairCtx& c, const Ff
     }
 }
 
-// Stage 2 by lane groups of G lanes over the clip queue: 32 / G pairs per
-// warp per work grab, lane l prefetching group l's pair. Pairs the groups
-// cannot hold go to deferQ for k_np_clip.
-template <bool kSub, int G>
+// Stage 2 by lane groups over the clip queue: four pairs per warp per work
+// grab, lane l < 4 prefetching group l's pair. Pairs the groups cannot hold
+// go to deferQ for k_np_clip.
+template <bool kSub>
 __global__ void __launch_bounds__(128, 4)
 k_np_clip_groups(const int2* __restrict__ pairs, const int4* __restrict__ subs, b3::BodiesDev Bd, b3::ShapesDev S,
                  NpParams P, float4* __restrict__ pairSep, const int* __restrict__ fastQ, int* __restrict__ slowQ,
                  int* __restrict__ deferQ, b3Contact4* __restrict__ contacts, uint32_t* __restrict__ manifoldFlag,
                  int32_t* __restrict__ scalars) {
     extern __shared__ __align__(16) unsigned char np_smem[];
-    constexpr int kPerWarp = 32 / G;
+    constexpr int kPerWarp = 32 / kClipGroup;
     const int lane = threadIdx.x & 31;
-    GroupScratchT<G>* Wg = reinterpret_cast<GroupScratchT<G>*>(np_smem) + (threadIdx.x >> 5) * kPerWarp;
-    const int g = lane / G;
-    const int gl = grp_lane<G>();
-    const unsigned gm = grp_mask<G>();
-    GroupScratchT<G>& W = Wg[g];
+    GroupScratch* Wg = reinterpret_cast<GroupScratch*>(np_smem) + (threadIdx.x >> 5) * kPerWarp;
+    const int g = lane / kClipGroup;
+    const int gl = grp_lane();
+    const unsigned gm = grp_mask();
+    GroupScratch& W = Wg[g];
     const int nFast = scalars[b3::S_NP_FAST];
     for (;;) {
         const int chunk = next_work(scalars + b3::S_NP_WORK2, nFast, kPerWarp);
@@ -2017,17 +2007,17 @@ k_np_clip_groups(const int2* __restrict__ pairs, const int4* __restrict__ subs, 
             const float4 s4 = W.pre.aux;
             const float3 sepf = make_float3(s4.x, s4.y, s4.z);
             bool faceTie = false;
-            const int bi = select_face_g<G>(S, c, false, sepf, -1.f, &faceTie);
-            const int ai = select_face_g<G>(S, c, true, sepf, 1.f, &faceTie);
+            const int bi = select_face_g(S, c, false, sepf, -1.f, &faceTie);
+            const int ai = select_face_g(S, c, true, sepf, 1.f, &faceTie);
             int buf = 0;
             bool slow = false, defer = false;
             int nOut = 0;
-            if (!faceTie && ref_face_clips(S, c, ai)) nOut = clip_f32_g<G>(c, S, P, ai, bi, W, &buf, &slow, &defer);
+            if (!faceTie && ref_face_clips(S, c, ai)) nOut = clip_f32_g(c, S, P, ai, bi, W, &buf, &slow, &defer);
             int4 idx = make_int4(0, 1, 2, 3);
             int nRed = nOut;
             bool tie = false;
             if (!defer && !faceTie && !slow && nOut > 4) {
-                idx = reduce_f32_g<G>(W.poly[buf], nOut, -sepf, &tie);
+                idx = reduce_f32_g(W.poly[buf], nOut, -sepf, &tie);
                 nRed = 4;
             }
             if (defer) {
@@ -2038,7 +2028,7 @@ k_np_clip_groups(const int2* __restrict__ pairs, const int4* __restrict__ subs, 
                     slowQ[atomicAdd(scalars + b3::S_NP_SLOW, 1)] = p;
                 }
             } else if (nOut > 0) {
-                emit_contact_g<G>(p, c, W.poly[buf], nRed, idx, -sepf, Bd, P, contacts, manifoldFlag);
+                emit_contact_g(p, c, W.poly[buf], nRed, idx, -sepf, Bd, P, contacts, manifoldFlag);
             } else if (gl == 0) {
                 manifoldFlag[p] = 0u;
             }
@@ -2826,6 +2816,7 @@ static int launch_np_stages(b3World_t* w, cudaStream_t st, const NpParams& P, bo
     B3_CUDA(cudaMemsetAsync(w->d.scalars + S_NP_DEFER, 0, sizeof(int32_t) * 6, st));
     const int threads = 32 * w->npWarpsPerBlock;
     const size_t smem = sizeof(WarpScratch) * w->npWarpsPerBlock;
+    const size_t smemGroups = sizeof(GroupScratch) * (32 / kClipGroup) * w->npWarpsPerBlock;
     auto grid_of = [&](const void* k) -> int {
         int occ = 1;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, threads, smem) != cudaSuccess || occ < 1) occ = 1;
@@ -2871,23 +2862,14 @@ static int launch_np_stages(b3World_t* w, cudaStream_t st, const NpParams& P, bo
     }
     if (tk) B3_CUDA(cudaEventRecord(w->npEv[2], st));
     if (w->clipGroups) {
-        // lane groups over the clip queue (8 lanes, or 4 with clipGroups 2);
-        // what they pass on, by warps
-        const bool four = w->clipGroups == 2;
-        const size_t smemGroups =
-            (four ? sizeof(GroupScratchT<4>) * 8 : sizeof(GroupScratchT<8>) * 4) * w->npWarpsPerBlock;
-        const void* kg = four ? (const void*)k_np_clip_groups<kSub, 4> : (const void*)k_np_clip_groups<kSub, 8>;
+        // lane groups over the clip queue; what they pass on, by warps
         int occG = 1;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occG, kg, threads, smemGroups) != cudaSuccess || occG < 1)
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occG, k_np_clip_groups<kSub>, threads, smemGroups) !=
+                cudaSuccess || occG < 1)
             occG = 1;
-        if (four)
-            k_np_clip_groups<kSub, 4><<<w->ctx->numSMs * occG, threads, smemGroups, st>>>(
-                w->d.pairs, w->d.subPairs, Bd, S, P, w->d.pairSep, w->d.npFast, w->d.npSlow, w->d.npDefer,
-                w->d.contacts, w->d.manifoldFlag, sc);
-        else
-            k_np_clip_groups<kSub, 8><<<w->ctx->numSMs * occG, threads, smemGroups, st>>>(
-                w->d.pairs, w->d.subPairs, Bd, S, P, w->d.pairSep, w->d.npFast, w->d.npSlow, w->d.npDefer,
-                w->d.contacts, w->d.manifoldFlag, sc);
+        k_np_clip_groups<kSub><<<w->ctx->numSMs * occG, threads, smemGroups, st>>>(
+            w->d.pairs, w->d.subPairs, Bd, S, P, w->d.pairSep, w->d.npFast, w->d.npSlow, w->d.npDefer,
+            w->d.contacts, w->d.manifoldFlag, sc);
         B3_CHECK_LAUNCH();
         k_np_clip<kSub><<<grid_of((const void*)k_np_clip<kSub>), threads, smem, st>>>(
             w->d.pairs, w->d.subPairs, Bd, S, P, w->d.pairSep, w->d.npDefer, S_NP_DEFER, S_NP_WORK5, w->d.npSlow,
@@ -2949,14 +2931,13 @@ int launch_narrowphase(b3World_t* w, cudaStream_t st) {
         B3_CUDA(cudaFuncSetAttribute(k_np_exact<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         B3_CUDA(cudaFuncSetAttribute(k_np_refine<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     }
-    // both lane-group clip widths, whichever the tuning selects later
-    const size_t smemGroups =
-        std::max(sizeof(GroupScratchT<4>) * 8, sizeof(GroupScratchT<8>) * 4) * w->npWarpsPerBlock;
+    const size_t smemGroups = sizeof(GroupScratch) * (32 / kClipGroup) * w->npWarpsPerBlock;
     if (smemGroups > 48 * 1024 && (size_t)w->npGroupSmemAttr < smemGroups) {
         w->npGroupSmemAttr = (int)smemGroups;
-        for (const void* k : {(const void*)k_np_clip_groups<false, 8>, (const void*)k_np_clip_groups<true, 8>,
-                              (const void*)k_np_clip_groups<false, 4>, (const void*)k_np_clip_groups<true, 4>})
-            B3_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemGroups));
+        B3_CUDA(cudaFuncSetAttribute(k_np_clip_groups<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smemGroups));
+        B3_CUDA(cudaFuncSetAttribute(k_np_clip_groups<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smemGroups));
     }
     const size_t smemFF = sizeof(GroupScratchFF) * (32 / kClipGroup) * w->npWarpsPerBlock;
     if (smemFF > 48 * 1024 && (size_t)w->npFFSmemAttr < smemFF) {

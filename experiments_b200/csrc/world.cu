@@ -1409,7 +1409,7 @@ extern "C" int b3_autotune(b3World w, int trialSteps, void* stream) {
     // The Jacobi launch shapes interact (a one-knob-at-a-time descent stops
     // in a local optimum), so they are searched jointly below on the solve
     // alone.
-    Knob knobs[] = {{&w->npWarpsPerBlock, 3, {1, 2, 4}}, {&w->clipGroups, 3, {0, 1, 2}}, {&w->solverMode, 2, {0, 1, 0}}};
+    Knob knobs[] = {{&w->npWarpsPerBlock, 3, {1, 2, 4}}, {&w->clipGroups, 2, {0, 1, 0}}, {&w->solverMode, 2, {0, 1, 0}}};
     const int numKnobs = w->gs ? 3 : 2;
     // one solve from the current contacts, timed (the solve leaves the body
     // state alone: the finish happens in the integration)
@@ -1533,7 +1533,7 @@ extern "C" int b3_set_tuning(b3World w, const int* values, int count) {
     const int clipG = count >= 10 ? values[9] : w->clipGroups;
     if ((np != 1 && np != 2 && np != 4) || (st != 64 && st != 128 && st != 256) || cap < 1 || cap > 8 ||
         (mode != 0 && mode != 1) || (gather != 0 && gather != 1) || (pairMode != 0 && pairMode != 1) ||
-        (clipG < 0 || clipG > 2))
+        (clipG != 0 && clipG != 1))
         return B3_ERR_INVALID_ARG;
     w->npWarpsPerBlock = np;
     w->solverThreads = st;

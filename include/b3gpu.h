@@ -614,18 +614,17 @@ int b3_autotune(b3World w, int trialSteps, void* stream);
  * body-average gather (0 = one copy at a time, 1 = four loads in flight;
  * bit-identical results), grid pair search form (0 = one thread per body
  * over its 27 cells, 1 = one warp per body, a lane per cell; the same pair
- * list and overflow counts bit for bit), narrowphase lane groups (0 = one
- * warp per pair in the clip and float-float stages; 1 = eight-lane groups,
- * four pairs per warp, in those stages; 2 = the same with four-lane groups,
- * eight pairs per warp, for the FP32 clip; the warp form takes the pairs
- * that do not fit a group's tables; bit-identical results). */
+ * list and overflow counts bit for bit), FP32 clip form (0 = one warp per
+ * pair, 1 = eight-lane groups, four pairs per warp, with the warp form for
+ * pairs whose faces or clipped polygon exceed 16 vertices; bit-identical
+ * results). */
 int b3_get_tuning(b3World w, int* values, int max, int* count);
 /* Set the tunables in b3_get_tuning's order (count >= 3; the pair-search
  * CTA size, the launch count and the trial count are read-only, indices 4,
  * 6, 7, 8 and 9 are optional):
  * narrowphase warps per CTA 1/2/4, Jacobi CTA size 64/128/256, Jacobi
  * blocks per SM cap 1..8, Jacobi mode 0/1, Jacobi gather 0/1, pair search
- * form 0/1, lane groups 0/1/2. */
+ * form 0/1, clip form 0/1. */
 int b3_set_tuning(b3World w, const int* values, int count);
 
 /* ------------------------------------------------------------------ */

@@ -167,12 +167,12 @@ def test_autotune_keeps_state_and_results(ctx):
     for x, y in zip(before, after):
         assert np.array_equal(x, y)
     t = a.tuning()
-    # trials: 3 narrowphase CTA sizes, 3 lane-group forms, 2 pair search
-    # forms, then the Jacobi shapes jointly (grid mode: 3 CTA sizes x 4 caps
-    # x 2 gathers; per-world mode: 3 x 2)
-    assert t[5] == 3 + 3 + 2 + 24 + 6
+    # trials: 3 narrowphase CTA sizes, 2 clip forms, 2 pair search forms,
+    # then the Jacobi shapes jointly (grid mode: 3 CTA sizes x 4 caps x 2
+    # gathers; per-world mode: 3 x 2)
+    assert t[5] == 3 + 2 + 2 + 24 + 6
     assert t[0] in (1, 2, 4) and t[6] in (0, 1) and t[2] in (64, 128, 256) and t[4] in (1, 2, 4, 8)
-    assert t[7] in (0, 1) and t[8] in (0, 1) and t[9] in (0, 1, 2)
+    assert t[7] in (0, 1) and t[8] in (0, 1) and t[9] in (0, 1)
     a.stepSimulation(10)
     b.stepSimulation(10)
     for x, y in zip(a.read_state(), b.read_state()):
