@@ -599,7 +599,7 @@ class PhysicsWorld:
     def tuning(self):
         """(narrowphase warps/CTA, pair CTA size, solver CTA size, kernels per
         captured step, Jacobi blocks per SM cap, configurations timed,
-        Jacobi mode, Jacobi gather, grid pair search form, FP32 clip form)."""
+        Jacobi mode, Jacobi gather, grid pair search form, narrowphase lane groups)."""
         v = (C.c_int * 10)()
         cnt = C.c_int()
         _check(self.lib.b3_get_tuning(self.h, v, 10, C.byref(cnt)), "b3_get_tuning")

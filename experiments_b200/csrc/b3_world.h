@@ -231,7 +231,8 @@ struct b3World_t {
                                // batched Gauss-Seidel: grid width 0 = manifolds / 8, 1 = manifolds / 64
     int solverGather = 0;      // Jacobi body averages: 0 = one copy at a time, 1 = four loads in flight
     int pairSearchMode = 0;    // grid pair search: 0 = thread per body, 1 = warp per body
-    int clipGroups = 1;        // FP32 clip: 0 = a warp per pair, 1 = 8-lane groups (warp for what does not fit)
+    int clipGroups = 1;        // clip and float-float stages: 0 = a warp per pair, 1 = 8-lane groups
+                               // (a warp per pair for what does not fit)
     int tunedTrials = 0;       // configurations the autotuner timed
     int npSmemAttr = 0;        // dynamic shared memory attribute set on the narrowphase kernels
     int npGroupSmemAttr = 0;   // the same for the lane-group clip

@@ -592,7 +592,7 @@ int b3_batch_world_stats(b3World w, float* out4, int numWorlds, void* stream);
  * partition worlds across GPUs by body count. */
 int b3_batch_world_offsets(b3World w, int* offsets, int maxWorlds, int* numWorlds);
 /* Autotuner over the launch shapes of the tunable kernels on the current
- * scene: the narrowphase warps per CTA (1/2/4) and the FP32 clip form by
+ * scene: the narrowphase warps per CTA (1/2/4) and the lane-group form by
  * trials of trialSteps eager steps from the same saved state; then the grid
  * pair search form
  * (thread or warp per body), each timed on three searches over the same
@@ -614,9 +614,10 @@ int b3_autotune(b3World w, int trialSteps, void* stream);
  * body-average gather (0 = one copy at a time, 1 = four loads in flight;
  * bit-identical results), grid pair search form (0 = one thread per body
  * over its 27 cells, 1 = one warp per body, a lane per cell; the same pair
- * list and overflow counts bit for bit), FP32 clip form (0 = one warp per
- * pair, 1 = eight-lane groups, four pairs per warp, with the warp form for
- * pairs whose faces or clipped polygon exceed 16 vertices; bit-identical
+ * list and overflow counts bit for bit), narrowphase lane groups (0 = one
+ * warp per pair in the FP32 clip and the float-float stages, 1 = eight-lane
+ * groups there, four pairs per warp, with the warp form for pairs that do
+ * not fit a group's 16-vertex tables or 8 candidates; bit-identical
  * results). */
 int b3_get_tuning(b3World w, int* values, int max, int* count);
 /* Set the tunables in b3_get_tuning's order (count >= 3; the pair-search
@@ -624,7 +625,7 @@ int b3_get_tuning(b3World w, int* values, int max, int* count);
  * 6, 7, 8 and 9 are optional):
  * narrowphase warps per CTA 1/2/4, Jacobi CTA size 64/128/256, Jacobi
  * blocks per SM cap 1..8, Jacobi mode 0/1, Jacobi gather 0/1, pair search
- * form 0/1, clip form 0/1. */
+ * form 0/1, lane groups 0/1. */
 int b3_set_tuning(b3World w, const int* values, int count);
 
 /* ------------------------------------------------------------------ */
