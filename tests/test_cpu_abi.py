@@ -115,6 +115,33 @@ def test_invalid_arguments_are_reported(host_ctx):
     w.close()
 
 
+def test_tuning_values_round_trip_and_are_checked(host_ctx):
+    """b3_get_tuning / b3_set_tuning are host state: ten values (index 8 the
+    grid pair search form, index 9 the narrowphase lane-group form), the
+    read-only ones ignored on set, every out-of-range value refused."""
+    w = b3.PhysicsWorld(host_ctx, b3.default_config())
+    t = w.tuning()
+    assert len(t) == 10
+    assert t[8] in (0, 1) and t[9] in (0, 1)
+    want = [4, t[1], 64, t[3], 2, t[5], 1, 1, 1, 0]
+    w.set_tuning(want)
+    got = w.tuning()
+    for i in (0, 2, 4, 6, 7, 8, 9):
+        assert got[i] == want[i], i
+    # shorter lists keep the later values
+    w.set_tuning([2, t[1], 128])
+    got2 = w.tuning()
+    assert got2[0] == 2 and got2[2] == 128 and got2[8] == 1 and got2[9] == 0
+    lib = b3.load()
+    for i, bad in ((0, 3), (2, 96), (4, 0), (4, 9), (6, 2), (7, 2), (8, 2), (9, 2), (9, -1)):
+        v = list(got2)
+        v[i] = bad
+        arr = (C.c_int * len(v))(*v)
+        assert lib.b3_set_tuning(w.h, arr, len(v)) == 1, (i, bad)  # B3_ERR_INVALID_ARG
+    assert w.tuning() == got2  # a refused set changes nothing
+    w.close()
+
+
 def test_scene_generator_is_deterministic():
     a = scenes.c2(dims=(4, 2, 4))
     b = scenes.c2(dims=(4, 2, 4))
